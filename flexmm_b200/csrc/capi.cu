@@ -1,0 +1,318 @@
+// C-ABI entry points (include/flexmm_b200.h): operator sets, plans, passes.
+#include <string.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/flexmm_b200.h"
+#include "fmm.cuh"
+
+using namespace fmmb;
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(const Error &e) {
+  g_last_error = e.what();
+  return e.code;
+}
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    f();
+    return FMM_OK;
+  } catch (const Error &e) {
+    return fail(e);
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return FMM_ERR_INVALID_ARGUMENT;
+  }
+}
+
+struct LevelEntry {
+  DevBuf<double> buf;
+  LevelOpsDev dev;
+};
+
+int pad8(int n) { return (n + 7) & ~7; }
+
+// Keep freed stream-ordered allocations in this process's default pool, so
+// that plans created repeatedly reuse device memory instead of returning it
+// to the driver at every synchronisation.
+void retain_pool_memory() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  static thread_local int done_for = -1;
+  if (done_for == dev) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = ~uint64_t(0);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done_for = dev;
+}
+}  // namespace
+
+struct fmm_ops {
+  int kernel_id;
+  KernelParams kp;
+  int neq, np;
+  std::vector<std::unique_ptr<LevelEntry>> levels;
+};
+
+struct fmm_plan {
+  fmm_ops *ops;
+  cudaStream_t stream;
+  TreeDev td;
+  TreeHost th;
+  std::vector<int> bound;  // per level: ops entry id or -1
+  DevBuf<LevelOpsDev> ops_dev;
+  DevBuf<double> tau_s, mult, ple, loc;
+  bool have_expansions = false;
+};
+
+extern "C" {
+
+const char *fmm_last_error(void) { return g_last_error.c_str(); }
+
+int fmm_ops_create(int kernel_id, const double *kparams, int nequiv, fmm_ops **out) {
+  return guarded([&] {
+    FMMB_CHECK(out, ERR_INVALID_ARGUMENT, "out is NULL");
+    FMMB_CHECK(kernel_id == KERNEL_LAPLACE, ERR_UNSUPPORTED, "unknown kernel id");
+    FMMB_CHECK(nequiv >= 1 && nequiv <= FMM_MAX_NEQUIV, ERR_INVALID_ARGUMENT,
+               "nequiv must be in [1, 64]");
+    auto *o = new fmm_ops();
+    o->kernel_id = kernel_id;
+    for (int i = 0; i < 4; ++i) o->kp.p[i] = kparams ? kparams[i] : 0.0;
+    o->neq = nequiv;
+    o->np = pad8(nequiv);
+    *out = o;
+  });
+}
+
+int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
+  return guarded([&] {
+    FMMB_CHECK(ops && lv && level_id, ERR_INVALID_ARGUMENT, "NULL argument");
+    const int n = ops->neq, np = ops->np;
+    // host staging in the padded device layout
+    std::vector<double> h;
+    auto take = [&](size_t count) {
+      size_t at = h.size();
+      h.resize(at + ((count + 1) & ~size_t(1)), 0.0);  // keep 16-byte alignment
+      return at;
+    };
+    const size_t o_lx = take(np), o_ly = take(np), o_u = take(size_t(np) * np), o_s = take(np),
+                 o_vh = take(size_t(np) * np), o_m2mct = take(size_t(4) * np * np),
+                 o_m2mc = take(size_t(4) * np * np);
+    for (int k = 0; k < n; ++k) {
+      h[o_lx + k] = lv->large_x[k];
+      h[o_ly + k] = lv->large_y[k];
+      h[o_s + k] = lv->c2e_sinv[k];
+    }
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < n; ++k) {
+        h[o_u + size_t(i) * np + k] = lv->c2e_u[size_t(i) * n + k];
+        h[o_vh + size_t(i) * np + k] = lv->c2e_vh[size_t(i) * n + k];
+      }
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < n; ++k) {
+          const double v = lv->m2mc[size_t(i) * 4 * n + c * n + k];
+          h[o_m2mct + size_t(c * np + k) * np + i] = v;   // [4np x np]
+          h[o_m2mc + size_t(i) * 4 * np + c * np + k] = v;  // [np x 4np]
+        }
+    size_t o_m2l[FMM_N_OFFSETS];
+    int kind[FMM_N_OFFSETS], rp[FMM_N_OFFSETS];
+    for (int o = 0; o < FMM_N_OFFSETS; ++o) {
+      const int r = lv->m2l_rank[o];
+      o_m2l[o] = 0;
+      rp[o] = 0;
+      if (r == 0) {
+        kind[o] = M2L_NULL;
+      } else if (r < 0) {
+        kind[o] = M2L_DENSE;
+        o_m2l[o] = take(size_t(np) * np);
+        const double *a = lv->m2l_a[o];  // [n x n] (out i, in k); store D^T [k][i]
+        for (int i = 0; i < n; ++i)
+          for (int k = 0; k < n; ++k) h[o_m2l[o] + size_t(k) * np + i] = a[size_t(i) * n + k];
+      } else {
+        FMMB_CHECK(r <= n, ERR_INVALID_ARGUMENT, "M2L rank exceeds nequiv");
+        kind[o] = M2L_SVD;
+        const int p = pad8(r);
+        rp[o] = p;
+        o_m2l[o] = take(size_t(np) * p + size_t(p) * np);
+        const double *m2 = lv->m2l_a[o];  // [n x r]
+        const double *m1 = lv->m2l_b[o];  // [r x n]
+        for (int q = 0; q < r; ++q)
+          for (int k = 0; k < n; ++k) h[o_m2l[o] + size_t(k) * p + q] = m1[size_t(q) * n + k];
+        const size_t base2 = o_m2l[o] + size_t(np) * p;
+        for (int i = 0; i < n; ++i)
+          for (int q = 0; q < r; ++q) h[base2 + size_t(q) * np + i] = m2[size_t(i) * r + q];
+      }
+    }
+    auto e = std::make_unique<LevelEntry>();
+    e->buf.alloc(h.size(), 0);
+    FMMB_CUDA(cudaMemcpy(e->buf.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    double *b = e->buf.get();
+    e->dev.lx = b + o_lx;
+    e->dev.ly = b + o_ly;
+    e->dev.u = b + o_u;
+    e->dev.sinv = b + o_s;
+    e->dev.vh = b + o_vh;
+    e->dev.m2mct = b + o_m2mct;
+    e->dev.m2mc = b + o_m2mc;
+    for (int o = 0; o < FMM_N_OFFSETS; ++o) {
+      e->dev.m2l[o] = kind[o] == M2L_NULL ? nullptr : b + o_m2l[o];
+      e->dev.kind[o] = kind[o];
+      e->dev.rp[o] = rp[o];
+    }
+    ops->levels.push_back(std::move(e));
+    *level_id = int(ops->levels.size()) - 1;
+  });
+}
+
+int fmm_ops_destroy(fmm_ops *ops) {
+  return guarded([&] {
+    if (!ops) return;
+    cudaDeviceSynchronize();
+    delete ops;
+  });
+}
+
+int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
+                    const double *bbox, void *stream, fmm_plan **out) {
+  return guarded([&] {
+    FMMB_CHECK(ops && x && y && bbox && out, ERR_INVALID_ARGUMENT, "NULL argument");
+    retain_pool_memory();
+    auto p = std::make_unique<fmm_plan>();
+    p->ops = ops;
+    p->stream = (cudaStream_t)stream;
+    build_tree(p->td, p->th, x, y, n, ncutoff, bbox, p->stream);
+    p->bound.assign(p->th.L, -1);
+    *out = p.release();
+  });
+}
+
+int fmm_plan_info(fmm_plan *p, int *n_levels, double *widths, int *n_nodes) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    if (n_levels) *n_levels = p->th.L;
+    for (int m = 0; m < p->th.L; ++m) {
+      if (widths) widths[m] = p->th.width[m];
+      if (n_nodes) n_nodes[m] = p->th.off[m + 1] - p->th.off[m];
+    }
+  });
+}
+
+int fmm_plan_bind(fmm_plan *p, int level, int level_id) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(level >= 0 && level < p->th.L, ERR_INVALID_ARGUMENT, "level out of range");
+    FMMB_CHECK(level_id >= 0 && level_id < (int)p->ops->levels.size(), ERR_INVALID_ARGUMENT,
+               "unknown operator entry");
+    p->bound[level] = level_id;
+  });
+}
+
+static PassArgs pass_args(fmm_plan *p) {
+  PassArgs a;
+  a.kernel_id = p->ops->kernel_id;
+  a.kp = p->ops->kp;
+  a.neq = p->ops->neq;
+  a.np = p->ops->np;
+  a.td = &p->td;
+  a.th = &p->th;
+  a.ops_host.assign(p->th.L, LevelOpsDev{});
+  for (int m = 0; m < p->th.L; ++m)
+    if (p->bound[m] >= 0) a.ops_host[m] = p->ops->levels[p->bound[m]]->dev;
+  a.ops_dev = p->ops_dev.get();
+  return a;
+}
+
+int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const TreeHost &th = p->th;
+    for (int m = 2; m < th.L; ++m)
+      FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
+    const int np = p->ops->np;
+    const int64_t total = th.n_total();
+    p->ops_dev.alloc(th.L, s);
+    PassArgs a = pass_args(p);
+    FMMB_CUDA(cudaMemcpyAsync(p->ops_dev.get(), a.ops_host.data(), th.L * sizeof(LevelOpsDev),
+                              cudaMemcpyHostToDevice, s));
+    a.ops_dev = p->ops_dev.get();
+    p->tau_s.alloc(th.n_points, s);
+    gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
+    p->mult.alloc(total * np, s);
+    p->ple.alloc(total * np, s);
+    p->loc.alloc(total * np, s);
+    p->mult.zero(s);
+    p->ple.zero(s);
+    p->loc.zero(s);
+    run_upward(a, p->tau_s.get(), p->mult.get(), s);
+    run_m2l(a, p->mult.get(), p->ple.get(), s);
+    run_downward(a, p->ple.get(), p->loc.get(), s);
+    p->have_expansions = true;
+  });
+}
+
+int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int check,
+                 double *out, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+    FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
+    if (m == 0) return;
+    FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
+    cudaStream_t s = (cudaStream_t)stream;
+    PassArgs a = pass_args(p);
+    DevBuf<uint64_t> tkeys;
+    DevBuf<int> tperm;
+    sort_points(tx, ty, m, p->th, tkeys, tperm, s);
+    DevBuf<double> txs, tys;
+    txs.alloc(m, s);
+    tys.alloc(m, s);
+    gather_sorted(tx, tperm.get(), m, txs.get(), s);
+    gather_sorted(ty, tperm.get(), m, tys.get(), s);
+    run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(), m,
+                 check, out, s);
+  });
+}
+
+int fmm_plan_destroy(fmm_plan *p) {
+  return guarded([&] {
+    if (!p) return;
+    cudaStreamSynchronize(p->stream);
+    delete p;
+  });
+}
+
+int fmm_tree_export(fmm_plan *p, double *xmin, double *ymin, int *bot, int *top, int *parent,
+                    int *child, uint8_t *flags, int *coll, int *il, int *ordv) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    const size_t T = p->th.n_total();
+    cudaStream_t s = p->stream;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+      if (dst && bytes) FMMB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    };
+    cp(xmin, p->td.xmin.get(), T * sizeof(double));
+    cp(ymin, p->td.ymin.get(), T * sizeof(double));
+    cp(bot, p->td.bot.get(), T * sizeof(int));
+    cp(top, p->td.top.get(), T * sizeof(int));
+    cp(parent, p->td.parent.get(), T * sizeof(int));
+    cp(child, p->td.child.get(), T * sizeof(int));
+    cp(flags, p->td.flags.get(), T * sizeof(uint8_t));
+    cp(coll, p->td.coll.get(), T * 9 * sizeof(int));
+    cp(il, p->td.il.get(), T * N_OFFSETS * sizeof(int));
+    cp(ordv, p->td.ordv.get(), size_t(p->th.n_points) * sizeof(int));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

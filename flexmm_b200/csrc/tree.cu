@@ -1,0 +1,597 @@
+// GPU quadtree build, reproducing the reference tree (flexmm/tree.py) box for box.
+//
+// The reference refines level by level, splitting every node with more than
+// `ppl` points (flexmm/tree.py:191-220), then enforces a 2:1 rule by
+// repeatedly splitting leaves with a colleague of subtree depth >= 2
+// (flexmm/tree.py:371-383, 529-541), then gives every leaf with a non-leaf
+// colleague four "fake" children (flexmm/tree.py:385-397, 542-553).
+//
+// Here the same tree is computed without sequential partitioning:
+//  1. every point gets a key of 29 quadrant digits by descending from the
+//     root with the reference's own float64 midpoint arithmetic
+//     (xmid = xmin + half_width, child xmin = xmid - half_width or xmid,
+//     class = 2*(x > xmid) + (y > ymid)), so every comparison is bit-identical;
+//  2. keys are radix-sorted: every box is a contiguous run of sorted keys;
+//  3. the initially split boxes S0 are the key prefixes with more than `ppl`
+//     points, read off the sorted keys (a run starting at i is longer than
+//     ppl iff key i and key i+ppl share the prefix);
+//  4. the 2:1 closure is computed bottom-up as a set: a box is split iff it
+//     is initially split or it neighbours (incl. diagonally) a box with a
+//     split child; the set is grown level by level in a GPU hash set.  This
+//     least fixpoint is the same one the reference's iteration reaches;
+//  5. X-list leaves are the real leaves adjacent to a split box;
+//  6. the parent boxes (split boxes and X-list leaves) are sorted by
+//     (level, morton); each contributes 4 consecutive children, so node
+//     arrays, ranges, colleagues and interaction lists follow from binary
+//     searches in sorted arrays.
+#include <cub/cub.cuh>
+
+#include "tree.cuh"
+
+namespace fmmb {
+namespace {
+
+constexpr int TPB = 256;
+
+struct Counters {
+  unsigned long long s0_count;
+  unsigned long long f_count;
+  unsigned long long x_count;
+  int max_level;
+  int too_deep;
+  int overflow;
+  int pad;
+};
+
+__device__ __forceinline__ int common_digits(uint64_t a, uint64_t b) {
+  uint64_t d = a ^ b;
+  if (d == 0) return MAXD;
+  return (__clzll((long long)d) - (64 - 2 * MAXD)) >> 1;
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+// insert; returns 1 if newly inserted, 0 if present, -1 if the table is full
+__device__ int hash_insert(uint64_t *tab, uint64_t mask, uint64_t key) {
+  uint64_t h = mix64(key) & mask;
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    unsigned long long cur =
+        atomicCAS((unsigned long long *)&tab[h], (unsigned long long)EMPTY_SLOT,
+                  (unsigned long long)key);
+    if (cur == EMPTY_SLOT) return 1;
+    if (cur == key) return 0;
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ bool hash_contains(const uint64_t *tab, uint64_t mask, uint64_t key) {
+  uint64_t h = mix64(key) & mask;
+  for (uint64_t probe = 0; probe <= mask; ++probe) {
+    uint64_t cur = tab[h];
+    if (cur == key) return true;
+    if (cur == EMPTY_SLOT) return false;
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+template <class T>
+__device__ __forceinline__ int64_t lower_bound(const T *a, int64_t lo, int64_t hi, T v) {
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (a[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// --- 1. point keys: the reference's descent, digit by digit -----------------
+__global__ void k_point_keys(const double *__restrict__ x, const double *__restrict__ y,
+                             int64_t n, double x0, double y0, double w0,
+                             uint64_t *__restrict__ keys, int *__restrict__ idx) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double px = x[i], py = y[i];
+    double xmin = x0, ymin = y0, w = w0;
+    uint64_t key = 0;
+#pragma unroll 1
+    for (int l = 0; l < MAXD; ++l) {
+      const double hw = 0.5 * w;
+      const double xm = __dadd_rn(xmin, hw);
+      const double ym = __dadd_rn(ymin, hw);
+      const int hx = px > xm, hy = py > ym;
+      key = (key << 2) | uint64_t(2 * hx + hy);
+      xmin = hx ? xm : __dsub_rn(xm, hw);
+      ymin = hy ? ym : __dsub_rn(ym, hw);
+      w = hw;
+    }
+    keys[i] = key;
+    idx[i] = int(i);
+  }
+}
+
+__global__ void k_gather_xy(const double *__restrict__ x, const double *__restrict__ y,
+                            const int *__restrict__ perm, int64_t n, double *__restrict__ sx,
+                            double *__restrict__ sy) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int j = perm[i];
+    sx[i] = x[j];
+    sy[i] = y[j];
+  }
+}
+
+// --- 3. initially split boxes ------------------------------------------------
+__global__ void k_initial_splits(const uint64_t *__restrict__ keys, int64_t n, int ppl,
+                                 uint64_t *__restrict__ out, unsigned long long cap,
+                                 Counters *cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const int cprev = (i == 0) ? -1 : common_digits(keys[i - 1], k);
+    const int cnext = (i + ppl < n) ? common_digits(k, keys[i + ppl]) : -1;
+    if (cnext <= cprev) continue;
+    if (cnext >= MAXD) {
+      atomicExch(&cnt->too_deep, 1);
+      continue;
+    }
+    const int cnt_here = cnext - cprev;
+    unsigned long long pos = atomicAdd(&cnt->s0_count, (unsigned long long)cnt_here);
+    atomicMax(&cnt->max_level, cnext);
+    for (int m = cprev + 1; m <= cnext; ++m) {
+      unsigned long long p = pos + (m - cprev - 1);
+      if (p < cap)
+        out[p] = box_code(m, k >> (2 * (MAXD - m)));
+      else
+        atomicExch(&cnt->overflow, 1);
+    }
+  }
+}
+
+__global__ void k_level_bounds(const uint64_t *__restrict__ codes, int64_t n, int L,
+                               int *__restrict__ bounds) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l > L) return;
+  bounds[l] = int(lower_bound<uint64_t>(codes, 0, n, box_code(l, 0)));
+}
+
+__global__ void k_hash_insert_all(const uint64_t *__restrict__ codes, int64_t n, uint64_t *tab,
+                                  uint64_t mask, Counters *cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (hash_insert(tab, mask, codes[i]) < 0) atomicExch(&cnt->overflow, 1);
+}
+
+// --- 4. balance closure, one level (m) per launch ------------------------------
+// S_m gains every box neighbouring the parent of a box of S_{m+1}.
+__global__ void k_balance(int m, const uint64_t *__restrict__ s0, const int *__restrict__ s0b,
+                          uint64_t *forced, const unsigned long long *__restrict__ fb,
+                          unsigned long long capf, uint64_t *tab, uint64_t mask, Counters *cnt) {
+  const int64_t a0 = s0b[m + 1], a1 = s0b[m + 2];
+  const int64_t n0 = a1 - a0;
+  // entries past the buffer capacity were never stored (overflow is flagged)
+  const int64_t f0 = (int64_t)min(fb[m + 1], capf), f1 = (int64_t)min(fb[m], capf);
+  const int64_t total = n0 + (f1 - f0);
+  const uint32_t side = 1u << m;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = (i < n0) ? s0[a0 + i] : forced[f0 + (i - n0)];
+    const uint64_t p = code_morton(c) >> 2;
+    uint32_t px, py;
+    morton_xy(p, m, px, py);
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int64_t qx = int64_t(px) + dx, qy = int64_t(py) + dy;
+        if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
+        const uint64_t q = box_code(m, morton_of(uint32_t(qx), uint32_t(qy), m));
+        const int r = hash_insert(tab, mask, q);
+        if (r < 0) {
+          atomicExch(&cnt->overflow, 1);
+        } else if (r == 1) {
+          unsigned long long pos = atomicAdd(&cnt->f_count, 1ULL);
+          if (pos < capf)
+            forced[pos] = q;
+          else
+            atomicExch(&cnt->overflow, 1);
+        }
+      }
+  }
+}
+
+// --- 5. X-list leaves: real leaves (parent split, self not split) next to a split box
+__global__ void k_xlist(const uint64_t *__restrict__ s0, int64_t n0, const uint64_t *__restrict__ forced,
+                        const unsigned long long *__restrict__ fcount, unsigned long long capf,
+                        int L, uint64_t *xl, unsigned long long capx, uint64_t *tab, uint64_t mask,
+                        Counters *cnt) {
+  const int64_t total = n0 + (int64_t)min(*fcount, capf);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = (i < n0) ? s0[i] : forced[i - n0];
+    const int m = code_level(c);
+    if (m < 1 || m > L - 2) continue;
+    uint32_t px, py;
+    morton_xy(code_morton(c), m, px, py);
+    const uint32_t side = 1u << m;
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy) {
+        if (dx == 0 && dy == 0) continue;
+        const int64_t qx = int64_t(px) + dx, qy = int64_t(py) + dy;
+        if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
+        const uint64_t qm = morton_of(uint32_t(qx), uint32_t(qy), m);
+        const uint64_t q = box_code(m, qm);
+        if (hash_contains(tab, mask, q)) continue;                        // split: not a leaf
+        if (!hash_contains(tab, mask, box_code(m - 1, qm >> 2))) continue;  // does not exist
+        const int r = hash_insert(tab, mask, q | XLIST_TAG);
+        if (r < 0) {
+          atomicExch(&cnt->overflow, 1);
+        } else if (r == 1) {
+          unsigned long long pos = atomicAdd(&cnt->x_count, 1ULL);
+          if (pos < capx)
+            xl[pos] = q;
+          else
+            atomicExch(&cnt->overflow, 1);
+        }
+      }
+  }
+}
+
+__global__ void k_concat_parents(const uint64_t *__restrict__ s0, int64_t n0,
+                                 const uint64_t *__restrict__ f, int64_t nf,
+                                 const uint64_t *__restrict__ xl, int64_t nx,
+                                 uint64_t *__restrict__ keys, uint8_t *__restrict__ isx) {
+  const int64_t total = n0 + nf + nx;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < n0) {
+      keys[i] = s0[i];
+      isx[i] = 0;
+    } else if (i < n0 + nf) {
+      keys[i] = f[i - n0];
+      isx[i] = 0;
+    } else {
+      keys[i] = xl[i - n0 - nf];
+      isx[i] = 1;
+    }
+  }
+}
+
+__device__ __forceinline__ int level_of(const int *__restrict__ off, int L, int g) {
+  int lo = 0, hi = L;  // find largest l with off[l] <= g
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (off[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// --- 6. node arrays -----------------------------------------------------------
+__global__ void k_node_codes(const int *__restrict__ off, int L, int total,
+                             const uint64_t *__restrict__ pkeys, const uint8_t *__restrict__ pisx,
+                             const int *__restrict__ pb, uint64_t *__restrict__ code,
+                             uint8_t *__restrict__ flags) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const int m = level_of(off, L, g);
+    if (m == 0) {
+      code[g] = 0;
+      flags[g] = 0;
+      continue;
+    }
+    const int j = g - off[m];
+    const int e = pb[m - 1] + (j >> 2);
+    code[g] = (code_morton(pkeys[e]) << 2) | uint64_t(j & 3);
+    flags[g] = pisx[e] ? NF_FAKE : 0;
+  }
+}
+
+__global__ void k_node_attrs(const int *__restrict__ off, int L, int total, double x0, double y0,
+                             double w0, const uint64_t *__restrict__ pts, int64_t npts,
+                             const uint64_t *__restrict__ pkeys, const uint8_t *__restrict__ pisx,
+                             const int *__restrict__ pb, const uint64_t *__restrict__ code,
+                             uint8_t *__restrict__ flags, double *__restrict__ xmin,
+                             double *__restrict__ ymin, double *__restrict__ xmid,
+                             double *__restrict__ ymid, int *__restrict__ bot,
+                             int *__restrict__ top, int *__restrict__ parent,
+                             int *__restrict__ child, int *__restrict__ coll) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const int m = level_of(off, L, g);
+    const uint64_t c = code[g];
+    // geometry: replay the descent along the node's digits (bit-exact with the reference)
+    double xm0 = x0, ym0 = y0, w = w0;
+    for (int l = 0; l < m; ++l) {
+      const int d = int((c >> (2 * (m - 1 - l))) & 3u);
+      const double hw = 0.5 * w;
+      const double xm = __dadd_rn(xm0, hw), ym = __dadd_rn(ym0, hw);
+      xm0 = (d >> 1) ? xm : __dsub_rn(xm, hw);
+      ym0 = (d & 1) ? ym : __dsub_rn(ym, hw);
+      w = hw;
+    }
+    const double hw = 0.5 * w;
+    xmin[g] = xm0;
+    ymin[g] = ym0;
+    xmid[g] = __dadd_rn(xm0, hw);
+    ymid[g] = __dadd_rn(ym0, hw);
+    // point range
+    const int sh = 2 * (MAXD - m);
+    bot[g] = int(lower_bound<uint64_t>(pts, 0, npts, c << sh));
+    top[g] = int(lower_bound<uint64_t>(pts, 0, npts, (c + 1) << sh));
+    // parent
+    parent[g] = (m == 0) ? -1
+                         : int(lower_bound<uint64_t>(code, off[m - 1], off[m], c >> 2));
+    // children: is this box a parent box?
+    uint8_t f = flags[g];
+    int ch = -1;
+    if (m < L - 1) {
+      const uint64_t key = box_code(m, c);
+      const int64_t e = lower_bound<uint64_t>(pkeys, pb[m], pb[m + 1], key);
+      if (e < pb[m + 1] && pkeys[e] == key) {
+        ch = off[m + 1] + 4 * int(e - pb[m]);
+        f |= NF_CHILDREN;
+        if (pisx[e]) f |= NF_XLIST;
+      }
+    }
+    if (!(f & NF_FAKE) && (ch < 0 || (f & NF_XLIST))) f |= NF_LEAF;
+    flags[g] = f;
+    child[g] = ch;
+    // colleagues: existing same-level boxes at offsets (-1..1)^2, self included
+    uint32_t ix, iy;
+    morton_xy(c, m, ix, iy);
+    const uint32_t side = 1u << m;
+    int k = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int64_t qx = int64_t(ix) + dx, qy = int64_t(iy) + dy;
+        int found = -1;
+        if (qx >= 0 && qy >= 0 && qx < side && qy < side) {
+          const uint64_t q = morton_of(uint32_t(qx), uint32_t(qy), m);
+          const int64_t e = lower_bound<uint64_t>(code, off[m], off[m + 1], q);
+          if (e < off[m + 1] && code[e] == q) found = int(e);
+        }
+        if (found >= 0) coll[int64_t(g) * 9 + (k++)] = found;
+      }
+    for (; k < 9; ++k) coll[int64_t(g) * 9 + k] = -1;
+  }
+}
+
+// far-field interaction lists of real nodes at levels >= 2: children of the
+// parent's colleagues that are not adjacent (build_interaction_list,
+// flexmm/tree.py:399-435), keeping only sources that hold points
+__global__ void k_interactions(const int *__restrict__ off, int L, int total,
+                               const uint64_t *__restrict__ code,
+                               const uint8_t *__restrict__ flags, const int *__restrict__ bot,
+                               const int *__restrict__ top, int *__restrict__ il) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const int m = level_of(off, L, g);
+    int *row = il + int64_t(g) * N_OFFSETS;
+    if (m < 2 || (flags[g] & NF_FAKE)) {
+      for (int o = 0; o < N_OFFSETS; ++o) row[o] = -1;
+      continue;
+    }
+    uint32_t ix, iy;
+    morton_xy(code[g], m, ix, iy);
+    const int64_t side = int64_t(1) << m;
+    const int64_t px = ix >> 1, py = iy >> 1;
+    int o = 0;
+    for (int a = -3; a <= 3; ++a)
+      for (int b = -3; b <= 3; ++b) {
+        if (a >= -1 && a <= 1 && b >= -1 && b <= 1) continue;
+        int found = -1;
+        const int64_t qx = int64_t(ix) + a, qy = int64_t(iy) + b;
+        if (qx >= 0 && qy >= 0 && qx < side && qy < side) {
+          const int64_t dpx = (qx >> 1) - px, dpy = (qy >> 1) - py;
+          if (dpx >= -1 && dpx <= 1 && dpy >= -1 && dpy <= 1) {
+            const uint64_t q = morton_of(uint32_t(qx), uint32_t(qy), m);
+            const int64_t e = lower_bound<uint64_t>(code, off[m], off[m + 1], q);
+            if (e < off[m + 1] && code[e] == q && top[e] > bot[e]) found = int(e);
+          }
+        }
+        row[o++] = found;
+      }
+  }
+}
+
+uint64_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+template <class K, class V>
+void radix_sort_pairs(const K *kin, K *kout, const V *vin, V *vout, int64_t n, int end_bit,
+                      cudaStream_t s) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit, s));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(bytes, s);
+  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, kin, kout, vin, vout, n, 0, end_bit, s));
+}
+
+}  // namespace
+
+void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
+                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s) {
+  DevBuf<uint64_t> k0;
+  DevBuf<int> i0;
+  k0.alloc(n, s);
+  i0.alloc(n, s);
+  keys.alloc(n, s);
+  perm.alloc(n, s);
+  if (n == 0) return;
+  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, k0.get(), i0.get());
+  FMMB_CUDA(cudaGetLastError());
+  radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * MAXD, s);
+}
+
+void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
+                const double bbox[4], cudaStream_t s) {
+  FMMB_CHECK(n > 0, ERR_INVALID_ARGUMENT, "tree needs at least one point");
+  FMMB_CHECK(ppl >= 1, ERR_INVALID_ARGUMENT, "Ncutoff must be >= 1");
+  FMMB_CHECK(n < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 points");
+  th.n_points = n;
+  th.ppl = ppl;
+  th.x0 = bbox[0];
+  th.y0 = bbox[2];
+  th.w0 = bbox[1] - bbox[0];
+  FMMB_CHECK(th.w0 > 0, ERR_INVALID_ARGUMENT, "bbox has non-positive width");
+
+  // 1-2: keys and sort
+  sort_points(x, y, n, th, td.pkeys, td.ordv, s);
+  td.sx.alloc(n, s);
+  td.sy.alloc(n, s);
+  k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, td.ordv.get(), n, td.sx.get(), td.sy.get());
+  FMMB_CUDA(cudaGetLastError());
+
+  DevBuf<Counters> cnt;
+  cnt.alloc(1, s);
+  cnt.zero(s);
+  Counters hc;
+
+  // 3: initial splits
+  const unsigned long long cap0 = (unsigned long long)MAXD * (n / (ppl + 1) + 1) + 64;
+  DevBuf<uint64_t> s0raw, s0;
+  s0raw.alloc(cap0, s);
+  k_initial_splits<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, s0raw.get(), cap0,
+                                                     cnt.get());
+  FMMB_CUDA(cudaGetLastError());
+  FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  FMMB_CUDA(cudaStreamSynchronize(s));
+  FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
+             "more than Ncutoff points share a box of width bbox/2^29 (coincident points?)");
+  FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
+  const int64_t n0 = (int64_t)hc.s0_count;
+  const int L = (n0 > 0) ? hc.max_level + 2 : 1;
+  th.L = L;
+
+  DevBuf<uint64_t> pk, pks;  // parent boxes (unsorted, sorted)
+  DevBuf<uint8_t> px, pxs;
+  DevBuf<int> pb;
+  std::vector<int> hpb(L + 1, 0);
+  int64_t np = 0;
+  if (n0 > 0) {
+    s0.alloc(n0, s);
+    {
+      size_t bytes = 0;
+      FMMB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, s0raw.get(), s0.get(), n0, 0, 64, s));
+      DevBuf<uint8_t> tmp;
+      tmp.alloc(bytes, s);
+      FMMB_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), bytes, s0raw.get(), s0.get(), n0, 0, 64, s));
+    }
+    DevBuf<int> s0b;
+    s0b.alloc(L + 2, s);
+    k_level_bounds<<<1, 64, 0, s>>>(s0.get(), n0, L + 1, s0b.get());
+    FMMB_CUDA(cudaGetLastError());
+
+    // 4: balance closure with a hash set; capacities grow on overflow
+    unsigned long long capf = 8ull * n0 + 4096, capx = 8ull * n0 + 4096;
+    for (int attempt = 0;; ++attempt) {
+      const uint64_t hcap = next_pow2(2 * (n0 + capf + capx));
+      DevBuf<uint64_t> tab, forced, xl;
+      DevBuf<unsigned long long> fb;
+      tab.alloc(hcap, s);
+      FMMB_CUDA(cudaMemsetAsync(tab.get(), 0xff, hcap * sizeof(uint64_t), s));
+      forced.alloc(capf, s);
+      xl.alloc(capx, s);
+      fb.alloc(L + 1, s);
+      fb.zero(s);
+      FMMB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(Counters), s));
+      k_hash_insert_all<<<grid_for(n0, TPB), TPB, 0, s>>>(s0.get(), n0, tab.get(), hcap - 1, cnt.get());
+      FMMB_CUDA(cudaGetLastError());
+      for (int m = L - 3; m >= 1; --m) {
+        FMMB_CUDA(cudaMemcpyAsync(fb.get() + m, &cnt.get()->f_count, sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToDevice, s));
+        k_balance<<<148 * 4, TPB, 0, s>>>(m, s0.get(), s0b.get(), forced.get(), fb.get(), capf,
+                                          tab.get(), hcap - 1, cnt.get());
+        FMMB_CUDA(cudaGetLastError());
+      }
+      // 5: X-list leaves
+      k_xlist<<<148 * 4, TPB, 0, s>>>(s0.get(), n0, forced.get(), &cnt.get()->f_count, capf, L,
+                                      xl.get(), capx, tab.get(), hcap - 1, cnt.get());
+      FMMB_CUDA(cudaGetLastError());
+      FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+      FMMB_CUDA(cudaStreamSynchronize(s));
+      if (hc.overflow) {
+        FMMB_CHECK(attempt < 6, ERR_CAPACITY, "tree balance buffers overflow");
+        capf = 4 * capf;
+        capx = 4 * capx;
+        continue;
+      }
+      const int64_t nf = (int64_t)hc.f_count, nx = (int64_t)hc.x_count;
+      np = n0 + nf + nx;
+      pk.alloc(np, s);
+      px.alloc(np, s);
+      k_concat_parents<<<grid_for(np, TPB), TPB, 0, s>>>(s0.get(), n0, forced.get(), nf, xl.get(),
+                                                          nx, pk.get(), px.get());
+      FMMB_CUDA(cudaGetLastError());
+      break;
+    }
+    // 6: sorted parent boxes and per-level bounds
+    pks.alloc(np, s);
+    pxs.alloc(np, s);
+    radix_sort_pairs(pk.get(), pks.get(), px.get(), pxs.get(), np, 64, s);
+    pb.alloc(L + 1, s);
+    k_level_bounds<<<1, 64, 0, s>>>(pks.get(), np, L, pb.get());
+    FMMB_CUDA(cudaGetLastError());
+    FMMB_CUDA(cudaMemcpyAsync(hpb.data(), pb.get(), (L + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+  } else {
+    pb.alloc(L + 1, s);
+    pb.zero(s);
+    pks.alloc(1, s);
+    pxs.alloc(1, s);
+  }
+
+  th.off.assign(L + 1, 0);
+  th.width.assign(L, 0.0);
+  th.off[0] = 0;
+  th.off[1] = 1;
+  for (int m = 1; m < L; ++m) th.off[m + 1] = th.off[m] + 4 * (hpb[m] - hpb[m - 1]);
+  double w = th.w0;
+  for (int m = 0; m < L; ++m) {
+    th.width[m] = w;
+    w = 0.5 * w;
+  }
+  const int total = th.off[L];
+  td.dev_off.alloc(L + 1, s);
+  FMMB_CUDA(cudaMemcpyAsync(td.dev_off.get(), th.off.data(), (L + 1) * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+  td.code.alloc(total, s);
+  td.flags.alloc(total, s);
+  td.xmin.alloc(total, s);
+  td.ymin.alloc(total, s);
+  td.xmid.alloc(total, s);
+  td.ymid.alloc(total, s);
+  td.bot.alloc(total, s);
+  td.top.alloc(total, s);
+  td.parent.alloc(total, s);
+  td.child.alloc(total, s);
+  td.coll.alloc(int64_t(total) * 9, s);
+  td.il.alloc(int64_t(total) * N_OFFSETS, s);
+  k_node_codes<<<grid_for(total, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total, pks.get(),
+                                                      pxs.get(), pb.get(), td.code.get(),
+                                                      td.flags.get());
+  FMMB_CUDA(cudaGetLastError());
+  k_node_attrs<<<grid_for(total, TPB), TPB, 0, s>>>(
+      td.dev_off.get(), L, total, th.x0, th.y0, th.w0, td.pkeys.get(), n, pks.get(), pxs.get(),
+      pb.get(), td.code.get(), td.flags.get(), td.xmin.get(), td.ymin.get(), td.xmid.get(),
+      td.ymid.get(), td.bot.get(), td.top.get(), td.parent.get(), td.child.get(), td.coll.get());
+  FMMB_CUDA(cudaGetLastError());
+  k_interactions<<<grid_for(total, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total, td.code.get(),
+                                                        td.flags.get(), td.bot.get(), td.top.get(),
+                                                        td.il.get());
+  FMMB_CUDA(cudaGetLastError());
+}
+
+}  // namespace fmmb

@@ -1,0 +1,68 @@
+// Quadtree data on the device.  Nodes of all levels live in one level-major
+// array; inside a level they are in Morton order, and the four children of a
+// box are consecutive (digit = 2*[x > xmid] + [y > ymid]).
+#pragma once
+#include "common.cuh"
+
+namespace fmmb {
+
+enum NodeFlag : uint8_t {
+  NF_LEAF = 1,      // real leaf (targets stop here); X-list leaves included
+  NF_FAKE = 2,      // fake leaf: child of an X-list leaf, source-only
+  NF_XLIST = 4,     // real leaf with a non-leaf colleague; owns 4 fake children
+  NF_CHILDREN = 8,  // has 4 children on the next level
+};
+
+constexpr int N_OFFSETS = 40;  // far-field offsets (-3..3)^2 minus (-1..1)^2
+
+// offset id 0..39 <-> (ox, oy); ids walk ox = -3..3 (outer), oy = -3..3 (inner)
+__host__ __device__ inline void offset_of(int id, int &ox, int &oy) {
+  int k = 0;
+  for (int a = -3; a <= 3; ++a)
+    for (int b = -3; b <= 3; ++b) {
+      if (a >= -1 && a <= 1 && b >= -1 && b <= 1) continue;
+      if (k == id) {
+        ox = a;
+        oy = b;
+        return;
+      }
+      ++k;
+    }
+  ox = oy = 0;
+}
+
+struct TreeDev {
+  // points (sorted by key)
+  DevBuf<uint64_t> pkeys;
+  DevBuf<int> ordv;       // sorted position -> original index
+  DevBuf<double> sx, sy;  // sorted source coordinates
+  // nodes
+  DevBuf<uint64_t> code;  // morton code at the node's level
+  DevBuf<double> xmin, ymin, xmid, ymid;
+  DevBuf<int> bot, top, parent, child;
+  DevBuf<uint8_t> flags;
+  DevBuf<int> coll;  // [n_total x 9], -1 padded
+  DevBuf<int> il;    // [n_total x 40] source node per offset, -1 if none
+  DevBuf<int> dev_off;  // level offsets [L+1]
+};
+
+struct TreeHost {
+  int L = 0;
+  int64_t n_points = 0;
+  int ppl = 0;
+  double x0 = 0, y0 = 0, w0 = 0;
+  std::vector<int> off;       // L+1
+  std::vector<double> width;  // per level
+  int n_total() const { return off.empty() ? 0 : off.back(); }
+};
+
+// Build the tree over device coordinates x, y (n points) on `stream`.
+void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
+                const double bbox[4], cudaStream_t stream);
+
+// Sort arbitrary target points by the same descent key; returns sorted keys
+// and the permutation sorted -> original.
+void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
+                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t stream);
+
+}  // namespace fmmb

@@ -1,0 +1,198 @@
+"""Operator precomputation and caching (the reference's Helper / Precomputation).
+
+Mirrors flexmm/flexmm2d/helpers.py:35-84 and flexmm/flexmm2d/kifmm.py:13-82:
+per box width, the equivalent / check circles, the check-to-equivalent
+solve, the M2M operator (whose transpose is L2L) and the 40 M2L operators,
+SVD-compressed exactly as M2L_Evaluator does.  The operators are formed on
+the host in FP64 with the kernel's numpy twin and uploaded once into a
+device operator set (``fmm_ops``); plans bind their levels to entries.
+
+Two deliberate differences from the reference:
+
+* the check-to-equivalent solve is stored as the SVD factors
+  (U, 1/S, VH) and applied on the GPU as two GEMMs and a scaling, as in
+  flexmm/kifmm2d/scalar/helpers.py:240-248, instead of LU (the two agree to
+  ~1e-15; an explicit inverse would not);
+* a helper is bound to one (kernel, Nequiv): passing it to an FMM with a
+  different kernel or Nequiv raises, instead of silently reusing the first
+  kernel's operators (the shared default ``helper=KI_Helper()`` of
+  flexmm/flexmm2d/kifmm.py:123).  With ``helper=None`` a process-wide helper
+  per (kernel, params, Nequiv) is used, so operators stay warm across objects.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+SVD_TOL = 1e-14        # M2L compression, flexmm/flexmm2d/helpers.py:197
+C2E_TOL = 1e-15        # SVD_Solver, flexmm/kifmm2d/scalar/helpers.py:241
+
+
+def width_key(width):
+    """Cache key of a box width (FloatDict, flexmm/flexmm2d/float_dict.py:23-24)."""
+    return round(width, 12)
+
+
+def surfaces(width, theta):
+    """Small (equivalent) and large (check) circles (flexmm/flexmm2d/kifmm.py:158-168)."""
+    dd = 0.0
+    r1 = 0.5 * width * (np.sqrt(2) + dd)
+    r2 = 0.5 * width * (4 - np.sqrt(2) - 2 * dd)
+    return r1 * np.cos(theta), r1 * np.sin(theta), r2 * np.cos(theta), r2 * np.sin(theta)
+
+
+def offsets():
+    """The 40 far-field offsets in device order (ox outer, oy inner)."""
+    return [(a, b) for a in range(-3, 4) for b in range(-3, 4) if not (abs(a) <= 1 and abs(b) <= 1)]
+
+
+class KIPrecomputation:
+    """Operators of one width (KI_Precomputation, flexmm/flexmm2d/kifmm.py:13-62)."""
+
+    def __init__(self, width, nequiv, kernel):
+        self.width = width
+        n = nequiv
+        theta = np.linspace(0, 2 * np.pi, n, endpoint=False)
+
+        def form(sx, sy, tx, ty):  # out[j, i] = K(s_i, t_j)
+            return np.ascontiguousarray(kernel.host(sx[None, :], sy[None, :], tx[:, None], ty[:, None]),
+                                        dtype=np.float64)
+
+        sx, sy, lx, ly = surfaces(width, theta)
+        s2l = form(sx, sy, lx, ly)
+        U, S, VH = np.linalg.svd(s2l)
+        with np.errstate(divide="ignore"):
+            self.c2e_sinv = np.where(S < C2E_TOL, 0.0, 1.0 / S)
+        self.c2e_u = np.ascontiguousarray(U)
+        self.c2e_vh = np.ascontiguousarray(VH)
+        ssx, ssy, _, _ = surfaces(0.5 * width, theta)
+        q = 0.25 * width
+        cex = np.concatenate([ssx - q, ssx - q, ssx + q, ssx + q])
+        cey = np.concatenate([ssy - q, ssy + q, ssy - q, ssy + q])
+        self.m2mc = form(cex, cey, lx, ly)
+        self.small_x, self.small_y = sx, sy
+        self.large_x, self.large_y = np.ascontiguousarray(lx), np.ascontiguousarray(ly)
+        # M2L_Evaluator semantics (flexmm/flexmm2d/helpers.py:5-33)
+        self.m2l_rank = np.zeros(len(offsets()), dtype=np.int32)
+        self.m2l_a = []
+        self.m2l_b = []
+        for o, (ox, oy) in enumerate(offsets()):
+            m = form(sx + ox * width, sy + oy * width, sx, sy)
+            Um, Sm, VHm = np.linalg.svd(m)
+            cuts = np.flatnonzero(Sm > SVD_TOL)
+            if cuts.size == 0:
+                self.m2l_rank[o] = 0
+                self.m2l_a.append(None)
+                self.m2l_b.append(None)
+                continue
+            r = int(cuts[-1]) + 1
+            if 2 * r < n:
+                self.m2l_rank[o] = r
+                self.m2l_a.append(np.ascontiguousarray(Um[:, :r]))
+                self.m2l_b.append(np.ascontiguousarray(VHm[:r] * Sm[:r, None]))
+            else:
+                self.m2l_rank[o] = -1
+                self.m2l_a.append(m)
+                self.m2l_b.append(None)
+
+    def upload(self, ops_handle):
+        dp = ctypes.POINTER(ctypes.c_double)
+
+        def ptr(a):
+            return a.ctypes.data_as(dp) if a is not None else ctypes.cast(None, dp)
+
+        arr_a = (dp * len(self.m2l_a))(*[ptr(a) for a in self.m2l_a])
+        arr_b = (dp * len(self.m2l_b))(*[ptr(b) for b in self.m2l_b])
+        lv = _lib.LevelOps(
+            large_x=ptr(self.large_x), large_y=ptr(self.large_y),
+            c2e_u=ptr(self.c2e_u), c2e_sinv=ptr(self.c2e_sinv), c2e_vh=ptr(self.c2e_vh),
+            m2mc=ptr(self.m2mc),
+            m2l_rank=self.m2l_rank.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            m2l_a=arr_a, m2l_b=arr_b)
+        lid = ctypes.c_int(-1)
+        _lib.call("fmm_ops_add", ops_handle, ctypes.byref(lv), ctypes.byref(lid))
+        return lid.value
+
+
+class OpsSet:
+    """Owner of one device operator set (``fmm_ops``); destroyed with its last reference."""
+
+    def __init__(self, kernel, nequiv):
+        h = ctypes.c_void_p()
+        params = (ctypes.c_double * 4)(*kernel.params)
+        _lib.call("fmm_ops_create", kernel.kernel_id, params, nequiv, ctypes.byref(h))
+        self.handle = h
+
+    def __del__(self):
+        try:
+            if self.handle is not None and _lib._LIB is not None:
+                _lib._LIB.fmm_ops_destroy(self.handle)
+        except Exception:
+            pass
+        self.handle = None
+
+
+class KI_Helper:
+    """Operator cache for one (kernel, Nequiv) (Helper, flexmm/flexmm2d/helpers.py:35-84)."""
+
+    def __init__(self, helper=None):
+        self.kernel = None
+        self.nequiv = None
+        self.precomputations = {}   # width_key -> KIPrecomputation
+        self._level_ids = {}        # width_key -> device operator entry
+        self._ops = None
+        if helper is not None:      # share the other helper's cache, like the reference
+            self.__dict__ = helper.__dict__
+
+    def attach(self, kernel, nequiv):
+        if self.kernel is None:
+            self.kernel = kernel
+            self.nequiv = nequiv
+        elif self.kernel.key != kernel.key or self.nequiv != nequiv:
+            raise ValueError(f"helper holds operators for {self.kernel} with Nequiv={self.nequiv}; "
+                             f"got {kernel} with Nequiv={nequiv}")
+
+    def ops_set(self):
+        if self._ops is None:
+            self._ops = OpsSet(self.kernel, self.nequiv)
+        return self._ops
+
+    def collect_widths(self):
+        return np.array(list(self.precomputations), dtype=float)
+
+    def get_bbox(self, px, py, bbox):
+        """Square bbox, snapped to a cached width (flexmm/flexmm2d/helpers.py:52-72)."""
+        if bbox is None:
+            bbox = [float(np.min(px)), float(np.max(px)), float(np.min(py)), float(np.max(py))]
+        widths = self.collect_widths()
+        if len(widths) > 0:
+            small = np.min(widths)
+            bw = max(bbox[1] - bbox[0], bbox[3] - bbox[2])
+            width = 2 ** np.ceil(np.log2(bw / small)) * small
+        else:
+            width = max(bbox[1] - bbox[0], bbox[3] - bbox[2])
+        cx = (bbox[1] + bbox[0]) / 2
+        cy = (bbox[3] + bbox[2]) / 2
+        return [float(cx - width / 2), float(cx + width / 2), float(cy - width / 2), float(cy + width / 2)]
+
+    def level_id(self, width):
+        key = width_key(width)
+        if key not in self.precomputations:
+            self.precomputations[key] = KIPrecomputation(width, self.nequiv, self.kernel)
+        if key not in self._level_ids:
+            self._level_ids[key] = self.precomputations[key].upload(self.ops_set().handle)
+        return self._level_ids[key]
+
+    def get_precomputation(self, width):
+        return self.precomputations[width_key(width)]
+
+
+_DEFAULT_HELPERS = {}
+
+
+def default_helper(kernel, nequiv):
+    key = (kernel.key, nequiv)
+    if key not in _DEFAULT_HELPERS:
+        _DEFAULT_HELPERS[key] = KI_Helper()
+    return _DEFAULT_HELPERS[key]

@@ -1,0 +1,216 @@
+"""KI_FMM: the reference's kernel-independent FMM object, on a B200.
+
+Same constructor, methods and results as flexmm/flexmm2d/kifmm.py:122-144
+(with FMM, flexmm/flexmm2d/fmm.py:32-176)::
+
+    F = KI_FMM(x, y, Laplace_Eval, Ncutoff, Nequiv, bbox=bbox, helper=helper)
+    F.build_expansions(tau)
+    u_src = F.source_evaluation(x, y)       # skips coincident source/target pairs
+    u_tgt = F.target_evaluation(tx, ty)
+
+Inputs may be numpy arrays (results come back as numpy) or torch tensors
+(results stay torch tensors on the GPU).  All work runs on the current CUDA
+device and torch's current stream, through ``libflexmm_b200.so``; there is
+no CPU path.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .helpers import KI_Helper, default_helper
+from .kernels import resolve
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _device_f64(a):
+    """(device float64 contiguous 1-D tensor, was_numpy)."""
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        t = a.reshape(-1)
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
+            t = t.to(device="cuda", dtype=torch.float64).contiguous()
+        return t, False
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+    return torch.from_numpy(arr).to("cuda", non_blocking=False), True
+
+
+def _stream():
+    return ctypes.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+
+class TreeLevel:
+    """One level of the GPU tree, with the reference's Level field names (flexmm/tree.py:275-360)."""
+
+
+class TreeView:
+    """Host copy of the GPU tree, shaped like the reference's Tree (flexmm/tree.py:447-589)."""
+
+    def __init__(self, fmm):
+        plan = fmm._plan
+        L, widths, counts = fmm._levels, fmm._widths, fmm._counts
+        T = int(sum(counts))
+        xmin = np.empty(T)
+        ymin = np.empty(T)
+        bot = np.empty(T, np.int32)
+        top = np.empty(T, np.int32)
+        parent = np.empty(T, np.int32)
+        child = np.empty(T, np.int32)
+        flags = np.empty(T, np.uint8)
+        coll = np.empty(T * 9, np.int32)
+        il = np.empty(T * _lib.N_OFFSETS, np.int32)
+        ordv = np.empty(fmm.N, np.int32)
+        vp = lambda a: ctypes.c_void_p(a.ctypes.data)
+        _lib.call("fmm_tree_export", plan, vp(xmin), vp(ymin), vp(bot), vp(top), vp(parent),
+                  vp(child), vp(flags), vp(coll), vp(il), vp(ordv))
+        coll = coll.reshape(T, 9)
+        il = il.reshape(T, _lib.N_OFFSETS)
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        self.bbox = list(fmm.bbox)
+        self.N = fmm.N
+        self.ordv = ordv.astype(np.int64)
+        self.levels = L
+        self.Levels = []
+        self._il = []
+        grid49 = np.array([(a + 3) * 7 + (b + 3) for a in range(-3, 4) for b in range(-3, 4)
+                           if not (abs(a) <= 1 and abs(b) <= 1)])
+        for m in range(L):
+            a, b = off[m], off[m + 1]
+            lv = TreeLevel()
+            lv.width = widths[m]
+            lv.half_width = 0.5 * widths[m]
+            lv.n_node = int(b - a)
+            lv.xmin = xmin[a:b]
+            lv.ymin = ymin[a:b]
+            lv.xmid = lv.xmin + lv.half_width
+            lv.ymid = lv.ymin + lv.half_width
+            lv.bot_ind = bot[a:b].astype(np.int64)
+            lv.top_ind = top[a:b].astype(np.int64)
+            lv.ns = lv.top_ind - lv.bot_ind
+            f = flags[a:b]
+            lv.leaf = (f & 1) != 0
+            lv.fake_leaf = (f & 2) != 0
+            lv.Xlist = (f & 4) != 0
+            ch = child[a:b].astype(np.int64)
+            lv.children_ind = np.where(ch >= 0, ch - off[m + 1] if m + 1 <= L else ch, -1)
+            par = parent[a:b].astype(np.int64)
+            lv.parent_ind = np.where(par >= 0, par - (off[m - 1] if m > 0 else 0), -1)
+            c = coll[a:b].astype(np.int64)
+            lv.colleagues = np.where(c >= 0, c - a, -1)
+            lv.compute_upwards = ((lv.leaf & ~lv.Xlist) | lv.fake_leaf) & (lv.ns > 0)
+            lv.compute_downwards = (~lv.leaf | lv.Xlist) & ~lv.fake_leaf
+            self.Levels.append(lv)
+            rows = il[a:b]
+            t, o = np.nonzero(rows >= 0)
+            self._il.append(np.stack([t, grid49[o], rows[t, o].astype(np.int64) - a], axis=1)
+                            if t.size else np.zeros((0, 3), np.int64))
+
+    def interaction_triples(self, ind):
+        """(target node, offset id (ox+3)*7+(oy+3), source node) of level ``ind``."""
+        return self._il[ind]
+
+
+class KI_FMM:
+    """Kernel-independent FMM (KI_FMM, flexmm/flexmm2d/kifmm.py:122-144)."""
+
+    def __init__(self, x, y, kernel_eval, Ncutoff=50, Nequiv=50, dtype=float, bbox=None,
+                 helper=None, verbose=False, **kernel_params):
+        if dtype not in (float, np.float64):
+            raise NotImplementedError("only real float64 charges are supported")
+        if Nequiv > _lib.MAX_NEQUIV:
+            raise ValueError(f"Nequiv must be <= {_lib.MAX_NEQUIV}")
+        _lib.load()
+        self.kernel = resolve(kernel_eval, **kernel_params)
+        self.Ncutoff = int(Ncutoff)
+        self.Nequiv = int(Nequiv)
+        self.dtype = dtype
+        self.verbose = verbose
+        self.helper = helper if helper is not None else default_helper(self.kernel, self.Nequiv)
+        if not isinstance(self.helper, KI_Helper):
+            raise TypeError("helper must be a flexmm_b200 KI_Helper")
+        self.helper.attach(self.kernel, self.Nequiv)
+        xd, _ = _device_f64(x)
+        yd, _ = _device_f64(y)
+        if xd.numel() != yd.numel():
+            raise ValueError("x and y differ in length")
+        self.N = int(xd.numel())
+        if bbox is None:
+            bb = [xd.min().item(), xd.max().item(), yd.min().item(), yd.max().item()]
+        else:
+            bb = [float(v) for v in bbox]
+        self.bbox = self.helper.get_bbox(None, None, bb)
+        st = time.time()
+        plan = ctypes.c_void_p()
+        bb_arr = (ctypes.c_double * 4)(*self.bbox)
+        _lib.call("fmm_plan_create", self.helper.ops_set().handle, ctypes.c_void_p(xd.data_ptr()),
+                  ctypes.c_void_p(yd.data_ptr()), self.N, self.Ncutoff, bb_arr, _stream(),
+                  ctypes.byref(plan))
+        self._plan = plan
+        self._ops = self.helper.ops_set()   # keep the operator set alive with the plan
+        nl = ctypes.c_int()
+        widths = (ctypes.c_double * _lib.MAX_LEVELS)()
+        counts = (ctypes.c_int * _lib.MAX_LEVELS)()
+        _lib.call("fmm_plan_info", plan, ctypes.byref(nl), widths, counts)
+        self._levels = nl.value
+        self._widths = [widths[i] for i in range(nl.value)]
+        self._counts = [counts[i] for i in range(nl.value)]
+        if verbose:
+            print("....Tree formed in:             {:0.1f}".format((time.time() - st) * 1000))
+        # operators for every level width (KI_Helper.prepare, flexmm/flexmm2d/kifmm.py:67-82)
+        for m, w in enumerate(self._widths):
+            _lib.call("fmm_plan_bind", plan, m, self.helper.level_id(w))
+        self._tree = None
+        self._expanded = False
+
+    @property
+    def tree(self):
+        if self._tree is None:
+            self._tree = TreeView(self)
+        return self._tree
+
+    def build_expansions(self, tau):
+        td, _ = _device_f64(tau)
+        if td.numel() != self.N:
+            raise ValueError(f"tau has {td.numel()} entries, expected {self.N}")
+        st = time.time()
+        _lib.call("fmm_build_expansions", self._plan, ctypes.c_void_p(td.data_ptr()), _stream())
+        self._tau = td   # kept alive until the stream has consumed it
+        self._expanded = True
+        if self.verbose:
+            _torch().cuda.synchronize()
+            print("....Time for expansions:        {:0.2f}".format(1000 * (time.time() - st)))
+
+    def _evaluate(self, x, y, check):
+        torch = _torch()
+        xd, was_np = _device_f64(x)
+        yd, _ = _device_f64(y)
+        if xd.numel() != yd.numel():
+            raise ValueError("x and y differ in length")
+        out = torch.empty(xd.numel(), dtype=torch.float64, device="cuda")
+        _lib.call("fmm_evaluate", self._plan, ctypes.c_void_p(xd.data_ptr()),
+                  ctypes.c_void_p(yd.data_ptr()), xd.numel(), 1 if check else 0,
+                  ctypes.c_void_p(out.data_ptr()), _stream())
+        if was_np:
+            return out.cpu().numpy().reshape(np.shape(x))
+        return out
+
+    def source_evaluation(self, x, y):
+        """Potential at (x, y), skipping coincident sources (flexmm/flexmm2d/fmm.py:158-159)."""
+        return self._evaluate(x, y, True)
+
+    def target_evaluation(self, x, y):
+        """Potential at (x, y) (flexmm/flexmm2d/fmm.py:160-161)."""
+        return self._evaluate(x, y, False)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_plan", None) is not None and _lib._LIB is not None:
+                _lib._LIB.fmm_plan_destroy(self._plan)
+        except Exception:
+            pass
+        self._plan = None

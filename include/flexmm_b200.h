@@ -1,0 +1,106 @@
+/* flexmm_b200: C ABI of the B200 2D FMM evaluation path.
+ *
+ * The reference (dbstein/flexmm) is a Python + Numba package with no native
+ * interface; these entry points replace the pieces of its Python object model
+ * that do the work, and the Python package flexmm_b200 binds them with ctypes
+ * behind the reference's own class names and signatures:
+ *
+ *   fmm_ops_*            the operator cache of a Helper: one entry per box
+ *                        width (KI_Helper.prepare / KI_Precomputation,
+ *                        flexmm/flexmm2d/kifmm.py:13-82; FloatDict keyed by
+ *                        width, flexmm/flexmm2d/float_dict.py:23-24)
+ *   fmm_plan_create      FMM.__init__ -> Tree(x, y, Ncutoff, bbox)
+ *                        (flexmm/flexmm2d/fmm.py:33-58, flexmm/tree.py:451-518)
+ *   fmm_plan_info /      the tree's level widths, to fill and bind the
+ *   fmm_plan_bind        operator cache (KI_Helper.prepare, kifmm.py:67-82)
+ *   fmm_build_expansions FMM.build_expansions(tau) (fmm.py:151-153)
+ *   fmm_evaluate         FMM.source_evaluation / target_evaluation
+ *                        (fmm.py:158-176); check=1 skips coincident pairs
+ *                        (helpers.py:99-107)
+ *   fmm_tree_export      the tree arrays (Tree.Levels[*], tree.py:275-360)
+ *
+ * Conventions: every function returns 0 (FMM_OK) or an FMM_ERR_* code and
+ * never aborts; fmm_last_error() gives the message of the calling thread's
+ * last failure.  Point, charge and output pointers are DEVICE pointers owned
+ * by the caller; `stream` is a cudaStream_t (NULL = legacy default stream).
+ * A plan must be used from one stream.  An operator set must outlive the
+ * plans bound to it.  Plans are independent and may be used concurrently.
+ */
+#ifndef FLEXMM_B200_H
+#define FLEXMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FMM_OK 0
+#define FMM_ERR_INVALID_ARGUMENT 1
+#define FMM_ERR_CUDA 2
+#define FMM_ERR_TREE_TOO_DEEP 3
+#define FMM_ERR_NOT_READY 4
+#define FMM_ERR_UNSUPPORTED 5
+#define FMM_ERR_CAPACITY 6
+
+/* kernels, registered under the reference's example names */
+#define FMM_KERNEL_LAPLACE 0 /* Laplace_Eval, examples/kifmm_laplace.py:24-29 */
+
+#define FMM_N_OFFSETS 40 /* far-field offsets (-3..3)^2 minus (-1..1)^2; id walks ox outer, oy inner */
+#define FMM_MAX_LEVELS 30
+#define FMM_MAX_NEQUIV 64
+
+typedef struct fmm_ops fmm_ops;
+typedef struct fmm_plan fmm_plan;
+
+/* Operators of one box width (row-major, natural sizes, n = nequiv).
+ * Replaces KI_Precomputation (flexmm/flexmm2d/kifmm.py:13-62) and
+ * Precomputation.compress / M2L_Evaluator (flexmm/flexmm2d/helpers.py:5-33,
+ * 196-218). */
+typedef struct fmm_level_ops {
+  const double *large_x, *large_y; /* [n] check circle of radius w(4-sqrt2)/2 */
+  const double *c2e_u;             /* [n*n] U of S2L = U diag(S) VH          */
+  const double *c2e_sinv;          /* [n] 1/S (0 for discarded values)        */
+  const double *c2e_vh;            /* [n*n] VH                                */
+  const double *m2mc;              /* [n * 4n] child equivalent circles -> check circle */
+  const int *m2l_rank;             /* [40] -1 dense, 0 null, r > 0 SVD rank   */
+  const double *const *m2l_a;      /* [40] dense: M2L [n*n]; SVD: M2 [n*r]    */
+  const double *const *m2l_b;      /* [40] SVD: M1 [r*n]; otherwise unused    */
+} fmm_level_ops;
+
+int fmm_ops_create(int kernel_id, const double *kernel_params /* [4] or NULL */, int nequiv,
+                   fmm_ops **out);
+int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *level, int *level_id);
+int fmm_ops_destroy(fmm_ops *ops);
+
+/* Build the quadtree of n sources (device x, y) with at most ncutoff points
+ * per leaf over the square bbox = {xmin, xmax, ymin, ymax} (host array). */
+int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
+                    const double *bbox, void *stream, fmm_plan **out);
+/* n_levels and, for each level, its box width and node count (host arrays of
+ * FMM_MAX_LEVELS entries). */
+int fmm_plan_info(fmm_plan *plan, int *n_levels, double *widths, int *n_nodes);
+/* Use operator entry level_id (from fmm_ops_add) for tree level `level`. */
+int fmm_plan_bind(fmm_plan *plan, int level, int level_id);
+/* tau: device charges [n] in the caller's (original) source order. */
+int fmm_build_expansions(fmm_plan *plan, const double *tau, void *stream);
+/* Potential at m device points into device out[m]; check != 0 skips sources
+ * that coincide with the target (source evaluation). */
+int fmm_evaluate(fmm_plan *plan, const double *tx, const double *ty, int64_t m, int check,
+                 double *out, void *stream);
+int fmm_plan_destroy(fmm_plan *plan);
+
+/* Copy the tree to host arrays sized by fmm_plan_info (nodes = sum n_nodes):
+ * xmin, ymin [nodes]; bot, top, parent, child [nodes]; flags [nodes]
+ * (1 leaf, 2 fake leaf, 4 X-list, 8 has children); coll [nodes*9];
+ * il [nodes*40] (source node per offset, -1 none); ordv [n] (sorted ->
+ * original source index).  Any pointer may be NULL. */
+int fmm_tree_export(fmm_plan *plan, double *xmin, double *ymin, int *bot, int *top, int *parent,
+                    int *child, uint8_t *flags, int *coll, int *il, int *ordv);
+
+const char *fmm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

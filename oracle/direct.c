@@ -1,0 +1,32 @@
+/* FP64 direct summation, the accuracy oracle for every FMM result.
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/ and bench.py to measure the error
+ * of FMM outputs against the exact sum.  Restates kernel_apply /
+ * kernel_apply_single_check (flexmm/flexmm2d/helpers.py:91-116): the sum over
+ * all sources, skipping a source that coincides with the target in both
+ * coordinates when `check` is set.
+ *
+ * Build: gcc -O2 -fopenmp -shared -fPIC direct.c -o _build/liboracle_direct.so -lm
+ * (no -ffast-math: the sums are plain IEEE double).
+ */
+#include <math.h>
+#include <stdint.h>
+
+/* Laplace: -log(|t-s|^2) / (4 pi), examples/kifmm_laplace.py:24-29 */
+void oracle_direct_laplace(const double *sx, const double *sy, const double *tau,
+                           int64_t ns, const double *tx, const double *ty,
+                           int64_t nt, int check, double *out)
+{
+    const double c = 1.0 / (4.0 * M_PI);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t j = 0; j < nt; ++j) {
+        double acc = 0.0;
+        const double x = tx[j], y = ty[j];
+        for (int64_t i = 0; i < ns; ++i) {
+            double dx = x - sx[i], dy = y - sy[i];
+            if (check && dx == 0.0 && dy == 0.0) continue;
+            acc += -log(dx * dx + dy * dy) * c * tau[i];
+        }
+        out[j] = acc;
+    }
+}

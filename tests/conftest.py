@@ -1,0 +1,49 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HERE = os.path.dirname(os.path.abspath(__file__))
+for p in (REPO, HERE):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(HERE, "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+
+
+def golden_cases():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load_golden(name):
+    import json
+    d = dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
+    d["meta"] = json.loads(str(d["meta"]))
+    if "tree_sha" in d:
+        d["tree_sha"] = json.loads(str(d["tree_sha"]))
+    return d
+
+
+def golden_inputs(meta):
+    sys.path.insert(0, GOLDEN)
+    from make_golden import case_inputs
+    return case_inputs(meta)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="session")
+def built_lib():
+    """Path of the built CUDA library (built here with nvcc when missing)."""
+    from flexmm_b200 import build
+    return build.build()

@@ -1,0 +1,154 @@
+"""Generate the golden fixtures by running the reference flexmm itself.
+
+Run in a container that has the reference checkout (it is copied into
+``oracle/_ref`` and imported with host shims by ``oracle.refimport``):
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py small      # only the quick ones
+
+For every case the inputs are regenerated from ``flexmm_b200.workloads``
+recipes (seeded numpy), the reference ``KI_FMM`` is built with a fresh
+``KI_Helper`` (never the shared default helper), and the fixture stores:
+
+* ``meta``      the case description (recipe, seed, sizes, Ncutoff, Nequiv, bbox)
+* ``inputs_sha`` sha256 of the input arrays, so drift of the generator is caught
+* ``src_idx`` / ``src_val``  source-evaluation results (all, or a seeded sample)
+* ``tgt_idx`` / ``tgt_val``  target-evaluation results (all, or a seeded sample)
+* ``direct_src`` / ``direct_tgt`` FP64 direct sums at the sampled points
+* ``tree_sha``  sha256 of every canonical tree array of the reference tree
+  (``tests/canon.py``), for cases small enough to canonicalise quickly
+"""
+import hashlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from flexmm_b200 import workloads  # noqa: E402
+from oracle import refimport  # noqa: E402
+from oracle.direct import direct_laplace  # noqa: E402
+import canon  # noqa: E402
+
+
+def sha(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def case_inputs(meta):
+    kind = meta["recipe"]
+    if kind == "uniform":
+        d = workloads.uniform(n=meta["n"], n_grid=meta["n_grid"], seed=meta["seed"])
+    elif kind == "clustered":
+        d = workloads.clustered(n=meta["n"], n_grid=meta["n_grid"], seed=meta["seed"])
+    elif kind == "circle":
+        d = workloads.circle(n=meta["n"], n_rhs=1, seed=meta["seed"])
+        d["tau"] = d["tau"][0]
+        g = np.linspace(-0.45, 0.45, meta["n_grid"])
+        gx, gy = np.meshgrid(g, g)
+        d["tx"], d["ty"] = gx.ravel(), gy.ravel()
+    elif kind == "duplicates":
+        rng = np.random.default_rng(meta["seed"])
+        n = meta["n"]
+        x = rng.uniform(-1, 1, n)
+        y = rng.uniform(-1, 1, n)
+        # every fifth point is repeated once: coincident sources
+        x[1::5] = x[0::5][: x[1::5].size]
+        y[1::5] = y[0::5][: y[1::5].size]
+        tau = rng.standard_normal(n)
+        tx, ty = workloads.grid(meta["n_grid"])
+        d = dict(x=x, y=y, tau=tau, tx=tx, ty=ty, bbox=[-1.0, 1.0, -1.0, 1.0])
+    else:
+        raise ValueError(kind)
+    if meta.get("bbox", "given") == "none":
+        d["bbox"] = None
+    return d
+
+
+CASES = {
+    # name: (meta, small)
+    "uniform_3k_q16": (dict(recipe="uniform", seed=10, n=3000, n_grid=41, ncut=16, neq=16), True),
+    "uniform_100_q16": (dict(recipe="uniform", seed=11, n=100, n_grid=9, ncut=16, neq=16), True),
+    "clustered_20k_q32": (dict(recipe="clustered", seed=12, n=20000, n_grid=64, ncut=32, neq=32), True),
+    "clustered_20k_q60": (dict(recipe="clustered", seed=13, n=20000, n_grid=64, ncut=64, neq=60), True),
+    "circle_20k_q24_nobbox": (dict(recipe="circle", seed=14, n=20000, n_grid=50, ncut=32, neq=24,
+                                   bbox="none"), True),
+    "duplicates_5k_q24": (dict(recipe="duplicates", seed=15, n=5000, n_grid=33, ncut=16, neq=24), True),
+    "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
+                              sample=2000), False),
+    "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
+                              sample=2000), False),
+    "clustered_1M_q24": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=24,
+                              sample=2000), False),
+}
+
+
+def run_case(name, meta, ref):
+    import numba
+    from flexmm.flexmm2d.kifmm import KI_FMM, KI_Helper
+
+    @numba.njit(fastmath=True)
+    def Laplace_Eval(sx, sy, tx, ty):
+        dx = tx - sx
+        dy = ty - sy
+        d2 = dx**2 + dy**2
+        return -np.log(d2) / (4 * np.pi)
+
+    d = case_inputs(meta)
+    t0 = time.time()
+    F = KI_FMM(d["x"], d["y"], Laplace_Eval, meta["ncut"], meta["neq"], bbox=d["bbox"],
+               helper=KI_Helper())
+    F.build_expansions(d["tau"])
+    us = F.source_evaluation(d["x"], d["y"])
+    ut = F.target_evaluation(d["tx"], d["ty"])
+    t1 = time.time()
+    rng = np.random.default_rng(12345)
+    if "sample" in meta:
+        si = np.sort(rng.choice(d["x"].size, meta["sample"], replace=False))
+        ti = np.sort(rng.choice(d["tx"].size, meta["sample"], replace=False))
+    else:
+        si = np.arange(d["x"].size)
+        ti = np.arange(d["tx"].size)
+    ds = direct_laplace(d["x"], d["y"], d["tau"], d["x"][si], d["y"][si], True)
+    dt = direct_laplace(d["x"], d["y"], d["tau"], d["tx"][ti], d["ty"][ti], False)
+    out = dict(
+        meta=json.dumps(meta),
+        inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),
+        bbox_used=np.array(F.bbox, dtype=np.float64),
+        levels=np.int64(F.tree.levels),
+        src_idx=si, src_val=us[si], tgt_idx=ti, tgt_val=ut[ti],
+        direct_src=ds, direct_tgt=dt,
+    )
+    if "sample" not in meta:
+        c = canon.canonical(F.tree)
+        out["tree_sha"] = json.dumps({k: sha(np.asarray(v, dtype=np.int64)) for k, v in c.items()})
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"{name}: levels {F.tree.levels} ref {t1 - t0:.1f}s  err vs direct src {rel(us[si], ds):.2e} "
+          f"tgt {rel(ut[ti], dt):.2e}", flush=True)
+
+
+def main():
+    only_small = len(sys.argv) > 1 and sys.argv[1] == "small"
+    names = [a for a in sys.argv[1:] if a in CASES]
+    refimport.build_ref()
+    ref = refimport.load_reference()
+    for name, (meta, small) in CASES.items():
+        if names and name not in names:
+            continue
+        if only_small and not small:
+            continue
+        run_case(name, meta, ref)
+
+
+if __name__ == "__main__":
+    main()

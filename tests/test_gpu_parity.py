@@ -1,0 +1,129 @@
+"""CUDA path against the reference (golden fixtures) and the CPU oracle.
+
+Bar: FP64 results within 1e-12 relative L2 of the reference's own outputs
+on the same inputs; the tree equal to the reference's box for box.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, golden_inputs, load_golden, rel_l2
+import canon
+
+pytestmark = pytest.mark.gpu
+
+PARITY = 1e-12
+
+
+def _fmm(d, meta, helper=None):
+    from flexmm_b200 import KI_FMM, KI_Helper
+    return KI_FMM(d["x"], d["y"], "Laplace_Eval", meta["ncut"], meta["neq"], bbox=d["bbox"],
+                  helper=helper if helper is not None else KI_Helper())
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_results_match_reference(built_lib, case):
+    g = load_golden(case)
+    meta = g["meta"]
+    d = golden_inputs(meta)
+    F = _fmm(d, meta)
+    assert np.array_equal(np.array(F.bbox), g["bbox_used"])
+    F.build_expansions(d["tau"])
+    us = F.source_evaluation(d["x"], d["y"])
+    ut = F.target_evaluation(d["tx"], d["ty"])
+    es = rel_l2(us[g["src_idx"]], g["src_val"])
+    et = rel_l2(ut[g["tgt_idx"]], g["tgt_val"])
+    assert es < PARITY and et < PARITY, (es, et)
+
+
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "sample" not in load_golden(c)["meta"]])
+def test_tree_matches_oracle(built_lib, case):
+    from oracle.tree import Tree
+    g = load_golden(case)
+    meta = g["meta"]
+    d = golden_inputs(meta)
+    F = _fmm(d, meta)
+    ot = Tree(d["x"], d["y"], meta["ncut"], F.bbox)
+    a = canon.canonical(F.tree, triples_fn=canon.gpu_triples, nonempty_sources=True)
+    b = canon.canonical(ot, nonempty_sources=True)
+    assert canon.compare(a, b) == []
+
+
+def _direct(d, tx, ty, check):
+    from oracle.direct import direct_laplace
+    return direct_laplace(d["x"], d["y"], d["tau"], tx, ty, check)
+
+
+@pytest.mark.parametrize("n,ncut", [(40, 64), (64, 64), (200, 64), (300, 100)])
+def test_shallow_trees_equal_direct_sum(built_lib, n, ncut):
+    """Trees of 1-2 levels (where the reference itself fails) reduce to the direct sum."""
+    from flexmm_b200 import KI_FMM, KI_Helper
+    rng = np.random.default_rng(n)
+    d = dict(x=rng.uniform(-1, 1, n), y=rng.uniform(-1, 1, n), tau=rng.standard_normal(n))
+    F = KI_FMM(d["x"], d["y"], "Laplace_Eval", ncut, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper())
+    F.build_expansions(d["tau"])
+    tx, ty = rng.uniform(-1, 1, 77), rng.uniform(-1, 1, 77)
+    if F.tree.levels < 3:
+        assert rel_l2(F.target_evaluation(tx, ty), _direct(d, tx, ty, False)) < 1e-13
+        assert rel_l2(F.source_evaluation(d["x"], d["y"]), _direct(d, d["x"], d["y"], True)) < 1e-13
+
+
+def test_matches_oracle_midsize_and_torch_inputs(built_lib):
+    import torch
+    from flexmm_b200 import workloads
+    from oracle.kifmm import KIFMM
+    from oracle.kernels import laplace
+    d = workloads.clustered(n=60000, n_grid=120, seed=21)
+    meta = dict(ncut=40, neq=40)
+    O = KIFMM(d["x"], d["y"], laplace, 40, 40, bbox=d["bbox"])
+    O.build_expansions(d["tau"])
+    F = _fmm(d, meta)
+    F.build_expansions(torch.from_numpy(d["tau"]).cuda())
+    ut = F.target_evaluation(torch.from_numpy(d["tx"]).cuda(), torch.from_numpy(d["ty"]).cuda())
+    assert isinstance(ut, torch.Tensor) and ut.is_cuda
+    assert rel_l2(ut.cpu().numpy(), O.target_evaluation(d["tx"], d["ty"])) < PARITY
+    us = F.source_evaluation(d["x"], d["y"])
+    assert rel_l2(us, O.source_evaluation(d["x"], d["y"])) < PARITY
+
+
+def test_targets_outside_bbox_follow_reference_descent(built_lib):
+    from flexmm_b200 import workloads
+    from oracle.kifmm import KIFMM
+    from oracle.kernels import laplace
+    d = workloads.uniform(n=20000, n_grid=10, seed=5)
+    rng = np.random.default_rng(9)
+    tx = rng.uniform(-1.3, 1.3, 3000)
+    ty = rng.uniform(-1.3, 1.3, 3000)
+    O = KIFMM(d["x"], d["y"], laplace, 32, 24, bbox=d["bbox"])
+    O.build_expansions(d["tau"])
+    F = _fmm(d, dict(ncut=32, neq=24))
+    F.build_expansions(d["tau"])
+    assert rel_l2(F.target_evaluation(tx, ty), O.target_evaluation(tx, ty)) < PARITY
+
+
+def test_helper_reuse_snaps_bbox_like_reference(built_lib):
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    from oracle.kifmm import snap_bbox
+    d = workloads.uniform(n=5000, n_grid=10, seed=6)
+    h = KI_Helper()
+    F1 = KI_FMM(d["x"], d["y"], "Laplace_Eval", 32, 16, bbox=[-1, 1, -1, 1], helper=h)
+    widths = h.collect_widths()
+    F2 = KI_FMM(d["x"] * 0.3, d["y"] * 0.3, "Laplace_Eval", 32, 16, bbox=None, helper=h)
+    bb = [np.min(d["x"] * 0.3), np.max(d["x"] * 0.3), np.min(d["y"] * 0.3), np.max(d["y"] * 0.3)]
+    assert np.allclose(F2.bbox, snap_bbox(None, None, bb, widths), rtol=0, atol=0)
+    with pytest.raises(ValueError):
+        KI_FMM(d["x"], d["y"], "Laplace_Eval", 32, 24, bbox=[-1, 1, -1, 1], helper=h)
+
+
+def test_empty_evaluation_and_errors(built_lib):
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    from flexmm_b200._lib import FMMError
+    d = workloads.uniform(n=3000, n_grid=10, seed=7)
+    F = KI_FMM(d["x"], d["y"], "Laplace_Eval", 32, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper())
+    with pytest.raises(FMMError):
+        F.target_evaluation(d["tx"], d["ty"])     # before build_expansions
+    F.build_expansions(d["tau"])
+    assert F.target_evaluation(np.zeros(0), np.zeros(0)).shape == (0,)
+    # more than Ncutoff coincident points cannot be split: clean error, no hang
+    x = np.zeros(100)
+    with pytest.raises(FMMError):
+        KI_FMM(x, x, "Laplace_Eval", 16, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper())
