@@ -1,0 +1,501 @@
+#!/usr/bin/env python
+"""Benchmark of the 2D Laplace KIFMM evaluation path on B200.
+
+Workload (one "step"): the clustered configuration -- 1,000,000 sources in
+20 Gaussian clusters (centres U[-0.9,0.9]^2, sigma 0.01), charges N(0,1),
+evaluated at the sources (self-interaction excluded) and on a 1000 x 1000
+grid over [-1,1]^2; at most 64 points per leaf.  A step is what the
+reference's examples time: build the FMM object (quadtree), form the
+expansions, evaluate at the sources, evaluate at the grid, with the
+per-width operators already cached (helper reuse).
+Metric: million points per second, (N_sources + N_targets) / step time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64]
+    python bench.py --impl reference ...    # the reference flexmm on the host CPU
+
+``value`` is timed on the device with CUDA events, inputs resident in HBM,
+L2 flushed between steps; ``e2e`` is the same step through the public API
+from pinned host buffers, copies and the read-back of both results included.
+With N > 1 (torchrun) every rank runs an independent replica of the step
+(the path does not shard a single problem); value sums the ranks' points
+over the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "Mpts/s, 1M Laplace KIFMM on 1 B200, mixed vs FP64 at rel err 1e-6; ref CPU"
+NCUT = 64
+NEQ = {"fp64": 60}
+C_LAPLACE = 20          # flops per Laplace kernel evaluation (9 arithmetic + log as 11)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=sorted(NEQ), default="fp64")
+    p.add_argument("--n", type=int, default=1_000_000, help="sources (default: the 1M config)")
+    p.add_argument("--grid", type=int, default=1000, help="grid targets per side")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-n", type=int, default=200_000)
+    p.add_argument("--json-only", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--ncu", action="store_true",
+                   help="profiling mode: warm-up and timed steps only (no accuracy, e2e, peaks)")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- helpers --
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            backend = "nccl"
+        else:
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def dist_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling (200 ms) while the timed loops run."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.rows = []
+        self.thread = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __enter__(self):
+        import threading
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, bufsize=1)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)   # first sample lands before the timed work starts
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread is not None:
+                self.thread.join(timeout=5)
+
+    def summary(self):
+        rows = self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        num = lambda v: v.replace(".", "", 1).isdigit()
+        sm = [float(r[1]) for r in rows if num(r[1])]
+        smax = [float(r[2]) for r in rows if num(r[2])]
+        pw = [float(r[3]) for r in rows if num(r[3])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(pw) if pw else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def fp64_peak_tflops(torch):
+    """FP64 throughput of this GPU, measured with a cuBLAS DGEMM (8192^3)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+# ------------------------------------------------------------- work counts --
+def work_counts(F, tx, ty, nequiv):
+    """Algorithmic work of one step from the tree (kernel evaluations, GEMM flops)."""
+    t = F.tree
+    ops_rank = {}
+    counts = dict(p2p_pairs_src=0, p2p_pairs_tgt=0, m2l_flops=0, s2m_ke=0, l2t_ke=0,
+                  m2m_flops=0, l2l_flops=0, c2e_flops=0)
+
+    def locate(px, py):
+        inds = np.zeros(px.size, np.int64)
+        locs = np.zeros(px.size, np.int64)
+        active = np.flatnonzero(~t.Levels[0].leaf[locs])
+        ind = 0
+        while active.size:
+            lv = t.Levels[ind]
+            loc = locs[active]
+            c = lv.children_ind[loc] + 2 * (px[active] > lv.xmid[loc]) + (py[active] > lv.ymid[loc])
+            ind += 1
+            locs[active] = c
+            inds[active] = ind
+            active = active[~t.Levels[ind].leaf[c]]
+        return inds, locs
+
+    def pairs(px, py):
+        inds, locs = locate(px, py)
+        tot = 0
+        for ind in np.unique(inds):
+            lv = t.Levels[ind]
+            sel = locs[inds == ind]
+            col = lv.colleagues[sel]
+            ok = col >= 0
+            tot += int(np.where(ok, lv.ns[np.where(ok, col, 0)], 0).sum())
+        return tot
+
+    x = F._x.cpu().numpy()
+    y = F._y.cpu().numpy()
+    counts["p2p_pairs_src"] = pairs(x, y)
+    counts["p2p_pairs_tgt"] = pairs(tx, ty)
+    counts["l2t_ke"] = nequiv * (x.size + tx.size)
+    n = nequiv
+    for ind, lv in enumerate(t.Levels):
+        if ind < 2:
+            continue
+        prec = F.helper.get_precomputation(lv.width)
+        ranks = prec.m2l_rank
+        tr = t.interaction_triples(ind)
+        if tr.size:
+            grid49 = np.array([(a + 3) * 7 + (b + 3) for a in range(-3, 4) for b in range(-3, 4)
+                               if not (abs(a) <= 1 and abs(b) <= 1)])
+            pos = {g: o for o, g in enumerate(grid49)}
+            per_off = np.bincount([pos[g] for g in tr[:, 1]], minlength=40)
+            fl = np.where(ranks < 0, 2 * n * n, 4 * n * np.maximum(ranks, 0))
+            counts["m2l_flops"] += int((per_off * fl).sum())
+        up = lv.compute_upwards
+        counts["s2m_ke"] += n * int(lv.ns[up].sum())
+        counts["m2m_flops"] += 2 * n * 4 * n * int(((lv.children_ind >= 0)).sum())
+        real = ~lv.fake_leaf
+        counts["c2e_flops"] += 2 * 4 * n * n * int(real.sum())
+        if ind >= 3:
+            counts["l2l_flops"] += 2 * n * n * int(real.sum())
+    return counts
+
+
+# ---------------------------------------------------------------- our arm --
+def run_ours(args, world, rank, local):
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, direct_evaluation, enable_timing, read_timing, workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    neq = NEQ[args.precision]
+    d = workloads.clustered(n=args.n, n_grid=args.grid)
+    n_src, n_tgt = d["x"].size, d["tx"].size
+    pts = n_src + n_tgt
+    xd, yd, taud, txd, tyd = (torch.from_numpy(d[k]).to(dev) for k in ("x", "y", "tau", "tx", "ty"))
+    helper = KI_Helper()
+
+    def step(x, y, tau, tx, ty):
+        F = KI_FMM(x, y, "Laplace_Eval", NCUT, neq, bbox=d["bbox"], helper=helper)
+        F.build_expansions(tau)
+        us = F.source_evaluation(x, y)
+        ut = F.target_evaluation(tx, ty)
+        return F, us, ut
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(max(args.warmup, 0)):
+        F, us, ut = step(xd, yd, taud, txd, tyd)
+    torch.cuda.synchronize()
+    if args.ncu:
+        for _ in range(args.steps):
+            step(xd, yd, taud, txd, tyd)
+        torch.cuda.synchronize()
+        return
+
+    # accuracy of this step's results: FP64 direct sums on 2000-point samples,
+    # and agreement with the reference's own outputs (committed fixture)
+    rng = np.random.default_rng(12345)
+    si = np.sort(rng.choice(n_src, min(2000, n_src), replace=False))
+    ti = np.sort(rng.choice(n_tgt, min(2000, n_tgt), replace=False))
+    us_h, ut_h = us.cpu().numpy(), ut.cpu().numpy()
+    ds = direct_evaluation("Laplace_Eval", xd, yd, taud, xd[si], yd[si], check=True).cpu().numpy()
+    dt = direct_evaluation("Laplace_Eval", xd, yd, taud, txd[ti], tyd[ti]).cpu().numpy()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    accuracy = {"src_rel_l2_vs_direct": rel(us_h[si], ds), "tgt_rel_l2_vs_direct": rel(ut_h[ti], dt),
+                "sample": "2000 sources + 2000 grid targets, FP64 direct sum on the GPU"}
+    gold = os.path.join(REPO, "tests", "golden", f"clustered_1M_q{neq}.npz")
+    if args.n == 1_000_000 and args.grid == 1000 and os.path.exists(gold):
+        g = np.load(gold)
+        accuracy["src_rel_l2_vs_reference"] = rel(us_h[g["src_idx"]], g["src_val"])
+        accuracy["tgt_rel_l2_vs_reference"] = rel(ut_h[g["tgt_idx"]], g["tgt_val"])
+
+    # launches of our kernels in one step (CUPTI through torch.profiler, untimed)
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step(xd, yd, taud, txd, tyd)
+        torch.cuda.synchronize()
+    launches_per_step = 0
+    for ev in prof.events():
+        if getattr(ev, "device_type", None) is not None and str(ev.device_type).endswith("CUDA"):
+            name = ev.name.lower()
+            if "memcpy" in name or "memset" in name:
+                continue
+            launches_per_step += 1
+
+    # timed region: K steps, L2 flushed between steps, CUDA events on the stream
+    enable_timing(True)
+    read_timing()
+    barrier(world)
+    torch.cuda.synchronize()
+    times = []
+    clk = ClockSampler(local).__enter__()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(xd, yd, taud, txd, tyd)
+        e1.record()
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier(world)
+    phases = read_timing()
+    enable_timing(False)
+    ms_total = sum(a.elapsed_time(b) for a, b in times)
+    ms_step = dist_max(ms_total / max(args.steps, 1), world)
+    value = world * pts / (ms_step * 1e-3) / 1e6
+
+    # end to end through the public API from pinned host memory
+    pin = {k: torch.from_numpy(d[k]).pin_memory() for k in ("x", "y", "tau", "tx", "ty")}
+    e2e_ms = []
+    barrier(world)
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        F2, us2, ut2 = step(pin["x"], pin["y"], pin["tau"], pin["tx"], pin["ty"])
+        e1.record()
+        torch.cuda.synchronize()
+        assert not us2.is_cuda and not ut2.is_cuda
+        e2e_ms.append(e0.elapsed_time(e1))
+    clk.__exit__(None, None, None)
+    e2e_step = dist_max(statistics.mean(e2e_ms), world)
+    h2d = 8 * (2 * n_src + n_src + 2 * n_src + 2 * n_tgt)
+    d2h = 8 * (n_src + n_tgt)
+
+    # roofline of the dominant kernel
+    counts = work_counts(F, d["tx"], d["ty"], neq)
+    kernel_flops = {
+        "evaluate": C_LAPLACE * (counts["p2p_pairs_src"] + counts["p2p_pairs_tgt"] + counts["l2t_ke"]),
+        "m2l": counts["m2l_flops"],
+        "upward": C_LAPLACE * counts["s2m_ke"] + counts["m2m_flops"] + counts["c2e_flops"] // 2,
+        "downward": counts["l2l_flops"] + counts["c2e_flops"] // 2,
+    }
+    dom = max(kernel_flops, key=lambda k: phases[k][0])
+    ms_k, n_launch = phases[dom]
+    flops_per_launch = kernel_flops[dom] * args.steps / max(n_launch, 1)
+    achieved = flops_per_launch / (ms_k / max(n_launch, 1) * 1e-3) / 1e12
+    peak = fp64_peak_tflops(torch)
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"{args.precision}:{dom}")
+    roofline = {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": "measured on this GPU: cuBLAS DGEMM 8192^3 (FP64 pipe), in bench.py",
+                "flops_per_launch": flops_per_launch,
+                "ms_per_launch": ms_k / max(n_launch, 1)}
+    phase_ms = {k: v[0] / max(args.steps, 1) for k, v in phases.items() if v[1]}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "precision": args.precision,
+        "data": "synthetic: seeded clustered sources and grid targets (no dataset)",
+        "config": {"workload": f"clustered Laplace KIFMM, {n_src} sources + {args.grid}^2 grid targets, "
+                               f"self + target evaluation", "n_sources": n_src, "n_targets": n_tgt,
+                   "ncutoff": NCUT, "nequiv": neq, "precision": args.precision,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MB write) between timed steps",
+                   "levels": F._levels, "nodes": int(sum(F._counts))},
+        "accuracy": accuracy,
+        "phase_ms_per_step": phase_ms,
+        "work_per_step": counts,
+        "clocks": clk.summary(),
+        "e2e": {"value": world * pts / (e2e_step * 1e-3) / 1e6, "unit": "Mpts/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": roofline,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_subprocess(args)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------- reference arm --
+def reference_step_fn(n_src, n_grid, neq):
+    """Closure timing one step of the reference flexmm on the host CPU."""
+    from oracle import refimport  # the reference itself (shimmed copy), checker-only
+    from flexmm_b200 import workloads
+    refimport.load_reference()
+    import numba
+    from flexmm.flexmm2d.kifmm import KI_FMM, KI_Helper
+
+    @numba.njit(fastmath=True)
+    def Laplace_Eval(sx, sy, tx, ty):
+        dx = tx - sx
+        dy = ty - sy
+        d2 = dx**2 + dy**2
+        return -np.log(d2) / (4 * np.pi)
+
+    d = workloads.clustered(n=n_src, n_grid=n_grid)
+    helper = KI_Helper()
+
+    def step():
+        t0 = time.perf_counter()
+        F = KI_FMM(d["x"], d["y"], Laplace_Eval, NCUT, neq, bbox=d["bbox"], helper=helper)
+        F.build_expansions(d["tau"])
+        F.source_evaluation(d["x"], d["y"])
+        F.target_evaluation(d["tx"], d["ty"])
+        return time.perf_counter() - t0
+
+    return step, d["x"].size + d["tx"].size
+
+
+def reference_available():
+    from oracle import refimport
+    return refimport.reference_available()
+
+
+def cpu_baseline_subprocess(args):
+    """Time the reference on the host in a fresh process (all cores)."""
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, NUMBA_NUM_THREADS=str(cores), CUDA_VISIBLE_DEVICES="")
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "2",
+           "--warmup", "1", "--precision", args.precision, "--cpu-sample-n",
+           str(args.cpu_sample_n), "--json-only"]
+    try:
+        r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+        line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+        ref = json.loads(line)
+        return ref.get("cpu_baseline", {"unavailable": ref.get("unavailable")})
+    except Exception as e:  # the GPU number stands without it
+        return {"unavailable": f"reference run failed: {type(e).__name__}: {e}"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    neq = NEQ[args.precision]
+    grid = int(round(np.sqrt(args.cpu_sample_n)))
+    base = {"impl": "reference", "metric": METRIC, "unit": "Mpts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded clustered sources and grid targets (no dataset)",
+            "config": {"workload": f"clustered Laplace KIFMM, {args.n} sources + {args.grid}^2 grid "
+                                   f"targets, self + target evaluation", "ncutoff": NCUT,
+                       "nequiv": neq, "precision": args.precision}}
+    if not reference_available():
+        base["unavailable"] = "reference copy oracle/_ref not built (needs the reference checkout)"
+        print(json.dumps(base), flush=True)
+        return
+    cores = int(os.environ.get("NUMBA_NUM_THREADS", os.cpu_count() or 1))
+    step, pts = reference_step_fn(args.cpu_sample_n, grid, neq)
+    for _ in range(max(args.warmup, 1)):
+        step()
+    ts = [step() for _ in range(max(args.steps, 1))]
+    sec = statistics.mean(ts)
+    value = pts / sec / 1e6
+    sample = (f"reference flexmm KI_FMM (numba, {cores} threads), clustered {args.cpu_sample_n} "
+              f"sources + {grid}^2 grid targets, Nequiv {neq}, warm JIT and operators; per step: "
+              f"tree + build_expansions + source_evaluation + target_evaluation")
+    base.update({"value": value, "ms_per_step": sec * 1e3,
+                 "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores,
+                                  "kind": "reference", "sample": sample},
+                 "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(base), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

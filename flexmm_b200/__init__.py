@@ -12,8 +12,9 @@ sm_100a CUDA behind the C ABI in ``include/flexmm_b200.h``); build it with
 """
 from .helpers import KI_Helper
 from .kernels import Kernel, Laplace, resolve
-from .kifmm import KI_FMM
+from .kifmm import KI_FMM, direct_evaluation, enable_timing, read_timing
 
 Laplace_Eval = Laplace()
 
-__all__ = ["KI_FMM", "KI_Helper", "Kernel", "Laplace", "Laplace_Eval", "resolve"]
+__all__ = ["KI_FMM", "KI_Helper", "Kernel", "Laplace", "Laplace_Eval", "resolve",
+           "direct_evaluation", "enable_timing", "read_timing"]

@@ -11,6 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libflexmm_b200.so")
 
 N_OFFSETS = 40
+N_PHASES = 8
+PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "spare"]
 MAX_LEVELS = 30
 MAX_NEQUIV = 64
 
@@ -48,6 +50,10 @@ SIGNATURES = [
     ("fmm_evaluate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),
     ("fmm_plan_destroy", ctypes.c_int, [_vp]),
     ("fmm_tree_export", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("fmm_direct", ctypes.c_int, [ctypes.c_int, _dp, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp,
+                                  ctypes.c_int64, ctypes.c_int, _vp, _vp]),
+    ("fmm_timing_enable", ctypes.c_int, [ctypes.c_int]),
+    ("fmm_timing_read", ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int64)]),
     ("fmm_last_error", ctypes.c_char_p, []),
 ]
 

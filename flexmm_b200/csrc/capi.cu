@@ -7,6 +7,7 @@
 
 #include "../../include/flexmm_b200.h"
 #include "fmm.cuh"
+#include "timing.cuh"
 
 using namespace fmmb;
 
@@ -189,7 +190,10 @@ int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, i
     auto p = std::make_unique<fmm_plan>();
     p->ops = ops;
     p->stream = (cudaStream_t)stream;
-    build_tree(p->td, p->th, x, y, n, ncutoff, bbox, p->stream);
+    {
+      PhaseTimer timer(PH_TREE, p->stream);
+      build_tree(p->td, p->th, x, y, n, ncutoff, bbox, p->stream);
+    }
     p->bound.assign(p->th.L, -1);
     *out = p.release();
   });
@@ -273,12 +277,15 @@ int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int
     PassArgs a = pass_args(p);
     DevBuf<uint64_t> tkeys;
     DevBuf<int> tperm;
-    sort_points(tx, ty, m, p->th, tkeys, tperm, s);
     DevBuf<double> txs, tys;
-    txs.alloc(m, s);
-    tys.alloc(m, s);
-    gather_sorted(tx, tperm.get(), m, txs.get(), s);
-    gather_sorted(ty, tperm.get(), m, tys.get(), s);
+    {
+      PhaseTimer timer(PH_SORT_TGT, s);
+      sort_points(tx, ty, m, p->th, tkeys, tperm, s);
+      txs.alloc(m, s);
+      tys.alloc(m, s);
+      gather_sorted(tx, tperm.get(), m, txs.get(), s);
+      gather_sorted(ty, tperm.get(), m, tys.get(), s);
+    }
     run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(), m,
                  check, out, s);
   });
@@ -312,6 +319,50 @@ int fmm_tree_export(fmm_plan *p, double *xmin, double *ymin, int *bot, int *top,
     cp(il, p->td.il.get(), T * N_OFFSETS * sizeof(int));
     cp(ordv, p->td.ordv.get(), size_t(p->th.n_points) * sizeof(int));
     FMMB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int fmm_direct(int kernel_id, const double *kparams, const double *sx, const double *sy,
+               const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
+               int check, double *out, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(kernel_id == KERNEL_LAPLACE, ERR_UNSUPPORTED, "unknown kernel id");
+    FMMB_CHECK(ns >= 0 && nt >= 0, ERR_INVALID_ARGUMENT, "negative size");
+    if (nt == 0) return;
+    FMMB_CHECK(tx && ty && out && (ns == 0 || (sx && sy && tau)), ERR_INVALID_ARGUMENT,
+               "NULL argument");
+    KernelParams kp;
+    for (int i = 0; i < 4; ++i) kp.p[i] = kparams ? kparams[i] : 0.0;
+    run_direct(kernel_id, kp, sx, sy, tau, ns, tx, ty, nt, check, out, (cudaStream_t)stream);
+  });
+}
+
+int fmm_timing_enable(int on) {
+  return guarded([&] {
+    auto &R = TimingRegistry::get();
+    std::lock_guard<std::mutex> g(R.mu);
+    R.enabled = on != 0;
+  });
+}
+
+int fmm_timing_read(double *ms, int64_t *launches) {
+  return guarded([&] {
+    auto &R = TimingRegistry::get();
+    std::lock_guard<std::mutex> g(R.mu);
+    for (int i = 0; i < FMM_N_PHASES; ++i) {
+      if (ms) ms[i] = 0.0;
+      if (launches) launches[i] = 0;
+    }
+    for (auto &r : R.recs) {
+      FMMB_CUDA(cudaEventSynchronize(r.b));
+      float t = 0.f;
+      FMMB_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+      if (ms) ms[r.phase] += t;
+      if (launches) launches[r.phase] += 1;
+      R.pool.push_back(r.a);
+      R.pool.push_back(r.b);
+    }
+    R.recs.clear();
   });
 }
 

@@ -16,6 +16,7 @@
 #include <cub/cub.cuh>
 
 #include "fmm.cuh"
+#include "timing.cuh"
 
 namespace fmmb {
 namespace {
@@ -391,6 +392,42 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
   }
 }
 
+// FP64 direct sum (kernel_apply / kernel_apply_single_check,
+// flexmm/flexmm2d/helpers.py:91-116): all sources, one target per thread,
+// sources staged through shared memory
+template <class KF>
+__global__ void __launch_bounds__(256) k_direct(KernelParams kp, const double *__restrict__ sx,
+                                                const double *__restrict__ sy,
+                                                const double *__restrict__ tau, int64_t ns,
+                                                const double *__restrict__ tx,
+                                                const double *__restrict__ ty, int64_t nt,
+                                                int check, double *__restrict__ out) {
+  __shared__ double qx[256], qy[256], qt[256];
+  const KF K(kp);
+  for (int64_t base = (int64_t)blockIdx.x * 256; base < nt; base += (int64_t)gridDim.x * 256) {
+    const int64_t i = base + threadIdx.x;
+    const bool valid = i < nt;
+    const double x = valid ? tx[i] : 0.0, y = valid ? ty[i] : 0.0;
+    double u = 0.0;
+    for (int64_t j0 = 0; j0 < ns; j0 += 256) {
+      const int nj = (int)(ns - j0 < 256 ? ns - j0 : 256);
+      __syncthreads();
+      if (threadIdx.x < nj) {
+        qx[threadIdx.x] = sx[j0 + threadIdx.x];
+        qy[threadIdx.x] = sy[j0 + threadIdx.x];
+        qt[threadIdx.x] = tau[j0 + threadIdx.x];
+      }
+      __syncthreads();
+      if (valid)
+        for (int j = 0; j < nj; ++j) {
+          if (check && x - qx[j] == 0.0 && y - qy[j] == 0.0) continue;
+          u = fma(K(qx[j], qy[j], x, y), qt[j], u);
+        }
+    }
+    if (valid) out[i] = u;
+  }
+}
+
 __global__ void k_gather_sorted(const double *__restrict__ v, const int *__restrict__ perm,
                                 int64_t n, double *__restrict__ o) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -409,6 +446,7 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   for (int m = th.L - 1; m >= 2; --m) {
     const int gb = th.off[m], ge = th.off[m + 1];
     const int tiles = (ge - gb + TN - 1) / TN;
+    PhaseTimer timer(PH_UPWARD, s);
     k_upward<KF><<<tiles, NT, sm, s>>>(m, a.kp, a.neq, np, gb, ge, td.flags.get(), td.bot.get(),
                                        td.top.get(), td.child.get(), td.xmid.get(), td.ymid.get(),
                                        td.sx.get(), td.sy.get(), tau_s, a.ops_dev, mult);
@@ -437,6 +475,7 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
   DevBuf<uint8_t> tmp;
   tmp.alloc(bytes, s);
   FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, nch.get(), choff.get(), total, s));
+  PhaseTimer timer(PH_EVAL, s);
   k_evaluate<KF><<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, total, th.L, td.dev_off.get(),
                                          choff.get(), nch.get(), tb.get(), te.get(), td.coll.get(),
                                          td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(),
@@ -468,6 +507,7 @@ void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s)
   tsd.alloc(th.L + 1, s);
   FMMB_CUDA(cudaMemcpyAsync(tsd.get(), ts.data(), ts.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   const size_t sm = sizeof(double) * (size_t)TN * a.np * 2;
+  PhaseTimer timer(PH_M2L, s);
   k_m2l<<<tiles, NT, sm, s>>>(tsd.get(), th.L, a.td->dev_off.get(), a.np, a.td->il.get(), a.ops_dev,
                               mult, ple);
   FMMB_CUDA(cudaGetLastError());
@@ -480,6 +520,7 @@ void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_
   for (int m = 2; m < th.L; ++m) {
     const int gb = th.off[m], ge = th.off[m + 1];
     const int tiles = (ge - gb + TN - 1) / TN;
+    PhaseTimer timer(PH_DOWNWARD, s);
     k_downward<<<tiles, NT, sm, s>>>(m, a.np, gb, ge, td.flags.get(), td.parent.get(), a.ops_dev,
                                      ple, loc);
     FMMB_CUDA(cudaGetLastError());
@@ -496,6 +537,21 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
+}
+
+void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const double *sy,
+                const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
+                int check, double *out, cudaStream_t s) {
+  if (nt == 0) return;
+  PhaseTimer timer(PH_DIRECT, s);
+  const int grid = grid_for(nt, 256, 148 * 64);
+  switch (kernel_id) {
+    case KERNEL_LAPLACE:
+      k_direct<LaplaceF64><<<grid, 256, 0, s>>>(kp, sx, sy, tau, ns, tx, ty, nt, check, out);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+  FMMB_CUDA(cudaGetLastError());
 }
 
 void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaStream_t s) {

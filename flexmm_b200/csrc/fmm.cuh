@@ -37,6 +37,9 @@ void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaS
 void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s);
 void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s);
 // targets: sorted coordinates, sorted keys, permutation sorted -> original
+void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const double *sy,
+                const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
+                int check, double *out, cudaStream_t s);
 void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaStream_t s);
 void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc,
                   const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,

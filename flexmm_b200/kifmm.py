@@ -29,15 +29,27 @@ def _torch():
 
 
 def _device_f64(a):
-    """(device float64 contiguous 1-D tensor, was_numpy)."""
+    """(device float64 contiguous 1-D tensor, kind) with kind in
+    {"numpy", "cpu", "cuda"}: results are returned in the same kind."""
     torch = _torch()
     if isinstance(a, torch.Tensor):
+        kind = "cuda" if a.is_cuda else "cpu"
         t = a.reshape(-1)
         if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
-            t = t.to(device="cuda", dtype=torch.float64).contiguous()
-        return t, False
+            t = t.to(device="cuda", dtype=torch.float64, non_blocking=t.is_pinned()).contiguous()
+        return t, kind
     arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
-    return torch.from_numpy(arr).to("cuda", non_blocking=False), True
+    return torch.from_numpy(arr).to("cuda", non_blocking=False), "numpy"
+
+
+def _as_kind(out, kind, shape):
+    if kind == "numpy":
+        return out.cpu().numpy().reshape(shape)
+    if kind == "cpu":
+        host = _torch().empty(out.shape, dtype=out.dtype, pin_memory=True)
+        host.copy_(out)
+        return host
+    return out
 
 
 def _stream():
@@ -152,6 +164,7 @@ class KI_FMM:
                   ctypes.byref(plan))
         self._plan = plan
         self._ops = self.helper.ops_set()   # keep the operator set alive with the plan
+        self._x, self._y = xd, yd
         nl = ctypes.c_int()
         widths = (ctypes.c_double * _lib.MAX_LEVELS)()
         counts = (ctypes.c_int * _lib.MAX_LEVELS)()
@@ -187,7 +200,7 @@ class KI_FMM:
 
     def _evaluate(self, x, y, check):
         torch = _torch()
-        xd, was_np = _device_f64(x)
+        xd, kind = _device_f64(x)
         yd, _ = _device_f64(y)
         if xd.numel() != yd.numel():
             raise ValueError("x and y differ in length")
@@ -195,9 +208,7 @@ class KI_FMM:
         _lib.call("fmm_evaluate", self._plan, ctypes.c_void_p(xd.data_ptr()),
                   ctypes.c_void_p(yd.data_ptr()), xd.numel(), 1 if check else 0,
                   ctypes.c_void_p(out.data_ptr()), _stream())
-        if was_np:
-            return out.cpu().numpy().reshape(np.shape(x))
-        return out
+        return _as_kind(out, kind, np.shape(x))
 
     def source_evaluation(self, x, y):
         """Potential at (x, y), skipping coincident sources (flexmm/flexmm2d/fmm.py:158-159)."""
@@ -207,6 +218,13 @@ class KI_FMM:
         """Potential at (x, y) (flexmm/flexmm2d/fmm.py:160-161)."""
         return self._evaluate(x, y, False)
 
+    def direct_evaluation(self, x, y, check=False):
+        """FP64 direct sum of this object's sources and charges at (x, y)
+        (kernel_apply / kernel_apply_single_check, flexmm/flexmm2d/helpers.py:91-116)."""
+        if not self._expanded:
+            raise RuntimeError("build_expansions has not run")
+        return direct_evaluation(self.kernel, self._x, self._y, self._tau, x, y, check)
+
     def __del__(self):
         try:
             if getattr(self, "_plan", None) is not None and _lib._LIB is not None:
@@ -214,3 +232,36 @@ class KI_FMM:
         except Exception:
             pass
         self._plan = None
+
+
+def direct_evaluation(kernel, sx, sy, tau, tx, ty, check=False):
+    """FP64 direct sum on the GPU: u(t) = sum_s K(s, t) tau_s, skipping
+    coincident pairs when ``check`` (flexmm/flexmm2d/helpers.py:91-116)."""
+    torch = _torch()
+    k = resolve(kernel)
+    sxd, _ = _device_f64(sx)
+    syd, _ = _device_f64(sy)
+    td, _ = _device_f64(tau)
+    txd, kind = _device_f64(tx)
+    tyd, _ = _device_f64(ty)
+    out = torch.empty(txd.numel(), dtype=torch.float64, device="cuda")
+    params = (ctypes.c_double * 4)(*k.params)
+    _lib.call("fmm_direct", k.kernel_id, params, ctypes.c_void_p(sxd.data_ptr()),
+              ctypes.c_void_p(syd.data_ptr()), ctypes.c_void_p(td.data_ptr()), sxd.numel(),
+              ctypes.c_void_p(txd.data_ptr()), ctypes.c_void_p(tyd.data_ptr()), txd.numel(),
+              1 if check else 0, ctypes.c_void_p(out.data_ptr()), _stream())
+    return _as_kind(out, kind, np.shape(tx))
+
+
+def enable_timing(on=True):
+    """Per-kernel CUDA-event timing inside the library (off by default)."""
+    _lib.load()
+    _lib.call("fmm_timing_enable", 1 if on else 0)
+
+
+def read_timing():
+    """{phase: (milliseconds, timed launches)} since the last read."""
+    ms = (ctypes.c_double * _lib.N_PHASES)()
+    n = (ctypes.c_int64 * _lib.N_PHASES)()
+    _lib.call("fmm_timing_read", ms, n)
+    return {name: (ms[i], n[i]) for i, name in enumerate(_lib.PHASES)}

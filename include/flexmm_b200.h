@@ -98,6 +98,24 @@ int fmm_plan_destroy(fmm_plan *plan);
 int fmm_tree_export(fmm_plan *plan, double *xmin, double *ymin, int *bot, int *top, int *parent,
                     int *child, uint8_t *flags, int *coll, int *il, int *ordv);
 
+/* FP64 direct sum over all ns sources at nt targets (device pointers);
+ * check != 0 skips coincident pairs.  Replaces kernel_apply /
+ * kernel_apply_single_check (flexmm/flexmm2d/helpers.py:91-116); used as the
+ * accuracy reference. */
+int fmm_direct(int kernel_id, const double *kernel_params, const double *sx, const double *sy,
+               const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
+               int check, double *out, void *stream);
+
+/* Per-kernel CUDA-event timing, the per-phase timers of the reference's
+ * verbose mode (flexmm/flexmm2d/fmm.py:24-30, 55-58, 106-107, 148-149).
+ * fmm_timing_read returns, per phase, the summed milliseconds and the number
+ * of timed launches since the last read, then clears them.  Phases:
+ * 0 tree build (span), 1 target sort, 2 upward, 3 M2L, 4 downward,
+ * 5 evaluation (L2T + P2P), 6 direct sum. */
+#define FMM_N_PHASES 8
+int fmm_timing_enable(int on);
+int fmm_timing_read(double *ms /* [FMM_N_PHASES] */, int64_t *launches /* [FMM_N_PHASES] */);
+
 const char *fmm_last_error(void);
 
 #ifdef __cplusplus
