@@ -7,12 +7,19 @@
 //  * check-to-equivalent is applied as VH^T diag(1/S) U^T, the factored SVD
 //    solve (flexmm/kifmm2d/scalar/helpers.py:240-248), never an explicit
 //    inverse; it agrees with the reference's LU solve to ~1e-15;
-//  * M2L is target-centric: a tile of target boxes gathers the source
-//    multipoles of one offset and multiplies by that offset's dense or
-//    SVD-factored operator, accumulating all 40 offsets in registers (the
-//    reference multiplies every multipole by every offset, then gathers);
+//  * M2L is target-centric: a tile of 64 target boxes of one parity class
+//    (position inside the parent: 27 of the 40 offsets can occur) gathers the
+//    source multipoles of one offset and multiplies them by that offset's
+//    dense or SVD-factored operator, accumulating all offsets in registers
+//    (the reference multiplies every multipole by every offset, then gathers);
 //  * L2L is parent-centric: one GEMM per tile of 8 parents produces the
-//    partial locals of their 32 children.
+//    partial locals of their 32 children;
+//  * fake leaves (source-only boxes) get no local expansions: they are never
+//    evaluated and never pass anything down;
+//  * the GEMMs run on the FP64 tensor cores (mma.sync m8n8k4 f64); the
+//    activations sit in shared memory with padded rows (stride 4 mod 16
+//    doubles: conflict-free fragment loads), the operators are read through
+//    the read-only cache.
 #include <cub/cub.cuh>
 
 #include "fmm.cuh"
@@ -21,70 +28,99 @@
 namespace fmmb {
 namespace {
 
-constexpr int TN = 32;    // nodes per tile
-constexpr int NT = 256;   // threads per tile CTA
-constexpr int TCH = 128;  // targets per evaluation work item
+constexpr int TN = 32;      // nodes per upward / downward tile
+constexpr int TM = 64;      // targets per M2L tile
+constexpr int NT = 256;     // threads per tile CTA
+constexpr int TCH = 128;    // targets per evaluation work item (= threads)
+constexpr int SMAX = 1024;  // sources staged per evaluation pass
 
-// acc[r][c] += sum_k A[(row0 + r) * lda + k] * B[k * ldb + col0 + c], r < R, c < 4
-template <int R>
-__device__ __forceinline__ void gemm_acc(const double *__restrict__ A, int lda,
-                                         const double *__restrict__ B, int ldb, int K, int row0,
-                                         int col0, double (&acc)[R][4]) {
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    const double2 b01 = *reinterpret_cast<const double2 *>(B + (size_t)k * ldb + col0);
-    const double2 b23 = *reinterpret_cast<const double2 *>(B + (size_t)k * ldb + col0 + 2);
+// the 27 offsets a target can see, by its parity class 2*(ix&1) + (iy&1)
+// (offset ids walk ox = -3..3 outer, oy = -3..3 inner, skipping (-1..1)^2)
+__constant__ int8_t c_class_off[4][27] = {
+    {8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32, 34, 35, 36, 37, 38, 39},
+    {7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31, 33, 34, 35, 36, 37, 38},
+    {1, 2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32},
+    {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31}};
+
+__host__ __device__ inline int pad_ld(int n) { return n + 4; }  // n multiple of 8 -> 4 or 12 mod 16
+
+// D[8x8] += A[8x4] . B[4x8] on the FP64 tensor cores
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// Warp tile: C[r0 + 8*rb + g][c0 + 8*cb*cstride + 2q + i] += sum_k A[.][k] * B[k][.]
+// for rb < RB and the column blocks cb < CB that start below ncols
+// (g = lane/4, q = lane%4; fragment layouts of mma.m8n8k4.f64).
+// A: shared memory, row-major, stride lda.  B: global, row-major [K][ldb].
+template <int RB, int CB>
+__device__ __forceinline__ void warp_gemm(const double *A, int lda, const double *__restrict__ B,
+                                          int ldb, int K, int r0, int c0, int cstride, int ncols,
+                                          double (&acc)[RB][CB][2]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const double *Ap = A + (r0 + g) * lda + q;
+  const double *Bp = B + (size_t)q * ldb + c0 + g;
+#pragma unroll 2
+  for (int k = 0; k < K; k += 4) {
+    double a[RB], b[CB];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const double a = A[(row0 + r) * lda + k];
-      acc[r][0] = fma(a, b01.x, acc[r][0]);
-      acc[r][1] = fma(a, b01.y, acc[r][1]);
-      acc[r][2] = fma(a, b23.x, acc[r][2]);
-      acc[r][3] = fma(a, b23.y, acc[r][3]);
-    }
+    for (int rb = 0; rb < RB; ++rb) a[rb] = Ap[8 * rb * lda + k];
+#pragma unroll
+    for (int cb = 0; cb < CB; ++cb)
+      b[cb] = (c0 + 8 * cb * cstride < ncols) ? __ldg(Bp + (size_t)k * ldb + 8 * cb * cstride) : 0.0;
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+      for (int cb = 0; cb < CB; ++cb)
+        if (c0 + 8 * cb * cstride < ncols) dmma(acc[rb][cb], a[rb], b[cb]);
   }
 }
 
-template <int R>
-__device__ __forceinline__ void zero_acc(double (&acc)[R][4]) {
+template <int RB, int CB>
+__device__ __forceinline__ void zero_acc(double (&acc)[RB][CB][2]) {
 #pragma unroll
-  for (int r = 0; r < R; ++r)
+  for (int rb = 0; rb < RB; ++rb)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+    for (int cb = 0; cb < CB; ++cb) acc[rb][cb][0] = acc[rb][cb][1] = 0.0;
 }
 
-// Check-to-equivalent on a tile held in smem P[TN][NP] -> T (scratch) -> out rows.
-// out[t][i] = sum_k VH[k][i] * sinv[k] * sum_j U[j][k] * P[t][j]
-__device__ void c2e_tile(const LevelOpsDev &op, int np, const double *P, double *T, int nloc,
-                         double *out_base, const uint8_t *write_mask) {
-  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-  const int row0 = 2 * ty, col0 = 4 * tx;
-  double acc[2][4];
+// Check-to-equivalent on a 32-row tile: out = ((P . U) * sinv) . VH.
+// P, T: shared [32][pad_ld(np)].  Row t goes to out_row[t] (global, np
+// doubles) when out_row[t] is not null.  Starts and ends with a barrier-free
+// read of P; the caller synchronises before.
+__device__ void c2e_tile(const LevelOpsDev &op, int np, const double *P, double *T,
+                         double *const *out_row) {
+  const int ldp = pad_ld(np);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int r0 = 8 * (warp & 3), c0 = 8 * (warp >> 2);
+  double acc[1][4][2];
   zero_acc(acc);
-  if (col0 < np) gemm_acc<2>(P, np, op.u, np, np, row0, col0, acc);
-  if (col0 < np) {
+  warp_gemm<1, 4>(P, ldp, op.u, np, np, r0, c0, 2, np, acc);
 #pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) T[(row0 + r) * np + col0 + c] = acc[r][c] * op.sinv[col0 + c];
+  for (int cb = 0; cb < 4; ++cb) {
+    const int col = c0 + 16 * cb + 2 * q;
+    if (col < np) {
+      T[(r0 + g) * ldp + col] = acc[0][cb][0] * op.sinv[col];
+      T[(r0 + g) * ldp + col + 1] = acc[0][cb][1] * op.sinv[col + 1];
+    }
   }
   __syncthreads();
   zero_acc(acc);
-  if (col0 < np) gemm_acc<2>(T, np, op.vh, np, np, row0, col0, acc);
-  if (col0 < np) {
+  warp_gemm<1, 4>(T, ldp, op.vh, np, np, r0, c0, 2, np, acc);
+  double *o = out_row[r0 + g];
+  if (o) {
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int t = row0 + r;
-      if (t < nloc && (!write_mask || write_mask[t])) {
-        double *o = out_base + (size_t)t * np + col0;
-        reinterpret_cast<double2 *>(o)[0] = make_double2(acc[r][0], acc[r][1]);
-        reinterpret_cast<double2 *>(o)[1] = make_double2(acc[r][2], acc[r][3]);
-      }
+    for (int cb = 0; cb < 4; ++cb) {
+      const int col = c0 + 16 * cb + 2 * q;
+      if (col < np) *reinterpret_cast<double2 *>(o + col) = make_double2(acc[0][cb][0], acc[0][cb][1]);
     }
   }
 }
 
 // ---------------------------------------------------------------- upward ----
+// One tile = 32 consecutive nodes of level m.
 template <class KF>
 __global__ void __launch_bounds__(NT) k_upward(int m, KernelParams kp, int neq, int np, int g_begin,
                                                int g_end, const uint8_t *__restrict__ flags,
@@ -99,18 +135,21 @@ __global__ void __launch_bounds__(NT) k_upward(int m, KernelParams kp, int neq, 
                                                const LevelOpsDev *__restrict__ ops,
                                                double *__restrict__ mult) {
   extern __shared__ double smem[];
-  double *P = smem;             // [TN][np]   check potentials
-  double *A = P + TN * np;      // [TN][4np]  children multipoles; later C2E scratch
+  const int ldp = pad_ld(np), lda = pad_ld(4 * np);
+  double *P = smem;           // [TN][ldp]  check potentials
+  double *A = P + TN * ldp;   // [TN][lda]  children multipoles; later C2E scratch
+  __shared__ double *orow[TN];
   const KF K(kp);
   const LevelOpsDev &op = ops[m];
   const int g0 = g_begin + blockIdx.x * TN;
   const int nloc = min(TN, g_end - g0);
-  for (int i = threadIdx.x; i < TN * np; i += NT) P[i] = 0.0;
-  for (int i = threadIdx.x; i < TN * 4 * np; i += NT) A[i] = 0.0;
+  for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = 0.0;
+  for (int i = threadIdx.x; i < TN * lda; i += NT) A[i] = 0.0;
+  if (threadIdx.x < TN) orow[threadIdx.x] = threadIdx.x < nloc ? mult + (size_t)(g0 + threadIdx.x) * np : nullptr;
   __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  // S2M (flexmm/flexmm2d/kifmm.py:96-105) for leaves and fake leaves with
-  // points; gather children multipoles for boxes with children (M2M)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // S2M (flexmm/flexmm2d/kifmm.py:96-105) for leaves and fake leaves holding
+  // points; children multipoles for boxes with children (M2M)
   for (int t = warp; t < nloc; t += NT / 32) {
     const int g = g0 + t;
     const uint8_t f = flags[g];
@@ -122,143 +161,182 @@ __global__ void __launch_bounds__(NT) k_upward(int m, KernelParams kp, int neq, 
         const double lxk = op.lx[k], lyk = op.ly[k];
         double acc = 0.0;
         for (int j = b; j < e; ++j) acc = fma(K(sx[j] - cx, sy[j] - cy, lxk, lyk), tau[j], acc);
-        P[t * np + k] = acc;
+        P[t * ldp + k] = acc;
       }
     } else if (f & NF_CHILDREN) {
-      const int c0 = child[g];
-      for (int q = lane; q < 4 * np; q += 32) A[t * 4 * np + q] = mult[(size_t)(c0 + q / np) * np + q % np];
+      const double *src = mult + (size_t)child[g] * np;  // 4 consecutive children rows
+      for (int qd = lane; qd < 4 * np; qd += 32) A[t * lda + qd] = src[qd];
     }
   }
   __syncthreads();
   // M2M: P[t] = M2MC . [children]  (flexmm/flexmm2d/fmm.py:93-96)
   {
-    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-    const int row0 = 2 * ty, col0 = 4 * tx;
-    double acc[2][4];
+    const int g = lane >> 2, q = lane & 3;
+    const int r0 = 8 * (warp & 3), c0 = 8 * (warp >> 2);
+    double acc[1][4][2];
     zero_acc(acc);
-    if (col0 < np) gemm_acc<2>(A, 4 * np, op.m2mct, np, 4 * np, row0, col0, acc);
-    __syncthreads();
-    if (col0 < np) {
+    warp_gemm<1, 4>(A, lda, op.m2mct, np, 4 * np, r0, c0, 2, np, acc);
+    const int t = r0 + g;
+    if (t < nloc && (flags[g0 + t] & NF_CHILDREN)) {
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int t = row0 + r;
-        if (t < nloc && (flags[g0 + t] & NF_CHILDREN))
-#pragma unroll
-          for (int c = 0; c < 4; ++c) P[t * np + col0 + c] = acc[r][c];
+      for (int cb = 0; cb < 4; ++cb) {
+        const int col = c0 + 16 * cb + 2 * q;
+        if (col < np) {
+          P[t * ldp + col] = acc[0][cb][0];
+          P[t * ldp + col + 1] = acc[0][cb][1];
+        }
       }
     }
   }
   __syncthreads();
-  c2e_tile(op, np, P, A, nloc, mult + (size_t)g0 * np, nullptr);
+  c2e_tile(op, np, P, A, orow);
 }
 
 // ------------------------------------------------------------------- M2L ----
-__global__ void __launch_bounds__(NT) k_m2l(const int *__restrict__ tile_start, int L,
-                                            const int *__restrict__ off, int np,
+struct M2LTiles {
+  int n_levels;
+  int tile_start[4 * FMM_MAX_LEVELS_DEV + 1];  // first tile of each (level, parity class)
+  int rg_lo[FMM_MAX_LEVELS_DEV];               // real groups of each level
+  int rg_cnt[FMM_MAX_LEVELS_DEV];
+};
+
+__global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *__restrict__ rg,
                                             const int *__restrict__ il,
                                             const LevelOpsDev *__restrict__ ops,
                                             const double *__restrict__ mult,
                                             double *__restrict__ ple) {
   extern __shared__ double smem[];
-  double *G = smem;           // [TN][np] gathered source multipoles
-  double *W = G + TN * np;    // [TN][np] SVD intermediate
-  int m = 2;
-  while (m + 1 < L && tile_start[m + 1] <= (int)blockIdx.x) ++m;
-  const int g0 = off[m] + TN * (blockIdx.x - tile_start[m]);
-  const int nloc = min(TN, off[m + 1] - g0);
+  const int ldp = pad_ld(np), ldw = pad_ld(32);
+  double *G = smem;            // [TM][ldp] gathered source multipoles
+  double *W = G + TM * ldp;    // [TM][ldw] SVD intermediate (rank <= 32)
+  __shared__ int tgt[TM], srow[TM];
+  // this block's (level, parity class, range of real groups)
+  int slot = 0;
+  while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= (int)blockIdx.x) ++slot;
+  const int m = slot >> 2, cls = slot & 3;
+  const int q0 = TM * (blockIdx.x - tiles.tile_start[slot]);
+  const int nloc = min(TM, tiles.rg_cnt[m] - q0);
+  if (threadIdx.x < TM)
+    tgt[threadIdx.x] = (threadIdx.x < nloc) ? rg[tiles.rg_lo[m] + q0 + threadIdx.x] + cls : -1;
+  __syncthreads();
   const LevelOpsDev &op = ops[m];
-  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-  const int row0 = 2 * ty, col0 = 4 * tx;
-  double acc[2][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  // dense / stage-2 mapping: rows 16*(warp&3) + [0,16), column blocks 8*(warp>>2) + 16*cb
+  const int r0 = 16 * (warp & 3), c0 = 8 * (warp >> 2);
+  double acc[2][4][2];
   zero_acc(acc);
-  for (int o = 0; o < N_OFFSETS; ++o) {
+  for (int oi = 0; oi < 27; ++oi) {
+    const int o = c_class_off[cls][oi];
     const int kind = op.kind[o];
     if (kind == M2L_NULL) continue;
-    const int has = (threadIdx.x < nloc) ? (il[(size_t)(g0 + threadIdx.x) * N_OFFSETS + o] >= 0) : 0;
-    if (!__syncthreads_or(has)) continue;
-    for (int i = threadIdx.x; i < TN * np; i += NT) {
-      const int t = i / np, k = i % np;
-      const int s = (t < nloc) ? il[(size_t)(g0 + t) * N_OFFSETS + o] : -1;
-      G[i] = (s >= 0) ? mult[(size_t)s * np + k] : 0.0;
+    int src = -1;
+    if (threadIdx.x < TM && tgt[threadIdx.x] >= 0) src = il[(size_t)tgt[threadIdx.x] * N_OFFSETS + o];
+    if (threadIdx.x < TM) srow[threadIdx.x] = src;
+    if (!__syncthreads_or(src >= 0)) continue;
+    // gather 64 rows of np doubles (zero rows where there is no source)
+    for (int i = threadIdx.x; i < TM * (np / 2); i += NT) {
+      const int t = i / (np / 2), k2 = 2 * (i % (np / 2));
+      const int s = srow[t];
+      double2 v = make_double2(0.0, 0.0);
+      if (s >= 0) v = *reinterpret_cast<const double2 *>(mult + (size_t)s * np + k2);
+      G[t * ldp + k2] = v.x;
+      G[t * ldp + k2 + 1] = v.y;
     }
     __syncthreads();
     if (kind == M2L_DENSE) {
-      if (col0 < np) gemm_acc<2>(G, np, op.m2l[o], np, np, row0, col0, acc);
+      warp_gemm<2, 4>(G, ldp, op.m2l[o], np, np, r0, c0, 2, np, acc);
     } else {
       const int rp = op.rp[o];
-      double w[2][4];
+      // stage 1: W[64][rp] = G . M1^T ; warp -> rows 8*warp + [0,8), column blocks 0..3
+      double w[1][4][2];
       zero_acc(w);
-      if (col0 < rp) gemm_acc<2>(G, np, op.m2l[o], rp, np, row0, col0, w);
-      if (col0 < rp) {
+      warp_gemm<1, 4>(G, ldp, op.m2l[o], rp, np, 8 * warp, 0, 1, rp, w);
 #pragma unroll
-        for (int r = 0; r < 2; ++r)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) W[(row0 + r) * rp + col0 + c] = w[r][c];
+      for (int cb = 0; cb < 4; ++cb) {
+        const int col = 8 * cb + 2 * q;
+        if (col < rp) {
+          W[(8 * warp + g) * ldw + col] = w[0][cb][0];
+          W[(8 * warp + g) * ldw + col + 1] = w[0][cb][1];
+        }
       }
       __syncthreads();
-      if (col0 < np) gemm_acc<2>(W, rp, op.m2l[o] + (size_t)np * rp, np, rp, row0, col0, acc);
+      // stage 2: acc += W . M2^T
+      warp_gemm<2, 4>(W, ldw, op.m2l[o] + (size_t)np * rp, np, rp, r0, c0, 2, np, acc);
     }
     __syncthreads();
   }
-  if (col0 < np) {
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int t = row0 + r;
-      if (t < nloc) {
-        double *o = ple + (size_t)(g0 + t) * np + col0;
-        reinterpret_cast<double2 *>(o)[0] = make_double2(acc[r][0], acc[r][1]);
-        reinterpret_cast<double2 *>(o)[1] = make_double2(acc[r][2], acc[r][3]);
+  for (int rb = 0; rb < 2; ++rb) {
+    const int t = r0 + 8 * rb + g;
+    if (t < nloc) {
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        const int col = c0 + 16 * cb + 2 * q;
+        if (col < np)
+          *reinterpret_cast<double2 *>(ple + (size_t)tgt[t] * np + col) =
+              make_double2(acc[rb][cb][0], acc[rb][cb][1]);
       }
     }
   }
 }
 
 // -------------------------------------------------------------- downward ----
-__global__ void __launch_bounds__(NT) k_downward(int m, int np, int g_begin, int g_end,
-                                                 const uint8_t *__restrict__ flags,
+// One tile = 8 real sibling groups of level m (32 nodes): L2L from their
+// parents (m >= 3), plus the M2L partial locals, then check-to-equivalent.
+__global__ void __launch_bounds__(NT) k_downward(int m, int np, int rg_lo, int rg_cnt,
+                                                 const int *__restrict__ rg,
                                                  const int *__restrict__ parent,
                                                  const LevelOpsDev *__restrict__ ops,
                                                  const double *__restrict__ ple,
                                                  double *__restrict__ loc) {
   extern __shared__ double smem[];
-  double *P = smem;            // [TN][np] = [8][4np] partial locals
-  double *T = P + TN * np;     // [TN][np] scratch (parent locals, then C2E)
-  __shared__ uint8_t real[TN];
+  const int ldp = pad_ld(np);
+  double *P = smem;           // [32][ldp] partial locals
+  double *T = P + TN * ldp;   // [32][ldp] parent locals, then C2E scratch
+  __shared__ int node[TN];
+  __shared__ double *orow[TN];
   const LevelOpsDev &op = ops[m];
-  const LevelOpsDev &opp = ops[m - 1];
-  const int g0 = g_begin + blockIdx.x * TN;
-  const int nloc = min(TN, g_end - g0);
-  if (threadIdx.x < TN) real[threadIdx.x] = (threadIdx.x < nloc) && !(flags[g0 + threadIdx.x] & NF_FAKE);
-  for (int i = threadIdx.x; i < TN * np; i += NT) {
-    const int t = i / np;
-    P[i] = (t < nloc) ? ple[(size_t)g0 * np + i] : 0.0;
-    T[i] = 0.0;
+  const int q0 = 8 * blockIdx.x;
+  const int ngrp = min(8, rg_cnt - q0);
+  if (threadIdx.x < TN) {
+    const int grp = threadIdx.x >> 2;
+    const int n = (grp < ngrp) ? rg[rg_lo + q0 + grp] + int(threadIdx.x & 3) : -1;
+    node[threadIdx.x] = n;
+    orow[threadIdx.x] = n >= 0 ? loc + (size_t)n * np : nullptr;
   }
   __syncthreads();
+  for (int i = threadIdx.x; i < TN * np; i += NT) {
+    const int t = i / np, k = i % np;
+    P[t * ldp + k] = (node[t] >= 0) ? ple[(size_t)node[t] * np + k] : 0.0;
+    T[t * ldp + k] = 0.0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
   if (m >= 3) {
-    // parent locals of the 8 sibling groups
+    const LevelOpsDev &opp = ops[m - 1];
     for (int i = threadIdx.x; i < 8 * np; i += NT) {
-      const int q = i / np, k = i % np;
-      const int t = 4 * q;
-      T[i] = (t < nloc && real[t]) ? loc[(size_t)parent[g0 + t] * np + k] : 0.0;
+      const int grp = i / np, k = i % np;
+      const int n0 = node[4 * grp];
+      T[grp * ldp + k] = (n0 >= 0) ? loc[(size_t)parent[n0] * np + k] : 0.0;
     }
     __syncthreads();
-    // L2L: [8 parents][4np] += Lp . M2MC  (flexmm/flexmm2d/fmm.py:140-147)
-    const int ty = threadIdx.x / 64, tx = threadIdx.x % 64;
-    const int row0 = 2 * ty, col0 = 4 * tx;
-    double acc[2][4];
+    // L2L: [8 parents][4np] = Lp . M2MC (flexmm/flexmm2d/fmm.py:140-147);
+    // warp -> column blocks warp + 8*cb of the 4np columns
+    double acc[1][4][2];
     zero_acc(acc);
-    if (col0 < 4 * np) gemm_acc<2>(T, np, opp.m2mc, 4 * np, np, row0, col0, acc);
-    __syncthreads();
-    if (col0 < 4 * np) {
+    warp_gemm<1, 4>(T, ldp, opp.m2mc, 4 * np, np, 0, 8 * warp, 8, 4 * np, acc);
 #pragma unroll
-      for (int r = 0; r < 2; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) P[(row0 + r) * 4 * np + col0 + c] += acc[r][c];
+    for (int cb = 0; cb < 4; ++cb) {
+      const int col = 8 * warp + 64 * cb + 2 * q;  // column of the 4np-wide parent row
+      if (col < 4 * np) {
+        const int c = col / np, i = col % np;
+        P[(4 * g + c) * ldp + i] += acc[0][cb][0];
+        P[(4 * g + c) * ldp + i + 1] += acc[0][cb][1];
+      }
     }
     __syncthreads();
   }
-  c2e_tile(op, np, P, T, nloc, loc + (size_t)g0 * np, real);
+  c2e_tile(op, np, P, T, orow);
 }
 
 // ------------------------------------------------------------ evaluation ----
@@ -301,6 +379,10 @@ __global__ void k_leaf_targets(int total, int L, const int *__restrict__ off,
   }
 }
 
+// One work item = (leaf, up to 128 of its targets).  G = 128 / targets
+// (rounded down to a power of two) threads share a target: they split the
+// circle points of L2T and the colleague sources of P2P, then reduce with
+// warp shuffles (and shared memory when G > 32).
 template <class KF>
 __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np, int total_nodes,
                                                   int L, const int *__restrict__ off,
@@ -323,7 +405,9 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
                                                   const int *__restrict__ tperm, int check,
                                                   double *__restrict__ out) {
   __shared__ double Ls[64], lxs[64], lys[64];
-  __shared__ double ssx[TCH], ssy[TCH], stau[TCH];
+  __shared__ double ssx[SMAX], ssy[SMAX], stau[SMAX];
+  __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
+  __shared__ double red[TCH / 32];
   const KF K(kp);
   const int n_items = choff[total_nodes - 1] + nchunk[total_nodes - 1];
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -342,52 +426,69 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
       }
       lev = a;
     }
-    const int ch = item - choff[g];
-    const int t0 = tb[g] + ch * TCH;
+    const int t0 = tb[g] + (item - choff[g]) * TCH;
     const int cnt = min(TCH, te[g] - t0);
-    const bool valid = threadIdx.x < cnt;
-    const int ti = t0 + threadIdx.x;
-    const double x = valid ? txs[ti] : 0.0, y = valid ? tys[ti] : 0.0;
+    int G = 1;
+    while (2 * G * cnt <= TCH) G *= 2;
+    const int t = threadIdx.x / G, sub = threadIdx.x % G;
+    const bool valid = t < cnt;
+    const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
     double u = 0.0;
+    if (threadIdx.x < 9) {
+      const int cg = coll[(size_t)g * 9 + threadIdx.x];
+      rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
+      rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
+    }
+    if (threadIdx.x == 0) rs[0] = 0;
     // L2T (flexmm/flexmm2d/kifmm.py:106-120); locals of levels 0-1 are zero
-    if (lev >= 2) {
+    if (lev >= 2)
       for (int k = threadIdx.x; k < neq; k += TCH) {
         Ls[k] = loc[(size_t)g * np + k];
         lxs[k] = ops[lev].lx[k];
         lys[k] = ops[lev].ly[k];
       }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
+    if (lev >= 2 && valid) {
+      const double dx = x - xmid[g], dy = y - ymid[g];
+      for (int k = sub; k < neq; k += G) u = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u);
+    }
+    __syncthreads();
+    // P2P over the colleagues' sorted source ranges (flexmm/flexmm2d/helpers.py:152-194)
+    const int ns = rs[9];
+    for (int base = 0; base < ns; base += SMAX) {
+      const int nb = min(SMAX, ns - base);
+      for (int i = threadIdx.x; i < nb; i += TCH) {
+        const int idx = base + i;
+        int c = 0;
+        while (idx >= rs[c + 1]) ++c;
+        const int j = rb[c] + (idx - rs[c]);
+        ssx[i] = sx[j];
+        ssy[i] = sy[j];
+        stau[i] = tau[j];
+      }
       __syncthreads();
       if (valid) {
-        const double dx = x - xmid[g], dy = y - ymid[g];
-        for (int k = 0; k < neq; ++k) u = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u);
-      }
-    }
-    // P2P over the colleagues' sorted source ranges (flexmm/flexmm2d/helpers.py:152-194)
-    for (int c = 0; c < 9; ++c) {
-      const int cg = coll[(size_t)g * 9 + c];
-      if (cg < 0) break;
-      const int b = bot[cg], e = top[cg];
-      double part = 0.0;
-      for (int j0 = b; j0 < e; j0 += TCH) {
-        const int nj = min(TCH, e - j0);
-        __syncthreads();
-        if (threadIdx.x < nj) {
-          ssx[threadIdx.x] = sx[j0 + threadIdx.x];
-          ssy[threadIdx.x] = sy[j0 + threadIdx.x];
-          stau[threadIdx.x] = tau[j0 + threadIdx.x];
-        }
-        __syncthreads();
-        if (valid) {
-          for (int j = 0; j < nj; ++j) {
-            const double qx = ssx[j], qy = ssy[j];
-            if (check && x - qx == 0.0 && y - qy == 0.0) continue;
-            part = fma(K(qx, qy, x, y), stau[j], part);
-          }
+        for (int j = sub; j < nb; j += G) {
+          const double qx = ssx[j], qy = ssy[j];
+          if (check && x - qx == 0.0 && y - qy == 0.0) continue;
+          u = fma(K(qx, qy, x, y), stau[j], u);
         }
       }
-      u += part;
+      __syncthreads();
     }
-    if (valid) out[tperm[ti]] = u;
+    // reduce over the G threads of each target
+    for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
+    if (G > 32) {
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
+      __syncthreads();
+      if (sub == 0) {
+        u = 0.0;
+        for (int w = 0; w < G / 32; ++w) u += red[(threadIdx.x >> 5) + w];
+      }
+    }
+    if (valid && sub == 0) out[tperm[t0 + t]] = u;
     __syncthreads();
   }
 }
@@ -440,9 +541,9 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int np = a.np;
-  const size_t sm = sizeof(double) * (size_t)TN * np * 5;
+  const size_t sm = sizeof(double) * (size_t)TN * (pad_ld(np) + pad_ld(4 * np));
   FMMB_CUDA(cudaFuncSetAttribute(k_upward<KF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(double) * TN * 64 * 5)));
+                                 int(sizeof(double) * TN * (pad_ld(64) + pad_ld(256)))));
   for (int m = th.L - 1; m >= 2; --m) {
     const int gb = th.off[m], ge = th.off[m + 1];
     const int tiles = (ge - gb + TN - 1) / TN;
@@ -496,33 +597,39 @@ void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream
 void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s) {
   const TreeHost &th = *a.th;
   if (th.L < 3) return;
-  std::vector<int> ts(th.L + 1, 0);
+  FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
+  M2LTiles tl{};
+  tl.n_levels = th.L;
   int tiles = 0;
-  for (int m = 2; m < th.L; ++m) {
-    ts[m] = tiles;
-    tiles += (th.off[m + 1] - th.off[m] + TN - 1) / TN;
+  for (int m = 0; m < th.L; ++m) {
+    tl.rg_lo[m] = th.rg_lo[m];
+    tl.rg_cnt[m] = th.rg_hi[m] - th.rg_lo[m];
+    for (int c = 0; c < 4; ++c) {
+      tl.tile_start[4 * m + c] = tiles;
+      if (m >= 2) tiles += (tl.rg_cnt[m] + TM - 1) / TM;
+    }
   }
-  ts[th.L] = tiles;
-  DevBuf<int> tsd;
-  tsd.alloc(th.L + 1, s);
-  FMMB_CUDA(cudaMemcpyAsync(tsd.get(), ts.data(), ts.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  const size_t sm = sizeof(double) * (size_t)TN * a.np * 2;
+  tl.tile_start[4 * th.L] = tiles;
+  if (tiles == 0) return;
+  const size_t sm = sizeof(double) * (size_t)TM * (pad_ld(a.np) + pad_ld(32));
+  FMMB_CUDA(cudaFuncSetAttribute(k_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(double) * TM * (pad_ld(64) + pad_ld(32)))));
   PhaseTimer timer(PH_M2L, s);
-  k_m2l<<<tiles, NT, sm, s>>>(tsd.get(), th.L, a.td->dev_off.get(), a.np, a.td->il.get(), a.ops_dev,
-                              mult, ple);
+  k_m2l<<<tiles, NT, sm, s>>>(tl, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev, mult, ple);
   FMMB_CUDA(cudaGetLastError());
 }
 
 void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
-  const size_t sm = sizeof(double) * (size_t)TN * a.np * 2;
+  const size_t sm = sizeof(double) * (size_t)TN * pad_ld(a.np) * 2;
   for (int m = 2; m < th.L; ++m) {
-    const int gb = th.off[m], ge = th.off[m + 1];
-    const int tiles = (ge - gb + TN - 1) / TN;
+    const int lo = th.rg_lo[m], cnt = th.rg_hi[m] - th.rg_lo[m];
+    if (cnt <= 0) continue;
+    const int tiles = (cnt + 7) / 8;
     PhaseTimer timer(PH_DOWNWARD, s);
-    k_downward<<<tiles, NT, sm, s>>>(m, a.np, gb, ge, td.flags.get(), td.parent.get(), a.ops_dev,
-                                     ple, loc);
+    k_downward<<<tiles, NT, sm, s>>>(m, a.np, lo, cnt, td.rg.get(), td.parent.get(), a.ops_dev, ple,
+                                     loc);
     FMMB_CUDA(cudaGetLastError());
   }
 }

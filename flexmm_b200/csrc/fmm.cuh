@@ -9,6 +9,7 @@
 namespace fmmb {
 
 constexpr int M2L_NULL = 0, M2L_DENSE = 1, M2L_SVD = 2;
+constexpr int FMM_MAX_LEVELS_DEV = 30;  // levels 0..29 (keys hold 29 digits)
 
 // Device view of one width's operators (all arrays zero padded to NP).
 struct LevelOpsDev {

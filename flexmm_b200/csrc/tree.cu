@@ -265,6 +265,32 @@ __global__ void k_concat_parents(const uint64_t *__restrict__ s0, int64_t n0,
   }
 }
 
+// real sibling groups: the children of split boxes (not of X-list leaves)
+__global__ void k_real_flags(const uint8_t *__restrict__ pisx, int64_t n, int *__restrict__ real) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    real[i] = pisx[i] ? 0 : 1;
+}
+
+__global__ void k_real_bounds(const int *__restrict__ pos, const int *__restrict__ real, int64_t n,
+                              const int *__restrict__ pb, int L, int *__restrict__ rgb) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l > L) return;
+  const int total = n ? pos[n - 1] + real[n - 1] : 0;
+  rgb[l] = (pb[l] < n) ? pos[pb[l]] : total;
+}
+
+__global__ void k_real_groups(const uint64_t *__restrict__ pkeys, const int *__restrict__ real,
+                              const int *__restrict__ pos, int64_t n, const int *__restrict__ pb,
+                              const int *__restrict__ off, int *__restrict__ rg) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    if (!real[e]) continue;
+    const int l = code_level(pkeys[e]);
+    rg[pos[e]] = off[l + 1] + 4 * int(e - pb[l]);
+  }
+}
+
 __device__ __forceinline__ int level_of(const int *__restrict__ off, int L, int g) {
   int lo = 0, hi = L;  // find largest l with off[l] <= g
   while (hi - lo > 1) {
@@ -477,7 +503,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
 
   DevBuf<uint64_t> pk, pks;  // parent boxes (unsorted, sorted)
   DevBuf<uint8_t> px, pxs;
-  DevBuf<int> pb;
+  DevBuf<int> pb, preal, ppos;
   std::vector<int> hpb(L + 1, 0);
   int64_t np = 0;
   if (n0 > 0) {
@@ -541,16 +567,31 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     pks.alloc(np, s);
     pxs.alloc(np, s);
     radix_sort_pairs(pk.get(), pks.get(), px.get(), pxs.get(), np, 64, s);
-    pb.alloc(L + 1, s);
+    // pb[0..L] and the real-group bounds rgb[0..L] share one buffer: one copy back
+    pb.alloc(2 * (L + 1), s);
     k_level_bounds<<<1, 64, 0, s>>>(pks.get(), np, L, pb.get());
     FMMB_CUDA(cudaGetLastError());
-    FMMB_CUDA(cudaMemcpyAsync(hpb.data(), pb.get(), (L + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    preal.alloc(np, s);
+    ppos.alloc(np, s);
+    k_real_flags<<<grid_for(np, TPB), TPB, 0, s>>>(pxs.get(), np, preal.get());
+    {
+      size_t bytes = 0;
+      FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, preal.get(), ppos.get(), np, s));
+      DevBuf<uint8_t> tmp;
+      tmp.alloc(bytes, s);
+      FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, preal.get(), ppos.get(), np, s));
+    }
+    k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1);
+    FMMB_CUDA(cudaGetLastError());
+    hpb.resize(2 * (L + 1));
+    FMMB_CUDA(cudaMemcpyAsync(hpb.data(), pb.get(), 2 * (L + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
   } else {
-    pb.alloc(L + 1, s);
+    pb.alloc(2 * (L + 1), s);
     pb.zero(s);
     pks.alloc(1, s);
     pxs.alloc(1, s);
+    hpb.assign(2 * (L + 1), 0);
   }
 
   th.off.assign(L + 1, 0);
@@ -567,6 +608,20 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   td.dev_off.alloc(L + 1, s);
   FMMB_CUDA(cudaMemcpyAsync(td.dev_off.get(), th.off.data(), (L + 1) * sizeof(int),
                             cudaMemcpyHostToDevice, s));
+  // real groups of level m (children of split boxes of level m-1): rg[rg_lo[m], rg_hi[m])
+  th.rg_lo.assign(L + 1, 0);
+  th.rg_hi.assign(L + 1, 0);
+  for (int m = 1; m < L; ++m) {
+    th.rg_lo[m] = hpb[L + 1 + m - 1];
+    th.rg_hi[m] = hpb[L + 1 + m];
+  }
+  const int n_real_groups = hpb[L + 1 + L];
+  td.rg.alloc(n_real_groups > 0 ? n_real_groups : 1, s);
+  if (np > 0 && n_real_groups > 0) {
+    k_real_groups<<<grid_for(np, TPB), TPB, 0, s>>>(pks.get(), preal.get(), ppos.get(), np, pb.get(),
+                                                     td.dev_off.get(), td.rg.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
   td.code.alloc(total, s);
   td.flags.alloc(total, s);
   td.xmin.alloc(total, s);

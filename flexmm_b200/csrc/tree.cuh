@@ -44,6 +44,7 @@ struct TreeDev {
   DevBuf<int> coll;  // [n_total x 9], -1 padded
   DevBuf<int> il;    // [n_total x 40] source node per offset, -1 if none
   DevBuf<int> dev_off;  // level offsets [L+1]
+  DevBuf<int> rg;       // first node of every real sibling group, level-major
 };
 
 struct TreeHost {
@@ -53,6 +54,7 @@ struct TreeHost {
   double x0 = 0, y0 = 0, w0 = 0;
   std::vector<int> off;       // L+1
   std::vector<double> width;  // per level
+  std::vector<int> rg_lo, rg_hi;  // per level: range of its real groups in rg
   int n_total() const { return off.empty() ? 0 : off.back(); }
 };
 
