@@ -54,6 +54,8 @@ SIGNATURES = [
                                   ctypes.c_int64, ctypes.c_int, _vp, _vp]),
     ("fmm_timing_enable", ctypes.c_int, [ctypes.c_int]),
     ("fmm_timing_read", ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int64)]),
+    ("fmm_evaluate_noalloc", ctypes.c_int,
+     [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),
     ("fmm_last_error", ctypes.c_char_p, []),
 ]
 

@@ -1,6 +1,8 @@
 // C-ABI entry points (include/flexmm_b200.h): operator sets, plans, passes.
 #include <string.h>
 
+#include <mutex>
+
 #include <memory>
 #include <string>
 #include <vector>
@@ -367,3 +369,99 @@ int fmm_timing_read(double *ms, int64_t *launches) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free evaluation.
+//
+// fmm_evaluate_noalloc does the work of fmm_evaluate without allocating
+// device memory: its scratch (target keys and permutation, sorted target
+// coordinates, per-node target ranges, sort and scan workspace) lives in the
+// file-scope array below.  The array is part of the library image, so every
+// GPU that loads the library holds it (NOALLOC_SCRATCH_BYTES) until the
+// process exits.  Every call shares it and it keeps the last call's contents;
+// nothing in it needs to start at zero (every scratch word is written before
+// it is read).  Calls that overlap on the GPU (two streams, two threads) race
+// on it and must be serialised by the caller.
+namespace {
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(24) << 20;  // 24 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// device address of the array, looked up once per device (with it current) by
+// the first call on that device; that first call should come before any
+// stream capture
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+void *noalloc_scratch_for_current_device() {
+  int dev = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  FMMB_CHECK(dev >= 0 && dev < NOALLOC_MAX_DEVICES, ERR_UNSUPPORTED, "device ordinal too large");
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    FMMB_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = ptr;
+  }
+  return g_noalloc_ptr[dev];
+}
+
+size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+}  // namespace
+
+extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double *ty, int64_t m,
+                                    int check, double *out, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+    FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
+    FMMB_CHECK(m <= FMM_NOALLOC_MAX_TARGETS, ERR_CAPACITY,
+               "fmm_evaluate_noalloc: more than FMM_NOALLOC_MAX_TARGETS targets");
+    const int total = p->th.n_total();
+    FMMB_CHECK(total <= FMM_NOALLOC_MAX_NODES, ERR_CAPACITY,
+               "fmm_evaluate_noalloc: tree has more than FMM_NOALLOC_MAX_NODES nodes");
+    if (m == 0) return;
+    FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char *base = static_cast<unsigned char *>(noalloc_scratch_for_current_device());
+    // carve the scratch
+    const size_t sort_bytes = round256(sort_points_scratch_bytes(m));
+    const size_t scan_bytes = round256(evaluate_scratch_bytes(total));
+    size_t at = 0;
+    auto carve = [&](size_t bytes) {
+      unsigned char *q = base + at;
+      at += round256(bytes);
+      return q;
+    };
+    uint64_t *k0 = (uint64_t *)carve(m * sizeof(uint64_t));
+    uint64_t *k1 = (uint64_t *)carve(m * sizeof(uint64_t));
+    int *i0 = (int *)carve(m * sizeof(int));
+    int *i1 = (int *)carve(m * sizeof(int));
+    double *txs = (double *)carve(m * sizeof(double));
+    double *tys = (double *)carve(m * sizeof(double));
+    int *tb = (int *)carve(total * sizeof(int));
+    int *te = (int *)carve(total * sizeof(int));
+    int *nch = (int *)carve(total * sizeof(int));
+    int *choff = (int *)carve(total * sizeof(int));
+    void *sort_tmp = carve(sort_bytes);
+    void *scan_tmp = carve(scan_bytes);
+    FMMB_CHECK(at <= NOALLOC_SCRATCH_BYTES, ERR_CAPACITY,
+               "fmm_evaluate_noalloc: scratch needs exceed the static array");
+    // the same passes as fmm_evaluate, on the static scratch
+    PassArgs a;
+    a.kernel_id = p->ops->kernel_id;
+    a.kp = p->ops->kp;
+    a.neq = p->ops->neq;
+    a.np = p->ops->np;
+    a.td = &p->td;
+    a.th = &p->th;
+    a.ops_dev = p->ops_dev.get();
+    const uint64_t *tkeys = nullptr;
+    const int *tperm = nullptr;
+    sort_points_scratch(tx, ty, m, p->th, k0, k1, i0, i1, sort_tmp, sort_bytes, &tkeys, &tperm, s);
+    gather_sorted(tx, tperm, m, txs, s);
+    gather_sorted(ty, tperm, m, tys, s);
+    run_evaluate_scratch(a, p->tau_s.get(), p->loc.get(), txs, tys, tkeys, tperm, m, check, out, tb,
+                         te, nch, choff, scan_tmp, scan_bytes, s);
+  });
+}

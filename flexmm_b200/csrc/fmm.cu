@@ -661,6 +661,38 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
   FMMB_CUDA(cudaGetLastError());
 }
 
+size_t evaluate_scratch_bytes(int total_nodes) {
+  size_t bytes = 0;
+  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int *)nullptr, (int *)nullptr,
+                                          total_nodes));
+  return bytes;
+}
+
+void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *loc,
+                          const double *txs, const double *tys, const uint64_t *tkeys,
+                          const int *tperm, int64_t m, int check, double *out, int *tb, int *te,
+                          int *nch, int *choff, void *temp, size_t temp_bytes, cudaStream_t s) {
+  if (m == 0) return;
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const int total = th.n_total();
+  k_leaf_targets<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), td.code.get(),
+                                                      td.flags.get(), tkeys, m, tb, te, nch);
+  FMMB_CUDA(cudaGetLastError());
+  size_t bytes = temp_bytes;
+  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, nch, choff, total, s));
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE:
+      k_evaluate<LaplaceF64><<<148 * 8, TCH, 0, s>>>(
+          a.kp, a.neq, a.np, total, th.L, td.dev_off.get(), choff, nch, tb, te, td.coll.get(),
+          td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s,
+          a.ops_dev, loc, txs, tys, tperm, check, out);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+  FMMB_CUDA(cudaGetLastError());
+}
+
 void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaStream_t s) {
   if (n == 0) return;
   k_gather_sorted<<<grid_for(n, 256), 256, 0, s>>>(v, perm, n, o);

@@ -46,4 +46,12 @@ void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc
                   const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
                   int64_t m, int check, double *out, cudaStream_t s);
 
+// Evaluation with caller-provided scratch: tb, te, nch, choff hold one int
+// per tree node, temp holds evaluate_scratch_bytes(nodes) bytes.
+size_t evaluate_scratch_bytes(int total_nodes);
+void run_evaluate_scratch(const PassArgs &a, const double *tau_sorted, const double *loc,
+                          const double *txs, const double *tys, const uint64_t *tkeys,
+                          const int *tperm, int64_t m, int check, double *out, int *tb, int *te,
+                          int *nch, int *choff, void *temp, size_t temp_bytes, cudaStream_t s);
+
 }  // namespace fmmb

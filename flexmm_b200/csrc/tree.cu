@@ -461,6 +461,31 @@ void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th
   radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * MAXD, s);
 }
 
+size_t sort_points_scratch_bytes(int64_t n) {
+  size_t bytes = 0;
+  cub::DoubleBuffer<uint64_t> kb(nullptr, nullptr);
+  cub::DoubleBuffer<int> vb(nullptr, nullptr);
+  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, n, 0, 2 * MAXD));
+  return bytes;
+}
+
+void sort_points_scratch(const double *x, const double *y, int64_t n, const TreeHost &th,
+                         uint64_t *k0, uint64_t *k1, int *i0, int *i1, void *temp,
+                         size_t temp_bytes, const uint64_t **keys, const int **perm,
+                         cudaStream_t s) {
+  *keys = k0;
+  *perm = i0;
+  if (n == 0) return;
+  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, k0, i0);
+  FMMB_CUDA(cudaGetLastError());
+  cub::DoubleBuffer<uint64_t> kb(k0, k1);
+  cub::DoubleBuffer<int> vb(i0, i1);
+  size_t bytes = temp_bytes;
+  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(temp, bytes, kb, vb, n, 0, 2 * MAXD, s));
+  *keys = kb.Current();
+  *perm = vb.Current();
+}
+
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
                 const double bbox[4], cudaStream_t s) {
   FMMB_CHECK(n > 0, ERR_INVALID_ARGUMENT, "tree needs at least one point");

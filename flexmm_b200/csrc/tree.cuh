@@ -67,4 +67,13 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
                  DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t stream);
 
+// The same keys and sort into caller-provided memory: k0/k1 and i0/i1 are
+// ping-pong buffers of n entries, temp holds sort_points_scratch_bytes(n)
+// bytes.  *keys / *perm point at the buffers holding the sorted result.
+size_t sort_points_scratch_bytes(int64_t n);
+void sort_points_scratch(const double *x, const double *y, int64_t n, const TreeHost &th,
+                         uint64_t *k0, uint64_t *k1, int *i0, int *i1, void *temp,
+                         size_t temp_bytes, const uint64_t **keys, const int **perm,
+                         cudaStream_t stream);
+
 }  // namespace fmmb

@@ -116,6 +116,23 @@ int fmm_direct(int kernel_id, const double *kernel_params, const double *sx, con
 int fmm_timing_enable(int on);
 int fmm_timing_read(double *ms /* [FMM_N_PHASES] */, int64_t *launches /* [FMM_N_PHASES] */);
 
+/* Allocation-free fmm_evaluate, for callers that cannot allocate device
+ * memory at evaluation time: e.g. an application that has reserved the whole
+ * GPU for its own pool, or a loop that must not touch the allocator.  It has
+ * no counterpart in the reference.  It computes exactly what fmm_evaluate
+ * computes, with the plan built and expanded beforehand; its scratch is a
+ * 24 MiB array inside the library (held on every GPU that loads it until
+ * exit), shared by all calls and keeping the last call's contents.  Calls
+ * that overlap on the GPU race on it: serialise them.  The first call on a
+ * device looks up the array's device address once (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Limits: m <=
+ * FMM_NOALLOC_MAX_TARGETS targets and a tree of at most FMM_NOALLOC_MAX_NODES
+ * nodes; larger requests fail with FMM_ERR_CAPACITY. */
+#define FMM_NOALLOC_MAX_TARGETS 262144
+#define FMM_NOALLOC_MAX_NODES 262144
+int fmm_evaluate_noalloc(fmm_plan *plan, const double *tx, const double *ty, int64_t m, int check,
+                         double *out, void *stream);
+
 const char *fmm_last_error(void);
 
 #ifdef __cplusplus
