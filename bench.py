@@ -36,7 +36,7 @@ sys.path.insert(0, REPO)
 
 METRIC = "Mpts/s, 1M Laplace KIFMM on 1 B200, mixed vs FP64 at rel err 1e-6; ref CPU"
 NCUT = 64
-NEQ = {"fp64": 60}
+NEQ = {"fp64": 60, "mixed": 24}
 C_LAPLACE = 20          # flops per Laplace kernel evaluation (9 arithmetic + log as 11)
 
 
@@ -46,7 +46,9 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=sorted(NEQ), default="fp64")
+    p.add_argument("--precision", choices=sorted(NEQ), default="mixed",
+                   help="headline form (the other form is measured alongside unless --only)")
+    p.add_argument("--only", action="store_true", help="measure only --precision")
     p.add_argument("--n", type=int, default=1_000_000, help="sources (default: the 1M config)")
     p.add_argument("--grid", type=int, default=1000, help="grid targets per side")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -159,11 +161,13 @@ def measured_peaks():
         return {}
 
 
-def fp64_peak_tflops(torch):
-    """FP64 throughput of this GPU, measured with a cuBLAS DGEMM (8192^3)."""
+def gemm_peak_tflops(torch, dtype, tf32=False):
+    """Throughput of this GPU for a cuBLAS GEMM (8192^3): float64 (FP64
+    pipe), float32 without TF32 (FP32 FMA pipe) or float32 with TF32."""
+    torch.backends.cuda.matmul.allow_tf32 = tf32
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
     for _ in range(2):
         torch.matmul(a, b)
     torch.cuda.synchronize()
@@ -176,6 +180,7 @@ def fp64_peak_tflops(torch):
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
     del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
@@ -183,9 +188,8 @@ def fp64_peak_tflops(torch):
 def work_counts(F, tx, ty, nequiv):
     """Algorithmic work of one step from the tree (kernel evaluations, GEMM flops)."""
     t = F.tree
-    ops_rank = {}
     counts = dict(p2p_pairs_src=0, p2p_pairs_tgt=0, m2l_flops=0, s2m_ke=0, l2t_ke=0,
-                  m2m_flops=0, l2l_flops=0, c2e_flops=0)
+                  m2m_flops=0, l2l_flops=0, c2e_flops=0, nequiv=nequiv)
 
     def locate(px, py):
         inds = np.zeros(px.size, np.int64)
@@ -243,35 +247,34 @@ def work_counts(F, tx, ty, nequiv):
 
 
 # ---------------------------------------------------------------- our arm --
-def run_ours(args, world, rank, local):
+def measure(args, world, local, d, precision, flush, counts_cache):
+    """Time one precision form: device-resident steps, e2e steps, accuracy, roofline."""
     import torch
-    from flexmm_b200 import KI_FMM, KI_Helper, direct_evaluation, enable_timing, read_timing, workloads
+    from flexmm_b200 import KI_FMM, KI_Helper, direct_evaluation, enable_timing, read_timing
 
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    neq = NEQ[args.precision]
-    d = workloads.clustered(n=args.n, n_grid=args.grid)
+    neq = NEQ[precision]
     n_src, n_tgt = d["x"].size, d["tx"].size
     pts = n_src + n_tgt
     xd, yd, taud, txd, tyd = (torch.from_numpy(d[k]).to(dev) for k in ("x", "y", "tau", "tx", "ty"))
     helper = KI_Helper()
 
     def step(x, y, tau, tx, ty):
-        F = KI_FMM(x, y, "Laplace_Eval", NCUT, neq, bbox=d["bbox"], helper=helper)
+        F = KI_FMM(x, y, "Laplace_Eval", NCUT, neq, bbox=d["bbox"], helper=helper,
+                   precision=precision)
         F.build_expansions(tau)
         us = F.source_evaluation(x, y)
         ut = F.target_evaluation(tx, ty)
         return F, us, ut
 
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    for _ in range(max(args.warmup, 0)):
+    for _ in range(max(args.warmup, 1)):
         F, us, ut = step(xd, yd, taud, txd, tyd)
     torch.cuda.synchronize()
     if args.ncu:
         for _ in range(args.steps):
             step(xd, yd, taud, txd, tyd)
         torch.cuda.synchronize()
-        return
+        return None
 
     # accuracy of this step's results: FP64 direct sums on 2000-point samples,
     # and agreement with the reference's own outputs (committed fixture)
@@ -295,13 +298,10 @@ def run_ours(args, world, rank, local):
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         step(xd, yd, taud, txd, tyd)
         torch.cuda.synchronize()
-    launches_per_step = 0
-    for ev in prof.events():
-        if getattr(ev, "device_type", None) is not None and str(ev.device_type).endswith("CUDA"):
-            name = ev.name.lower()
-            if "memcpy" in name or "memset" in name:
-                continue
-            launches_per_step += 1
+    launches_per_step = sum(
+        1 for ev in prof.events()
+        if str(getattr(ev, "device_type", "")).endswith("CUDA")
+        and "memcpy" not in ev.name.lower() and "memset" not in ev.name.lower())
 
     # timed region: K steps, L2 flushed between steps, CUDA events on the stream
     enable_timing(True)
@@ -322,9 +322,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     phases = read_timing()
     enable_timing(False)
-    ms_total = sum(a.elapsed_time(b) for a, b in times)
-    ms_step = dist_max(ms_total / max(args.steps, 1), world)
-    value = world * pts / (ms_step * 1e-3) / 1e6
+    ms_step = dist_max(sum(a.elapsed_time(b) for a, b in times) / max(args.steps, 1), world)
 
     # end to end through the public API from pinned host memory
     pin = {k: torch.from_numpy(d[k]).pin_memory() for k in ("x", "y", "tau", "tx", "ty")}
@@ -342,54 +340,129 @@ def run_ours(args, world, rank, local):
         e2e_ms.append(e0.elapsed_time(e1))
     clk.__exit__(None, None, None)
     e2e_step = dist_max(statistics.mean(e2e_ms), world)
-    h2d = 8 * (2 * n_src + n_src + 2 * n_src + 2 * n_tgt)
-    d2h = 8 * (n_src + n_tgt)
 
-    # roofline of the dominant kernel
-    counts = work_counts(F, d["tx"], d["ty"], neq)
+    if "counts" not in counts_cache:
+        counts_cache["counts"] = work_counts(F, d["tx"], d["ty"], neq)
+    c = dict(counts_cache["counts"])
+    scale = neq / c["nequiv"]
+    c["l2t_ke"] = int(c["l2t_ke"] * scale)
+    c["s2m_ke"] = int(c["s2m_ke"] * scale)
+    return dict(F=F, ms_step=ms_step, e2e_step=e2e_step, phases=phases, accuracy=accuracy,
+                launches=launches_per_step * args.steps, clocks=clk.summary(), neq=neq,
+                counts=work_counts_gemm(F, neq, c))
+
+
+def work_counts_gemm(F, neq, c):
+    """GEMM flops of one step at this Nequiv (the tree is the same for every Nequiv)."""
+    t = F.tree
+    n = neq
+    out = dict(c, m2l_flops=0, m2m_flops=0, l2l_flops=0, c2e_flops=0)
+    grid49 = np.array([(a + 3) * 7 + (b + 3) for a in range(-3, 4) for b in range(-3, 4)
+                       if not (abs(a) <= 1 and abs(b) <= 1)])
+    pos = {g: o for o, g in enumerate(grid49)}
+    for ind, lv in enumerate(t.Levels):
+        if ind < 2:
+            continue
+        ranks = F.helper.get_precomputation(lv.width).m2l_rank
+        tr = t.interaction_triples(ind)
+        if tr.size:
+            per_off = np.bincount([pos[g] for g in tr[:, 1]], minlength=40)
+            dense = F.precision == "mixed"   # the mixed form applies every M2L densely
+            fl = np.where((ranks < 0) | dense, 2 * n * n, 4 * n * np.maximum(ranks, 0))
+            fl = np.where(ranks == 0, 0, fl)
+            out["m2l_flops"] += int((per_off * fl).sum())
+        out["m2m_flops"] += 8 * n * n * int((lv.children_ind >= 0).sum())
+        real = ~lv.fake_leaf
+        out["c2e_flops"] += 8 * n * n * int(real.sum())
+        if ind >= 3:
+            out["l2l_flops"] += 2 * n * n * int(real.sum())
+    return out
+
+
+def roofline_of(res, precision, peaks, steps):
+    c = res["counts"]
+    ke = {"evaluate": c["p2p_pairs_src"] + c["p2p_pairs_tgt"] + c["l2t_ke"], "upward": c["s2m_ke"]}
     kernel_flops = {
-        "evaluate": C_LAPLACE * (counts["p2p_pairs_src"] + counts["p2p_pairs_tgt"] + counts["l2t_ke"]),
-        "m2l": counts["m2l_flops"],
-        "upward": C_LAPLACE * counts["s2m_ke"] + counts["m2m_flops"] + counts["c2e_flops"] // 2,
-        "downward": counts["l2l_flops"] + counts["c2e_flops"] // 2,
+        "evaluate": C_LAPLACE * ke["evaluate"],
+        "m2l": c["m2l_flops"],
+        "upward": C_LAPLACE * ke["upward"] + c["m2m_flops"] + c["c2e_flops"] // 2,
+        "downward": c["l2l_flops"] + c["c2e_flops"] // 2,
     }
-    dom = max(kernel_flops, key=lambda k: phases[k][0])
-    ms_k, n_launch = phases[dom]
-    flops_per_launch = kernel_flops[dom] * args.steps / max(n_launch, 1)
+    ph = res["phases"]
+    dom = max(kernel_flops, key=lambda k: ph[k][0])
+    ms_k, n_launch = ph[dom]
+    flops_per_launch = kernel_flops[dom] * steps / max(n_launch, 1)
     achieved = flops_per_launch / (ms_k / max(n_launch, 1) * 1e-3) / 1e12
-    peak = fp64_peak_tflops(torch)
+    if precision == "fp64":
+        bound, peak, src = "fp64", peaks["fp64"], "cuBLAS DGEMM 8192^3 on this GPU (FP64 pipe)"
+    elif dom in ("m2l", "downward"):
+        bound, peak, src = "tensor", peaks["tf32"], "cuBLAS TF32 GEMM 8192^3 on this GPU"
+    else:
+        bound, peak, src = "fp32", peaks["fp32"], "cuBLAS SGEMM 8192^3, TF32 off, on this GPU (FP32 pipe)"
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"{args.precision}:{dom}")
-    roofline = {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
-                "peak_source": "measured on this GPU: cuBLAS DGEMM 8192^3 (FP64 pipe), in bench.py",
-                "flops_per_launch": flops_per_launch,
-                "ms_per_launch": ms_k / max(n_launch, 1)}
-    phase_ms = {k: v[0] / max(args.steps, 1) for k, v in phases.items() if v[1]}
+        traffic = json.load(open(tpath)).get(f"{precision}:{dom}")
+    return {"bound": bound, "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_source": "measured in bench.py: " + src,
+            "flops_per_launch": flops_per_launch, "ms_per_launch": ms_k / max(n_launch, 1)}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from flexmm_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    d = workloads.clustered(n=args.n, n_grid=args.grid)
+    n_src, n_tgt = d["x"].size, d["tx"].size
+    pts = n_src + n_tgt
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    forms = [args.precision] + ([] if args.only else [p for p in NEQ if p != args.precision])
+    cache = {}
+    res = {p: measure(args, world, local, d, p, flush, cache) for p in forms}
+    if args.ncu:
+        return
+    peaks = {"fp64": gemm_peak_tflops(torch, torch.float64),
+             "fp32": gemm_peak_tflops(torch, torch.float32),
+             "tf32": gemm_peak_tflops(torch, torch.float32, tf32=True)}
+    main = res[args.precision]
+
+    def summary(p, r):
+        return {"value": world * pts / (r["ms_step"] * 1e-3) / 1e6, "ms_per_step": r["ms_step"],
+                "nequiv": r["neq"], "accuracy": r["accuracy"],
+                "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in r["phases"].items() if v[1]},
+                "e2e_value": world * pts / (r["e2e_step"] * 1e-3) / 1e6,
+                "roofline": roofline_of(r, p, peaks, args.steps)}
 
     out = {
-        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "metric": METRIC, "value": world * pts / (main["ms_step"] * 1e-3) / 1e6, "unit": "Mpts/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "precision": args.precision,
+        "dtype": "f32+tf32x3/f64" if args.precision == "mixed" else "f64",
+        "precision": args.precision,
         "data": "synthetic: seeded clustered sources and grid targets (no dataset)",
         "config": {"workload": f"clustered Laplace KIFMM, {n_src} sources + {args.grid}^2 grid targets, "
                                f"self + target evaluation", "n_sources": n_src, "n_targets": n_tgt,
-                   "ncutoff": NCUT, "nequiv": neq, "precision": args.precision,
+                   "ncutoff": NCUT, "nequiv": main["neq"], "precision": args.precision,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed (256 MB write) between timed steps",
-                   "levels": F._levels, "nodes": int(sum(F._counts))},
-        "accuracy": accuracy,
-        "phase_ms_per_step": phase_ms,
-        "work_per_step": counts,
-        "clocks": clk.summary(),
-        "e2e": {"value": world * pts / (e2e_step * 1e-3) / 1e6, "unit": "Mpts/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
-        "gpu_launches": launches_per_step * args.steps,
-        "roofline": roofline,
+                   "levels": main["F"]._levels, "nodes": int(sum(main["F"]._counts))},
+        "accuracy": main["accuracy"],
+        "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in main["phases"].items() if v[1]},
+        "work_per_step": main["counts"],
+        "clocks": main["clocks"],
+        "e2e": {"value": world * pts / (main["e2e_step"] * 1e-3) / 1e6, "unit": "Mpts/s",
+                "h2d_bytes_per_step": 8 * (5 * n_src + 2 * n_tgt),
+                "d2h_bytes_per_step": 8 * (n_src + n_tgt), "ms_per_step": main["e2e_step"]},
+        "gpu_launches": main["launches"],
+        "roofline": roofline_of(main, args.precision, peaks, args.steps),
+        "peaks_measured_tflops": peaks,
     }
+    for p in forms[1:]:
+        out[p] = summary(p, res[p])
+    if "fp64" in res and "mixed" in res:
+        out["mixed_over_fp64"] = res["fp64"]["ms_step"] / res["mixed"]["ms_step"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_subprocess(args)
     if rank == 0:

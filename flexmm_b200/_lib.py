@@ -11,6 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libflexmm_b200.so")
 
 N_OFFSETS = 40
+PRECISION = {"fp64": 0, "mixed": 1}
 N_PHASES = 8
 PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "spare"]
 MAX_LEVELS = 30
@@ -28,6 +29,7 @@ _vp = ctypes.c_void_p
 
 class LevelOps(ctypes.Structure):
     _fields_ = [
+        ("width", ctypes.c_double),
         ("large_x", _dp), ("large_y", _dp),
         ("c2e_u", _dp), ("c2e_sinv", _dp), ("c2e_vh", _dp),
         ("m2mc", _dp),
@@ -46,6 +48,7 @@ SIGNATURES = [
      [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _dp, _vp, ctypes.POINTER(_vp)]),
     ("fmm_plan_info", ctypes.c_int, [_vp, _ip, _dp, _ip]),
     ("fmm_plan_bind", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("fmm_plan_set_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("fmm_build_expansions", ctypes.c_int, [_vp, _vp, _vp]),
     ("fmm_evaluate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),
     ("fmm_plan_destroy", ctypes.c_int, [_vp]),

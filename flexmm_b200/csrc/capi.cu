@@ -36,10 +36,36 @@ int guarded(F &&f) {
 
 struct LevelEntry {
   DevBuf<double> buf;
+  DevBuf<float> buf32;
   LevelOpsDev dev;
 };
 
+// round to TF32 (10 explicit mantissa bits), to nearest, ties away from zero
+float tf32_rna(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u += 0x1000u;
+  u &= 0xffffe000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
 int pad8(int n) { return (n + 7) & ~7; }
+
+bool kernel_scaled(int kernel_id) {
+  switch (kernel_id) {
+    case KERNEL_LAPLACE: return LaplaceF32::kScaled;
+    default: return false;
+  }
+}
+
+double kernel_offset(int kernel_id, const KernelParams &kp, double w) {
+  switch (kernel_id) {
+    case KERNEL_LAPLACE: return LaplaceF32::offset(w, kp);
+    default: return 0.0;
+  }
+}
 
 // Keep freed stream-ordered allocations in this process's default pool, so
 // that plans created repeatedly reuse device memory instead of returning it
@@ -73,6 +99,10 @@ struct fmm_plan {
   std::vector<int> bound;  // per level: ops entry id or -1
   DevBuf<LevelOpsDev> ops_dev;
   DevBuf<double> tau_s, mult, ple, loc;
+  DevBuf<float> mult32, loc32;  // mixed precision: FP32 expansions ...
+  DevBuf<double> msum, lsum;    // ... and their FP64 component sums
+  DevBuf<double> tsum;          // per node: FP64 sum of its charges
+  int precision = PREC_FP64;
   bool have_expansions = false;
 };
 
@@ -155,7 +185,90 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
           for (int q = 0; q < r; ++q) h[base2 + size_t(q) * np + i] = m2[size_t(i) * r + q];
       }
     }
+    // mixed precision: dense operators minus their mean, as TF32 hi + lo
+    std::vector<float> f;
+    auto takef = [&](size_t count) {
+      size_t at = f.size();
+      f.resize(at + ((count + 3) & ~size_t(3)), 0.f);  // 16-byte aligned blocks
+      return at;
+    };
+    auto split = [&](double v, size_t hi_at, size_t lo_at) {
+      const float hi = tf32_rna((float)v);
+      f[hi_at] = hi;
+      f[lo_at] = tf32_rna((float)(v - (double)hi));
+    };
+    // FP32 evaluations of scale-invariant kernels work in width units
+    const bool scaled = kernel_scaled(ops->kernel_id);
+    FMMB_CHECK(!scaled || lv->width > 0, ERR_INVALID_ARGUMENT, "level width must be positive");
+    const double inv_w = scaled ? 1.0 / lv->width : 1.0;
+    const size_t f_lx = takef(np), f_ly = takef(np);
+    for (int k = 0; k < n; ++k) {
+      f[f_lx + k] = (float)(lv->large_x[k] * inv_w);
+      f[f_ly + k] = (float)(lv->large_y[k] * inv_w);
+    }
+    double c_m2m = 0.0;
+    for (size_t i = 0; i < size_t(n) * 4 * n; ++i) c_m2m += lv->m2mc[i];
+    c_m2m /= double(n) * 4 * n;
+    const size_t f_m2mct_h = takef(size_t(4) * np * np), f_m2mct_l = takef(size_t(4) * np * np);
+    const size_t f_m2mc_h = takef(size_t(4) * np * np), f_m2mc_l = takef(size_t(4) * np * np);
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < n; ++k) {
+          const double v = lv->m2mc[size_t(i) * 4 * n + c * n + k] - c_m2m;
+          const size_t t1 = size_t(c * np + k) * np + i, t2 = size_t(i) * 4 * np + c * np + k;
+          split(v, f_m2mct_h + t1, f_m2mct_l + t1);
+          split(v, f_m2mc_h + t2, f_m2mc_l + t2);
+        }
+    size_t f_m2l_h[FMM_N_OFFSETS], f_m2l_l[FMM_N_OFFSETS];
+    double c_m2l[FMM_N_OFFSETS];
+    std::vector<double> dense(size_t(n) * n);
+    for (int o = 0; o < FMM_N_OFFSETS; ++o) {
+      const int r = lv->m2l_rank[o];
+      c_m2l[o] = 0.0;
+      f_m2l_h[o] = f_m2l_l[o] = 0;
+      if (r == 0) continue;
+      if (r < 0) {
+        for (size_t i = 0; i < size_t(n) * n; ++i) dense[i] = lv->m2l_a[o][i];
+      } else {  // the truncated operator M2 . M1, as the reference applies it
+        for (int i = 0; i < n; ++i)
+          for (int k = 0; k < n; ++k) {
+            double acc = 0.0;
+            for (int q = 0; q < r; ++q) acc += lv->m2l_a[o][size_t(i) * r + q] * lv->m2l_b[o][size_t(q) * n + k];
+            dense[size_t(i) * n + k] = acc;
+          }
+      }
+      double c = 0.0;
+      for (size_t i = 0; i < size_t(n) * n; ++i) c += dense[i];
+      c /= double(n) * n;
+      c_m2l[o] = c;
+      f_m2l_h[o] = takef(size_t(np) * np);
+      f_m2l_l[o] = takef(size_t(np) * np);
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k) {
+          const size_t t = size_t(k) * np + i;  // B layout [K = source comp][N = target comp]
+          split(dense[size_t(i) * n + k] - c, f_m2l_h[o] + t, f_m2l_l[o] + t);
+        }
+    }
     auto e = std::make_unique<LevelEntry>();
+    e->buf32.alloc(f.size(), 0);
+    FMMB_CUDA(cudaMemcpy(e->buf32.get(), f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    {
+      float *fb = e->buf32.get();
+      e->dev.lx32 = fb + f_lx;
+      e->dev.ly32 = fb + f_ly;
+      e->dev.m2mct_hi = fb + f_m2mct_h;
+      e->dev.m2mct_lo = fb + f_m2mct_l;
+      e->dev.m2mc_hi = fb + f_m2mc_h;
+      e->dev.m2mc_lo = fb + f_m2mc_l;
+      e->dev.c_m2m = c_m2m;
+      e->dev.inv_w = inv_w;
+      e->dev.kofs = scaled ? kernel_offset(ops->kernel_id, ops->kp, lv->width) : 0.0;
+      for (int o = 0; o < FMM_N_OFFSETS; ++o) {
+        e->dev.m2l_hi[o] = lv->m2l_rank[o] == 0 ? nullptr : fb + f_m2l_h[o];
+        e->dev.m2l_lo[o] = lv->m2l_rank[o] == 0 ? nullptr : fb + f_m2l_l[o];
+        e->dev.c_m2l[o] = c_m2l[o];
+      }
+    }
     e->buf.alloc(h.size(), 0);
     FMMB_CUDA(cudaMemcpy(e->buf.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     double *b = e->buf.get();
@@ -212,6 +325,16 @@ int fmm_plan_info(fmm_plan *p, int *n_levels, double *widths, int *n_nodes) {
   });
 }
 
+int fmm_plan_set_precision(fmm_plan *p, int precision) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(precision == PREC_FP64 || precision == PREC_MIXED, ERR_INVALID_ARGUMENT,
+               "precision must be FMM_PRECISION_FP64 or FMM_PRECISION_MIXED");
+    p->precision = precision;
+    p->have_expansions = false;
+  });
+}
+
 int fmm_plan_bind(fmm_plan *p, int level, int level_id) {
   return guarded([&] {
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
@@ -253,15 +376,31 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
     a.ops_dev = p->ops_dev.get();
     p->tau_s.alloc(th.n_points, s);
     gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
-    p->mult.alloc(total * np, s);
     p->ple.alloc(total * np, s);
-    p->loc.alloc(total * np, s);
-    p->mult.zero(s);
     p->ple.zero(s);
-    p->loc.zero(s);
-    run_upward(a, p->tau_s.get(), p->mult.get(), s);
-    run_m2l(a, p->mult.get(), p->ple.get(), s);
-    run_downward(a, p->ple.get(), p->loc.get(), s);
+    if (p->precision == PREC_MIXED) {
+      p->mult32.alloc(total * np, s);
+      p->loc32.alloc(total * np, s);
+      p->msum.alloc(total, s);
+      p->lsum.alloc(total, s);
+      p->mult32.zero(s);
+      p->loc32.zero(s);
+      p->msum.zero(s);
+      p->lsum.zero(s);
+      p->tsum.alloc(total, s);
+      node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
+      run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(), s);
+      run_m2l_mixed(a, p->mult32.get(), p->msum.get(), p->ple.get(), s);
+      run_downward_mixed(a, p->ple.get(), p->loc32.get(), p->lsum.get(), s);
+    } else {
+      p->mult.alloc(total * np, s);
+      p->loc.alloc(total * np, s);
+      p->mult.zero(s);
+      p->loc.zero(s);
+      run_upward(a, p->tau_s.get(), p->mult.get(), s);
+      run_m2l(a, p->mult.get(), p->ple.get(), s);
+      run_downward(a, p->ple.get(), p->loc.get(), s);
+    }
     p->have_expansions = true;
   });
 }
@@ -288,8 +427,12 @@ int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int
       gather_sorted(tx, tperm.get(), m, txs.get(), s);
       gather_sorted(ty, tperm.get(), m, tys.get(), s);
     }
-    run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(), m,
-                 check, out, s);
+    if (p->precision == PREC_MIXED)
+      run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(), txs.get(),
+                         tys.get(), tkeys.get(), tperm.get(), m, check, out, s);
+    else
+      run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(),
+                   m, check, out, s);
   });
 }
 
@@ -414,6 +557,8 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
   return guarded([&] {
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+    FMMB_CHECK(p->precision == PREC_FP64, ERR_UNSUPPORTED,
+               "fmm_evaluate_noalloc evaluates FP64 plans only");
     FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
     FMMB_CHECK(m <= FMM_NOALLOC_MAX_TARGETS, ERR_CAPACITY,
                "fmm_evaluate_noalloc: more than FMM_NOALLOC_MAX_TARGETS targets");

@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 
 #include "fmm.cuh"
+#include "gemm.cuh"
 #include "timing.cuh"
 
 namespace fmmb {
@@ -41,83 +42,6 @@ __constant__ int8_t c_class_off[4][27] = {
     {7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31, 33, 34, 35, 36, 37, 38},
     {1, 2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32},
     {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31}};
-
-__host__ __device__ inline int pad_ld(int n) { return n + 4; }  // n multiple of 8 -> 4 or 12 mod 16
-
-// D[8x8] += A[8x4] . B[4x8] on the FP64 tensor cores
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
-}
-
-// Warp tile: C[r0 + 8*rb + g][c0 + 8*cb*cstride + 2q + i] += sum_k A[.][k] * B[k][.]
-// for rb < RB and the column blocks cb < CB that start below ncols
-// (g = lane/4, q = lane%4; fragment layouts of mma.m8n8k4.f64).
-// A: shared memory, row-major, stride lda.  B: global, row-major [K][ldb].
-template <int RB, int CB>
-__device__ __forceinline__ void warp_gemm(const double *A, int lda, const double *__restrict__ B,
-                                          int ldb, int K, int r0, int c0, int cstride, int ncols,
-                                          double (&acc)[RB][CB][2]) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-  const double *Ap = A + (r0 + g) * lda + q;
-  const double *Bp = B + (size_t)q * ldb + c0 + g;
-#pragma unroll 2
-  for (int k = 0; k < K; k += 4) {
-    double a[RB], b[CB];
-#pragma unroll
-    for (int rb = 0; rb < RB; ++rb) a[rb] = Ap[8 * rb * lda + k];
-#pragma unroll
-    for (int cb = 0; cb < CB; ++cb)
-      b[cb] = (c0 + 8 * cb * cstride < ncols) ? __ldg(Bp + (size_t)k * ldb + 8 * cb * cstride) : 0.0;
-#pragma unroll
-    for (int rb = 0; rb < RB; ++rb)
-#pragma unroll
-      for (int cb = 0; cb < CB; ++cb)
-        if (c0 + 8 * cb * cstride < ncols) dmma(acc[rb][cb], a[rb], b[cb]);
-  }
-}
-
-template <int RB, int CB>
-__device__ __forceinline__ void zero_acc(double (&acc)[RB][CB][2]) {
-#pragma unroll
-  for (int rb = 0; rb < RB; ++rb)
-#pragma unroll
-    for (int cb = 0; cb < CB; ++cb) acc[rb][cb][0] = acc[rb][cb][1] = 0.0;
-}
-
-// Check-to-equivalent on a 32-row tile: out = ((P . U) * sinv) . VH.
-// P, T: shared [32][pad_ld(np)].  Row t goes to out_row[t] (global, np
-// doubles) when out_row[t] is not null.  Starts and ends with a barrier-free
-// read of P; the caller synchronises before.
-__device__ void c2e_tile(const LevelOpsDev &op, int np, const double *P, double *T,
-                         double *const *out_row) {
-  const int ldp = pad_ld(np);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-  const int r0 = 8 * (warp & 3), c0 = 8 * (warp >> 2);
-  double acc[1][4][2];
-  zero_acc(acc);
-  warp_gemm<1, 4>(P, ldp, op.u, np, np, r0, c0, 2, np, acc);
-#pragma unroll
-  for (int cb = 0; cb < 4; ++cb) {
-    const int col = c0 + 16 * cb + 2 * q;
-    if (col < np) {
-      T[(r0 + g) * ldp + col] = acc[0][cb][0] * op.sinv[col];
-      T[(r0 + g) * ldp + col + 1] = acc[0][cb][1] * op.sinv[col + 1];
-    }
-  }
-  __syncthreads();
-  zero_acc(acc);
-  warp_gemm<1, 4>(T, ldp, op.vh, np, np, r0, c0, 2, np, acc);
-  double *o = out_row[r0 + g];
-  if (o) {
-#pragma unroll
-    for (int cb = 0; cb < 4; ++cb) {
-      const int col = c0 + 16 * cb + 2 * q;
-      if (col < np) *reinterpret_cast<double2 *>(o + col) = make_double2(acc[0][cb][0], acc[0][cb][1]);
-    }
-  }
-}
 
 // ---------------------------------------------------------------- upward ----
 // One tile = 32 consecutive nodes of level m.
@@ -558,33 +482,47 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
 template <class KF>
 void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
                    const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
+                   double *out, cudaStream_t s);
+
+}  // namespace
+
+void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const int total = th.n_total();
+  it.tb.alloc(total, s);
+  it.te.alloc(total, s);
+  it.nch.alloc(total, s);
+  it.choff.alloc(total, s);
+  k_leaf_targets<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), td.code.get(),
+                                                      td.flags.get(), tkeys, m, it.tb.get(),
+                                                      it.te.get(), it.nch.get());
+  FMMB_CUDA(cudaGetLastError());
+  size_t bytes = 0;
+  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, it.nch.get(), it.choff.get(), total, s));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(bytes, s);
+  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, it.nch.get(), it.choff.get(), total, s));
+}
+
+namespace {
+template <class KF>
+void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
+                   const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
                    double *out, cudaStream_t s) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int total = th.n_total();
-  DevBuf<int> tb, te, nch, choff;
-  tb.alloc(total, s);
-  te.alloc(total, s);
-  nch.alloc(total, s);
-  choff.alloc(total, s);
-  k_leaf_targets<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), td.code.get(),
-                                                      td.flags.get(), tkeys, m, tb.get(), te.get(),
-                                                      nch.get());
-  FMMB_CUDA(cudaGetLastError());
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, nch.get(), choff.get(), total, s));
-  DevBuf<uint8_t> tmp;
-  tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, nch.get(), choff.get(), total, s));
+  EvalItems it;
+  eval_items(a, tkeys, m, it, s);
   PhaseTimer timer(PH_EVAL, s);
   k_evaluate<KF><<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, total, th.L, td.dev_off.get(),
-                                         choff.get(), nch.get(), tb.get(), te.get(), td.coll.get(),
-                                         td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(),
-                                         td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc, txs, tys,
-                                         tperm, check, out);
+                                         it.choff.get(), it.nch.get(), it.tb.get(), it.te.get(),
+                                         td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+                                         td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+                                         loc, txs, tys, tperm, check, out);
   FMMB_CUDA(cudaGetLastError());
 }
-
 }  // namespace
 
 void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s) {

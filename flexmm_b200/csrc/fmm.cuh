@@ -22,7 +22,22 @@ struct LevelOpsDev {
   const double *m2l[N_OFFSETS];  // dense: D^T [NP x NP]; svd: M1^T [NP x RP] then M2^T [RP x NP]
   int kind[N_OFFSETS];
   int rp[N_OFFSETS];
+  // mixed precision: operators minus their mean c (the mean enters exactly as
+  // c * sum(input), in FP64), rounded to TF32 as hi + lo pairs, B layout [K][N]
+  const float *lx32, *ly32;             // [NP]
+  const float *m2mct_hi, *m2mct_lo;     // [4NP x NP]
+  const float *m2mc_hi, *m2mc_lo;       // [NP x 4NP]
+  const float *m2l_hi[N_OFFSETS], *m2l_lo[N_OFFSETS];  // [NP x NP] dense (D - c)^T
+  double c_m2m;
+  double c_m2l[N_OFFSETS];
+  // kernel scaling of the FP32 evaluations: coordinates are multiplied by
+  // inv_w (1/width for scale-invariant kernels, else 1) and kofs (the
+  // kernel's offset(width), else 0) times the charge sum is added in FP64;
+  // lx32 / ly32 hold the check circle already scaled
+  double inv_w, kofs;
 };
+
+constexpr int PREC_FP64 = 0, PREC_MIXED = 1;
 
 struct PassArgs {
   int kernel_id;
@@ -45,6 +60,26 @@ void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaS
 void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc,
                   const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
                   int64_t m, int check, double *out, cudaStream_t s);
+
+// Evaluation work items: per leaf its range of sorted targets, split into
+// chunks of 128 targets; choff = exclusive scan of the chunk counts.
+struct EvalItems {
+  DevBuf<int> tb, te, nch, choff;
+};
+void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s);
+
+// Mixed precision (fmm_mixed.cu): FP32 multipoles / locals with FP64 sums.
+void node_charge_sums(const PassArgs &a, const double *tau_sorted, double *tsum, cudaStream_t s);
+void run_upward_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum, float *mult32,
+                      double *msum, cudaStream_t s);
+void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, double *ple,
+                   cudaStream_t s);
+void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, double *lsum,
+                        cudaStream_t s);
+void run_evaluate_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum,
+                        const float *loc32, const double *lsum, const double *txs,
+                        const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
+                        int check, double *out, cudaStream_t s);
 
 // Evaluation with caller-provided scratch: tb, te, nch, choff hold one int
 // per tree node, temp holds evaluate_scratch_bytes(nodes) bytes.

@@ -1,0 +1,607 @@
+// Mixed-precision FMM passes: the same tree, operators and pass structure as
+// fmm.cu, with FP32 kernel evaluations and split-precision tensor-core GEMMs.
+//
+//  * S2M, L2T and P2P evaluate the kernel in FP32 on coordinates taken
+//    relative to the box centre (the subtraction is done in FP64, so no
+//    absolute position error enters); P2P sums with Kahan compensation, and a
+//    pair that coincides in FP32 is redone in FP64 (so coincident points are
+//    skipped exactly as in the reference, flexmm/flexmm2d/helpers.py:99-107);
+//  * M2M, M2L and L2L are 3xTF32 tensor-core GEMMs (hi*hi + hi*lo + lo*hi,
+//    FP32 accumulate per k-step, partial sums added in FP64) on operators
+//    with their mean removed: for an operator
+//    B = c*1*1^T + B', B.x = B'.x + c*sum(x), where sum(x) is carried in FP64
+//    per box.  The log kernel's operators are dominated by a per-level
+//    constant (-log(w^2)/4pi); without the deflation the TF32 rounding of
+//    that constant costs an order of magnitude of accuracy;
+//  * multipoles and locals are stored as FP32 plus their FP64 component sum;
+//  * check-to-equivalent stays FP64 (the FP64 tensor-core tiles of fmm.cu).
+// Error against FP64 direct summation on the 1M clustered workload at
+// Nequiv 24: ~4e-7 relative L2 (the FP64 path at Nequiv 24: ~2e-7).
+#include <cub/cub.cuh>
+
+#include "fmm.cuh"
+#include "gemm.cuh"
+#include "timing.cuh"
+
+namespace fmmb {
+namespace {
+
+constexpr int TN = 32;      // nodes per upward / downward tile
+constexpr int TM = 64;      // targets per M2L tile
+constexpr int NT = 256;     // threads per tile CTA
+constexpr int TCH = 128;    // targets per evaluation work item (= threads)
+constexpr int SMAX = 2048;  // sources staged per evaluation pass
+
+__constant__ int8_t c_class_off_mx[4][27] = {
+    {8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32, 34, 35, 36, 37, 38, 39},
+    {7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31, 33, 34, 35, 36, 37, 38},
+    {1, 2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32},
+    {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31}};
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// D[16x8] += A[16x8] . B[8x8], TF32 inputs, FP32 accumulate
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// 3xTF32 warp tile: C[r0 + g (+8)][n0 + 8*cb*nstride + 2q (+1)] += A . B for the
+// column blocks below ncols.  A: shared float [.][lda] (split to hi/lo here);
+// B: global hi/lo float [K][ldb] (pre-split).  K multiple of 8.
+// The tensor cores' FP32 accumulation does not round to nearest (it behaves
+// like truncation, which biases long sums), so every k-step's three products
+// go into a fresh zero fragment and the partial sums are accumulated in FP64.
+template <int CB>
+__device__ __forceinline__ void warp_gemm_x3(const float *A, int lda, const float *__restrict__ Bh,
+                                             const float *__restrict__ Bl, int ldb, int K, int r0,
+                                             int n0, int nstride, int ncols, double (&acc)[CB][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  for (int k0 = 0; k0 < K; k0 += 8) {
+    const float a[4] = {A[(r0 + g) * lda + k0 + q], A[(r0 + g + 8) * lda + k0 + q],
+                        A[(r0 + g) * lda + k0 + q + 4], A[(r0 + g + 8) * lda + k0 + q + 4]};
+    uint32_t ah[4], al[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      ah[i] = to_tf32(a[i]);
+      al[i] = to_tf32(a[i] - __uint_as_float(ah[i]));
+    }
+#pragma unroll
+    for (int cb = 0; cb < CB; ++cb) {
+      const int n = n0 + 8 * cb * nstride;
+      if (n < ncols) {
+        const size_t i0 = (size_t)(k0 + q) * ldb + n + g, i1 = i0 + (size_t)4 * ldb;
+        const uint32_t bh0 = __float_as_uint(__ldg(Bh + i0)), bh1 = __float_as_uint(__ldg(Bh + i1));
+        const uint32_t bl0 = __float_as_uint(__ldg(Bl + i0)), bl1 = __float_as_uint(__ldg(Bl + i1));
+        float part[4] = {0.f, 0.f, 0.f, 0.f};
+        mma_tf32(part, al, bh0, bh1);
+        mma_tf32(part, ah, bl0, bl1);
+        mma_tf32(part, ah, bh0, bh1);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[cb][i] += (double)part[i];
+      }
+    }
+  }
+}
+
+__host__ __device__ inline int pad_f(int n) { return n + 4; }  // float rows: stride 4 mod 32 words
+
+// FP64 C2E result rows in shared memory -> FP32 rows + FP64 component sums
+__device__ __forceinline__ void store_mixed(const double *P, int ldp, int np, int neq,
+                                            const int *node, int ntile, float *out32,
+                                            double *outsum) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = warp; t < ntile; t += NT / 32) {
+    const int n = node[t];
+    if (n < 0) continue;
+    double s = 0.0;
+    for (int k = lane; k < np; k += 32) {
+      const double v = k < neq ? P[t * ldp + k] : 0.0;
+      out32[(size_t)n * np + k] = (float)v;
+      s += v;
+    }
+    for (int w = 16; w >= 1; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
+    if (lane == 0) outsum[n] = s;
+  }
+}
+
+// ---------------------------------------------------------------- upward ----
+template <class KF32>
+__global__ void __launch_bounds__(NT) k_upward_mx(int m, KernelParams kp, int neq, int np, int g_begin,
+                                                  int g_end, const uint8_t *__restrict__ flags,
+                                                  const int *__restrict__ bot,
+                                                  const int *__restrict__ top,
+                                                  const int *__restrict__ child,
+                                                  const double *__restrict__ xmid,
+                                                  const double *__restrict__ ymid,
+                                                  const double *__restrict__ sx,
+                                                  const double *__restrict__ sy,
+                                                  const double *__restrict__ tau,
+                                                  const double *__restrict__ tsum,
+                                                  const LevelOpsDev *__restrict__ ops,
+                                                  float *__restrict__ mult32,
+                                                  double *__restrict__ msum) {
+  extern __shared__ double smem[];
+  const int ldp = pad_ld(np), lda = pad_f(4 * np);
+  double *P = smem;                                   // [TN][ldp] check potentials
+  double *T = P + TN * ldp;                           // [TN][ldp] C2E scratch
+  float *A = reinterpret_cast<float *>(T + TN * ldp); // [TN][lda] children multipoles (FP32)
+  __shared__ float srcx[NT / 32][32], srcy[NT / 32][32], srct[NT / 32][32];
+  __shared__ double csum[TN];
+  __shared__ int node[TN];
+  __shared__ double *orow[TN];
+  const KF32 K(kp);
+  const LevelOpsDev &op = ops[m];
+  const int g0 = g_begin + blockIdx.x * TN;
+  const int nloc = min(TN, g_end - g0);
+  for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = T[i] = 0.0;
+  for (int i = threadIdx.x; i < TN * lda; i += NT) A[i] = 0.f;
+  if (threadIdx.x < TN) {
+    csum[threadIdx.x] = 0.0;
+    node[threadIdx.x] = (int)threadIdx.x < nloc ? g0 + (int)threadIdx.x : -1;
+    orow[threadIdx.x] = P + threadIdx.x * ldp;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // S2M in FP32 (flexmm/flexmm2d/kifmm.py:96-105) / gather children (M2M)
+  for (int t = warp; t < nloc; t += NT / 32) {
+    const int g = g0 + t;
+    const uint8_t f = flags[g];
+    const int b = bot[g], e = top[g];
+    const bool up = (((f & NF_LEAF) && !(f & NF_XLIST)) || (f & NF_FAKE)) && e > b;
+    if (up) {
+      const double cx = xmid[g], cy = ymid[g], iw = op.inv_w;
+      float acc0 = 0.f, acc1 = 0.f;
+      const float lx0 = lane < neq ? op.lx32[lane] : 0.f, ly0 = lane < neq ? op.ly32[lane] : 0.f;
+      const float lx1 = lane + 32 < neq ? op.lx32[lane + 32] : 0.f;
+      const float ly1 = lane + 32 < neq ? op.ly32[lane + 32] : 0.f;
+      for (int j0 = b; j0 < e; j0 += 32) {
+        const int nj = min(32, e - j0);
+        if (lane < nj) {
+          srcx[warp][lane] = (float)((sx[j0 + lane] - cx) * iw);
+          srcy[warp][lane] = (float)((sy[j0 + lane] - cy) * iw);
+          srct[warp][lane] = (float)tau[j0 + lane];
+        }
+        __syncwarp();
+        if (lane < neq)
+          for (int j = 0; j < nj; ++j) acc0 = fmaf(K(srcx[warp][j], srcy[warp][j], lx0, ly0), srct[warp][j], acc0);
+        if (lane + 32 < neq)
+          for (int j = 0; j < nj; ++j) acc1 = fmaf(K(srcx[warp][j], srcy[warp][j], lx1, ly1), srct[warp][j], acc1);
+        __syncwarp();
+      }
+      const double c0 = op.kofs * tsum[g];  // kernel offset times the box's charge, FP64
+      if (lane < neq) P[t * ldp + lane] = c0 + (double)acc0;
+      if (lane + 32 < neq) P[t * ldp + lane + 32] = c0 + (double)acc1;
+    } else if (f & NF_CHILDREN) {
+      const int c0 = child[g];
+      const float *src = mult32 + (size_t)c0 * np;
+      for (int qd = lane; qd < 4 * np; qd += 32) A[t * lda + qd] = src[qd];
+      if (lane == 0) csum[t] = msum[c0] + msum[c0 + 1] + msum[c0 + 2] + msum[c0 + 3];
+    }
+  }
+  __syncthreads();
+  // M2M: P[t] = (M2MC - c) . children + c * sum(children)   (flexmm/flexmm2d/fmm.py:93-96)
+  {
+    const int g = lane >> 2, q = lane & 3;
+    const int r0 = 16 * (warp & 1), n0 = 8 * (warp >> 1);
+    double acc[2][4] = {};
+    warp_gemm_x3<2>(A, lda, op.m2mct_hi, op.m2mct_lo, np, 4 * np, r0, n0, 4, np, acc);
+#pragma unroll
+    for (int cb = 0; cb < 2; ++cb)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int t = r0 + g + 8 * h, col = n0 + 32 * cb + 2 * q;
+        if (t < nloc && col < np && (flags[g0 + t] & NF_CHILDREN)) {
+          const double r1 = op.c_m2m * csum[t];
+          if (col < neq) P[t * ldp + col] = acc[cb][2 * h] + r1;
+          if (col + 1 < neq) P[t * ldp + col + 1] = acc[cb][2 * h + 1] + r1;
+        }
+      }
+  }
+  __syncthreads();
+  c2e_tile(op, np, P, T, orow);
+  __syncthreads();
+  store_mixed(P, ldp, np, neq, node, TN, mult32, msum);
+}
+
+// ------------------------------------------------------------------- M2L ----
+struct M2LTilesMx {
+  int n_levels;
+  int tile_start[4 * FMM_MAX_LEVELS_DEV + 1];
+  int rg_lo[FMM_MAX_LEVELS_DEV];
+  int rg_cnt[FMM_MAX_LEVELS_DEV];
+};
+
+// 64 targets of one parity class per CTA, 4 warps x 16 target rows; output
+// FP64 partial locals = FP32 tensor-core sum + FP64 rank-one terms
+__global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int np,
+                                                const int *__restrict__ rg,
+                                                const int *__restrict__ il,
+                                                const LevelOpsDev *__restrict__ ops,
+                                                const float *__restrict__ mult32,
+                                                const double *__restrict__ msum,
+                                                double *__restrict__ ple) {
+  extern __shared__ float smf[];
+  const int ldg = pad_f(np);
+  float *G = smf;  // [TM][ldg]
+  __shared__ int tgt[TM], srow[TM];
+  __shared__ double r1s[TM];
+  int slot = 0;
+  while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= (int)blockIdx.x) ++slot;
+  const int m = slot >> 2, cls = slot & 3;
+  const int q0 = TM * (blockIdx.x - tiles.tile_start[slot]);
+  const int nloc = min(TM, tiles.rg_cnt[m] - q0);
+  if (threadIdx.x < TM)
+    tgt[threadIdx.x] = (threadIdx.x < nloc) ? rg[tiles.rg_lo[m] + q0 + threadIdx.x] + cls : -1;
+  __syncthreads();
+  const LevelOpsDev &op = ops[m];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  double acc[8][4] = {};
+  double r1 = 0.0;  // rank-one FP64 sum of target threadIdx.x
+  for (int oi = 0; oi < 27; ++oi) {
+    const int o = c_class_off_mx[cls][oi];
+    if (op.kind[o] == M2L_NULL) continue;
+    int src = -1;
+    if (threadIdx.x < TM && tgt[threadIdx.x] >= 0) src = il[(size_t)tgt[threadIdx.x] * N_OFFSETS + o];
+    if (threadIdx.x < TM) {
+      srow[threadIdx.x] = src;
+      if (src >= 0) r1 += op.c_m2l[o] * msum[src];
+    }
+    if (!__syncthreads_or(src >= 0)) continue;
+    for (int i = threadIdx.x; i < TM * (np / 4); i += 128) {
+      const int t = i / (np / 4), k4 = 4 * (i % (np / 4));
+      const int s = srow[t];
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (s >= 0) v = *reinterpret_cast<const float4 *>(mult32 + (size_t)s * np + k4);
+      *reinterpret_cast<float4 *>(G + t * ldg + k4) = v;
+    }
+    __syncthreads();
+    warp_gemm_x3<8>(G, ldg, op.m2l_hi[o], op.m2l_lo[o], np, np, 16 * warp, 0, 1, np, acc);
+    __syncthreads();
+  }
+  if (threadIdx.x < TM) r1s[threadIdx.x] = r1;
+  __syncthreads();
+#pragma unroll
+  for (int cb = 0; cb < 8; ++cb)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = 16 * warp + g + 8 * h, col = 8 * cb + 2 * q;
+      if (t < nloc && col < np) {
+        double *o = ple + (size_t)tgt[t] * np + col;
+        o[0] = col < neq ? acc[cb][2 * h] + r1s[t] : 0.0;
+        o[1] = col + 1 < neq ? acc[cb][2 * h + 1] + r1s[t] : 0.0;
+      }
+    }
+}
+
+// -------------------------------------------------------------- downward ----
+__global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int rg_lo, int rg_cnt,
+                                                    const int *__restrict__ rg,
+                                                    const int *__restrict__ parent,
+                                                    const LevelOpsDev *__restrict__ ops,
+                                                    const double *__restrict__ ple,
+                                                    float *__restrict__ loc32,
+                                                    double *__restrict__ lsum) {
+  extern __shared__ double smem[];
+  const int ldp = pad_ld(np), ldl = pad_f(np);
+  double *P = smem;                                     // [32][ldp] partial locals
+  double *T = P + TN * ldp;                             // [32][ldp] C2E scratch
+  float *Lp = reinterpret_cast<float *>(T + TN * ldp);  // [16][ldl] parent locals (rows 8-15 zero)
+  __shared__ int node[TN];
+  __shared__ double *orow[TN];
+  __shared__ double psum[8];
+  const LevelOpsDev &op = ops[m];
+  const int q0 = 8 * blockIdx.x;
+  const int ngrp = min(8, rg_cnt - q0);
+  if (threadIdx.x < TN) {
+    const int grp = threadIdx.x >> 2;
+    node[threadIdx.x] = (grp < ngrp) ? rg[rg_lo + q0 + grp] + int(threadIdx.x & 3) : -1;
+    orow[threadIdx.x] = P + threadIdx.x * ldp;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < TN * np; i += NT) {
+    const int t = i / np, k = i % np;
+    P[t * ldp + k] = (node[t] >= 0) ? ple[(size_t)node[t] * np + k] : 0.0;
+    T[t * ldp + k] = 0.0;
+  }
+  for (int i = threadIdx.x; i < 16 * ldl; i += NT) Lp[i] = 0.f;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  if (m >= 3) {
+    const LevelOpsDev &opp = ops[m - 1];
+    for (int i = threadIdx.x; i < 8 * np; i += NT) {
+      const int grp = i / np, k = i % np;
+      const int n0 = node[4 * grp];
+      Lp[grp * ldl + k] = (n0 >= 0) ? loc32[(size_t)parent[n0] * np + k] : 0.f;
+    }
+    if (threadIdx.x < 8) {
+      const int n0 = node[4 * threadIdx.x];
+      psum[threadIdx.x] = (n0 >= 0) ? lsum[parent[n0]] : 0.0;
+    }
+    __syncthreads();
+    // L2L: [8 parents][4np] = Lp . (M2MC - c) + c * sum(Lp)   (flexmm/flexmm2d/fmm.py:140-147)
+    double acc[4][4] = {};
+    warp_gemm_x3<4>(Lp, ldl, opp.m2mc_hi, opp.m2mc_lo, 4 * np, np, 0, 8 * warp, 8, 4 * np, acc);
+    if (g < 8) {
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        const int col = 8 * warp + 64 * cb + 2 * q;
+        if (col < 4 * np) {
+          const int c = col / np, i = col % np;
+          const double r1 = opp.c_m2m * psum[g];
+          if (i < neq) P[(4 * g + c) * ldp + i] += acc[cb][0] + r1;
+          if (i + 1 < neq) P[(4 * g + c) * ldp + i + 1] += acc[cb][1] + r1;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  c2e_tile(op, np, P, T, orow);
+  __syncthreads();
+  store_mixed(P, ldp, np, neq, node, TN, loc32, lsum);
+}
+
+// ------------------------------------------------------------ evaluation ----
+template <class KF32, class KF64>
+__global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, int np, int total_nodes,
+                                                     int L, const int *__restrict__ off,
+                                                     const int *__restrict__ choff,
+                                                     const int *__restrict__ nchunk,
+                                                     const int *__restrict__ tb,
+                                                     const int *__restrict__ te,
+                                                     const int *__restrict__ coll,
+                                                     const int *__restrict__ bot,
+                                                     const int *__restrict__ top,
+                                                     const double *__restrict__ xmid,
+                                                     const double *__restrict__ ymid,
+                                                     const double *__restrict__ sx,
+                                                     const double *__restrict__ sy,
+                                                     const double *__restrict__ tau,
+                                                     const double *__restrict__ tsum,
+                                                     const LevelOpsDev *__restrict__ ops,
+                                                     const float *__restrict__ loc32,
+                                                     const double *__restrict__ lsum,
+                                                     const double *__restrict__ txs,
+                                                     const double *__restrict__ tys,
+                                                     const int *__restrict__ tperm, int check,
+                                                     double *__restrict__ out) {
+  __shared__ float Ls[64], lxs[64], lys[64];
+  __shared__ float ssx[SMAX], ssy[SMAX], stau[SMAX];
+  __shared__ int sidx[SMAX];
+  __shared__ int rb[9], rs[10];
+  __shared__ double red[TCH / 32];
+  __shared__ double csrc;  // charge sum of the colleagues' sources
+  const KF32 K(kp);
+  const KF64 K64(kp);
+  const int n_items = choff[total_nodes - 1] + nchunk[total_nodes - 1];
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    int lo = 0, hi = total_nodes;
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (choff[mid] <= item) lo = mid; else hi = mid;
+    }
+    const int g = lo;
+    int lev = 0;
+    {
+      int a = 0, b = L;
+      while (b - a > 1) {
+        int mid = (a + b) >> 1;
+        if (off[mid] <= g) a = mid; else b = mid;
+      }
+      lev = a;
+    }
+    const int t0 = tb[g] + (item - choff[g]) * TCH;
+    const int cnt = min(TCH, te[g] - t0);
+    int G = 1;
+    while (2 * G * cnt <= TCH) G *= 2;
+    const int t = threadIdx.x / G, sub = threadIdx.x % G;
+    const bool valid = t < cnt;
+    const double cx = xmid[g], cy = ymid[g];
+    const double iw = ops[lev].inv_w, kofs = ops[lev].kofs;
+    const double x = valid ? txs[t0 + t] : cx, y = valid ? tys[t0 + t] : cy;
+    const float tx = (float)((x - cx) * iw), ty = (float)((y - cy) * iw);
+    if (threadIdx.x < 32) {
+      const int cg = threadIdx.x < 9 ? coll[(size_t)g * 9 + threadIdx.x] : -1;
+      if (threadIdx.x < 9) {
+        rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
+        rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
+      }
+      double cs = cg >= 0 ? tsum[cg] : 0.0;
+      for (int w = 16; w >= 1; w >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, w);
+      if (threadIdx.x == 0) csrc = cs;
+    }
+    if (threadIdx.x == 0) rs[0] = 0;
+    if (lev >= 2)
+      for (int k = threadIdx.x; k < neq; k += TCH) {
+        Ls[k] = loc32[(size_t)g * np + k];
+        lxs[k] = ops[lev].lx32[k];
+        lys[k] = ops[lev].ly32[k];
+      }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
+    float ul = 0.f;  // L2T part (flexmm/flexmm2d/kifmm.py:106-120)
+    if (lev >= 2 && valid)
+      for (int k = sub; k < neq; k += G) ul = fmaf(K(lxs[k], lys[k], tx, ty), Ls[k], ul);
+    __syncthreads();
+    // P2P (flexmm/flexmm2d/helpers.py:152-194), Kahan-compensated FP32
+    float s = 0.f, comp = 0.f;
+    double exact = 0.0;
+    const int ns = rs[9];
+    for (int base = 0; base < ns; base += SMAX) {
+      const int nb = min(SMAX, ns - base);
+      for (int i = threadIdx.x; i < nb; i += TCH) {
+        const int idx = base + i;
+        int c = 0;
+        while (idx >= rs[c + 1]) ++c;
+        const int j = rb[c] + (idx - rs[c]);
+        ssx[i] = (float)((sx[j] - cx) * iw);
+        ssy[i] = (float)((sy[j] - cy) * iw);
+        stau[i] = (float)tau[j];
+        sidx[i] = j;
+      }
+      __syncthreads();
+      if (valid) {
+        for (int j = sub; j < nb; j += G) {
+          const float dx = tx - ssx[j], dy = ty - ssy[j];
+          if (dx * dx + dy * dy == 0.f) {
+            // coincident in FP32: decide and evaluate in FP64 on the exact
+            // coordinates (the kernel offset of this source is already in csrc)
+            const int jj = sidx[j];
+            const double qx = sx[jj], qy = sy[jj];
+            exact -= kofs * tau[jj];
+            if (check && x - qx == 0.0 && y - qy == 0.0) continue;
+            exact += K64(qx, qy, x, y) * tau[jj];
+            continue;
+          }
+          const float v = K(ssx[j], ssy[j], tx, ty) * stau[j] - comp;
+          const float tt = s + v;
+          comp = (tt - s) - v;
+          s = tt;
+        }
+      }
+      __syncthreads();
+    }
+    double u = (double)ul + (double)s - (double)comp + exact;
+    if (sub == 0) u += kofs * (csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
+    for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
+    if (G > 32) {
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
+      __syncthreads();
+      if (sub == 0) {
+        u = 0.0;
+        for (int w = 0; w < G / 32; ++w) u += red[(threadIdx.x >> 5) + w];
+      }
+    }
+    if (valid && sub == 0) out[tperm[t0 + t]] = u;
+    __syncthreads();
+  }
+}
+
+// per node: FP64 sum of its charges (one warp per node)
+__global__ void k_node_charge_sums(int total, const int *__restrict__ bot, const int *__restrict__ top,
+                                   const double *__restrict__ tau, double *__restrict__ tsum) {
+  const int lane = threadIdx.x & 31;
+  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total;
+       g += (gridDim.x * blockDim.x) >> 5) {
+    double v = 0.0;
+    for (int j = bot[g] + lane; j < top[g]; j += 32) v += tau[j];
+    for (int w = 16; w >= 1; w >>= 1) v += __shfl_xor_sync(0xffffffffu, v, w);
+    if (lane == 0) tsum[g] = v;
+  }
+}
+
+template <class KF32>
+void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, float *mult32,
+                    double *msum, cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const int np = a.np;
+  auto bytes = [](int n) {
+    return sizeof(double) * (size_t)TN * pad_ld(n) * 2 + sizeof(float) * (size_t)TN * pad_f(4 * n);
+  };
+  FMMB_CUDA(cudaFuncSetAttribute(k_upward_mx<KF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(bytes(64))));
+  for (int m = th.L - 1; m >= 2; --m) {
+    const int gb = th.off[m], ge = th.off[m + 1];
+    const int tiles = (ge - gb + TN - 1) / TN;
+    PhaseTimer timer(PH_UPWARD, s);
+    k_upward_mx<KF32><<<tiles, NT, bytes(np), s>>>(m, a.kp, a.neq, np, gb, ge, td.flags.get(),
+                                                   td.bot.get(), td.top.get(), td.child.get(),
+                                                   td.xmid.get(), td.ymid.get(), td.sx.get(),
+                                                   td.sy.get(), tau_s, tsum, a.ops_dev, mult32, msum);
+    FMMB_CUDA(cudaGetLastError());
+  }
+}
+
+}  // namespace
+
+void node_charge_sums(const PassArgs &a, const double *tau_s, double *tsum, cudaStream_t s) {
+  const int total = a.th->n_total();
+  k_node_charge_sums<<<grid_for((int64_t)total * 32, 256), 256, 0, s>>>(total, a.td->bot.get(),
+                                                                        a.td->top.get(), tau_s, tsum);
+  FMMB_CUDA(cudaGetLastError());
+}
+
+void run_upward_mixed(const PassArgs &a, const double *tau_s, const double *tsum, float *mult32,
+                      double *msum, cudaStream_t s) {
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE: upward_mx_impl<LaplaceF32>(a, tau_s, tsum, mult32, msum, s); break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+}
+
+void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, double *ple,
+                   cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  if (th.L < 3) return;
+  FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
+  M2LTilesMx tl{};
+  tl.n_levels = th.L;
+  int tiles = 0;
+  for (int m = 0; m < th.L; ++m) {
+    tl.rg_lo[m] = th.rg_lo[m];
+    tl.rg_cnt[m] = th.rg_hi[m] - th.rg_lo[m];
+    for (int c = 0; c < 4; ++c) {
+      tl.tile_start[4 * m + c] = tiles;
+      if (m >= 2) tiles += (tl.rg_cnt[m] + TM - 1) / TM;
+    }
+  }
+  tl.tile_start[4 * th.L] = tiles;
+  if (tiles == 0) return;
+  const size_t sm = sizeof(float) * (size_t)TM * pad_f(a.np);
+  PhaseTimer timer(PH_M2L, s);
+  k_m2l_mx<<<tiles, 128, sm, s>>>(tl, a.neq, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev, mult32,
+                                  msum, ple);
+  FMMB_CUDA(cudaGetLastError());
+}
+
+void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, double *lsum,
+                        cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const size_t sm = sizeof(double) * (size_t)TN * pad_ld(a.np) * 2 +
+                    sizeof(float) * (size_t)16 * pad_f(a.np);
+  for (int m = 2; m < th.L; ++m) {
+    const int lo = th.rg_lo[m], cnt = th.rg_hi[m] - th.rg_lo[m];
+    if (cnt <= 0) continue;
+    PhaseTimer timer(PH_DOWNWARD, s);
+    k_downward_mx<<<(cnt + 7) / 8, NT, sm, s>>>(m, a.neq, a.np, lo, cnt, td.rg.get(), td.parent.get(),
+                                                a.ops_dev, ple, loc32, lsum);
+    FMMB_CUDA(cudaGetLastError());
+  }
+}
+
+void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *tsum,
+                        const float *loc32, const double *lsum, const double *txs,
+                        const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
+                        int check, double *out, cudaStream_t s) {
+  if (m == 0) return;
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const int total = th.n_total();
+  EvalItems it;
+  eval_items(a, tkeys, m, it, s);
+  PhaseTimer timer(PH_EVAL, s);
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE:
+      k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * 8, TCH, 0, s>>>(
+          a.kp, a.neq, a.np, total, th.L, td.dev_off.get(), it.choff.get(), it.nch.get(),
+          it.tb.get(), it.te.get(), td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+          td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, tsum, a.ops_dev, loc32, lsum, txs, tys,
+          tperm, check, out);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+  FMMB_CUDA(cudaGetLastError());
+}
+
+}  // namespace fmmb

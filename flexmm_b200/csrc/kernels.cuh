@@ -9,6 +9,8 @@
 #pragma once
 #include <math.h>
 
+#include <cmath>
+
 #include "common.cuh"
 
 namespace fmmb {
@@ -25,6 +27,22 @@ struct LaplaceF64 {
     const double dx = tx - sx, dy = ty - sy;
     return -log(dx * dx + dy * dy) * (1.0 / (4.0 * M_PI));
   }
+};
+
+// FP32 evaluation for the mixed-precision passes.  The log kernel is scale
+// invariant up to a constant, K(w r) = offset(w) + K(r) with offset(w) =
+// -log(w^2)/(4 pi): the mixed passes evaluate K in FP32 on coordinates divided
+// by the box width (O(1) arguments, so FP32 keeps the kernel's variation to
+// ~1e-7 absolute) and add offset(w) times the charge sum in FP64.  Kernels
+// without such a decomposition set kScaled = false and offset() = 0.
+struct LaplaceF32 {
+  static constexpr bool kScaled = true;
+  __host__ __device__ explicit LaplaceF32(const KernelParams &) {}
+  __device__ __forceinline__ float operator()(float sx, float sy, float tx, float ty) const {
+    const float dx = tx - sx, dy = ty - sy;
+    return -logf(dx * dx + dy * dy) * (float)(1.0 / (4.0 * M_PI));
+  }
+  static double offset(double w, const KernelParams &) { return -std::log(w * w) / (4.0 * M_PI); }
 };
 
 }  // namespace fmmb

@@ -105,7 +105,7 @@ class KIPrecomputation:
         arr_a = (dp * len(self.m2l_a))(*[ptr(a) for a in self.m2l_a])
         arr_b = (dp * len(self.m2l_b))(*[ptr(b) for b in self.m2l_b])
         lv = _lib.LevelOps(
-            large_x=ptr(self.large_x), large_y=ptr(self.large_y),
+            width=self.width, large_x=ptr(self.large_x), large_y=ptr(self.large_y),
             c2e_u=ptr(self.c2e_u), c2e_sinv=ptr(self.c2e_sinv), c2e_vh=ptr(self.c2e_vh),
             m2mc=ptr(self.m2mc),
             m2l_rank=self.m2l_rank.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),

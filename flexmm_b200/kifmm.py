@@ -9,7 +9,10 @@ Same constructor, methods and results as flexmm/flexmm2d/kifmm.py:122-144
     u_tgt = F.target_evaluation(tx, ty)
 
 Inputs may be numpy arrays (results come back as numpy) or torch tensors
-(results stay torch tensors on the GPU).  All work runs on the current CUDA
+(results stay torch tensors on the GPU).  ``precision="mixed"`` selects the
+split-precision form (FP32 kernel evaluations, 3xTF32 tensor-core far-field
+GEMMs, FP64 check-to-equivalent); the default ``"fp64"`` matches the
+reference to 1e-12.  All work runs on the current CUDA
 device and torch's current stream, through ``libflexmm_b200.so``; there is
 no CPU path.
 """
@@ -131,11 +134,14 @@ class KI_FMM:
     """Kernel-independent FMM (KI_FMM, flexmm/flexmm2d/kifmm.py:122-144)."""
 
     def __init__(self, x, y, kernel_eval, Ncutoff=50, Nequiv=50, dtype=float, bbox=None,
-                 helper=None, verbose=False, **kernel_params):
+                 helper=None, verbose=False, precision="fp64", **kernel_params):
         if dtype not in (float, np.float64):
             raise NotImplementedError("only real float64 charges are supported")
         if Nequiv > _lib.MAX_NEQUIV:
             raise ValueError(f"Nequiv must be <= {_lib.MAX_NEQUIV}")
+        if precision not in _lib.PRECISION:
+            raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
+        self.precision = precision
         _lib.load()
         self.kernel = resolve(kernel_eval, **kernel_params)
         self.Ncutoff = int(Ncutoff)
@@ -164,6 +170,7 @@ class KI_FMM:
                   ctypes.byref(plan))
         self._plan = plan
         self._ops = self.helper.ops_set()   # keep the operator set alive with the plan
+        _lib.call("fmm_plan_set_precision", plan, _lib.PRECISION[precision])
         self._x, self._y = xd, yd
         nl = ctypes.c_int()
         widths = (ctypes.c_double * _lib.MAX_LEVELS)()

@@ -58,6 +58,7 @@ typedef struct fmm_plan fmm_plan;
  * Precomputation.compress / M2L_Evaluator (flexmm/flexmm2d/helpers.py:5-33,
  * 196-218). */
 typedef struct fmm_level_ops {
+  double width;                    /* box width w of this level               */
   const double *large_x, *large_y; /* [n] check circle of radius w(4-sqrt2)/2 */
   const double *c2e_u;             /* [n*n] U of S2L = U diag(S) VH          */
   const double *c2e_sinv;          /* [n] 1/S (0 for discarded values)        */
@@ -80,6 +81,16 @@ int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, i
 /* n_levels and, for each level, its box width and node count (host arrays of
  * FMM_MAX_LEVELS entries). */
 int fmm_plan_info(fmm_plan *plan, int *n_levels, double *widths, int *n_nodes);
+/* Arithmetic of the passes (the precision forms of the path):
+ *   FMM_PRECISION_FP64   everything in FP64 (matches the reference to 1e-12);
+ *   FMM_PRECISION_MIXED  FP32 kernel evaluations (P2P with compensated sums),
+ *                        split-precision (3xTF32) tensor-core M2M / M2L / L2L
+ *                        with FP32 accumulate on mean-deflated operators,
+ *                        FP64 check-to-equivalent and final accumulation.
+ * Set before fmm_build_expansions (it invalidates previous expansions). */
+#define FMM_PRECISION_FP64 0
+#define FMM_PRECISION_MIXED 1
+int fmm_plan_set_precision(fmm_plan *plan, int precision);
 /* Use operator entry level_id (from fmm_ops_add) for tree level `level`. */
 int fmm_plan_bind(fmm_plan *plan, int level, int level_id);
 /* tau: device charges [n] in the caller's (original) source order. */

@@ -1,0 +1,43 @@
+"""Mixed-precision form: error against FP64 direct summation (bar: 1e-6 relative L2)."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+BAR = 1e-6
+
+
+def _run(d, ncut, neq, precision, tx, ty):
+    from flexmm_b200 import KI_FMM, KI_Helper
+    F = KI_FMM(d["x"], d["y"], "Laplace_Eval", ncut, neq, bbox=d["bbox"], helper=KI_Helper(),
+               precision=precision)
+    F.build_expansions(d["tau"])
+    return F, F.source_evaluation(d["x"], d["y"]), F.target_evaluation(tx, ty)
+
+
+@pytest.mark.parametrize("recipe,n,neq", [("clustered", 200_000, 24), ("uniform", 100_000, 24),
+                                          ("clustered", 100_000, 32)])
+def test_mixed_error_vs_direct_sum(built_lib, recipe, n, neq):
+    from flexmm_b200 import direct_evaluation, workloads
+    d = getattr(workloads, recipe)(n=n, n_grid=300, seed=41)
+    F, us, ut = _run(d, 64, neq, "mixed", d["tx"], d["ty"])
+    rng = np.random.default_rng(1)
+    si = rng.choice(d["x"].size, 2000, replace=False)
+    ti = rng.choice(d["tx"].size, 2000, replace=False)
+    ds = direct_evaluation("Laplace_Eval", d["x"], d["y"], d["tau"], d["x"][si], d["y"][si], check=True)
+    dt = direct_evaluation("Laplace_Eval", d["x"], d["y"], d["tau"], d["tx"][ti], d["ty"][ti])
+    es, et = rel_l2(us[si], ds), rel_l2(ut[ti], dt)
+    assert es < BAR and et < BAR, (es, et)
+
+
+def test_mixed_coincident_points_are_skipped_exactly(built_lib):
+    """Duplicated sources: the FP32 path must still skip exactly the coincident pairs."""
+    from conftest import golden_inputs, load_golden
+    g = load_golden("duplicates_5k_q24")
+    d = golden_inputs(g["meta"])
+    F, us, ut = _run(d, g["meta"]["ncut"], g["meta"]["neq"], "mixed", d["tx"], d["ty"])
+    assert np.isfinite(us).all() and np.isfinite(ut).all()
+    assert rel_l2(us, g["direct_src"]) < BAR
+    assert rel_l2(ut, g["direct_tgt"]) < BAR
