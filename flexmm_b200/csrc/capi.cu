@@ -421,7 +421,8 @@ int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int
     DevBuf<double> txs, tys;
     {
       PhaseTimer timer(PH_SORT_TGT, s);
-      sort_points(tx, ty, m, p->th, tkeys, tperm, s);
+      // leaves live on levels <= L-1: their first L-1 digits decide everything
+      sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1);
       txs.alloc(m, s);
       tys.alloc(m, s);
       gather_sorted(tx, tperm.get(), m, txs.get(), s);
@@ -588,6 +589,8 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
     int *te = (int *)carve(total * sizeof(int));
     int *nch = (int *)carve(total * sizeof(int));
     int *choff = (int *)carve(total * sizeof(int));
+    int4 *items = (int4 *)carve((total + m / EVAL_CHUNK + 1) * sizeof(int4));
+    int *n_items = (int *)carve(sizeof(int));
     void *sort_tmp = carve(sort_bytes);
     void *scan_tmp = carve(scan_bytes);
     FMMB_CHECK(at <= NOALLOC_SCRATCH_BYTES, ERR_CAPACITY,
@@ -607,6 +610,6 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
     gather_sorted(tx, tperm, m, txs, s);
     gather_sorted(ty, tperm, m, tys, s);
     run_evaluate_scratch(a, p->tau_s.get(), p->loc.get(), txs, tys, tkeys, tperm, m, check, out, tb,
-                         te, nch, choff, scan_tmp, scan_bytes, s);
+                         te, nch, choff, items, n_items, scan_tmp, scan_bytes, s);
   });
 }

@@ -303,17 +303,35 @@ __global__ void k_leaf_targets(int total, int L, const int *__restrict__ off,
   }
 }
 
+// expand the per-leaf chunk counts into a flat item list
+__global__ void k_make_items(int total, int L, const int *__restrict__ off, const int *__restrict__ tb,
+                             const int *__restrict__ te, const int *__restrict__ nch,
+                             const int *__restrict__ choff, int4 *__restrict__ items,
+                             int *__restrict__ n_items) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    if (g == total - 1) *n_items = choff[g] + nch[g];
+    const int n = nch[g];
+    if (n == 0) continue;
+    int lo = 0, hi = L;
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (off[mid] <= g) lo = mid; else hi = mid;
+    }
+    for (int c = 0; c < n; ++c) {
+      const int t0 = tb[g] + c * TCH;
+      items[choff[g] + c] = make_int4(g, lo, t0, min(TCH, te[g] - t0));
+    }
+  }
+}
+
 // One work item = (leaf, up to 128 of its targets).  G = 128 / targets
 // (rounded down to a power of two) threads share a target: they split the
 // circle points of L2T and the colleague sources of P2P, then reduce with
 // warp shuffles (and shared memory when G > 32).
 template <class KF>
-__global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np, int total_nodes,
-                                                  int L, const int *__restrict__ off,
-                                                  const int *__restrict__ choff,
-                                                  const int *__restrict__ nchunk,
-                                                  const int *__restrict__ tb,
-                                                  const int *__restrict__ te,
+__global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np,
+                                                  const int4 *__restrict__ items,
+                                                  const int *__restrict__ n_items_ptr,
                                                   const int *__restrict__ coll,
                                                   const int *__restrict__ bot,
                                                   const int *__restrict__ top,
@@ -333,31 +351,15 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
   __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
   __shared__ double red[TCH / 32];
   const KF K(kp);
-  const int n_items = choff[total_nodes - 1] + nchunk[total_nodes - 1];
+  const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    int lo = 0, hi = total_nodes;  // last g with choff[g] <= item
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (choff[mid] <= item) lo = mid; else hi = mid;
-    }
-    const int g = lo;
-    int lev = 0;
-    {
-      int a = 0, b = L;
-      while (b - a > 1) {
-        int mid = (a + b) >> 1;
-        if (off[mid] <= g) a = mid; else b = mid;
-      }
-      lev = a;
-    }
-    const int t0 = tb[g] + (item - choff[g]) * TCH;
-    const int cnt = min(TCH, te[g] - t0);
+    const int4 it = items[item];
+    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
     int G = 1;
     while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
     const bool valid = t < cnt;
     const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
-    double u = 0.0;
     if (threadIdx.x < 9) {
       const int cg = coll[(size_t)g * 9 + threadIdx.x];
       rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
@@ -374,12 +376,26 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     __syncthreads();
     if (threadIdx.x == 0)
       for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
     if (lev >= 2 && valid) {
       const double dx = x - xmid[g], dy = y - ymid[g];
-      for (int k = sub; k < neq; k += G) u = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u);
+      int k = sub;
+      for (; k + 3 * G < neq; k += 4 * G) {
+        u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
+        u1 = fma(K(lxs[k + G], lys[k + G], dx, dy), Ls[k + G], u1);
+        u2 = fma(K(lxs[k + 2 * G], lys[k + 2 * G], dx, dy), Ls[k + 2 * G], u2);
+        u3 = fma(K(lxs[k + 3 * G], lys[k + 3 * G], dx, dy), Ls[k + 3 * G], u3);
+      }
+      for (; k < neq; k += G) u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
     }
     __syncthreads();
-    // P2P over the colleagues' sorted source ranges (flexmm/flexmm2d/helpers.py:152-194)
+    // P2P over the colleagues' sorted source ranges (flexmm/flexmm2d/helpers.py:152-194);
+    // a coincident pair is skipped when check is set (helpers.py:99-107)
+    auto pair = [&](int j) -> double {
+      const double qx = ssx[j], qy = ssy[j];
+      const double v = K(qx, qy, x, y) * stau[j];
+      return (check && x - qx == 0.0 && y - qy == 0.0) ? 0.0 : v;
+    };
     const int ns = rs[9];
     for (int base = 0; base < ns; base += SMAX) {
       const int nb = min(SMAX, ns - base);
@@ -394,15 +410,19 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
       }
       __syncthreads();
       if (valid) {
-        for (int j = sub; j < nb; j += G) {
-          const double qx = ssx[j], qy = ssy[j];
-          if (check && x - qx == 0.0 && y - qy == 0.0) continue;
-          u = fma(K(qx, qy, x, y), stau[j], u);
+        int j = sub;
+        for (; j + 3 * G < nb; j += 4 * G) {
+          u0 += pair(j);
+          u1 += pair(j + G);
+          u2 += pair(j + 2 * G);
+          u3 += pair(j + 3 * G);
         }
+        for (; j < nb; j += G) u0 += pair(j);
       }
       __syncthreads();
     }
     // reduce over the G threads of each target
+    double u = (u0 + u1) + (u2 + u3);
     for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
     if (G > 32) {
       if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
@@ -503,6 +523,12 @@ void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &
   DevBuf<uint8_t> tmp;
   tmp.alloc(bytes, s);
   FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, it.nch.get(), it.choff.get(), total, s));
+  it.items.alloc(total + m / TCH + 1, s);
+  it.n_items.alloc(1, s);
+  k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), it.tb.get(),
+                                                    it.te.get(), it.nch.get(), it.choff.get(),
+                                                    it.items.get(), it.n_items.get());
+  FMMB_CUDA(cudaGetLastError());
 }
 
 namespace {
@@ -516,8 +542,7 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
   EvalItems it;
   eval_items(a, tkeys, m, it, s);
   PhaseTimer timer(PH_EVAL, s);
-  k_evaluate<KF><<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, total, th.L, td.dev_off.get(),
-                                         it.choff.get(), it.nch.get(), it.tb.get(), it.te.get(),
+  k_evaluate<KF><<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(),
                                          td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
                                          td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
                                          loc, txs, tys, tperm, check, out);
@@ -609,7 +634,8 @@ size_t evaluate_scratch_bytes(int total_nodes) {
 void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *loc,
                           const double *txs, const double *tys, const uint64_t *tkeys,
                           const int *tperm, int64_t m, int check, double *out, int *tb, int *te,
-                          int *nch, int *choff, void *temp, size_t temp_bytes, cudaStream_t s) {
+                          int *nch, int *choff, int4 *items, int *n_items, void *temp,
+                          size_t temp_bytes, cudaStream_t s) {
   if (m == 0) return;
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
@@ -619,12 +645,15 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   FMMB_CUDA(cudaGetLastError());
   size_t bytes = temp_bytes;
   FMMB_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, nch, choff, total, s));
+  k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), tb, te, nch, choff,
+                                                    items, n_items);
+  FMMB_CUDA(cudaGetLastError());
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
       k_evaluate<LaplaceF64><<<148 * 8, TCH, 0, s>>>(
-          a.kp, a.neq, a.np, total, th.L, td.dev_off.get(), choff, nch, tb, te, td.coll.get(),
-          td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s,
-          a.ops_dev, loc, txs, tys, tperm, check, out);
+          a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(), td.top.get(),
+          td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc, txs, tys,
+          tperm, check, out);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

@@ -65,7 +65,10 @@ void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc
 // chunks of 128 targets; choff = exclusive scan of the chunk counts.
 struct EvalItems {
   DevBuf<int> tb, te, nch, choff;
+  DevBuf<int4> items;   // (leaf, level, first sorted target, count)
+  DevBuf<int> n_items;  // device count of items
 };
+constexpr int EVAL_CHUNK = 128;  // targets per evaluation work item
 void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s);
 
 // Mixed precision (fmm_mixed.cu): FP32 multipoles / locals with FP64 sums.
@@ -87,6 +90,7 @@ size_t evaluate_scratch_bytes(int total_nodes);
 void run_evaluate_scratch(const PassArgs &a, const double *tau_sorted, const double *loc,
                           const double *txs, const double *tys, const uint64_t *tkeys,
                           const int *tperm, int64_t m, int check, double *out, int *tb, int *te,
-                          int *nch, int *choff, void *temp, size_t temp_bytes, cudaStream_t s);
+                          int *nch, int *choff, int4 *items, int *n_items, void *temp,
+                          size_t temp_bytes, cudaStream_t s);
 
 }  // namespace fmmb

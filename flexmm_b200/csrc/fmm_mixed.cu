@@ -2,9 +2,11 @@
 // fmm.cu, with FP32 kernel evaluations and split-precision tensor-core GEMMs.
 //
 //  * S2M, L2T and P2P evaluate the kernel in FP32 on coordinates taken
-//    relative to the box centre (the subtraction is done in FP64, so no
-//    absolute position error enters); P2P sums with Kahan compensation, and a
-//    pair that coincides in FP32 is redone in FP64 (so coincident points are
+//    relative to the box centre and divided by its width (the subtraction is
+//    done in FP64, so no absolute position error enters; a scale-invariant
+//    kernel's constant offset times the charge sum is added in FP64); P2P
+//    sums FP32 partials of a few terms into FP64, and a pair that coincides
+//    in FP32 is redone in FP64 (so coincident points are
 //    skipped exactly as in the reference, flexmm/flexmm2d/helpers.py:99-107);
 //  * M2M, M2L and L2L are 3xTF32 tensor-core GEMMs (hi*hi + hi*lo + lo*hi,
 //    FP32 accumulate per k-step, partial sums added in FP64) on operators
@@ -350,13 +352,13 @@ __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int 
 }
 
 // ------------------------------------------------------------ evaluation ----
+// P2P pairs are summed in FP32 over at most 4 x 8 terms per thread, then in
+// FP64 (cascaded summation: the FP32 rounding stays relative to short partial
+// sums); the kernel offset terms are added in FP64.
 template <class KF32, class KF64>
-__global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, int np, int total_nodes,
-                                                     int L, const int *__restrict__ off,
-                                                     const int *__restrict__ choff,
-                                                     const int *__restrict__ nchunk,
-                                                     const int *__restrict__ tb,
-                                                     const int *__restrict__ te,
+__global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, int np,
+                                                     const int4 *__restrict__ items,
+                                                     const int *__restrict__ n_items_ptr,
                                                      const int *__restrict__ coll,
                                                      const int *__restrict__ bot,
                                                      const int *__restrict__ top,
@@ -381,25 +383,10 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
   __shared__ double csrc;  // charge sum of the colleagues' sources
   const KF32 K(kp);
   const KF64 K64(kp);
-  const int n_items = choff[total_nodes - 1] + nchunk[total_nodes - 1];
+  const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    int lo = 0, hi = total_nodes;
-    while (hi - lo > 1) {
-      int mid = (lo + hi) >> 1;
-      if (choff[mid] <= item) lo = mid; else hi = mid;
-    }
-    const int g = lo;
-    int lev = 0;
-    {
-      int a = 0, b = L;
-      while (b - a > 1) {
-        int mid = (a + b) >> 1;
-        if (off[mid] <= g) a = mid; else b = mid;
-      }
-      lev = a;
-    }
-    const int t0 = tb[g] + (item - choff[g]) * TCH;
-    const int cnt = min(TCH, te[g] - t0);
+    const int4 it = items[item];
+    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
     int G = 1;
     while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
@@ -428,12 +415,19 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
     __syncthreads();
     if (threadIdx.x == 0)
       for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
-    float ul = 0.f;  // L2T part (flexmm/flexmm2d/kifmm.py:106-120)
-    if (lev >= 2 && valid)
-      for (int k = sub; k < neq; k += G) ul = fmaf(K(lxs[k], lys[k], tx, ty), Ls[k], ul);
+    double acc = 0.0;
+    if (lev >= 2 && valid) {  // L2T (flexmm/flexmm2d/kifmm.py:106-120)
+      float p0 = 0.f, p1 = 0.f;
+      int k = sub;
+      for (; k + G < neq; k += 2 * G) {
+        p0 = fmaf(K(lxs[k], lys[k], tx, ty), Ls[k], p0);
+        p1 = fmaf(K(lxs[k + G], lys[k + G], tx, ty), Ls[k + G], p1);
+      }
+      if (k < neq) p0 = fmaf(K(lxs[k], lys[k], tx, ty), Ls[k], p0);
+      acc = (double)p0 + (double)p1;
+    }
     __syncthreads();
-    // P2P (flexmm/flexmm2d/helpers.py:152-194), Kahan-compensated FP32
-    float s = 0.f, comp = 0.f;
+    // P2P (flexmm/flexmm2d/helpers.py:152-194)
     double exact = 0.0;
     const int ns = rs[9];
     for (int base = 0; base < ns; base += SMAX) {
@@ -450,27 +444,40 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
       }
       __syncthreads();
       if (valid) {
-        for (int j = sub; j < nb; j += G) {
-          const float dx = tx - ssx[j], dy = ty - ssy[j];
-          if (dx * dx + dy * dy == 0.f) {
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+        int nsum = 0;
+        int j = sub;
+        auto pair = [&](int jj) -> float {
+          const float dx = tx - ssx[jj], dy = ty - ssy[jj];
+          const float d2 = dx * dx + dy * dy;
+          if (d2 == 0.f) {
             // coincident in FP32: decide and evaluate in FP64 on the exact
-            // coordinates (the kernel offset of this source is already in csrc)
-            const int jj = sidx[j];
-            const double qx = sx[jj], qy = sy[jj];
-            exact -= kofs * tau[jj];
-            if (check && x - qx == 0.0 && y - qy == 0.0) continue;
-            exact += K64(qx, qy, x, y) * tau[jj];
-            continue;
+            // coordinates (this source's kernel offset is already in csrc)
+            const int q = sidx[jj];
+            const double qx = sx[q], qy = sy[q];
+            exact -= kofs * tau[q];
+            if (!(check && x - qx == 0.0 && y - qy == 0.0)) exact += K64(qx, qy, x, y) * tau[q];
+            return 0.f;
           }
-          const float v = K(ssx[j], ssy[j], tx, ty) * stau[j] - comp;
-          const float tt = s + v;
-          comp = (tt - s) - v;
-          s = tt;
+          return K(ssx[jj], ssy[jj], tx, ty) * stau[jj];
+        };
+        for (; j + 3 * G < nb; j += 4 * G) {
+          p0 += pair(j);
+          p1 += pair(j + G);
+          p2 += pair(j + 2 * G);
+          p3 += pair(j + 3 * G);
+          if (++nsum == 8) {
+            acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+            p0 = p1 = p2 = p3 = 0.f;
+            nsum = 0;
+          }
         }
+        for (; j < nb; j += G) p0 += pair(j);
+        acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
       }
       __syncthreads();
     }
-    double u = (double)ul + (double)s - (double)comp + exact;
+    double u = acc + exact;
     if (sub == 0) u += kofs * (csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
     for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
     if (G > 32) {
@@ -594,10 +601,9 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
       k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * 8, TCH, 0, s>>>(
-          a.kp, a.neq, a.np, total, th.L, td.dev_off.get(), it.choff.get(), it.nch.get(),
-          it.tb.get(), it.te.get(), td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
-          td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, tsum, a.ops_dev, loc32, lsum, txs, tys,
-          tperm, check, out);
+          a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, tsum,
+          a.ops_dev, loc32, lsum, txs, tys, tperm, check, out);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

@@ -40,8 +40,13 @@ struct Counters {
   int max_level;
   int too_deep;
   int overflow;
-  int pad;
+  int need_full_sort;
 };
+
+// The source keys are first sorted on their top SORT_DIGITS digits only; that
+// fixes every box of levels <= SORT_DIGITS.  A tree that would split a box of
+// level >= SORT_DIGITS is redone with a full sort.
+constexpr int SORT_DIGITS = 16;
 
 __device__ __forceinline__ int common_digits(uint64_t a, uint64_t b) {
   uint64_t d = a ^ b;
@@ -132,9 +137,10 @@ __global__ void k_gather_xy(const double *__restrict__ x, const double *__restri
 }
 
 // --- 3. initially split boxes ------------------------------------------------
+// keys sorted on their top `sorted_digits` digits
 __global__ void k_initial_splits(const uint64_t *__restrict__ keys, int64_t n, int ppl,
-                                 uint64_t *__restrict__ out, unsigned long long cap,
-                                 Counters *cnt) {
+                                 int sorted_digits, uint64_t *__restrict__ out,
+                                 unsigned long long cap, Counters *cnt) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = keys[i];
@@ -143,6 +149,10 @@ __global__ void k_initial_splits(const uint64_t *__restrict__ keys, int64_t n, i
     if (cnext <= cprev) continue;
     if (cnext >= MAXD) {
       atomicExch(&cnt->too_deep, 1);
+      continue;
+    }
+    if (sorted_digits < MAXD && cnext >= sorted_digits) {
+      atomicExch(&cnt->need_full_sort, 1);
       continue;
     }
     const int cnt_here = cnext - cprev;
@@ -330,7 +340,8 @@ __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, doub
                              double *__restrict__ ymin, double *__restrict__ xmid,
                              double *__restrict__ ymid, int *__restrict__ bot,
                              int *__restrict__ top, int *__restrict__ parent,
-                             int *__restrict__ child, int *__restrict__ coll) {
+                             int *__restrict__ child, int *__restrict__ coll,
+                             int *__restrict__ nix, int *__restrict__ niy) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     const int m = level_of(off, L, g);
     const uint64_t c = code[g];
@@ -374,6 +385,8 @@ __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, doub
     // colleagues: existing same-level boxes at offsets (-1..1)^2, self included
     uint32_t ix, iy;
     morton_xy(c, m, ix, iy);
+    nix[g] = int(ix);
+    niy[g] = int(iy);
     const uint32_t side = 1u << m;
     int k = 0;
     for (int dx = -1; dx <= 1; ++dx)
@@ -391,40 +404,42 @@ __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, doub
   }
 }
 
-// far-field interaction lists of real nodes at levels >= 2: children of the
-// parent's colleagues that are not adjacent (build_interaction_list,
-// flexmm/tree.py:399-435), keeping only sources that hold points
+// offset id (0..39) of a 7x7 cell (ox+3)*7 + (oy+3); -1 for the (-1..1)^2 centre
+__constant__ int8_t c_cell_to_offset[49] = {
+    0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15, -1,
+    -1, -1, 16, 17, 18, 19, -1, -1, -1, 20, 21, 22, 23, -1, -1, -1, 24,
+    25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39};
+
+// far-field interaction lists of real nodes at levels >= 2: the children of
+// the parent's colleagues (parent excluded) that are not adjacent
+// (build_interaction_list, flexmm/tree.py:399-435), keeping only sources
+// that hold points
 __global__ void k_interactions(const int *__restrict__ off, int L, int total,
-                               const uint64_t *__restrict__ code,
-                               const uint8_t *__restrict__ flags, const int *__restrict__ bot,
-                               const int *__restrict__ top, int *__restrict__ il) {
+                               const uint8_t *__restrict__ flags, const int *__restrict__ parent,
+                               const int *__restrict__ child, const int *__restrict__ coll,
+                               const int *__restrict__ ix, const int *__restrict__ iy,
+                               const int *__restrict__ bot, const int *__restrict__ top,
+                               int *__restrict__ il) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
-    const int m = level_of(off, L, g);
     int *row = il + int64_t(g) * N_OFFSETS;
-    if (m < 2 || (flags[g] & NF_FAKE)) {
-      for (int o = 0; o < N_OFFSETS; ++o) row[o] = -1;
-      continue;
-    }
-    uint32_t ix, iy;
-    morton_xy(code[g], m, ix, iy);
-    const int64_t side = int64_t(1) << m;
-    const int64_t px = ix >> 1, py = iy >> 1;
-    int o = 0;
-    for (int a = -3; a <= 3; ++a)
-      for (int b = -3; b <= 3; ++b) {
-        if (a >= -1 && a <= 1 && b >= -1 && b <= 1) continue;
-        int found = -1;
-        const int64_t qx = int64_t(ix) + a, qy = int64_t(iy) + b;
-        if (qx >= 0 && qy >= 0 && qx < side && qy < side) {
-          const int64_t dpx = (qx >> 1) - px, dpy = (qy >> 1) - py;
-          if (dpx >= -1 && dpx <= 1 && dpy >= -1 && dpy <= 1) {
-            const uint64_t q = morton_of(uint32_t(qx), uint32_t(qy), m);
-            const int64_t e = lower_bound<uint64_t>(code, off[m], off[m + 1], q);
-            if (e < off[m + 1] && code[e] == q && top[e] > bot[e]) found = int(e);
-          }
-        }
-        row[o++] = found;
+    for (int o = 0; o < N_OFFSETS; ++o) row[o] = -1;
+    if (g < off[min(2, L)] || (flags[g] & NF_FAKE)) continue;
+    const int P = parent[g];
+    const int tx = ix[g], ty = iy[g];
+    for (int j = 0; j < 9; ++j) {
+      const int c = coll[int64_t(P) * 9 + j];
+      if (c < 0) break;
+      if (c == P) continue;
+      const int ch = child[c];
+      if (ch < 0) continue;
+      for (int k = 0; k < 4; ++k) {
+        const int cc = ch + k;
+        const int ox = ix[cc] - tx, oy = iy[cc] - ty;
+        if (ox < -3 || ox > 3 || oy < -3 || oy > 3) continue;
+        const int o = c_cell_to_offset[(ox + 3) * 7 + (oy + 3)];
+        if (o >= 0 && top[cc] > bot[cc]) row[o] = cc;
       }
+    }
   }
 }
 
@@ -435,20 +450,22 @@ uint64_t next_pow2(uint64_t v) {
 }
 
 template <class K, class V>
-void radix_sort_pairs(const K *kin, K *kout, const V *vin, V *vout, int64_t n, int end_bit,
-                      cudaStream_t s) {
+void radix_sort_pairs(const K *kin, K *kout, const V *vin, V *vout, int64_t n, int begin_bit,
+                      int end_bit, cudaStream_t s) {
   if (n <= 0) return;
   size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit, s));
+  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, begin_bit,
+                                            end_bit, s));
   DevBuf<uint8_t> tmp;
   tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, kin, kout, vin, vout, n, 0, end_bit, s));
+  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, kin, kout, vin, vout, n, begin_bit,
+                                            end_bit, s));
 }
 
 }  // namespace
 
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
-                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s) {
+                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s, int sorted_digits) {
   DevBuf<uint64_t> k0;
   DevBuf<int> i0;
   k0.alloc(n, s);
@@ -458,7 +475,8 @@ void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th
   if (n == 0) return;
   k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, k0.get(), i0.get());
   FMMB_CUDA(cudaGetLastError());
-  radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * MAXD, s);
+  const int digits = sorted_digits < 1 ? 1 : (sorted_digits > MAXD ? MAXD : sorted_digits);
+  radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * (MAXD - digits), 2 * MAXD, s);
 }
 
 size_t sort_points_scratch_bytes(int64_t n) {
@@ -498,30 +516,30 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   th.w0 = bbox[1] - bbox[0];
   FMMB_CHECK(th.w0 > 0, ERR_INVALID_ARGUMENT, "bbox has non-positive width");
 
-  // 1-2: keys and sort
-  sort_points(x, y, n, th, td.pkeys, td.ordv, s);
+  DevBuf<Counters> cnt;
+  cnt.alloc(1, s);
+  Counters hc;
+  const unsigned long long cap0 = (unsigned long long)MAXD * (n / (ppl + 1) + 1) + 64;
+  DevBuf<uint64_t> s0raw, s0;
+  s0raw.alloc(cap0, s);
+  // 1-3: keys, sort (top digits first), initial splits
+  for (int digits = SORT_DIGITS;; digits = MAXD) {
+    sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits);
+    cnt.zero(s);
+    k_initial_splits<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, s0raw.get(),
+                                                       cap0, cnt.get());
+    FMMB_CUDA(cudaGetLastError());
+    FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
+               "more than Ncutoff points share a box of width bbox/2^29 (coincident points?)");
+    FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
+    if (!hc.need_full_sort || digits == MAXD) break;
+  }
   td.sx.alloc(n, s);
   td.sy.alloc(n, s);
   k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, td.ordv.get(), n, td.sx.get(), td.sy.get());
   FMMB_CUDA(cudaGetLastError());
-
-  DevBuf<Counters> cnt;
-  cnt.alloc(1, s);
-  cnt.zero(s);
-  Counters hc;
-
-  // 3: initial splits
-  const unsigned long long cap0 = (unsigned long long)MAXD * (n / (ppl + 1) + 1) + 64;
-  DevBuf<uint64_t> s0raw, s0;
-  s0raw.alloc(cap0, s);
-  k_initial_splits<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, s0raw.get(), cap0,
-                                                     cnt.get());
-  FMMB_CUDA(cudaGetLastError());
-  FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
-  FMMB_CUDA(cudaStreamSynchronize(s));
-  FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
-             "more than Ncutoff points share a box of width bbox/2^29 (coincident points?)");
-  FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
   const int64_t n0 = (int64_t)hc.s0_count;
   const int L = (n0 > 0) ? hc.max_level + 2 : 1;
   th.L = L;
@@ -563,12 +581,12 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
       for (int m = L - 3; m >= 1; --m) {
         FMMB_CUDA(cudaMemcpyAsync(fb.get() + m, &cnt.get()->f_count, sizeof(unsigned long long),
                                   cudaMemcpyDeviceToDevice, s));
-        k_balance<<<148 * 4, TPB, 0, s>>>(m, s0.get(), s0b.get(), forced.get(), fb.get(), capf,
+        k_balance<<<64, TPB, 0, s>>>(m, s0.get(), s0b.get(), forced.get(), fb.get(), capf,
                                           tab.get(), hcap - 1, cnt.get());
         FMMB_CUDA(cudaGetLastError());
       }
       // 5: X-list leaves
-      k_xlist<<<148 * 4, TPB, 0, s>>>(s0.get(), n0, forced.get(), &cnt.get()->f_count, capf, L,
+      k_xlist<<<148, TPB, 0, s>>>(s0.get(), n0, forced.get(), &cnt.get()->f_count, capf, L,
                                       xl.get(), capx, tab.get(), hcap - 1, cnt.get());
       FMMB_CUDA(cudaGetLastError());
       FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
@@ -591,7 +609,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     // 6: sorted parent boxes and per-level bounds
     pks.alloc(np, s);
     pxs.alloc(np, s);
-    radix_sort_pairs(pk.get(), pks.get(), px.get(), pxs.get(), np, 64, s);
+    radix_sort_pairs(pk.get(), pks.get(), px.get(), pxs.get(), np, 0, 64, s);
     // pb[0..L] and the real-group bounds rgb[0..L] share one buffer: one copy back
     pb.alloc(2 * (L + 1), s);
     k_level_bounds<<<1, 64, 0, s>>>(pks.get(), np, L, pb.get());
@@ -659,6 +677,8 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   td.child.alloc(total, s);
   td.coll.alloc(int64_t(total) * 9, s);
   td.il.alloc(int64_t(total) * N_OFFSETS, s);
+  td.ix.alloc(total, s);
+  td.iy.alloc(total, s);
   k_node_codes<<<grid_for(total, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total, pks.get(),
                                                       pxs.get(), pb.get(), td.code.get(),
                                                       td.flags.get());
@@ -666,11 +686,12 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   k_node_attrs<<<grid_for(total, TPB), TPB, 0, s>>>(
       td.dev_off.get(), L, total, th.x0, th.y0, th.w0, td.pkeys.get(), n, pks.get(), pxs.get(),
       pb.get(), td.code.get(), td.flags.get(), td.xmin.get(), td.ymin.get(), td.xmid.get(),
-      td.ymid.get(), td.bot.get(), td.top.get(), td.parent.get(), td.child.get(), td.coll.get());
+      td.ymid.get(), td.bot.get(), td.top.get(), td.parent.get(), td.child.get(), td.coll.get(),
+      td.ix.get(), td.iy.get());
   FMMB_CUDA(cudaGetLastError());
-  k_interactions<<<grid_for(total, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total, td.code.get(),
-                                                        td.flags.get(), td.bot.get(), td.top.get(),
-                                                        td.il.get());
+  k_interactions<<<grid_for(total, TPB), TPB, 0, s>>>(
+      td.dev_off.get(), L, total, td.flags.get(), td.parent.get(), td.child.get(), td.coll.get(),
+      td.ix.get(), td.iy.get(), td.bot.get(), td.top.get(), td.il.get());
   FMMB_CUDA(cudaGetLastError());
 }
 

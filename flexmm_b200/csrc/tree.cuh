@@ -45,6 +45,7 @@ struct TreeDev {
   DevBuf<int> il;    // [n_total x 40] source node per offset, -1 if none
   DevBuf<int> dev_off;  // level offsets [L+1]
   DevBuf<int> rg;       // first node of every real sibling group, level-major
+  DevBuf<int> ix, iy;   // integer box coordinates at the node's level
 };
 
 struct TreeHost {
@@ -62,10 +63,12 @@ struct TreeHost {
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
                 const double bbox[4], cudaStream_t stream);
 
-// Sort arbitrary target points by the same descent key; returns sorted keys
-// and the permutation sorted -> original.
+// Sort arbitrary points by the same descent key on its top `sorted_digits`
+// quadrant digits (enough to place them in boxes of levels <= sorted_digits);
+// returns the keys in that order and the permutation sorted -> original.
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
-                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t stream);
+                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t stream,
+                 int sorted_digits = MAXD);
 
 // The same keys and sort into caller-provided memory: k0/k1 and i0/i1 are
 // ping-pong buffers of n entries, temp holds sort_points_scratch_bytes(n)
