@@ -32,7 +32,7 @@ constexpr int TN = 32;      // nodes per upward / downward tile
 constexpr int TM = 64;      // targets per M2L tile
 constexpr int NT = 256;     // threads per tile CTA
 constexpr int TCH = 128;    // targets per evaluation work item (= threads)
-constexpr int SMAX = 2048;  // sources staged per evaluation pass
+constexpr int SMAX = 1024;  // sources staged per evaluation pass
 
 __constant__ int8_t c_class_off_mx[4][27] = {
     {8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32, 34, 35, 36, 37, 38, 39},
@@ -174,9 +174,9 @@ __global__ void __launch_bounds__(NT) k_upward_mx(int m, KernelParams kp, int ne
         }
         __syncwarp();
         if (lane < neq)
-          for (int j = 0; j < nj; ++j) acc0 = fmaf(K(srcx[warp][j], srcy[warp][j], lx0, ly0), srct[warp][j], acc0);
+          for (int j = 0; j < nj; ++j) acc0 = fmaf(K(lx0 - srcx[warp][j], ly0 - srcy[warp][j]), srct[warp][j], acc0);
         if (lane + 32 < neq)
-          for (int j = 0; j < nj; ++j) acc1 = fmaf(K(srcx[warp][j], srcy[warp][j], lx1, ly1), srct[warp][j], acc1);
+          for (int j = 0; j < nj; ++j) acc1 = fmaf(K(lx1 - srcx[warp][j], ly1 - srcy[warp][j]), srct[warp][j], acc1);
         __syncwarp();
       }
       const double c0 = op.kofs * tsum[g];  // kernel offset times the box's charge, FP64
@@ -376,8 +376,7 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
                                                      const int *__restrict__ tperm, int check,
                                                      double *__restrict__ out) {
   __shared__ float Ls[64], lxs[64], lys[64];
-  __shared__ float ssx[SMAX], ssy[SMAX], stau[SMAX];
-  __shared__ int sidx[SMAX];
+  __shared__ float4 src[SMAX];  // (x, y, charge, sorted index) in width units of the leaf
   __shared__ int rb[9], rs[10];
   __shared__ double red[TCH / 32];
   __shared__ double csrc;  // charge sum of the colleagues' sources
@@ -420,14 +419,15 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
       float p0 = 0.f, p1 = 0.f;
       int k = sub;
       for (; k + G < neq; k += 2 * G) {
-        p0 = fmaf(K(lxs[k], lys[k], tx, ty), Ls[k], p0);
-        p1 = fmaf(K(lxs[k + G], lys[k + G], tx, ty), Ls[k + G], p1);
+        p0 = fmaf(K(tx - lxs[k], ty - lys[k]), Ls[k], p0);
+        p1 = fmaf(K(tx - lxs[k + G], ty - lys[k + G]), Ls[k + G], p1);
       }
-      if (k < neq) p0 = fmaf(K(lxs[k], lys[k], tx, ty), Ls[k], p0);
+      if (k < neq) p0 = fmaf(K(tx - lxs[k], ty - lys[k]), Ls[k], p0);
       acc = (double)p0 + (double)p1;
     }
     __syncthreads();
-    // P2P (flexmm/flexmm2d/helpers.py:152-194)
+    // P2P (flexmm/flexmm2d/helpers.py:152-194): branch-free FP32 sweep;
+    // pairs that coincide in FP32 contribute 0 there and are redone below
     double exact = 0.0;
     const int ns = rs[9];
     for (int base = 0; base < ns; base += SMAX) {
@@ -437,43 +437,46 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
         int c = 0;
         while (idx >= rs[c + 1]) ++c;
         const int j = rb[c] + (idx - rs[c]);
-        ssx[i] = (float)((sx[j] - cx) * iw);
-        ssy[i] = (float)((sy[j] - cy) * iw);
-        stau[i] = (float)tau[j];
-        sidx[i] = j;
+        src[i] = make_float4((float)((sx[j] - cx) * iw), (float)((sy[j] - cy) * iw), (float)tau[j],
+                             __int_as_float(j));
       }
       __syncthreads();
       if (valid) {
         float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
-        int nsum = 0;
-        int j = sub;
-        auto pair = [&](int jj) -> float {
-          const float dx = tx - ssx[jj], dy = ty - ssy[jj];
-          const float d2 = dx * dx + dy * dy;
-          if (d2 == 0.f) {
-            // coincident in FP32: decide and evaluate in FP64 on the exact
-            // coordinates (this source's kernel offset is already in csrc)
-            const int q = sidx[jj];
-            const double qx = sx[q], qy = sy[q];
-            exact -= kofs * tau[q];
-            if (!(check && x - qx == 0.0 && y - qy == 0.0)) exact += K64(qx, qy, x, y) * tau[q];
-            return 0.f;
-          }
-          return K(ssx[jj], ssy[jj], tx, ty) * stau[jj];
+        bool hit = false;
+        auto pair = [&](const float4 q) -> float {
+          const float dx = tx - q.x, dy = ty - q.y;
+          const bool z = dx * dx + dy * dy == 0.f;
+          hit |= z;
+          return z ? 0.f : K(dx, dy) * q.z;
         };
+        int j = sub, nsum = 0;
         for (; j + 3 * G < nb; j += 4 * G) {
-          p0 += pair(j);
-          p1 += pair(j + G);
-          p2 += pair(j + 2 * G);
-          p3 += pair(j + 3 * G);
+          p0 += pair(src[j]);
+          p1 += pair(src[j + G]);
+          p2 += pair(src[j + 2 * G]);
+          p3 += pair(src[j + 3 * G]);
           if (++nsum == 8) {
             acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
             p0 = p1 = p2 = p3 = 0.f;
             nsum = 0;
           }
         }
-        for (; j < nb; j += G) p0 += pair(j);
+        for (; j < nb; j += G) p0 += pair(src[j]);
         acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+        if (hit) {
+          // coincident in FP32: decide and evaluate in FP64 on the exact
+          // coordinates (the source's kernel offset is already in csrc)
+          for (int jj = sub; jj < nb; jj += G) {
+            const float4 q4 = src[jj];
+            const float dx = tx - q4.x, dy = ty - q4.y;
+            if (dx * dx + dy * dy != 0.f) continue;
+            const int q = __float_as_int(q4.w);
+            const double qx = sx[q], qy = sy[q];
+            exact -= kofs * tau[q];
+            if (!(check && x - qx == 0.0 && y - qy == 0.0)) exact += K64(qx, qy, x, y) * tau[q];
+          }
+        }
       }
       __syncthreads();
     }
@@ -493,17 +496,11 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
   }
 }
 
-// per node: FP64 sum of its charges (one warp per node)
+// per node: FP64 sum of its charges, as a difference of prefix sums
 __global__ void k_node_charge_sums(int total, const int *__restrict__ bot, const int *__restrict__ top,
-                                   const double *__restrict__ tau, double *__restrict__ tsum) {
-  const int lane = threadIdx.x & 31;
-  for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total;
-       g += (gridDim.x * blockDim.x) >> 5) {
-    double v = 0.0;
-    for (int j = bot[g] + lane; j < top[g]; j += 32) v += tau[j];
-    for (int w = 16; w >= 1; w >>= 1) v += __shfl_xor_sync(0xffffffffu, v, w);
-    if (lane == 0) tsum[g] = v;
-  }
+                                   const double *__restrict__ pre, double *__restrict__ tsum) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x)
+    tsum[g] = pre[top[g]] - pre[bot[g]];
 }
 
 template <class KF32>
@@ -533,8 +530,17 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
 
 void node_charge_sums(const PassArgs &a, const double *tau_s, double *tsum, cudaStream_t s) {
   const int total = a.th->n_total();
-  k_node_charge_sums<<<grid_for((int64_t)total * 32, 256), 256, 0, s>>>(total, a.td->bot.get(),
-                                                                        a.td->top.get(), tau_s, tsum);
+  const int64_t n = a.th->n_points;
+  DevBuf<double> pre;
+  pre.alloc(n + 1, s);
+  FMMB_CUDA(cudaMemsetAsync(pre.get(), 0, sizeof(double), s));
+  size_t bytes = 0;
+  FMMB_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, tau_s, pre.get() + 1, n, s));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(bytes, s);
+  FMMB_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), bytes, tau_s, pre.get() + 1, n, s));
+  k_node_charge_sums<<<grid_for(total, 256), 256, 0, s>>>(total, a.td->bot.get(), a.td->top.get(),
+                                                          pre.get(), tsum);
   FMMB_CUDA(cudaGetLastError());
 }
 
@@ -600,7 +606,7 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
   PhaseTimer timer(PH_EVAL, s);
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
-      k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * 8, TCH, 0, s>>>(
+      k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * 16, TCH, 0, s>>>(
           a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, tsum,
           a.ops_dev, loc32, lsum, txs, tys, tperm, check, out);

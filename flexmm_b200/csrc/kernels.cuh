@@ -40,8 +40,8 @@ struct LaplaceF32 {
   __host__ __device__ explicit LaplaceF32(const KernelParams &) {}
   // -log(d2)/(4 pi) = -(ln 2 / 4 pi) * log2(d2): one hardware log2 (MUFU) per
   // pair; on width-scaled coordinates its error is ~2e-7 of log2, ~1e-8 of K
-  __device__ __forceinline__ float operator()(float sx, float sy, float tx, float ty) const {
-    const float dx = tx - sx, dy = ty - sy;
+  // (dx, dy) = target - source
+  __device__ __forceinline__ float operator()(float dx, float dy) const {
     return __log2f(dx * dx + dy * dy) * (float)(-0.69314718055994531 / (4.0 * M_PI));
   }
   static double offset(double w, const KernelParams &) { return -std::log(w * w) / (4.0 * M_PI); }
