@@ -102,6 +102,7 @@ struct fmm_plan {
   DevBuf<float> mult32, loc32;  // mixed precision: FP32 expansions ...
   DevBuf<double> msum, lsum;    // ... and their FP64 component sums
   DevBuf<double> tsum;          // per node: FP64 sum of its charges
+  DevBuf<int> err;              // set by kernels whose bounded waits ran out
   int precision = PREC_FP64;
   bool have_expansions = false;
 };
@@ -220,12 +221,14 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
           split(v, f_m2mc_h + t2, f_m2mc_l + t2);
         }
     size_t f_m2l_h[FMM_N_OFFSETS], f_m2l_l[FMM_N_OFFSETS];
+    size_t f_tc_h[FMM_N_OFFSETS], f_tc_l[FMM_N_OFFSETS];
+    const int ntc = (np + 15) & ~15;  // tensor-core N: multiple of 16
     double c_m2l[FMM_N_OFFSETS];
     std::vector<double> dense(size_t(n) * n);
     for (int o = 0; o < FMM_N_OFFSETS; ++o) {
       const int r = lv->m2l_rank[o];
       c_m2l[o] = 0.0;
-      f_m2l_h[o] = f_m2l_l[o] = 0;
+      f_m2l_h[o] = f_m2l_l[o] = f_tc_h[o] = f_tc_l[o] = 0;
       if (r == 0) continue;
       if (r < 0) {
         for (size_t i = 0; i < size_t(n) * n; ++i) dense[i] = lv->m2l_a[o][i];
@@ -243,10 +246,14 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
       c_m2l[o] = c;
       f_m2l_h[o] = takef(size_t(np) * np);
       f_m2l_l[o] = takef(size_t(np) * np);
+      f_tc_h[o] = takef(size_t(ntc) * np);
+      f_tc_l[o] = takef(size_t(ntc) * np);
       for (int i = 0; i < n; ++i)
         for (int k = 0; k < n; ++k) {
           const size_t t = size_t(k) * np + i;  // B layout [K = source comp][N = target comp]
           split(dense[size_t(i) * n + k] - c, f_m2l_h[o] + t, f_m2l_l[o] + t);
+          const size_t u = size_t(i) * np + k;  // tcgen05 B: N x K, K-major
+          split(dense[size_t(i) * n + k] - c, f_tc_h[o] + u, f_tc_l[o] + u);
         }
     }
     auto e = std::make_unique<LevelEntry>();
@@ -266,6 +273,8 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
       for (int o = 0; o < FMM_N_OFFSETS; ++o) {
         e->dev.m2l_hi[o] = lv->m2l_rank[o] == 0 ? nullptr : fb + f_m2l_h[o];
         e->dev.m2l_lo[o] = lv->m2l_rank[o] == 0 ? nullptr : fb + f_m2l_l[o];
+        e->dev.m2l_tc_hi[o] = lv->m2l_rank[o] == 0 ? nullptr : fb + f_tc_h[o];
+        e->dev.m2l_tc_lo[o] = lv->m2l_rank[o] == 0 ? nullptr : fb + f_tc_l[o];
         e->dev.c_m2l[o] = c_m2l[o];
       }
     }
@@ -390,7 +399,9 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       p->tsum.alloc(total, s);
       node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
       run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(), s);
-      run_m2l_mixed(a, p->mult32.get(), p->msum.get(), p->ple.get(), s);
+      p->err.alloc(1, s);
+      p->err.zero(s);
+      run_m2l_mixed(a, p->mult32.get(), p->msum.get(), p->ple.get(), p->err.get(), s);
       run_downward_mixed(a, p->ple.get(), p->loc32.get(), p->lsum.get(), s);
     } else {
       p->mult.alloc(total * np, s);
@@ -434,6 +445,19 @@ int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int
     else
       run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(),
                    m, check, out, s);
+  });
+}
+
+int fmm_plan_status(fmm_plan *p) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CUDA(cudaStreamSynchronize(p->stream));
+    FMMB_CUDA(cudaGetLastError());
+    if (p->err.get()) {
+      int h = 0;
+      FMMB_CUDA(cudaMemcpy(&h, p->err.get(), sizeof(int), cudaMemcpyDeviceToHost));
+      FMMB_CHECK(h == 0, ERR_CUDA, "a tensor-core wait ran out of time; results are invalid");
+    }
   });
 }
 

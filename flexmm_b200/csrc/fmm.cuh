@@ -28,6 +28,7 @@ struct LevelOpsDev {
   const float *m2mct_hi, *m2mct_lo;     // [4NP x NP]
   const float *m2mc_hi, *m2mc_lo;       // [NP x 4NP]
   const float *m2l_hi[N_OFFSETS], *m2l_lo[N_OFFSETS];  // [NP x NP] dense (D - c)^T
+  const float *m2l_tc_hi[N_OFFSETS], *m2l_tc_lo[N_OFFSETS];  // [NT x NP] (D - c), NT = NP rounded to 16
   double c_m2m;
   double c_m2l[N_OFFSETS];
   // kernel scaling of the FP32 evaluations: coordinates are multiplied by
@@ -76,7 +77,7 @@ void node_charge_sums(const PassArgs &a, const double *tau_sorted, double *tsum,
 void run_upward_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum, float *mult32,
                       double *msum, cudaStream_t s);
 void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, double *ple,
-                   cudaStream_t s);
+                   int *err, cudaStream_t s);
 void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, double *lsum,
                         cudaStream_t s);
 void run_evaluate_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum,

@@ -21,8 +21,12 @@
 // Nequiv 24: ~4e-7 relative L2 (the FP64 path at Nequiv 24: ~2e-7).
 #include <cub/cub.cuh>
 
+#include <cstdlib>
+#include <string>
+
 #include "fmm.cuh"
 #include "gemm.cuh"
+#include "tcgen05.cuh"
 #include "timing.cuh"
 
 namespace fmmb {
@@ -282,6 +286,151 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
         o[1] = col + 1 < neq ? acc[cb][2 * h + 1] + r1s[t] : 0.0;
       }
     }
+}
+
+// ---------------------------------------------------- M2L on tcgen05 ----
+// 128 targets of one parity class per CTA (MMA M = 128), one thread per
+// target.  Per offset, the gathered source multipoles (A: 128 x K) and the
+// deflated operator (B: N x K, N = NP rounded up to 16) are staged in shared
+// memory as TF32 hi/lo pairs in the K-major core-matrix layout (8 rows x 16
+// bytes per core matrix, core matrices along K contiguous: LBO = 128 B,
+// SBO = NP/4 * 128 B) and multiplied by tcgen05.mma kind::tf32 into tensor
+// memory.  Each k-step's three split products (lo.hi, hi.lo, hi.hi) go to
+// their own 32 TMEM columns, which the epilogue adds into FP64 registers (the
+// tensor cores truncate their FP32 accumulation).  Two buffers: the MMAs of
+// one offset run while the threads stage the next and read the previous.
+constexpr int TCM = 128;       // targets per CTA = MMA M
+constexpr int TC_MAX_NP = 32;  // up to 4 k-steps x 32 TMEM columns per buffer
+constexpr int TC_COLS = 256;   // TMEM columns per CTA (2 buffers x 128)
+constexpr uint32_t TC_MAX_TRIES = 1u << 20;
+
+__global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, int np,
+                                                   const int *__restrict__ rg,
+                                                   const int *__restrict__ il,
+                                                   const LevelOpsDev *__restrict__ ops,
+                                                   const float *__restrict__ mult32,
+                                                   const double *__restrict__ msum,
+                                                   double *__restrict__ ple, int *err) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int ntc = (np + 15) & ~15;
+  const int nks = np / 8, nk4 = np / 4;
+  const uint32_t a_sz = (uint32_t(TCM) * np * 4 + 1023u) & ~1023u;
+  const uint32_t b_sz = (uint32_t(ntc) * np * 4 + 1023u) & ~1023u;
+  unsigned char *A0 = smraw;            // [buf][hi, lo] operand blocks of a_sz bytes
+  unsigned char *B0 = smraw + 4 * a_sz;  // [buf][hi, lo] operand blocks of b_sz bytes
+  const int warp = threadIdx.x >> 5;
+  int slot = 0;
+  while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= (int)blockIdx.x) ++slot;
+  const int m = slot >> 2, cls = slot & 3;
+  const int q0 = TCM * (blockIdx.x - tiles.tile_start[slot]);
+  const int nloc = min(TCM, tiles.rg_cnt[m] - q0);
+  const int tg = (int)threadIdx.x < nloc ? rg[tiles.rg_lo[m] + q0 + threadIdx.x] + cls : -1;
+  const LevelOpsDev &op = ops[m];
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_base), TC_COLS);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(tc::smem_u32(&mbar[0]), 1);
+    tc::mbar_init(tc::smem_u32(&mbar[1]), 1);
+    tc::fence_mbar_init();
+    abort_flag = 0;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = tc::idesc_tf32(TCM, ntc);
+  const uint32_t lbo = 128, sbo = uint32_t(nk4) * 128;
+  double acc[32];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+  double r1 = 0.0;
+  int issued = 0, waits0 = 0, waits1 = 0;
+  auto epilogue = [&](int b) {
+    const uint32_t parity = uint32_t(b ? waits1 : waits0) & 1u;
+    if (b) ++waits1; else ++waits0;
+    if (!tc::mbar_wait(tc::smem_u32(&mbar[b]), parity, TC_MAX_TRIES)) {
+      atomicExch(&abort_flag, 1);
+      atomicExch(err, 1);
+    }
+    tc::fence_after_sync();
+    for (int ks = 0; ks < nks; ++ks) {
+      float v[32];
+      tc::tmem_ld32(tmem + (uint32_t(32 * warp) << 16) + uint32_t(b * 128 + ks * 32), v);
+#pragma unroll
+      for (int c = 0; c < 32; ++c) acc[c] += (double)v[c];
+    }
+    tc::fence_before_sync();
+  };
+  for (int oi = 0; oi < 27; ++oi) {
+    const int o = c_class_off_mx[cls][oi];
+    if (op.kind[o] == M2L_NULL) continue;
+    const int src = tg >= 0 ? il[(size_t)tg * N_OFFSETS + o] : -1;
+    const int any = __syncthreads_or(src >= 0);
+    if (abort_flag) break;
+    if (!any) continue;
+    const int buf = issued & 1;
+    // stage A: this thread's target row, TF32 hi / lo
+    if (src >= 0) r1 += op.c_m2l[o] * msum[src];
+    {
+      const int r = threadIdx.x;
+      unsigned char *ah = A0 + (2 * buf) * a_sz, *al = A0 + (2 * buf + 1) * a_sz;
+      for (int k4 = 0; k4 < nk4; ++k4) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (src >= 0) v = *reinterpret_cast<const float4 *>(mult32 + (size_t)src * np + 4 * k4);
+        const float4 h = make_float4(__uint_as_float(to_tf32(v.x)), __uint_as_float(to_tf32(v.y)),
+                                     __uint_as_float(to_tf32(v.z)), __uint_as_float(to_tf32(v.w)));
+        const float4 l = make_float4(__uint_as_float(to_tf32(v.x - h.x)), __uint_as_float(to_tf32(v.y - h.y)),
+                                     __uint_as_float(to_tf32(v.z - h.z)), __uint_as_float(to_tf32(v.w - h.w)));
+        const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
+        *reinterpret_cast<float4 *>(ah + off) = h;
+        *reinterpret_cast<float4 *>(al + off) = l;
+      }
+    }
+    // stage B: the offset's operator, ntc rows x np, hi and lo
+    {
+      const int units = ntc * nk4;
+      for (int u = threadIdx.x; u < 2 * units; u += TCM) {
+        const int part = u >= units, uu = part ? u - units : u;
+        const int n = uu / nk4, k4 = uu % nk4;
+        const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
+        const float4 v = *reinterpret_cast<const float4 *>(bsrc + (size_t)n * np + 4 * k4);
+        const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
+        *reinterpret_cast<float4 *>(B0 + (2 * buf + part) * b_sz + off) = v;
+      }
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc::fence_after_sync();
+      for (int ks = 0; ks < nks; ++ks) {
+        const uint32_t d = tmem + uint32_t(buf * 128 + ks * 32);
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {  // lo.hi, hi.lo, hi.hi
+          const int apart = p == 0 ? 1 : 0, bpart = p == 1 ? 1 : 0;
+          const uint64_t ad = tc::desc_kmajor(tc::smem_u32(A0 + (2 * buf + apart) * a_sz) + ks * 256u, lbo, sbo);
+          const uint64_t bd = tc::desc_kmajor(tc::smem_u32(B0 + (2 * buf + bpart) * b_sz) + ks * 256u, lbo, sbo);
+          tc::mma_tf32(d, ad, bd, idesc, p > 0 ? 1u : 0u);
+        }
+      }
+      tc::commit(tc::smem_u32(&mbar[buf]));
+    }
+    if (issued >= 1) epilogue(buf ^ 1);
+    ++issued;
+  }
+  if (issued >= 1 && !abort_flag) epilogue((issued - 1) & 1);
+  if (tg >= 0) {
+    double *o = ple + (size_t)tg * np;
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+      if (c < np) o[c] = c < neq ? acc[c] + r1 : 0.0;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tmem, TC_COLS);
 }
 
 // -------------------------------------------------------------- downward ----
@@ -553,7 +702,7 @@ void run_upward_mixed(const PassArgs &a, const double *tau_s, const double *tsum
 }
 
 void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, double *ple,
-                   cudaStream_t s) {
+                   int *err, cudaStream_t s) {
   const TreeHost &th = *a.th;
   if (th.L < 3) return;
   FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
@@ -570,6 +719,37 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, d
   }
   tl.tile_start[4 * th.L] = tiles;
   if (tiles == 0) return;
+  static const bool force_sync = [] {
+    const char *e = getenv("FLEXMM_B200_M2L");
+    return e && std::string(e) == "mma_sync";
+  }();
+  if (a.np <= TC_MAX_NP && !force_sync) {
+    // tensor-memory accumulators: 256 columns per CTA, so at most 2 CTAs per
+    // SM (512 columns); the shared-memory request enforces that
+    int ctiles = 0;
+    M2LTilesMx tc{};
+    tc.n_levels = th.L;
+    for (int m = 0; m < th.L; ++m) {
+      tc.rg_lo[m] = tl.rg_lo[m];
+      tc.rg_cnt[m] = tl.rg_cnt[m];
+      for (int c = 0; c < 4; ++c) {
+        tc.tile_start[4 * m + c] = ctiles;
+        if (m >= 2) ctiles += (tc.rg_cnt[m] + TCM - 1) / TCM;
+      }
+    }
+    tc.tile_start[4 * th.L] = ctiles;
+    const size_t ntc = (a.np + 15) & ~15;
+    const size_t a_sz = (size_t(TCM) * a.np * 4 + 1023) & ~size_t(1023);
+    const size_t b_sz = (ntc * a.np * 4 + 1023) & ~size_t(1023);
+    size_t sm = 4 * a_sz + 4 * b_sz + 1024;
+    if (sm < 80 * 1024) sm = 80 * 1024;
+    FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    PhaseTimer timer(PH_M2L, s);
+    k_m2l_tc<<<ctiles, TCM, sm, s>>>(tc, a.neq, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
+                                     mult32, msum, ple, err);
+    FMMB_CUDA(cudaGetLastError());
+    return;
+  }
   const size_t sm = sizeof(float) * (size_t)TM * pad_f(a.np);
   PhaseTimer timer(PH_M2L, s);
   k_m2l_mx<<<tiles, 128, sm, s>>>(tl, a.neq, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev, mult32,

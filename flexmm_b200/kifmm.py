@@ -225,6 +225,10 @@ class KI_FMM:
         """Potential at (x, y) (flexmm/flexmm2d/fmm.py:160-161)."""
         return self._evaluate(x, y, False)
 
+    def status(self):
+        """Wait for this object's GPU work and raise if a kernel reported a failure."""
+        _lib.call("fmm_plan_status", self._plan)
+
     def direct_evaluation(self, x, y, check=False):
         """FP64 direct sum of this object's sources and charges at (x, y)
         (kernel_apply / kernel_apply_single_check, flexmm/flexmm2d/helpers.py:91-116)."""

@@ -100,6 +100,9 @@ int fmm_build_expansions(fmm_plan *plan, const double *tau, void *stream);
 int fmm_evaluate(fmm_plan *plan, const double *tx, const double *ty, int64_t m, int check,
                  double *out, void *stream);
 int fmm_plan_destroy(fmm_plan *plan);
+/* Wait for the plan's work and report failures of it: FMM_ERR_CUDA when a
+ * kernel stopped one of its bounded waits (the results are then invalid). */
+int fmm_plan_status(fmm_plan *plan);
 
 /* Copy the tree to host arrays sized by fmm_plan_info (nodes = sum n_nodes):
  * xmin, ymin [nodes]; bot, top, parent, child [nodes]; flags [nodes]

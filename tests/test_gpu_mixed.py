@@ -41,3 +41,36 @@ def test_mixed_coincident_points_are_skipped_exactly(built_lib):
     assert np.isfinite(us).all() and np.isfinite(ut).all()
     assert rel_l2(us, g["direct_src"]) < BAR
     assert rel_l2(ut, g["direct_tgt"]) < BAR
+
+
+_SYNC_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, {repo!r})
+from flexmm_b200 import KI_FMM, KI_Helper, workloads
+d = workloads.clustered(n=150_000, n_grid=200, seed=43)
+F = KI_FMM(d["x"], d["y"], "Laplace_Eval", 64, 24, bbox=d["bbox"], helper=KI_Helper(), precision="mixed")
+F.build_expansions(d["tau"])
+np.save({out!r}, F.target_evaluation(d["tx"], d["ty"]))
+"""
+
+
+def test_tcgen05_m2l_matches_warp_mma_m2l(built_lib, tmp_path):
+    """The tcgen05 M2L (default for Nequiv <= 32) and the warp-level mma.sync
+    M2L (diagnostic switch FLEXMM_B200_M2L=mma_sync) give the same far field."""
+    import os
+    import subprocess
+    import sys
+    from conftest import REPO
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    d = workloads.clustered(n=150_000, n_grid=200, seed=43)
+    F = KI_FMM(d["x"], d["y"], "Laplace_Eval", 64, 24, bbox=d["bbox"], helper=KI_Helper(),
+               precision="mixed")
+    F.build_expansions(d["tau"])
+    ut = F.target_evaluation(d["tx"], d["ty"])
+    F.status()   # no bounded wait ran out
+    out = str(tmp_path / "sync.npy")
+    env = dict(os.environ, FLEXMM_B200_M2L="mma_sync")
+    subprocess.run([sys.executable, "-c", _SYNC_SCRIPT.format(repo=REPO, out=out)], env=env,
+                   check=True, timeout=600)
+    us = np.load(out)
+    assert rel_l2(ut, us) < 1e-8
