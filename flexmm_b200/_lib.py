@@ -12,8 +12,9 @@ LIB_PATH = os.path.join(HERE, "_lib", "libflexmm_b200.so")
 
 N_OFFSETS = 40
 PRECISION = {"fp64": 0, "mixed": 1}
-N_PHASES = 8
-PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "spare"]
+N_PHASES = 12
+PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "tree_splits",
+          "tree_balance", "tree_nodes", "prep", "spare"]
 MAX_LEVELS = 30
 MAX_NEQUIV = 64
 
@@ -51,6 +52,7 @@ SIGNATURES = [
     ("fmm_plan_set_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("fmm_build_expansions", ctypes.c_int, [_vp, _vp, _vp]),
     ("fmm_evaluate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),
+    ("fmm_evaluate_sources", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     ("fmm_plan_destroy", ctypes.c_int, [_vp]),
     ("fmm_plan_status", ctypes.c_int, [_vp]),
     ("fmm_tree_export", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

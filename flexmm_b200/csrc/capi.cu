@@ -378,6 +378,7 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
     const int np = p->ops->np;
     const int64_t total = th.n_total();
+    std::unique_ptr<PhaseTimer> t_prep(new PhaseTimer(PH_PREP, s));
     p->ops_dev.alloc(th.L, s);
     PassArgs a = pass_args(p);
     FMMB_CUDA(cudaMemcpyAsync(p->ops_dev.get(), a.ops_host.data(), th.L * sizeof(LevelOpsDev),
@@ -398,6 +399,7 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       p->lsum.zero(s);
       p->tsum.alloc(total, s);
       node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
+      t_prep.reset();
       run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(), s);
       p->err.alloc(1, s);
       p->err.zero(s);
@@ -408,6 +410,7 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       p->loc.alloc(total * np, s);
       p->mult.zero(s);
       p->loc.zero(s);
+      t_prep.reset();
       run_upward(a, p->tau_s.get(), p->mult.get(), s);
       run_m2l(a, p->mult.get(), p->ple.get(), s);
       run_downward(a, p->ple.get(), p->loc.get(), s);
@@ -445,6 +448,26 @@ int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int
     else
       run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(),
                    m, check, out, s);
+  });
+}
+
+int fmm_evaluate_sources(fmm_plan *p, int check, double *out, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+    FMMB_CHECK(out, ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    PassArgs a = pass_args(p);
+    const TreeDev &td = p->td;
+    const int64_t m = p->th.n_points;
+    // the tree's sorted copy: keys sorted on at least their top L-1 digits,
+    // which is all that leaf location reads
+    if (p->precision == PREC_MIXED)
+      run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(),
+                         td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, out, s);
+    else
+      run_evaluate(a, p->tau_s.get(), p->loc.get(), td.sx.get(), td.sy.get(), td.pkeys.get(),
+                   td.ordv.get(), m, check, out, s);
   });
 }
 

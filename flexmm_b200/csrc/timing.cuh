@@ -18,7 +18,11 @@ enum Phase : int {
   PH_DOWNWARD = 4,  // k_downward launches (L2L + C2E)
   PH_EVAL = 5,      // k_evaluate launch (L2T + P2P)
   PH_DIRECT = 6,    // direct sums
-  N_PHASES = 8
+  PH_TREE_SPLITS = 7,   // tree: point keys, sort, initial splits (to the first host round trip)
+  PH_TREE_BALANCE = 8,  // tree: 2:1 closure and X-list (to the second)
+  PH_TREE_NODES = 9,    // tree: parent-box sort, node arrays, colleagues, interaction lists
+  PH_PREP = 10,         // expansions: charge gather, buffers, per-node charge sums
+  N_PHASES = 12
 };
 
 struct TimingRegistry {

@@ -26,6 +26,9 @@
 //     searches in sorted arrays.
 #include <cub/cub.cuh>
 
+#include <memory>
+
+#include "timing.cuh"
 #include "tree.cuh"
 
 namespace fmmb {
@@ -41,6 +44,9 @@ struct Counters {
   int too_deep;
   int overflow;
   int need_full_sort;
+  unsigned int bar_count;  // grid barrier of the cooperative balance kernel
+  unsigned int bar_gen;
+  int bar_timeout;
 };
 
 // The source keys are first sorted on their top SORT_DIGITS digits only; that
@@ -77,10 +83,11 @@ __device__ int hash_insert(uint64_t *tab, uint64_t mask, uint64_t key) {
   return -1;
 }
 
+// reads through L2: the table is filled by atomics from every SM
 __device__ bool hash_contains(const uint64_t *tab, uint64_t mask, uint64_t key) {
   uint64_t h = mix64(key) & mask;
   for (uint64_t probe = 0; probe <= mask; ++probe) {
-    uint64_t cur = tab[h];
+    const uint64_t cur = __ldcg(&tab[h]);
     if (cur == key) return true;
     if (cur == EMPTY_SLOT) return false;
     h = (h + 1) & mask;
@@ -137,29 +144,58 @@ __global__ void k_gather_xy(const double *__restrict__ x, const double *__restri
 }
 
 // --- 3. initially split boxes ------------------------------------------------
-// keys sorted on their top `sorted_digits` digits
-__global__ void k_initial_splits(const uint64_t *__restrict__ keys, int64_t n, int ppl,
-                                 int sorted_digits, uint64_t *__restrict__ out,
-                                 unsigned long long cap, Counters *cnt) {
+// With keys sorted on their top `sorted_digits` digits, point i starts a box
+// of every level in (cprev, cnext] that holds more than ppl points: the run
+// from i is longer than ppl iff key i and key i+ppl share that prefix.
+__device__ __forceinline__ void split_range(const uint64_t *__restrict__ keys, int64_t n, int ppl,
+                                            int64_t i, int &cprev, int &cnext) {
+  const uint64_t k = keys[i];
+  cprev = (i == 0) ? -1 : common_digits(keys[i - 1], k);
+  cnext = (i + ppl < n) ? common_digits(k, keys[i + ppl]) : -1;
+}
+
+// number of split boxes each point starts; flags trees too deep for the key
+// or for the partial sort; deepest split level
+__global__ void k_split_counts(const uint64_t *__restrict__ keys, int64_t n, int ppl,
+                               int sorted_digits, unsigned long long *__restrict__ counts,
+                               Counters *cnt) {
+  int lmax = -1;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
+    int cprev, cnext;
+    split_range(keys, n, ppl, i, cprev, cnext);
+    unsigned long long c = 0;
+    if (cnext > cprev) {
+      if (cnext >= MAXD) {
+        atomicExch(&cnt->too_deep, 1);
+      } else if (sorted_digits < MAXD && cnext >= sorted_digits) {
+        atomicExch(&cnt->need_full_sort, 1);
+      } else {
+        c = (unsigned long long)(cnext - cprev);
+        lmax = max(lmax, cnext);
+      }
+    }
+    counts[i] = c;
+  }
+  for (int o = 16; o >= 1; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+  if ((threadIdx.x & 31) == 0 && lmax >= 0) atomicMax(&cnt->max_level, lmax);
+}
+
+// writes the split boxes at their scanned positions: point-major, so every
+// level's boxes come out in increasing morton order
+__global__ void k_split_emit(const uint64_t *__restrict__ keys, int64_t n, int ppl,
+                             const unsigned long long *__restrict__ counts,
+                             const unsigned long long *__restrict__ pos, uint64_t *__restrict__ out,
+                             unsigned long long cap, Counters *cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == n - 1) cnt->s0_count = pos[i] + counts[i];
+    if (!counts[i]) continue;
+    int cprev, cnext;
+    split_range(keys, n, ppl, i, cprev, cnext);
     const uint64_t k = keys[i];
-    const int cprev = (i == 0) ? -1 : common_digits(keys[i - 1], k);
-    const int cnext = (i + ppl < n) ? common_digits(k, keys[i + ppl]) : -1;
-    if (cnext <= cprev) continue;
-    if (cnext >= MAXD) {
-      atomicExch(&cnt->too_deep, 1);
-      continue;
-    }
-    if (sorted_digits < MAXD && cnext >= sorted_digits) {
-      atomicExch(&cnt->need_full_sort, 1);
-      continue;
-    }
-    const int cnt_here = cnext - cprev;
-    unsigned long long pos = atomicAdd(&cnt->s0_count, (unsigned long long)cnt_here);
-    atomicMax(&cnt->max_level, cnext);
     for (int m = cprev + 1; m <= cnext; ++m) {
-      unsigned long long p = pos + (m - cprev - 1);
+      const unsigned long long p = pos[i] + (unsigned long long)(m - cprev - 1);
       if (p < cap)
         out[p] = box_code(m, k >> (2 * (MAXD - m)));
       else
@@ -168,120 +204,169 @@ __global__ void k_initial_splits(const uint64_t *__restrict__ keys, int64_t n, i
   }
 }
 
-__global__ void k_level_bounds(const uint64_t *__restrict__ codes, int64_t n, int L,
+// bounds[l] = first index of a code of level >= l, l = 0..L (codes sorted by level)
+__global__ void k_level_starts(const uint64_t *__restrict__ codes, int64_t n, int L,
                                int *__restrict__ bounds) {
-  int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l > L) return;
-  bounds[l] = int(lower_bound<uint64_t>(codes, 0, n, box_code(l, 0)));
-}
-
-__global__ void k_hash_insert_all(const uint64_t *__restrict__ codes, int64_t n, uint64_t *tab,
-                                  uint64_t mask, Counters *cnt) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    if (hash_insert(tab, mask, codes[i]) < 0) atomicExch(&cnt->overflow, 1);
-}
-
-// --- 4. balance closure, one level (m) per launch ------------------------------
-// S_m gains every box neighbouring the parent of a box of S_{m+1}.
-__global__ void k_balance(int m, const uint64_t *__restrict__ s0, const int *__restrict__ s0b,
-                          uint64_t *forced, const unsigned long long *__restrict__ fb,
-                          unsigned long long capf, uint64_t *tab, uint64_t mask, Counters *cnt) {
-  const int64_t a0 = s0b[m + 1], a1 = s0b[m + 2];
-  const int64_t n0 = a1 - a0;
-  // entries past the buffer capacity were never stored (overflow is flagged)
-  const int64_t f0 = (int64_t)min(fb[m + 1], capf), f1 = (int64_t)min(fb[m], capf);
-  const int64_t total = n0 + (f1 - f0);
-  const uint32_t side = 1u << m;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t c = (i < n0) ? s0[a0 + i] : forced[f0 + (i - n0)];
-    const uint64_t p = code_morton(c) >> 2;
-    uint32_t px, py;
-    morton_xy(p, m, px, py);
-    for (int dx = -1; dx <= 1; ++dx)
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int64_t qx = int64_t(px) + dx, qy = int64_t(py) + dy;
-        if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
-        const uint64_t q = box_code(m, morton_of(uint32_t(qx), uint32_t(qy), m));
-        const int r = hash_insert(tab, mask, q);
-        if (r < 0) {
-          atomicExch(&cnt->overflow, 1);
-        } else if (r == 1) {
-          unsigned long long pos = atomicAdd(&cnt->f_count, 1ULL);
-          if (pos < capf)
-            forced[pos] = q;
-          else
-            atomicExch(&cnt->overflow, 1);
-        }
-      }
+    const int lv = min(code_level(codes[i]), L + 1);
+    const int prev = (i == 0) ? -1 : min(code_level(codes[i - 1]), L + 1);
+    for (int l = prev + 1; l <= min(lv, L); ++l) bounds[l] = int(i);
+    if (i == n - 1)
+      for (int l = lv + 1; l <= L; ++l) bounds[l] = int(n);
   }
 }
 
-// --- 5. X-list leaves: real leaves (parent split, self not split) next to a split box
-__global__ void k_xlist(const uint64_t *__restrict__ s0, int64_t n0, const uint64_t *__restrict__ forced,
-                        const unsigned long long *__restrict__ fcount, unsigned long long capf,
-                        int L, uint64_t *xl, unsigned long long capx, uint64_t *tab, uint64_t mask,
-                        Counters *cnt) {
-  const int64_t total = n0 + (int64_t)min(*fcount, capf);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t c = (i < n0) ? s0[i] : forced[i - n0];
+// --- 4-5. balance closure and X-list: one cooperative launch ------------------
+// Grid-wide barrier for a cooperative launch.  Every wait is bounded: after
+// BARRIER_TRIES polls the block flags bar_timeout and every block returns.
+// The last block to arrive stores f_count to *snap (if given) before it
+// releases the others.
+constexpr unsigned int BARRIER_TRIES = 1u << 22;
+
+__device__ bool grid_sync(Counters *cnt, unsigned long long *snap) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *gen = &cnt->bar_gen;
+    const unsigned int g = *gen;
+    __threadfence();
+    int good = 1;
+    if (atomicAdd(&cnt->bar_count, 1u) == gridDim.x - 1) {
+      atomicExch(&cnt->bar_count, 0u);
+      if (snap) *snap = atomicAdd(&cnt->f_count, 0ull);
+      __threadfence();
+      atomicAdd(&cnt->bar_gen, 1u);
+    } else {
+      unsigned int tries = 0;
+      while (*gen == g) {
+        if (++tries > BARRIER_TRIES) {
+          atomicExch(&cnt->bar_timeout, 1);
+          good = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+    ok = good && !*(volatile int *)&cnt->bar_timeout;
+  }
+  __syncthreads();
+  return ok;
+}
+
+// 4: S_m gains every box neighbouring the parent of a box of S_{m+1}, for
+//    m = mtop..1, with S = S0 (sorted, bounds s0b) plus the boxes forced so
+//    far; forced[fb[m+1], fb[m]) are the boxes forced at level m+1.
+// 5: X-list leaves: real leaves (parent split, self not split) next to a
+//    split box.
+// Boxes written by other blocks are read through L2 (__ldcg).
+__global__ void __launch_bounds__(TPB) k_balance_xlist(
+    int mtop, int L, const uint64_t *__restrict__ s0, int64_t n0, const int *__restrict__ s0b,
+    uint64_t *forced, unsigned long long *fb, unsigned long long capf, uint64_t *xl,
+    unsigned long long capx, uint64_t *tab, uint64_t mask, Counters *cnt) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = tid; i < n0; i += nthr)
+    if (hash_insert(tab, mask, s0[i]) < 0) atomicExch(&cnt->overflow, 1);
+  if (!grid_sync(cnt, nullptr)) return;
+  for (int m = mtop; m >= 1; --m) {
+    const int64_t a0 = s0b[m + 1], na = s0b[m + 2] - a0;
+    const int64_t f0 = (int64_t)min(__ldcg(&fb[m + 1]), capf);
+    const int64_t f1 = (int64_t)min(__ldcg(&fb[m]), capf);
+    const int64_t work = 9 * (na + (f1 - f0));
+    const int64_t side = int64_t(1) << m;
+    for (int64_t w = tid; w < work; w += nthr) {
+      const int64_t i = w / 9;
+      const int d = int(w - 9 * i);
+      const uint64_t c = (i < na) ? s0[a0 + i] : __ldcg(&forced[f0 + (i - na)]);
+      uint32_t px, py;
+      morton_xy(code_morton(c) >> 2, m, px, py);
+      const int64_t qx = int64_t(px) + d / 3 - 1, qy = int64_t(py) + d % 3 - 1;
+      if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
+      const uint64_t q = box_code(m, morton_of(uint32_t(qx), uint32_t(qy), m));
+      const int r = hash_insert(tab, mask, q);
+      if (r < 0) {
+        atomicExch(&cnt->overflow, 1);
+      } else if (r == 1) {
+        const unsigned long long pos = atomicAdd(&cnt->f_count, 1ULL);
+        if (pos < capf)
+          forced[pos] = q;
+        else
+          atomicExch(&cnt->overflow, 1);
+      }
+    }
+    if (!grid_sync(cnt, &fb[m - 1])) return;
+  }
+  const int64_t nf = (int64_t)min(__ldcg(&fb[0]), capf);
+  const int64_t work = 8 * (n0 + nf);
+  for (int64_t w = tid; w < work; w += nthr) {
+    const int64_t i = w / 8;
+    int d = int(w - 8 * i);
+    d += (d >= 4);  // skip the centre of the 3x3 block
+    const uint64_t c = (i < n0) ? s0[i] : __ldcg(&forced[i - n0]);
     const int m = code_level(c);
     if (m < 1 || m > L - 2) continue;
     uint32_t px, py;
     morton_xy(code_morton(c), m, px, py);
-    const uint32_t side = 1u << m;
-    for (int dx = -1; dx <= 1; ++dx)
-      for (int dy = -1; dy <= 1; ++dy) {
-        if (dx == 0 && dy == 0) continue;
-        const int64_t qx = int64_t(px) + dx, qy = int64_t(py) + dy;
-        if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
-        const uint64_t qm = morton_of(uint32_t(qx), uint32_t(qy), m);
-        const uint64_t q = box_code(m, qm);
-        if (hash_contains(tab, mask, q)) continue;                        // split: not a leaf
-        if (!hash_contains(tab, mask, box_code(m - 1, qm >> 2))) continue;  // does not exist
-        const int r = hash_insert(tab, mask, q | XLIST_TAG);
-        if (r < 0) {
-          atomicExch(&cnt->overflow, 1);
-        } else if (r == 1) {
-          unsigned long long pos = atomicAdd(&cnt->x_count, 1ULL);
-          if (pos < capx)
-            xl[pos] = q;
-          else
-            atomicExch(&cnt->overflow, 1);
-        }
-      }
-  }
-}
-
-__global__ void k_concat_parents(const uint64_t *__restrict__ s0, int64_t n0,
-                                 const uint64_t *__restrict__ f, int64_t nf,
-                                 const uint64_t *__restrict__ xl, int64_t nx,
-                                 uint64_t *__restrict__ keys, uint8_t *__restrict__ isx) {
-  const int64_t total = n0 + nf + nx;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    if (i < n0) {
-      keys[i] = s0[i];
-      isx[i] = 0;
-    } else if (i < n0 + nf) {
-      keys[i] = f[i - n0];
-      isx[i] = 0;
-    } else {
-      keys[i] = xl[i - n0 - nf];
-      isx[i] = 1;
+    const int64_t side = int64_t(1) << m;
+    const int64_t qx = int64_t(px) + d / 3 - 1, qy = int64_t(py) + d % 3 - 1;
+    if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
+    const uint64_t qm = morton_of(uint32_t(qx), uint32_t(qy), m);
+    const uint64_t q = box_code(m, qm);
+    if (hash_contains(tab, mask, q)) continue;                        // split: not a leaf
+    if (!hash_contains(tab, mask, box_code(m - 1, qm >> 2))) continue;  // does not exist
+    const int r = hash_insert(tab, mask, q | XLIST_TAG);
+    if (r < 0) {
+      atomicExch(&cnt->overflow, 1);
+    } else if (r == 1) {
+      const unsigned long long pos = atomicAdd(&cnt->x_count, 1ULL);
+      if (pos < capx)
+        xl[pos] = q;
+      else
+        atomicExch(&cnt->overflow, 1);
     }
   }
 }
 
-// real sibling groups: the children of split boxes (not of X-list leaves)
-__global__ void k_real_flags(const uint8_t *__restrict__ pisx, int64_t n, int *__restrict__ real) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    real[i] = pisx[i] ? 0 : 1;
+// --- 6. parent boxes ------------------------------------------------------------
+// Parent boxes (split boxes, then X-list leaves) as compact sort keys:
+// ((level << mb) | morton) << 1 | is_xlist, mb = 2 * (deepest parent level).
+__global__ void k_parent_keys(const uint64_t *__restrict__ s0, int64_t n0,
+                              const uint64_t *__restrict__ f, int64_t nf,
+                              const uint64_t *__restrict__ xl, int64_t nx, int mb,
+                              uint64_t *__restrict__ keys) {
+  const int64_t total = n0 + nf + nx;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = (i < n0) ? s0[i] : (i < n0 + nf) ? f[i - n0] : xl[i - n0 - nf];
+    const uint64_t v = (uint64_t(code_level(c)) << mb) | code_morton(c);
+    keys[i] = (v << 1) | uint64_t(i >= n0 + nf);
+  }
 }
 
+// sorted compact keys -> box codes, X-list flags, real flags (children of
+// split boxes form real sibling groups) and level starts pb[0..L]
+__global__ void k_parent_decode(const uint64_t *__restrict__ keys, int64_t n, int mb, int L,
+                                uint64_t *__restrict__ codes, uint8_t *__restrict__ isx,
+                                int *__restrict__ real, int *__restrict__ pb) {
+  const uint64_t mmask = (uint64_t(1) << mb) - 1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const int x = int(k & 1);
+    const int lv = int((k >> 1) >> mb);
+    codes[i] = box_code(lv, (k >> 1) & mmask);
+    isx[i] = uint8_t(x);
+    real[i] = 1 - x;
+    const int prev = (i == 0) ? -1 : int((keys[i - 1] >> 1) >> mb);
+    for (int l = prev + 1; l <= min(lv, L); ++l) pb[l] = int(i);
+    if (i == n - 1)
+      for (int l = lv + 1; l <= L; ++l) pb[l] = int(n);
+  }
+}
+
+// real sibling groups: the children of split boxes (not of X-list leaves)
 __global__ void k_real_bounds(const int *__restrict__ pos, const int *__restrict__ real, int64_t n,
                               const int *__restrict__ pb, int L, int *__restrict__ rgb) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
@@ -462,6 +547,38 @@ void radix_sort_pairs(const K *kin, K *kout, const V *vin, V *vout, int64_t n, i
                                             end_bit, s));
 }
 
+template <class K>
+void sort_keys(const K *kin, K *kout, int64_t n, int begin_bit, int end_bit, cudaStream_t s) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  FMMB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, kin, kout, n, begin_bit, end_bit, s));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(bytes, s);
+  FMMB_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), bytes, kin, kout, n, begin_bit, end_bit, s));
+}
+
+template <class T>
+void exclusive_sum(const T *in, T *out, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  size_t bytes = 0;
+  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(bytes, s);
+  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s));
+}
+
+// blocks of a cooperative launch: all co-resident, at most 2 per SM
+int cooperative_grid(const void *kernel, int threads) {
+  int dev = 0, coop = 0, sms = 0, per = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  FMMB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  FMMB_CHECK(coop, ERR_UNSUPPORTED, "the device does not support cooperative launches");
+  FMMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  FMMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0));
+  FMMB_CHECK(per >= 1, ERR_CUDA, "cooperative kernel does not fit on an SM");
+  return sms * (per < 2 ? per : 2);
+}
+
 }  // namespace
 
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
@@ -521,13 +638,21 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   Counters hc;
   const unsigned long long cap0 = (unsigned long long)MAXD * (n / (ppl + 1) + 1) + 64;
   DevBuf<uint64_t> s0raw, s0;
+  DevBuf<unsigned long long> scount, spos;
   s0raw.alloc(cap0, s);
-  // 1-3: keys, sort (top digits first), initial splits
+  scount.alloc(n, s);
+  spos.alloc(n, s);
+  // 1-3: keys, sort (top digits first), initial splits in point order
+  std::unique_ptr<PhaseTimer> t_split(new PhaseTimer(PH_TREE_SPLITS, s));
   for (int digits = SORT_DIGITS;; digits = MAXD) {
     sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits);
     cnt.zero(s);
-    k_initial_splits<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, s0raw.get(),
-                                                       cap0, cnt.get());
+    k_split_counts<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, scount.get(),
+                                                     cnt.get());
+    FMMB_CUDA(cudaGetLastError());
+    exclusive_sum(scount.get(), spos.get(), n, s);
+    k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
+                                                   s0raw.get(), cap0, cnt.get());
     FMMB_CUDA(cudaGetLastError());
     FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
@@ -536,6 +661,10 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
     if (!hc.need_full_sort || digits == MAXD) break;
   }
+  scount.release();
+  spos.release();
+  t_split.reset();
+  std::unique_ptr<PhaseTimer> t_bal(new PhaseTimer(PH_TREE_BALANCE, s));
   td.sx.alloc(n, s);
   td.sy.alloc(n, s);
   k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, td.ordv.get(), n, td.sx.get(), td.sy.get());
@@ -544,26 +673,24 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   const int L = (n0 > 0) ? hc.max_level + 2 : 1;
   th.L = L;
 
-  DevBuf<uint64_t> pk, pks;  // parent boxes (unsorted, sorted)
-  DevBuf<uint8_t> px, pxs;
+  DevBuf<uint64_t> pk, pkc, pks;  // parent boxes: compact keys (unsorted, sorted), codes
+  DevBuf<uint8_t> pxs;
   DevBuf<int> pb, preal, ppos;
   std::vector<int> hpb(L + 1, 0);
   int64_t np = 0;
   if (n0 > 0) {
+    // split boxes by (level, morton): a stable sort on the level bits keeps
+    // the morton order every level already has
     s0.alloc(n0, s);
-    {
-      size_t bytes = 0;
-      FMMB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, s0raw.get(), s0.get(), n0, 0, 64, s));
-      DevBuf<uint8_t> tmp;
-      tmp.alloc(bytes, s);
-      FMMB_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), bytes, s0raw.get(), s0.get(), n0, 0, 64, s));
-    }
+    sort_keys(s0raw.get(), s0.get(), n0, LEVEL_SHIFT, LEVEL_SHIFT + 5, s);
     DevBuf<int> s0b;
     s0b.alloc(L + 2, s);
-    k_level_bounds<<<1, 64, 0, s>>>(s0.get(), n0, L + 1, s0b.get());
+    k_level_starts<<<grid_for(n0, TPB), TPB, 0, s>>>(s0.get(), n0, L + 1, s0b.get());
     FMMB_CUDA(cudaGetLastError());
 
-    // 4: balance closure with a hash set; capacities grow on overflow
+    // 4-5: balance closure and X-list in one cooperative launch over a hash
+    // set; capacities grow on overflow
+    const int mb = 2 * (L - 2);  // morton bits of the deepest parent level
     unsigned long long capf = 8ull * n0 + 4096, capx = 8ull * n0 + 4096;
     for (int attempt = 0;; ++attempt) {
       const uint64_t hcap = next_pow2(2 * (n0 + capf + capx));
@@ -576,21 +703,23 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
       fb.alloc(L + 1, s);
       fb.zero(s);
       FMMB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(Counters), s));
-      k_hash_insert_all<<<grid_for(n0, TPB), TPB, 0, s>>>(s0.get(), n0, tab.get(), hcap - 1, cnt.get());
-      FMMB_CUDA(cudaGetLastError());
-      for (int m = L - 3; m >= 1; --m) {
-        FMMB_CUDA(cudaMemcpyAsync(fb.get() + m, &cnt.get()->f_count, sizeof(unsigned long long),
-                                  cudaMemcpyDeviceToDevice, s));
-        k_balance<<<64, TPB, 0, s>>>(m, s0.get(), s0b.get(), forced.get(), fb.get(), capf,
-                                          tab.get(), hcap - 1, cnt.get());
-        FMMB_CUDA(cudaGetLastError());
+      {
+        int mtop = L - 3, Lk = L;
+        const uint64_t *s0p = s0.get();
+        const int *s0bp = s0b.get();
+        uint64_t *fp = forced.get(), *xp = xl.get(), *tp = tab.get();
+        unsigned long long *fbp = fb.get();
+        uint64_t mask = hcap - 1;
+        Counters *cp = cnt.get();
+        int64_t n0k = n0;
+        void *args[] = {&mtop, &Lk, &s0p, &n0k, &s0bp, &fp, &fbp, &capf, &xp, &capx, &tp, &mask, &cp};
+        FMMB_CUDA(cudaLaunchCooperativeKernel((const void *)k_balance_xlist,
+                                              cooperative_grid((const void *)k_balance_xlist, TPB),
+                                              TPB, args, 0, s));
       }
-      // 5: X-list leaves
-      k_xlist<<<148, TPB, 0, s>>>(s0.get(), n0, forced.get(), &cnt.get()->f_count, capf, L,
-                                      xl.get(), capx, tab.get(), hcap - 1, cnt.get());
-      FMMB_CUDA(cudaGetLastError());
       FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
       FMMB_CUDA(cudaStreamSynchronize(s));
+      FMMB_CHECK(!hc.bar_timeout, ERR_CUDA, "tree balance: a grid barrier wait ran out of time");
       if (hc.overflow) {
         FMMB_CHECK(attempt < 6, ERR_CAPACITY, "tree balance buffers overflow");
         capf = 4 * capf;
@@ -600,30 +729,25 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
       const int64_t nf = (int64_t)hc.f_count, nx = (int64_t)hc.x_count;
       np = n0 + nf + nx;
       pk.alloc(np, s);
-      px.alloc(np, s);
-      k_concat_parents<<<grid_for(np, TPB), TPB, 0, s>>>(s0.get(), n0, forced.get(), nf, xl.get(),
-                                                          nx, pk.get(), px.get());
+      k_parent_keys<<<grid_for(np, TPB), TPB, 0, s>>>(s0.get(), n0, forced.get(), nf, xl.get(), nx,
+                                                       mb, pk.get());
       FMMB_CUDA(cudaGetLastError());
       break;
     }
-    // 6: sorted parent boxes and per-level bounds
+    // 6: sorted parent boxes, per-level bounds, real sibling groups
+    t_bal.reset();
+    pkc.alloc(np, s);
+    sort_keys(pk.get(), pkc.get(), np, 0, 1 + mb + 5, s);
     pks.alloc(np, s);
     pxs.alloc(np, s);
-    radix_sort_pairs(pk.get(), pks.get(), px.get(), pxs.get(), np, 0, 64, s);
-    // pb[0..L] and the real-group bounds rgb[0..L] share one buffer: one copy back
-    pb.alloc(2 * (L + 1), s);
-    k_level_bounds<<<1, 64, 0, s>>>(pks.get(), np, L, pb.get());
-    FMMB_CUDA(cudaGetLastError());
     preal.alloc(np, s);
     ppos.alloc(np, s);
-    k_real_flags<<<grid_for(np, TPB), TPB, 0, s>>>(pxs.get(), np, preal.get());
-    {
-      size_t bytes = 0;
-      FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, preal.get(), ppos.get(), np, s));
-      DevBuf<uint8_t> tmp;
-      tmp.alloc(bytes, s);
-      FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, preal.get(), ppos.get(), np, s));
-    }
+    // pb[0..L] and the real-group bounds rgb[0..L] share one buffer: one copy back
+    pb.alloc(2 * (L + 1), s);
+    k_parent_decode<<<grid_for(np, TPB), TPB, 0, s>>>(pkc.get(), np, mb, L, pks.get(), pxs.get(),
+                                                       preal.get(), pb.get());
+    FMMB_CUDA(cudaGetLastError());
+    exclusive_sum(preal.get(), ppos.get(), np, s);
     k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1);
     FMMB_CUDA(cudaGetLastError());
     hpb.resize(2 * (L + 1));
@@ -637,6 +761,8 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     hpb.assign(2 * (L + 1), 0);
   }
 
+  t_bal.reset();
+  PhaseTimer t_nodes(PH_TREE_NODES, s);
   th.off.assign(L + 1, 0);
   th.width.assign(L, 0.0);
   th.off[0] = 0;

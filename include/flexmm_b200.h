@@ -99,6 +99,14 @@ int fmm_build_expansions(fmm_plan *plan, const double *tau, void *stream);
  * that coincide with the target (source evaluation). */
 int fmm_evaluate(fmm_plan *plan, const double *tx, const double *ty, int64_t m, int check,
                  double *out, void *stream);
+/* Potential at the plan's own source points (the coordinates given to
+ * fmm_plan_create, as the tree build copied them) into device out[n], in the
+ * caller's original source order; check != 0 skips coincident sources.
+ * Equal to fmm_evaluate(plan, x, y, n, check, out, stream) on unchanged x, y,
+ * without re-reading, re-locating and re-sorting the points: the tree already
+ * holds them sorted by leaf.  Replaces FMM.source_evaluation(x, y) called on
+ * the FMM's own sources (flexmm/flexmm2d/fmm.py:158-159, 162-176). */
+int fmm_evaluate_sources(fmm_plan *plan, int check, double *out, void *stream);
 int fmm_plan_destroy(fmm_plan *plan);
 /* Wait for the plan's work and report failures of it: FMM_ERR_CUDA when a
  * kernel stopped one of its bounded waits (the results are then invalid). */
@@ -125,8 +133,10 @@ int fmm_direct(int kernel_id, const double *kernel_params, const double *sx, con
  * fmm_timing_read returns, per phase, the summed milliseconds and the number
  * of timed launches since the last read, then clears them.  Phases:
  * 0 tree build (span), 1 target sort, 2 upward, 3 M2L, 4 downward,
- * 5 evaluation (L2T + P2P), 6 direct sum. */
-#define FMM_N_PHASES 8
+ * 5 evaluation (L2T + P2P), 6 direct sum, 7-9 the tree build's three
+ * stages (keys/sort/initial splits, 2:1 closure and X-list, node arrays),
+ * 10 expansion set-up (charge gather, buffers, charge sums). */
+#define FMM_N_PHASES 12
 int fmm_timing_enable(int on);
 int fmm_timing_read(double *ms /* [FMM_N_PHASES] */, int64_t *launches /* [FMM_N_PHASES] */);
 

@@ -127,3 +127,29 @@ def test_empty_evaluation_and_errors(built_lib):
     x = np.zeros(100)
     with pytest.raises(FMMError):
         KI_FMM(x, x, "Laplace_Eval", 16, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_own_source_evaluation_equals_general_path(built_lib, precision):
+    """source_evaluation on the FMM's own tensors runs fmm_evaluate_sources
+    (the tree's sorted copy); copies of the same points take the general path
+    (upload, locate, sort).  Both give the same potentials, and an in-place
+    change of the inputs turns the shortcut off."""
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper
+    g = load_golden("clustered_20k_q32")
+    meta = g["meta"]
+    d = golden_inputs(meta)
+    x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
+    F = KI_FMM(x, y, "Laplace_Eval", meta["ncut"], meta["neq"], bbox=d["bbox"], helper=KI_Helper(),
+               precision=precision)
+    F.build_expansions(torch.from_numpy(d["tau"]).cuda())
+    assert F._own_sources(x, y)
+    u_own = F.source_evaluation(x, y).cpu().numpy()
+    u_gen = F.source_evaluation(x.clone(), y.clone()).cpu().numpy()
+    F.status()
+    assert rel_l2(u_own, u_gen) < 1e-14
+    if precision == "fp64":
+        assert rel_l2(u_own[g["src_idx"]], g["src_val"]) < PARITY
+    x.add_(0.0)
+    assert not F._own_sources(x, y)
