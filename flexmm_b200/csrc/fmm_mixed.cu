@@ -37,6 +37,7 @@ constexpr int TM = 64;      // targets per M2L tile
 constexpr int NT = 256;     // threads per tile CTA
 constexpr int TCH = 128;    // targets per evaluation work item (= threads)
 constexpr int SMAX = 1024;  // sources staged per evaluation pass
+constexpr int EVAL_BLOCKS_PER_SM = 12;  // 40 registers, 17 KB shared memory per block
 
 __constant__ int8_t c_class_off_mx[4][27] = {
     {8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32, 34, 35, 36, 37, 38, 39},
@@ -501,91 +502,124 @@ __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int 
 }
 
 // ------------------------------------------------------------ evaluation ----
+// Per work item, everything the evaluation reads before its first source:
+// the leaf's centre, its colleagues' charge sum and source ranges.  Built by
+// one thread per item, so the evaluation kernel starts an item with a single
+// coalesced 128-byte read (prefetched during the previous item).
+struct __align__(16) EvalDesc {
+  double cx, cy, csrc;
+  int g, lev, t0, cnt;
+  int rb[9];   // first sorted source of each colleague
+  int rs[10];  // exclusive prefix of the colleagues' source counts
+  int pad[3];
+};
+static_assert(sizeof(EvalDesc) == 128, "EvalDesc is read as 32 words");
+
+__global__ void k_eval_desc(const int4 *__restrict__ items, const int *__restrict__ n_items_ptr,
+                            const int *__restrict__ coll, const int *__restrict__ bot,
+                            const int *__restrict__ top, const double *__restrict__ xmid,
+                            const double *__restrict__ ymid, const double *__restrict__ tsum,
+                            EvalDesc *__restrict__ desc) {
+  const int n_items = *n_items_ptr;
+  for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < n_items;
+       item += gridDim.x * blockDim.x) {
+    const int4 it = items[item];
+    EvalDesc d;
+    d.g = it.x;
+    d.lev = it.y;
+    d.t0 = it.z;
+    d.cnt = it.w;
+    d.cx = xmid[it.x];
+    d.cy = ymid[it.x];
+    double cs = 0.0;
+    int acc = 0;
+    d.rs[0] = 0;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const int cg = coll[(size_t)it.x * 9 + c];
+      const int b = cg >= 0 ? bot[cg] : 0, n = cg >= 0 ? top[cg] - b : 0;
+      if (cg >= 0) cs += tsum[cg];
+      d.rb[c] = b;
+      acc += n;
+      d.rs[c + 1] = acc;
+    }
+    d.csrc = cs;
+    d.pad[0] = d.pad[1] = d.pad[2] = 0;
+    desc[item] = d;
+  }
+}
+
 // P2P pairs are summed in FP32 over at most 4 x 8 terms per thread, then in
 // FP64 (cascaded summation: the FP32 rounding stays relative to short partial
 // sums); the kernel offset terms are added in FP64.
 template <class KF32, class KF64>
-__global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, int np,
-                                                     const int4 *__restrict__ items,
+__global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelParams kp, int neq, int np,
+                                                     const EvalDesc *__restrict__ desc,
                                                      const int *__restrict__ n_items_ptr,
-                                                     const int *__restrict__ coll,
-                                                     const int *__restrict__ bot,
-                                                     const int *__restrict__ top,
-                                                     const double *__restrict__ xmid,
-                                                     const double *__restrict__ ymid,
                                                      const double *__restrict__ sx,
                                                      const double *__restrict__ sy,
                                                      const double *__restrict__ tau,
-                                                     const double *__restrict__ tsum,
                                                      const LevelOpsDev *__restrict__ ops,
                                                      const float *__restrict__ loc32,
                                                      const double *__restrict__ lsum,
                                                      const double *__restrict__ txs,
                                                      const double *__restrict__ tys,
                                                      const int *__restrict__ tperm, int check,
-                                                     double *__restrict__ out) {
-  __shared__ float Ls[64], lxs[64], lys[64];
+                                                     double *__restrict__ out,
+                                                     int *__restrict__ next_item) {
+  __shared__ EvalDesc D;
   __shared__ float4 src[SMAX];  // (x, y, charge, sorted index) in width units of the leaf
-  __shared__ int rb[9], rs[10];
   __shared__ double red[TCH / 32];
-  __shared__ double csrc;  // charge sum of the colleagues' sources
+  __shared__ int s_next;
   const KF32 K(kp);
   const KF64 K64(kp);
   const int n_items = *n_items_ptr;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int4 it = items[item];
-    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
+  const int *dw = reinterpret_cast<const int *>(desc);
+  // items are handed out dynamically: the block works on `item`, holds the
+  // descriptor of `nxt` in registers and fetches the index after that
+  int item = blockIdx.x, nxt = blockIdx.x + gridDim.x;
+  int nextw = 0;
+  if (item < n_items && threadIdx.x < 32) nextw = __ldg(dw + (size_t)item * 32 + threadIdx.x);
+  while (item < n_items) {
+    if (threadIdx.x < 32) reinterpret_cast<int *>(&D)[threadIdx.x] = nextw;
+    __syncthreads();
+    if (nxt < n_items && threadIdx.x < 32) nextw = __ldg(dw + (size_t)nxt * 32 + threadIdx.x);
+    int after = 0;
+    if (threadIdx.x == 0) after = atomicAdd(next_item, 1) + 2 * gridDim.x;
+    const int g = D.g, lev = D.lev, t0 = D.t0, cnt = D.cnt, ns = D.rs[9];
     int G = 1;
     while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
     const bool valid = t < cnt;
-    const double cx = xmid[g], cy = ymid[g];
+    const double cx = D.cx, cy = D.cy;
     const double iw = ops[lev].inv_w, kofs = ops[lev].kofs;
     const double x = valid ? txs[t0 + t] : cx, y = valid ? tys[t0 + t] : cy;
     const float tx = (float)((x - cx) * iw), ty = (float)((y - cy) * iw);
-    if (threadIdx.x < 32) {
-      const int cg = threadIdx.x < 9 ? coll[(size_t)g * 9 + threadIdx.x] : -1;
-      if (threadIdx.x < 9) {
-        rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
-        rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
-      }
-      double cs = cg >= 0 ? tsum[cg] : 0.0;
-      for (int w = 16; w >= 1; w >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, w);
-      if (threadIdx.x == 0) csrc = cs;
-    }
-    if (threadIdx.x == 0) rs[0] = 0;
-    if (lev >= 2)
-      for (int k = threadIdx.x; k < neq; k += TCH) {
-        Ls[k] = loc32[(size_t)g * np + k];
-        lxs[k] = ops[lev].lx32[k];
-        lys[k] = ops[lev].ly32[k];
-      }
-    __syncthreads();
-    if (threadIdx.x == 0)
-      for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
     double acc = 0.0;
-    if (lev >= 2 && valid) {  // L2T (flexmm/flexmm2d/kifmm.py:106-120)
+    if (lev >= 2 && valid) {  // L2T (flexmm/flexmm2d/kifmm.py:106-120), operands through L1
+      const float *Lg = loc32 + (size_t)g * np;
+      const float *lx = ops[lev].lx32, *ly = ops[lev].ly32;
       float p0 = 0.f, p1 = 0.f;
       int k = sub;
       for (; k + G < neq; k += 2 * G) {
-        p0 = fmaf(K(tx - lxs[k], ty - lys[k]), Ls[k], p0);
-        p1 = fmaf(K(tx - lxs[k + G], ty - lys[k + G]), Ls[k + G], p1);
+        p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
+        p1 = fmaf(K(tx - __ldg(lx + k + G), ty - __ldg(ly + k + G)), __ldg(Lg + k + G), p1);
       }
-      if (k < neq) p0 = fmaf(K(tx - lxs[k], ty - lys[k]), Ls[k], p0);
+      if (k < neq) p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
       acc = (double)p0 + (double)p1;
     }
-    __syncthreads();
     // P2P (flexmm/flexmm2d/helpers.py:152-194): branch-free FP32 sweep;
     // pairs that coincide in FP32 contribute 0 there and are redone below
     double exact = 0.0;
-    const int ns = rs[9];
     for (int base = 0; base < ns; base += SMAX) {
       const int nb = min(SMAX, ns - base);
+      if (base > 0) __syncthreads();  // previous chunk fully read
       for (int i = threadIdx.x; i < nb; i += TCH) {
         const int idx = base + i;
         int c = 0;
-        while (idx >= rs[c + 1]) ++c;
-        const int j = rb[c] + (idx - rs[c]);
+#pragma unroll
+        for (int k = 1; k < 9; ++k) c += (idx >= D.rs[k]);
+        const int j = D.rb[c] + (idx - D.rs[c]);
         src[i] = make_float4((float)((sx[j] - cx) * iw), (float)((sy[j] - cy) * iw), (float)tau[j],
                              __int_as_float(j));
       }
@@ -627,10 +661,9 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
           }
         }
       }
-      __syncthreads();
     }
     double u = acc + exact;
-    if (sub == 0) u += kofs * (csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
+    if (sub == 0) u += kofs * (D.csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
     for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
     if (G > 32) {
       if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
@@ -641,7 +674,10 @@ __global__ void __launch_bounds__(TCH) k_evaluate_mx(KernelParams kp, int neq, i
       }
     }
     if (valid && sub == 0) out[tperm[t0 + t]] = u;
-    __syncthreads();
+    if (threadIdx.x == 0) s_next = after;
+    __syncthreads();  // D and src are rewritten by the next item
+    item = nxt;
+    nxt = s_next;
   }
 }
 
@@ -783,13 +819,21 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
   const int total = th.n_total();
   EvalItems it;
   eval_items(a, tkeys, m, it, s);
+  DevBuf<EvalDesc> desc;
+  desc.alloc(total + m / TCH + 1, s);
+  DevBuf<int> next_item;
+  next_item.alloc(1, s);
+  next_item.zero(s);
+  k_eval_desc<<<grid_for(total + m / TCH + 1, 256), 256, 0, s>>>(
+      it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+      td.ymid.get(), tsum, desc.get());
+  FMMB_CUDA(cudaGetLastError());
   PhaseTimer timer(PH_EVAL, s);
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
-      k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * 16, TCH, 0, s>>>(
-          a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
-          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, tsum,
-          a.ops_dev, loc32, lsum, txs, tys, tperm, check, out);
+      k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * EVAL_BLOCKS_PER_SM, TCH, 0, s>>>(
+          a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
+          a.ops_dev, loc32, lsum, txs, tys, tperm, check, out, next_item.get());
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
