@@ -121,50 +121,62 @@ __device__ __forceinline__ void store_mixed(const double *P, int ldp, int np, in
 }
 
 // ---------------------------------------------------------------- upward ----
+__device__ __forceinline__ int node_level(const int *__restrict__ off, int L, int g) {
+  int lo = 0, hi = L;  // largest l with off[l] <= g
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// S2M + C2E of every S2M node (leaves holding points) of every level, in one
+// launch (flexmm/flexmm2d/kifmm.py:96-105 then fmm.py:86-90).  A tile is TN
+// consecutive entries of the level-major node list; C2E runs once for each
+// level the tile holds.
 template <class KF32>
-__global__ void __launch_bounds__(NT) k_upward_mx(int m, KernelParams kp, int neq, int np, int g_begin,
-                                                  int g_end, const uint8_t *__restrict__ flags,
-                                                  const int *__restrict__ bot,
-                                                  const int *__restrict__ top,
-                                                  const int *__restrict__ child,
-                                                  const double *__restrict__ xmid,
-                                                  const double *__restrict__ ymid,
-                                                  const double *__restrict__ sx,
-                                                  const double *__restrict__ sy,
-                                                  const double *__restrict__ tau,
-                                                  const double *__restrict__ tsum,
-                                                  const LevelOpsDev *__restrict__ ops,
-                                                  float *__restrict__ mult32,
-                                                  double *__restrict__ msum) {
+__global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np, int L,
+                                               const int *__restrict__ off,
+                                               const int *__restrict__ uplist,
+                                               const int *__restrict__ n_up_ptr,
+                                               const int *__restrict__ bot,
+                                               const int *__restrict__ top,
+                                               const double *__restrict__ xmid,
+                                               const double *__restrict__ ymid,
+                                               const double *__restrict__ sx,
+                                               const double *__restrict__ sy,
+                                               const double *__restrict__ tau,
+                                               const double *__restrict__ tsum,
+                                               const LevelOpsDev *__restrict__ ops,
+                                               float *__restrict__ mult32,
+                                               double *__restrict__ msum) {
   extern __shared__ double smem[];
-  const int ldp = pad_ld(np), lda = pad_f(4 * np);
-  double *P = smem;                                   // [TN][ldp] check potentials
-  double *T = P + TN * ldp;                           // [TN][ldp] C2E scratch
-  float *A = reinterpret_cast<float *>(T + TN * ldp); // [TN][lda] children multipoles (FP32)
+  const int ldp = pad_ld(np);
+  double *P = smem;          // [TN][ldp] check potentials
+  double *T = P + TN * ldp;  // [TN][ldp] C2E scratch
   __shared__ float srcx[NT / 32][32], srcy[NT / 32][32], srct[NT / 32][32];
-  __shared__ double csum[TN];
-  __shared__ int node[TN];
+  __shared__ int node[TN], nlev[TN];
   __shared__ double *orow[TN];
   const KF32 K(kp);
-  const LevelOpsDev &op = ops[m];
-  const int g0 = g_begin + blockIdx.x * TN;
-  const int nloc = min(TN, g_end - g0);
-  for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = T[i] = 0.0;
-  for (int i = threadIdx.x; i < TN * lda; i += NT) A[i] = 0.f;
-  if (threadIdx.x < TN) {
-    csum[threadIdx.x] = 0.0;
-    node[threadIdx.x] = (int)threadIdx.x < nloc ? g0 + (int)threadIdx.x : -1;
-    orow[threadIdx.x] = P + threadIdx.x * ldp;
-  }
-  __syncthreads();
+  const int n_up = *n_up_ptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // S2M in FP32 (flexmm/flexmm2d/kifmm.py:96-105) / gather children (M2M)
-  for (int t = warp; t < nloc; t += NT / 32) {
-    const int g = g0 + t;
-    const uint8_t f = flags[g];
-    const int b = bot[g], e = top[g];
-    const bool up = (((f & NF_LEAF) && !(f & NF_XLIST)) || (f & NF_FAKE)) && e > b;
-    if (up) {
+  for (int i = threadIdx.x; i < TN * ldp; i += NT) T[i] = 0.0;
+  for (int tile = blockIdx.x; tile * TN < n_up; tile += gridDim.x) {
+    const int i0 = tile * TN, nloc = min(TN, n_up - i0);
+    for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = 0.0;
+    if (threadIdx.x < TN) {
+      const int g = (int)threadIdx.x < nloc ? uplist[i0 + threadIdx.x] : -1;
+      node[threadIdx.x] = g;
+      nlev[threadIdx.x] = g >= 0 ? node_level(off, L, g) : -1;
+    }
+    __syncthreads();
+    for (int t = warp; t < nloc; t += NT / 32) {
+      const int g = node[t];
+      const LevelOpsDev &op = ops[nlev[t]];
+      const int b = bot[g], e = top[g];
       const double cx = xmid[g], cy = ymid[g], iw = op.inv_w;
       float acc0 = 0.f, acc1 = 0.f;
       const float lx0 = lane < neq ? op.lx32[lane] : 0.f, ly0 = lane < neq ? op.ly32[lane] : 0.f;
@@ -187,16 +199,55 @@ __global__ void __launch_bounds__(NT) k_upward_mx(int m, KernelParams kp, int ne
       const double c0 = op.kofs * tsum[g];  // kernel offset times the box's charge, FP64
       if (lane < neq) P[t * ldp + lane] = c0 + (double)acc0;
       if (lane + 32 < neq) P[t * ldp + lane + 32] = c0 + (double)acc1;
-    } else if (f & NF_CHILDREN) {
-      const int c0 = child[g];
-      const float *src = mult32 + (size_t)c0 * np;
-      for (int qd = lane; qd < 4 * np; qd += 32) A[t * lda + qd] = src[qd];
-      if (lane == 0) csum[t] = msum[c0] + msum[c0 + 1] + msum[c0 + 2] + msum[c0 + 3];
     }
+    const int mlo = nlev[0], mhi = nlev[nloc - 1];
+    for (int m = mlo; m <= mhi; ++m) {
+      __syncthreads();
+      if (threadIdx.x < TN) orow[threadIdx.x] = nlev[threadIdx.x] == m ? P + threadIdx.x * ldp : nullptr;
+      __syncthreads();
+      c2e_tile(ops[m], np, P, T, orow);
+    }
+    __syncthreads();
+    store_mixed(P, ldp, np, neq, node, TN, mult32, msum);
+    __syncthreads();
+  }
+}
+
+// M2M + C2E of the parent boxes of level m (flexmm/flexmm2d/fmm.py:91-98):
+// TN parent groups per tile; their children are the contiguous node rows
+// c_first + 4e .. c_first + 4e + 3 of level m+1.
+// P[t] = (M2MC - c) . children + c * sum(children)
+__global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_first, int n_groups,
+                                               const int *__restrict__ parent,
+                                               const LevelOpsDev *__restrict__ ops, float *mult32,
+                                               double *msum) {
+  extern __shared__ double smem[];
+  const int ldp = pad_ld(np), lda = pad_f(4 * np);
+  double *P = smem;                                    // [TN][ldp] check potentials
+  double *T = P + TN * ldp;                            // [TN][ldp] C2E scratch
+  float *A = reinterpret_cast<float *>(T + TN * ldp);  // [TN][lda] children multipoles (FP32)
+  __shared__ double csum[TN];
+  __shared__ int node[TN];
+  __shared__ double *orow[TN];
+  const LevelOpsDev &op = ops[m];
+  const int e0 = blockIdx.x * TN, nloc = min(TN, n_groups - e0);
+  const float *Ag = mult32 + (size_t)(c_first + 4 * e0) * np;
+  const int rowlen = 4 * np;
+  for (int i = threadIdx.x; i < TN * rowlen; i += NT) {
+    const int t = i / rowlen, k = i - t * rowlen;
+    A[t * lda + k] = t < nloc ? Ag[i] : 0.f;
+  }
+  for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = T[i] = 0.0;
+  if (threadIdx.x < TN) {
+    const int t = threadIdx.x;
+    const int c0 = c_first + 4 * (e0 + t);
+    node[t] = t < nloc ? parent[c0] : -1;
+    csum[t] = t < nloc ? (msum[c0] + msum[c0 + 1]) + (msum[c0 + 2] + msum[c0 + 3]) : 0.0;
+    orow[t] = P + t * ldp;
   }
   __syncthreads();
-  // M2M: P[t] = (M2MC - c) . children + c * sum(children)   (flexmm/flexmm2d/fmm.py:93-96)
   {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const int r0 = 16 * (warp & 1), n0 = 8 * (warp >> 1);
     double acc[2][4] = {};
@@ -206,7 +257,7 @@ __global__ void __launch_bounds__(NT) k_upward_mx(int m, KernelParams kp, int ne
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int t = r0 + g + 8 * h, col = n0 + 32 * cb + 2 * q;
-        if (t < nloc && col < np && (flags[g0 + t] & NF_CHILDREN)) {
+        if (t < nloc && col < np) {
           const double r1 = op.c_m2m * csum[t];
           if (col < neq) P[t * ldp + col] = acc[cb][2 * h] + r1;
           if (col + 1 < neq) P[t * ldp + col + 1] = acc[cb][2 * h + 1] + r1;
@@ -608,8 +659,11 @@ __global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelP
       if (k < neq) p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
       acc = (double)p0 + (double)p1;
     }
-    // P2P (flexmm/flexmm2d/helpers.py:152-194): branch-free FP32 sweep;
-    // pairs that coincide in FP32 contribute 0 there and are redone below
+    // P2P (flexmm/flexmm2d/helpers.py:152-194): branch-free FP32 sweep with
+    // the kernel's scale folded into the staged charges.  A pair closer than
+    // FLT_MIN in squared width units (coincident in FP32) contributes 0 there
+    // and is redone in FP64 on the exact coordinates: the one such pair a
+    // thread meets (a source evaluated at itself) directly, more by a rescan.
     double exact = 0.0;
     for (int base = 0; base < ns; base += SMAX) {
       const int nb = min(SMAX, ns - base);
@@ -620,44 +674,53 @@ __global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelP
 #pragma unroll
         for (int k = 1; k < 9; ++k) c += (idx >= D.rs[k]);
         const int j = D.rb[c] + (idx - D.rs[c]);
-        src[i] = make_float4((float)((sx[j] - cx) * iw), (float)((sy[j] - cy) * iw), (float)tau[j],
-                             __int_as_float(j));
+        src[i] = make_float4((float)((sx[j] - cx) * iw), (float)((sy[j] - cy) * iw),
+                             (float)tau[j] * KF32::kScale, __int_as_float(j));
       }
       __syncthreads();
       if (valid) {
         float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
-        bool hit = false;
-        auto pair = [&](const float4 q) -> float {
+        int nhit = 0, hj = 0;
+        auto pair = [&](const float4 q, int jj, float &p) {
           const float dx = tx - q.x, dy = ty - q.y;
-          const bool z = dx * dx + dy * dy == 0.f;
-          hit |= z;
-          return z ? 0.f : K(dx, dy) * q.z;
+          const float d2 = fmaf(dy, dy, dx * dx);
+          const bool z = d2 < 1.17549435e-38f;  // FLT_MIN
+          nhit += z;
+          hj = z ? jj : hj;
+          const float v = K.radial(d2);
+          p = fmaf(z ? 0.f : v, q.z, p);
         };
         int j = sub, nsum = 0;
         for (; j + 3 * G < nb; j += 4 * G) {
-          p0 += pair(src[j]);
-          p1 += pair(src[j + G]);
-          p2 += pair(src[j + 2 * G]);
-          p3 += pair(src[j + 3 * G]);
+          pair(src[j], j, p0);
+          pair(src[j + G], j + G, p1);
+          pair(src[j + 2 * G], j + 2 * G, p2);
+          pair(src[j + 3 * G], j + 3 * G, p3);
           if (++nsum == 8) {
             acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
             p0 = p1 = p2 = p3 = 0.f;
             nsum = 0;
           }
         }
-        for (; j < nb; j += G) p0 += pair(src[j]);
+        for (; j < nb; j += G) pair(src[j], j, p0);
         acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
-        if (hit) {
-          // coincident in FP32: decide and evaluate in FP64 on the exact
-          // coordinates (the source's kernel offset is already in csrc)
-          for (int jj = sub; jj < nb; jj += G) {
-            const float4 q4 = src[jj];
-            const float dx = tx - q4.x, dy = ty - q4.y;
-            if (dx * dx + dy * dy != 0.f) continue;
-            const int q = __float_as_int(q4.w);
+        if (nhit) {
+          // the source's kernel offset is already in csrc: take it out and
+          // add the FP64 kernel unless the points coincide exactly (check)
+          auto fix = [&](int jj) {
+            const int q = __float_as_int(src[jj].w);
             const double qx = sx[q], qy = sy[q];
             exact -= kofs * tau[q];
             if (!(check && x - qx == 0.0 && y - qy == 0.0)) exact += K64(qx, qy, x, y) * tau[q];
+          };
+          if (nhit == 1) {
+            fix(hj);
+          } else {
+            for (int jj = sub; jj < nb; jj += G) {
+              const float4 q4 = src[jj];
+              const float dx = tx - q4.x, dy = ty - q4.y;
+              if (fmaf(dy, dy, dx * dx) < 1.17549435e-38f) fix(jj);
+            }
           }
         }
       }
@@ -694,19 +757,25 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int np = a.np;
-  auto bytes = [](int n) {
-    return sizeof(double) * (size_t)TN * pad_ld(n) * 2 + sizeof(float) * (size_t)TN * pad_f(4 * n);
-  };
-  FMMB_CUDA(cudaFuncSetAttribute(k_upward_mx<KF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(bytes(64))));
-  for (int m = th.L - 1; m >= 2; --m) {
-    const int gb = th.off[m], ge = th.off[m + 1];
-    const int tiles = (ge - gb + TN - 1) / TN;
-    PhaseTimer timer(PH_UPWARD, s);
-    k_upward_mx<KF32><<<tiles, NT, bytes(np), s>>>(m, a.kp, a.neq, np, gb, ge, td.flags.get(),
-                                                   td.bot.get(), td.top.get(), td.child.get(),
-                                                   td.xmid.get(), td.ymid.get(), td.sx.get(),
-                                                   td.sy.get(), tau_s, tsum, a.ops_dev, mult32, msum);
+  if (th.L < 3) return;
+  const size_t pbytes = sizeof(double) * (size_t)TN * pad_ld(np) * 2;
+  const size_t abytes = pbytes + sizeof(float) * (size_t)TN * pad_f(4 * np);
+  PhaseTimer timer(PH_UPWARD, s);
+  k_s2m_mx<KF32><<<148 * 4, NT, pbytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
+                                              td.uplist.get(), td.n_up.get(), td.bot.get(),
+                                              td.top.get(), td.xmid.get(), td.ymid.get(),
+                                              td.sx.get(), td.sy.get(), tau_s, tsum, a.ops_dev,
+                                              mult32, msum);
+  FMMB_CUDA(cudaGetLastError());
+  FMMB_CUDA(cudaFuncSetAttribute(k_m2m_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(double) * (size_t)TN * pad_ld(64) * 2 +
+                                     sizeof(float) * (size_t)TN * pad_f(4 * 64))));
+  for (int m = th.L - 2; m >= 2; --m) {
+    const int c_first = th.off[m + 1];
+    const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
+    if (n_groups == 0) continue;
+    k_m2m_mx<<<(n_groups + TN - 1) / TN, NT, abytes, s>>>(m, a.neq, np, c_first, n_groups,
+                                                         td.parent.get(), a.ops_dev, mult32, msum);
     FMMB_CUDA(cudaGetLastError());
   }
 }

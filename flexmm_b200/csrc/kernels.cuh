@@ -29,21 +29,36 @@ struct LaplaceF64 {
   }
 };
 
+// log2 on the special-function unit, denormal inputs flushed to zero
+// (lg2.approx.ftz.f32: relative error ~2^-22 on normal inputs).
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // FP32 evaluation for the mixed-precision passes.  The log kernel is scale
 // invariant up to a constant, K(w r) = offset(w) + K(r) with offset(w) =
 // -log(w^2)/(4 pi): the mixed passes evaluate K in FP32 on coordinates divided
 // by the box width (O(1) arguments, so FP32 keeps the kernel's variation to
 // ~1e-7 absolute) and add offset(w) times the charge sum in FP64.  Kernels
 // without such a decomposition set kScaled = false and offset() = 0.
+//
+// Radial form used by the P2P loop: K(dx, dy) = kScale * radial(dx^2 + dy^2),
+// with kScale folded into the staged charges.  radial() is only called on
+// squared distances >= FLT_MIN (smaller ones are coincident pairs, handled
+// apart in FP64).
 struct LaplaceF32 {
   static constexpr bool kScaled = true;
+  static constexpr float kScale = (float)(-0.69314718055994531 / (4.0 * M_PI));  // -ln2 / (4 pi)
   __host__ __device__ explicit LaplaceF32(const KernelParams &) {}
-  // -log(d2)/(4 pi) = -(ln 2 / 4 pi) * log2(d2): one hardware log2 (MUFU) per
-  // pair; on width-scaled coordinates its error is ~2e-7 of log2, ~1e-8 of K
+  // -log(d2)/(4 pi) = -(ln 2 / 4 pi) * log2(d2); on width-scaled coordinates
+  // the hardware log2's error is ~2e-7 of log2, ~1e-8 of K
   // (dx, dy) = target - source
   __device__ __forceinline__ float operator()(float dx, float dy) const {
-    return __log2f(dx * dx + dy * dy) * (float)(-0.69314718055994531 / (4.0 * M_PI));
+    return lg2_ftz(dx * dx + dy * dy) * kScale;
   }
+  __device__ __forceinline__ float radial(float d2) const { return lg2_ftz(d2); }
   static double offset(double w, const KernelParams &) { return -std::log(w * w) / (4.0 * M_PI); }
 };
 

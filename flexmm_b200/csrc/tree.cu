@@ -528,6 +528,25 @@ __global__ void k_interactions(const int *__restrict__ off, int L, int total,
   }
 }
 
+// S2M nodes: see TreeDev::uplist
+__global__ void k_up_flags(int g0, int total, const uint8_t *__restrict__ flags,
+                           const int *__restrict__ bot, const int *__restrict__ top,
+                           int *__restrict__ f) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const uint8_t fl = flags[g];
+    const bool up = (((fl & NF_LEAF) && !(fl & NF_XLIST)) || (fl & NF_FAKE)) && top[g] > bot[g];
+    f[g] = (g >= g0 && up) ? 1 : 0;
+  }
+}
+
+__global__ void k_up_scatter(int total, const int *__restrict__ f, const int *__restrict__ pos,
+                             int *__restrict__ list, int *__restrict__ count) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    if (f[g]) list[pos[g]] = g;
+    if (g == total - 1) *count = pos[g] + f[g];
+  }
+}
+
 uint64_t next_pow2(uint64_t v) {
   uint64_t p = 1;
   while (p < v) p <<= 1;
@@ -819,6 +838,22 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
       td.dev_off.get(), L, total, td.flags.get(), td.parent.get(), td.child.get(), td.coll.get(),
       td.ix.get(), td.iy.get(), td.bot.get(), td.top.get(), td.il.get());
   FMMB_CUDA(cudaGetLastError());
+  // S2M node list
+  {
+    DevBuf<int> f, pos;
+    f.alloc(total, s);
+    pos.alloc(total, s);
+    td.uplist.alloc(total, s);
+    td.n_up.alloc(1, s);
+    const int g0 = L > 2 ? th.off[2] : total;
+    k_up_flags<<<grid_for(total, TPB), TPB, 0, s>>>(g0, total, td.flags.get(), td.bot.get(),
+                                                     td.top.get(), f.get());
+    FMMB_CUDA(cudaGetLastError());
+    exclusive_sum(f.get(), pos.get(), total, s);
+    k_up_scatter<<<grid_for(total, TPB), TPB, 0, s>>>(total, f.get(), pos.get(), td.uplist.get(),
+                                                       td.n_up.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
 }
 
 }  // namespace fmmb

@@ -46,6 +46,10 @@ struct TreeDev {
   DevBuf<int> dev_off;  // level offsets [L+1]
   DevBuf<int> rg;       // first node of every real sibling group, level-major
   DevBuf<int> ix, iy;   // integer box coordinates at the node's level
+  // nodes at levels >= 2 whose multipoles come from their own points (S2M):
+  // real leaves that are not X-list leaves, and fake leaves, holding points;
+  // in node order (so level-major).  Count on the device.
+  DevBuf<int> uplist, n_up;
 };
 
 struct TreeHost {
