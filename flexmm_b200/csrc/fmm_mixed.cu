@@ -63,13 +63,14 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 
 // 3xTF32 warp tile: C[r0 + g (+8)][n0 + 8*cb*nstride + 2q (+1)] += A . B for the
 // column blocks below ncols.  A: shared float [.][lda] (split to hi/lo here);
-// B: global hi/lo float [K][ldb] (pre-split).  K multiple of 8.
+// B: hi/lo float [K][ldb] (pre-split), in global memory or, with SB, staged
+// in shared memory.  K multiple of 8.
 // The tensor cores' FP32 accumulation does not round to nearest (it behaves
 // like truncation, which biases long sums), so every k-step's three products
 // go into a fresh zero fragment and the partial sums are accumulated in FP64.
-template <int CB>
-__device__ __forceinline__ void warp_gemm_x3(const float *A, int lda, const float *__restrict__ Bh,
-                                             const float *__restrict__ Bl, int ldb, int K, int r0,
+template <int CB, bool SB = false>
+__device__ __forceinline__ void warp_gemm_x3(const float *A, int lda, const float *Bh,
+                                             const float *Bl, int ldb, int K, int r0,
                                              int n0, int nstride, int ncols, double (&acc)[CB][4]) {
   const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
   for (int k0 = 0; k0 < K; k0 += 8) {
@@ -86,8 +87,10 @@ __device__ __forceinline__ void warp_gemm_x3(const float *A, int lda, const floa
       const int n = n0 + 8 * cb * nstride;
       if (n < ncols) {
         const size_t i0 = (size_t)(k0 + q) * ldb + n + g, i1 = i0 + (size_t)4 * ldb;
-        const uint32_t bh0 = __float_as_uint(__ldg(Bh + i0)), bh1 = __float_as_uint(__ldg(Bh + i1));
-        const uint32_t bl0 = __float_as_uint(__ldg(Bl + i0)), bl1 = __float_as_uint(__ldg(Bl + i1));
+        const uint32_t bh0 = __float_as_uint(SB ? Bh[i0] : __ldg(Bh + i0));
+        const uint32_t bh1 = __float_as_uint(SB ? Bh[i1] : __ldg(Bh + i1));
+        const uint32_t bl0 = __float_as_uint(SB ? Bl[i0] : __ldg(Bl + i0));
+        const uint32_t bl1 = __float_as_uint(SB ? Bl[i1] : __ldg(Bl + i1));
         float part[4] = {0.f, 0.f, 0.f, 0.f};
         mma_tf32(part, al, bh0, bh1);
         mma_tf32(part, ah, bl0, bl1);
@@ -157,6 +160,7 @@ __global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np,
   const int ldp = pad_ld(np);
   double *P = smem;          // [TN][ldp] check potentials
   double *T = P + TN * ldp;  // [TN][ldp] C2E scratch
+  double *Cs = T + TN * ldp;  // staged C2E operators of one level
   __shared__ float srcx[NT / 32][32], srcy[NT / 32][32], srct[NT / 32][32];
   __shared__ int node[TN], nlev[TN];
   __shared__ double *orow[TN];
@@ -173,6 +177,8 @@ __global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np,
       nlev[threadIdx.x] = g >= 0 ? node_level(off, L, g) : -1;
     }
     __syncthreads();
+    const int mlo = nlev[0], mhi = nlev[nloc - 1];
+    C2EView cv = c2e_stage(ops[mlo], np, Cs);  // in flight during S2M
     for (int t = warp; t < nloc; t += NT / 32) {
       const int g = node[t];
       const LevelOpsDev &op = ops[nlev[t]];
@@ -200,12 +206,13 @@ __global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np,
       if (lane < neq) P[t * ldp + lane] = c0 + (double)acc0;
       if (lane + 32 < neq) P[t * ldp + lane + 32] = c0 + (double)acc1;
     }
-    const int mlo = nlev[0], mhi = nlev[nloc - 1];
     for (int m = mlo; m <= mhi; ++m) {
       __syncthreads();
+      if (m > mlo) cv = c2e_stage(ops[m], np, Cs);
       if (threadIdx.x < TN) orow[threadIdx.x] = nlev[threadIdx.x] == m ? P + threadIdx.x * ldp : nullptr;
+      cp_async_wait_all();
       __syncthreads();
-      c2e_tile(ops[m], np, P, T, orow);
+      c2e_tile<true>(cv, np, P, T, orow);
     }
     __syncthreads();
     store_mixed(P, ldp, np, neq, node, TN, mult32, msum);
@@ -217,25 +224,35 @@ __global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np,
 // TN parent groups per tile; their children are the contiguous node rows
 // c_first + 4e .. c_first + 4e + 3 of level m+1.
 // P[t] = (M2MC - c) . children + c * sum(children)
+template <bool kStageB>
 __global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_first, int n_groups,
                                                const int *__restrict__ parent,
                                                const LevelOpsDev *__restrict__ ops, float *mult32,
                                                double *msum) {
   extern __shared__ double smem[];
-  const int ldp = pad_ld(np), lda = pad_f(4 * np);
+  const int ldp = pad_ld(np), lda = pad_f(4 * np), ldb = ldb_f(np);
   double *P = smem;                                    // [TN][ldp] check potentials
   double *T = P + TN * ldp;                            // [TN][ldp] C2E scratch
-  float *A = reinterpret_cast<float *>(T + TN * ldp);  // [TN][lda] children multipoles (FP32)
+  double *Cs = T + TN * ldp;                           // staged C2E operators
+  float *A = reinterpret_cast<float *>(Cs + c2e_stage_doubles(np));  // [TN][lda] children (FP32)
+  float *Bh = A + TN * lda, *Bl = Bh + 4 * np * ldb;  // staged (M2MC - c)^T hi / lo [4np][ldb]
   __shared__ double csum[TN];
   __shared__ int node[TN];
   __shared__ double *orow[TN];
   const LevelOpsDev &op = ops[m];
   const int e0 = blockIdx.x * TN, nloc = min(TN, n_groups - e0);
+  // operators and the tile's children multipoles (contiguous rows) in flight together
+  const C2EView cv = c2e_stage(op, np, Cs);
+  if (kStageB) {
+    stage_rows(Bh, ldb, op.m2mct_hi, 4 * np, np);
+    stage_rows(Bl, ldb, op.m2mct_lo, 4 * np, np);
+  }
   const float *Ag = mult32 + (size_t)(c_first + 4 * e0) * np;
+  stage_rows(A, lda, Ag, nloc, 4 * np);
   const int rowlen = 4 * np;
-  for (int i = threadIdx.x; i < TN * rowlen; i += NT) {
+  for (int i = threadIdx.x + nloc * rowlen; i < TN * rowlen; i += NT) {
     const int t = i / rowlen, k = i - t * rowlen;
-    A[t * lda + k] = t < nloc ? Ag[i] : 0.f;
+    A[t * lda + k] = 0.f;
   }
   for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = T[i] = 0.0;
   if (threadIdx.x < TN) {
@@ -245,13 +262,17 @@ __global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_fir
     csum[t] = t < nloc ? (msum[c0] + msum[c0 + 1]) + (msum[c0 + 2] + msum[c0 + 3]) : 0.0;
     orow[t] = P + t * ldp;
   }
+  cp_async_wait_all();
   __syncthreads();
   {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const int r0 = 16 * (warp & 1), n0 = 8 * (warp >> 1);
     double acc[2][4] = {};
-    warp_gemm_x3<2>(A, lda, op.m2mct_hi, op.m2mct_lo, np, 4 * np, r0, n0, 4, np, acc);
+    if (kStageB)
+      warp_gemm_x3<2, true>(A, lda, Bh, Bl, ldb, 4 * np, r0, n0, 4, np, acc);
+    else
+      warp_gemm_x3<2, false>(A, lda, op.m2mct_hi, op.m2mct_lo, np, 4 * np, r0, n0, 4, np, acc);
 #pragma unroll
     for (int cb = 0; cb < 2; ++cb)
 #pragma unroll
@@ -265,9 +286,23 @@ __global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_fir
       }
   }
   __syncthreads();
-  c2e_tile(op, np, P, T, orow);
+  c2e_tile<true>(cv, np, P, T, orow);
   __syncthreads();
   store_mixed(P, ldp, np, neq, node, TN, mult32, msum);
+}
+
+// shared memory of k_m2m_mx
+size_t m2m_mx_smem(int np, bool stage_b) {
+  return sizeof(double) * ((size_t)2 * TN * pad_ld(np) + c2e_stage_doubles(np)) +
+         sizeof(float) * ((size_t)TN * pad_f(4 * np) + (stage_b ? (size_t)2 * 4 * np * ldb_f(np) : 0));
+}
+
+// largest dynamic shared memory a block may request on this device
+size_t smem_optin() {
+  int dev = 0, v = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  FMMB_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  return size_t(v);
 }
 
 // ------------------------------------------------------------------- M2L ----
@@ -366,7 +401,10 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
-  __shared__ int abort_flag;
+  __shared__ int s_src[27][TCM];  // source node per class offset and target
+  __shared__ int s_act[27];       // offsets with work, in class order
+  __shared__ int s_nact;
+  __shared__ unsigned int s_mask;
   const int ntc = (np + 15) & ~15;
   const int nks = np / 8, nk4 = np / 4;
   const uint32_t a_sz = (uint32_t(TCM) * np * 4 + 1023u) & ~1023u;
@@ -386,7 +424,7 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
     tc::mbar_init(tc::smem_u32(&mbar[0]), 1);
     tc::mbar_init(tc::smem_u32(&mbar[1]), 1);
     tc::fence_mbar_init();
-    abort_flag = 0;
+    s_mask = 0u;
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -394,16 +432,38 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = tc::idesc_tf32(TCM, ntc);
   const uint32_t lbo = 128, sbo = uint32_t(nk4) * 128;
+  // the class's offsets that have an operator and a source for some target
+  // of the tile, and every target's source per offset
+  {
+    unsigned int mask = 0;
+    for (int oi = 0; oi < 27; ++oi) {
+      const int o = c_class_off_mx[cls][oi];
+      const int sidx = (tg >= 0 && op.kind[o] != M2L_NULL) ? il[(size_t)tg * N_OFFSETS + o] : -1;
+      s_src[oi][threadIdx.x] = sidx;
+      if (sidx >= 0) mask |= 1u << oi;
+    }
+    mask = __reduce_or_sync(0xffffffffu, mask);
+    if ((threadIdx.x & 31) == 0) atomicOr(&s_mask, mask);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int oi = 0; oi < 27; ++oi)
+      if ((s_mask >> oi) & 1u) s_act[n++] = oi;
+    s_nact = n;
+  }
+  __syncthreads();
+  const int nact = s_nact;
   double acc[32];
 #pragma unroll
   for (int c = 0; c < 32; ++c) acc[c] = 0.0;
   double r1 = 0.0;
-  int issued = 0, waits0 = 0, waits1 = 0;
+  int issued = 0, waits0 = 0, waits1 = 0, my_abort = 0;
   auto epilogue = [&](int b) {
     const uint32_t parity = uint32_t(b ? waits1 : waits0) & 1u;
     if (b) ++waits1; else ++waits0;
     if (!tc::mbar_wait(tc::smem_u32(&mbar[b]), parity, TC_MAX_TRIES)) {
-      atomicExch(&abort_flag, 1);
+      my_abort = 1;
       atomicExch(err, 1);
     }
     tc::fence_after_sync();
@@ -415,22 +475,44 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
     }
     tc::fence_before_sync();
   };
-  for (int oi = 0; oi < 27; ++oi) {
-    const int o = c_class_off_mx[cls][oi];
-    if (op.kind[o] == M2L_NULL) continue;
-    const int src = tg >= 0 ? il[(size_t)tg * N_OFFSETS + o] : -1;
-    const int any = __syncthreads_or(src >= 0);
-    if (abort_flag) break;
-    if (!any) continue;
+  // the next offset's source row, operator slice and charge sum are loaded
+  // into registers while the current offset is staged, multiplied and read
+  const int units = ntc * nk4;
+  float4 pa[8], pb[4];
+  double pm = 0.0;
+  int psrc = -1;
+  auto prefetch = [&](int ai) {
+    const int oi = s_act[ai], o = c_class_off_mx[cls][oi];
+    psrc = s_src[oi][threadIdx.x];
+#pragma unroll
+    for (int k4 = 0; k4 < 8; ++k4)
+      pa[k4] = (k4 < nk4 && psrc >= 0)
+                   ? __ldg(reinterpret_cast<const float4 *>(mult32 + (size_t)psrc * np) + k4)
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
+    pm = psrc >= 0 ? op.c_m2l[o] * __ldg(msum + psrc) : 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int u = (int)threadIdx.x + i * TCM;
+      if (u < 2 * units) {
+        const int part = u >= units, uu = part ? u - units : u;
+        const int n = uu / nk4, k4 = uu % nk4;
+        const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
+        pb[i] = __ldg(reinterpret_cast<const float4 *>(bsrc + (size_t)n * np) + k4);
+      }
+    }
+  };
+  if (nact > 0) prefetch(0);
+  for (int ai = 0; ai < nact; ++ai) {
     const int buf = issued & 1;
+    r1 += pm;
     // stage A: this thread's target row, TF32 hi / lo
-    if (src >= 0) r1 += op.c_m2l[o] * msum[src];
     {
       const int r = threadIdx.x;
       unsigned char *ah = A0 + (2 * buf) * a_sz, *al = A0 + (2 * buf + 1) * a_sz;
-      for (int k4 = 0; k4 < nk4; ++k4) {
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (src >= 0) v = *reinterpret_cast<const float4 *>(mult32 + (size_t)src * np + 4 * k4);
+#pragma unroll
+      for (int k4 = 0; k4 < 8; ++k4) {
+        if (k4 >= nk4) break;
+        const float4 v = pa[k4];
         const float4 h = make_float4(__uint_as_float(to_tf32(v.x)), __uint_as_float(to_tf32(v.y)),
                                      __uint_as_float(to_tf32(v.z)), __uint_as_float(to_tf32(v.w)));
         const float4 l = make_float4(__uint_as_float(to_tf32(v.x - h.x)), __uint_as_float(to_tf32(v.y - h.y)),
@@ -441,20 +523,20 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
       }
     }
     // stage B: the offset's operator, ntc rows x np, hi and lo
-    {
-      const int units = ntc * nk4;
-      for (int u = threadIdx.x; u < 2 * units; u += TCM) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int u = (int)threadIdx.x + i * TCM;
+      if (u < 2 * units) {
         const int part = u >= units, uu = part ? u - units : u;
         const int n = uu / nk4, k4 = uu % nk4;
-        const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
-        const float4 v = *reinterpret_cast<const float4 *>(bsrc + (size_t)n * np + 4 * k4);
         const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
-        *reinterpret_cast<float4 *>(B0 + (2 * buf + part) * b_sz + off) = v;
+        *reinterpret_cast<float4 *>(B0 + (2 * buf + part) * b_sz + off) = pb[i];
       }
     }
+    if (ai + 1 < nact) prefetch(ai + 1);
     tc::fence_proxy_async();
     tc::fence_before_sync();
-    __syncthreads();
+    if (__syncthreads_or(my_abort)) break;
     if (threadIdx.x == 0) {
       tc::fence_after_sync();
       for (int ks = 0; ks < nks; ++ks) {
@@ -472,7 +554,15 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
     if (issued >= 1) epilogue(buf ^ 1);
     ++issued;
   }
-  if (issued >= 1 && !abort_flag) epilogue((issued - 1) & 1);
+  const int aborted = __syncthreads_or(my_abort);
+  if (issued >= 1 && !aborted) epilogue((issued - 1) & 1);
+  if (aborted) {
+    // wait (bounded) for the commits still outstanding before TMEM is freed
+    for (; waits0 < (issued + 1) / 2; ++waits0)
+      tc::mbar_wait(tc::smem_u32(&mbar[0]), uint32_t(waits0) & 1u, TC_MAX_TRIES);
+    for (; waits1 < issued / 2; ++waits1)
+      tc::mbar_wait(tc::smem_u32(&mbar[1]), uint32_t(waits1) & 1u, TC_MAX_TRIES);
+  }
   if (tg >= 0) {
     double *o = ple + (size_t)tg * np;
 #pragma unroll
@@ -486,6 +576,7 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
 }
 
 // -------------------------------------------------------------- downward ----
+template <bool kStageB>
 __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int rg_lo, int rg_cnt,
                                                     const int *__restrict__ rg,
                                                     const int *__restrict__ parent,
@@ -494,16 +585,24 @@ __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int 
                                                     float *__restrict__ loc32,
                                                     double *__restrict__ lsum) {
   extern __shared__ double smem[];
-  const int ldp = pad_ld(np), ldl = pad_f(np);
-  double *P = smem;                                     // [32][ldp] partial locals
-  double *T = P + TN * ldp;                             // [32][ldp] C2E scratch
-  float *Lp = reinterpret_cast<float *>(T + TN * ldp);  // [16][ldl] parent locals (rows 8-15 zero)
+  const int ldp = pad_ld(np), ldl = pad_f(np), ldb = ldb_f(4 * np);
+  double *P = smem;                                      // [32][ldp] partial locals
+  double *T = P + TN * ldp;                              // [32][ldp] C2E scratch
+  double *Cs = T + TN * ldp;                             // staged C2E operators
+  float *Lp = reinterpret_cast<float *>(Cs + c2e_stage_doubles(np));  // [16][ldl] parent locals
+  float *Bh = Lp + 16 * ldl, *Bl = Bh + np * ldb;       // staged (M2MC - c) hi / lo [np][ldb]
   __shared__ int node[TN];
   __shared__ double *orow[TN];
   __shared__ double psum[8];
   const LevelOpsDev &op = ops[m];
   const int q0 = 8 * blockIdx.x;
   const int ngrp = min(8, rg_cnt - q0);
+  // operators in flight while the node indices and locals are read
+  const C2EView cv = c2e_stage(op, np, Cs);
+  if (kStageB && m >= 3) {
+    stage_rows(Bh, ldb, ops[m - 1].m2mc_hi, np, 4 * np);
+    stage_rows(Bl, ldb, ops[m - 1].m2mc_lo, np, 4 * np);
+  }
   if (threadIdx.x < TN) {
     const int grp = threadIdx.x >> 2;
     node[threadIdx.x] = (grp < ngrp) ? rg[rg_lo + q0 + grp] + int(threadIdx.x & 3) : -1;
@@ -529,10 +628,15 @@ __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int 
       const int n0 = node[4 * threadIdx.x];
       psum[threadIdx.x] = (n0 >= 0) ? lsum[parent[n0]] : 0.0;
     }
+    cp_async_wait_all();
     __syncthreads();
     // L2L: [8 parents][4np] = Lp . (M2MC - c) + c * sum(Lp)   (flexmm/flexmm2d/fmm.py:140-147)
     double acc[4][4] = {};
-    warp_gemm_x3<4>(Lp, ldl, opp.m2mc_hi, opp.m2mc_lo, 4 * np, np, 0, 8 * warp, 8, 4 * np, acc);
+    if (kStageB)
+      warp_gemm_x3<4, true>(Lp, ldl, Bh, Bl, ldb, np, 0, 8 * warp, 8, 4 * np, acc);
+    else
+      warp_gemm_x3<4, false>(Lp, ldl, opp.m2mc_hi, opp.m2mc_lo, 4 * np, np, 0, 8 * warp, 8, 4 * np,
+                             acc);
     if (g < 8) {
 #pragma unroll
       for (int cb = 0; cb < 4; ++cb) {
@@ -545,9 +649,10 @@ __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int 
         }
       }
     }
-    __syncthreads();
   }
-  c2e_tile(op, np, P, T, orow);
+  cp_async_wait_all();
+  __syncthreads();
+  c2e_tile<true>(cv, np, P, T, orow);
   __syncthreads();
   store_mixed(P, ldp, np, neq, node, TN, loc32, lsum);
 }
@@ -758,8 +863,9 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
   const TreeDev &td = *a.td;
   const int np = a.np;
   if (th.L < 3) return;
-  const size_t pbytes = sizeof(double) * (size_t)TN * pad_ld(np) * 2;
-  const size_t abytes = pbytes + sizeof(float) * (size_t)TN * pad_f(4 * np);
+  const size_t pbytes = sizeof(double) * ((size_t)TN * pad_ld(np) * 2 + c2e_stage_doubles(np));
+  FMMB_CUDA(cudaFuncSetAttribute(k_s2m_mx<KF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(pbytes)));
   PhaseTimer timer(PH_UPWARD, s);
   k_s2m_mx<KF32><<<148 * 4, NT, pbytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
                                               td.uplist.get(), td.n_up.get(), td.bot.get(),
@@ -767,15 +873,17 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
                                               td.sx.get(), td.sy.get(), tau_s, tsum, a.ops_dev,
                                               mult32, msum);
   FMMB_CUDA(cudaGetLastError());
-  FMMB_CUDA(cudaFuncSetAttribute(k_m2m_mx, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(double) * (size_t)TN * pad_ld(64) * 2 +
-                                     sizeof(float) * (size_t)TN * pad_f(4 * 64))));
+  // operators staged in shared memory when they fit (static smem ~1 KB aside)
+  const bool stage_b = m2m_mx_smem(np, true) + 4096 <= smem_optin();
+  const size_t mbytes = m2m_mx_smem(np, stage_b);
+  auto kern = stage_b ? k_m2m_mx<true> : k_m2m_mx<false>;
+  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mbytes)));
   for (int m = th.L - 2; m >= 2; --m) {
     const int c_first = th.off[m + 1];
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
     if (n_groups == 0) continue;
-    k_m2m_mx<<<(n_groups + TN - 1) / TN, NT, abytes, s>>>(m, a.neq, np, c_first, n_groups,
-                                                         td.parent.get(), a.ops_dev, mult32, msum);
+    kern<<<(n_groups + TN - 1) / TN, NT, mbytes, s>>>(m, a.neq, np, c_first, n_groups,
+                                                     td.parent.get(), a.ops_dev, mult32, msum);
     FMMB_CUDA(cudaGetLastError());
   }
 }
@@ -866,14 +974,20 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
                         cudaStream_t s) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
-  const size_t sm = sizeof(double) * (size_t)TN * pad_ld(a.np) * 2 +
-                    sizeof(float) * (size_t)16 * pad_f(a.np);
+  auto bytes = [&](bool stage_b) {
+    return sizeof(double) * ((size_t)TN * pad_ld(a.np) * 2 + c2e_stage_doubles(a.np)) +
+           sizeof(float) * ((size_t)16 * pad_f(a.np) + (stage_b ? (size_t)2 * a.np * ldb_f(4 * a.np) : 0));
+  };
+  const bool stage_b = bytes(true) + 4096 <= smem_optin();
+  const size_t sm = bytes(stage_b);
+  auto kern = stage_b ? k_downward_mx<true> : k_downward_mx<false>;
+  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   for (int m = 2; m < th.L; ++m) {
     const int lo = th.rg_lo[m], cnt = th.rg_hi[m] - th.rg_lo[m];
     if (cnt <= 0) continue;
     PhaseTimer timer(PH_DOWNWARD, s);
-    k_downward_mx<<<(cnt + 7) / 8, NT, sm, s>>>(m, a.neq, a.np, lo, cnt, td.rg.get(), td.parent.get(),
-                                                a.ops_dev, ple, loc32, lsum);
+    kern<<<(cnt + 7) / 8, NT, sm, s>>>(m, a.neq, a.np, lo, cnt, td.rg.get(), td.parent.get(),
+                                       a.ops_dev, ple, loc32, lsum);
     FMMB_CUDA(cudaGetLastError());
   }
 }
