@@ -392,7 +392,12 @@ def work_counts_gemm(F, neq, c):
     return out
 
 
-def roofline_of(res, precision, peaks, steps):
+# DRAM bytes (read + write) per launch of the dominant kernel on the default
+# workload, from one ncu capture of it (profiles/k_evaluate_traffic_clustered1M.md)
+NCU_TRAFFIC_BYTES = {("mixed", "evaluate"): 43_461_560, ("fp64", "evaluate"): 53_386_240}
+
+
+def roofline_of(res, precision, peaks, steps, default_workload):
     c = res["counts"]
     ke = {"evaluate": c["p2p_pairs_src"] + c["p2p_pairs_tgt"] + c["l2t_ke"], "upward": c["s2m_ke"]}
     kernel_flops = {
@@ -412,10 +417,7 @@ def roofline_of(res, precision, peaks, steps):
         bound, peak, src = "tensor", peaks["tf32"], "cuBLAS TF32 GEMM 8192^3 on this GPU"
     else:
         bound, peak, src = "fp32", peaks["fp32"], "cuBLAS SGEMM 8192^3, TF32 off, on this GPU (FP32 pipe)"
-    traffic = None
-    tpath = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"{precision}:{dom}")
+    traffic = NCU_TRAFFIC_BYTES.get((precision, dom)) if default_workload else None
     return {"bound": bound, "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": "measured in bench.py: " + src,
             "flops_per_launch": flops_per_launch, "ms_per_launch": ms_k / max(n_launch, 1)}
@@ -440,13 +442,14 @@ def run_ours(args, world, rank, local):
              "fp32": gemm_peak_tflops(torch, torch.float32),
              "tf32": gemm_peak_tflops(torch, torch.float32, tf32=True)}
     main = res[args.precision]
+    default_workload = args.n == 1_000_000 and args.grid == 1000
 
     def summary(p, r):
         return {"value": world * pts / (r["ms_step"] * 1e-3) / 1e6, "ms_per_step": r["ms_step"],
                 "nequiv": r["neq"], "accuracy": r["accuracy"],
                 "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in r["phases"].items() if v[1]},
                 "e2e_value": world * pts / (r["e2e_step"] * 1e-3) / 1e6,
-                "roofline": roofline_of(r, p, peaks, args.steps)}
+                "roofline": roofline_of(r, p, peaks, args.steps, default_workload)}
 
     out = {
         "metric": METRIC, "value": world * pts / (main["ms_step"] * 1e-3) / 1e6, "unit": "Mpts/s",
@@ -470,7 +473,7 @@ def run_ours(args, world, rank, local):
                 "d2h_bytes_per_step": 8 * (n_src + n_tgt), "ms_per_step": main["e2e_step"],
                 "ms_samples": [round(v, 3) for v in main["e2e_samples"]]},
         "gpu_launches": main["launches"],
-        "roofline": roofline_of(main, args.precision, peaks, args.steps),
+        "roofline": roofline_of(main, args.precision, peaks, args.steps, default_workload),
         "peaks_measured_tflops": peaks,
     }
     for p in forms[1:]:
