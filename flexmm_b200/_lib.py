@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libflexmm_b200.so")
 
 N_OFFSETS = 40
 PRECISION = {"fp64": 0, "mixed": 1}
+EVALUATORS = {"potential": (0, 1), "gradient": (1, 3)}   # id, outputs
 N_PHASES = 12
 PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "tree_splits",
           "tree_balance", "tree_nodes", "prep", "spare"]
@@ -53,6 +54,10 @@ SIGNATURES = [
     ("fmm_build_expansions", ctypes.c_int, [_vp, _vp, _vp]),
     ("fmm_evaluate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),
     ("fmm_evaluate_sources", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    ("fmm_evaluate_outputs", ctypes.c_int,
+     [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
+    ("fmm_evaluate_sources_outputs", ctypes.c_int,
+     [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
     ("fmm_plan_destroy", ctypes.c_int, [_vp]),
     ("fmm_plan_status", ctypes.c_int, [_vp]),
     ("fmm_tree_export", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

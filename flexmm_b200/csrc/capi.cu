@@ -419,55 +419,86 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
   });
 }
 
+namespace {
+// outputs of an evaluator id (FMM_EVAL_*)
+int evaluator_outputs(int evaluator) {
+  FMMB_CHECK(evaluator == FMM_EVAL_POTENTIAL || evaluator == FMM_EVAL_GRADIENT,
+             ERR_INVALID_ARGUMENT, "evaluator must be FMM_EVAL_POTENTIAL or FMM_EVAL_GRADIENT");
+  return evaluator == FMM_EVAL_GRADIENT ? 3 : 1;
+}
+
+void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, int64_t m,
+                     int check, double *out, int64_t ld_out, cudaStream_t s) {
+  FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+  FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+  FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
+  if (m == 0) return;
+  FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
+  FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
+  FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the target count");
+  PassArgs a = pass_args(p);
+  DevBuf<uint64_t> tkeys;
+  DevBuf<int> tperm;
+  DevBuf<double> txs, tys;
+  {
+    PhaseTimer timer(PH_SORT_TGT, s);
+    // leaves live on levels <= L-1: their first L-1 digits decide everything
+    sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1);
+    txs.alloc(m, s);
+    tys.alloc(m, s);
+    gather_sorted(tx, tperm.get(), m, txs.get(), s);
+    gather_sorted(ty, tperm.get(), m, tys.get(), s);
+  }
+  if (p->precision == PREC_MIXED)
+    run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(), txs.get(),
+                       tys.get(), tkeys.get(), tperm.get(), m, check, nout, out, ld_out, s);
+  else
+    run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(),
+                 m, check, nout, out, ld_out, s);
+}
+
+void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t ld_out,
+                          cudaStream_t s) {
+  FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+  FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+  FMMB_CHECK(out, ERR_INVALID_ARGUMENT, "NULL argument");
+  const TreeDev &td = p->td;
+  const int64_t m = p->th.n_points;
+  FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the source count");
+  PassArgs a = pass_args(p);
+  // the tree's sorted copy: keys sorted on at least their top L-1 digits,
+  // which is all that leaf location reads
+  if (p->precision == PREC_MIXED)
+    run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(),
+                       td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, nout,
+                       out, ld_out, s);
+  else
+    run_evaluate(a, p->tau_s.get(), p->loc.get(), td.sx.get(), td.sy.get(), td.pkeys.get(),
+                 td.ordv.get(), m, check, nout, out, ld_out, s);
+}
+}  // namespace
+
 int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int check,
                  double *out, void *stream) {
-  return guarded([&] {
-    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
-    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
-    FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
-    if (m == 0) return;
-    FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
-    FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
-    cudaStream_t s = (cudaStream_t)stream;
-    PassArgs a = pass_args(p);
-    DevBuf<uint64_t> tkeys;
-    DevBuf<int> tperm;
-    DevBuf<double> txs, tys;
-    {
-      PhaseTimer timer(PH_SORT_TGT, s);
-      // leaves live on levels <= L-1: their first L-1 digits decide everything
-      sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1);
-      txs.alloc(m, s);
-      tys.alloc(m, s);
-      gather_sorted(tx, tperm.get(), m, txs.get(), s);
-      gather_sorted(ty, tperm.get(), m, tys.get(), s);
-    }
-    if (p->precision == PREC_MIXED)
-      run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(), txs.get(),
-                         tys.get(), tkeys.get(), tperm.get(), m, check, out, s);
-    else
-      run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(),
-                   m, check, out, s);
-  });
+  return guarded([&] { evaluate_points(p, 1, tx, ty, m, check, out, m, (cudaStream_t)stream); });
 }
 
 int fmm_evaluate_sources(fmm_plan *p, int check, double *out, void *stream) {
+  return guarded([&] { evaluate_own_sources(p, 1, check, out, 0, (cudaStream_t)stream); });
+}
+
+int fmm_evaluate_outputs(fmm_plan *p, int evaluator, const double *tx, const double *ty,
+                         int64_t m, int check, double *out, int64_t ld_out, void *stream) {
   return guarded([&] {
-    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
-    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
-    FMMB_CHECK(out, ERR_INVALID_ARGUMENT, "NULL argument");
-    cudaStream_t s = (cudaStream_t)stream;
-    PassArgs a = pass_args(p);
-    const TreeDev &td = p->td;
-    const int64_t m = p->th.n_points;
-    // the tree's sorted copy: keys sorted on at least their top L-1 digits,
-    // which is all that leaf location reads
-    if (p->precision == PREC_MIXED)
-      run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(),
-                         td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, out, s);
-    else
-      run_evaluate(a, p->tau_s.get(), p->loc.get(), td.sx.get(), td.sy.get(), td.pkeys.get(),
-                   td.ordv.get(), m, check, out, s);
+    evaluate_points(p, evaluator_outputs(evaluator), tx, ty, m, check, out, ld_out,
+                    (cudaStream_t)stream);
+  });
+}
+
+int fmm_evaluate_sources_outputs(fmm_plan *p, int evaluator, int check, double *out,
+                                 int64_t ld_out, void *stream) {
+  return guarded([&] {
+    evaluate_own_sources(p, evaluator_outputs(evaluator), check, out, ld_out, (cudaStream_t)stream);
   });
 }
 

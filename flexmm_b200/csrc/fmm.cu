@@ -328,7 +328,9 @@ __global__ void k_make_items(int total, int L, const int *__restrict__ off, cons
 // (rounded down to a power of two) threads share a target: they split the
 // circle points of L2T and the colleague sources of P2P, then reduce with
 // warp shuffles (and shared memory when G > 32).
-template <class KF>
+// NOUT = 1: potential; NOUT = 3: potential and its gradient in the target
+// position (rows of out, stride ld_out).
+template <class KF, int NOUT>
 __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np,
                                                   const int4 *__restrict__ items,
                                                   const int *__restrict__ n_items_ptr,
@@ -345,11 +347,11 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
                                                   const double *__restrict__ txs,
                                                   const double *__restrict__ tys,
                                                   const int *__restrict__ tperm, int check,
-                                                  double *__restrict__ out) {
+                                                  double *__restrict__ out, int64_t ld_out) {
   __shared__ double Ls[64], lxs[64], lys[64];
   __shared__ double ssx[SMAX], ssy[SMAX], stau[SMAX];
   __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
-  __shared__ double red[TCH / 32];
+  __shared__ double red[NOUT][TCH / 32];
   const KF K(kp);
   const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -377,16 +379,21 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     if (threadIdx.x == 0)
       for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
     double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
+    double gu = 0.0, gx = 0.0, gy = 0.0;  // NOUT = 3
     if (lev >= 2 && valid) {
       const double dx = x - xmid[g], dy = y - ymid[g];
-      int k = sub;
-      for (; k + 3 * G < neq; k += 4 * G) {
-        u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
-        u1 = fma(K(lxs[k + G], lys[k + G], dx, dy), Ls[k + G], u1);
-        u2 = fma(K(lxs[k + 2 * G], lys[k + 2 * G], dx, dy), Ls[k + 2 * G], u2);
-        u3 = fma(K(lxs[k + 3 * G], lys[k + 3 * G], dx, dy), Ls[k + 3 * G], u3);
+      if constexpr (NOUT == 1) {
+        int k = sub;
+        for (; k + 3 * G < neq; k += 4 * G) {
+          u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
+          u1 = fma(K(lxs[k + G], lys[k + G], dx, dy), Ls[k + G], u1);
+          u2 = fma(K(lxs[k + 2 * G], lys[k + 2 * G], dx, dy), Ls[k + 2 * G], u2);
+          u3 = fma(K(lxs[k + 3 * G], lys[k + 3 * G], dx, dy), Ls[k + 3 * G], u3);
+        }
+        for (; k < neq; k += G) u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
+      } else {
+        for (int k = sub; k < neq; k += G) K.grad(lxs[k], lys[k], dx, dy, Ls[k], gu, gx, gy);
       }
-      for (; k < neq; k += G) u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
     }
     __syncthreads();
     // P2P over the colleagues' sorted source ranges (flexmm/flexmm2d/helpers.py:152-194);
@@ -410,29 +417,47 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
       }
       __syncthreads();
       if (valid) {
-        int j = sub;
-        for (; j + 3 * G < nb; j += 4 * G) {
-          u0 += pair(j);
-          u1 += pair(j + G);
-          u2 += pair(j + 2 * G);
-          u3 += pair(j + 3 * G);
+        if constexpr (NOUT == 1) {
+          int j = sub;
+          for (; j + 3 * G < nb; j += 4 * G) {
+            u0 += pair(j);
+            u1 += pair(j + G);
+            u2 += pair(j + 2 * G);
+            u3 += pair(j + 3 * G);
+          }
+          for (; j < nb; j += G) u0 += pair(j);
+        } else {
+          for (int j = sub; j < nb; j += G) {
+            const double qx = ssx[j], qy = ssy[j];
+            if (!(check && x - qx == 0.0 && y - qy == 0.0)) K.grad(qx, qy, x, y, stau[j], gu, gx, gy);
+          }
         }
-        for (; j < nb; j += G) u0 += pair(j);
       }
       __syncthreads();
     }
     // reduce over the G threads of each target
-    double u = (u0 + u1) + (u2 + u3);
-    for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
-    if (G > 32) {
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
-      __syncthreads();
-      if (sub == 0) {
-        u = 0.0;
-        for (int w = 0; w < G / 32; ++w) u += red[(threadIdx.x >> 5) + w];
-      }
+    double r[NOUT];
+    if constexpr (NOUT == 1) {
+      r[0] = (u0 + u1) + (u2 + u3);
+    } else {
+      r[0] = gu;
+      r[1] = gx;
+      r[2] = gy;
     }
-    if (valid && sub == 0) out[tperm[t0 + t]] = u;
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      double u = r[o];
+      for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
+      if (G > 32) {
+        if ((threadIdx.x & 31) == 0) red[o][threadIdx.x >> 5] = u;
+        __syncthreads();
+        if (sub == 0) {
+          u = 0.0;
+          for (int w = 0; w < G / 32; ++w) u += red[o][(threadIdx.x >> 5) + w];
+        }
+      }
+      if (valid && sub == 0) out[o * ld_out + tperm[t0 + t]] = u;
+    }
     __syncthreads();
   }
 }
@@ -535,17 +560,16 @@ namespace {
 template <class KF>
 void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
                    const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
-                   double *out, cudaStream_t s) {
-  const TreeHost &th = *a.th;
+                   int nout, double *out, int64_t ld_out, cudaStream_t s) {
   const TreeDev &td = *a.td;
-  const int total = th.n_total();
   EvalItems it;
   eval_items(a, tkeys, m, it, s);
   PhaseTimer timer(PH_EVAL, s);
-  k_evaluate<KF><<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(),
-                                         td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
-                                         td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
-                                         loc, txs, tys, tperm, check, out);
+  auto kern = nout == 3 ? k_evaluate<KF, 3> : k_evaluate<KF, 1>;
+  kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(),
+                               td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
+                               td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out,
+                               ld_out);
   FMMB_CUDA(cudaGetLastError());
 }
 }  // namespace
@@ -599,11 +623,11 @@ void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_
 
 void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
                   const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
-                  double *out, cudaStream_t s) {
+                  int nout, double *out, int64_t ld_out, cudaStream_t s) {
   if (m == 0) return;
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
-      evaluate_impl<LaplaceF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, out, s);
+      evaluate_impl<LaplaceF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out, ld_out, s);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
@@ -650,10 +674,10 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   FMMB_CUDA(cudaGetLastError());
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
-      k_evaluate<LaplaceF64><<<148 * 8, TCH, 0, s>>>(
+      k_evaluate<LaplaceF64, 1><<<148 * 8, TCH, 0, s>>>(
           a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(), td.top.get(),
           td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc, txs, tys,
-          tperm, check, out);
+          tperm, check, out, 0);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

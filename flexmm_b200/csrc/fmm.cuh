@@ -58,9 +58,11 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
                 const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
                 int check, double *out, cudaStream_t s);
 void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaStream_t s);
+// nout = 1: potential into out[m]; nout = 3: potential and its gradient in the
+// target position into out[0..2][m] (row stride ld_out)
 void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc,
                   const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
-                  int64_t m, int check, double *out, cudaStream_t s);
+                  int64_t m, int check, int nout, double *out, int64_t ld_out, cudaStream_t s);
 
 // Evaluation work items: per leaf its range of sorted targets, split into
 // chunks of 128 targets; choff = exclusive scan of the chunk counts.
@@ -83,7 +85,7 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
 void run_evaluate_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum,
                         const float *loc32, const double *lsum, const double *txs,
                         const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
-                        int check, double *out, cudaStream_t s);
+                        int check, int nout, double *out, int64_t ld_out, cudaStream_t s);
 
 // Evaluation with caller-provided scratch: tb, te, nch, choff hold one int
 // per tree node, temp holds evaluate_scratch_bytes(nodes) bytes.

@@ -705,27 +705,35 @@ __global__ void k_eval_desc(const int4 *__restrict__ items, const int *__restric
   }
 }
 
+// reciprocal on the special-function unit, denormals flushed
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // P2P pairs are summed in FP32 over at most 4 x 8 terms per thread, then in
 // FP64 (cascaded summation: the FP32 rounding stays relative to short partial
-// sums); the kernel offset terms are added in FP64.
-template <class KF32, class KF64>
-__global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelParams kp, int neq, int np,
-                                                     const EvalDesc *__restrict__ desc,
-                                                     const int *__restrict__ n_items_ptr,
-                                                     const double *__restrict__ sx,
-                                                     const double *__restrict__ sy,
-                                                     const double *__restrict__ tau,
-                                                     const LevelOpsDev *__restrict__ ops,
-                                                     const float *__restrict__ loc32,
-                                                     const double *__restrict__ lsum,
-                                                     const double *__restrict__ txs,
-                                                     const double *__restrict__ tys,
-                                                     const int *__restrict__ tperm, int check,
-                                                     double *__restrict__ out,
-                                                     int *__restrict__ next_item) {
+// sums); the kernel offset terms are added in FP64.  NOUT = 1: potential;
+// NOUT = 3: potential and its gradient in the target position (rows of out,
+// stride ld_out); the gradient is summed on width-scaled coordinates and
+// scaled by 1/w in FP64.
+template <class KF32, class KF64, int NOUT>
+__global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
+    k_evaluate_mx(KernelParams kp, int neq, int np, const EvalDesc *__restrict__ desc,
+                  const int *__restrict__ n_items_ptr, const double *__restrict__ sx,
+                  const double *__restrict__ sy, const double *__restrict__ tau,
+                  const LevelOpsDev *__restrict__ ops, const float *__restrict__ loc32,
+                  const double *__restrict__ lsum, const double *__restrict__ txs,
+                  const double *__restrict__ tys, const int *__restrict__ tperm, int check,
+                  double *__restrict__ out, int64_t ld_out, int *__restrict__ next_item) {
   __shared__ EvalDesc D;
   __shared__ float4 src[SMAX];  // (x, y, charge, sorted index) in width units of the leaf
-  __shared__ double red[TCH / 32];
+  // NOUT = 3: the low parts of the source coordinates (x = hi + lo): the
+  // gradient is dominated by the closest pairs, whose FP32 differences would
+  // otherwise lose the digits below 2^-24 of the leaf width
+  __shared__ float2 src_lo[NOUT == 3 ? SMAX : 1];
+  __shared__ double red[NOUT][TCH / 32];
   __shared__ int s_next;
   const KF32 K(kp);
   const KF64 K64(kp);
@@ -750,26 +758,44 @@ __global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelP
     const double cx = D.cx, cy = D.cy;
     const double iw = ops[lev].inv_w, kofs = ops[lev].kofs;
     const double x = valid ? txs[t0 + t] : cx, y = valid ? tys[t0 + t] : cy;
-    const float tx = (float)((x - cx) * iw), ty = (float)((y - cy) * iw);
-    double acc = 0.0;
+    const double txd = (x - cx) * iw, tyd = (y - cy) * iw;
+    const float tx = (float)txd, ty = (float)tyd;
+    const float tx_lo = (float)(txd - (double)tx), ty_lo = (float)(tyd - (double)ty);
+    double acc = 0.0, accx = 0.0, accy = 0.0;  // accx, accy: kScale * (dx, dy) / d2 sums
     if (lev >= 2 && valid) {  // L2T (flexmm/flexmm2d/kifmm.py:106-120), operands through L1
       const float *Lg = loc32 + (size_t)g * np;
       const float *lx = ops[lev].lx32, *ly = ops[lev].ly32;
-      float p0 = 0.f, p1 = 0.f;
-      int k = sub;
-      for (; k + G < neq; k += 2 * G) {
-        p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
-        p1 = fmaf(K(tx - __ldg(lx + k + G), ty - __ldg(ly + k + G)), __ldg(Lg + k + G), p1);
+      if constexpr (NOUT == 1) {
+        float p0 = 0.f, p1 = 0.f;
+        int k = sub;
+        for (; k + G < neq; k += 2 * G) {
+          p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
+          p1 = fmaf(K(tx - __ldg(lx + k + G), ty - __ldg(ly + k + G)), __ldg(Lg + k + G), p1);
+        }
+        if (k < neq) p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
+        acc = (double)p0 + (double)p1;
+      } else {
+        float p0 = 0.f, px = 0.f, py = 0.f;
+        for (int k = sub; k < neq; k += G) {
+          const float dx = tx - __ldg(lx + k), dy = ty - __ldg(ly + k);
+          const float d2 = fmaf(dy, dy, dx * dx);
+          const float q = __ldg(Lg + k) * KF32::kScale;
+          p0 = fmaf(K.radial(d2), q, p0);
+          const float qr = rcp_ftz(d2) * q;
+          px = fmaf(dx, qr, px);
+          py = fmaf(dy, qr, py);
+        }
+        acc = (double)p0;
+        accx = (double)px;
+        accy = (double)py;
       }
-      if (k < neq) p0 = fmaf(K(tx - __ldg(lx + k), ty - __ldg(ly + k)), __ldg(Lg + k), p0);
-      acc = (double)p0 + (double)p1;
     }
     // P2P (flexmm/flexmm2d/helpers.py:152-194): branch-free FP32 sweep with
     // the kernel's scale folded into the staged charges.  A pair closer than
     // FLT_MIN in squared width units (coincident in FP32) contributes 0 there
     // and is redone in FP64 on the exact coordinates: the one such pair a
     // thread meets (a source evaluated at itself) directly, more by a rescan.
-    double exact = 0.0;
+    double exact = 0.0, exact_x = 0.0, exact_y = 0.0;
     for (int base = 0; base < ns; base += SMAX) {
       const int nb = min(SMAX, ns - base);
       if (base > 0) __syncthreads();  // previous chunk fully read
@@ -779,36 +805,71 @@ __global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelP
 #pragma unroll
         for (int k = 1; k < 9; ++k) c += (idx >= D.rs[k]);
         const int j = D.rb[c] + (idx - D.rs[c]);
-        src[i] = make_float4((float)((sx[j] - cx) * iw), (float)((sy[j] - cy) * iw),
-                             (float)tau[j] * KF32::kScale, __int_as_float(j));
+        const double qx = (sx[j] - cx) * iw, qy = (sy[j] - cy) * iw;
+        src[i] = make_float4((float)qx, (float)qy, (float)tau[j] * KF32::kScale, __int_as_float(j));
+        if constexpr (NOUT == 3)
+          src_lo[i] = make_float2((float)(qx - (double)(float)qx), (float)(qy - (double)(float)qy));
       }
       __syncthreads();
       if (valid) {
-        float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
         int nhit = 0, hj = 0;
-        auto pair = [&](const float4 q, int jj, float &p) {
-          const float dx = tx - q.x, dy = ty - q.y;
-          const float d2 = fmaf(dy, dy, dx * dx);
-          const bool z = d2 < 1.17549435e-38f;  // FLT_MIN
-          nhit += z;
-          hj = z ? jj : hj;
-          const float v = K.radial(d2);
-          p = fmaf(z ? 0.f : v, q.z, p);
-        };
-        int j = sub, nsum = 0;
-        for (; j + 3 * G < nb; j += 4 * G) {
-          pair(src[j], j, p0);
-          pair(src[j + G], j + G, p1);
-          pair(src[j + 2 * G], j + 2 * G, p2);
-          pair(src[j + 3 * G], j + 3 * G, p3);
-          if (++nsum == 8) {
-            acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
-            p0 = p1 = p2 = p3 = 0.f;
-            nsum = 0;
+        if constexpr (NOUT == 1) {
+          float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+          auto pair = [&](const float4 q, int jj, float &p) {
+            const float dx = tx - q.x, dy = ty - q.y;
+            const float d2 = fmaf(dy, dy, dx * dx);
+            const bool z = d2 < 1.17549435e-38f;  // FLT_MIN
+            nhit += z;
+            hj = z ? jj : hj;
+            const float v = K.radial(d2);
+            p = fmaf(z ? 0.f : v, q.z, p);
+          };
+          int j = sub, nsum = 0;
+          for (; j + 3 * G < nb; j += 4 * G) {
+            pair(src[j], j, p0);
+            pair(src[j + G], j + G, p1);
+            pair(src[j + 2 * G], j + 2 * G, p2);
+            pair(src[j + 3 * G], j + 3 * G, p3);
+            if (++nsum == 8) {
+              acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+              p0 = p1 = p2 = p3 = 0.f;
+              nsum = 0;
+            }
           }
+          for (; j < nb; j += G) pair(src[j], j, p0);
+          acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+        } else {
+          float p[2] = {0.f, 0.f}, px[2] = {0.f, 0.f}, py[2] = {0.f, 0.f};
+          auto pair = [&](const float4 q, int jj, int a) {
+            // hi parts first: exact for close points (Sterbenz), then the low parts
+            const float2 ql = src_lo[jj];
+            const float dx = (tx - q.x) + (tx_lo - ql.x), dy = (ty - q.y) + (ty_lo - ql.y);
+            const float d2 = fmaf(dy, dy, dx * dx);
+            const bool z = d2 < 1.17549435e-38f;  // FLT_MIN
+            nhit += z;
+            hj = z ? jj : hj;
+            p[a] = fmaf(z ? 0.f : K.radial(d2), q.z, p[a]);
+            const float qr = z ? 0.f : rcp_ftz(d2) * q.z;
+            px[a] = fmaf(dx, qr, px[a]);
+            py[a] = fmaf(dy, qr, py[a]);
+          };
+          int j = sub, nsum = 0;
+          for (; j + G < nb; j += 2 * G) {
+            pair(src[j], j, 0);
+            pair(src[j + G], j + G, 1);
+            if (++nsum == 16) {
+              acc += (double)p[0] + (double)p[1];
+              accx += (double)px[0] + (double)px[1];
+              accy += (double)py[0] + (double)py[1];
+              p[0] = p[1] = px[0] = px[1] = py[0] = py[1] = 0.f;
+              nsum = 0;
+            }
+          }
+          if (j < nb) pair(src[j], j, 0);
+          acc += (double)p[0] + (double)p[1];
+          accx += (double)px[0] + (double)px[1];
+          accy += (double)py[0] + (double)py[1];
         }
-        for (; j < nb; j += G) pair(src[j], j, p0);
-        acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
         if (nhit) {
           // the source's kernel offset is already in csrc: take it out and
           // add the FP64 kernel unless the points coincide exactly (check)
@@ -816,32 +877,51 @@ __global__ void __launch_bounds__(TCH, EVAL_BLOCKS_PER_SM) k_evaluate_mx(KernelP
             const int q = __float_as_int(src[jj].w);
             const double qx = sx[q], qy = sy[q];
             exact -= kofs * tau[q];
-            if (!(check && x - qx == 0.0 && y - qy == 0.0)) exact += K64(qx, qy, x, y) * tau[q];
+            if (!(check && x - qx == 0.0 && y - qy == 0.0)) {
+              if constexpr (NOUT == 1)
+                exact += K64(qx, qy, x, y) * tau[q];
+              else
+                K64.grad(qx, qy, x, y, tau[q], exact, exact_x, exact_y);
+            }
           };
           if (nhit == 1) {
             fix(hj);
           } else {
             for (int jj = sub; jj < nb; jj += G) {
               const float4 q4 = src[jj];
-              const float dx = tx - q4.x, dy = ty - q4.y;
+              float dx = tx - q4.x, dy = ty - q4.y;
+              if constexpr (NOUT == 3) {
+                dx += tx_lo - src_lo[jj].x;
+                dy += ty_lo - src_lo[jj].y;
+              }
               if (fmaf(dy, dy, dx * dx) < 1.17549435e-38f) fix(jj);
             }
           }
         }
       }
     }
-    double u = acc + exact;
-    if (sub == 0) u += kofs * (D.csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
-    for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
-    if (G > 32) {
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
-      __syncthreads();
-      if (sub == 0) {
-        u = 0.0;
-        for (int w = 0; w < G / 32; ++w) u += red[(threadIdx.x >> 5) + w];
-      }
+    double r[NOUT];
+    r[0] = acc + exact;
+    if (sub == 0) r[0] += kofs * (D.csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
+    if constexpr (NOUT == 3) {
+      const double gs = KF32::kGradScale / (double)KF32::kScale * iw;
+      r[1] = accx * gs + exact_x;
+      r[2] = accy * gs + exact_y;
     }
-    if (valid && sub == 0) out[tperm[t0 + t]] = u;
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      double u = r[o];
+      for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
+      if (G > 32) {
+        if ((threadIdx.x & 31) == 0) red[o][threadIdx.x >> 5] = u;
+        __syncthreads();
+        if (sub == 0) {
+          u = 0.0;
+          for (int w = 0; w < G / 32; ++w) u += red[o][(threadIdx.x >> 5) + w];
+        }
+      }
+      if (valid && sub == 0) out[o * ld_out + tperm[t0 + t]] = u;
+    }
     if (threadIdx.x == 0) s_next = after;
     __syncthreads();  // D and src are rewritten by the next item
     item = nxt;
@@ -995,7 +1075,7 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
 void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *tsum,
                         const float *loc32, const double *lsum, const double *txs,
                         const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
-                        int check, double *out, cudaStream_t s) {
+                        int check, int nout, double *out, int64_t ld_out, cudaStream_t s) {
   if (m == 0) return;
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
@@ -1013,11 +1093,15 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
   FMMB_CUDA(cudaGetLastError());
   PhaseTimer timer(PH_EVAL, s);
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE:
-      k_evaluate_mx<LaplaceF32, LaplaceF64><<<148 * EVAL_BLOCKS_PER_SM, TCH, 0, s>>>(
-          a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
-          a.ops_dev, loc32, lsum, txs, tys, tperm, check, out, next_item.get());
+    case KERNEL_LAPLACE: {
+      auto kern = nout == 3 ? k_evaluate_mx<LaplaceF32, LaplaceF64, 3>
+                            : k_evaluate_mx<LaplaceF32, LaplaceF64, 1>;
+      const int per_sm = nout == 3 ? 6 : EVAL_BLOCKS_PER_SM;
+      kern<<<148 * per_sm, TCH, 0, s>>>(a.kp, a.neq, a.np, desc.get(), it.n_items.get(),
+                                        td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc32, lsum,
+                                        txs, tys, tperm, check, out, ld_out, next_item.get());
       break;
+    }
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
   FMMB_CUDA(cudaGetLastError());

@@ -27,6 +27,16 @@ struct LaplaceF64 {
     const double dx = tx - sx, dy = ty - sy;
     return -log(dx * dx + dy * dy) * (1.0 / (4.0 * M_PI));
   }
+  // potential and its gradient in the target position, times q, added to
+  // (u, ux, uy) (Gradient_Eval, examples/pure_kifmm_laplace_gradient.py:32-55)
+  __device__ __forceinline__ void grad(double sx, double sy, double tx, double ty, double q,
+                                       double &u, double &ux, double &uy) const {
+    const double dx = tx - sx, dy = ty - sy, d2 = dx * dx + dy * dy;
+    const double s = -(1.0 / (2.0 * M_PI)) / d2 * q;
+    u += -log(d2) * (1.0 / (4.0 * M_PI)) * q;
+    ux += s * dx;
+    uy += s * dy;
+  }
 };
 
 // log2 on the special-function unit, denormal inputs flushed to zero
@@ -59,6 +69,9 @@ struct LaplaceF32 {
     return lg2_ftz(dx * dx + dy * dy) * kScale;
   }
   __device__ __forceinline__ float radial(float d2) const { return lg2_ftz(d2); }
+  // gradient in the target position: kGradScale * (dx, dy) / d2 on width-scaled
+  // coordinates (times 1/w for absolute units)
+  static constexpr double kGradScale = -1.0 / (2.0 * M_PI);
   static double offset(double w, const KernelParams &) { return -std::log(w * w) / (4.0 * M_PI); }
 };
 

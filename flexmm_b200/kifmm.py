@@ -191,6 +191,8 @@ class KI_FMM:
             _lib.call("fmm_plan_bind", plan, m, self.helper.level_id(w))
         self._tree = None
         self._expanded = False
+        # named evaluators (kifmm2d FMM.__init__ registers 'potential_evaluation')
+        self._evaluators = {"potential_evaluation": "potential"}
 
     @property
     def tree(self):
@@ -209,6 +211,45 @@ class KI_FMM:
         if self.verbose:
             _torch().cuda.synchronize()
             print("....Time for expansions:        {:0.2f}".format(1000 * (time.time() - st)))
+
+    def register_evaluator(self, KAS1, KAS2, name, outputs):
+        """Name an evaluator (kifmm2d FMM.register_evaluator, flexmm/kifmm2d/scalar/fmm.py:172-173).
+
+        The reference compiles the user's pair of numba functions (L2T and
+        P2P forms) into its loops.  Here the device evaluators are built in
+        and the pair selects one by its output count: 1 output is the
+        potential, 3 outputs are the potential and its gradient in the target
+        position (u, du/dx, du/dy), as the reference's gradient example
+        defines them (examples/pure_kifmm_laplace_gradient.py:32-55)."""
+        if outputs == 1:
+            self._evaluators[name] = "potential"
+        elif outputs == 3:
+            self._evaluators[name] = "gradient"
+        else:
+            raise NotImplementedError("built-in evaluators have 1 (potential) or 3 (gradient) outputs")
+
+    def evaluate_to_points(self, x, y, name, check):
+        """Evaluator `name` at (x, y) -> [outputs, M] (flexmm/kifmm2d/scalar/fmm.py:178-199);
+        `check` skips sources that coincide with the target."""
+        if name not in self._evaluators:
+            raise KeyError(f"evaluator {name!r} is not registered; registered: {sorted(self._evaluators)}")
+        eid, nout = _lib.EVALUATORS[self._evaluators[name]]
+        torch = _torch()
+        if check and self._own_sources(x, y):
+            out = torch.empty((nout, self.N), dtype=torch.float64, device="cuda")
+            _lib.call("fmm_evaluate_sources_outputs", self._plan, eid, 1,
+                      ctypes.c_void_p(out.data_ptr()), self.N, _stream())
+            return _as_kind(out, "cuda" if x.is_cuda else "cpu", (nout, self.N))
+        xd, kind = _device_f64(x)
+        yd, _ = _device_f64(y)
+        if xd.numel() != yd.numel():
+            raise ValueError("x and y differ in length")
+        m = xd.numel()
+        out = torch.empty((nout, m), dtype=torch.float64, device="cuda")
+        _lib.call("fmm_evaluate_outputs", self._plan, eid, ctypes.c_void_p(xd.data_ptr()),
+                  ctypes.c_void_p(yd.data_ptr()), m, 1 if check else 0,
+                  ctypes.c_void_p(out.data_ptr()), m, _stream())
+        return _as_kind(out, kind, (nout, m))
 
     def _evaluate(self, x, y, check):
         torch = _torch()

@@ -107,6 +107,21 @@ int fmm_evaluate(fmm_plan *plan, const double *tx, const double *ty, int64_t m, 
  * holds them sorted by leaf.  Replaces FMM.source_evaluation(x, y) called on
  * the FMM's own sources (flexmm/flexmm2d/fmm.py:158-159, 162-176). */
 int fmm_evaluate_sources(fmm_plan *plan, int check, double *out, void *stream);
+
+/* Several outputs per point, as the reference's named evaluators
+ * (kifmm2d FMM.register_evaluator + evaluate_to_points,
+ * flexmm/kifmm2d/scalar/fmm.py:172-199, helpers.py:176-238):
+ *   FMM_EVAL_POTENTIAL  1 row:  u
+ *   FMM_EVAL_GRADIENT   3 rows: u, du/dx, du/dy (derivatives in the target
+ *                       position; examples/pure_kifmm_laplace_gradient.py:32-55)
+ * Row r of the result is out[r * ld_out .. r * ld_out + m), ld_out >= m. */
+#define FMM_EVAL_POTENTIAL 0
+#define FMM_EVAL_GRADIENT 1
+int fmm_evaluate_outputs(fmm_plan *plan, int evaluator, const double *tx, const double *ty,
+                         int64_t m, int check, double *out, int64_t ld_out, void *stream);
+/* The same at the plan's own source points (see fmm_evaluate_sources). */
+int fmm_evaluate_sources_outputs(fmm_plan *plan, int evaluator, int check, double *out,
+                                 int64_t ld_out, void *stream);
 int fmm_plan_destroy(fmm_plan *plan);
 /* Wait for the plan's work and report failures of it: FMM_ERR_CUDA when a
  * kernel stopped one of its bounded waits (the results are then invalid). */

@@ -30,3 +30,30 @@ void oracle_direct_laplace(const double *sx, const double *sy, const double *tau
         out[j] = acc;
     }
 }
+
+/* Laplace potential and its gradient in the target position, rows
+ * out[0..2][nt] = (u, du/dx, du/dy): the reference's Gradient_Eval
+ * (examples/pure_kifmm_laplace_gradient.py:32-55) summed over all sources,
+ * with the same coincidence skip (flexmm/kifmm2d/scalar/helpers.py:200-205). */
+void oracle_direct_laplace_grad(const double *sx, const double *sy, const double *tau,
+                                int64_t ns, const double *tx, const double *ty,
+                                int64_t nt, int check, double *out)
+{
+    const double c = 1.0 / (4.0 * M_PI), g = -1.0 / (2.0 * M_PI);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t j = 0; j < nt; ++j) {
+        double u = 0.0, ux = 0.0, uy = 0.0;
+        const double x = tx[j], y = ty[j];
+        for (int64_t i = 0; i < ns; ++i) {
+            double dx = x - sx[i], dy = y - sy[i];
+            if (check && dx == 0.0 && dy == 0.0) continue;
+            double d2 = dx * dx + dy * dy;
+            u += -log(d2) * c * tau[i];
+            ux += g * dx / d2 * tau[i];
+            uy += g * dy / d2 * tau[i];
+        }
+        out[j] = u;
+        out[nt + j] = ux;
+        out[2 * nt + j] = uy;
+    }
+}

@@ -26,6 +26,9 @@ def _load():
         f = _lib.oracle_direct_laplace
         f.argtypes = [dp, dp, dp, ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
         f.restype = None
+        g = _lib.oracle_direct_laplace_grad
+        g.argtypes = f.argtypes
+        g.restype = None
     return _lib
 
 
@@ -39,4 +42,14 @@ def direct_laplace(sx, sy, tau, tx, ty, check):
     out = np.empty(tx.size)
     lib.oracle_direct_laplace(_p(sx), _p(sy), _p(tau), sx.size, _p(tx), _p(ty), tx.size,
                               1 if check else 0, _p(out))
+    return out
+
+
+def direct_laplace_grad(sx, sy, tau, tx, ty, check):
+    """FP64 direct sum of the Laplace potential and its target gradient -> [3, nt]."""
+    lib = _load()
+    sx, sy, tau, tx, ty = (np.ascontiguousarray(a, dtype=np.float64) for a in (sx, sy, tau, tx, ty))
+    out = np.empty((3, tx.size))
+    lib.oracle_direct_laplace_grad(_p(sx), _p(sy), _p(tau), sx.size, _p(tx), _p(ty), tx.size,
+                                   1 if check else 0, _p(out))
     return out

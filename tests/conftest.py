@@ -17,8 +17,11 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
-def golden_cases():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+def golden_cases(gradient=False):
+    """Fixture names: potential cases, or (gradient=True) the grad_* cases
+    whose results are [3, n] rows (u, du/dx, du/dy)."""
+    names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    return [n for n in names if n.startswith("grad_") == gradient]
 
 
 def load_golden(name):

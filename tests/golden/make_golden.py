@@ -17,6 +17,12 @@ recipes (seeded numpy), the reference ``KI_FMM`` is built with a fresh
 * ``direct_src`` / ``direct_tgt`` FP64 direct sums at the sampled points
 * ``tree_sha``  sha256 of every canonical tree array of the reference tree
   (``tests/canon.py``), for cases small enough to canonicalise quickly
+
+Gradient cases (``grad_*``) run the reference's kifmm2d FMM with the
+gradient evaluator of examples/pure_kifmm_laplace_gradient.py
+(``register_evaluator(..., 'gradient', 3)`` + ``evaluate_to_points``) and store
+``src_val`` / ``tgt_val`` as [3, n] rows (u, du/dx, du/dy), with the FP64
+direct sums ``direct_src`` / ``direct_tgt`` likewise.
 """
 import hashlib
 import json
@@ -33,7 +39,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 
 from flexmm_b200 import workloads  # noqa: E402
 from oracle import refimport  # noqa: E402
-from oracle.direct import direct_laplace  # noqa: E402
+from oracle.direct import direct_laplace, direct_laplace_grad  # noqa: E402
 import canon  # noqa: E402
 
 
@@ -83,6 +89,12 @@ CASES = {
     "circle_20k_q24_nobbox": (dict(recipe="circle", seed=14, n=20000, n_grid=50, ncut=32, neq=24,
                                    bbox="none"), True),
     "duplicates_5k_q24": (dict(recipe="duplicates", seed=15, n=5000, n_grid=33, ncut=16, neq=24), True),
+    "grad_uniform_3k_q16": (dict(recipe="uniform", seed=16, n=3000, n_grid=41, ncut=16, neq=16,
+                                 gradient=True), True),
+    "grad_clustered_20k_q32": (dict(recipe="clustered", seed=17, n=20000, n_grid=64, ncut=32,
+                                    neq=32, gradient=True), True),
+    "grad_duplicates_5k_q24": (dict(recipe="duplicates", seed=18, n=5000, n_grid=33, ncut=16,
+                                    neq=24, gradient=True), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -137,6 +149,64 @@ def run_case(name, meta, ref):
           f"tgt {rel(ut[ti], dt):.2e}", flush=True)
 
 
+def run_gradient_case(name, meta, ref):
+    import numba
+    from flexmm.kifmm2d.scalar.fmm import FMM
+
+    # the reference example's kernels (examples/pure_kifmm_laplace_gradient.py:24-55)
+    @numba.njit(fastmath=True)
+    def Eval(sx, sy, tx, ty):
+        dx = tx - sx
+        dy = ty - sy
+        d2 = dx * dx + dy * dy
+        return -np.log(d2) / (4 * np.pi)
+
+    @numba.njit(fastmath=True)
+    def Gradient_Eval1(sx, sy, tx, ty, tau, extras):
+        dx = tx - sx
+        dy = ty - sy
+        d2 = dx * dx + dy * dy
+        id2 = 1.0 / d2
+        scale = -1.0 / (2 * np.pi)
+        return -np.log(d2) / (4 * np.pi) * tau, scale * dx * id2 * tau, scale * dy * id2 * tau
+
+    @numba.njit(fastmath=True)
+    def Gradient_Eval2(sx, sy, tx, ty, tau, extras):
+        dx = tx - sx
+        dy = ty - sy
+        d2 = dx * dx + dy * dy
+        id2 = 1.0 / d2
+        scale = -1.0 / (2 * np.pi)
+        return (-np.log(d2) / (4 * np.pi) * tau[0], scale * dx * id2 * tau[0],
+                scale * dy * id2 * tau[0])
+
+    d = case_inputs(meta)
+    t0 = time.time()
+    F = FMM(d["x"], d["y"], Eval, meta["ncut"], meta["neq"], bbox=d["bbox"])
+    F.build_expansions(d["tau"])
+    F.register_evaluator(Gradient_Eval1, Gradient_Eval2, "gradient", 3)
+    us = F.evaluate_to_points(d["x"], d["y"], "gradient", True)
+    ut = F.evaluate_to_points(d["tx"], d["ty"], "gradient", False)
+    t1 = time.time()
+    si = np.arange(d["x"].size)
+    ti = np.arange(d["tx"].size)
+    ds = direct_laplace_grad(d["x"], d["y"], d["tau"], d["x"], d["y"], True)
+    dt = direct_laplace_grad(d["x"], d["y"], d["tau"], d["tx"], d["ty"], False)
+    out = dict(
+        meta=json.dumps(meta),
+        inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),
+        bbox_used=np.array(F.bbox, dtype=np.float64),
+        levels=np.int64(F.tree.levels),
+        src_idx=si, src_val=us, tgt_idx=ti, tgt_val=ut,
+        direct_src=ds, direct_tgt=dt,
+    )
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"{name}: levels {F.tree.levels} ref {t1 - t0:.1f}s  err vs direct "
+          + " ".join(f"src[{r}] {rel(us[r], ds[r]):.2e} tgt[{r}] {rel(ut[r], dt[r]):.2e}" for r in range(3)),
+          flush=True)
+
+
 def main():
     only_small = len(sys.argv) > 1 and sys.argv[1] == "small"
     names = [a for a in sys.argv[1:] if a in CASES]
@@ -147,7 +217,7 @@ def main():
             continue
         if only_small and not small:
             continue
-        run_case(name, meta, ref)
+        (run_gradient_case if meta.get("gradient") else run_case)(name, meta, ref)
 
 
 if __name__ == "__main__":
