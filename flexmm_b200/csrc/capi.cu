@@ -1,6 +1,10 @@
 // C-ABI entry points (include/flexmm_b200.h): operator sets, plans, passes.
 #include <string.h>
 
+#include <algorithm>
+#include <cmath>
+
+#include <map>
 #include <mutex>
 
 #include <memory>
@@ -52,6 +56,77 @@ float tf32_rna(float x) {
 }
 
 int pad8(int n) { return (n + 7) & ~7; }
+
+// sqrt(x) e^x K_n(x), n = 0, 1, for x >= 1: trapezoidal rule on
+// int_0^inf exp(-2x sinh^2(t/2)) cosh^n(t) dt (exponent without cancellation;
+// step below the integrand's width 1/sqrt(x); summed from the small terms up)
+double bessel_g_host(int n, double x) {
+  const double h = std::min(1.0 / 16.0, 0.2 / std::sqrt(x));
+  const int m = (int)std::ceil(std::acosh(1.0 + 60.0 / x) / h);
+  double s = 0.0;
+  for (int i = m; i >= 1; --i) {
+    const double t = i * h, sh = std::sinh(0.5 * t);
+    s += std::exp(-2.0 * x * sh * sh) * (n ? std::cosh(t) : 1.0);
+  }
+  s += 0.5;  // t = 0
+  return std::sqrt(x) * h * s;
+}
+
+// Chebyshev coefficients of g_0, g_1 on the octaves [2^j, 2^(j+1)) (bessel.cuh)
+const std::vector<double> &bessel_table_host() {
+  static const std::vector<double> tab = [] {
+    std::vector<double> t(BESSEL_TABLE_DOUBLES);
+    const int N = BESSEL_NCHEB;
+    for (int n = 0; n < 2; ++n)
+      for (int j = 0; j < BESSEL_OCTAVES; ++j) {
+        const double a = std::ldexp(1.0, j);
+        double f[BESSEL_NCHEB];
+        for (int k = 0; k < N; ++k)
+          f[k] = bessel_g_host(n, 1.5 * a + 0.5 * a * std::cos(M_PI * (k + 0.5) / N));
+        for (int i = 0; i < N; ++i) {
+          double c = 0.0;
+          for (int k = 0; k < N; ++k) c += f[k] * std::cos(M_PI * i * (k + 0.5) / N);
+          t[(n * BESSEL_OCTAVES + j) * N + i] = (i == 0 ? 1.0 : 2.0) * c / N;
+        }
+      }
+    return t;
+  }();
+  return tab;
+}
+
+// the Bessel tables on the current device (uploaded once per device, kept
+// until exit)
+const double *bessel_table_device() {
+  static std::mutex mu;
+  static std::map<int, double *> per_device;
+  int dev = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  auto it = per_device.find(dev);
+  if (it != per_device.end()) return it->second;
+  const std::vector<double> &h = bessel_table_host();
+  double *d = nullptr;
+  FMMB_CUDA(cudaMalloc((void **)&d, h.size() * sizeof(double)));
+  FMMB_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  per_device[dev] = d;
+  return d;
+}
+
+bool kernel_known(int kernel_id) {
+  return kernel_id == KERNEL_LAPLACE || kernel_id == KERNEL_MOD_HELMHOLTZ;
+}
+
+// a kernel's device parameters: the caller's values plus the tables it reads
+KernelParams kernel_params(int kernel_id, const double *kparams) {
+  KernelParams kp{};
+  for (int i = 0; i < 4; ++i) kp.p[i] = kparams ? kparams[i] : 0.0;
+  kp.table = nullptr;
+  if (kernel_id == KERNEL_MOD_HELMHOLTZ) {
+    FMMB_CHECK(kp.p[0] > 0.0, ERR_INVALID_ARGUMENT, "modified Helmholtz needs k = kparams[0] > 0");
+    kp.table = bessel_table_device();
+  }
+  return kp;
+}
 
 bool kernel_scaled(int kernel_id) {
   switch (kernel_id) {
@@ -114,12 +189,13 @@ const char *fmm_last_error(void) { return g_last_error.c_str(); }
 int fmm_ops_create(int kernel_id, const double *kparams, int nequiv, fmm_ops **out) {
   return guarded([&] {
     FMMB_CHECK(out, ERR_INVALID_ARGUMENT, "out is NULL");
-    FMMB_CHECK(kernel_id == KERNEL_LAPLACE, ERR_UNSUPPORTED, "unknown kernel id");
+    FMMB_CHECK(kernel_known(kernel_id), ERR_UNSUPPORTED, "unknown kernel id");
     FMMB_CHECK(nequiv >= 1 && nequiv <= FMM_MAX_NEQUIV, ERR_INVALID_ARGUMENT,
                "nequiv must be in [1, 64]");
+    const KernelParams kp = kernel_params(kernel_id, kparams);
     auto *o = new fmm_ops();
     o->kernel_id = kernel_id;
-    for (int i = 0; i < 4; ++i) o->kp.p[i] = kparams ? kparams[i] : 0.0;
+    o->kp = kp;
     o->neq = nequiv;
     o->np = pad8(nequiv);
     *out = o;
@@ -339,6 +415,8 @@ int fmm_plan_set_precision(fmm_plan *p, int precision) {
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CHECK(precision == PREC_FP64 || precision == PREC_MIXED, ERR_INVALID_ARGUMENT,
                "precision must be FMM_PRECISION_FP64 or FMM_PRECISION_MIXED");
+    FMMB_CHECK(precision == PREC_FP64 || kernel_scaled(p->ops->kernel_id), ERR_UNSUPPORTED,
+               "the mixed form needs a scale-invariant kernel (Laplace)");
     p->precision = precision;
     p->have_expansions = false;
   });
@@ -550,13 +628,12 @@ int fmm_direct(int kernel_id, const double *kparams, const double *sx, const dou
                const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
                int check, double *out, void *stream) {
   return guarded([&] {
-    FMMB_CHECK(kernel_id == KERNEL_LAPLACE, ERR_UNSUPPORTED, "unknown kernel id");
+    FMMB_CHECK(kernel_known(kernel_id), ERR_UNSUPPORTED, "unknown kernel id");
     FMMB_CHECK(ns >= 0 && nt >= 0, ERR_INVALID_ARGUMENT, "negative size");
     if (nt == 0) return;
     FMMB_CHECK(tx && ty && out && (ns == 0 || (sx && sy && tau)), ERR_INVALID_ARGUMENT,
                "NULL argument");
-    KernelParams kp;
-    for (int i = 0; i < 4; ++i) kp.p[i] = kparams ? kparams[i] : 0.0;
+    const KernelParams kp = kernel_params(kernel_id, kparams);
     run_direct(kernel_id, kp, sx, sy, tau, ns, tx, ty, nt, check, out, (cudaStream_t)stream);
   });
 }

@@ -577,6 +577,7 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
 void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s) {
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: upward_impl<LaplaceF64>(a, tau_s, mult, s); break;
+    case KERNEL_MOD_HELMHOLTZ: upward_impl<ModHelmholtzF64>(a, tau_s, mult, s); break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
@@ -629,6 +630,10 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
     case KERNEL_LAPLACE:
       evaluate_impl<LaplaceF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out, ld_out, s);
       break;
+    case KERNEL_MOD_HELMHOLTZ:
+      evaluate_impl<ModHelmholtzF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
+                                     ld_out, s);
+      break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
@@ -642,6 +647,9 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
   switch (kernel_id) {
     case KERNEL_LAPLACE:
       k_direct<LaplaceF64><<<grid, 256, 0, s>>>(kp, sx, sy, tau, ns, tx, ty, nt, check, out);
+      break;
+    case KERNEL_MOD_HELMHOLTZ:
+      k_direct<ModHelmholtzF64><<<grid, 256, 0, s>>>(kp, sx, sy, tau, ns, tx, ty, nt, check, out);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

@@ -1,6 +1,7 @@
 // Device kernel functors, registered under the reference's example names.
 //
 //   Laplace_Eval: -log(|t-s|^2) / (4 pi)       examples/kifmm_laplace.py:24-29
+//   Modified_Helmholtz_Eval: K0(k |t-s|) / (2 pi)  examples/kifmm_modified_helmholtz.py:33-39
 //
 // A functor evaluates K(source, target) for source (sx, sy) and target
 // (tx, ty); the FMM kernels are templated on it, so the functor inlines into
@@ -11,14 +12,18 @@
 
 #include <cmath>
 
+#include "bessel.cuh"
 #include "common.cuh"
 
 namespace fmmb {
 
-enum KernelId : int { KERNEL_LAPLACE = 0 };
+enum KernelId : int { KERNEL_LAPLACE = 0, KERNEL_MOD_HELMHOLTZ = 1 };
 
+// the caller's parameters (p[0] = helmholtz k for the modified Helmholtz
+// kernel) and the device's Bessel tables (bessel.cuh)
 struct KernelParams {
   double p[4];
+  const double *table;
 };
 
 struct LaplaceF64 {
@@ -34,6 +39,31 @@ struct LaplaceF64 {
     const double dx = tx - sx, dy = ty - sy, d2 = dx * dx + dy * dy;
     const double s = -(1.0 / (2.0 * M_PI)) / d2 * q;
     u += -log(d2) * (1.0 / (4.0 * M_PI)) * q;
+    ux += s * dx;
+    uy += s * dy;
+  }
+};
+
+struct ModHelmholtzF64 {
+  double k;
+  const double *tab;
+  __host__ __device__ explicit ModHelmholtzF64(const KernelParams &kp) : k(kp.p[0]), tab(kp.table) {}
+  __device__ __forceinline__ double operator()(double sx, double sy, double tx, double ty) const {
+    const double dx = tx - sx, dy = ty - sy;
+    double k0, k1;
+    bessel_k01<false>(k * sqrt(dx * dx + dy * dy), tab, k0, k1);
+    return k0 * (1.0 / (2.0 * M_PI));
+  }
+  // potential and its gradient in the target position, times q:
+  // d/dt K0(k r) = -k K1(k r) (t - s) / r
+  // (examples/pure_kifmm_modified_helmholtz_gradient.py:45-70)
+  __device__ __forceinline__ void grad(double sx, double sy, double tx, double ty, double q,
+                                       double &u, double &ux, double &uy) const {
+    const double dx = tx - sx, dy = ty - sy, r = sqrt(dx * dx + dy * dy);
+    double k0, k1;
+    bessel_k01<true>(k * r, tab, k0, k1);
+    const double s = -k * k1 / r * (1.0 / (2.0 * M_PI)) * q;
+    u += k0 * (1.0 / (2.0 * M_PI)) * q;
     ux += s * dx;
     uy += s * dy;
   }

@@ -44,21 +44,56 @@ def _laplace_host(p, sx, sy, tx, ty):
     return -np.log(d2) / (4 * np.pi)
 
 
+def _mod_helmholtz_host(p, sx, sy, tx, ty):
+    # examples/kifmm_modified_helmholtz.py:33-39: K0(k d) / (2 pi)
+    from scipy.special import k0
+    dx = tx - sx
+    dy = ty - sy
+    return k0(p[0] * np.sqrt(dx * dx + dy * dy)) / (2 * np.pi)
+
+
 KERNEL_LAPLACE = 0
+KERNEL_MOD_HELMHOLTZ = 1
 
 
 def Laplace():
     return Kernel("Laplace_Eval", KERNEL_LAPLACE, (), _laplace_host)
 
 
-_BY_NAME = {"Laplace_Eval": Laplace, "Laplace": Laplace}
+def ModifiedHelmholtz(helmholtz_k):
+    """K0(k |t - s|) / (2 pi), k = helmholtz_k > 0."""
+    if not helmholtz_k > 0:
+        raise ValueError("helmholtz_k must be positive")
+    return Kernel("Modified_Helmholtz_Eval", KERNEL_MOD_HELMHOLTZ, (helmholtz_k,),
+                  _mod_helmholtz_host)
+
+
+_BY_NAME = {"Laplace_Eval": Laplace, "Laplace": Laplace,
+            "Modified_Helmholtz_Eval": ModifiedHelmholtz, "ModifiedHelmholtz": ModifiedHelmholtz}
+# parameters a reference-style kernel function reads from its module's globals
+_GLOBAL_PARAMS = {"Modified_Helmholtz_Eval": ("helmholtz_k",)}
+
+
+def _function_globals(fn):
+    fn = getattr(fn, "py_func", fn)  # numba dispatcher -> python function
+    return getattr(fn, "__globals__", {})
 
 
 def resolve(kernel_eval, **params):
-    """Map a Kernel, a registered name, or a function named like one to a Kernel."""
+    """Map a Kernel, a registered name, or a function named like one to a Kernel.
+
+    The reference's example kernels close over module globals (the modified
+    Helmholtz example reads ``helmholtz_k``); a function passed here supplies
+    such a parameter the same way unless it is given as a keyword."""
     if isinstance(kernel_eval, Kernel):
         return kernel_eval
     name = kernel_eval if isinstance(kernel_eval, str) else getattr(kernel_eval, "__name__", None)
     if name not in _BY_NAME:
         raise ValueError(f"kernel {name!r} is not registered; registered: {sorted(_BY_NAME)}")
+    for key in _GLOBAL_PARAMS.get(name, ()):
+        if key not in params:
+            g = _function_globals(kernel_eval) if not isinstance(kernel_eval, str) else {}
+            if key not in g:
+                raise ValueError(f"kernel {name!r} needs {key}= (or a module global {key})")
+            params[key] = float(g[key])
     return _BY_NAME[name](**params)

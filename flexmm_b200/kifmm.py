@@ -305,11 +305,11 @@ class KI_FMM:
         self._plan = None
 
 
-def direct_evaluation(kernel, sx, sy, tau, tx, ty, check=False):
+def direct_evaluation(kernel, sx, sy, tau, tx, ty, check=False, **kernel_params):
     """FP64 direct sum on the GPU: u(t) = sum_s K(s, t) tau_s, skipping
     coincident pairs when ``check`` (flexmm/flexmm2d/helpers.py:91-116)."""
     torch = _torch()
-    k = resolve(kernel)
+    k = resolve(kernel, **kernel_params)
     sxd, _ = _device_f64(sx)
     syd, _ = _device_f64(sy)
     td, _ = _device_f64(tau)

@@ -53,3 +53,40 @@ def direct_laplace_grad(sx, sy, tau, tx, ty, check):
     lib.oracle_direct_laplace_grad(_p(sx), _p(sy), _p(tau), sx.size, _p(tx), _p(ty), tx.size,
                                    1 if check else 0, _p(out))
     return out
+
+
+def _mh_pairs(sx, sy, tau, tx, ty, k, check, grad):
+    """Chunked numpy/scipy direct sum of K0(k r)/(2 pi) (and its target gradient)."""
+    from scipy.special import k0, k1
+    nt = tx.size
+    out = np.zeros((3 if grad else 1, nt))
+    step = max(1, 4_000_000 // max(sx.size, 1))
+    for a in range(0, nt, step):
+        b = min(nt, a + step)
+        dx = tx[a:b, None] - sx[None, :]
+        dy = ty[a:b, None] - sy[None, :]
+        r = np.sqrt(dx * dx + dy * dy)
+        skip = (dx == 0) & (dy == 0) if check else np.zeros(r.shape, dtype=bool)
+        rs = np.where(skip, 1.0, r)
+        w = np.where(skip, 0.0, tau[None, :])
+        out[0, a:b] = (k0(k * rs) / (2 * np.pi) * w).sum(1)
+        if grad:
+            s = -k * k1(k * rs) / rs / (2 * np.pi) * w
+            out[1, a:b] = (s * dx).sum(1)
+            out[2, a:b] = (s * dy).sum(1)
+    return out
+
+
+def direct_mod_helmholtz(sx, sy, tau, tx, ty, k, check):
+    """FP64 direct sum of the modified Helmholtz kernel K0(k r)/(2 pi)
+    (examples/kifmm_modified_helmholtz.py:33-39), skipping coincident pairs
+    when ``check``; K0 from scipy.special (test infrastructure only)."""
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tau, tx, ty)]
+    return _mh_pairs(*a, float(k), check, False)[0]
+
+
+def direct_mod_helmholtz_grad(sx, sy, tau, tx, ty, k, check):
+    """Potential and target gradient of the modified Helmholtz kernel -> [3, nt]
+    (examples/pure_kifmm_modified_helmholtz_gradient.py:45-70)."""
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tau, tx, ty)]
+    return _mh_pairs(*a, float(k), check, True)

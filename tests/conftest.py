@@ -50,3 +50,22 @@ def built_lib():
     """Path of the built CUDA library (built here with nvcc when missing)."""
     from flexmm_b200 import build
     return build.build()
+
+
+def kernel_of(meta):
+    """(registered kernel name, kernel keyword parameters) of a golden case."""
+    if meta.get("kernel", "laplace") == "laplace":
+        return "Laplace_Eval", {}
+    return "Modified_Helmholtz_Eval", {"helmholtz_k": meta["k"]}
+
+
+def oracle_kernel(meta):
+    from oracle.kernels import laplace, mod_helmholtz
+    return laplace if meta.get("kernel", "laplace") == "laplace" else mod_helmholtz(meta["k"])
+
+
+def oracle_direct(meta, sx, sy, tau, tx, ty, check):
+    from oracle.direct import direct_laplace, direct_mod_helmholtz
+    if meta.get("kernel", "laplace") == "laplace":
+        return direct_laplace(sx, sy, tau, tx, ty, check)
+    return direct_mod_helmholtz(sx, sy, tau, tx, ty, meta["k"], check)

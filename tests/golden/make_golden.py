@@ -39,7 +39,8 @@ sys.path.insert(0, os.path.dirname(HERE))
 
 from flexmm_b200 import workloads  # noqa: E402
 from oracle import refimport  # noqa: E402
-from oracle.direct import direct_laplace, direct_laplace_grad  # noqa: E402
+from oracle.direct import (direct_laplace, direct_laplace_grad, direct_mod_helmholtz,  # noqa: E402
+                           direct_mod_helmholtz_grad)
 import canon  # noqa: E402
 
 
@@ -95,6 +96,14 @@ CASES = {
                                     neq=32, gradient=True), True),
     "grad_duplicates_5k_q24": (dict(recipe="duplicates", seed=18, n=5000, n_grid=33, ncut=16,
                                     neq=24, gradient=True), True),
+    "mh_uniform_3k_q24_k5": (dict(recipe="uniform", seed=19, n=3000, n_grid=41, ncut=16, neq=24,
+                                  kernel="mh", k=5.0), True),
+    "mh_circle_20k_q40_k10": (dict(recipe="circle", seed=20, n=20000, n_grid=50, ncut=64, neq=40,
+                                   kernel="mh", k=10.0, bbox="none"), True),
+    "mh_duplicates_5k_q24_k5": (dict(recipe="duplicates", seed=21, n=5000, n_grid=33, ncut=16,
+                                     neq=24, kernel="mh", k=5.0), True),
+    "grad_mh_clustered_20k_q32_k5": (dict(recipe="clustered", seed=22, n=20000, n_grid=64, ncut=32,
+                                          neq=32, kernel="mh", k=5.0, gradient=True), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -104,16 +113,52 @@ CASES = {
 }
 
 
-def run_case(name, meta, ref):
-    import numba
-    from flexmm.flexmm2d.kifmm import KI_FMM, KI_Helper
+def scipy_bessel():
+    """numba-callable K0, K1 from scipy.special.cython_special (the reference's
+    examples tabulate the same functions with function_generator, which is
+    not installed)."""
+    import ctypes
+    from numba.extending import get_cython_function_address
+    f = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_double)
+    return (f(get_cython_function_address("scipy.special.cython_special", "k0")),
+            f(get_cython_function_address("scipy.special.cython_special", "k1")))
 
+
+def reference_kernel(meta):
+    """The reference example's scalar kernel for the case (numba)."""
+    import numba
+    if meta.get("kernel", "laplace") == "laplace":
+        @numba.njit(fastmath=True)
+        def Laplace_Eval(sx, sy, tx, ty):
+            dx = tx - sx
+            dy = ty - sy
+            d2 = dx**2 + dy**2
+            return -np.log(d2) / (4 * np.pi)
+        return Laplace_Eval
+    k0c, _ = scipy_bessel()
+    hk = float(meta["k"])
+
+    # examples/kifmm_modified_helmholtz.py:33-39
     @numba.njit(fastmath=True)
-    def Laplace_Eval(sx, sy, tx, ty):
+    def Modified_Helmholtz_Eval(sx, sy, tx, ty):
         dx = tx - sx
         dy = ty - sy
-        d2 = dx**2 + dy**2
-        return -np.log(d2) / (4 * np.pi)
+        d = np.sqrt(dx**2 + dy**2)
+        return k0c(hk * d) / (2 * np.pi)
+    return Modified_Helmholtz_Eval
+
+
+def direct(meta, grad, *args):
+    if meta.get("kernel", "laplace") == "laplace":
+        return (direct_laplace_grad if grad else direct_laplace)(*args)
+    sx, sy, tau, tx, ty, check = args
+    f = direct_mod_helmholtz_grad if grad else direct_mod_helmholtz
+    return f(sx, sy, tau, tx, ty, meta["k"], check)
+
+
+def run_case(name, meta, ref):
+    from flexmm.flexmm2d.kifmm import KI_FMM, KI_Helper
+    Laplace_Eval = reference_kernel(meta)
 
     d = case_inputs(meta)
     t0 = time.time()
@@ -130,8 +175,8 @@ def run_case(name, meta, ref):
     else:
         si = np.arange(d["x"].size)
         ti = np.arange(d["tx"].size)
-    ds = direct_laplace(d["x"], d["y"], d["tau"], d["x"][si], d["y"][si], True)
-    dt = direct_laplace(d["x"], d["y"], d["tau"], d["tx"][ti], d["ty"][ti], False)
+    ds = direct(meta, False, d["x"], d["y"], d["tau"], d["x"][si], d["y"][si], True)
+    dt = direct(meta, False, d["x"], d["y"], d["tau"], d["tx"][ti], d["ty"][ti], False)
     out = dict(
         meta=json.dumps(meta),
         inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),
@@ -153,32 +198,49 @@ def run_gradient_case(name, meta, ref):
     import numba
     from flexmm.kifmm2d.scalar.fmm import FMM
 
-    # the reference example's kernels (examples/pure_kifmm_laplace_gradient.py:24-55)
-    @numba.njit(fastmath=True)
-    def Eval(sx, sy, tx, ty):
-        dx = tx - sx
-        dy = ty - sy
-        d2 = dx * dx + dy * dy
-        return -np.log(d2) / (4 * np.pi)
+    Eval = reference_kernel(meta)
+    if meta.get("kernel", "laplace") == "laplace":
+        # examples/pure_kifmm_laplace_gradient.py:32-55
+        @numba.njit(fastmath=True)
+        def Gradient_Eval1(sx, sy, tx, ty, tau, extras):
+            dx = tx - sx
+            dy = ty - sy
+            d2 = dx * dx + dy * dy
+            id2 = 1.0 / d2
+            scale = -1.0 / (2 * np.pi)
+            return -np.log(d2) / (4 * np.pi) * tau, scale * dx * id2 * tau, scale * dy * id2 * tau
 
-    @numba.njit(fastmath=True)
-    def Gradient_Eval1(sx, sy, tx, ty, tau, extras):
-        dx = tx - sx
-        dy = ty - sy
-        d2 = dx * dx + dy * dy
-        id2 = 1.0 / d2
-        scale = -1.0 / (2 * np.pi)
-        return -np.log(d2) / (4 * np.pi) * tau, scale * dx * id2 * tau, scale * dy * id2 * tau
+        @numba.njit(fastmath=True)
+        def Gradient_Eval2(sx, sy, tx, ty, tau, extras):
+            dx = tx - sx
+            dy = ty - sy
+            d2 = dx * dx + dy * dy
+            id2 = 1.0 / d2
+            scale = -1.0 / (2 * np.pi)
+            return (-np.log(d2) / (4 * np.pi) * tau[0], scale * dx * id2 * tau[0],
+                    scale * dy * id2 * tau[0])
+    else:
+        k0c, k1c = scipy_bessel()
+        hk = float(meta["k"])
 
-    @numba.njit(fastmath=True)
-    def Gradient_Eval2(sx, sy, tx, ty, tau, extras):
-        dx = tx - sx
-        dy = ty - sy
-        d2 = dx * dx + dy * dy
-        id2 = 1.0 / d2
-        scale = -1.0 / (2 * np.pi)
-        return (-np.log(d2) / (4 * np.pi) * tau[0], scale * dx * id2 * tau[0],
-                scale * dy * id2 * tau[0])
+        # examples/pure_kifmm_modified_helmholtz_gradient.py:45-70
+        @numba.njit(fastmath=True)
+        def Gradient_Eval1(sx, sy, tx, ty, tau, extras):
+            dx = tx - sx
+            dy = ty - sy
+            d = np.sqrt(dx**2 + dy**2)
+            scale = 1.0 / (2 * np.pi)
+            g = -hk * k1c(hk * d) * scale / d * tau
+            return k0c(hk * d) * scale * tau, dx * g, dy * g
+
+        @numba.njit(fastmath=True)
+        def Gradient_Eval2(sx, sy, tx, ty, tau, extras):
+            dx = tx - sx
+            dy = ty - sy
+            d = np.sqrt(dx**2 + dy**2)
+            scale = 1.0 / (2 * np.pi)
+            g = -hk * k1c(hk * d) * scale / d * tau[0]
+            return k0c(hk * d) * scale * tau[0], dx * g, dy * g
 
     d = case_inputs(meta)
     t0 = time.time()
@@ -190,8 +252,8 @@ def run_gradient_case(name, meta, ref):
     t1 = time.time()
     si = np.arange(d["x"].size)
     ti = np.arange(d["tx"].size)
-    ds = direct_laplace_grad(d["x"], d["y"], d["tau"], d["x"], d["y"], True)
-    dt = direct_laplace_grad(d["x"], d["y"], d["tau"], d["tx"], d["ty"], False)
+    ds = direct(meta, True, d["x"], d["y"], d["tau"], d["x"], d["y"], True)
+    dt = direct(meta, True, d["x"], d["y"], d["tau"], d["tx"], d["ty"], False)
     out = dict(
         meta=json.dumps(meta),
         inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),

@@ -6,7 +6,7 @@ on the same inputs; the tree equal to the reference's box for box.
 import numpy as np
 import pytest
 
-from conftest import golden_cases, golden_inputs, load_golden, rel_l2
+from conftest import golden_cases, golden_inputs, kernel_of, load_golden, oracle_direct, rel_l2
 import canon
 
 pytestmark = pytest.mark.gpu
@@ -16,7 +16,8 @@ PARITY = 1e-12
 
 def _fmm(d, meta, helper=None):
     from flexmm_b200 import KI_FMM, KI_Helper
-    return KI_FMM(d["x"], d["y"], "Laplace_Eval", meta["ncut"], meta["neq"], bbox=d["bbox"],
+    name, params = kernel_of(meta)
+    return KI_FMM(d["x"], d["y"], name, meta["ncut"], meta["neq"], bbox=d["bbox"], **params,
                   helper=helper if helper is not None else KI_Helper())
 
 
@@ -153,3 +154,32 @@ def test_own_source_evaluation_equals_general_path(built_lib, precision):
         assert rel_l2(u_own[g["src_idx"]], g["src_val"]) < PARITY
     x.add_(0.0)
     assert not F._own_sources(x, y)
+
+
+@pytest.mark.parametrize("k", [0.5, 5.0, 10.0, 200.0])
+def test_mod_helmholtz_direct_sum_matches_scipy(built_lib, k):
+    """The device K0 (series below 1, per-octave Chebyshev tables above) in the
+    FP64 direct sum, against scipy's K0, with k r spanning 1e-7 .. ~600."""
+    from flexmm_b200 import direct_evaluation
+    from oracle.direct import direct_mod_helmholtz
+    rng = np.random.default_rng(int(k * 10))
+    r = np.geomspace(1e-7, 600.0, 3000)  # k * distance from a fixed source at 0
+    th = rng.uniform(0, 2 * np.pi, r.size)
+    sx, sy, tau = np.zeros(1), np.zeros(1), np.ones(1)
+    tx, ty = r * np.cos(th) / k, r * np.sin(th) / k
+    got = direct_evaluation("Modified_Helmholtz_Eval", sx, sy, tau, tx, ty, helmholtz_k=k)
+    ref = direct_mod_helmholtz(sx, sy, tau, tx, ty, k, False)
+    nz = ref > 1e-300
+    # K0(x) has relative condition number ~x: one rounding of the distance
+    # (the device contracts dx*dx + dy*dy into an FMA) moves it by ~x * 1e-16
+    assert np.max(np.abs(got[nz] / ref[nz] - 1) / (1.0 + r[nz])) < 2e-14
+    assert np.all(np.abs(got[~nz]) < 1e-290)
+
+
+def test_mixed_form_rejects_non_scale_invariant_kernel(built_lib):
+    from flexmm_b200 import KI_FMM, KI_Helper
+    rng = np.random.default_rng(5)
+    x, y = rng.uniform(-1, 1, 2000), rng.uniform(-1, 1, 2000)
+    with pytest.raises(RuntimeError, match="scale-invariant"):
+        KI_FMM(x, y, "Modified_Helmholtz_Eval", 32, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper(),
+               precision="mixed", helmholtz_k=5.0)
