@@ -41,11 +41,24 @@ class LevelOps(ctypes.Structure):
     ]
 
 
+class BBLevelOps(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_double),
+        ("m2l_rank", _ip),
+        ("m2l_a", ctypes.POINTER(_dp)),
+        ("m2l_b", ctypes.POINTER(_dp)),
+    ]
+
+
+BB_MAX_P = 16
+
 # (name, restype, argtypes) of every exported entry point
 SIGNATURES = [
     ("fmm_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("fmm_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(LevelOps), _ip]),
     ("fmm_ops_destroy", ctypes.c_int, [_vp]),
+    ("fmm_bb_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.POINTER(_vp)]),
+    ("fmm_bb_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(BBLevelOps), _ip]),
     ("fmm_plan_create", ctypes.c_int,
      [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _dp, _vp, ctypes.POINTER(_vp)]),
     ("fmm_plan_info", ctypes.c_int, [_vp, _ip, _dp, _ip]),

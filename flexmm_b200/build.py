@@ -23,6 +23,10 @@ NVCC_FLAGS = [
 ]
 
 
+# cuBLAS for the black-box FMM's translation GEMMs
+LINK = ["-lcublas", "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
+
+
 def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
@@ -45,7 +49,7 @@ def build(force=False, verbose=False):
     os.makedirs(OUT_DIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
     tmp = LIB + ".tmp"
-    cmd = [nvcc] + NVCC_FLAGS + ["-I", INCLUDE] + sources() + ["-o", tmp]
+    cmd = [nvcc] + NVCC_FLAGS + ["-I", INCLUDE] + sources() + ["-o", tmp] + LINK
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

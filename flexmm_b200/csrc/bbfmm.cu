@@ -1,0 +1,425 @@
+// Black-box (Chebyshev) FMM passes in FP64 (flexmm/flexmm2d/bbfmm.py).
+//
+// The expansions of a box are p x p Chebyshev coefficients on the box scaled
+// to [-1, 1]^2 (NQ = p^2, rows padded to np):
+//  * S2M: Chebyshev moments of the box's sources,
+//    M[a p + b] = sum_j T_a(x_j) T_b(y_j) tau_j (anterpolate2, bbfmm.py:11-24,
+//    source2pMs, bbfmm.py:186-196); no check-to-equivalent step;
+//  * M2M / L2L: the level-independent M2MC [NQ x 4NQ] and its transpose
+//    (bbfmm.py:145-161) on the contiguous child rows of each parent group;
+//  * M2L: per level and offset VI K VI^T (bbfmm.py:101-122), the 40 offsets
+//    of a level applied as ONE GEMM over the offset-concatenated operator
+//    [NQ x 40 NQ] and a gathered [targets x 40 NQ] block (a missing source
+//    is a zero block);
+//  * L2T: the local coefficients evaluated as a 2-D Chebyshev series
+//    (chebeval2d1, bbfmm.py:25-31, L2targets, bbfmm.py:198-210);
+//  * P2P: the same colleague sweep as the KIFMM evaluation.
+// The GEMMs are cuBLAS DGEMMs on the plan's stream; gathers, scatters,
+// moments and evaluation are the kernels below.
+#include <cublas_v2.h>
+
+#include <algorithm>
+#include <string>
+
+#include "fmm.cuh"
+#include "timing.cuh"
+
+namespace fmmb {
+namespace {
+
+constexpr int BB_MAX_P = 16;
+constexpr int TCH_BB = 128;   // evaluation threads per work item
+constexpr int SMAX_BB = 1024;  // sources staged per evaluation pass
+
+#define FMMB_BLAS(call)                                                                     \
+  do {                                                                                      \
+    cublasStatus_t st_ = (call);                                                            \
+    if (st_ != CUBLAS_STATUS_SUCCESS)                                                       \
+      throw Error(ERR_CUDA, std::string("cuBLAS error ") + std::to_string(int(st_)) + " in " \
+                                + #call);                                                   \
+  } while (0)
+
+__device__ __forceinline__ int bb_node_level(const int *__restrict__ off, int L, int g) {
+  int lo = 0, hi = L;  // largest l with off[l] <= g
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// 2 / width per level: maps a box to [-1, 1]^2 (width_adj, bbfmm.py:122)
+struct BBScale {
+  double inv_hw[FMM_MAX_LEVELS_DEV];
+};
+
+// S2M moments, one warp per S2M node; lane owns outputs q = lane + 32 k
+__global__ void __launch_bounds__(128) k_bb_s2m(int p, int np, int L, BBScale sc,
+                                                const int *__restrict__ off,
+                                                const int *__restrict__ uplist,
+                                                const int *__restrict__ n_up_ptr,
+                                                const int *__restrict__ bot,
+                                                const int *__restrict__ top,
+                                                const double *__restrict__ xmid,
+                                                const double *__restrict__ ymid,
+                                                const double *__restrict__ sx,
+                                                const double *__restrict__ sy,
+                                                const double *__restrict__ tau,
+                                                double *__restrict__ mult) {
+  __shared__ double Tx[4][32][BB_MAX_P], Ty[4][32][BB_MAX_P], tw[4][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_up = *n_up_ptr, nq = p * p;
+  int qa[8], qb[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int q = lane + 32 * k;
+    qa[k] = q < nq ? q / p : 0;
+    qb[k] = q < nq ? q % p : 0;
+  }
+  for (int i = blockIdx.x * 4 + warp; i < n_up; i += gridDim.x * 4) {
+    const int g = uplist[i];
+    const double a = sc.inv_hw[bb_node_level(off, L, g)];
+    const double cx = xmid[g], cy = ymid[g];
+    const int b = bot[g], e = top[g];
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+    for (int j0 = b; j0 < e; j0 += 32) {
+      const int nj = min(32, e - j0);
+      if (lane < nj) {
+        const double x = (sx[j0 + lane] - cx) * a, y = (sy[j0 + lane] - cy) * a;
+        double t0 = 1.0, t1 = x, u0 = 1.0, u1 = y;
+        Tx[warp][lane][0] = 1.0;
+        Ty[warp][lane][0] = 1.0;
+        for (int n = 1; n < p; ++n) {
+          Tx[warp][lane][n] = t1;
+          Ty[warp][lane][n] = u1;
+          const double t2 = 2.0 * x * t1 - t0, u2 = 2.0 * y * u1 - u0;
+          t0 = t1;
+          t1 = t2;
+          u0 = u1;
+          u1 = u2;
+        }
+        tw[warp][lane] = tau[j0 + lane];
+      }
+      __syncwarp();
+      for (int jj = 0; jj < nj; ++jj) {
+        const double t = tw[warp][jj];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (lane + 32 * k < nq) acc[k] = fma(Tx[warp][jj][qa[k]] * Ty[warp][jj][qb[k]], t, acc[k]);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int q = lane + 32 * k;
+      if (q < np) mult[(size_t)g * np + q] = q < nq ? acc[k] : 0.0;
+    }
+  }
+}
+
+// rows[e] -> dst row node(e) = parent[c_first + 4 e]  (M2M results to parent rows)
+__global__ void k_bb_to_parents(int n_groups, int np, int c_first, const int *__restrict__ parent,
+                                const double *__restrict__ rows, double *__restrict__ dst) {
+  const int64_t total = (int64_t)n_groups * np;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int e = int(i / np), q = int(i - (int64_t)e * np);
+    dst[(size_t)parent[c_first + 4 * e] * np + q] = rows[i];
+  }
+}
+
+// M2L gather of a level: row 4 g + c (node rg[g] + c) holds, for each offset
+// o, the source multipole il[node][o] (zeros if none) at columns o np .. o np + np
+__global__ void k_bb_m2l_gather(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
+                                const int *__restrict__ il, const double *__restrict__ mult,
+                                double *__restrict__ sbig) {
+  const int64_t rowlen = (int64_t)N_OFFSETS * np;
+  const int64_t total = (int64_t)n_groups * 4 * rowlen;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = i / rowlen;
+    const int col = int(i - row * rowlen), o = col / np, q = col - o * np;
+    const int node = rg[rg_lo + int(row >> 2)] + int(row & 3);
+    const int s = il[(size_t)node * N_OFFSETS + o];
+    sbig[i] = s >= 0 ? mult[(size_t)s * np + q] : 0.0;
+  }
+}
+
+// ple[node(row)] += y[row]
+__global__ void k_bb_add_rows(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
+                              const double *__restrict__ y, double *__restrict__ ple) {
+  const int64_t total = (int64_t)n_groups * 4 * np;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = i / np;
+    const int q = int(i - row * np);
+    const int node = rg[rg_lo + int(row >> 2)] + int(row & 3);
+    ple[(size_t)node * np + q] += y[i];
+  }
+}
+
+// L2L gather: the parent local of every real group of a level
+__global__ void k_bb_parent_locals(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
+                                   const int *__restrict__ parent, const double *__restrict__ ple,
+                                   double *__restrict__ lp) {
+  const int64_t total = (int64_t)n_groups * np;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int g = int(i / np), q = int(i - (int64_t)g * np);
+    lp[i] = ple[(size_t)parent[rg[rg_lo + g]] * np + q];
+  }
+}
+
+// L2L scatter: the 4 children of group g are the consecutive rows rg[g] .. rg[g] + 3
+__global__ void k_bb_add_children(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
+                                  const double *__restrict__ c, double *__restrict__ ple) {
+  const int64_t rowlen = 4 * (int64_t)np;
+  const int64_t total = (int64_t)n_groups * rowlen;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int g = int(i / rowlen);
+    const int64_t k = i - (int64_t)g * rowlen;
+    ple[(size_t)rg[rg_lo + g] * np + k] += c[i];
+  }
+}
+
+// Evaluation: L2T as a 2-D Chebyshev series of the leaf's local coefficients,
+// P2P over the colleagues (as k_evaluate).  One work item = (leaf, up to 128
+// of its targets); G threads share a target.
+template <class KF>
+__global__ void __launch_bounds__(TCH_BB) k_bb_evaluate(KernelParams kp, int p, int np, BBScale sc,
+                                                        const int4 *__restrict__ items,
+                                                        const int *__restrict__ n_items_ptr,
+                                                        const int *__restrict__ coll,
+                                                        const int *__restrict__ bot,
+                                                        const int *__restrict__ top,
+                                                        const double *__restrict__ xmid,
+                                                        const double *__restrict__ ymid,
+                                                        const double *__restrict__ sx,
+                                                        const double *__restrict__ sy,
+                                                        const double *__restrict__ tau,
+                                                        const double *__restrict__ loc,
+                                                        const double *__restrict__ txs,
+                                                        const double *__restrict__ tys,
+                                                        const int *__restrict__ tperm, int check,
+                                                        double *__restrict__ out) {
+  __shared__ double ssx[SMAX_BB], ssy[SMAX_BB], stau[SMAX_BB];
+  __shared__ int rb[9], rs[10];
+  __shared__ double red[TCH_BB / 32];
+  const KF K(kp);
+  const int n_items = *n_items_ptr;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int4 it = items[item];
+    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
+    int G = 1;
+    while (2 * G * cnt <= TCH_BB) G *= 2;
+    const int t = threadIdx.x / G, sub = threadIdx.x % G;
+    const bool valid = t < cnt;
+    const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
+    if (threadIdx.x < 9) {
+      const int cg = coll[(size_t)g * 9 + threadIdx.x];
+      rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
+      rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
+    }
+    if (threadIdx.x == 0) rs[0] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
+    double u = 0.0;
+    if (lev >= 2 && valid) {
+      // sum_a T_a(x) sum_b c[a p + b] T_b(y), rows a split over the G threads
+      const double a = sc.inv_hw[lev];
+      const double xh = (x - xmid[g]) * a, yh = (y - ymid[g]) * a;
+      double ty[BB_MAX_P];
+      ty[0] = 1.0;
+      ty[1] = yh;
+#pragma unroll
+      for (int b = 2; b < BB_MAX_P; ++b) ty[b] = 2.0 * yh * ty[b - 1] - ty[b - 2];
+      const double *cr = loc + (size_t)g * np;
+      double tp = 1.0, tc = xh;  // T_{ar-1}, T_ar as ar advances
+      for (int ar = 0; ar < p; ++ar) {
+        const double tx = ar == 0 ? 1.0 : tc;
+        if (ar % G == sub) {
+          double s = 0.0;
+#pragma unroll
+          for (int b = 0; b < BB_MAX_P; ++b)
+            if (b < p) s = fma(__ldg(cr + ar * p + b), ty[b], s);
+          u = fma(tx, s, u);
+        }
+        if (ar >= 1) {
+          const double tn = 2.0 * xh * tc - tp;
+          tp = tc;
+          tc = tn;
+        }
+      }
+    }
+    __syncthreads();
+    auto pair = [&](int j) -> double {
+      const double qx = ssx[j], qy = ssy[j];
+      const double v = K(qx, qy, x, y) * stau[j];
+      return (check && x - qx == 0.0 && y - qy == 0.0) ? 0.0 : v;
+    };
+    const int ns = rs[9];
+    double u1 = 0.0, u2 = 0.0, u3 = 0.0;
+    for (int base = 0; base < ns; base += SMAX_BB) {
+      const int nb = min(SMAX_BB, ns - base);
+      for (int i = threadIdx.x; i < nb; i += TCH_BB) {
+        const int idx = base + i;
+        int c = 0;
+        while (idx >= rs[c + 1]) ++c;
+        const int j = rb[c] + (idx - rs[c]);
+        ssx[i] = sx[j];
+        ssy[i] = sy[j];
+        stau[i] = tau[j];
+      }
+      __syncthreads();
+      if (valid) {
+        int j = sub;
+        for (; j + 3 * G < nb; j += 4 * G) {
+          u += pair(j);
+          u1 += pair(j + G);
+          u2 += pair(j + 2 * G);
+          u3 += pair(j + 3 * G);
+        }
+        for (; j < nb; j += G) u += pair(j);
+      }
+      __syncthreads();
+    }
+    u = (u + u1) + (u2 + u3);
+    for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
+    if (G > 32) {
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
+      __syncthreads();
+      if (sub == 0) {
+        u = 0.0;
+        for (int w = 0; w < G / 32; ++w) u += red[(threadIdx.x >> 5) + w];
+      }
+    }
+    if (valid && sub == 0) out[tperm[t0 + t]] = u;
+    __syncthreads();
+  }
+}
+
+BBScale bb_scale(const TreeHost &th) {
+  BBScale sc{};
+  for (int m = 0; m < th.L && m < FMM_MAX_LEVELS_DEV; ++m) sc.inv_hw[m] = 2.0 / th.width[m];
+  return sc;
+}
+
+}  // namespace
+
+void run_bb_upward(const BBArgs &b, const double *tau_s, double *mult, cudaStream_t s) {
+  const TreeHost &th = *b.th;
+  const TreeDev &td = *b.td;
+  if (th.L < 3) return;
+  FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
+  const int np = b.np;
+  const BBScale sc = bb_scale(th);
+  PhaseTimer timer(PH_UPWARD, s);
+  k_bb_s2m<<<148 * 8, 128, 0, s>>>(b.p, np, th.L, sc, td.dev_off.get(), td.uplist.get(),
+                                   td.n_up.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+                                   td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, mult);
+  FMMB_CUDA(cudaGetLastError());
+  int max_groups = 0;
+  for (int m = th.L - 2; m >= 2; --m)
+    max_groups = std::max(max_groups, (th.off[m + 2] - th.off[m + 1]) / 4);
+  if (max_groups == 0) return;
+  DevBuf<double> rows;
+  rows.alloc((size_t)max_groups * np, s);
+  FMMB_BLAS(cublasSetStream(b.blas, s));
+  const double one = 1.0, zero = 0.0;
+  for (int m = th.L - 2; m >= 2; --m) {
+    const int c_first = th.off[m + 1];
+    const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
+    if (n_groups == 0) continue;
+    // rows[e] = M2MC . (children of group e): column-major rows^T (np x n) =
+    // M2MC (np x 4np) . children^T (4np x n); M2MC row-major = its transpose column-major
+    FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n_groups, 4 * np, &one, b.m2mc,
+                          4 * np, mult + (size_t)c_first * np, 4 * np, &zero, rows.get(), np));
+    k_bb_to_parents<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
+        n_groups, np, c_first, td.parent.get(), rows.get(), mult);
+    FMMB_CUDA(cudaGetLastError());
+  }
+}
+
+void run_bb_downward(const BBArgs &b, const double *mult, double *ple, cudaStream_t s) {
+  const TreeHost &th = *b.th;
+  const TreeDev &td = *b.td;
+  if (th.L < 3) return;
+  const int np = b.np;
+  int max_groups = 0;
+  for (int m = 2; m < th.L; ++m) max_groups = std::max(max_groups, th.rg_hi[m] - th.rg_lo[m]);
+  if (max_groups == 0) return;
+  DevBuf<double> sbig, y, lp, c;
+  sbig.alloc((size_t)max_groups * 4 * N_OFFSETS * np, s);
+  y.alloc((size_t)max_groups * 4 * np, s);
+  lp.alloc((size_t)max_groups * np, s);
+  c.alloc((size_t)max_groups * 4 * np, s);
+  FMMB_BLAS(cublasSetStream(b.blas, s));
+  const double one = 1.0, zero = 0.0;
+  for (int m = 2; m < th.L; ++m) {
+    const int lo = th.rg_lo[m], n_groups = th.rg_hi[m] - th.rg_lo[m];
+    if (n_groups == 0) continue;
+    const int n = 4 * n_groups;
+    if (m >= 3) {  // L2L from level m-1: children += parent local . M2MC (bbfmm.py:161, fmm.py:140-147)
+      PhaseTimer timer(PH_DOWNWARD, s);
+      k_bb_parent_locals<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
+          n_groups, np, td.rg.get(), lo, td.parent.get(), ple, lp.get());
+      FMMB_CUDA(cudaGetLastError());
+      FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_N, CUBLAS_OP_N, 4 * np, n_groups, np, &one, b.m2mc,
+                            4 * np, lp.get(), np, &zero, c.get(), 4 * np));
+      k_bb_add_children<<<grid_for((int64_t)n_groups * 4 * np, 256), 256, 0, s>>>(
+          n_groups, np, td.rg.get(), lo, c.get(), ple);
+      FMMB_CUDA(cudaGetLastError());
+    }
+    {  // M2L of level m: all 40 offsets in one GEMM (fmm.py:118-131)
+      PhaseTimer timer(PH_M2L, s);
+      k_bb_m2l_gather<<<grid_for((int64_t)n * N_OFFSETS * np, 256, 148 * 64), 256, 0, s>>>(
+          n_groups, np, td.rg.get(), lo, td.il.get(), mult, sbig.get());
+      FMMB_CUDA(cudaGetLastError());
+      FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, N_OFFSETS * np, &one,
+                            b.m2l_cat[m], N_OFFSETS * np, sbig.get(), N_OFFSETS * np, &zero, y.get(),
+                            np));
+      k_bb_add_rows<<<grid_for((int64_t)n * np, 256), 256, 0, s>>>(n_groups, np, td.rg.get(), lo,
+                                                                    y.get(), ple);
+      FMMB_CUDA(cudaGetLastError());
+    }
+  }
+}
+
+void run_bb_evaluate(const BBArgs &b, const double *tau_s, const double *loc, const double *txs,
+                     const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
+                     int check, double *out, cudaStream_t s) {
+  if (m == 0) return;
+  const TreeDev &td = *b.td;
+  PassArgs a{};
+  a.th = b.th;
+  a.td = b.td;
+  EvalItems it;
+  eval_items(a, tkeys, m, it, s);
+  const BBScale sc = bb_scale(*b.th);
+  PhaseTimer timer(PH_EVAL, s);
+  switch (b.kernel_id) {
+    case KERNEL_LAPLACE:
+      k_bb_evaluate<LaplaceF64><<<148 * 8, TCH_BB, 0, s>>>(
+          b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
+          tys, tperm, check, out);
+      break;
+    case KERNEL_MOD_HELMHOLTZ:
+      k_bb_evaluate<ModHelmholtzF64><<<148 * 8, TCH_BB, 0, s>>>(
+          b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
+          tys, tperm, check, out);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+  FMMB_CUDA(cudaGetLastError());
+}
+
+}  // namespace fmmb

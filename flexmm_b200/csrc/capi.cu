@@ -42,6 +42,7 @@ struct LevelEntry {
   DevBuf<double> buf;
   DevBuf<float> buf32;
   LevelOpsDev dev;
+  DevBuf<double> bb_m2l;  // black-box FMM: [np x 40 np], offset blocks side by side
 };
 
 // round to TF32 (10 explicit mantissa bits), to nearest, ties away from zero
@@ -159,10 +160,15 @@ void retain_pool_memory() {
 }
 }  // namespace
 
+constexpr int METHOD_KIFMM = 0, METHOD_BBFMM = 1;
+
 struct fmm_ops {
   int kernel_id;
   KernelParams kp;
   int neq, np;
+  int method = METHOD_KIFMM;
+  int p = 0;                  // black-box FMM: Chebyshev order
+  DevBuf<double> bb_m2mc;     // black-box FMM: M2MC [np x 4np]
   std::vector<std::unique_ptr<LevelEntry>> levels;
 };
 
@@ -180,6 +186,10 @@ struct fmm_plan {
   DevBuf<int> err;              // set by kernels whose bounded waits ran out
   int precision = PREC_FP64;
   bool have_expansions = false;
+  cublasHandle_t blas = nullptr;  // black-box FMM translations
+  ~fmm_plan() {
+    if (blas) cublasDestroy(blas);
+  }
 };
 
 extern "C" {
@@ -205,6 +215,8 @@ int fmm_ops_create(int kernel_id, const double *kparams, int nequiv, fmm_ops **o
 int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
   return guarded([&] {
     FMMB_CHECK(ops && lv && level_id, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(ops->method == METHOD_KIFMM, ERR_INVALID_ARGUMENT,
+               "black-box operator sets take fmm_bb_ops_add");
     const int n = ops->neq, np = ops->np;
     // host staging in the padded device layout
     std::vector<double> h;
@@ -374,6 +386,65 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
   });
 }
 
+int fmm_bb_ops_create(int kernel_id, const double *kparams, int p, const double *m2mc,
+                      fmm_ops **out) {
+  return guarded([&] {
+    FMMB_CHECK(out && m2mc, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(kernel_known(kernel_id), ERR_UNSUPPORTED, "unknown kernel id");
+    FMMB_CHECK(p >= 2 && p <= FMM_BB_MAX_P, ERR_INVALID_ARGUMENT, "p must be in [2, 16]");
+    const KernelParams kp = kernel_params(kernel_id, kparams);
+    const int n = p * p, np = pad8(n);
+    std::vector<double> h(size_t(np) * 4 * np, 0.0);
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < n; ++k) h[size_t(i) * 4 * np + c * np + k] = m2mc[size_t(i) * 4 * n + c * n + k];
+    auto o = std::make_unique<fmm_ops>();
+    o->kernel_id = kernel_id;
+    o->kp = kp;
+    o->neq = n;
+    o->np = np;
+    o->method = METHOD_BBFMM;
+    o->p = p;
+    o->bb_m2mc.alloc(h.size(), 0);
+    FMMB_CUDA(cudaMemcpy(o->bb_m2mc.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    *out = o.release();
+  });
+}
+
+int fmm_bb_ops_add(fmm_ops *ops, const fmm_bb_level_ops *lv, int *level_id) {
+  return guarded([&] {
+    FMMB_CHECK(ops && lv && level_id && lv->m2l_rank, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(ops->method == METHOD_BBFMM, ERR_INVALID_ARGUMENT,
+               "fmm_bb_ops_add needs a black-box operator set (fmm_bb_ops_create)");
+    const int n = ops->neq, np = ops->np;
+    const size_t ld = size_t(N_OFFSETS) * np;
+    std::vector<double> h(size_t(np) * ld, 0.0);
+    for (int o = 0; o < N_OFFSETS; ++o) {
+      const int r = lv->m2l_rank[o];
+      if (r == 0) continue;
+      FMMB_CHECK(lv->m2l_a[o], ERR_INVALID_ARGUMENT, "missing M2L operator");
+      if (r < 0) {  // dense [n x n]
+        for (int i = 0; i < n; ++i)
+          for (int k = 0; k < n; ++k) h[size_t(i) * ld + size_t(o) * np + k] = lv->m2l_a[o][size_t(i) * n + k];
+      } else {  // the truncated operator M2 . M1 ([n x r] . [r x n]), as the reference applies it
+        FMMB_CHECK(r <= n && lv->m2l_b[o], ERR_INVALID_ARGUMENT, "bad M2L factors");
+        for (int i = 0; i < n; ++i)
+          for (int k = 0; k < n; ++k) {
+            double acc = 0.0;
+            for (int q = 0; q < r; ++q) acc += lv->m2l_a[o][size_t(i) * r + q] * lv->m2l_b[o][size_t(q) * n + k];
+            h[size_t(i) * ld + size_t(o) * np + k] = acc;
+          }
+      }
+    }
+    auto e = std::make_unique<LevelEntry>();
+    e->dev.inv_w = 1.0 / lv->width;
+    e->bb_m2l.alloc(h.size(), 0);
+    FMMB_CUDA(cudaMemcpy(e->bb_m2l.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ops->levels.push_back(std::move(e));
+    *level_id = int(ops->levels.size()) - 1;
+  });
+}
+
 int fmm_ops_destroy(fmm_ops *ops) {
   return guarded([&] {
     if (!ops) return;
@@ -417,6 +488,8 @@ int fmm_plan_set_precision(fmm_plan *p, int precision) {
                "precision must be FMM_PRECISION_FP64 or FMM_PRECISION_MIXED");
     FMMB_CHECK(precision == PREC_FP64 || kernel_scaled(p->ops->kernel_id), ERR_UNSUPPORTED,
                "the mixed form needs a scale-invariant kernel (Laplace)");
+    FMMB_CHECK(precision == PREC_FP64 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
+               "the black-box FMM has an FP64 form only");
     p->precision = precision;
     p->have_expansions = false;
   });
@@ -447,6 +520,28 @@ static PassArgs pass_args(fmm_plan *p) {
   return a;
 }
 
+static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
+  BBArgs b{};
+  b.kernel_id = p->ops->kernel_id;
+  b.kp = p->ops->kp;
+  b.p = p->ops->p;
+  b.np = p->ops->np;
+  b.td = &p->td;
+  b.th = &p->th;
+  if (!p->blas) {
+    FMMB_CHECK(cublasCreate(&p->blas) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasCreate failed");
+    // no TF32 / reduced-precision paths: the black-box form is FP64 end to end
+    FMMB_CHECK(cublasSetMathMode(p->blas, CUBLAS_PEDANTIC_MATH) == CUBLAS_STATUS_SUCCESS, ERR_CUDA,
+               "cublasSetMathMode failed");
+  }
+  FMMB_CHECK(cublasSetStream(p->blas, s) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasSetStream failed");
+  b.blas = p->blas;
+  b.m2mc = p->ops->bb_m2mc.get();
+  for (int m = 0; m < p->th.L && m < FMM_MAX_LEVELS_DEV; ++m)
+    b.m2l_cat[m] = p->bound[m] >= 0 ? p->ops->levels[p->bound[m]]->bb_m2l.get() : nullptr;
+  return b;
+}
+
 int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
   return guarded([&] {
     FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
@@ -456,6 +551,19 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
     const int np = p->ops->np;
     const int64_t total = th.n_total();
+    if (p->ops->method == METHOD_BBFMM) {
+      BBArgs b = bb_args(p, s);
+      p->tau_s.alloc(th.n_points, s);
+      gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
+      p->mult.alloc(total * np, s);
+      p->ple.alloc(total * np, s);
+      p->mult.zero(s);
+      p->ple.zero(s);
+      run_bb_upward(b, p->tau_s.get(), p->mult.get(), s);
+      run_bb_downward(b, p->mult.get(), p->ple.get(), s);
+      p->have_expansions = true;
+      return;
+    }
     std::unique_ptr<PhaseTimer> t_prep(new PhaseTimer(PH_PREP, s));
     p->ops_dev.alloc(th.L, s);
     PassArgs a = pass_args(p);
@@ -514,6 +622,8 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
   FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
   FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
   FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the target count");
+  FMMB_CHECK(nout == 1 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
+             "the black-box FMM evaluates potentials only");
   PassArgs a = pass_args(p);
   DevBuf<uint64_t> tkeys;
   DevBuf<int> tperm;
@@ -527,7 +637,10 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
     gather_sorted(tx, tperm.get(), m, txs.get(), s);
     gather_sorted(ty, tperm.get(), m, tys.get(), s);
   }
-  if (p->precision == PREC_MIXED)
+  if (p->ops->method == METHOD_BBFMM)
+    run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), txs.get(), tys.get(), tkeys.get(),
+                    tperm.get(), m, check, out, s);
+  else if (p->precision == PREC_MIXED)
     run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(), txs.get(),
                        tys.get(), tkeys.get(), tperm.get(), m, check, nout, out, ld_out, s);
   else
@@ -543,10 +656,15 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
   const TreeDev &td = p->td;
   const int64_t m = p->th.n_points;
   FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the source count");
+  FMMB_CHECK(nout == 1 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
+             "the black-box FMM evaluates potentials only");
   PassArgs a = pass_args(p);
   // the tree's sorted copy: keys sorted on at least their top L-1 digits,
   // which is all that leaf location reads
-  if (p->precision == PREC_MIXED)
+  if (p->ops->method == METHOD_BBFMM)
+    run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), td.sx.get(), td.sy.get(),
+                    td.pkeys.get(), td.ordv.get(), m, check, out, s);
+  else if (p->precision == PREC_MIXED)
     run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(),
                        td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, nout,
                        out, ld_out, s);
@@ -715,6 +833,8 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
     FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
     FMMB_CHECK(p->precision == PREC_FP64, ERR_UNSUPPORTED,
                "fmm_evaluate_noalloc evaluates FP64 plans only");
+    FMMB_CHECK(p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
+               "fmm_evaluate_noalloc evaluates KIFMM plans only");
     FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
     FMMB_CHECK(m <= FMM_NOALLOC_MAX_TARGETS, ERR_CAPACITY,
                "fmm_evaluate_noalloc: more than FMM_NOALLOC_MAX_TARGETS targets");

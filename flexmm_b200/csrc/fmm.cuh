@@ -3,6 +3,8 @@
 // circle), partial locals from M2L, and locals (equivalent densities on the
 // large circle).
 #pragma once
+#include <cublas_v2.h>
+
 #include "kernels.cuh"
 #include "tree.cuh"
 
@@ -49,6 +51,27 @@ struct PassArgs {
   const LevelOpsDev *ops_dev;   // device array indexed by level
   std::vector<LevelOpsDev> ops_host;
 };
+
+// Black-box (Chebyshev) FMM (bbfmm.cu): p x p coefficients per box, NQ = p^2
+// padded to np columns; M2MC [np x 4np] row-major (level independent);
+// m2l_cat[m]: level m's 40 M2L operators side by side, [np x 40 np] row-major,
+// block o holding VI K VI^T of offset o (zero for a null offset).
+struct BBArgs {
+  int kernel_id;
+  KernelParams kp;
+  int p, np;
+  const TreeDev *td;
+  const TreeHost *th;
+  cublasHandle_t blas;
+  const double *m2mc;
+  const double *m2l_cat[FMM_MAX_LEVELS_DEV];
+};
+void run_bb_upward(const BBArgs &b, const double *tau_sorted, double *mult, cudaStream_t s);
+// M2L and L2L, level by level; the locals are the partial locals (no solve)
+void run_bb_downward(const BBArgs &b, const double *mult, double *ple, cudaStream_t s);
+void run_bb_evaluate(const BBArgs &b, const double *tau_sorted, const double *loc,
+                     const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
+                     int64_t m, int check, double *out, cudaStream_t s);
 
 void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaStream_t s);
 void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s);

@@ -133,12 +133,19 @@ class TreeView:
 class KI_FMM:
     """Kernel-independent FMM (KI_FMM, flexmm/flexmm2d/kifmm.py:122-144)."""
 
+    _helper_cls = KI_Helper
+    _max_nequiv = _lib.MAX_NEQUIV
+
+    @staticmethod
+    def _default_helper(kernel, nequiv):
+        return default_helper(kernel, nequiv)
+
     def __init__(self, x, y, kernel_eval, Ncutoff=50, Nequiv=50, dtype=float, bbox=None,
                  helper=None, verbose=False, precision="fp64", **kernel_params):
         if dtype not in (float, np.float64):
             raise NotImplementedError("only real float64 charges are supported")
-        if Nequiv > _lib.MAX_NEQUIV:
-            raise ValueError(f"Nequiv must be <= {_lib.MAX_NEQUIV}")
+        if Nequiv > self._max_nequiv:
+            raise ValueError(f"Nequiv must be <= {self._max_nequiv}")
         if precision not in _lib.PRECISION:
             raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
         self.precision = precision
@@ -148,9 +155,9 @@ class KI_FMM:
         self.Nequiv = int(Nequiv)
         self.dtype = dtype
         self.verbose = verbose
-        self.helper = helper if helper is not None else default_helper(self.kernel, self.Nequiv)
-        if not isinstance(self.helper, KI_Helper):
-            raise TypeError("helper must be a flexmm_b200 KI_Helper")
+        self.helper = helper if helper is not None else self._default_helper(self.kernel, self.Nequiv)
+        if not isinstance(self.helper, self._helper_cls):
+            raise TypeError(f"helper must be a flexmm_b200 {self._helper_cls.__name__}")
         self.helper.attach(self.kernel, self.Nequiv)
         xd, _ = _device_f64(x)
         yd, _ = _device_f64(y)

@@ -69,6 +69,27 @@ typedef struct fmm_level_ops {
   const double *const *m2l_b;      /* [40] SVD: M1 [r*n]; otherwise unused    */
 } fmm_level_ops;
 
+/* Black-box (Chebyshev) FMM operator set, BB_FMM / BB_Helper
+ * (flexmm/flexmm2d/bbfmm.py:133-231): Chebyshev order p (2..16, NQ = p^2
+ * coefficients per box) and the level-independent M2MC [NQ x 4NQ] (child
+ * blocks ordered (-,-), (-,+), (+,-), (+,+)), row-major host memory.  Plans
+ * built on it run S2M moments, M2M, M2L, L2L, L2T as the reference's BB_FMM,
+ * in FP64; fmm_plan_create / bind / build_expansions / evaluate take it like
+ * a KIFMM set. */
+#define FMM_BB_MAX_P 16
+int fmm_bb_ops_create(int kernel_id, const double *kparams, int p, const double *m2mc,
+                      fmm_ops **out);
+/* One box width's 40 M2L operators VI K VI^T (bbfmm.py:101-122), in the
+ * fmm_level_ops convention: rank < 0 dense [NQ x NQ] in m2l_a, rank > 0 the
+ * factors M2 [NQ x r] (m2l_a) and M1 [r x NQ] (m2l_b), 0 none. */
+typedef struct fmm_bb_level_ops {
+  double width;
+  const int *m2l_rank;
+  const double *const *m2l_a;
+  const double *const *m2l_b;
+} fmm_bb_level_ops;
+int fmm_bb_ops_add(fmm_ops *ops, const fmm_bb_level_ops *lv, int *level_id);
+
 int fmm_ops_create(int kernel_id, const double *kernel_params /* [4] or NULL */, int nequiv,
                    fmm_ops **out);
 int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *level, int *level_id);

@@ -69,3 +69,16 @@ def oracle_direct(meta, sx, sy, tau, tx, ty, check):
     if meta.get("kernel", "laplace") == "laplace":
         return direct_laplace(sx, sy, tau, tx, ty, check)
     return direct_mod_helmholtz(sx, sy, tau, tx, ty, meta["k"], check)
+
+
+def make_fmm(d, meta, helper=None, precision="fp64", x=None, y=None):
+    """Our FMM object for a golden case: KI_FMM, or BB_FMM for black-box cases."""
+    from flexmm_b200 import BB_FMM, BB_Helper, KI_FMM, KI_Helper
+    name, params = kernel_of(meta)
+    x = d["x"] if x is None else x
+    y = d["y"] if y is None else y
+    if meta.get("method") == "bb":
+        return BB_FMM(x, y, name, meta["ncut"], meta["p"], bbox=d["bbox"],
+                      helper=helper if helper is not None else BB_Helper(), **params)
+    return KI_FMM(x, y, name, meta["ncut"], meta["neq"], bbox=d["bbox"],
+                  helper=helper if helper is not None else KI_Helper(), precision=precision, **params)

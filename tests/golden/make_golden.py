@@ -104,6 +104,14 @@ CASES = {
                                      neq=24, kernel="mh", k=5.0), True),
     "grad_mh_clustered_20k_q32_k5": (dict(recipe="clustered", seed=22, n=20000, n_grid=64, ncut=32,
                                           neq=32, kernel="mh", k=5.0, gradient=True), True),
+    "bb_uniform_3k_p8": (dict(recipe="uniform", seed=23, n=3000, n_grid=41, ncut=32, neq=64,
+                              method="bb", p=8), True),
+    "bb_clustered_20k_p12": (dict(recipe="clustered", seed=24, n=20000, n_grid=64, ncut=64, neq=144,
+                                  method="bb", p=12), True),
+    "bb_uniform_10k_p16": (dict(recipe="uniform", seed=25, n=10000, n_grid=50, ncut=64, neq=256,
+                                method="bb", p=16), True),
+    "bb_mh_duplicates_5k_p10_k5": (dict(recipe="duplicates", seed=26, n=5000, n_grid=33, ncut=32,
+                                        neq=100, method="bb", p=10, kernel="mh", k=5.0), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -159,6 +167,12 @@ def direct(meta, grad, *args):
 def run_case(name, meta, ref):
     from flexmm.flexmm2d.kifmm import KI_FMM, KI_Helper
     Laplace_Eval = reference_kernel(meta)
+    if meta.get("method") == "bb":  # black-box FMM, flexmm/flexmm2d/bbfmm.py:212-231
+        from flexmm.flexmm2d.bbfmm import BB_FMM, BB_Helper
+
+        def KI_FMM(x, y, kernel, ncut, neq, bbox, helper):  # noqa: F811
+            return BB_FMM(x, y, kernel, ncut, meta["p"], bbox=bbox, helper=BB_Helper())
+        KI_Helper = type(None)  # noqa: F811
 
     d = case_inputs(meta)
     t0 = time.time()

@@ -6,7 +6,7 @@ on the same inputs; the tree equal to the reference's box for box.
 import numpy as np
 import pytest
 
-from conftest import golden_cases, golden_inputs, kernel_of, load_golden, oracle_direct, rel_l2
+from conftest import golden_cases, golden_inputs, kernel_of, load_golden, make_fmm, oracle_direct, rel_l2
 import canon
 
 pytestmark = pytest.mark.gpu
@@ -15,10 +15,7 @@ PARITY = 1e-12
 
 
 def _fmm(d, meta, helper=None):
-    from flexmm_b200 import KI_FMM, KI_Helper
-    name, params = kernel_of(meta)
-    return KI_FMM(d["x"], d["y"], name, meta["ncut"], meta["neq"], bbox=d["bbox"], **params,
-                  helper=helper if helper is not None else KI_Helper())
+    return make_fmm(d, meta, helper)
 
 
 @pytest.mark.parametrize("case", golden_cases())

@@ -31,7 +31,7 @@ def test_oracle_tree_matches_reference_tree(case):
     assert not bad, f"canonical tree fields differ from the reference: {bad}"
 
 
-@pytest.mark.parametrize("case", SMALL)
+@pytest.mark.parametrize("case", [c for c in SMALL if load_golden(c)["meta"].get("method") != "bb"])
 def test_oracle_results_match_reference(case):
     g = load_golden(case)
     meta = g["meta"]
@@ -72,6 +72,9 @@ def test_reference_accuracy_recorded(case):
     """The stored reference outputs agree with FP64 direct sums to the FMM's own accuracy."""
     g = load_golden(case)
     neq = g["meta"]["neq"]
-    tol = {16: 1e-4, 24: 1e-6, 32: 1e-8, 40: 1e-9, 60: 1e-13}[neq]
+    if g["meta"].get("method") == "bb":  # black-box FMM: p^2 coefficients
+        tol = {64: 1e-6, 100: 1e-7, 144: 1e-9, 256: 1e-12}[neq]
+    else:
+        tol = {16: 1e-4, 24: 1e-6, 32: 1e-8, 40: 1e-9, 60: 1e-13}[neq]
     assert rel_l2(g["src_val"], g["direct_src"]) < tol
     assert rel_l2(g["tgt_val"], g["direct_tgt"]) < tol
