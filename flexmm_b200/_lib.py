@@ -57,6 +57,7 @@ SIGNATURES = [
     ("fmm_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("fmm_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(LevelOps), _ip]),
     ("fmm_ops_destroy", ctypes.c_int, [_vp]),
+    ("fmm_kernel_table_create", ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip]),
     ("fmm_bb_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.POINTER(_vp)]),
     ("fmm_bb_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(BBLevelOps), _ip]),
     ("fmm_plan_create", ctypes.c_int,

@@ -411,6 +411,12 @@ void run_bb_evaluate(const BBArgs &b, const double *tau_s, const double *loc, co
           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
           tys, tperm, check, out);
       break;
+    case KERNEL_RADIAL_TABLE:
+      k_bb_evaluate<RadialTableF64><<<148 * 8, TCH_BB, 0, s>>>(
+          b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
+          tys, tperm, check, out);
+      break;
     case KERNEL_MOD_HELMHOLTZ:
       k_bb_evaluate<ModHelmholtzF64><<<148 * 8, TCH_BB, 0, s>>>(
           b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),

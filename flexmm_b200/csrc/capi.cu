@@ -113,8 +113,19 @@ const double *bessel_table_device() {
   return d;
 }
 
+// tabulated radial kernels registered by fmm_kernel_table_create: host
+// coefficients plus their per-device copies (kept until exit)
+struct RadialTable {
+  int j0, noct, ncheb;
+  std::vector<double> coef;
+  std::map<int, double *> dev;
+};
+std::mutex g_tables_mu;
+std::vector<std::unique_ptr<RadialTable>> g_tables;
+
 bool kernel_known(int kernel_id) {
-  return kernel_id == KERNEL_LAPLACE || kernel_id == KERNEL_MOD_HELMHOLTZ;
+  return kernel_id == KERNEL_LAPLACE || kernel_id == KERNEL_MOD_HELMHOLTZ ||
+         kernel_id == KERNEL_RADIAL_TABLE;
 }
 
 // a kernel's device parameters: the caller's values plus the tables it reads
@@ -125,6 +136,25 @@ KernelParams kernel_params(int kernel_id, const double *kparams) {
   if (kernel_id == KERNEL_MOD_HELMHOLTZ) {
     FMMB_CHECK(kp.p[0] > 0.0, ERR_INVALID_ARGUMENT, "modified Helmholtz needs k = kparams[0] > 0");
     kp.table = bessel_table_device();
+  }
+  if (kernel_id == KERNEL_RADIAL_TABLE) {
+    std::lock_guard<std::mutex> g(g_tables_mu);
+    const int id = int(kp.p[0]);
+    FMMB_CHECK(kp.p[0] == double(id) && id >= 0 && id < (int)g_tables.size() && g_tables[id],
+               ERR_INVALID_ARGUMENT, "kparams[0] is not a table id from fmm_kernel_table_create");
+    RadialTable &t = *g_tables[id];
+    int dev = 0;
+    FMMB_CUDA(cudaGetDevice(&dev));
+    if (!t.dev.count(dev)) {
+      double *d = nullptr;
+      FMMB_CUDA(cudaMalloc((void **)&d, t.coef.size() * sizeof(double)));
+      FMMB_CUDA(cudaMemcpy(d, t.coef.data(), t.coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+      t.dev[dev] = d;
+    }
+    kp.table = t.dev[dev];
+    kp.p[1] = t.j0;
+    kp.p[2] = t.noct;
+    kp.p[3] = t.ncheb;
   }
   return kp;
 }
@@ -442,6 +472,24 @@ int fmm_bb_ops_add(fmm_ops *ops, const fmm_bb_level_ops *lv, int *level_id) {
     FMMB_CUDA(cudaMemcpy(e->bb_m2l.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     ops->levels.push_back(std::move(e));
     *level_id = int(ops->levels.size()) - 1;
+  });
+}
+
+int fmm_kernel_table_create(const double *coef, int j0, int n_octaves, int n_cheb, int *table_id) {
+  return guarded([&] {
+    FMMB_CHECK(coef && table_id, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(n_octaves >= 1 && n_octaves <= 2048 && n_cheb >= 1 && n_cheb <= 64, ERR_INVALID_ARGUMENT,
+               "table size out of range");
+    FMMB_CHECK(j0 >= -1000 && j0 + n_octaves <= 1000, ERR_INVALID_ARGUMENT, "octave range out of range");
+    auto t = std::make_unique<RadialTable>();
+    t->j0 = j0;
+    t->noct = n_octaves;
+    t->ncheb = n_cheb;
+    t->coef.assign(coef, coef + size_t(n_octaves) * n_cheb);
+    for (double v : t->coef) FMMB_CHECK(std::isfinite(v), ERR_INVALID_ARGUMENT, "non-finite coefficient");
+    std::lock_guard<std::mutex> g(g_tables_mu);
+    g_tables.push_back(std::move(t));
+    *table_id = int(g_tables.size()) - 1;
   });
 }
 

@@ -578,6 +578,7 @@ void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: upward_impl<LaplaceF64>(a, tau_s, mult, s); break;
     case KERNEL_MOD_HELMHOLTZ: upward_impl<ModHelmholtzF64>(a, tau_s, mult, s); break;
+    case KERNEL_RADIAL_TABLE: upward_impl<RadialTableF64>(a, tau_s, mult, s); break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
@@ -634,6 +635,11 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
       evaluate_impl<ModHelmholtzF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
                                      ld_out, s);
       break;
+    case KERNEL_RADIAL_TABLE:
+      FMMB_CHECK(nout == 1, ERR_UNSUPPORTED, "tabulated kernels evaluate potentials only");
+      evaluate_impl<RadialTableF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
+                                    ld_out, s);
+      break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
@@ -650,6 +656,9 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
       break;
     case KERNEL_MOD_HELMHOLTZ:
       k_direct<ModHelmholtzF64><<<grid, 256, 0, s>>>(kp, sx, sy, tau, ns, tx, ty, nt, check, out);
+      break;
+    case KERNEL_RADIAL_TABLE:
+      k_direct<RadialTableF64><<<grid, 256, 0, s>>>(kp, sx, sy, tau, ns, tx, ty, nt, check, out);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

@@ -2,6 +2,8 @@
 //
 //   Laplace_Eval: -log(|t-s|^2) / (4 pi)       examples/kifmm_laplace.py:24-29
 //   Modified_Helmholtz_Eval: K0(k |t-s|) / (2 pi)  examples/kifmm_modified_helmholtz.py:33-39
+//   a tabulated radial kernel f(|t-s|), as the reference's examples build
+//   with function_generator (e.g. the Struve kernel, examples/bbfmm_struve.py:29-46)
 //
 // A functor evaluates K(source, target) for source (sx, sy) and target
 // (tx, ty); the FMM kernels are templated on it, so the functor inlines into
@@ -17,7 +19,7 @@
 
 namespace fmmb {
 
-enum KernelId : int { KERNEL_LAPLACE = 0, KERNEL_MOD_HELMHOLTZ = 1 };
+enum KernelId : int { KERNEL_LAPLACE = 0, KERNEL_MOD_HELMHOLTZ = 1, KERNEL_RADIAL_TABLE = 2 };
 
 // the caller's parameters (p[0] = helmholtz k for the modified Helmholtz
 // kernel) and the device's Bessel tables (bessel.cuh)
@@ -67,6 +69,41 @@ struct ModHelmholtzF64 {
     ux += s * dx;
     uy += s * dy;
   }
+};
+
+// K(s, t) = f(|t - s|) with f tabulated as Chebyshev series on the octaves
+// [2^j, 2^(j+1)), j = j0 .. j0 + noct - 1 (table [noct][ncheb], built on the
+// host from any function; the octave grid resolves power-law and log
+// behaviour at 0).  Distances outside the tabulated range are clamped to it.
+struct RadialTableF64 {
+  const double *tab;
+  int j0, noct, ncheb;
+  __host__ __device__ explicit RadialTableF64(const KernelParams &kp)
+      : tab(kp.table), j0(int(kp.p[1])), noct(int(kp.p[2])), ncheb(int(kp.p[3])) {}
+  __device__ __forceinline__ double f(double r) const {
+    const double lo = ldexp(1.0, j0), hi = ldexp(1.0, j0 + noct);
+    r = fmin(fmax(r, lo), hi * (1.0 - 1e-16));
+    int e;
+    frexp(r, &e);
+    const int oct = e - 1 - j0;
+    const double a = ldexp(1.0, e - 1);
+    const double u = (2.0 * r - 3.0 * a) / a;
+    const double *c = tab + oct * ncheb;
+    double b1 = 0.0, b2 = 0.0;
+    for (int i = ncheb - 1; i >= 1; --i) {
+      const double b0 = fma(2.0 * u, b1, -b2) + __ldg(c + i);
+      b2 = b1;
+      b1 = b0;
+    }
+    return fma(u, b1, -b2) + __ldg(c);
+  }
+  __device__ __forceinline__ double operator()(double sx, double sy, double tx, double ty) const {
+    const double dx = tx - sx, dy = ty - sy;
+    return f(sqrt(dx * dx + dy * dy));
+  }
+  // a tabulated kernel carries no derivative table: gradients are not offered
+  __device__ __forceinline__ void grad(double, double, double, double, double, double &, double &,
+                                       double &) const {}
 };
 
 // log2 on the special-function unit, denormal inputs flushed to zero

@@ -54,6 +54,102 @@ def _mod_helmholtz_host(p, sx, sy, tx, ty):
 
 KERNEL_LAPLACE = 0
 KERNEL_MOD_HELMHOLTZ = 1
+KERNEL_RADIAL_TABLE = 2
+
+
+def _cheb_nodes(n):
+    return np.cos(np.pi * (np.arange(n) + 0.5) / n)
+
+
+def _clenshaw(c, u):
+    b1 = np.zeros_like(u)
+    b2 = np.zeros_like(u)
+    for ci in c[:0:-1]:
+        b1, b2 = 2 * u * b1 - b2 + ci, b1
+    return u * b1 - b2 + c[0]
+
+
+class RadialTable:
+    """f(r) as Chebyshev series of degree n-1 on the octaves [2^j, 2^(j+1))
+    covering [a, b] (the device evaluates the same table, csrc/kernels.cuh
+    RadialTableF64).  The reference's examples tabulate their special-function
+    kernels the same way with function_generator (FunctionGenerator(f, a, b,
+    tol), examples/bbfmm_struve.py:34-36); octaves resolve a power-law or log
+    singularity at 0 with a fixed degree."""
+
+    def __init__(self, f, a, b, tol=1e-12, n=24):
+        if not 0 < a < b:
+            raise ValueError("need 0 < a < b")
+        self.j0 = int(np.floor(np.log2(a)))
+        j1 = int(np.ceil(np.log2(b)))
+        self.noct = max(1, j1 - self.j0)
+        self.n = int(n)
+        u = _cheb_nodes(self.n)
+        coef = np.empty((self.noct, self.n))
+        k = np.arange(self.n)
+        cosm = np.cos(np.pi * np.outer(np.arange(self.n), k + 0.5) / self.n)
+        rng = np.random.default_rng(0)
+        worst = 0.0
+        for o in range(self.noct):
+            lo = 2.0 ** (self.j0 + o)
+            fx = np.asarray(f(lo * (1.5 + 0.5 * u)), dtype=np.float64)
+            if not np.all(np.isfinite(fx)):
+                raise ValueError(f"f is not finite on [{lo}, {2 * lo})")
+            c = 2.0 / self.n * cosm.dot(fx)
+            c[0] *= 0.5
+            coef[o] = c
+            uc = rng.uniform(-1, 1, 3 * self.n)
+            ref = np.asarray(f(lo * (1.5 + 0.5 * uc)), dtype=np.float64)
+            err = np.abs(_clenshaw(c, uc) - ref) / np.maximum(np.abs(ref), 1e-300)
+            worst = max(worst, float(err.max()))
+        if worst > tol:
+            raise ValueError(f"tabulation error {worst:.1e} above tol {tol:.1e}; raise n")
+        self.coef = np.ascontiguousarray(coef)
+        self.max_rel_err = worst
+        self.table_id = None
+
+    def __call__(self, r):
+        """Host evaluation of the tabulated f (operator formation)."""
+        r = np.asarray(r, dtype=np.float64)
+        lo, hi = 2.0 ** self.j0, 2.0 ** (self.j0 + self.noct)
+        r = np.clip(r, lo, hi * (1 - 1e-16))
+        _, e = np.frexp(r)
+        o = e - 1 - self.j0
+        a = np.ldexp(1.0, e - 1)
+        u = (2 * r - 3 * a) / a
+        c = self.coef[o]
+        b1 = np.zeros_like(u)
+        b2 = np.zeros_like(u)
+        for i in range(self.n - 1, 0, -1):
+            b1, b2 = 2 * u * b1 - b2 + c[..., i], b1
+        return u * b1 - b2 + c[..., 0]
+
+    def register(self):
+        """Upload to the library (once); returns the table id."""
+        if self.table_id is None:
+            import ctypes
+            from . import _lib
+            tid = ctypes.c_int(-1)
+            _lib.call("fmm_kernel_table_create", self.coef.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                      self.j0, self.noct, self.n, ctypes.byref(tid))
+            self.table_id = tid.value
+        return self.table_id
+
+
+def radial(f, a, b, tol=1e-12, n=24, name="Radial"):
+    """A kernel K(s, t) = f(|t - s|) from any vectorised function f, tabulated
+    on [a, b] (the reference's ``FunctionGenerator(f, a, b, tol)`` plus the
+    scalar kernel that calls it, e.g. examples/bbfmm_struve.py:29-46)."""
+    table = RadialTable(f, a, b, tol=tol, n=n)
+    tid = table.register()
+
+    def host(p, sx, sy, tx, ty):
+        dx = tx - sx
+        dy = ty - sy
+        return table(np.sqrt(dx * dx + dy * dy))
+    k = Kernel(name, KERNEL_RADIAL_TABLE, (tid, table.j0, table.noct, table.n), host)
+    k.table = table
+    return k
 
 
 def Laplace():

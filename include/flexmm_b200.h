@@ -69,6 +69,20 @@ typedef struct fmm_level_ops {
   const double *const *m2l_b;      /* [40] SVD: M1 [r*n]; otherwise unused    */
 } fmm_level_ops;
 
+/* Kernel ids: 0 Laplace -log(r^2)/(4 pi) (examples/kifmm_laplace.py:24-29);
+ * 1 modified Helmholtz K0(k r)/(2 pi), kparams[0] = k
+ * (examples/kifmm_modified_helmholtz.py:25-39); 2 a tabulated radial kernel
+ * f(r), kparams[0] = the id from fmm_kernel_table_create. */
+#define FMM_KERNEL_MOD_HELMHOLTZ 1
+#define FMM_KERNEL_RADIAL_TABLE 2
+/* Register a radial kernel f(r) tabulated as Chebyshev series on the octaves
+ * [2^j, 2^(j+1)), j = j0 .. j0 + n_octaves - 1: coef[n_octaves][n_cheb],
+ * series in u = (2 r - 3 2^j) / 2^j.  Replaces the reference examples'
+ * function_generator tables (examples/bbfmm_struve.py:34-46,
+ * kifmm_modified_helmholtz.py:28).  Distances outside the range are clamped
+ * to it.  Tables live until the process exits. */
+int fmm_kernel_table_create(const double *coef, int j0, int n_octaves, int n_cheb, int *table_id);
+
 /* Black-box (Chebyshev) FMM operator set, BB_FMM / BB_Helper
  * (flexmm/flexmm2d/bbfmm.py:133-231): Chebyshev order p (2..16, NQ = p^2
  * coefficients per box) and the level-independent M2MC [NQ x 4NQ] (child

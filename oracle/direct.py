@@ -90,3 +90,41 @@ def direct_mod_helmholtz_grad(sx, sy, tau, tx, ty, k, check):
     (examples/pure_kifmm_modified_helmholtz_gradient.py:45-70)."""
     a = [np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tau, tx, ty)]
     return _mh_pairs(*a, float(k), check, True)
+
+
+def struve_gf(x):
+    """The Struve Green's function of examples/bbfmm_struve.py:29-33, scipy.
+
+    scipy's struve returns NaN on short intervals (measured: order -2 near
+    x = 25.8463 and 28.995, order -3 near 27.329, each ~3e-5 wide); there the
+    value is the cubic through GF at x +- 1e-4 and x +- 2e-4, outside them
+    (GF is smooth on that scale: interpolation error ~1e-15 relative)."""
+    from scipy.special import struve, yn
+
+    def gf(v):
+        return (v * (yn(1, v) - struve(-3, v)) - 4 * struve(-2, v)) / v ** 2
+    x = np.asarray(x, dtype=np.float64)
+    out = gf(x)
+    bad = ~np.isfinite(out)
+    if np.any(bad):
+        xb = x[bad]
+        h = 1e-4
+        f = [gf(xb + k * h) for k in (-2, -1, 1, 2)]
+        # Lagrange weights of the nodes -2h, -h, h, 2h at 0
+        out[bad] = (-f[0] + 4 * f[1] + 4 * f[2] - f[3]) / 6.0
+    return out
+
+
+def direct_radial(f, sx, sy, tau, tx, ty, check):
+    """FP64 direct sum of a radial kernel f(|t - s|) (numpy; test infrastructure)."""
+    sx, sy, tau, tx, ty = (np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tau, tx, ty))
+    out = np.zeros(tx.size)
+    step = max(1, 2_000_000 // max(sx.size, 1))
+    for a in range(0, tx.size, step):
+        b = min(tx.size, a + step)
+        dx = tx[a:b, None] - sx[None, :]
+        dy = ty[a:b, None] - sy[None, :]
+        r = np.sqrt(dx * dx + dy * dy)
+        skip = (dx == 0) & (dy == 0) if check else np.zeros(r.shape, dtype=bool)
+        out[a:b] = (f(np.where(skip, 1.0, r)) * np.where(skip, 0.0, tau[None, :])).sum(1)
+    return out

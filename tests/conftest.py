@@ -52,15 +52,35 @@ def built_lib():
     return build.build()
 
 
+_STRUVE = {}
+
+
+def struve_kernel():
+    """The Struve example's kernel as a tabulated radial kernel (one per process)."""
+    if "k" not in _STRUVE:
+        from flexmm_b200.kernels import radial
+        from oracle.direct import struve_gf
+        # scipy's GF loses relative accuracy to cancellation at large r
+        # (~1e-12 below r = 10, ~1e-6 at 256): the fit tolerance follows it
+        _STRUVE["k"] = radial(struve_gf, 1e-30, 256.0, tol=1e-5, name="Kernel")
+    return _STRUVE["k"]
+
+
 def kernel_of(meta):
-    """(registered kernel name, kernel keyword parameters) of a golden case."""
-    if meta.get("kernel", "laplace") == "laplace":
+    """(kernel: registered name or Kernel, kernel keyword parameters) of a golden case."""
+    kind = meta.get("kernel", "laplace")
+    if kind == "laplace":
         return "Laplace_Eval", {}
+    if kind == "struve":
+        return struve_kernel(), {}
     return "Modified_Helmholtz_Eval", {"helmholtz_k": meta["k"]}
 
 
 def oracle_kernel(meta):
     from oracle.kernels import laplace, mod_helmholtz
+    if meta.get("kernel", "laplace") == "struve":
+        from oracle.direct import struve_gf
+        return lambda sx, sy, tx, ty: struve_gf(np.sqrt((tx - sx) ** 2 + (ty - sy) ** 2))
     return laplace if meta.get("kernel", "laplace") == "laplace" else mod_helmholtz(meta["k"])
 
 

@@ -40,7 +40,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 from flexmm_b200 import workloads  # noqa: E402
 from oracle import refimport  # noqa: E402
 from oracle.direct import (direct_laplace, direct_laplace_grad, direct_mod_helmholtz,  # noqa: E402
-                           direct_mod_helmholtz_grad)
+                           direct_mod_helmholtz_grad, direct_radial, struve_gf)
 import canon  # noqa: E402
 
 
@@ -63,6 +63,14 @@ def case_inputs(meta):
         g = np.linspace(-0.45, 0.45, meta["n_grid"])
         gx, gy = np.meshgrid(g, g)
         d["tx"], d["ty"] = gx.ravel(), gy.ravel()
+    elif kind == "square100":  # the Struve example's layout, examples/bbfmm_struve.py:48-53
+        rng = np.random.default_rng(meta["seed"])
+        n = meta["n"]
+        x, y = rng.uniform(0, 100, n), rng.uniform(0, 100, n)
+        tau = rng.uniform(0, 1, n)
+        g = np.linspace(0, 100, meta["n_grid"])
+        gx, gy = np.meshgrid(g, g)
+        d = dict(x=x, y=y, tau=tau, tx=gx.ravel(), ty=gy.ravel(), bbox=[-10.0, 110.0, -10.0, 110.0])
     elif kind == "duplicates":
         rng = np.random.default_rng(meta["seed"])
         n = meta["n"]
@@ -112,6 +120,8 @@ CASES = {
                                 method="bb", p=16), True),
     "bb_mh_duplicates_5k_p10_k5": (dict(recipe="duplicates", seed=26, n=5000, n_grid=33, ncut=32,
                                         neq=100, method="bb", p=10, kernel="mh", k=5.0), True),
+    "bb_struve_square_5k_p12": (dict(recipe="square100", seed=27, n=5000, n_grid=41, ncut=30,
+                                     neq=144, method="bb", p=12, kernel="struve"), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -143,6 +153,22 @@ def reference_kernel(meta):
             d2 = dx**2 + dy**2
             return -np.log(d2) / (4 * np.pi)
         return Laplace_Eval
+    if meta["kernel"] == "struve":
+        import ctypes
+        from numba.extending import get_cython_function_address
+        st = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_double, ctypes.c_double)(
+            get_cython_function_address("scipy.special.cython_special", "struve"))
+        y1 = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_double)(
+            get_cython_function_address("scipy.special.cython_special", "y1"))
+
+        # examples/bbfmm_struve.py:29-46, GF from scipy instead of function_generator
+        @numba.njit(fastmath=True)
+        def Kernel(sx, sy, tx, ty):
+            dx = tx - sx
+            dy = ty - sy
+            d = np.sqrt(dx**2 + dy**2)
+            return (d * (y1(d) - st(-3.0, d)) - 4 * st(-2.0, d)) / d**2
+        return Kernel
     k0c, _ = scipy_bessel()
     hk = float(meta["k"])
 
@@ -159,6 +185,8 @@ def reference_kernel(meta):
 def direct(meta, grad, *args):
     if meta.get("kernel", "laplace") == "laplace":
         return (direct_laplace_grad if grad else direct_laplace)(*args)
+    if meta["kernel"] == "struve":
+        return direct_radial(struve_gf, *args)
     sx, sy, tau, tx, ty, check = args
     f = direct_mod_helmholtz_grad if grad else direct_mod_helmholtz
     return f(sx, sy, tau, tx, ty, meta["k"], check)

@@ -180,3 +180,19 @@ def test_mixed_form_rejects_non_scale_invariant_kernel(built_lib):
     with pytest.raises(RuntimeError, match="scale-invariant"):
         KI_FMM(x, y, "Modified_Helmholtz_Eval", 32, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper(),
                precision="mixed", helmholtz_k=5.0)
+
+
+def test_radial_table_kernel_device_matches_host_table(built_lib):
+    """The tabulated radial kernel on the device (direct sum) against the same
+    table evaluated on the host and against the function it was fitted to."""
+    from conftest import struve_kernel
+    from flexmm_b200 import direct_evaluation
+    from oracle.direct import struve_gf
+    k = struve_kernel()
+    r = np.geomspace(1e-6, 200.0, 4000)
+    th = np.linspace(0, 2 * np.pi, r.size)
+    tx, ty = r * np.cos(th), r * np.sin(th)
+    got = direct_evaluation(k, np.zeros(1), np.zeros(1), np.ones(1), tx, ty)
+    np.testing.assert_allclose(got, k.table(r), rtol=1e-13)
+    near = r < 10
+    np.testing.assert_allclose(got[near], struve_gf(r[near]), rtol=5e-12)
