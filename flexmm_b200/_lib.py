@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libflexmm_b200.so")
 
 N_OFFSETS = 40
 PRECISION = {"fp64": 0, "mixed": 1}
-EVALUATORS = {"potential": (0, 1), "gradient": (1, 3)}   # id, outputs
+EVALUATORS = {"potential": (0, 1), "gradient": (1, 3), "stokes": (2, 3)}   # id, outputs
 N_PHASES = 12
 PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "tree_splits",
           "tree_balance", "tree_nodes", "prep", "spare"]
@@ -52,11 +52,27 @@ class BBLevelOps(ctypes.Structure):
 
 BB_MAX_P = 16
 
+
+class StokesLevelOps(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_double),
+        ("large_x", _dp), ("large_y", _dp),
+        ("e2c_u", _dp), ("e2c_sinv", _dp), ("e2c_vh", _dp),
+        ("c2e_u", _dp), ("c2e_sinv", _dp), ("c2e_vh", _dp),
+        ("m2mc", _dp), ("l2lc", _dp),
+        ("m2l_rank", _ip),
+        ("m2l_a", ctypes.POINTER(_dp)),
+        ("m2l_b", ctypes.POINTER(_dp)),
+    ]
+
 # (name, restype, argtypes) of every exported entry point
 SIGNATURES = [
     ("fmm_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("fmm_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(LevelOps), _ip]),
     ("fmm_ops_destroy", ctypes.c_int, [_vp]),
+    ("fmm_stokes_ops_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("fmm_stokes_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(StokesLevelOps), _ip]),
+    ("fmm_build_expansions2", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("fmm_kernel_table_create", ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip]),
     ("fmm_bb_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.POINTER(_vp)]),
     ("fmm_bb_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(BBLevelOps), _ip]),

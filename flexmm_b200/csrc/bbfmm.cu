@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <string>
 
+#include "dense.cuh"
 #include "fmm.cuh"
 #include "timing.cuh"
 
@@ -30,26 +31,6 @@ namespace {
 constexpr int BB_MAX_P = 16;
 constexpr int TCH_BB = 128;   // evaluation threads per work item
 constexpr int SMAX_BB = 1024;  // sources staged per evaluation pass
-
-#define FMMB_BLAS(call)                                                                     \
-  do {                                                                                      \
-    cublasStatus_t st_ = (call);                                                            \
-    if (st_ != CUBLAS_STATUS_SUCCESS)                                                       \
-      throw Error(ERR_CUDA, std::string("cuBLAS error ") + std::to_string(int(st_)) + " in " \
-                                + #call);                                                   \
-  } while (0)
-
-__device__ __forceinline__ int bb_node_level(const int *__restrict__ off, int L, int g) {
-  int lo = 0, hi = L;  // largest l with off[l] <= g
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= g)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
 
 // 2 / width per level: maps a box to [-1, 1]^2 (width_adj, bbfmm.py:122)
 struct BBScale {
@@ -81,7 +62,7 @@ __global__ void __launch_bounds__(128) k_bb_s2m(int p, int np, int L, BBScale sc
   }
   for (int i = blockIdx.x * 4 + warp; i < n_up; i += gridDim.x * 4) {
     const int g = uplist[i];
-    const double a = sc.inv_hw[bb_node_level(off, L, g)];
+    const double a = sc.inv_hw[node_level_of(off, L, g)];
     const double cx = xmid[g], cy = ymid[g];
     const int b = bot[g], e = top[g];
     double acc[8];
@@ -119,72 +100,6 @@ __global__ void __launch_bounds__(128) k_bb_s2m(int p, int np, int L, BBScale sc
       const int q = lane + 32 * k;
       if (q < np) mult[(size_t)g * np + q] = q < nq ? acc[k] : 0.0;
     }
-  }
-}
-
-// rows[e] -> dst row node(e) = parent[c_first + 4 e]  (M2M results to parent rows)
-__global__ void k_bb_to_parents(int n_groups, int np, int c_first, const int *__restrict__ parent,
-                                const double *__restrict__ rows, double *__restrict__ dst) {
-  const int64_t total = (int64_t)n_groups * np;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int e = int(i / np), q = int(i - (int64_t)e * np);
-    dst[(size_t)parent[c_first + 4 * e] * np + q] = rows[i];
-  }
-}
-
-// M2L gather of a level: row 4 g + c (node rg[g] + c) holds, for each offset
-// o, the source multipole il[node][o] (zeros if none) at columns o np .. o np + np
-__global__ void k_bb_m2l_gather(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
-                                const int *__restrict__ il, const double *__restrict__ mult,
-                                double *__restrict__ sbig) {
-  const int64_t rowlen = (int64_t)N_OFFSETS * np;
-  const int64_t total = (int64_t)n_groups * 4 * rowlen;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = i / rowlen;
-    const int col = int(i - row * rowlen), o = col / np, q = col - o * np;
-    const int node = rg[rg_lo + int(row >> 2)] + int(row & 3);
-    const int s = il[(size_t)node * N_OFFSETS + o];
-    sbig[i] = s >= 0 ? mult[(size_t)s * np + q] : 0.0;
-  }
-}
-
-// ple[node(row)] += y[row]
-__global__ void k_bb_add_rows(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
-                              const double *__restrict__ y, double *__restrict__ ple) {
-  const int64_t total = (int64_t)n_groups * 4 * np;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = i / np;
-    const int q = int(i - row * np);
-    const int node = rg[rg_lo + int(row >> 2)] + int(row & 3);
-    ple[(size_t)node * np + q] += y[i];
-  }
-}
-
-// L2L gather: the parent local of every real group of a level
-__global__ void k_bb_parent_locals(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
-                                   const int *__restrict__ parent, const double *__restrict__ ple,
-                                   double *__restrict__ lp) {
-  const int64_t total = (int64_t)n_groups * np;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int g = int(i / np), q = int(i - (int64_t)g * np);
-    lp[i] = ple[(size_t)parent[rg[rg_lo + g]] * np + q];
-  }
-}
-
-// L2L scatter: the 4 children of group g are the consecutive rows rg[g] .. rg[g] + 3
-__global__ void k_bb_add_children(int n_groups, int np, const int *__restrict__ rg, int rg_lo,
-                                  const double *__restrict__ c, double *__restrict__ ple) {
-  const int64_t rowlen = 4 * (int64_t)np;
-  const int64_t total = (int64_t)n_groups * rowlen;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int g = int(i / rowlen);
-    const int64_t k = i - (int64_t)g * rowlen;
-    ple[(size_t)rg[rg_lo + g] * np + k] += c[i];
   }
 }
 
@@ -341,7 +256,7 @@ void run_bb_upward(const BBArgs &b, const double *tau_s, double *mult, cudaStrea
     // M2MC (np x 4np) . children^T (4np x n); M2MC row-major = its transpose column-major
     FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n_groups, 4 * np, &one, b.m2mc,
                           4 * np, mult + (size_t)c_first * np, 4 * np, &zero, rows.get(), np));
-    k_bb_to_parents<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
+    k_rows_to_parents<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
         n_groups, np, c_first, td.parent.get(), rows.get(), mult);
     FMMB_CUDA(cudaGetLastError());
   }
@@ -368,24 +283,24 @@ void run_bb_downward(const BBArgs &b, const double *mult, double *ple, cudaStrea
     const int n = 4 * n_groups;
     if (m >= 3) {  // L2L from level m-1: children += parent local . M2MC (bbfmm.py:161, fmm.py:140-147)
       PhaseTimer timer(PH_DOWNWARD, s);
-      k_bb_parent_locals<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
+      k_gather_parent_rows<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
           n_groups, np, td.rg.get(), lo, td.parent.get(), ple, lp.get());
       FMMB_CUDA(cudaGetLastError());
       FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_N, CUBLAS_OP_N, 4 * np, n_groups, np, &one, b.m2mc,
                             4 * np, lp.get(), np, &zero, c.get(), 4 * np));
-      k_bb_add_children<<<grid_for((int64_t)n_groups * 4 * np, 256), 256, 0, s>>>(
+      k_add_child_rows<<<grid_for((int64_t)n_groups * 4 * np, 256), 256, 0, s>>>(
           n_groups, np, td.rg.get(), lo, c.get(), ple);
       FMMB_CUDA(cudaGetLastError());
     }
     {  // M2L of level m: all 40 offsets in one GEMM (fmm.py:118-131)
       PhaseTimer timer(PH_M2L, s);
-      k_bb_m2l_gather<<<grid_for((int64_t)n * N_OFFSETS * np, 256, 148 * 64), 256, 0, s>>>(
+      k_m2l_gather_cat<<<grid_for((int64_t)n * N_OFFSETS * np, 256, 148 * 64), 256, 0, s>>>(
           n_groups, np, td.rg.get(), lo, td.il.get(), mult, sbig.get());
       FMMB_CUDA(cudaGetLastError());
       FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, N_OFFSETS * np, &one,
                             b.m2l_cat[m], N_OFFSETS * np, sbig.get(), N_OFFSETS * np, &zero, y.get(),
                             np));
-      k_bb_add_rows<<<grid_for((int64_t)n * np, 256), 256, 0, s>>>(n_groups, np, td.rg.get(), lo,
+      k_add_group_rows<<<grid_for((int64_t)n * np, 256), 256, 0, s>>>(n_groups, np, td.rg.get(), lo,
                                                                     y.get(), ple);
       FMMB_CUDA(cudaGetLastError());
     }

@@ -43,6 +43,8 @@ struct LevelEntry {
   DevBuf<float> buf32;
   LevelOpsDev dev;
   DevBuf<double> bb_m2l;  // black-box FMM: [np x 40 np], offset blocks side by side
+  DevBuf<double> st;      // Stokes FMM: this width's operators (StokesArgs::Level layout)
+  StokesArgs::Level st_lev{};
 };
 
 // round to TF32 (10 explicit mantissa bits), to nearest, ties away from zero
@@ -190,7 +192,7 @@ void retain_pool_memory() {
 }
 }  // namespace
 
-constexpr int METHOD_KIFMM = 0, METHOD_BBFMM = 1;
+constexpr int METHOD_KIFMM = 0, METHOD_BBFMM = 1, METHOD_STOKES = 2;
 
 struct fmm_ops {
   int kernel_id;
@@ -216,7 +218,8 @@ struct fmm_plan {
   DevBuf<int> err;              // set by kernels whose bounded waits ran out
   int precision = PREC_FP64;
   bool have_expansions = false;
-  cublasHandle_t blas = nullptr;  // black-box FMM translations
+  DevBuf<double> tau2_s, partial;  // Stokes FMM: sorted fy; partial multipoles
+  cublasHandle_t blas = nullptr;  // black-box and Stokes FMM translations
   ~fmm_plan() {
     if (blas) cublasDestroy(blas);
   }
@@ -246,7 +249,7 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
   return guarded([&] {
     FMMB_CHECK(ops && lv && level_id, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(ops->method == METHOD_KIFMM, ERR_INVALID_ARGUMENT,
-               "black-box operator sets take fmm_bb_ops_add");
+               "black-box and Stokes operator sets take fmm_bb_ops_add / fmm_stokes_ops_add");
     const int n = ops->neq, np = ops->np;
     // host staging in the padded device layout
     std::vector<double> h;
@@ -493,6 +496,86 @@ int fmm_kernel_table_create(const double *coef, int j0, int n_octaves, int n_che
   });
 }
 
+int fmm_stokes_ops_create(int nequiv, fmm_ops **out) {
+  return guarded([&] {
+    FMMB_CHECK(out, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(nequiv >= 1 && nequiv <= FMM_MAX_NEQUIV, ERR_INVALID_ARGUMENT, "nequiv must be in [1, 64]");
+    auto o = std::make_unique<fmm_ops>();
+    o->kernel_id = -1;
+    o->kp = KernelParams{};
+    o->neq = nequiv;
+    o->np = pad8(2 * nequiv + 1);
+    o->method = METHOD_STOKES;
+    *out = o.release();
+  });
+}
+
+int fmm_stokes_ops_add(fmm_ops *ops, const fmm_stokes_level_ops *lv, int *level_id) {
+  return guarded([&] {
+    FMMB_CHECK(ops && lv && level_id && lv->m2l_rank, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(ops->method == METHOD_STOKES, ERR_INVALID_ARGUMENT,
+               "fmm_stokes_ops_add needs a Stokes operator set (fmm_stokes_ops_create)");
+    const int neq = ops->neq, n1 = 2 * neq + 1, n2 = 2 * neq, np = ops->np;
+    const size_t sq = size_t(np) * np, ld = size_t(N_OFFSETS) * np;
+    std::vector<double> h;
+    auto take = [&](size_t count) {
+      size_t at = h.size();
+      h.resize(at + ((count + 1) & ~size_t(1)), 0.0);  // 16-byte aligned blocks
+      return at;
+    };
+    const size_t o_lx = take(neq), o_ly = take(neq);
+    const size_t o_eu = take(sq), o_ev = take(sq), o_cu = take(sq), o_cv = take(sq);
+    const size_t o_mm = take(4 * sq), o_ll = take(4 * sq), o_cat = take(size_t(np) * ld);
+    for (int k = 0; k < neq; ++k) {
+      h[o_lx + k] = lv->large_x[k];
+      h[o_ly + k] = lv->large_y[k];
+    }
+    // x = (b . U) . (diag(1/S) VH); the C2E solve drops the extra unknown (column n2)
+    auto solve = [&](const double *u, const double *sinv, const double *vh, size_t ou, size_t ov,
+                     bool drop_extra) {
+      for (int i = 0; i < n1; ++i)
+        for (int j = 0; j < n1; ++j) {
+          h[ou + size_t(i) * np + j] = u[size_t(i) * n1 + j];
+          if (!(drop_extra && j == n2)) h[ov + size_t(i) * np + j] = sinv[i] * vh[size_t(i) * n1 + j];
+        }
+    };
+    solve(lv->e2c_u, lv->e2c_sinv, lv->e2c_vh, o_eu, o_ev, false);
+    solve(lv->c2e_u, lv->c2e_sinv, lv->c2e_vh, o_cu, o_cv, true);
+    for (int i = 0; i < n1; ++i)
+      for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < n2; ++k) {
+          h[o_mm + size_t(c * np + k) * np + i] = lv->m2mc[size_t(i) * 4 * n2 + c * n2 + k];
+          h[o_ll + size_t(k) * 4 * np + c * np + i] = lv->l2lc[size_t(c * n1 + i) * n2 + k];
+        }
+    for (int o = 0; o < N_OFFSETS; ++o) {
+      const int r = lv->m2l_rank[o];
+      if (r == 0) continue;
+      FMMB_CHECK(lv->m2l_a[o], ERR_INVALID_ARGUMENT, "missing M2L operator");
+      for (int i = 0; i < n1; ++i)
+        for (int k = 0; k < n2; ++k) {
+          double v;
+          if (r < 0) {
+            v = lv->m2l_a[o][size_t(i) * n2 + k];
+          } else {  // M2 [n1 x r] . M1 [r x n2], the reference's truncated operator
+            FMMB_CHECK(lv->m2l_b[o], ERR_INVALID_ARGUMENT, "bad M2L factors");
+            v = 0.0;
+            for (int q = 0; q < r; ++q) v += lv->m2l_a[o][size_t(i) * r + q] * lv->m2l_b[o][size_t(q) * n2 + k];
+          }
+          h[o_cat + size_t(i) * ld + size_t(o) * np + k] = v;
+        }
+    }
+    auto e = std::make_unique<LevelEntry>();
+    e->st.alloc(h.size(), 0);
+    FMMB_CUDA(cudaMemcpy(e->st.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    double *b = e->st.get();
+    e->st_lev = StokesArgs::Level{b + o_lx, b + o_ly, b + o_eu, b + o_ev, b + o_cu,
+                                  b + o_cv, b + o_mm, b + o_ll, b + o_cat};
+    e->dev.inv_w = 1.0 / lv->width;
+    ops->levels.push_back(std::move(e));
+    *level_id = int(ops->levels.size()) - 1;
+  });
+}
+
 int fmm_ops_destroy(fmm_ops *ops) {
   return guarded([&] {
     if (!ops) return;
@@ -537,7 +620,7 @@ int fmm_plan_set_precision(fmm_plan *p, int precision) {
     FMMB_CHECK(precision == PREC_FP64 || kernel_scaled(p->ops->kernel_id), ERR_UNSUPPORTED,
                "the mixed form needs a scale-invariant kernel (Laplace)");
     FMMB_CHECK(precision == PREC_FP64 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
-               "the black-box FMM has an FP64 form only");
+               "the black-box and Stokes FMMs have an FP64 form only");
     p->precision = precision;
     p->have_expansions = false;
   });
@@ -568,6 +651,29 @@ static PassArgs pass_args(fmm_plan *p) {
   return a;
 }
 
+static void ensure_blas(fmm_plan *p, cudaStream_t s) {
+  if (!p->blas) {
+    FMMB_CHECK(cublasCreate(&p->blas) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasCreate failed");
+    // no TF32 / reduced-precision paths: these forms are FP64 end to end
+    FMMB_CHECK(cublasSetMathMode(p->blas, CUBLAS_PEDANTIC_MATH) == CUBLAS_STATUS_SUCCESS, ERR_CUDA,
+               "cublasSetMathMode failed");
+  }
+  FMMB_CHECK(cublasSetStream(p->blas, s) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasSetStream failed");
+}
+
+static StokesArgs stokes_args(fmm_plan *p, cudaStream_t s) {
+  ensure_blas(p, s);
+  StokesArgs a{};
+  a.neq = p->ops->neq;
+  a.np = p->ops->np;
+  a.td = &p->td;
+  a.th = &p->th;
+  a.blas = p->blas;
+  for (int m = 0; m < p->th.L && m < FMM_MAX_LEVELS_DEV; ++m)
+    if (p->bound[m] >= 0) a.lev[m] = p->ops->levels[p->bound[m]]->st_lev;
+  return a;
+}
+
 static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
   BBArgs b{};
   b.kernel_id = p->ops->kernel_id;
@@ -576,13 +682,7 @@ static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
   b.np = p->ops->np;
   b.td = &p->td;
   b.th = &p->th;
-  if (!p->blas) {
-    FMMB_CHECK(cublasCreate(&p->blas) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasCreate failed");
-    // no TF32 / reduced-precision paths: the black-box form is FP64 end to end
-    FMMB_CHECK(cublasSetMathMode(p->blas, CUBLAS_PEDANTIC_MATH) == CUBLAS_STATUS_SUCCESS, ERR_CUDA,
-               "cublasSetMathMode failed");
-  }
-  FMMB_CHECK(cublasSetStream(p->blas, s) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasSetStream failed");
+  ensure_blas(p, s);
   b.blas = p->blas;
   b.m2mc = p->ops->bb_m2mc.get();
   for (int m = 0; m < p->th.L && m < FMM_MAX_LEVELS_DEV; ++m)
@@ -590,9 +690,37 @@ static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
   return b;
 }
 
+int fmm_build_expansions2(fmm_plan *p, const double *fx, const double *fy, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p && fx && fy, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(p->ops->method == METHOD_STOKES, ERR_INVALID_ARGUMENT,
+               "fmm_build_expansions2 takes Stokes plans (two force components)");
+    cudaStream_t s = (cudaStream_t)stream;
+    const TreeHost &th = p->th;
+    for (int m = 2; m < th.L; ++m)
+      FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
+    const int np = p->ops->np;
+    const int64_t total = th.n_total();
+    StokesArgs a = stokes_args(p, s);
+    p->tau_s.alloc(th.n_points, s);
+    p->tau2_s.alloc(th.n_points, s);
+    gather_sorted(fx, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
+    gather_sorted(fy, p->td.ordv.get(), th.n_points, p->tau2_s.get(), s);
+    for (DevBuf<double> *b : {&p->partial, &p->mult, &p->ple, &p->loc}) {
+      b->alloc(total * np, s);
+      b->zero(s);
+    }
+    run_stokes_upward(a, p->tau_s.get(), p->tau2_s.get(), p->partial.get(), p->mult.get(), s);
+    run_stokes_downward(a, p->mult.get(), p->ple.get(), p->loc.get(), s);
+    p->have_expansions = true;
+  });
+}
+
 int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
   return guarded([&] {
     FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(p->ops->method != METHOD_STOKES, ERR_INVALID_ARGUMENT,
+               "Stokes plans take fmm_build_expansions2 (two force components)");
     cudaStream_t s = (cudaStream_t)stream;
     const TreeHost &th = p->th;
     for (int m = 2; m < th.L; ++m)
@@ -656,9 +784,19 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
 namespace {
 // outputs of an evaluator id (FMM_EVAL_*)
 int evaluator_outputs(int evaluator) {
-  FMMB_CHECK(evaluator == FMM_EVAL_POTENTIAL || evaluator == FMM_EVAL_GRADIENT,
-             ERR_INVALID_ARGUMENT, "evaluator must be FMM_EVAL_POTENTIAL or FMM_EVAL_GRADIENT");
-  return evaluator == FMM_EVAL_GRADIENT ? 3 : 1;
+  FMMB_CHECK(evaluator == FMM_EVAL_POTENTIAL || evaluator == FMM_EVAL_GRADIENT ||
+                 evaluator == FMM_EVAL_STOKES,
+             ERR_INVALID_ARGUMENT, "evaluator must be one of FMM_EVAL_POTENTIAL, _GRADIENT, _STOKES");
+  return evaluator == FMM_EVAL_POTENTIAL ? 1 : 3;
+}
+
+// a plan's method accepts the evaluator (Stokes plans: (u, v, p) only)
+void check_evaluator(fmm_plan *p, int evaluator) {
+  FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+  const bool st = p->ops->method == METHOD_STOKES;
+  FMMB_CHECK(st == (evaluator == FMM_EVAL_STOKES), ERR_INVALID_ARGUMENT,
+             st ? "Stokes plans evaluate FMM_EVAL_STOKES (u, v, p)"
+                : "FMM_EVAL_STOKES needs a Stokes plan");
 }
 
 void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, int64_t m,
@@ -670,12 +808,13 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
   FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
   FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
   FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the target count");
-  FMMB_CHECK(nout == 1 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
+  FMMB_CHECK(nout == 1 || p->ops->method != METHOD_BBFMM, ERR_UNSUPPORTED,
              "the black-box FMM evaluates potentials only");
   PassArgs a = pass_args(p);
   DevBuf<uint64_t> tkeys;
   DevBuf<int> tperm;
   DevBuf<double> txs, tys;
+  // evaluator ids carry the output count; Stokes plans produce (u, v, p)
   {
     PhaseTimer timer(PH_SORT_TGT, s);
     // leaves live on levels <= L-1: their first L-1 digits decide everything
@@ -685,7 +824,10 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
     gather_sorted(tx, tperm.get(), m, txs.get(), s);
     gather_sorted(ty, tperm.get(), m, tys.get(), s);
   }
-  if (p->ops->method == METHOD_BBFMM)
+  if (p->ops->method == METHOD_STOKES)
+    run_stokes_evaluate(stokes_args(p, s), p->tau_s.get(), p->tau2_s.get(), p->loc.get(), txs.get(),
+                        tys.get(), tkeys.get(), tperm.get(), m, check, out, ld_out, s);
+  else if (p->ops->method == METHOD_BBFMM)
     run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), txs.get(), tys.get(), tkeys.get(),
                     tperm.get(), m, check, out, s);
   else if (p->precision == PREC_MIXED)
@@ -704,12 +846,16 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
   const TreeDev &td = p->td;
   const int64_t m = p->th.n_points;
   FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the source count");
-  FMMB_CHECK(nout == 1 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
+  FMMB_CHECK(nout == 1 || p->ops->method != METHOD_BBFMM, ERR_UNSUPPORTED,
              "the black-box FMM evaluates potentials only");
   PassArgs a = pass_args(p);
   // the tree's sorted copy: keys sorted on at least their top L-1 digits,
   // which is all that leaf location reads
-  if (p->ops->method == METHOD_BBFMM)
+  if (p->ops->method == METHOD_STOKES)
+    run_stokes_evaluate(stokes_args(p, s), p->tau_s.get(), p->tau2_s.get(), p->loc.get(),
+                        td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, out,
+                        ld_out, s);
+  else if (p->ops->method == METHOD_BBFMM)
     run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), td.sx.get(), td.sy.get(),
                     td.pkeys.get(), td.ordv.get(), m, check, out, s);
   else if (p->precision == PREC_MIXED)
@@ -724,25 +870,34 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
 
 int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int check,
                  double *out, void *stream) {
-  return guarded([&] { evaluate_points(p, 1, tx, ty, m, check, out, m, (cudaStream_t)stream); });
+  return guarded([&] {
+    check_evaluator(p, FMM_EVAL_POTENTIAL);
+    evaluate_points(p, 1, tx, ty, m, check, out, m, (cudaStream_t)stream);
+  });
 }
 
 int fmm_evaluate_sources(fmm_plan *p, int check, double *out, void *stream) {
-  return guarded([&] { evaluate_own_sources(p, 1, check, out, 0, (cudaStream_t)stream); });
+  return guarded([&] {
+    check_evaluator(p, FMM_EVAL_POTENTIAL);
+    evaluate_own_sources(p, 1, check, out, 0, (cudaStream_t)stream);
+  });
 }
 
 int fmm_evaluate_outputs(fmm_plan *p, int evaluator, const double *tx, const double *ty,
                          int64_t m, int check, double *out, int64_t ld_out, void *stream) {
   return guarded([&] {
-    evaluate_points(p, evaluator_outputs(evaluator), tx, ty, m, check, out, ld_out,
-                    (cudaStream_t)stream);
+    const int nout = evaluator_outputs(evaluator);
+    check_evaluator(p, evaluator);
+    evaluate_points(p, nout, tx, ty, m, check, out, ld_out, (cudaStream_t)stream);
   });
 }
 
 int fmm_evaluate_sources_outputs(fmm_plan *p, int evaluator, int check, double *out,
                                  int64_t ld_out, void *stream) {
   return guarded([&] {
-    evaluate_own_sources(p, evaluator_outputs(evaluator), check, out, ld_out, (cudaStream_t)stream);
+    const int nout = evaluator_outputs(evaluator);
+    check_evaluator(p, evaluator);
+    evaluate_own_sources(p, nout, check, out, ld_out, (cudaStream_t)stream);
   });
 }
 

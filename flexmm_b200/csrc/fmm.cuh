@@ -73,6 +73,33 @@ void run_bb_evaluate(const BBArgs &b, const double *tau_sorted, const double *lo
                      const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
                      int64_t m, int check, double *out, cudaStream_t s);
 
+// Stokes FMM (stokes.cu): rows of np = pad8(2 Neq + 1) doubles; per level
+// the large circle and the row-major operators of the GEMMs:
+//   e2c_u, e2c_vhs [np x np]: E2C solve x = (b . U) . (diag(1/S) VH);
+//   c2e_u, c2e_vhs [np x np]: C2E solve, the extra unknown's column zeroed;
+//   m2mc [4np x np]: parent check row = children rows . m2mc;
+//   l2lc [np x 4np]: children partial-local rows = local row . l2lc;
+//   m2l_cat [np x 40np]: the 40 M2L operators side by side.
+struct StokesArgs {
+  int neq, np;
+  const TreeDev *td;
+  const TreeHost *th;
+  cublasHandle_t blas;
+  struct Level {
+    const double *lx, *ly;
+    const double *e2c_u, *e2c_vhs, *c2e_u, *c2e_vhs, *m2mc, *l2lc, *m2l_cat;
+  } lev[FMM_MAX_LEVELS_DEV];
+};
+void run_stokes_upward(const StokesArgs &a, const double *fx, const double *fy, double *partial,
+                       double *mult, cudaStream_t s);
+void run_stokes_downward(const StokesArgs &a, const double *mult, double *ple, double *loc,
+                         cudaStream_t s);
+// out rows (u, v, p), stride ld_out
+void run_stokes_evaluate(const StokesArgs &a, const double *fx, const double *fy, const double *loc,
+                         const double *txs, const double *tys, const uint64_t *tkeys,
+                         const int *tperm, int64_t m, int check, double *out, int64_t ld_out,
+                         cudaStream_t s);
+
 void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaStream_t s);
 void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s);
 void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s);

@@ -1,0 +1,318 @@
+// Stokes FMM passes in FP64 (flexmm/kifmm2d/vector/stokes_fmm.py:550-858).
+//
+// A box carries 2 Neq + 1 values (row of np doubles): the equivalent forces
+// (fx, fy) on Neq points of a circle plus one extra unknown of the corrected
+// (pressure-augmented) forms; check values are the velocities (u, v) on Neq
+// points plus the pressure at the circle's centre.  Per level:
+//  * upward: partial = S2M (velocities on the check circle from the leaf's
+//    sources; pressure row 0, as upwards_pass, stokes_fmm.py:259-291, ignores
+//    kernel_add's pressure) + M2MC . children (extra unknowns excluded), then
+//    the factored-SVD solve of the corrected equivalent-to-check form
+//    (E2C_SVD, stokes_fmm.py:553-558);
+//  * downward: partial locals += L2LC . parent local (real sibling groups) and
+//    += M2L . source multipoles (the 40 offsets as one offset-concatenated
+//    GEMM, a missing source a zero block), then the C2E solve, extra unknown
+//    dropped (stokes_fmm.py:712-733);
+//  * evaluation: (u, v, p) from the leaf's local forces on the large circle
+//    (local_expansion_evaluation, stokes_fmm.py:331-360) plus the colleagues'
+//    sources (neighbor_evaluation, stokes_fmm.py:361-396).
+// Solves and translations are cuBLAS DGEMMs on the plan's stream.
+#include <cublas_v2.h>
+
+#include <algorithm>
+
+#include "dense.cuh"
+#include "fmm.cuh"
+#include "timing.cuh"
+
+namespace fmmb {
+namespace {
+
+constexpr int TCH_ST = 128;
+constexpr int SMAX_ST = 1024;
+
+struct StokesCircles {
+  const double *lx[FMM_MAX_LEVELS_DEV], *ly[FMM_MAX_LEVELS_DEV];  // large circle, per level
+};
+
+// one Stokeslet pair, unscaled: u, v times 1/(4 pi), p times 1/(2 pi) later
+// (kernel_apply_single, stokes_fmm.py:166-187)
+__device__ __forceinline__ void stokeslet(double dx, double dy, double fx, double fy, double &u,
+                                          double &v, double &p) {
+  const double id2 = 1.0 / (dx * dx + dy * dy);
+  const double logid = 0.5 * log(id2);
+  const double dxdy = dx * dy * id2;
+  u += (logid + dx * dx * id2) * fx + dxdy * fy;
+  v += dxdy * fx + (logid + dy * dy * id2) * fy;
+  p += (fx * dx + fy * dy) * id2;
+}
+
+// S2M: velocities at the large circle's points from the box's sources; one
+// warp per S2M node, lane k owns check points k and k + 32
+__global__ void __launch_bounds__(128) k_stokes_s2m(int neq, int np, int L, StokesCircles cir,
+                                                    const int *__restrict__ off,
+                                                    const int *__restrict__ uplist,
+                                                    const int *__restrict__ n_up_ptr,
+                                                    const int *__restrict__ bot,
+                                                    const int *__restrict__ top,
+                                                    const double *__restrict__ xmid,
+                                                    const double *__restrict__ ymid,
+                                                    const double *__restrict__ sx,
+                                                    const double *__restrict__ sy,
+                                                    const double *__restrict__ fx,
+                                                    const double *__restrict__ fy,
+                                                    double *__restrict__ partial) {
+  __shared__ double qx[4][32], qy[4][32], qf[4][32], qg[4][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_up = *n_up_ptr;
+  for (int i = blockIdx.x * 4 + warp; i < n_up; i += gridDim.x * 4) {
+    const int g = uplist[i];
+    const int m = node_level_of(off, L, g);
+    const double cx = xmid[g], cy = ymid[g];
+    double ex[2], ey[2], u[2] = {0.0, 0.0}, v[2] = {0.0, 0.0}, p[2] = {0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = lane + 32 * h;
+      ex[h] = k < neq ? cir.lx[m][k] : 0.0;
+      ey[h] = k < neq ? cir.ly[m][k] : 0.0;
+    }
+    const int b = bot[g], e = top[g];
+    for (int j0 = b; j0 < e; j0 += 32) {
+      const int nj = min(32, e - j0);
+      if (lane < nj) {
+        qx[warp][lane] = sx[j0 + lane] - cx;
+        qy[warp][lane] = sy[j0 + lane] - cy;
+        qf[warp][lane] = fx[j0 + lane];
+        qg[warp][lane] = fy[j0 + lane];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (lane + 32 * h < neq)
+          for (int j = 0; j < nj; ++j)
+            stokeslet(ex[h] - qx[warp][j], ey[h] - qy[warp][j], qf[warp][j], qg[warp][j], u[h],
+                      v[h], p[h]);
+      __syncwarp();
+    }
+    const double us = 0.25 / M_PI;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = lane + 32 * h;
+      if (k < neq) {
+        partial[(size_t)g * np + k] = u[h] * us;
+        partial[(size_t)g * np + neq + k] = v[h] * us;
+      }
+    }
+  }
+}
+
+// Evaluation: (u, v, p) rows of out (stride ld_out).  One work item = (leaf,
+// up to 128 of its targets); G threads share a target.
+__global__ void __launch_bounds__(TCH_ST) k_stokes_evaluate(
+    int neq, int np, StokesCircles cir, const int4 *__restrict__ items,
+    const int *__restrict__ n_items_ptr, const int *__restrict__ coll, const int *__restrict__ bot,
+    const int *__restrict__ top, const double *__restrict__ xmid, const double *__restrict__ ymid,
+    const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ fx,
+    const double *__restrict__ fy, const double *__restrict__ loc, const double *__restrict__ txs,
+    const double *__restrict__ tys, const int *__restrict__ tperm, int check,
+    double *__restrict__ out, int64_t ld_out) {
+  __shared__ double ssx[SMAX_ST], ssy[SMAX_ST], sfx[SMAX_ST], sfy[SMAX_ST];
+  __shared__ int rb[9], rs[10];
+  __shared__ double red[3][TCH_ST / 32];
+  const int n_items = *n_items_ptr;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int4 it = items[item];
+    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
+    int G = 1;
+    while (2 * G * cnt <= TCH_ST) G *= 2;
+    const int t = threadIdx.x / G, sub = threadIdx.x % G;
+    const bool valid = t < cnt;
+    const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
+    if (threadIdx.x < 9) {
+      const int cg = coll[(size_t)g * 9 + threadIdx.x];
+      rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
+      rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
+    }
+    if (threadIdx.x == 0) rs[0] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
+    double u = 0.0, v = 0.0, p = 0.0;
+    if (lev >= 2 && valid) {  // L2T: local forces on the large circle
+      const double dx0 = x - xmid[g], dy0 = y - ymid[g];
+      const double *lf = loc + (size_t)g * np;
+      for (int k = sub; k < neq; k += G)
+        stokeslet(dx0 - cir.lx[lev][k], dy0 - cir.ly[lev][k], lf[k], lf[neq + k], u, v, p);
+    }
+    __syncthreads();
+    const int ns = rs[9];
+    for (int base = 0; base < ns; base += SMAX_ST) {
+      const int nb = min(SMAX_ST, ns - base);
+      for (int i = threadIdx.x; i < nb; i += TCH_ST) {
+        const int idx = base + i;
+        int c = 0;
+        while (idx >= rs[c + 1]) ++c;
+        const int j = rb[c] + (idx - rs[c]);
+        ssx[i] = sx[j];
+        ssy[i] = sy[j];
+        sfx[i] = fx[j];
+        sfy[i] = fy[j];
+      }
+      __syncthreads();
+      if (valid)
+        for (int j = sub; j < nb; j += G) {
+          const double dx = x - ssx[j], dy = y - ssy[j];
+          if (!(check && dx == 0.0 && dy == 0.0)) stokeslet(dx, dy, sfx[j], sfy[j], u, v, p);
+        }
+      __syncthreads();
+    }
+    double r[3] = {u * (0.25 / M_PI), v * (0.25 / M_PI), p * (0.5 / M_PI)};
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+      double w = r[o];
+      for (int s = min(G, 32) >> 1; s >= 1; s >>= 1) w += __shfl_xor_sync(0xffffffffu, w, s);
+      if (G > 32) {
+        if ((threadIdx.x & 31) == 0) red[o][threadIdx.x >> 5] = w;
+        __syncthreads();
+        if (sub == 0) {
+          w = 0.0;
+          for (int q = 0; q < G / 32; ++q) w += red[o][(threadIdx.x >> 5) + q];
+        }
+      }
+      if (valid && sub == 0) out[o * ld_out + tperm[t0 + t]] = w;
+    }
+    __syncthreads();
+  }
+}
+
+StokesCircles circles(const StokesArgs &a) {
+  StokesCircles c{};
+  for (int m = 0; m < a.th->L && m < FMM_MAX_LEVELS_DEV; ++m) {
+    c.lx[m] = a.lev[m].lx;
+    c.ly[m] = a.lev[m].ly;
+  }
+  return c;
+}
+
+// rows [r0, r0 + n) of x := ((b . U) . VHs), row-major np x np operators
+void solve_rows(const StokesArgs &a, const double *u, const double *vhs, const double *b, double *x,
+                double *tmp, int n) {
+  const double one = 1.0, zero = 0.0;
+  const int np = a.np;
+  FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, np, n, np, &one, u, np, b, np, &zero, tmp, np));
+  FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, np, n, np, &one, vhs, np, tmp, np, &zero, x, np));
+}
+
+}  // namespace
+
+void run_stokes_upward(const StokesArgs &a, const double *fx, const double *fy, double *partial,
+                       double *mult, cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  if (th.L < 3) return;
+  FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
+  const int np = a.np;
+  PhaseTimer timer(PH_UPWARD, s);
+  k_stokes_s2m<<<148 * 8, 128, 0, s>>>(a.neq, np, th.L, circles(a), td.dev_off.get(),
+                                       td.uplist.get(), td.n_up.get(), td.bot.get(), td.top.get(),
+                                       td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), fx, fy,
+                                       partial);
+  FMMB_CUDA(cudaGetLastError());
+  int max_rows = 0;
+  for (int m = 2; m < th.L; ++m) max_rows = std::max(max_rows, th.off[m + 1] - th.off[m]);
+  DevBuf<double> tmp;
+  tmp.alloc((size_t)max_rows * np, s);
+  FMMB_BLAS(cublasSetStream(a.blas, s));
+  const double one = 1.0, zero = 0.0;
+  for (int m = th.L - 1; m >= 2; --m) {
+    if (m <= th.L - 2) {  // partial of level m's parents += M2MC . children
+      const int c_first = th.off[m + 1];
+      const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
+      if (n_groups > 0) {
+        FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, np, n_groups, 4 * np, &one,
+                              a.lev[m].m2mc, np, mult + (size_t)c_first * np, 4 * np, &zero,
+                              tmp.get(), np));
+        k_rows_to_parents<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
+            n_groups, np, c_first, td.parent.get(), tmp.get(), partial);
+        FMMB_CUDA(cudaGetLastError());
+      }
+    }
+    const int r0 = th.off[m], n = th.off[m + 1] - th.off[m];
+    if (n > 0)
+      solve_rows(a, a.lev[m].e2c_u, a.lev[m].e2c_vhs, partial + (size_t)r0 * np,
+                 mult + (size_t)r0 * np, tmp.get(), n);
+  }
+}
+
+void run_stokes_downward(const StokesArgs &a, const double *mult, double *ple, double *loc,
+                         cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  if (th.L < 3) return;
+  const int np = a.np;
+  int max_groups = 0, max_rows = 0;
+  for (int m = 2; m < th.L; ++m) {
+    max_groups = std::max(max_groups, th.rg_hi[m] - th.rg_lo[m]);
+    max_rows = std::max(max_rows, th.off[m + 1] - th.off[m]);
+  }
+  DevBuf<double> sbig, y, lp, c, tmp;
+  sbig.alloc((size_t)std::max(max_groups, 1) * 4 * N_OFFSETS * np, s);
+  y.alloc((size_t)std::max(max_groups, 1) * 4 * np, s);
+  lp.alloc((size_t)std::max(max_groups, 1) * np, s);
+  c.alloc((size_t)std::max(max_groups, 1) * 4 * np, s);
+  tmp.alloc((size_t)std::max(max_rows, 1) * np, s);
+  FMMB_BLAS(cublasSetStream(a.blas, s));
+  const double one = 1.0, zero = 0.0;
+  for (int m = 2; m < th.L; ++m) {
+    const int lo = th.rg_lo[m], n_groups = th.rg_hi[m] - th.rg_lo[m];
+    if (n_groups > 0) {
+      const int n = 4 * n_groups;
+      if (m >= 3) {  // L2L from level m-1 (stokes_fmm.py:726-733)
+        PhaseTimer timer(PH_DOWNWARD, s);
+        k_gather_parent_rows<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
+            n_groups, np, td.rg.get(), lo, td.parent.get(), loc, lp.get());
+        FMMB_CUDA(cudaGetLastError());
+        FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, 4 * np, n_groups, np, &one,
+                              a.lev[m - 1].l2lc, 4 * np, lp.get(), np, &zero, c.get(), 4 * np));
+        k_add_child_rows<<<grid_for((int64_t)n_groups * 4 * np, 256), 256, 0, s>>>(
+            n_groups, np, td.rg.get(), lo, c.get(), ple);
+        FMMB_CUDA(cudaGetLastError());
+      }
+      PhaseTimer timer(PH_M2L, s);
+      k_m2l_gather_cat<<<grid_for((int64_t)n * N_OFFSETS * np, 256, 148 * 64), 256, 0, s>>>(
+          n_groups, np, td.rg.get(), lo, td.il.get(), mult, sbig.get());
+      FMMB_CUDA(cudaGetLastError());
+      FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, N_OFFSETS * np, &one,
+                            a.lev[m].m2l_cat, N_OFFSETS * np, sbig.get(), N_OFFSETS * np, &zero,
+                            y.get(), np));
+      k_add_group_rows<<<grid_for((int64_t)n * np, 256), 256, 0, s>>>(n_groups, np, td.rg.get(),
+                                                                       lo, y.get(), ple);
+      FMMB_CUDA(cudaGetLastError());
+    }
+    const int r0 = th.off[m], nr = th.off[m + 1] - th.off[m];
+    if (nr > 0)
+      solve_rows(a, a.lev[m].c2e_u, a.lev[m].c2e_vhs, ple + (size_t)r0 * np, loc + (size_t)r0 * np,
+                 tmp.get(), nr);
+  }
+}
+
+void run_stokes_evaluate(const StokesArgs &a, const double *fx, const double *fy, const double *loc,
+                         const double *txs, const double *tys, const uint64_t *tkeys,
+                         const int *tperm, int64_t m, int check, double *out, int64_t ld_out,
+                         cudaStream_t s) {
+  if (m == 0) return;
+  const TreeDev &td = *a.td;
+  PassArgs pa{};
+  pa.th = a.th;
+  pa.td = a.td;
+  EvalItems it;
+  eval_items(pa, tkeys, m, it, s);
+  PhaseTimer timer(PH_EVAL, s);
+  k_stokes_evaluate<<<148 * 8, TCH_ST, 0, s>>>(
+      a.neq, a.np, circles(a), it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+      td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), fx, fy, loc, txs, tys,
+      tperm, check, out, ld_out);
+  FMMB_CUDA(cudaGetLastError());
+}
+
+}  // namespace fmmb

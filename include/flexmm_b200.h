@@ -69,6 +69,34 @@ typedef struct fmm_level_ops {
   const double *const *m2l_b;      /* [40] SVD: M1 [r*n]; otherwise unused    */
 } fmm_level_ops;
 
+/* Stokes FMM operator set (kifmm2d/vector/stokes_fmm.py:550-858): Nequiv
+ * points per circle, 2 Nequiv + 1 values per box.  Per box width the host
+ * supplies (n1 = 2 Nequiv + 1, n2 = 2 Nequiv, row-major, FP64):
+ *   large_x/y [Nequiv]  the check / local-equivalent circle (dd = 0.1);
+ *   e2c_u, e2c_sinv, e2c_vh   SVD of the corrected small-to-large form
+ *                             [n1 x n1], 1/S with 0 where S < 1e-15;
+ *   c2e_u, c2e_sinv, c2e_vh   the same for the large-to-small form;
+ *   m2mc [n1 x 4 n2]      children equivalent forces -> parent check values;
+ *   l2lc [4 n1 x n2]      parent local forces -> children partial locals;
+ *   m2l: per offset rank < 0 dense [n1 x n2], rank > 0 M2 [n1 x r], M1 [r x n2].
+ * (Precomputation, stokes_fmm.py:541-591.)  Plans on such a set build with
+ * fmm_build_expansions2 and evaluate with FMM_EVAL_STOKES. */
+typedef struct fmm_stokes_level_ops {
+  double width;
+  const double *large_x, *large_y;
+  const double *e2c_u, *e2c_sinv, *e2c_vh;
+  const double *c2e_u, *c2e_sinv, *c2e_vh;
+  const double *m2mc, *l2lc;
+  const int *m2l_rank;
+  const double *const *m2l_a;
+  const double *const *m2l_b;
+} fmm_stokes_level_ops;
+int fmm_stokes_ops_create(int nequiv, fmm_ops **out);
+int fmm_stokes_ops_add(fmm_ops *ops, const fmm_stokes_level_ops *lv, int *level_id);
+/* FMM.build_expansions(taux, tauy) of the Stokes FMM (stokes_fmm.py:642-735):
+ * device forces in the caller's source order. */
+int fmm_build_expansions2(fmm_plan *plan, const double *fx, const double *fy, void *stream);
+
 /* Kernel ids: 0 Laplace -log(r^2)/(4 pi) (examples/kifmm_laplace.py:24-29);
  * 1 modified Helmholtz K0(k r)/(2 pi), kparams[0] = k
  * (examples/kifmm_modified_helmholtz.py:25-39); 2 a tabulated radial kernel
@@ -152,6 +180,7 @@ int fmm_evaluate_sources(fmm_plan *plan, int check, double *out, void *stream);
  * Row r of the result is out[r * ld_out .. r * ld_out + m), ld_out >= m. */
 #define FMM_EVAL_POTENTIAL 0
 #define FMM_EVAL_GRADIENT 1
+#define FMM_EVAL_STOKES 2 /* Stokes plans: 3 rows u, v, p (stokes_fmm.py:820-835) */
 int fmm_evaluate_outputs(fmm_plan *plan, int evaluator, const double *tx, const double *ty,
                          int64_t m, int check, double *out, int64_t ld_out, void *stream);
 /* The same at the plan's own source points (see fmm_evaluate_sources). */

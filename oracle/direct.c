@@ -57,3 +57,32 @@ void oracle_direct_laplace_grad(const double *sx, const double *sy, const double
         out[2 * nt + j] = uy;
     }
 }
+
+/* Stokeslet direct sum: rows out[0..2][nt] = (u, v, p) from forces (fx, fy),
+ * kernel_apply_single / kernel_apply_single_check of
+ * flexmm/kifmm2d/vector/stokes_fmm.py:100-187: u, v scaled by 1/(4 pi),
+ * p by 1/(2 pi); coincident pairs skipped when check. */
+void oracle_direct_stokes(const double *sx, const double *sy, const double *fx,
+                          const double *fy, int64_t ns, const double *tx, const double *ty,
+                          int64_t nt, int check, double *out)
+{
+    const double us = 0.25 / M_PI, ps = 0.5 / M_PI;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t j = 0; j < nt; ++j) {
+        double u = 0.0, v = 0.0, p = 0.0;
+        const double x = tx[j], y = ty[j];
+        for (int64_t i = 0; i < ns; ++i) {
+            double dx = x - sx[i], dy = y - sy[i];
+            if (check && dx == 0.0 && dy == 0.0) continue;
+            double id2 = 1.0 / (dx * dx + dy * dy);
+            double logid = 0.5 * log(id2);
+            double dxdy = dx * dy * id2;
+            u += (logid + dx * dx * id2) * fx[i] + dxdy * fy[i];
+            v += dxdy * fx[i] + (logid + dy * dy * id2) * fy[i];
+            p += (fx[i] * dx + fy[i] * dy) * id2;
+        }
+        out[j] = u * us;
+        out[nt + j] = v * us;
+        out[2 * nt + j] = p * ps;
+    }
+}

@@ -29,6 +29,9 @@ def _load():
         g = _lib.oracle_direct_laplace_grad
         g.argtypes = f.argtypes
         g.restype = None
+        h = _lib.oracle_direct_stokes
+        h.argtypes = [dp, dp, dp, dp, ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
+        h.restype = None
     return _lib
 
 
@@ -127,4 +130,14 @@ def direct_radial(f, sx, sy, tau, tx, ty, check):
         r = np.sqrt(dx * dx + dy * dy)
         skip = (dx == 0) & (dy == 0) if check else np.zeros(r.shape, dtype=bool)
         out[a:b] = (f(np.where(skip, 1.0, r)) * np.where(skip, 0.0, tau[None, :])).sum(1)
+    return out
+
+
+def direct_stokes(sx, sy, fx, fy, tx, ty, check):
+    """FP64 Stokeslet direct sum -> [3, nt] rows (u, v, p)."""
+    lib = _load()
+    sx, sy, fx, fy, tx, ty = (np.ascontiguousarray(a, dtype=np.float64) for a in (sx, sy, fx, fy, tx, ty))
+    out = np.empty((3, tx.size))
+    lib.oracle_direct_stokes(_p(sx), _p(sy), _p(fx), _p(fy), sx.size, _p(tx), _p(ty), tx.size,
+                             1 if check else 0, _p(out))
     return out

@@ -17,11 +17,14 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
-def golden_cases(gradient=False):
-    """Fixture names: potential cases, or (gradient=True) the grad_* cases
-    whose results are [3, n] rows (u, du/dx, du/dy)."""
+def golden_cases(gradient=False, stokes=False):
+    """Fixture names: potential cases; (gradient=True) the grad_* cases whose
+    results are [3, n] rows (u, du/dx, du/dy); (stokes=True) the stokes_*
+    cases, rows (u, v, p)."""
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
-    return [n for n in names if n.startswith("grad_") == gradient]
+    if stokes:
+        return [n for n in names if n.startswith("stokes_")]
+    return [n for n in names if n.startswith("grad_") == gradient and not n.startswith("stokes_")]
 
 
 def load_golden(name):

@@ -40,7 +40,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 from flexmm_b200 import workloads  # noqa: E402
 from oracle import refimport  # noqa: E402
 from oracle.direct import (direct_laplace, direct_laplace_grad, direct_mod_helmholtz,  # noqa: E402
-                           direct_mod_helmholtz_grad, direct_radial, struve_gf)
+                           direct_mod_helmholtz_grad, direct_radial, direct_stokes, struve_gf)
 import canon  # noqa: E402
 
 
@@ -86,6 +86,8 @@ def case_inputs(meta):
         raise ValueError(kind)
     if meta.get("bbox", "given") == "none":
         d["bbox"] = None
+    if meta.get("method") == "stokes":  # second force component
+        d["tau2"] = np.random.default_rng(meta["seed"] + 1000).standard_normal(d["x"].size)
     return d
 
 
@@ -122,6 +124,12 @@ CASES = {
                                         neq=100, method="bb", p=10, kernel="mh", k=5.0), True),
     "bb_struve_square_5k_p12": (dict(recipe="square100", seed=27, n=5000, n_grid=41, ncut=30,
                                      neq=144, method="bb", p=12, kernel="struve"), True),
+    "stokes_uniform_3k_q16": (dict(recipe="uniform", seed=28, n=3000, n_grid=41, ncut=16, neq=16,
+                                   method="stokes"), True),
+    "stokes_clustered_20k_q32": (dict(recipe="clustered", seed=29, n=20000, n_grid=64, ncut=64,
+                                      neq=32, method="stokes"), True),
+    "stokes_duplicates_5k_q24": (dict(recipe="duplicates", seed=30, n=5000, n_grid=33, ncut=16,
+                                      neq=24, method="stokes"), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -311,6 +319,35 @@ def run_gradient_case(name, meta, ref):
           flush=True)
 
 
+def run_stokes_case(name, meta, ref):
+    """The reference's Stokes FMM (flexmm/kifmm2d/vector/stokes_fmm.py:592-858):
+    src_val / tgt_val are [3, n] rows (u, v, p)."""
+    from flexmm.kifmm2d.vector.stokes_fmm import FMM
+    d = case_inputs(meta)
+    t0 = time.time()
+    F = FMM(d["x"], d["y"], meta["neq"], meta["ncut"], bbox=d["bbox"])
+    F.precompute()
+    F.build_expansions(d["tau"], d["tau2"])
+    us = np.array(F.evaluate_to_points(d["x"], d["y"], True))
+    ut = np.array(F.evaluate_to_points(d["tx"], d["ty"], False))
+    t1 = time.time()
+    ds = direct_stokes(d["x"], d["y"], d["tau"], d["tau2"], d["x"], d["y"], True)
+    dt = direct_stokes(d["x"], d["y"], d["tau"], d["tau2"], d["tx"], d["ty"], False)
+    out = dict(
+        meta=json.dumps(meta),
+        inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),
+        bbox_used=np.array(F.bbox, dtype=np.float64),
+        levels=np.int64(F.tree.levels),
+        src_idx=np.arange(d["x"].size), src_val=us, tgt_idx=np.arange(d["tx"].size), tgt_val=ut,
+        direct_src=ds, direct_tgt=dt,
+    )
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"{name}: levels {F.tree.levels} ref {t1 - t0:.1f}s  err vs direct "
+          + " ".join(f"src[{r}] {rel(us[r], ds[r]):.2e} tgt[{r}] {rel(ut[r], dt[r]):.2e}" for r in range(3)),
+          flush=True)
+
+
 def main():
     only_small = len(sys.argv) > 1 and sys.argv[1] == "small"
     names = [a for a in sys.argv[1:] if a in CASES]
@@ -321,7 +358,10 @@ def main():
             continue
         if only_small and not small:
             continue
-        (run_gradient_case if meta.get("gradient") else run_case)(name, meta, ref)
+        if meta.get("method") == "stokes":
+            run_stokes_case(name, meta, ref)
+        else:
+            (run_gradient_case if meta.get("gradient") else run_case)(name, meta, ref)
 
 
 if __name__ == "__main__":
