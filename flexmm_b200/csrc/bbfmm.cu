@@ -105,8 +105,10 @@ __global__ void __launch_bounds__(128) k_bb_s2m(int p, int np, int L, BBScale sc
 
 // Evaluation: L2T as a 2-D Chebyshev series of the leaf's local coefficients,
 // P2P over the colleagues (as k_evaluate).  One work item = (leaf, up to 128
-// of its targets); G threads share a target.
-template <class KF>
+// of its targets); G threads share a target.  NOUT = 3 adds the gradient in
+// the target position: the series' derivative (T_n' by its recurrence,
+// chebeval2d_dx / _dy, bbfmm.py:32-45) and the kernel's gradient.
+template <class KF, int NOUT>
 __global__ void __launch_bounds__(TCH_BB) k_bb_evaluate(KernelParams kp, int p, int np, BBScale sc,
                                                         const int4 *__restrict__ items,
                                                         const int *__restrict__ n_items_ptr,
@@ -122,10 +124,10 @@ __global__ void __launch_bounds__(TCH_BB) k_bb_evaluate(KernelParams kp, int p, 
                                                         const double *__restrict__ txs,
                                                         const double *__restrict__ tys,
                                                         const int *__restrict__ tperm, int check,
-                                                        double *__restrict__ out) {
+                                                        double *__restrict__ out, int64_t ld_out) {
   __shared__ double ssx[SMAX_BB], ssy[SMAX_BB], stau[SMAX_BB];
   __shared__ int rb[9], rs[10];
-  __shared__ double red[TCH_BB / 32];
+  __shared__ double red[NOUT][TCH_BB / 32];
   const KF K(kp);
   const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -145,33 +147,54 @@ __global__ void __launch_bounds__(TCH_BB) k_bb_evaluate(KernelParams kp, int p, 
     __syncthreads();
     if (threadIdx.x == 0)
       for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
-    double u = 0.0;
+    double u = 0.0, gx = 0.0, gy = 0.0;
     if (lev >= 2 && valid) {
       // sum_a T_a(x) sum_b c[a p + b] T_b(y), rows a split over the G threads
       const double a = sc.inv_hw[lev];
       const double xh = (x - xmid[g]) * a, yh = (y - ymid[g]) * a;
-      double ty[BB_MAX_P];
+      double ty[BB_MAX_P], dty[BB_MAX_P];
       ty[0] = 1.0;
       ty[1] = yh;
+      dty[0] = 0.0;
+      dty[1] = 1.0;
 #pragma unroll
-      for (int b = 2; b < BB_MAX_P; ++b) ty[b] = 2.0 * yh * ty[b - 1] - ty[b - 2];
+      for (int b = 2; b < BB_MAX_P; ++b) {
+        ty[b] = 2.0 * yh * ty[b - 1] - ty[b - 2];
+        if (NOUT == 3) dty[b] = 2.0 * ty[b - 1] + 2.0 * yh * dty[b - 1] - dty[b - 2];
+      }
       const double *cr = loc + (size_t)g * np;
-      double tp = 1.0, tc = xh;  // T_{ar-1}, T_ar as ar advances
+      double tp = 1.0, tc = xh;    // T_{ar-1}, T_ar as ar advances
+      double dtp = 0.0, dtc = 1.0;  // their derivatives
       for (int ar = 0; ar < p; ++ar) {
-        const double tx = ar == 0 ? 1.0 : tc;
+        const double tx = ar == 0 ? 1.0 : tc, dtx = ar == 0 ? 0.0 : dtc;
         if (ar % G == sub) {
-          double s = 0.0;
+          double s = 0.0, sd = 0.0;
 #pragma unroll
           for (int b = 0; b < BB_MAX_P; ++b)
-            if (b < p) s = fma(__ldg(cr + ar * p + b), ty[b], s);
+            if (b < p) {
+              const double c = __ldg(cr + ar * p + b);
+              s = fma(c, ty[b], s);
+              if (NOUT == 3) sd = fma(c, dty[b], sd);
+            }
           u = fma(tx, s, u);
+          if (NOUT == 3) {
+            gx = fma(dtx, s, gx);
+            gy = fma(tx, sd, gy);
+          }
         }
         if (ar >= 1) {
           const double tn = 2.0 * xh * tc - tp;
+          if (NOUT == 3) {
+            const double dtn = 2.0 * tc + 2.0 * xh * dtc - dtp;
+            dtp = dtc;
+            dtc = dtn;
+          }
           tp = tc;
           tc = tn;
         }
       }
+      gx *= a;  // d/dx = (2 / w) d/dxh
+      gy *= a;
     }
     __syncthreads();
     auto pair = [&](int j) -> double {
@@ -194,28 +217,39 @@ __global__ void __launch_bounds__(TCH_BB) k_bb_evaluate(KernelParams kp, int p, 
       }
       __syncthreads();
       if (valid) {
-        int j = sub;
-        for (; j + 3 * G < nb; j += 4 * G) {
-          u += pair(j);
-          u1 += pair(j + G);
-          u2 += pair(j + 2 * G);
-          u3 += pair(j + 3 * G);
+        if constexpr (NOUT == 1) {
+          int j = sub;
+          for (; j + 3 * G < nb; j += 4 * G) {
+            u += pair(j);
+            u1 += pair(j + G);
+            u2 += pair(j + 2 * G);
+            u3 += pair(j + 3 * G);
+          }
+          for (; j < nb; j += G) u += pair(j);
+        } else {
+          for (int j = sub; j < nb; j += G) {
+            const double qx = ssx[j], qy = ssy[j];
+            if (!(check && x - qx == 0.0 && y - qy == 0.0)) K.grad(qx, qy, x, y, stau[j], u, gx, gy);
+          }
         }
-        for (; j < nb; j += G) u += pair(j);
       }
       __syncthreads();
     }
-    u = (u + u1) + (u2 + u3);
-    for (int w = min(G, 32) >> 1; w >= 1; w >>= 1) u += __shfl_xor_sync(0xffffffffu, u, w);
-    if (G > 32) {
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
-      __syncthreads();
-      if (sub == 0) {
-        u = 0.0;
-        for (int w = 0; w < G / 32; ++w) u += red[(threadIdx.x >> 5) + w];
+    double r[3] = {(u + u1) + (u2 + u3), gx, gy};
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+      double w = r[o];
+      for (int q = min(G, 32) >> 1; q >= 1; q >>= 1) w += __shfl_xor_sync(0xffffffffu, w, q);
+      if (G > 32) {
+        if ((threadIdx.x & 31) == 0) red[o][threadIdx.x >> 5] = w;
+        __syncthreads();
+        if (sub == 0) {
+          w = 0.0;
+          for (int q = 0; q < G / 32; ++q) w += red[o][(threadIdx.x >> 5) + q];
+        }
       }
+      if (valid && sub == 0) out[o * ld_out + tperm[t0 + t]] = w;
     }
-    if (valid && sub == 0) out[tperm[t0 + t]] = u;
     __syncthreads();
   }
 }
@@ -309,7 +343,7 @@ void run_bb_downward(const BBArgs &b, const double *mult, double *ple, cudaStrea
 
 void run_bb_evaluate(const BBArgs &b, const double *tau_s, const double *loc, const double *txs,
                      const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
-                     int check, double *out, cudaStream_t s) {
+                     int check, int nout, double *out, int64_t ld_out, cudaStream_t s) {
   if (m == 0) return;
   const TreeDev &td = *b.td;
   PassArgs a{};
@@ -319,24 +353,22 @@ void run_bb_evaluate(const BBArgs &b, const double *tau_s, const double *loc, co
   eval_items(a, tkeys, m, it, s);
   const BBScale sc = bb_scale(*b.th);
   PhaseTimer timer(PH_EVAL, s);
+  auto launch = [&](auto kern) {
+    kern<<<148 * 8, TCH_BB, 0, s>>>(b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(),
+                                    td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+                                    td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs, tys,
+                                    tperm, check, out, ld_out);
+  };
   switch (b.kernel_id) {
     case KERNEL_LAPLACE:
-      k_bb_evaluate<LaplaceF64><<<148 * 8, TCH_BB, 0, s>>>(
-          b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
-          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
-          tys, tperm, check, out);
-      break;
-    case KERNEL_RADIAL_TABLE:
-      k_bb_evaluate<RadialTableF64><<<148 * 8, TCH_BB, 0, s>>>(
-          b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
-          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
-          tys, tperm, check, out);
+      nout == 3 ? launch(k_bb_evaluate<LaplaceF64, 3>) : launch(k_bb_evaluate<LaplaceF64, 1>);
       break;
     case KERNEL_MOD_HELMHOLTZ:
-      k_bb_evaluate<ModHelmholtzF64><<<148 * 8, TCH_BB, 0, s>>>(
-          b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
-          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs,
-          tys, tperm, check, out);
+      nout == 3 ? launch(k_bb_evaluate<ModHelmholtzF64, 3>) : launch(k_bb_evaluate<ModHelmholtzF64, 1>);
+      break;
+    case KERNEL_RADIAL_TABLE:
+      FMMB_CHECK(nout == 1, ERR_UNSUPPORTED, "tabulated kernels evaluate potentials only");
+      launch(k_bb_evaluate<RadialTableF64, 1>);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

@@ -808,8 +808,6 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
   FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
   FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
   FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the target count");
-  FMMB_CHECK(nout == 1 || p->ops->method != METHOD_BBFMM, ERR_UNSUPPORTED,
-             "the black-box FMM evaluates potentials only");
   PassArgs a = pass_args(p);
   DevBuf<uint64_t> tkeys;
   DevBuf<int> tperm;
@@ -829,7 +827,7 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
                         tys.get(), tkeys.get(), tperm.get(), m, check, out, ld_out, s);
   else if (p->ops->method == METHOD_BBFMM)
     run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), txs.get(), tys.get(), tkeys.get(),
-                    tperm.get(), m, check, out, s);
+                    tperm.get(), m, check, nout, out, ld_out, s);
   else if (p->precision == PREC_MIXED)
     run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(), txs.get(),
                        tys.get(), tkeys.get(), tperm.get(), m, check, nout, out, ld_out, s);
@@ -846,8 +844,6 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
   const TreeDev &td = p->td;
   const int64_t m = p->th.n_points;
   FMMB_CHECK(nout == 1 || ld_out >= m, ERR_INVALID_ARGUMENT, "ld_out is smaller than the source count");
-  FMMB_CHECK(nout == 1 || p->ops->method != METHOD_BBFMM, ERR_UNSUPPORTED,
-             "the black-box FMM evaluates potentials only");
   PassArgs a = pass_args(p);
   // the tree's sorted copy: keys sorted on at least their top L-1 digits,
   // which is all that leaf location reads
@@ -857,7 +853,7 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
                         ld_out, s);
   else if (p->ops->method == METHOD_BBFMM)
     run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), td.sx.get(), td.sy.get(),
-                    td.pkeys.get(), td.ordv.get(), m, check, out, s);
+                    td.pkeys.get(), td.ordv.get(), m, check, nout, out, ld_out, s);
   else if (p->precision == PREC_MIXED)
     run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(),
                        td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, nout,

@@ -69,9 +69,10 @@ struct BBArgs {
 void run_bb_upward(const BBArgs &b, const double *tau_sorted, double *mult, cudaStream_t s);
 // M2L and L2L, level by level; the locals are the partial locals (no solve)
 void run_bb_downward(const BBArgs &b, const double *mult, double *ple, cudaStream_t s);
+// nout = 1 potential, 3 potential and target gradient (rows, stride ld_out)
 void run_bb_evaluate(const BBArgs &b, const double *tau_sorted, const double *loc,
                      const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
-                     int64_t m, int check, double *out, cudaStream_t s);
+                     int64_t m, int check, int nout, double *out, int64_t ld_out, cudaStream_t s);
 
 // Stokes FMM (stokes.cu): rows of np = pad8(2 Neq + 1) doubles; per level
 // the large circle and the row-major operators of the GEMMs:
