@@ -70,6 +70,10 @@ SIGNATURES = [
     ("fmm_ops_create", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("fmm_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(LevelOps), _ip]),
     ("fmm_ops_destroy", ctypes.c_int, [_vp]),
+    ("fmm_build_expansions_multi", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int64, _vp]),
+    ("fmm_evaluate_multi", ctypes.c_int,
+     [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
+    ("fmm_evaluate_sources_multi", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
     ("fmm_stokes_ops_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     ("fmm_stokes_ops_add", ctypes.c_int, [_vp, ctypes.POINTER(StokesLevelOps), _ip]),
     ("fmm_build_expansions2", ctypes.c_int, [_vp, _vp, _vp, _vp]),

@@ -219,6 +219,7 @@ struct fmm_plan {
   int precision = PREC_FP64;
   bool have_expansions = false;
   DevBuf<double> tau2_s, partial;  // Stokes FMM: sorted fy; partial multipoles
+  int n_rhs = 1;                   // charge columns of the last build (multi-RHS)
   cublasHandle_t blas = nullptr;  // black-box and Stokes FMM translations
   ~fmm_plan() {
     if (blas) cublasDestroy(blas);
@@ -716,11 +717,96 @@ int fmm_build_expansions2(fmm_plan *p, const double *fx, const double *fy, void 
   });
 }
 
+int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_t ld_tau,
+                               void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->precision == PREC_FP64, ERR_UNSUPPORTED,
+               "several charge columns: FP64 KIFMM plans");
+    const TreeHost &th = p->th;
+    FMMB_CHECK(n_rhs >= 1 && ld_tau >= th.n_points, ERR_INVALID_ARGUMENT, "bad n_rhs or ld_tau");
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int m = 2; m < th.L; ++m)
+      FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
+    const int np = p->ops->np;
+    const int64_t total = th.n_total(), n = th.n_points, cs = total * np;
+    p->ops_dev.alloc(th.L, s);
+    PassArgs a = pass_args(p);
+    FMMB_CUDA(cudaMemcpyAsync(p->ops_dev.get(), a.ops_host.data(), th.L * sizeof(LevelOpsDev),
+                              cudaMemcpyHostToDevice, s));
+    a.ops_dev = p->ops_dev.get();
+    p->tau_s.alloc((size_t)n_rhs * n, s);
+    p->mult.alloc((size_t)n_rhs * cs, s);
+    p->ple.alloc((size_t)n_rhs * cs, s);
+    p->loc.alloc((size_t)n_rhs * cs, s);
+    p->mult.zero(s);
+    p->ple.zero(s);
+    p->loc.zero(s);
+    for (int r = 0; r < n_rhs; ++r) {
+      double *tr = p->tau_s.get() + (size_t)r * n;
+      gather_sorted(tau + (size_t)r * ld_tau, p->td.ordv.get(), n, tr, s);
+      run_upward(a, tr, p->mult.get() + (size_t)r * cs, s);
+      run_m2l(a, p->mult.get() + (size_t)r * cs, p->ple.get() + (size_t)r * cs, s);
+      run_downward(a, p->ple.get() + (size_t)r * cs, p->loc.get() + (size_t)r * cs, s);
+    }
+    p->n_rhs = n_rhs;
+    p->have_expansions = true;
+  });
+}
+
+int fmm_evaluate_multi(fmm_plan *p, const double *tx, const double *ty, int64_t m, int check,
+                       double *out, int64_t ld_out, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+    FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->precision == PREC_FP64, ERR_UNSUPPORTED,
+               "several charge columns: FP64 KIFMM plans");
+    FMMB_CHECK(m >= 0 && ld_out >= m, ERR_INVALID_ARGUMENT, "bad target count or ld_out");
+    if (m == 0) return;
+    FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    PassArgs a = pass_args(p);
+    a.ops_dev = p->ops_dev.get();
+    DevBuf<uint64_t> tkeys;
+    DevBuf<int> tperm;
+    DevBuf<double> txs, tys;
+    {
+      PhaseTimer timer(PH_SORT_TGT, s);
+      sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1);
+      txs.alloc(m, s);
+      tys.alloc(m, s);
+      gather_sorted(tx, tperm.get(), m, txs.get(), s);
+      gather_sorted(ty, tperm.get(), m, tys.get(), s);
+    }
+    run_evaluate_multi(a, p->tau_s.get(), p->th.n_points, p->n_rhs, p->loc.get(),
+                       (int64_t)p->th.n_total() * p->ops->np, txs.get(), tys.get(), tkeys.get(),
+                       tperm.get(), m, check, out, ld_out, s);
+  });
+}
+
+int fmm_evaluate_sources_multi(fmm_plan *p, int check, double *out, int64_t ld_out, void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
+    FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->precision == PREC_FP64, ERR_UNSUPPORTED,
+               "several charge columns: FP64 KIFMM plans");
+    FMMB_CHECK(out && ld_out >= p->th.n_points, ERR_INVALID_ARGUMENT, "NULL out or ld_out too small");
+    cudaStream_t s = (cudaStream_t)stream;
+    PassArgs a = pass_args(p);
+    a.ops_dev = p->ops_dev.get();
+    const TreeDev &td = p->td;
+    run_evaluate_multi(a, p->tau_s.get(), p->th.n_points, p->n_rhs, p->loc.get(),
+                       (int64_t)p->th.n_total() * p->ops->np, td.sx.get(), td.sy.get(),
+                       td.pkeys.get(), td.ordv.get(), p->th.n_points, check, out, ld_out, s);
+  });
+}
+
 int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
   return guarded([&] {
     FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(p->ops->method != METHOD_STOKES, ERR_INVALID_ARGUMENT,
                "Stokes plans take fmm_build_expansions2 (two force components)");
+    p->n_rhs = 1;
     cudaStream_t s = (cudaStream_t)stream;
     const TreeHost &th = p->th;
     for (int m = 2; m < th.L; ++m)

@@ -22,6 +22,8 @@
 //    the read-only cache.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "fmm.cuh"
 #include "gemm.cuh"
 #include "timing.cuh"
@@ -464,6 +466,108 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
 
 // FP64 direct sum (kernel_apply / kernel_apply_single_check,
 // flexmm/flexmm2d/helpers.py:91-116): all sources, one target per thread,
+// Several charge columns on one tree (multi-RHS): columns r0 .. r0 + R - 1
+// of the charges (stride n_src) and locals (stride col_stride); each kernel
+// value (L2T and P2P) is computed once and applied to the R columns.  Output
+// row r of out (stride ld_out).  One work item = (leaf, up to 128 targets).
+constexpr int SMAX_MR = 256;
+template <class KF, int R>
+__global__ void __launch_bounds__(TCH) k_evaluate_multi(KernelParams kp, int neq, int np, int ncol,
+                                                        const int4 *__restrict__ items,
+                                                        const int *__restrict__ n_items_ptr,
+                                                        const int *__restrict__ coll,
+                                                        const int *__restrict__ bot,
+                                                        const int *__restrict__ top,
+                                                        const double *__restrict__ xmid,
+                                                        const double *__restrict__ ymid,
+                                                        const double *__restrict__ sx,
+                                                        const double *__restrict__ sy,
+                                                        const double *__restrict__ tau, int64_t n_src,
+                                                        const LevelOpsDev *__restrict__ ops,
+                                                        const double *__restrict__ loc,
+                                                        int64_t col_stride,
+                                                        const double *__restrict__ txs,
+                                                        const double *__restrict__ tys,
+                                                        const int *__restrict__ tperm, int check,
+                                                        double *__restrict__ out, int64_t ld_out) {
+  __shared__ double ssx[SMAX_MR], ssy[SMAX_MR], stau[R][SMAX_MR];
+  __shared__ int rb[9], rs[10];
+  __shared__ double red[R][TCH / 32];
+  const KF K(kp);
+  const int n_items = *n_items_ptr;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int4 it = items[item];
+    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
+    int G = 1;
+    while (2 * G * cnt <= TCH) G *= 2;
+    const int t = threadIdx.x / G, sub = threadIdx.x % G;
+    const bool valid = t < cnt;
+    const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
+    if (threadIdx.x < 9) {
+      const int cg = coll[(size_t)g * 9 + threadIdx.x];
+      rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
+      rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
+    }
+    if (threadIdx.x == 0) rs[0] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
+    double u[R];
+#pragma unroll
+    for (int c = 0; c < R; ++c) u[c] = 0.0;
+    if (lev >= 2 && valid) {  // L2T, one kernel value per circle point for all columns
+      const double dx = x - xmid[g], dy = y - ymid[g];
+      const double *lx = ops[lev].lx, *ly = ops[lev].ly;
+      for (int k = sub; k < neq; k += G) {
+        const double kv = K(lx[k], ly[k], dx, dy);
+#pragma unroll
+        for (int c = 0; c < R; ++c)
+          if (c < ncol) u[c] = fma(kv, loc[c * col_stride + (size_t)g * np + k], u[c]);
+      }
+    }
+    __syncthreads();
+    const int ns = rs[9];
+    for (int base = 0; base < ns; base += SMAX_MR) {
+      const int nb = min(SMAX_MR, ns - base);
+      for (int i = threadIdx.x; i < nb; i += TCH) {
+        const int idx = base + i;
+        int c = 0;
+        while (idx >= rs[c + 1]) ++c;
+        const int j = rb[c] + (idx - rs[c]);
+        ssx[i] = sx[j];
+        ssy[i] = sy[j];
+#pragma unroll
+        for (int q = 0; q < R; ++q) stau[q][i] = q < ncol ? tau[q * n_src + j] : 0.0;
+      }
+      __syncthreads();
+      if (valid)
+        for (int j = sub; j < nb; j += G) {
+          const double qx = ssx[j], qy = ssy[j];
+          if (check && x - qx == 0.0 && y - qy == 0.0) continue;
+          const double kv = K(qx, qy, x, y);
+#pragma unroll
+          for (int c = 0; c < R; ++c) u[c] = fma(kv, stau[c][j], u[c]);
+        }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      double w = u[c];
+      for (int q = min(G, 32) >> 1; q >= 1; q >>= 1) w += __shfl_xor_sync(0xffffffffu, w, q);
+      if (G > 32) {
+        if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = w;
+        __syncthreads();
+        if (sub == 0) {
+          w = 0.0;
+          for (int q = 0; q < G / 32; ++q) w += red[c][(threadIdx.x >> 5) + q];
+        }
+      }
+      if (valid && sub == 0 && c < ncol) out[c * ld_out + tperm[t0 + t]] = w;
+    }
+    __syncthreads();
+  }
+}
+
 // sources staged through shared memory
 template <class KF>
 __global__ void __launch_bounds__(256) k_direct(KernelParams kp, const double *__restrict__ sx,
@@ -639,6 +743,51 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
       FMMB_CHECK(nout == 1, ERR_UNSUPPORTED, "tabulated kernels evaluate potentials only");
       evaluate_impl<RadialTableF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
                                     ld_out, s);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+}
+
+namespace {
+template <class KF>
+void evaluate_multi_impl(const PassArgs &a, const double *tau_s, int64_t n_src, int n_rhs,
+                         const double *loc, int64_t col_stride, const double *txs,
+                         const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
+                         int check, double *out, int64_t ld_out, cudaStream_t s) {
+  const TreeDev &td = *a.td;
+  EvalItems it;
+  eval_items(a, tkeys, m, it, s);
+  PhaseTimer timer(PH_EVAL, s);
+  constexpr int R = 8;
+  for (int r0 = 0; r0 < n_rhs; r0 += R) {
+    const int ncol = std::min(R, n_rhs - r0);
+    k_evaluate_multi<KF, R><<<148 * 8, TCH, 0, s>>>(
+        a.kp, a.neq, a.np, ncol, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+        td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s + r0 * n_src,
+        n_src, a.ops_dev, loc + r0 * col_stride, col_stride, txs, tys, tperm, check,
+        out + r0 * ld_out, ld_out);
+    FMMB_CUDA(cudaGetLastError());
+  }
+}
+}  // namespace
+
+void run_evaluate_multi(const PassArgs &a, const double *tau_s, int64_t n_src, int n_rhs,
+                        const double *loc, int64_t col_stride, const double *txs, const double *tys,
+                        const uint64_t *tkeys, const int *tperm, int64_t m, int check, double *out,
+                        int64_t ld_out, cudaStream_t s) {
+  if (m == 0 || n_rhs == 0) return;
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE:
+      evaluate_multi_impl<LaplaceF64>(a, tau_s, n_src, n_rhs, loc, col_stride, txs, tys, tkeys,
+                                      tperm, m, check, out, ld_out, s);
+      break;
+    case KERNEL_MOD_HELMHOLTZ:
+      evaluate_multi_impl<ModHelmholtzF64>(a, tau_s, n_src, n_rhs, loc, col_stride, txs, tys, tkeys,
+                                           tperm, m, check, out, ld_out, s);
+      break;
+    case KERNEL_RADIAL_TABLE:
+      evaluate_multi_impl<RadialTableF64>(a, tau_s, n_src, n_rhs, loc, col_stride, txs, tys, tkeys,
+                                          tperm, m, check, out, ld_out, s);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }

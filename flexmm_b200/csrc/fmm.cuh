@@ -101,6 +101,12 @@ void run_stokes_evaluate(const StokesArgs &a, const double *fx, const double *fy
                          const int *tperm, int64_t m, int check, double *out, int64_t ld_out,
                          cudaStream_t s);
 
+// n_rhs charge columns (stride n_src, sorted order) and their locals (stride
+// col_stride): out row r (stride ld_out) for column r
+void run_evaluate_multi(const PassArgs &a, const double *tau_sorted, int64_t n_src, int n_rhs,
+                        const double *loc, int64_t col_stride, const double *txs, const double *tys,
+                        const uint64_t *tkeys, const int *tperm, int64_t m, int check, double *out,
+                        int64_t ld_out, cudaStream_t s);
 void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaStream_t s);
 void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s);
 void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s);

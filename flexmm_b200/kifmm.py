@@ -208,6 +208,23 @@ class KI_FMM:
         return self._tree
 
     def build_expansions(self, tau):
+        """Charges in the caller's source order: [N], or [k, N] for k charge
+        columns on one tree (kifmm2d's tau layout, flexmm/kifmm2d/scalar/fmm.py:71-87;
+        FP64 form), whose evaluations then return [k, M]."""
+        self._n_rhs = None
+        if np.ndim(tau) == 2:
+            torch = _torch()
+            t = tau if isinstance(tau, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(tau, dtype=np.float64))
+            td = t.to(device="cuda", dtype=torch.float64).contiguous()
+            k, n = td.shape
+            if n != self.N:
+                raise ValueError(f"tau has {n} columns, expected {self.N}")
+            _lib.call("fmm_build_expansions_multi", self._plan, ctypes.c_void_p(td.data_ptr()), k, n,
+                      _stream())
+            self._tau = td
+            self._n_rhs = k
+            self._expanded = True
+            return
         td, _ = _device_f64(tau)
         if td.numel() != self.N:
             raise ValueError(f"tau has {td.numel()} entries, expected {self.N}")
@@ -258,7 +275,26 @@ class KI_FMM:
                   ctypes.c_void_p(out.data_ptr()), m, _stream())
         return _as_kind(out, kind, (nout, m))
 
+    def _evaluate_multi(self, x, y, check):
+        torch = _torch()
+        k = self._n_rhs
+        if check and self._own_sources(x, y):
+            out = torch.empty((k, self.N), dtype=torch.float64, device="cuda")
+            _lib.call("fmm_evaluate_sources_multi", self._plan, 1, ctypes.c_void_p(out.data_ptr()),
+                      self.N, _stream())
+            return _as_kind(out, "cuda" if x.is_cuda else "cpu", (k, self.N))
+        xd, kind = _device_f64(x)
+        yd, _ = _device_f64(y)
+        m = xd.numel()
+        out = torch.empty((k, m), dtype=torch.float64, device="cuda")
+        _lib.call("fmm_evaluate_multi", self._plan, ctypes.c_void_p(xd.data_ptr()),
+                  ctypes.c_void_p(yd.data_ptr()), m, 1 if check else 0,
+                  ctypes.c_void_p(out.data_ptr()), m, _stream())
+        return _as_kind(out, kind, (k, m))
+
     def _evaluate(self, x, y, check):
+        if getattr(self, "_n_rhs", None):
+            return self._evaluate_multi(x, y, check)
         torch = _torch()
         xd, kind = _device_f64(x)
         yd, _ = _device_f64(y)
@@ -281,7 +317,7 @@ class KI_FMM:
         Called with the very tensors the FMM was built on (unchanged), the
         evaluation runs on the tree's sorted copy of them (fmm_evaluate_sources)
         instead of uploading, locating and sorting the points again."""
-        if not self._own_sources(x, y):
+        if not self._own_sources(x, y) or getattr(self, "_n_rhs", None):
             return self._evaluate(x, y, True)
         torch = _torch()
         out = torch.empty(self.N, dtype=torch.float64, device="cuda")

@@ -171,6 +171,18 @@ int fmm_evaluate(fmm_plan *plan, const double *tx, const double *ty, int64_t m, 
  * the FMM's own sources (flexmm/flexmm2d/fmm.py:158-159, 162-176). */
 int fmm_evaluate_sources(fmm_plan *plan, int check, double *out, void *stream);
 
+/* Several charge columns on one tree (multi-RHS; the reference's kifmm2d
+ * FMM takes tau [k, N], flexmm/kifmm2d/scalar/fmm.py:71-87): column r is
+ * tau[r * ld_tau .. + n), caller's source order.  FP64 KIFMM plans.  The
+ * evaluation computes each kernel value once for up to 8 columns; result
+ * row r is out[r * ld_out .. + m).  fmm_evaluate after a multi build uses
+ * column 0. */
+int fmm_build_expansions_multi(fmm_plan *plan, const double *tau, int n_rhs, int64_t ld_tau,
+                               void *stream);
+int fmm_evaluate_multi(fmm_plan *plan, const double *tx, const double *ty, int64_t m, int check,
+                       double *out, int64_t ld_out, void *stream);
+int fmm_evaluate_sources_multi(fmm_plan *plan, int check, double *out, int64_t ld_out, void *stream);
+
 /* Several outputs per point, as the reference's named evaluators
  * (kifmm2d FMM.register_evaluator + evaluate_to_points,
  * flexmm/kifmm2d/scalar/fmm.py:172-199, helpers.py:176-238):
