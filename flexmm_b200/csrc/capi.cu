@@ -213,6 +213,7 @@ struct fmm_plan {
   DevBuf<LevelOpsDev> ops_dev;
   DevBuf<double> tau_s, mult, ple, loc;
   DevBuf<float> mult32, loc32;  // mixed precision: FP32 expansions ...
+  DevBuf<float> mult_tc;        // ... multipoles split TF32 hi / lo ...
   DevBuf<double> msum, lsum;    // ... and their FP64 component sums
   DevBuf<double> tsum;          // per node: FP64 sum of its charges
   DevBuf<int> err;              // set by kernels whose bounded waits ran out
@@ -841,17 +842,21 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       p->loc32.alloc(total * np, s);
       p->msum.alloc(total, s);
       p->lsum.alloc(total, s);
+      p->mult_tc.alloc(total * 2 * np, s);
       p->mult32.zero(s);
+      p->mult_tc.zero(s);
       p->loc32.zero(s);
       p->msum.zero(s);
       p->lsum.zero(s);
       p->tsum.alloc(total, s);
       node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
       t_prep.reset();
-      run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(), s);
+      run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(),
+                       p->mult_tc.get(), s);
       p->err.alloc(1, s);
       p->err.zero(s);
-      run_m2l_mixed(a, p->mult32.get(), p->msum.get(), p->ple.get(), p->err.get(), s);
+      run_m2l_mixed(a, p->mult32.get(), p->mult_tc.get(), p->msum.get(), p->ple.get(),
+                    p->err.get(), s);
       run_downward_mixed(a, p->ple.get(), p->loc32.get(), p->lsum.get(), s);
     } else {
       p->mult.alloc(total * np, s);

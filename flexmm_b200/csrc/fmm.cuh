@@ -133,10 +133,11 @@ void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &
 
 // Mixed precision (fmm_mixed.cu): FP32 multipoles / locals with FP64 sums.
 void node_charge_sums(const PassArgs &a, const double *tau_sorted, double *tsum, cudaStream_t s);
+// mult_tc: [node][TF32 hi np | lo np] copy of mult32, the tcgen05 M2L operand
 void run_upward_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum, float *mult32,
-                      double *msum, cudaStream_t s);
-void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, double *ple,
-                   int *err, cudaStream_t s);
+                      double *msum, float *mult_tc, cudaStream_t s);
+void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc, const double *msum,
+                   double *ple, int *err, cudaStream_t s);
 void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, double *lsum,
                         cudaStream_t s);
 void run_evaluate_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum,

@@ -105,9 +105,11 @@ __device__ __forceinline__ void warp_gemm_x3(const float *A, int lda, const floa
 __host__ __device__ inline int pad_f(int n) { return n + 4; }  // float rows: stride 4 mod 32 words
 
 // FP64 C2E result rows in shared memory -> FP32 rows + FP64 component sums
+// out_tc (optional): the same rows split as TF32 hi, lo ([node][hi np | lo np]),
+// the operand format of the tcgen05 M2L
 __device__ __forceinline__ void store_mixed(const double *P, int ldp, int np, int neq,
                                             const int *node, int ntile, float *out32,
-                                            double *outsum) {
+                                            double *outsum, float *out_tc = nullptr) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int t = warp; t < ntile; t += NT / 32) {
     const int n = node[t];
@@ -115,7 +117,13 @@ __device__ __forceinline__ void store_mixed(const double *P, int ldp, int np, in
     double s = 0.0;
     for (int k = lane; k < np; k += 32) {
       const double v = k < neq ? P[t * ldp + k] : 0.0;
-      out32[(size_t)n * np + k] = (float)v;
+      const float f = (float)v;
+      out32[(size_t)n * np + k] = f;
+      if (out_tc) {
+        const float h = __uint_as_float(to_tf32(f));
+        out_tc[(size_t)n * 2 * np + k] = h;
+        out_tc[(size_t)n * 2 * np + np + k] = __uint_as_float(to_tf32(f - h));
+      }
       s += v;
     }
     for (int w = 16; w >= 1; w >>= 1) s += __shfl_xor_sync(0xffffffffu, s, w);
@@ -155,7 +163,8 @@ __global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np,
                                                const double *__restrict__ tsum,
                                                const LevelOpsDev *__restrict__ ops,
                                                float *__restrict__ mult32,
-                                               double *__restrict__ msum) {
+                                               double *__restrict__ msum,
+                                               float *__restrict__ mult_tc) {
   extern __shared__ double smem[];
   const int ldp = pad_ld(np);
   double *P = smem;          // [TN][ldp] check potentials
@@ -215,7 +224,7 @@ __global__ void __launch_bounds__(NT) k_s2m_mx(KernelParams kp, int neq, int np,
       c2e_tile<true>(cv, np, P, T, orow);
     }
     __syncthreads();
-    store_mixed(P, ldp, np, neq, node, TN, mult32, msum);
+    store_mixed(P, ldp, np, neq, node, TN, mult32, msum, mult_tc);
     __syncthreads();
   }
 }
@@ -228,7 +237,7 @@ template <bool kStageB>
 __global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_first, int n_groups,
                                                const int *__restrict__ parent,
                                                const LevelOpsDev *__restrict__ ops, float *mult32,
-                                               double *msum) {
+                                               double *msum, float *mult_tc) {
   extern __shared__ double smem[];
   const int ldp = pad_ld(np), lda = pad_f(4 * np), ldb = ldb_f(np);
   double *P = smem;                                    // [TN][ldp] check potentials
@@ -288,7 +297,7 @@ __global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_fir
   __syncthreads();
   c2e_tile<true>(cv, np, P, T, orow);
   __syncthreads();
-  store_mixed(P, ldp, np, neq, node, TN, mult32, msum);
+  store_mixed(P, ldp, np, neq, node, TN, mult32, msum, mult_tc);
 }
 
 // shared memory of k_m2m_mx
@@ -377,25 +386,40 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 
 // ---------------------------------------------------- M2L on tcgen05 ----
 // 128 targets of one parity class per CTA (MMA M = 128), one thread per
-// target.  Per offset, the gathered source multipoles (A: 128 x K) and the
-// deflated operator (B: N x K, N = NP rounded up to 16) are staged in shared
-// memory as TF32 hi/lo pairs in the K-major core-matrix layout (8 rows x 16
-// bytes per core matrix, core matrices along K contiguous: LBO = 128 B,
-// SBO = NP/4 * 128 B) and multiplied by tcgen05.mma kind::tf32 into tensor
-// memory.  Each k-step's three split products (lo.hi, hi.lo, hi.hi) go to
-// their own 32 TMEM columns, which the epilogue adds into FP64 registers (the
-// tensor cores truncate their FP32 accumulation).  Two buffers: the MMAs of
-// one offset run while the threads stage the next and read the previous.
+// target.  Per offset, the gathered source multipoles (A: 128 x K, read
+// pre-split as TF32 hi / lo from the upward pass's mult_tc rows) and the
+// deflated operator (B: N x K, N = NP rounded up to 16) are copied into shared
+// memory with cp.async in the K-major core-matrix layout (8 rows x 16 bytes
+// per core matrix, core matrices along K contiguous: LBO = 128 B, SBO =
+// NP/4 * 128 B) through a 3-stage pipeline, and multiplied by tcgen05.mma
+// kind::tf32 into tensor memory.  Each k-step's three split products (lo.hi,
+// hi.lo, hi.hi) go to their own 32 TMEM columns (the tensor cores truncate
+// their FP32 accumulation); the epilogue adds the k-step slots in FP32 (round
+// to nearest) and the result into FP64 registers.  Two TMEM buffers: the MMAs
+// of one offset run while the threads read the previous offset's results and
+// copy operands two offsets ahead.
 constexpr int TCM = 128;       // targets per CTA = MMA M
 constexpr int TC_MAX_NP = 32;  // up to 4 k-steps x 32 TMEM columns per buffer
 constexpr int TC_COLS = 256;   // TMEM columns per CTA (2 buffers x 128)
+constexpr int TC_STAGES = 3;   // operand stages in shared memory
 constexpr uint32_t TC_MAX_TRIES = 1u << 20;
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// shared memory of k_m2l_tc: TC_STAGES x (A hi, A lo, B hi, B lo)
+size_t m2l_tc_stage_bytes(int np) {
+  const size_t ntc = (np + 15) & ~15;
+  const size_t a_sz = (size_t(TCM) * np * 4 + 1023) & ~size_t(1023);
+  const size_t b_sz = (ntc * np * 4 + 1023) & ~size_t(1023);
+  return 2 * a_sz + 2 * b_sz;
+}
 
 __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, int np,
                                                    const int *__restrict__ rg,
                                                    const int *__restrict__ il,
                                                    const LevelOpsDev *__restrict__ ops,
-                                                   const float *__restrict__ mult32,
+                                                   const float *__restrict__ mult_tc,
                                                    const double *__restrict__ msum,
                                                    double *__restrict__ ple, int *err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -409,8 +433,7 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
   const int nks = np / 8, nk4 = np / 4;
   const uint32_t a_sz = (uint32_t(TCM) * np * 4 + 1023u) & ~1023u;
   const uint32_t b_sz = (uint32_t(ntc) * np * 4 + 1023u) & ~1023u;
-  unsigned char *A0 = smraw;            // [buf][hi, lo] operand blocks of a_sz bytes
-  unsigned char *B0 = smraw + 4 * a_sz;  // [buf][hi, lo] operand blocks of b_sz bytes
+  const uint32_t st_sz = 2 * a_sz + 2 * b_sz;  // one stage: A hi, A lo, B hi, B lo
   const int warp = threadIdx.x >> 5;
   int slot = 0;
   while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= (int)blockIdx.x) ++slot;
@@ -454,6 +477,38 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
   }
   __syncthreads();
   const int nact = s_nact;
+  const int units = ntc * nk4;  // 16-byte chunks of one B part
+  // start copying offset ai's operands into stage ai % TC_STAGES; returns the
+  // charge-sum term c_o * msum[src] of this thread's source
+  auto issue = [&](int ai) -> double {
+    const int oi = s_act[ai], o = c_class_off_mx[cls][oi];
+    const int src = s_src[oi][threadIdx.x];
+    unsigned char *st = smraw + (ai % TC_STAGES) * st_sz;
+    const int r = threadIdx.x;
+    unsigned char *ah = st, *al = st + a_sz;
+    if (src >= 0) {
+      const float *row = mult_tc + (size_t)src * 2 * np;
+      for (int k4 = 0; k4 < nk4; ++k4) {
+        const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
+        cp_async16(ah + off, row + 4 * k4);
+        cp_async16(al + off, row + np + 4 * k4);
+      }
+    } else {
+      for (int k4 = 0; k4 < nk4; ++k4) {
+        const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
+        *reinterpret_cast<float4 *>(ah + off) = make_float4(0.f, 0.f, 0.f, 0.f);
+        *reinterpret_cast<float4 *>(al + off) = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+    for (int u = threadIdx.x; u < 2 * units; u += TCM) {
+      const int part = u >= units, uu = part ? u - units : u;
+      const int n = uu / nk4, k4 = uu - (uu / nk4) * nk4;
+      const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
+      const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
+      cp_async16(st + 2 * a_sz + part * b_sz + off, bsrc + (size_t)n * np + 4 * k4);
+    }
+    return src >= 0 ? op.c_m2l[o] * __ldg(msum + src) : 0.0;
+  };
   double acc[32];
 #pragma unroll
   for (int c = 0; c < 32; ++c) acc[c] = 0.0;
@@ -467,95 +522,58 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
       atomicExch(err, 1);
     }
     tc::fence_after_sync();
+    float sum[32];
     for (int ks = 0; ks < nks; ++ks) {
       float v[32];
       tc::tmem_ld32(tmem + (uint32_t(32 * warp) << 16) + uint32_t(b * 128 + ks * 32), v);
 #pragma unroll
-      for (int c = 0; c < 32; ++c) acc[c] += (double)v[c];
+      for (int c = 0; c < 32; ++c) sum[c] = ks == 0 ? v[c] : sum[c] + v[c];
     }
+#pragma unroll
+    for (int c = 0; c < 32; ++c) acc[c] += (double)sum[c];
     tc::fence_before_sync();
   };
-  // the next offset's source row, operator slice and charge sum are loaded
-  // into registers while the current offset is staged, multiplied and read
-  const int units = ntc * nk4;
-  float4 pa[8], pb[4];
-  double pm = 0.0;
-  int psrc = -1;
-  auto prefetch = [&](int ai) {
-    const int oi = s_act[ai], o = c_class_off_mx[cls][oi];
-    psrc = s_src[oi][threadIdx.x];
-#pragma unroll
-    for (int k4 = 0; k4 < 8; ++k4)
-      pa[k4] = (k4 < nk4 && psrc >= 0)
-                   ? __ldg(reinterpret_cast<const float4 *>(mult32 + (size_t)psrc * np) + k4)
-                   : make_float4(0.f, 0.f, 0.f, 0.f);
-    pm = psrc >= 0 ? op.c_m2l[o] * __ldg(msum + psrc) : 0.0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int u = (int)threadIdx.x + i * TCM;
-      if (u < 2 * units) {
-        const int part = u >= units, uu = part ? u - units : u;
-        const int n = uu / nk4, k4 = uu % nk4;
-        const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
-        pb[i] = __ldg(reinterpret_cast<const float4 *>(bsrc + (size_t)n * np) + k4);
-      }
-    }
-  };
-  if (nact > 0) prefetch(0);
+  // prologue: offsets 0 and 1 in flight (one commit group each, possibly empty)
+  // charge-sum terms of the offsets in flight: pm0 (ai), pm1 (ai + 1)
+  double pm0 = 0.0, pm1 = 0.0;
+  if (nact > 0) pm0 = issue(0);
+  cp_async_commit();
+  if (nact > 1) pm1 = issue(1);
+  cp_async_commit();
+  static_assert(TC_STAGES == 3, "the prologue fills TC_STAGES - 1 = 2 stages");
   for (int ai = 0; ai < nact; ++ai) {
     const int buf = issued & 1;
-    r1 += pm;
-    // stage A: this thread's target row, TF32 hi / lo
-    {
-      const int r = threadIdx.x;
-      unsigned char *ah = A0 + (2 * buf) * a_sz, *al = A0 + (2 * buf + 1) * a_sz;
-#pragma unroll
-      for (int k4 = 0; k4 < 8; ++k4) {
-        if (k4 >= nk4) break;
-        const float4 v = pa[k4];
-        const float4 h = make_float4(__uint_as_float(to_tf32(v.x)), __uint_as_float(to_tf32(v.y)),
-                                     __uint_as_float(to_tf32(v.z)), __uint_as_float(to_tf32(v.w)));
-        const float4 l = make_float4(__uint_as_float(to_tf32(v.x - h.x)), __uint_as_float(to_tf32(v.y - h.y)),
-                                     __uint_as_float(to_tf32(v.z - h.z)), __uint_as_float(to_tf32(v.w - h.w)));
-        const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
-        *reinterpret_cast<float4 *>(ah + off) = h;
-        *reinterpret_cast<float4 *>(al + off) = l;
-      }
-    }
-    // stage B: the offset's operator, ntc rows x np, hi and lo
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int u = (int)threadIdx.x + i * TCM;
-      if (u < 2 * units) {
-        const int part = u >= units, uu = part ? u - units : u;
-        const int n = uu / nk4, k4 = uu % nk4;
-        const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
-        *reinterpret_cast<float4 *>(B0 + (2 * buf + part) * b_sz + off) = pb[i];
-      }
-    }
-    if (ai + 1 < nact) prefetch(ai + 1);
+    // this thread's copies of offset ai done; everyone's after the barrier
+    cp_async_wait_1();
     tc::fence_proxy_async();
     tc::fence_before_sync();
     if (__syncthreads_or(my_abort)) break;
+    r1 += pm0;
     if (threadIdx.x == 0) {
       tc::fence_after_sync();
+      unsigned char *st = smraw + (ai % TC_STAGES) * st_sz;
       for (int ks = 0; ks < nks; ++ks) {
         const uint32_t d = tmem + uint32_t(buf * 128 + ks * 32);
 #pragma unroll
         for (int p = 0; p < 3; ++p) {  // lo.hi, hi.lo, hi.hi
           const int apart = p == 0 ? 1 : 0, bpart = p == 1 ? 1 : 0;
-          const uint64_t ad = tc::desc_kmajor(tc::smem_u32(A0 + (2 * buf + apart) * a_sz) + ks * 256u, lbo, sbo);
-          const uint64_t bd = tc::desc_kmajor(tc::smem_u32(B0 + (2 * buf + bpart) * b_sz) + ks * 256u, lbo, sbo);
+          const uint64_t ad = tc::desc_kmajor(tc::smem_u32(st + apart * a_sz) + ks * 256u, lbo, sbo);
+          const uint64_t bd = tc::desc_kmajor(tc::smem_u32(st + 2 * a_sz + bpart * b_sz) + ks * 256u, lbo, sbo);
           tc::mma_tf32(d, ad, bd, idesc, p > 0 ? 1u : 0u);
         }
       }
       tc::commit(tc::smem_u32(&mbar[buf]));
     }
-    if (issued >= 1) epilogue(buf ^ 1);
+    if (issued >= 1) epilogue(buf ^ 1);  // MMAs of offset ai-1 done: its stage is free
     ++issued;
+    const int nx = ai + TC_STAGES - 1;  // refill the stage of offset ai - 1
+    pm0 = pm1;
+    pm1 = nx < nact ? issue(nx) : 0.0;
+    cp_async_commit();
   }
   const int aborted = __syncthreads_or(my_abort);
   if (issued >= 1 && !aborted) epilogue((issued - 1) & 1);
+  cp_async_wait_all();
   if (aborted) {
     // wait (bounded) for the commits still outstanding before TMEM is freed
     for (; waits0 < (issued + 1) / 2; ++waits0)
@@ -938,7 +956,7 @@ __global__ void k_node_charge_sums(int total, const int *__restrict__ bot, const
 
 template <class KF32>
 void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, float *mult32,
-                    double *msum, cudaStream_t s) {
+                    double *msum, float *mult_tc, cudaStream_t s) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int np = a.np;
@@ -951,7 +969,7 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
                                               td.uplist.get(), td.n_up.get(), td.bot.get(),
                                               td.top.get(), td.xmid.get(), td.ymid.get(),
                                               td.sx.get(), td.sy.get(), tau_s, tsum, a.ops_dev,
-                                              mult32, msum);
+                                              mult32, msum, mult_tc);
   FMMB_CUDA(cudaGetLastError());
   // operators staged in shared memory when they fit (static smem ~1 KB aside)
   const bool stage_b = m2m_mx_smem(np, true) + 4096 <= smem_optin();
@@ -963,7 +981,8 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
     if (n_groups == 0) continue;
     kern<<<(n_groups + TN - 1) / TN, NT, mbytes, s>>>(m, a.neq, np, c_first, n_groups,
-                                                     td.parent.get(), a.ops_dev, mult32, msum);
+                                                     td.parent.get(), a.ops_dev, mult32, msum,
+                                                     mult_tc);
     FMMB_CUDA(cudaGetLastError());
   }
 }
@@ -987,15 +1006,15 @@ void node_charge_sums(const PassArgs &a, const double *tau_s, double *tsum, cuda
 }
 
 void run_upward_mixed(const PassArgs &a, const double *tau_s, const double *tsum, float *mult32,
-                      double *msum, cudaStream_t s) {
+                      double *msum, float *mult_tc, cudaStream_t s) {
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE: upward_mx_impl<LaplaceF32>(a, tau_s, tsum, mult32, msum, s); break;
+    case KERNEL_LAPLACE: upward_mx_impl<LaplaceF32>(a, tau_s, tsum, mult32, msum, mult_tc, s); break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
 
-void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, double *ple,
-                   int *err, cudaStream_t s) {
+void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc, const double *msum,
+                   double *ple, int *err, cudaStream_t s) {
   const TreeHost &th = *a.th;
   if (th.L < 3) return;
   FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
@@ -1031,15 +1050,12 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const double *msum, d
       }
     }
     tc.tile_start[4 * th.L] = ctiles;
-    const size_t ntc = (a.np + 15) & ~15;
-    const size_t a_sz = (size_t(TCM) * a.np * 4 + 1023) & ~size_t(1023);
-    const size_t b_sz = (ntc * a.np * 4 + 1023) & ~size_t(1023);
-    size_t sm = 4 * a_sz + 4 * b_sz + 1024;
+    size_t sm = TC_STAGES * m2l_tc_stage_bytes(a.np);
     if (sm < 80 * 1024) sm = 80 * 1024;
     FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     PhaseTimer timer(PH_M2L, s);
     k_m2l_tc<<<ctiles, TCM, sm, s>>>(tc, a.neq, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
-                                     mult32, msum, ple, err);
+                                     mult_tc, msum, ple, err);
     FMMB_CUDA(cudaGetLastError());
     return;
   }
