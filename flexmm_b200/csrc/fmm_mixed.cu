@@ -744,7 +744,8 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
                   const LevelOpsDev *__restrict__ ops, const float *__restrict__ loc32,
                   const double *__restrict__ lsum, const double *__restrict__ txs,
                   const double *__restrict__ tys, const int *__restrict__ tperm, int check,
-                  double *__restrict__ out, int64_t ld_out, int *__restrict__ next_item) {
+                  int self_eval, double *__restrict__ out, int64_t ld_out,
+                  int *__restrict__ next_item) {
   __shared__ EvalDesc D;
   __shared__ float4 src[SMAX];  // (x, y, charge, sorted index) in width units of the leaf
   // NOUT = 3: the low parts of the source coordinates (x = hi + lo): the
@@ -814,6 +815,24 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
     // and is redone in FP64 on the exact coordinates: the one such pair a
     // thread meets (a source evaluated at itself) directly, more by a rescan.
     double exact = 0.0, exact_x = 0.0, exact_y = 0.0;
+    // source evaluation (targets are the tree's sorted sources): the range
+    // [own_lo, own_lo + own_n) of the item's concatenated sources that holds
+    // its targets, and this target's own index there
+    int own = -1, own_lo = 0, own_n = 0;
+    if (self_eval) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        const int n = D.rs[c + 1] - D.rs[c];
+        if (t0 >= D.rb[c] && t0 < D.rb[c] + n) {
+          own_lo = D.rs[c];
+          own_n = n;
+          if (valid && t0 + t < D.rb[c] + n) own = D.rs[c] + (t0 + t - D.rb[c]);
+        }
+      }
+    }
+    // untested sweeps first, except where most targets coincide with a
+    // source that is not known by index (general-path source evaluation)
+    const bool fast = self_eval || !check;
     for (int base = 0; base < ns; base += SMAX) {
       const int nb = min(SMAX, ns - base);
       if (base > 0) __syncthreads();  // previous chunk fully read
@@ -830,6 +849,131 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
       }
       __syncthreads();
       if (valid) {
+        // a coincident pair: the source's kernel offset is already in csrc:
+        // take it out and add the FP64 kernel unless the points coincide
+        // exactly (check)
+        auto fix = [&](int jj) {
+          const int q = __float_as_int(src[jj].w);
+          const double qx = sx[q], qy = sy[q];
+          exact -= kofs * tau[q];
+          if (!(check && x - qx == 0.0 && y - qy == 0.0)) {
+            if constexpr (NOUT == 1)
+              exact += K64(qx, qy, x, y) * tau[q];
+            else
+              K64.grad(qx, qy, x, y, tau[q], exact, exact_x, exact_y);
+          }
+        };
+        // Fast sweep, no pair tests: a pair closer than FLT_MIN (squared,
+        // width units) makes the flushed log2 (and reciprocal) infinite, so a
+        // non-finite sum sends the chunk to the tested sweep below.  In source
+        // evaluation the own leaf's range [sa, sb) is swept last, rotated so
+        // that each thread starts after its own point and never meets it; the
+        // other ranges have bounds common to all threads (no divergence).
+        static_assert(KF32::kInfAtZero, "the fast sweep needs radial(d2 < FLT_MIN) = +-inf");
+        const int sa = own_lo - base, sb = sa + own_n;
+        const bool rot = own >= 0 && sa >= 0 && sb <= nb;
+        const int o = own - base - sa;  // own point within [sa, sb)
+        const double acc0 = acc, accx0 = accx, accy0 = accy;
+        if (fast) {
+          if constexpr (NOUT == 1) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+            auto pair = [&](const float4 q, float &p) {
+              const float dx = tx - q.x, dy = ty - q.y;
+              p = fmaf(K.radial(fmaf(dy, dy, dx * dx)), q.z, p);
+            };
+            auto flush = [&] {
+              acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+              p0 = p1 = p2 = p3 = 0.f;
+            };
+            auto sweep = [&](int lo, int hi) {
+              int j = lo + sub, nsum = 0;
+              for (; j + 3 * G < hi; j += 4 * G) {
+                pair(src[j], p0);
+                pair(src[j + G], p1);
+                pair(src[j + 2 * G], p2);
+                pair(src[j + 3 * G], p3);
+                if (++nsum == 8) {
+                  flush();
+                  nsum = 0;
+                }
+              }
+              for (; j < hi; j += G) pair(src[j], p0);
+              flush();
+            };
+            if (rot) {
+              sweep(0, sa);
+              sweep(sb, nb);
+              // own leaf: offsets 1 .. own_n-1 from the own point, cyclically
+              int k = sub + 1;
+              for (; k + G < own_n; k += 2 * G) {
+                int j0 = o + k, j1 = o + k + G;
+                j0 -= j0 >= own_n ? own_n : 0;
+                j1 -= j1 >= own_n ? own_n : 0;
+                pair(src[sa + j0], p0);
+                pair(src[sa + j1], p1);
+              }
+              if (k < own_n) {
+                int j0 = o + k;
+                j0 -= j0 >= own_n ? own_n : 0;
+                pair(src[sa + j0], p2);
+              }
+              flush();
+            } else {
+              sweep(0, nb);
+            }
+          } else {
+            float p[2] = {0.f, 0.f}, px[2] = {0.f, 0.f}, py[2] = {0.f, 0.f};
+            auto pair = [&](int jj, int a) {
+              const float4 q = src[jj];
+              const float2 ql = src_lo[jj];
+              const float dx = (tx - q.x) + (tx_lo - ql.x), dy = (ty - q.y) + (ty_lo - ql.y);
+              const float d2 = fmaf(dy, dy, dx * dx);
+              p[a] = fmaf(K.radial(d2), q.z, p[a]);
+              const float qr = rcp_ftz(d2) * q.z;
+              px[a] = fmaf(dx, qr, px[a]);
+              py[a] = fmaf(dy, qr, py[a]);
+            };
+            auto flush = [&] {
+              acc += (double)p[0] + (double)p[1];
+              accx += (double)px[0] + (double)px[1];
+              accy += (double)py[0] + (double)py[1];
+              p[0] = p[1] = px[0] = px[1] = py[0] = py[1] = 0.f;
+            };
+            auto sweep = [&](int lo, int hi) {
+              int j = lo + sub, nsum = 0;
+              for (; j + G < hi; j += 2 * G) {
+                pair(j, 0);
+                pair(j + G, 1);
+                if (++nsum == 16) {
+                  flush();
+                  nsum = 0;
+                }
+              }
+              if (j < hi) pair(j, 0);
+              flush();
+            };
+            if (rot) {
+              sweep(0, sa);
+              sweep(sb, nb);
+              for (int k = sub + 1; k < own_n; k += G) {
+                int j0 = o + k;
+                j0 -= j0 >= own_n ? own_n : 0;
+                pair(sa + j0, (k / G) & 1);
+              }
+              flush();
+            } else {
+              sweep(0, nb);
+            }
+          }
+        }
+        bool finite = fast && isfinite(acc);
+        if constexpr (NOUT == 3) finite = finite && isfinite(accx) && isfinite(accy);
+        if (finite) {
+          if (rot && sub == 0) fix(sa + o);  // all G threads of the target skipped it
+        } else {
+        acc = acc0;
+        accx = accx0;
+        accy = accy0;
         int nhit = 0, hj = 0;
         if constexpr (NOUT == 1) {
           float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
@@ -889,19 +1033,6 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
           accy += (double)py[0] + (double)py[1];
         }
         if (nhit) {
-          // the source's kernel offset is already in csrc: take it out and
-          // add the FP64 kernel unless the points coincide exactly (check)
-          auto fix = [&](int jj) {
-            const int q = __float_as_int(src[jj].w);
-            const double qx = sx[q], qy = sy[q];
-            exact -= kofs * tau[q];
-            if (!(check && x - qx == 0.0 && y - qy == 0.0)) {
-              if constexpr (NOUT == 1)
-                exact += K64(qx, qy, x, y) * tau[q];
-              else
-                K64.grad(qx, qy, x, y, tau[q], exact, exact_x, exact_y);
-            }
-          };
           if (nhit == 1) {
             fix(hj);
           } else {
@@ -916,6 +1047,7 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
             }
           }
         }
+        }  // tested sweep
       }
     }
     double r[NOUT];
@@ -1107,6 +1239,9 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
       it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
       td.ymid.get(), tsum, desc.get());
   FMMB_CUDA(cudaGetLastError());
+  // targets that are the tree's own sorted sources: each target's own point
+  // is left out of the pair sweep
+  const int self_eval = txs == td.sx.get() && tys == td.sy.get();
   PhaseTimer timer(PH_EVAL, s);
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: {
@@ -1115,7 +1250,8 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
       const int per_sm = nout == 3 ? 6 : EVAL_BLOCKS_PER_SM;
       kern<<<148 * per_sm, TCH, 0, s>>>(a.kp, a.neq, a.np, desc.get(), it.n_items.get(),
                                         td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc32, lsum,
-                                        txs, tys, tperm, check, out, ld_out, next_item.get());
+                                        txs, tys, tperm, check, self_eval, out, ld_out,
+                                        next_item.get());
       break;
     }
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");

@@ -127,6 +127,8 @@ __device__ __forceinline__ float lg2_ftz(float x) {
 // apart in FP64).
 struct LaplaceF32 {
   static constexpr bool kScaled = true;
+  // radial(d2) is -inf for d2 below FLT_MIN (the flushed log2 of 0)
+  static constexpr bool kInfAtZero = true;
   static constexpr float kScale = (float)(-0.69314718055994531 / (4.0 * M_PI));  // -ln2 / (4 pi)
   __host__ __device__ explicit LaplaceF32(const KernelParams &) {}
   // -log(d2)/(4 pi) = -(ln 2 / 4 pi) * log2(d2); on width-scaled coordinates

@@ -73,4 +73,6 @@ def test_tcgen05_m2l_matches_warp_mma_m2l(built_lib, tmp_path):
     subprocess.run([sys.executable, "-c", _SYNC_SCRIPT.format(repo=REPO, out=out)], env=env,
                    check=True, timeout=600)
     us = np.load(out)
-    assert rel_l2(ut, us) < 1e-8
+    # both are FP32-rounded forms of the same translation (the tcgen05 path
+    # adds its k-step slots in FP32): ~1e-8 apart, against ~1e-7 form error
+    assert rel_l2(ut, us) < 3e-8

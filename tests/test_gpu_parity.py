@@ -146,7 +146,11 @@ def test_own_source_evaluation_equals_general_path(built_lib, precision):
     u_own = F.source_evaluation(x, y).cpu().numpy()
     u_gen = F.source_evaluation(x.clone(), y.clone()).cpu().numpy()
     F.status()
-    assert rel_l2(u_own, u_gen) < 1e-14
+    # FP64: the same arithmetic.  Mixed: the own-source sweep leaves each
+    # target's own point out of its FP32 partial sums while the general path
+    # zeroes it in place, so the FP32 summation order differs (~1e-9 here,
+    # against the form's ~1e-7 error)
+    assert rel_l2(u_own, u_gen) < (1e-14 if precision == "fp64" else 1e-8)
     if precision == "fp64":
         assert rel_l2(u_own[g["src_idx"]], g["src_val"]) < PARITY
     x.add_(0.0)

@@ -100,8 +100,10 @@ def test_gradient_on_own_sources_equals_general_path(built_lib, precision):
     a = F.evaluate_to_points(x, y, "gradient", True).cpu().numpy()
     b = F.evaluate_to_points(x.clone(), y.clone(), "gradient", True).cpu().numpy()
     F.status()
+    # mixed: the own-source sweep's FP32 partial sums leave each target's own
+    # point out instead of zeroing it in place (a different FP32 order)
     for r in range(3):
-        assert rel_l2(a[r], b[r]) < 1e-14
+        assert rel_l2(a[r], b[r]) < (1e-14 if precision == "fp64" else 1e-7)
     if precision == "fp64":
         for r in range(3):
             assert rel_l2(a[r], g["src_val"][r]) < PARITY
