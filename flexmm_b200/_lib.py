@@ -84,6 +84,7 @@ SIGNATURES = [
      [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _dp, _vp, ctypes.POINTER(_vp)]),
     ("fmm_plan_info", ctypes.c_int, [_vp, _ip, _dp, _ip]),
     ("fmm_plan_bind", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("fmm_plan_bind_levels", ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     ("fmm_plan_set_precision", ctypes.c_int, [_vp, ctypes.c_int]),
     ("fmm_build_expansions", ctypes.c_int, [_vp, _vp, _vp]),
     ("fmm_evaluate", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),

@@ -42,6 +42,7 @@ struct LevelEntry {
   DevBuf<double> buf;
   DevBuf<float> buf32;
   LevelOpsDev dev;
+  DevBuf<LevelOpsDev> dev_copy;  // `dev` in device memory, gathered per plan by a kernel
   DevBuf<double> bb_m2l;  // black-box FMM: [np x 40 np], offset blocks side by side
   DevBuf<double> st;      // Stokes FMM: this width's operators (StokesArgs::Level layout)
   StokesArgs::Level st_lev{};
@@ -416,6 +417,8 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *lv, int *level_id) {
       e->dev.kind[o] = kind[o];
       e->dev.rp[o] = rp[o];
     }
+    e->dev_copy.alloc(1, 0);
+    FMMB_CUDA(cudaMemcpy(e->dev_copy.get(), &e->dev, sizeof(LevelOpsDev), cudaMemcpyHostToDevice));
     ops->levels.push_back(std::move(e));
     *level_id = int(ops->levels.size()) - 1;
   });
@@ -638,6 +641,17 @@ int fmm_plan_bind(fmm_plan *p, int level, int level_id) {
   });
 }
 
+int fmm_plan_bind_levels(fmm_plan *p, int n_levels, const int *level_ids) {
+  return guarded([&] {
+    FMMB_CHECK(p && (level_ids || n_levels == 0), ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(n_levels >= 0 && n_levels <= p->th.L, ERR_INVALID_ARGUMENT, "level count out of range");
+    for (int m = 0; m < n_levels; ++m)
+      FMMB_CHECK(level_ids[m] >= -1 && level_ids[m] < (int)p->ops->levels.size(),
+                 ERR_INVALID_ARGUMENT, "unknown operator entry");
+    for (int m = 0; m < n_levels; ++m) p->bound[m] = level_ids[m];
+  });
+}
+
 static PassArgs pass_args(fmm_plan *p) {
   PassArgs a;
   a.kernel_id = p->ops->kernel_id;
@@ -646,11 +660,34 @@ static PassArgs pass_args(fmm_plan *p) {
   a.np = p->ops->np;
   a.td = &p->td;
   a.th = &p->th;
-  a.ops_host.assign(p->th.L, LevelOpsDev{});
-  for (int m = 0; m < p->th.L; ++m)
-    if (p->bound[m] >= 0) a.ops_host[m] = p->ops->levels[p->bound[m]]->dev;
   a.ops_dev = p->ops_dev.get();
   return a;
+}
+
+// The plan's per-level operator table, gathered on the device from the
+// operator set's entries (no host copy: the launch arguments carry the
+// entries' addresses)
+struct LevelOpsSrc {
+  const LevelOpsDev *p[FMM_MAX_LEVELS_DEV];
+};
+static_assert(sizeof(LevelOpsDev) % sizeof(int) == 0, "LevelOpsDev is copied as words");
+
+__global__ void k_gather_level_ops(LevelOpsSrc src, LevelOpsDev *__restrict__ dst) {
+  constexpr int NW = int(sizeof(LevelOpsDev) / sizeof(int));
+  const int *from = reinterpret_cast<const int *>(src.p[blockIdx.x]);
+  int *to = reinterpret_cast<int *>(dst + blockIdx.x);
+  for (int i = threadIdx.x; i < NW; i += blockDim.x) to[i] = from ? from[i] : 0;
+}
+
+static void upload_level_ops(fmm_plan *p, cudaStream_t s) {
+  const int L = p->th.L;
+  FMMB_CHECK(L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
+  p->ops_dev.alloc(L, s);
+  LevelOpsSrc src{};
+  for (int m = 0; m < L; ++m)
+    if (p->bound[m] >= 0) src.p[m] = p->ops->levels[p->bound[m]]->dev_copy.get();
+  k_gather_level_ops<<<L, 128, 0, s>>>(src, p->ops_dev.get());
+  FMMB_CUDA(cudaGetLastError());
 }
 
 static void ensure_blas(fmm_plan *p, cudaStream_t s) {
@@ -731,11 +768,8 @@ int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_
       FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
     const int np = p->ops->np;
     const int64_t total = th.n_total(), n = th.n_points, cs = total * np;
-    p->ops_dev.alloc(th.L, s);
+    upload_level_ops(p, s);
     PassArgs a = pass_args(p);
-    FMMB_CUDA(cudaMemcpyAsync(p->ops_dev.get(), a.ops_host.data(), th.L * sizeof(LevelOpsDev),
-                              cudaMemcpyHostToDevice, s));
-    a.ops_dev = p->ops_dev.get();
     p->tau_s.alloc((size_t)n_rhs * n, s);
     p->mult.alloc((size_t)n_rhs * cs, s);
     p->ple.alloc((size_t)n_rhs * cs, s);
@@ -828,11 +862,8 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       return;
     }
     std::unique_ptr<PhaseTimer> t_prep(new PhaseTimer(PH_PREP, s));
-    p->ops_dev.alloc(th.L, s);
+    upload_level_ops(p, s);
     PassArgs a = pass_args(p);
-    FMMB_CUDA(cudaMemcpyAsync(p->ops_dev.get(), a.ops_host.data(), th.L * sizeof(LevelOpsDev),
-                              cudaMemcpyHostToDevice, s));
-    a.ops_dev = p->ops_dev.get();
     p->tau_s.alloc(th.n_points, s);
     gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
     p->ple.alloc(total * np, s);
@@ -1002,11 +1033,10 @@ int fmm_plan_status(fmm_plan *p) {
 }
 
 int fmm_plan_destroy(fmm_plan *p) {
-  return guarded([&] {
-    if (!p) return;
-    cudaStreamSynchronize(p->stream);
-    delete p;
-  });
+  // no host wait: the plan's device buffers go back to the pool with
+  // cudaFreeAsync on the stream they were allocated on, after the work
+  // already queued there
+  return guarded([&] { delete p; });
 }
 
 int fmm_tree_export(fmm_plan *p, double *xmin, double *ymin, int *bot, int *top, int *parent,

@@ -49,7 +49,6 @@ struct PassArgs {
   const TreeDev *td;
   const TreeHost *th;
   const LevelOpsDev *ops_dev;   // device array indexed by level
-  std::vector<LevelOpsDev> ops_host;
 };
 
 // Black-box (Chebyshev) FMM (bbfmm.cu): p x p coefficients per box, NQ = p^2

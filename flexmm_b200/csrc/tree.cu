@@ -26,6 +26,8 @@
 //     searches in sorted arrays.
 #include <cub/cub.cuh>
 
+#include <cmath>
+
 #include <memory>
 
 #include "timing.cuh"
@@ -107,30 +109,82 @@ __device__ __forceinline__ int64_t lower_bound(const T *a, int64_t lo, int64_t h
   return lo;
 }
 
-// --- 1. point keys: the reference's descent, digit by digit -----------------
+// --- 1. point keys -----------------------------------------------------------
+// The reference locates a point by descending the tree: at each level it
+// compares the point with the box midpoint xmin + w/2, computed level by
+// level in FP64.  key_descent restates that descent digit by digit.
+__device__ __forceinline__ uint64_t key_descent(double px, double py, double x0, double y0,
+                                                double w0) {
+  double xmin = x0, ymin = y0, w = w0;
+  uint64_t key = 0;
+#pragma unroll 1
+  for (int l = 0; l < MAXD; ++l) {
+    const double hw = 0.5 * w;
+    const double xm = __dadd_rn(xmin, hw);
+    const double ym = __dadd_rn(ymin, hw);
+    const int hx = px > xm, hy = py > ym;
+    key = (key << 2) | uint64_t(2 * hx + hy);
+    xmin = hx ? xm : __dsub_rn(xm, hw);
+    ymin = hy ? ym : __dsub_rn(ym, hw);
+    w = hw;
+  }
+  return key;
+}
+
+// bits 0..28 of v to the even bit positions 0..56
+__device__ __forceinline__ uint64_t spread_bits(uint64_t v) {
+  v &= (uint64_t(1) << MAXD) - 1;
+  v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+  v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+  v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  v = (v | (v << 2)) & 0x3333333333333333ull;
+  v = (v | (v << 1)) & 0x5555555555555555ull;
+  return v;
+}
+
+// Every midpoint of the descent lies on a line x0 + k w0 / 2^MAXD, off by
+// its accumulated FP64 rounding at most.  A point whose scaled coordinate
+// q = (p - x0) 2^MAXD / w0 is farther than `margin` from every integer is on
+// the same side of all of them as floor(q) says, so its digits are the bits
+// of floor(q) (interleaved x, y); points within the margin (and NaN or
+// infinite ones) take the descent itself.  The margin covers both roundings
+// with a wide factor; the host sets it.
 __global__ void k_point_keys(const double *__restrict__ x, const double *__restrict__ y,
-                             int64_t n, double x0, double y0, double w0,
-                             uint64_t *__restrict__ keys, int *__restrict__ idx) {
+                             int64_t n, double x0, double y0, double w0, double scale,
+                             double margin, uint64_t *__restrict__ keys, int *__restrict__ idx) {
+  const double qmax = double(uint64_t(1) << MAXD);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const double px = x[i], py = y[i];
-    double xmin = x0, ymin = y0, w = w0;
-    uint64_t key = 0;
-#pragma unroll 1
-    for (int l = 0; l < MAXD; ++l) {
-      const double hw = 0.5 * w;
-      const double xm = __dadd_rn(xmin, hw);
-      const double ym = __dadd_rn(ymin, hw);
-      const int hx = px > xm, hy = py > ym;
-      key = (key << 2) | uint64_t(2 * hx + hy);
-      xmin = hx ? xm : __dsub_rn(xm, hw);
-      ymin = hy ? ym : __dsub_rn(ym, hw);
-      w = hw;
+    const double qx = (px - x0) * scale, qy = (py - y0) * scale;
+    const bool clear = fabs(qx - rint(qx)) > margin && fabs(qy - rint(qy)) > margin;
+    uint64_t key;
+    if (clear) {
+      const double fx = fmin(fmax(floor(qx), 0.0), qmax - 1.0);
+      const double fy = fmin(fmax(floor(qy), 0.0), qmax - 1.0);
+      key = (spread_bits(uint64_t(fx)) << 1) | spread_bits(uint64_t(fy));
+    } else {
+      key = key_descent(px, py, x0, y0, w0);
     }
     keys[i] = key;
     idx[i] = int(i);
   }
 }
+
+namespace {
+// scale and margin of k_point_keys for a tree box (x0, y0, w0)
+void key_params(double x0, double y0, double w0, double &scale, double &margin) {
+  scale = std::ldexp(1.0, MAXD) / w0;
+  // A descent midpoint is off its line by at most two roundings per level,
+  // each within half an ulp of the box's largest coordinate X: MAXD 2^-51 X,
+  // i.e. 29 2^-22 X / w0 < 7e-6 X / w0 in units of q.  q itself is within
+  // 3 2^-53 of its value relative, 2e-7 absolute.  2^-14 (6.1e-5) times
+  // max(1, X / w0) covers both about 8 times over.
+  const double big = std::fmax(std::fmax(std::fabs(x0), std::fabs(x0 + w0)),
+                               std::fmax(std::fabs(y0), std::fabs(y0 + w0)));
+  margin = std::ldexp(1.0, -14) * std::fmax(1.0, big / w0);
+}
+}  // namespace
 
 __global__ void k_gather_xy(const double *__restrict__ x, const double *__restrict__ y,
                             const int *__restrict__ perm, int64_t n, double *__restrict__ sx,
@@ -417,6 +471,13 @@ __global__ void k_node_codes(const int *__restrict__ off, int L, int total,
   }
 }
 
+// Per node: 12 binary searches (8 colleagues, point range bot / top,
+// parent, children), run as one branchless loop: a search over a range of n
+// keys takes ceil(log2 n) steps whatever it looks for, so the searches of
+// each step issue their loads together and the dependent chain is as long
+// as the longest search (~20 loads for 1M points), not the sum of all.
+constexpr int NA_SEARCH = 12;
+
 __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, double x0, double y0,
                              double w0, const uint64_t *__restrict__ pts, int64_t npts,
                              const uint64_t *__restrict__ pkeys, const uint8_t *__restrict__ pisx,
@@ -430,6 +491,90 @@ __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, doub
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     const int m = level_of(off, L, g);
     const uint64_t c = code[g];
+    uint32_t ix, iy;
+    morton_xy(c, m, ix, iy);
+    nix[g] = int(ix);
+    niy[g] = int(iy);
+    // searches: 0-7 colleagues (offsets (-1..1)^2 without the centre, in
+    // offset order), 8 bot, 9 top, 10 parent, 11 children.  Every step of
+    // every search is taken (a finished or empty one steps by 0 and reloads
+    // a valid element), so each step's 12 loads issue together.
+    auto arr = [&](int k) -> const uint64_t * {
+      return (k == 8 || k == 9) ? pts : (k == 11 ? pkeys : code);
+    };
+    uint64_t val[NA_SEARCH];
+    int base[NA_SEARCH], len[NA_SEARCH];
+    const uint32_t side = 1u << m;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int d = k + (k >= 4);
+      const int64_t qx = int64_t(ix) + d / 3 - 1, qy = int64_t(iy) + d % 3 - 1;
+      const bool in = qx >= 0 && qy >= 0 && qx < side && qy < side;
+      val[k] = in ? morton_of(uint32_t(qx), uint32_t(qy), m) : 0;
+      base[k] = off[m];  // level m holds this node: a valid index
+      len[k] = in ? off[m + 1] - off[m] : 0;
+    }
+    const int sh = 2 * (MAXD - m);
+    val[8] = c << sh, base[8] = 0, len[8] = int(npts);
+    val[9] = (c + 1) << sh, base[9] = 0, len[9] = int(npts);
+    val[10] = c >> 2, base[10] = m > 0 ? off[m - 1] : 0, len[10] = m > 0 ? off[m] - off[m - 1] : 0;
+    const bool has_pb = m < L - 1 && pb[m + 1] > pb[m];
+    val[11] = box_code(m, c), base[11] = has_pb ? pb[m] : 0;  // pkeys[0] exists
+    len[11] = has_pb ? pb[m + 1] - pb[m] : 0;
+    // bot / top (k = 8, 9) want the lower bound: the last element below the
+    // key moves the window; the others look the key itself up: the last
+    // element not above it does, and the window ends on the key if present
+    auto lower = [](int k) { return k == 8 || k == 9; };
+    for (bool more = true; more;) {
+      uint64_t a[NA_SEARCH];
+#pragma unroll
+      for (int k = 0; k < NA_SEARCH; ++k) a[k] = __ldg(arr(k) + base[k] + (len[k] >> 1));
+      more = false;
+#pragma unroll
+      for (int k = 0; k < NA_SEARCH; ++k) {
+        const int half = len[k] >> 1;
+        base[k] += (lower(k) ? a[k] < val[k] : a[k] <= val[k]) ? half : 0;
+        len[k] -= half;
+        more |= len[k] > 1;
+      }
+    }
+    int lb[NA_SEARCH];  // lower bound (k = 8, 9) or the key's index (others, if eq)
+    bool eq[NA_SEARCH];
+#pragma unroll
+    for (int k = 0; k < NA_SEARCH; ++k) {
+      const uint64_t v = __ldg(arr(k) + base[k]);
+      lb[k] = base[k] + (lower(k) && len[k] == 1 && v < val[k] ? 1 : 0);
+      eq[k] = len[k] == 1 && v == val[k];
+    }
+    bot[g] = lb[8];
+    top[g] = lb[9];
+    parent[g] = m == 0 ? -1 : lb[10];
+    // children: is this box a parent box?
+    uint8_t f = flags[g];
+    int ch = -1;
+    if (eq[11]) {
+      ch = off[m + 1] + 4 * (lb[11] - pb[m]);
+      f |= NF_CHILDREN;
+      if (pisx[lb[11]]) f |= NF_XLIST;
+    }
+    if (!(f & NF_FAKE) && (ch < 0 || (f & NF_XLIST))) f |= NF_LEAF;
+    flags[g] = f;
+    child[g] = ch;
+    // colleagues: existing same-level boxes at offsets (-1..1)^2, self
+    // included, first in offset order, then -1
+    int kc = 0;
+#pragma unroll
+    for (int d = 0; d < 9; ++d) {
+      int found;
+      if (d == 4) {
+        found = g;
+      } else {
+        const int k = d - (d > 4);
+        found = eq[k] ? lb[k] : -1;
+      }
+      if (found >= 0) coll[int64_t(g) * 9 + (kc++)] = found;
+    }
+    for (; kc < 9; ++kc) coll[int64_t(g) * 9 + kc] = -1;
     // geometry: replay the descent along the node's digits (bit-exact with the reference)
     double xm0 = x0, ym0 = y0, w = w0;
     for (int l = 0; l < m; ++l) {
@@ -445,47 +590,6 @@ __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, doub
     ymin[g] = ym0;
     xmid[g] = __dadd_rn(xm0, hw);
     ymid[g] = __dadd_rn(ym0, hw);
-    // point range
-    const int sh = 2 * (MAXD - m);
-    bot[g] = int(lower_bound<uint64_t>(pts, 0, npts, c << sh));
-    top[g] = int(lower_bound<uint64_t>(pts, 0, npts, (c + 1) << sh));
-    // parent
-    parent[g] = (m == 0) ? -1
-                         : int(lower_bound<uint64_t>(code, off[m - 1], off[m], c >> 2));
-    // children: is this box a parent box?
-    uint8_t f = flags[g];
-    int ch = -1;
-    if (m < L - 1) {
-      const uint64_t key = box_code(m, c);
-      const int64_t e = lower_bound<uint64_t>(pkeys, pb[m], pb[m + 1], key);
-      if (e < pb[m + 1] && pkeys[e] == key) {
-        ch = off[m + 1] + 4 * int(e - pb[m]);
-        f |= NF_CHILDREN;
-        if (pisx[e]) f |= NF_XLIST;
-      }
-    }
-    if (!(f & NF_FAKE) && (ch < 0 || (f & NF_XLIST))) f |= NF_LEAF;
-    flags[g] = f;
-    child[g] = ch;
-    // colleagues: existing same-level boxes at offsets (-1..1)^2, self included
-    uint32_t ix, iy;
-    morton_xy(c, m, ix, iy);
-    nix[g] = int(ix);
-    niy[g] = int(iy);
-    const uint32_t side = 1u << m;
-    int k = 0;
-    for (int dx = -1; dx <= 1; ++dx)
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int64_t qx = int64_t(ix) + dx, qy = int64_t(iy) + dy;
-        int found = -1;
-        if (qx >= 0 && qy >= 0 && qx < side && qy < side) {
-          const uint64_t q = morton_of(uint32_t(qx), uint32_t(qy), m);
-          const int64_t e = lower_bound<uint64_t>(code, off[m], off[m + 1], q);
-          if (e < off[m + 1] && code[e] == q) found = int(e);
-        }
-        if (found >= 0) coll[int64_t(g) * 9 + (k++)] = found;
-      }
-    for (; k < 9; ++k) coll[int64_t(g) * 9 + k] = -1;
   }
 }
 
@@ -505,24 +609,32 @@ __global__ void k_interactions(const int *__restrict__ off, int L, int total,
                                const int *__restrict__ ix, const int *__restrict__ iy,
                                const int *__restrict__ bot, const int *__restrict__ top,
                                int *__restrict__ il) {
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+  // 8 lanes per node: lane j takes the parent's colleague j (and 8), with
+  // its four children
+  const int sub = threadIdx.x & 7;
+  const unsigned gmask = 0xffu << (threadIdx.x & 24);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x / 8;
+  for (int64_t gg = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 8; gg < total;
+       gg += stride) {
+    const int g = int(gg);
     int *row = il + int64_t(g) * N_OFFSETS;
-    for (int o = 0; o < N_OFFSETS; ++o) row[o] = -1;
-    if (g < off[min(2, L)] || (flags[g] & NF_FAKE)) continue;
+    for (int o = sub; o < N_OFFSETS; o += 8) row[o] = -1;
+    if (g < off[min(2, L)] || (flags[g] & NF_FAKE)) continue;  // the same for the whole group
+    __syncwarp(gmask);  // the -1 row before the entries
     const int P = parent[g];
     const int tx = ix[g], ty = iy[g];
-    for (int j = 0; j < 9; ++j) {
+    for (int j = sub; j < 9; j += 8) {
       const int c = coll[int64_t(P) * 9 + j];
-      if (c < 0) break;
-      if (c == P) continue;
+      if (c < 0 || c == P) continue;
       const int ch = child[c];
       if (ch < 0) continue;
+#pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int cc = ch + k;
         const int ox = ix[cc] - tx, oy = iy[cc] - ty;
         if (ox < -3 || ox > 3 || oy < -3 || oy > 3) continue;
         const int o = c_cell_to_offset[(ox + 3) * 7 + (oy + 3)];
-        if (o >= 0 && top[cc] > bot[cc]) row[o] = cc;
+        if (o >= 0 && top[cc] > bot[cc]) row[o] = cc;  // distinct boxes: distinct offsets
       }
     }
   }
@@ -609,7 +721,10 @@ void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th
   keys.alloc(n, s);
   perm.alloc(n, s);
   if (n == 0) return;
-  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, k0.get(), i0.get());
+  double scale, margin;
+  key_params(th.x0, th.y0, th.w0, scale, margin);
+  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin,
+                                                 k0.get(), i0.get());
   FMMB_CUDA(cudaGetLastError());
   const int digits = sorted_digits < 1 ? 1 : (sorted_digits > MAXD ? MAXD : sorted_digits);
   radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * (MAXD - digits), 2 * MAXD, s);
@@ -630,7 +745,10 @@ void sort_points_scratch(const double *x, const double *y, int64_t n, const Tree
   *keys = k0;
   *perm = i0;
   if (n == 0) return;
-  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, k0, i0);
+  double scale, margin;
+  key_params(th.x0, th.y0, th.w0, scale, margin);
+  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin, k0,
+                                                 i0);
   FMMB_CUDA(cudaGetLastError());
   cub::DoubleBuffer<uint64_t> kb(k0, k1);
   cub::DoubleBuffer<int> vb(i0, i1);
@@ -673,6 +791,11 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
                                                    s0raw.get(), cap0, cnt.get());
     FMMB_CUDA(cudaGetLastError());
+    // the sorted coordinates need no count: queued before the host waits
+    td.sx.alloc(n, s);
+    td.sy.alloc(n, s);
+    k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, td.ordv.get(), n, td.sx.get(), td.sy.get());
+    FMMB_CUDA(cudaGetLastError());
     FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
     FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
@@ -684,10 +807,6 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   spos.release();
   t_split.reset();
   std::unique_ptr<PhaseTimer> t_bal(new PhaseTimer(PH_TREE_BALANCE, s));
-  td.sx.alloc(n, s);
-  td.sy.alloc(n, s);
-  k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, td.ordv.get(), n, td.sx.get(), td.sy.get());
-  FMMB_CUDA(cudaGetLastError());
   const int64_t n0 = (int64_t)hc.s0_count;
   const int L = (n0 > 0) ? hc.max_level + 2 : 1;
   th.L = L;
@@ -834,7 +953,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
       td.ymid.get(), td.bot.get(), td.top.get(), td.parent.get(), td.child.get(), td.coll.get(),
       td.ix.get(), td.iy.get());
   FMMB_CUDA(cudaGetLastError());
-  k_interactions<<<grid_for(total, TPB), TPB, 0, s>>>(
+  k_interactions<<<grid_for(int64_t(total) * 8, TPB), TPB, 0, s>>>(
       td.dev_off.get(), L, total, td.flags.get(), td.parent.get(), td.child.get(), td.coll.get(),
       td.ix.get(), td.iy.get(), td.bot.get(), td.top.get(), td.il.get());
   FMMB_CUDA(cudaGetLastError());

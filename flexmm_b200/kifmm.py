@@ -194,8 +194,8 @@ class KI_FMM:
         if verbose:
             print("....Tree formed in:             {:0.1f}".format((time.time() - st) * 1000))
         # operators for every level width (KI_Helper.prepare, flexmm/flexmm2d/kifmm.py:67-82)
-        for m, w in enumerate(self._widths):
-            _lib.call("fmm_plan_bind", plan, m, self.helper.level_id(w))
+        ids = (ctypes.c_int * nl.value)(*[self.helper.level_id(w) for w in self._widths])
+        _lib.call("fmm_plan_bind_levels", plan, nl.value, ctypes.cast(ids, ctypes.c_void_p))
         self._tree = None
         self._expanded = False
         # named evaluators (kifmm2d FMM.__init__ registers 'potential_evaluation')

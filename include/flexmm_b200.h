@@ -13,6 +13,7 @@
  *                        (flexmm/flexmm2d/fmm.py:33-58, flexmm/tree.py:451-518)
  *   fmm_plan_info /      the tree's level widths, to fill and bind the
  *   fmm_plan_bind        operator cache (KI_Helper.prepare, kifmm.py:67-82)
+ *   fmm_plan_bind_levels the same for all levels at once
  *   fmm_build_expansions FMM.build_expansions(tau) (fmm.py:151-153)
  *   fmm_evaluate         FMM.source_evaluation / target_evaluation
  *                        (fmm.py:158-176); check=1 skips coincident pairs
@@ -156,6 +157,10 @@ int fmm_plan_info(fmm_plan *plan, int *n_levels, double *widths, int *n_nodes);
 int fmm_plan_set_precision(fmm_plan *plan, int precision);
 /* Use operator entry level_id (from fmm_ops_add) for tree level `level`. */
 int fmm_plan_bind(fmm_plan *plan, int level, int level_id);
+/* fmm_plan_bind for levels 0 .. n_levels-1 in one call: level_ids[l] for
+ * level l (-1 leaves a level unbound).  Same operator cache as
+ * fmm_plan_bind (KI_Helper.prepare, kifmm.py:67-82). */
+int fmm_plan_bind_levels(fmm_plan *plan, int n_levels, const int *level_ids);
 /* tau: device charges [n] in the caller's (original) source order. */
 int fmm_build_expansions(fmm_plan *plan, const double *tau, void *stream);
 /* Potential at m device points into device out[m]; check != 0 skips sources
@@ -198,6 +203,9 @@ int fmm_evaluate_outputs(fmm_plan *plan, int evaluator, const double *tx, const 
 /* The same at the plan's own source points (see fmm_evaluate_sources). */
 int fmm_evaluate_sources_outputs(fmm_plan *plan, int evaluator, int check, double *out,
                                  int64_t ld_out, void *stream);
+/* Releases the plan without waiting for the GPU: its device memory returns to
+ * the pool in stream order on the plan's stream (one stream per plan), so a
+ * loop that builds a plan per step keeps the host ahead of the GPU. */
 int fmm_plan_destroy(fmm_plan *plan);
 /* Wait for the plan's work and report failures of it: FMM_ERR_CUDA when a
  * kernel stopped one of its bounded waits (the results are then invalid). */

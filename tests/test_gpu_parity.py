@@ -46,6 +46,53 @@ def test_tree_matches_oracle(built_lib, case):
     assert canon.compare(a, b) == []
 
 
+def _descent_lines(p, x0, w0, levels):
+    """The midpoints the reference's descent compares point p with, level by
+    level (FP64, the same recurrence: xm = xmin + w/2)."""
+    out, xmin, w = [], x0, w0
+    for _ in range(levels):
+        hw = 0.5 * w
+        xm = xmin + hw
+        out.append(xm)
+        xmin = xm if p > xm else xm - hw
+        w = hw
+    return out
+
+
+def test_tree_with_points_on_split_lines_matches_oracle(built_lib):
+    """Points exactly on the descent's midpoints and one ulp either side, in
+    a box away from the origin (the midpoints carry FP64 rounding): the
+    device's fixed-point keys fall back to the descent there, so every point
+    lands in the reference's leaf."""
+    from flexmm_b200 import KI_FMM, KI_Helper
+    from oracle.tree import Tree
+    rng = np.random.default_rng(77)
+    bbox = [1000.3, 1000.3 + 0.9, -3.7, -3.7 + 0.9]
+    n = 12000
+    x = bbox[0] + 0.9 * rng.random(n)
+    y = bbox[2] + 0.9 * rng.random(n)
+    F0 = KI_FMM(x, y, "Laplace_Eval", 24, 16, bbox=bbox, helper=KI_Helper())
+    bb = F0.bbox
+    w0 = bb[1] - bb[0]
+    xs, ys = [x], [y]
+    for i in range(300):
+        lx = _descent_lines(x[i], bb[0], w0, 14)
+        ly = _descent_lines(y[i], bb[2], w0, 14)
+        for a, b in zip(lx, ly):
+            for v in (a, np.nextafter(a, -np.inf), np.nextafter(a, np.inf)):
+                xs.append(np.array([v, v, x[i]]))
+                ys.append(np.array([y[i], b, b]))
+    # coarse midpoints are shared by many base points: keep each point once
+    xy = np.unique(np.stack([np.concatenate(xs), np.concatenate(ys)], axis=1), axis=0)
+    x, y = xy[:, 0].copy(), xy[:, 1].copy()
+    F = KI_FMM(x, y, "Laplace_Eval", 24, 16, bbox=bbox, helper=KI_Helper())
+    assert list(F.bbox) == list(bb)   # the same box as the lines were drawn in
+    ot = Tree(x, y, 24, F.bbox)
+    a = canon.canonical(F.tree, triples_fn=canon.gpu_triples, nonempty_sources=True)
+    b = canon.canonical(ot, nonempty_sources=True)
+    assert canon.compare(a, b) == []
+
+
 def _direct(d, tx, ty, check):
     from oracle.direct import direct_laplace
     return direct_laplace(d["x"], d["y"], d["tau"], tx, ty, check)
