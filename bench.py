@@ -123,7 +123,12 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, bufsize=1)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
-            time.sleep(0.3)   # first sample lands before the timed work starts
+            # nvidia-smi's start-up must not overlap the timed work: wait for
+            # its first sample (bounded), then a little more
+            t_end = time.time() + 5.0
+            while not self.rows and time.time() < t_end:
+                time.sleep(0.05)
+            time.sleep(0.2)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -305,12 +310,14 @@ def measure(args, world, local, d, precision, flush, counts_cache):
         and "memcpy" not in ev.name.lower() and "memset" not in ev.name.lower())
 
     # timed region: K steps, L2 flushed between steps, CUDA events on the stream
-    enable_timing(True)
-    read_timing()
+    # (the library's per-phase event timers stay off here: they put event
+    # records between its kernels)
     barrier(world)
     torch.cuda.synchronize()
     times = []
     clk = ClockSampler(local).__enter__()
+    step(xd, yd, taud, txd, tyd)  # one untimed step with the sampler running
+    torch.cuda.synchronize()
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -321,9 +328,19 @@ def measure(args, world, local, d, precision, flush, counts_cache):
         times.append((e0, e1))
     torch.cuda.synchronize()
     barrier(world)
+    step_samples = [round(a.elapsed_time(b), 3) for a, b in times]
+    ms_step = dist_max(sum(a.elapsed_time(b) for a, b in times) / max(args.steps, 1), world)
+
+    # per-phase breakdown from separate, untimed steps with the timers on
+    n_phase = args.steps  # the breakdown is normalised per timed step count
+    enable_timing(True)
+    read_timing()
+    for _ in range(n_phase):
+        flush.fill_(1.0)
+        step(xd, yd, taud, txd, tyd)
+    torch.cuda.synchronize()
     phases = read_timing()
     enable_timing(False)
-    ms_step = dist_max(sum(a.elapsed_time(b) for a, b in times) / max(args.steps, 1), world)
 
     # end to end through the public API from pinned host memory
     pin = {k: torch.from_numpy(d[k]).pin_memory() for k in ("x", "y", "tau", "tx", "ty")}
@@ -359,8 +376,8 @@ def measure(args, world, local, d, precision, flush, counts_cache):
     # source evaluation on the FMM's own (unchanged) source tensors reads the
     # tree's copy: x, y are then uploaded once per step, not twice
     src_reused = F2._own_sources(pin["x"], pin["y"])
-    return dict(F=F, ms_step=ms_step, e2e_step=e2e_step, phases=phases, accuracy=accuracy,
-                src_reused=src_reused, e2e_samples=e2e_ms,
+    return dict(F=F, ms_step=ms_step, step_samples=step_samples, e2e_step=e2e_step, phases=phases,
+                accuracy=accuracy, src_reused=src_reused, e2e_samples=e2e_ms,
                 launches=launches_per_step * args.steps, clocks=clk.summary(), neq=neq,
                 counts=work_counts_gemm(F, neq, c))
 
@@ -454,7 +471,7 @@ def run_ours(args, world, rank, local):
     out = {
         "metric": METRIC, "value": world * pts / (main["ms_step"] * 1e-3) / 1e6, "unit": "Mpts/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_step"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_samples": main["step_samples"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+tf32x3/f64" if args.precision == "mixed" else "f64",
         "precision": args.precision,
         "data": "synthetic: seeded clustered sources and grid targets (no dataset)",

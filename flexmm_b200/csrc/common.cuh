@@ -99,6 +99,33 @@ struct DevBuf {
   T *get() const { return p; }
 };
 
+// Programmatic dependent launch: a kernel launched by launch_pdl may start
+// while the kernel before it in the stream is still running.  It must call
+// pdl_wait() before it touches anything an earlier kernel writes (after that
+// call every earlier kernel has completed and its writes are visible), and
+// calls pdl_trigger() only after pdl_wait(), so the kernel after it cannot
+// overtake the ones before it.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+void launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  FMMB_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...));
+}
+
 inline int grid_for(int64_t n, int threads, int cap = 148 * 16) {
   int64_t g = (n + threads - 1) / threads;
   if (g < 1) g = 1;

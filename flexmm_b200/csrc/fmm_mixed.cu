@@ -256,6 +256,8 @@ __global__ void __launch_bounds__(NT) k_m2m_mx(int m, int neq, int np, int c_fir
     stage_rows(Bh, ldb, op.m2mct_hi, 4 * np, np);
     stage_rows(Bl, ldb, op.m2mct_lo, 4 * np, np);
   }
+  pdl_wait();  // the children's multipoles come from the kernels before
+  pdl_trigger();
   const float *Ag = mult32 + (size_t)(c_first + 4 * e0) * np;
   stage_rows(A, lda, Ag, nloc, 4 * np);
   const int rowlen = 4 * np;
@@ -626,6 +628,8 @@ __global__ void __launch_bounds__(NT) k_downward_mx(int m, int neq, int np, int 
     node[threadIdx.x] = (grp < ngrp) ? rg[rg_lo + q0 + grp] + int(threadIdx.x & 3) : -1;
     orow[threadIdx.x] = P + threadIdx.x * ldp;
   }
+  pdl_wait();  // M2L results and the parents' locals come from the kernels before
+  pdl_trigger();
   __syncthreads();
   for (int i = threadIdx.x; i < TN * np; i += NT) {
     const int t = i / np, k = i % np;
@@ -1112,10 +1116,9 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
     const int c_first = th.off[m + 1];
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
     if (n_groups == 0) continue;
-    kern<<<(n_groups + TN - 1) / TN, NT, mbytes, s>>>(m, a.neq, np, c_first, n_groups,
-                                                     td.parent.get(), a.ops_dev, mult32, msum,
-                                                     mult_tc);
-    FMMB_CUDA(cudaGetLastError());
+    // level m's operators are staged while level m+1 finishes
+    launch_pdl(kern, dim3((n_groups + TN - 1) / TN), dim3(NT), mbytes, s, m, a.neq, np, c_first,
+               n_groups, td.parent.get(), a.ops_dev, mult32, msum, mult_tc);
   }
 }
 
@@ -1214,9 +1217,8 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
     const int lo = th.rg_lo[m], cnt = th.rg_hi[m] - th.rg_lo[m];
     if (cnt <= 0) continue;
     PhaseTimer timer(PH_DOWNWARD, s);
-    kern<<<(cnt + 7) / 8, NT, sm, s>>>(m, a.neq, a.np, lo, cnt, td.rg.get(), td.parent.get(),
-                                       a.ops_dev, ple, loc32, lsum);
-    FMMB_CUDA(cudaGetLastError());
+    launch_pdl(kern, dim3((cnt + 7) / 8), dim3(NT), sm, s, m, a.neq, a.np, lo, cnt, td.rg.get(),
+               td.parent.get(), a.ops_dev, ple, loc32, lsum);
   }
 }
 
