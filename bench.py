@@ -410,8 +410,8 @@ def work_counts_gemm(F, neq, c):
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel on the default
-# workload, from one ncu capture of it (profiles/k_evaluate_traffic_clustered1M.md)
-NCU_TRAFFIC_BYTES = {("mixed", "evaluate"): 43_461_560, ("fp64", "evaluate"): 53_386_240}
+# workload, from one ncu capture of it (profiles/traffic_clustered1M.md)
+NCU_TRAFFIC_BYTES = {("mixed", "evaluate"): 44_016_384, ("fp64", "evaluate"): 53_386_240}
 
 
 def roofline_of(res, precision, peaks, steps, default_workload):
