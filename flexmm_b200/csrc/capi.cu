@@ -807,11 +807,10 @@ int fmm_evaluate_multi(fmm_plan *p, const double *tx, const double *ty, int64_t 
     DevBuf<double> txs, tys;
     {
       PhaseTimer timer(PH_SORT_TGT, s);
-      sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1);
       txs.alloc(m, s);
       tys.alloc(m, s);
-      gather_sorted(tx, tperm.get(), m, txs.get(), s);
-      gather_sorted(ty, tperm.get(), m, tys.get(), s);
+      sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
+                  tys.get());
     }
     run_evaluate_multi(a, p->tau_s.get(), p->th.n_points, p->n_rhs, p->loc.get(),
                        (int64_t)p->th.n_total() * p->ops->np, txs.get(), tys.get(), tkeys.get(),
@@ -938,11 +937,10 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
   {
     PhaseTimer timer(PH_SORT_TGT, s);
     // leaves live on levels <= L-1: their first L-1 digits decide everything
-    sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1);
     txs.alloc(m, s);
     tys.alloc(m, s);
-    gather_sorted(tx, tperm.get(), m, txs.get(), s);
-    gather_sorted(ty, tperm.get(), m, tys.get(), s);
+    sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
+                tys.get());
   }
   if (p->ops->method == METHOD_STOKES)
     run_stokes_evaluate(stokes_args(p, s), p->tau_s.get(), p->tau2_s.get(), p->loc.get(), txs.get(),

@@ -149,25 +149,56 @@ __device__ __forceinline__ uint64_t spread_bits(uint64_t v) {
 // of floor(q) (interleaved x, y); points within the margin (and NaN or
 // infinite ones) take the descent itself.  The margin covers both roundings
 // with a wide factor; the host sets it.
+__device__ __forceinline__ uint64_t point_key(double px, double py, double x0, double y0,
+                                               double w0, double scale, double margin) {
+  const double qmax = double(uint64_t(1) << MAXD);
+  const double qx = (px - x0) * scale, qy = (py - y0) * scale;
+  const bool clear = fabs(qx - rint(qx)) > margin && fabs(qy - rint(qy)) > margin;
+  if (!clear) return key_descent(px, py, x0, y0, w0);
+  const double fx = fmin(fmax(floor(qx), 0.0), qmax - 1.0);
+  const double fy = fmin(fmax(floor(qy), 0.0), qmax - 1.0);
+  return (spread_bits(uint64_t(fx)) << 1) | spread_bits(uint64_t(fy));
+}
+
 __global__ void k_point_keys(const double *__restrict__ x, const double *__restrict__ y,
                              int64_t n, double x0, double y0, double w0, double scale,
                              double margin, uint64_t *__restrict__ keys, int *__restrict__ idx) {
-  const double qmax = double(uint64_t(1) << MAXD);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double px = x[i], py = y[i];
-    const double qx = (px - x0) * scale, qy = (py - y0) * scale;
-    const bool clear = fabs(qx - rint(qx)) > margin && fabs(qy - rint(qy)) > margin;
-    uint64_t key;
-    if (clear) {
-      const double fx = fmin(fmax(floor(qx), 0.0), qmax - 1.0);
-      const double fy = fmin(fmax(floor(qy), 0.0), qmax - 1.0);
-      key = (spread_bits(uint64_t(fx)) << 1) | spread_bits(uint64_t(fy));
-    } else {
-      key = key_descent(px, py, x0, y0, w0);
-    }
-    keys[i] = key;
+    keys[i] = point_key(x[i], y[i], x0, y0, w0, scale, margin);
     idx[i] = int(i);
+  }
+}
+
+// The top KEY32_DIGITS digits of the key as a 32-bit sort key: a sort on at
+// most that many digits moves 8-byte pairs instead of 12-byte ones.
+constexpr int KEY32_DIGITS = 16;
+
+__global__ void k_point_keys32(const double *__restrict__ x, const double *__restrict__ y,
+                               int64_t n, double x0, double y0, double w0, double scale,
+                               double margin, uint32_t *__restrict__ keys, int *__restrict__ idx) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    keys[i] = uint32_t(point_key(x[i], y[i], x0, y0, w0, scale, margin) >> (2 * (MAXD - KEY32_DIGITS)));
+    idx[i] = int(i);
+  }
+}
+
+// sorted order: the full keys (recomputed from the points) and, if sx is
+// given, the coordinates
+__global__ void k_gather_keyed(const double *__restrict__ x, const double *__restrict__ y,
+                               const int *__restrict__ perm, int64_t n, double x0, double y0,
+                               double w0, double scale, double margin, double *__restrict__ sx,
+                               double *__restrict__ sy, uint64_t *__restrict__ keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int j = perm[i];
+    const double px = x[j], py = y[j];
+    if (sx) {
+      sx[i] = px;
+      sy[i] = py;
+    }
+    keys[i] = point_key(px, py, x0, y0, w0, scale, margin);
   }
 }
 
@@ -713,21 +744,44 @@ int cooperative_grid(const void *kernel, int threads) {
 }  // namespace
 
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
-                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s, int sorted_digits) {
-  DevBuf<uint64_t> k0;
-  DevBuf<int> i0;
-  k0.alloc(n, s);
-  i0.alloc(n, s);
+                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s, int sorted_digits,
+                 double *sx, double *sy) {
   keys.alloc(n, s);
   perm.alloc(n, s);
   if (n == 0) return;
   double scale, margin;
   key_params(th.x0, th.y0, th.w0, scale, margin);
+  const int digits = sorted_digits < 1 ? 1 : (sorted_digits > MAXD ? MAXD : sorted_digits);
+  if (digits <= KEY32_DIGITS) {
+    // 32-bit sort keys; the 64-bit keys follow in sorted order (a stable
+    // sort on the same top digits: the same permutation)
+    DevBuf<uint32_t> k0, k1;
+    DevBuf<int> i0;
+    k0.alloc(n, s);
+    k1.alloc(n, s);
+    i0.alloc(n, s);
+    k_point_keys32<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin,
+                                                     k0.get(), i0.get());
+    FMMB_CUDA(cudaGetLastError());
+    radix_sort_pairs(k0.get(), k1.get(), i0.get(), perm.get(), n, 2 * (KEY32_DIGITS - digits),
+                     2 * KEY32_DIGITS, s);
+    k_gather_keyed<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, perm.get(), n, th.x0, th.y0, th.w0, scale,
+                                                     margin, sx, sy, keys.get());
+    FMMB_CUDA(cudaGetLastError());
+    return;
+  }
+  DevBuf<uint64_t> k0;
+  DevBuf<int> i0;
+  k0.alloc(n, s);
+  i0.alloc(n, s);
   k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin,
                                                  k0.get(), i0.get());
   FMMB_CUDA(cudaGetLastError());
-  const int digits = sorted_digits < 1 ? 1 : (sorted_digits > MAXD ? MAXD : sorted_digits);
   radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * (MAXD - digits), 2 * MAXD, s);
+  if (sx) {
+    k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, perm.get(), n, sx, sy);
+    FMMB_CUDA(cudaGetLastError());
+  }
 }
 
 size_t sort_points_scratch_bytes(int64_t n) {
@@ -781,8 +835,10 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   spos.alloc(n, s);
   // 1-3: keys, sort (top digits first), initial splits in point order
   std::unique_ptr<PhaseTimer> t_split(new PhaseTimer(PH_TREE_SPLITS, s));
+  td.sx.alloc(n, s);
+  td.sy.alloc(n, s);
   for (int digits = SORT_DIGITS;; digits = MAXD) {
-    sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits);
+    sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits, td.sx.get(), td.sy.get());
     cnt.zero(s);
     k_split_counts<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, scount.get(),
                                                      cnt.get());
@@ -790,11 +846,6 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     exclusive_sum(scount.get(), spos.get(), n, s);
     k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
                                                    s0raw.get(), cap0, cnt.get());
-    FMMB_CUDA(cudaGetLastError());
-    // the sorted coordinates need no count: queued before the host waits
-    td.sx.alloc(n, s);
-    td.sy.alloc(n, s);
-    k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, td.ordv.get(), n, td.sx.get(), td.sy.get());
     FMMB_CUDA(cudaGetLastError());
     FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));

@@ -69,10 +69,11 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
 
 // Sort arbitrary points by the same descent key on its top `sorted_digits`
 // quadrant digits (enough to place them in boxes of levels <= sorted_digits);
-// returns the keys in that order and the permutation sorted -> original.
+// returns the keys in that order and the permutation sorted -> original,
+// and (if sx, sy are given) the coordinates in that order.
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
                  DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t stream,
-                 int sorted_digits = MAXD);
+                 int sorted_digits = MAXD, double *sx = nullptr, double *sy = nullptr);
 
 // The same keys and sort into caller-provided memory: k0/k1 and i0/i1 are
 // ping-pong buffers of n entries, temp holds sort_points_scratch_bytes(n)
