@@ -589,6 +589,11 @@ int fmm_ops_destroy(fmm_ops *ops) {
   });
 }
 
+// the tree's host-side level offsets: build_tree returns before they arrive
+static void tree_ready(fmm_plan *p) {
+  if (p) finalize_tree(p->th);
+}
+
 int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
                     const double *bbox, void *stream, fmm_plan **out) {
   return guarded([&] {
@@ -609,6 +614,7 @@ int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, i
 int fmm_plan_info(fmm_plan *p, int *n_levels, double *widths, int *n_nodes) {
   return guarded([&] {
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    if (n_nodes) tree_ready(p);  // level counts need the finished tree; L and widths do not
     if (n_levels) *n_levels = p->th.L;
     for (int m = 0; m < p->th.L; ++m) {
       if (widths) widths[m] = p->th.width[m];
@@ -731,6 +737,7 @@ static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
 
 int fmm_build_expansions2(fmm_plan *p, const double *fx, const double *fy, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p && fx && fy, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(p->ops->method == METHOD_STOKES, ERR_INVALID_ARGUMENT,
                "fmm_build_expansions2 takes Stokes plans (two force components)");
@@ -758,6 +765,7 @@ int fmm_build_expansions2(fmm_plan *p, const double *fx, const double *fy, void 
 int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_t ld_tau,
                                void *stream) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->precision == PREC_FP64, ERR_UNSUPPORTED,
                "several charge columns: FP64 KIFMM plans");
@@ -792,6 +800,7 @@ int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_
 int fmm_evaluate_multi(fmm_plan *p, const double *tx, const double *ty, int64_t m, int check,
                        double *out, int64_t ld_out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
     FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->precision == PREC_FP64, ERR_UNSUPPORTED,
@@ -820,6 +829,7 @@ int fmm_evaluate_multi(fmm_plan *p, const double *tx, const double *ty, int64_t 
 
 int fmm_evaluate_sources_multi(fmm_plan *p, int check, double *out, int64_t ld_out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
     FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->precision == PREC_FP64, ERR_UNSUPPORTED,
@@ -837,6 +847,7 @@ int fmm_evaluate_sources_multi(fmm_plan *p, int check, double *out, int64_t ld_o
 
 int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(p->ops->method != METHOD_STOKES, ERR_INVALID_ARGUMENT,
                "Stokes plans take fmm_build_expansions2 (two force components)");
@@ -987,6 +998,7 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
 int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int check,
                  double *out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     check_evaluator(p, FMM_EVAL_POTENTIAL);
     evaluate_points(p, 1, tx, ty, m, check, out, m, (cudaStream_t)stream);
   });
@@ -994,6 +1006,7 @@ int fmm_evaluate(fmm_plan *p, const double *tx, const double *ty, int64_t m, int
 
 int fmm_evaluate_sources(fmm_plan *p, int check, double *out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     check_evaluator(p, FMM_EVAL_POTENTIAL);
     evaluate_own_sources(p, 1, check, out, 0, (cudaStream_t)stream);
   });
@@ -1002,6 +1015,7 @@ int fmm_evaluate_sources(fmm_plan *p, int check, double *out, void *stream) {
 int fmm_evaluate_outputs(fmm_plan *p, int evaluator, const double *tx, const double *ty,
                          int64_t m, int check, double *out, int64_t ld_out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     const int nout = evaluator_outputs(evaluator);
     check_evaluator(p, evaluator);
     evaluate_points(p, nout, tx, ty, m, check, out, ld_out, (cudaStream_t)stream);
@@ -1011,6 +1025,7 @@ int fmm_evaluate_outputs(fmm_plan *p, int evaluator, const double *tx, const dou
 int fmm_evaluate_sources_outputs(fmm_plan *p, int evaluator, int check, double *out,
                                  int64_t ld_out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     const int nout = evaluator_outputs(evaluator);
     check_evaluator(p, evaluator);
     evaluate_own_sources(p, nout, check, out, ld_out, (cudaStream_t)stream);
@@ -1019,6 +1034,7 @@ int fmm_evaluate_sources_outputs(fmm_plan *p, int evaluator, int check, double *
 
 int fmm_plan_status(fmm_plan *p) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CUDA(cudaStreamSynchronize(p->stream));
     FMMB_CUDA(cudaGetLastError());
@@ -1040,6 +1056,7 @@ int fmm_plan_destroy(fmm_plan *p) {
 int fmm_tree_export(fmm_plan *p, double *xmin, double *ymin, int *bot, int *top, int *parent,
                     int *child, uint8_t *flags, int *coll, int *il, int *ordv) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     const size_t T = p->th.n_total();
     cudaStream_t s = p->stream;
@@ -1147,6 +1164,7 @@ size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double *ty, int64_t m,
                                     int check, double *out, void *stream) {
   return guarded([&] {
+    tree_ready(p);
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CHECK(p->have_expansions, ERR_NOT_READY, "build_expansions has not run");
     FMMB_CHECK(p->precision == PREC_FP64, ERR_UNSUPPORTED,

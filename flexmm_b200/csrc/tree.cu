@@ -29,6 +29,7 @@
 #include <cmath>
 
 #include <memory>
+#include <mutex>
 
 #include "timing.cuh"
 #include "tree.cuh"
@@ -484,10 +485,21 @@ __device__ __forceinline__ int level_of(const int *__restrict__ off, int L, int 
 }
 
 // --- 6. node arrays -----------------------------------------------------------
-__global__ void k_node_codes(const int *__restrict__ off, int L, int total,
+// level offsets from the per-level parent-box bounds (one thread)
+__global__ void k_level_offsets(const int *__restrict__ pb, int L, int *__restrict__ off) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  off[0] = 0;
+  if (L >= 1) off[1] = 1;
+  for (int m = 1; m < L; ++m) off[m + 1] = off[m] + 4 * (pb[m] - pb[m - 1]);
+}
+
+// The node kernels are launched for an upper bound of the node count (the
+// host does not wait for it); the count itself is off[L] in device memory.
+__global__ void k_node_codes(const int *__restrict__ off, int L, int total_ub,
                              const uint64_t *__restrict__ pkeys, const uint8_t *__restrict__ pisx,
                              const int *__restrict__ pb, uint64_t *__restrict__ code,
                              uint8_t *__restrict__ flags) {
+  const int total = min(off[L], total_ub);
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     const int m = level_of(off, L, g);
     if (m == 0) {
@@ -509,7 +521,7 @@ __global__ void k_node_codes(const int *__restrict__ off, int L, int total,
 // as the longest search (~20 loads for 1M points), not the sum of all.
 constexpr int NA_SEARCH = 12;
 
-__global__ void k_node_attrs(const int *__restrict__ off, int L, int total, double x0, double y0,
+__global__ void k_node_attrs(const int *__restrict__ off, int L, int total_ub, double x0, double y0,
                              double w0, const uint64_t *__restrict__ pts, int64_t npts,
                              const uint64_t *__restrict__ pkeys, const uint8_t *__restrict__ pisx,
                              const int *__restrict__ pb, const uint64_t *__restrict__ code,
@@ -519,6 +531,7 @@ __global__ void k_node_attrs(const int *__restrict__ off, int L, int total, doub
                              int *__restrict__ top, int *__restrict__ parent,
                              int *__restrict__ child, int *__restrict__ coll,
                              int *__restrict__ nix, int *__restrict__ niy) {
+  const int total = min(off[L], total_ub);
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     const int m = level_of(off, L, g);
     const uint64_t c = code[g];
@@ -634,7 +647,7 @@ __constant__ int8_t c_cell_to_offset[49] = {
 // the parent's colleagues (parent excluded) that are not adjacent
 // (build_interaction_list, flexmm/tree.py:399-435), keeping only sources
 // that hold points
-__global__ void k_interactions(const int *__restrict__ off, int L, int total,
+__global__ void k_interactions(const int *__restrict__ off, int L, int total_ub,
                                const uint8_t *__restrict__ flags, const int *__restrict__ parent,
                                const int *__restrict__ child, const int *__restrict__ coll,
                                const int *__restrict__ ix, const int *__restrict__ iy,
@@ -642,6 +655,7 @@ __global__ void k_interactions(const int *__restrict__ off, int L, int total,
                                int *__restrict__ il) {
   // 8 lanes per node: lane j takes the parent's colleague j (and 8), with
   // its four children
+  const int total = min(off[L], total_ub);
   const int sub = threadIdx.x & 7;
   const unsigned gmask = 0xffu << (threadIdx.x & 24);
   const int64_t stride = (int64_t)gridDim.x * blockDim.x / 8;
@@ -672,18 +686,26 @@ __global__ void k_interactions(const int *__restrict__ off, int L, int total,
 }
 
 // S2M nodes: see TreeDev::uplist
-__global__ void k_up_flags(int g0, int total, const uint8_t *__restrict__ flags,
-                           const int *__restrict__ bot, const int *__restrict__ top,
-                           int *__restrict__ f) {
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+__global__ void k_up_flags(const int *__restrict__ off, int L, int total_ub,
+                           const uint8_t *__restrict__ flags, const int *__restrict__ bot,
+                           const int *__restrict__ top, int *__restrict__ f) {
+  const int total = min(off[L], total_ub);
+  const int g0 = L > 2 ? off[2] : total;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total_ub; g += gridDim.x * blockDim.x) {
+    if (g >= total) {
+      f[g] = 0;
+      continue;
+    }
     const uint8_t fl = flags[g];
     const bool up = (((fl & NF_LEAF) && !(fl & NF_XLIST)) || (fl & NF_FAKE)) && top[g] > bot[g];
     f[g] = (g >= g0 && up) ? 1 : 0;
   }
 }
 
-__global__ void k_up_scatter(int total, const int *__restrict__ f, const int *__restrict__ pos,
+__global__ void k_up_scatter(const int *__restrict__ off, int L, int total_ub,
+                             const int *__restrict__ f, const int *__restrict__ pos,
                              int *__restrict__ list, int *__restrict__ count) {
+  const int total = min(off[L], total_ub);
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     if (f[g]) list[pos[g]] = g;
     if (g == total - 1) *count = pos[g] + f[g];
@@ -742,6 +764,75 @@ int cooperative_grid(const void *kernel, int threads) {
 }
 
 }  // namespace
+
+// Small pinned host blocks for the per-level counts, kept for reuse: pinned
+// allocation is slow, and a plan is built per step in many loops.
+namespace {
+constexpr int PINNED_INTS = 64;  // >= 2 (MAXD + 2)
+std::mutex g_pinned_mu;
+std::vector<int *> g_pinned_free;
+
+int *pinned_acquire() {
+  {
+    std::lock_guard<std::mutex> g(g_pinned_mu);
+    if (!g_pinned_free.empty()) {
+      int *p = g_pinned_free.back();
+      g_pinned_free.pop_back();
+      return p;
+    }
+  }
+  // pinned allocation can take milliseconds: 16 blocks at a time (never freed)
+  constexpr int CHUNK = 16;
+  int *p = nullptr;
+  FMMB_CUDA(cudaHostAlloc((void **)&p, CHUNK * PINNED_INTS * sizeof(int), cudaHostAllocDefault));
+  std::lock_guard<std::mutex> g(g_pinned_mu);
+  for (int i = 1; i < CHUNK; ++i) g_pinned_free.push_back(p + i * PINNED_INTS);
+  return p;
+}
+
+void pinned_release(int *p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> g(g_pinned_mu);
+  g_pinned_free.push_back(p);
+}
+
+void begin_pending_counts(TreeHost &th, const int *dev_counts, int count, cudaStream_t s) {
+  FMMB_CHECK(count <= PINNED_INTS, ERR_INVALID_ARGUMENT, "too many levels");
+  if (!th.pending_counts) th.pending_counts = pinned_acquire();
+  if (!th.ready) FMMB_CUDA(cudaEventCreateWithFlags(&th.ready, cudaEventDisableTiming));
+  FMMB_CUDA(cudaMemcpyAsync(th.pending_counts, dev_counts, count * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+  FMMB_CUDA(cudaEventRecord(th.ready, s));
+  th.pending = true;
+  th.off.clear();
+  th.rg_lo.clear();
+  th.rg_hi.clear();
+}
+}  // namespace
+
+void finalize_tree(TreeHost &th) {
+  if (!th.pending) return;
+  FMMB_CUDA(cudaEventSynchronize(th.ready));
+  const int L = th.L;
+  const int *hpb = th.pending_counts;  // [0, L]: parent-box bounds; [L+1, 2L+1]: real groups
+  th.off.assign(L + 1, 0);
+  if (L >= 1) th.off[1] = 1;
+  for (int m = 1; m < L; ++m) th.off[m + 1] = th.off[m] + 4 * (hpb[m] - hpb[m - 1]);
+  th.rg_lo.assign(L + 1, 0);
+  th.rg_hi.assign(L + 1, 0);
+  for (int m = 1; m < L; ++m) {
+    th.rg_lo[m] = hpb[L + 1 + m - 1];
+    th.rg_hi[m] = hpb[L + 1 + m];
+  }
+  th.pending = false;
+}
+
+TreeHost::~TreeHost() {
+  // a copy still in flight writes into the pinned block: let it land first
+  if (pending && ready) cudaEventSynchronize(ready);
+  if (ready) cudaEventDestroy(ready);
+  pinned_release(pending_counts);
+}
 
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
                  DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s, int sorted_digits,
@@ -865,7 +956,6 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   DevBuf<uint64_t> pk, pkc, pks;  // parent boxes: compact keys (unsorted, sorted), codes
   DevBuf<uint8_t> pxs;
   DevBuf<int> pb, preal, ppos;
-  std::vector<int> hpb(L + 1, 0);
   int64_t np = 0;
   if (n0 > 0) {
     // split boxes by (level, morton): a stable sort on the level bits keeps
@@ -939,89 +1029,78 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     exclusive_sum(preal.get(), ppos.get(), np, s);
     k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1);
     FMMB_CUDA(cudaGetLastError());
-    hpb.resize(2 * (L + 1));
-    FMMB_CUDA(cudaMemcpyAsync(hpb.data(), pb.get(), 2 * (L + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMMB_CUDA(cudaStreamSynchronize(s));
   } else {
     pb.alloc(2 * (L + 1), s);
     pb.zero(s);
     pks.alloc(1, s);
     pxs.alloc(1, s);
-    hpb.assign(2 * (L + 1), 0);
   }
 
   t_bal.reset();
   PhaseTimer t_nodes(PH_TREE_NODES, s);
-  th.off.assign(L + 1, 0);
   th.width.assign(L, 0.0);
-  th.off[0] = 0;
-  th.off[1] = 1;
-  for (int m = 1; m < L; ++m) th.off[m + 1] = th.off[m] + 4 * (hpb[m] - hpb[m - 1]);
   double w = th.w0;
   for (int m = 0; m < L; ++m) {
     th.width[m] = w;
     w = 0.5 * w;
   }
-  const int total = th.off[L];
+  // level offsets on the device; their host copy (with the real-group
+  // bounds) travels back without a wait (finalize_tree)
   td.dev_off.alloc(L + 1, s);
-  FMMB_CUDA(cudaMemcpyAsync(td.dev_off.get(), th.off.data(), (L + 1) * sizeof(int),
-                            cudaMemcpyHostToDevice, s));
-  // real groups of level m (children of split boxes of level m-1): rg[rg_lo[m], rg_hi[m])
-  th.rg_lo.assign(L + 1, 0);
-  th.rg_hi.assign(L + 1, 0);
-  for (int m = 1; m < L; ++m) {
-    th.rg_lo[m] = hpb[L + 1 + m - 1];
-    th.rg_hi[m] = hpb[L + 1 + m];
-  }
-  const int n_real_groups = hpb[L + 1 + L];
-  td.rg.alloc(n_real_groups > 0 ? n_real_groups : 1, s);
-  if (np > 0 && n_real_groups > 0) {
+  k_level_offsets<<<1, 1, 0, s>>>(pb.get(), L, td.dev_off.get());
+  FMMB_CUDA(cudaGetLastError());
+  begin_pending_counts(th, pb.get(), 2 * (L + 1), s);
+  // every parent box has 4 children: at most 1 + 4 np nodes, np real groups
+  const int total_ub = 1 + 4 * int(np);
+  td.rg.alloc(np > 0 ? np : 1, s);
+  if (np > 0) {
     k_real_groups<<<grid_for(np, TPB), TPB, 0, s>>>(pks.get(), preal.get(), ppos.get(), np, pb.get(),
                                                      td.dev_off.get(), td.rg.get());
     FMMB_CUDA(cudaGetLastError());
   }
-  td.code.alloc(total, s);
-  td.flags.alloc(total, s);
-  td.xmin.alloc(total, s);
-  td.ymin.alloc(total, s);
-  td.xmid.alloc(total, s);
-  td.ymid.alloc(total, s);
-  td.bot.alloc(total, s);
-  td.top.alloc(total, s);
-  td.parent.alloc(total, s);
-  td.child.alloc(total, s);
-  td.coll.alloc(int64_t(total) * 9, s);
-  td.il.alloc(int64_t(total) * N_OFFSETS, s);
-  td.ix.alloc(total, s);
-  td.iy.alloc(total, s);
-  k_node_codes<<<grid_for(total, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total, pks.get(),
-                                                      pxs.get(), pb.get(), td.code.get(),
-                                                      td.flags.get());
+  td.code.alloc(total_ub, s);
+  td.flags.alloc(total_ub, s);
+  td.xmin.alloc(total_ub, s);
+  td.ymin.alloc(total_ub, s);
+  td.xmid.alloc(total_ub, s);
+  td.ymid.alloc(total_ub, s);
+  td.bot.alloc(total_ub, s);
+  td.top.alloc(total_ub, s);
+  td.parent.alloc(total_ub, s);
+  td.child.alloc(total_ub, s);
+  td.coll.alloc(int64_t(total_ub) * 9, s);
+  td.il.alloc(int64_t(total_ub) * N_OFFSETS, s);
+  td.ix.alloc(total_ub, s);
+  td.iy.alloc(total_ub, s);
+  k_node_codes<<<grid_for(total_ub, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total_ub, pks.get(),
+                                                         pxs.get(), pb.get(), td.code.get(),
+                                                         td.flags.get());
   FMMB_CUDA(cudaGetLastError());
-  k_node_attrs<<<grid_for(total, TPB), TPB, 0, s>>>(
-      td.dev_off.get(), L, total, th.x0, th.y0, th.w0, td.pkeys.get(), n, pks.get(), pxs.get(),
+  k_node_attrs<<<grid_for(total_ub, TPB), TPB, 0, s>>>(
+      td.dev_off.get(), L, total_ub, th.x0, th.y0, th.w0, td.pkeys.get(), n, pks.get(), pxs.get(),
       pb.get(), td.code.get(), td.flags.get(), td.xmin.get(), td.ymin.get(), td.xmid.get(),
       td.ymid.get(), td.bot.get(), td.top.get(), td.parent.get(), td.child.get(), td.coll.get(),
       td.ix.get(), td.iy.get());
   FMMB_CUDA(cudaGetLastError());
-  k_interactions<<<grid_for(int64_t(total) * 8, TPB), TPB, 0, s>>>(
-      td.dev_off.get(), L, total, td.flags.get(), td.parent.get(), td.child.get(), td.coll.get(),
+  k_interactions<<<grid_for(int64_t(total_ub) * 8, TPB), TPB, 0, s>>>(
+      td.dev_off.get(), L, total_ub, td.flags.get(), td.parent.get(), td.child.get(), td.coll.get(),
       td.ix.get(), td.iy.get(), td.bot.get(), td.top.get(), td.il.get());
   FMMB_CUDA(cudaGetLastError());
   // S2M node list
   {
     DevBuf<int> f, pos;
-    f.alloc(total, s);
-    pos.alloc(total, s);
-    td.uplist.alloc(total, s);
+    f.alloc(total_ub, s);
+    pos.alloc(total_ub, s);
+    td.uplist.alloc(total_ub, s);
     td.n_up.alloc(1, s);
-    const int g0 = L > 2 ? th.off[2] : total;
-    k_up_flags<<<grid_for(total, TPB), TPB, 0, s>>>(g0, total, td.flags.get(), td.bot.get(),
-                                                     td.top.get(), f.get());
+    k_up_flags<<<grid_for(total_ub, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total_ub,
+                                                         td.flags.get(), td.bot.get(), td.top.get(),
+                                                         f.get());
     FMMB_CUDA(cudaGetLastError());
-    exclusive_sum(f.get(), pos.get(), total, s);
-    k_up_scatter<<<grid_for(total, TPB), TPB, 0, s>>>(total, f.get(), pos.get(), td.uplist.get(),
-                                                       td.n_up.get());
+    exclusive_sum(f.get(), pos.get(), total_ub, s);
+    k_up_scatter<<<grid_for(total_ub, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total_ub, f.get(),
+                                                           pos.get(), td.uplist.get(),
+                                                           td.n_up.get());
     FMMB_CUDA(cudaGetLastError());
   }
 }

@@ -57,11 +57,26 @@ struct TreeHost {
   int64_t n_points = 0;
   int ppl = 0;
   double x0 = 0, y0 = 0, w0 = 0;
-  std::vector<int> off;       // L+1
+  std::vector<int> off;       // L+1 (after finalize_tree)
   std::vector<double> width;  // per level
-  std::vector<int> rg_lo, rg_hi;  // per level: range of its real groups in rg
+  std::vector<int> rg_lo, rg_hi;  // per level: range of its real groups in rg (after finalize_tree)
   int n_total() const { return off.empty() ? 0 : off.back(); }
+  // build_tree returns before the per-level counts reach the host: they
+  // come back by an asynchronous copy into pinned memory, `ready` marks its
+  // completion, and finalize_tree() fills off / rg_lo / rg_hi from them.
+  bool pending = false;
+  int *pending_counts = nullptr;  // pinned, 2 (L+1) ints
+  cudaEvent_t ready = nullptr;
+  TreeHost() = default;
+  TreeHost(const TreeHost &) = delete;
+  TreeHost &operator=(const TreeHost &) = delete;
+  ~TreeHost();
 };
+
+// Wait for the per-level counts of the last build_tree and fill the host
+// offsets (a no-op once done).  Every use of off, rg_lo, rg_hi or n_total()
+// after build_tree comes after this.
+void finalize_tree(TreeHost &th);
 
 // Build the tree over device coordinates x, y (n points) on `stream`.
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,

@@ -186,11 +186,11 @@ class KI_FMM:
                         if isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor) else None)
         nl = ctypes.c_int()
         widths = (ctypes.c_double * _lib.MAX_LEVELS)()
-        counts = (ctypes.c_int * _lib.MAX_LEVELS)()
-        _lib.call("fmm_plan_info", plan, ctypes.byref(nl), widths, counts)
+        # level count and widths only: the per-level node counts would wait for
+        # the GPU (the tree's last kernels still run while the plan is set up)
+        _lib.call("fmm_plan_info", plan, ctypes.byref(nl), widths, None)
         self._levels = nl.value
         self._widths = [widths[i] for i in range(nl.value)]
-        self._counts = [counts[i] for i in range(nl.value)]
         if verbose:
             print("....Tree formed in:             {:0.1f}".format((time.time() - st) * 1000))
         # operators for every level width (KI_Helper.prepare, flexmm/flexmm2d/kifmm.py:67-82)
@@ -200,6 +200,13 @@ class KI_FMM:
         self._expanded = False
         # named evaluators (kifmm2d FMM.__init__ registers 'potential_evaluation')
         self._evaluators = {"potential_evaluation": "potential"}
+
+    @property
+    def _counts(self):
+        """Nodes per level (waits for the tree's construction to finish)."""
+        counts = (ctypes.c_int * _lib.MAX_LEVELS)()
+        _lib.call("fmm_plan_info", self._plan, None, None, counts)
+        return [counts[i] for i in range(self._levels)]
 
     @property
     def tree(self):
