@@ -133,6 +133,17 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def wait_for_sample(self, timeout=1.0):
+        """Return just after the next sample lands: a timed loop of a few tens of
+        ms then runs between two nvidia-smi queries (a query can stall the
+        GPU for milliseconds)."""
+        if self.proc is None:
+            return
+        n0 = len(self.rows)
+        t_end = time.time() + timeout
+        while len(self.rows) == n0 and time.time() < t_end:
+            time.sleep(0.001)
+
     def __exit__(self, *exc):
         if self.proc is not None:
             time.sleep(0.25)
@@ -318,6 +329,7 @@ def measure(args, world, local, d, precision, flush, counts_cache):
     clk = ClockSampler(local).__enter__()
     step(xd, yd, taud, txd, tyd)  # one untimed step with the sampler running
     torch.cuda.synchronize()
+    clk.wait_for_sample()
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -353,6 +365,7 @@ def measure(args, world, local, d, precision, flush, counts_cache):
     gc.collect()
     gc.disable()  # a collector pause inside one timed step is host noise, not the library
     barrier(world)
+    clk.wait_for_sample()
     for _ in range(args.steps):
         flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)

@@ -387,29 +387,42 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 }
 
 // ---------------------------------------------------- M2L on tcgen05 ----
-// 128 targets of one parity class per CTA (MMA M = 128), one thread per
-// target.  Per offset, the gathered source multipoles (A: 128 x K, read
-// pre-split as TF32 hi / lo from the upward pass's mult_tc rows) and the
-// deflated operator (B: N x K, N = NP rounded up to 16) are copied into shared
-// memory with cp.async in the K-major core-matrix layout (8 rows x 16 bytes
-// per core matrix, core matrices along K contiguous: LBO = 128 B, SBO =
-// NP/4 * 128 B) through a 3-stage pipeline, and multiplied by tcgen05.mma
-// kind::tf32 into tensor memory.  Each k-step's three split products (lo.hi,
-// hi.lo, hi.hi) go to their own 32 TMEM columns (the tensor cores truncate
-// their FP32 accumulation); the epilogue adds the k-step slots in FP32 (round
-// to nearest) and the result into FP64 registers.  Two TMEM buffers: the MMAs
-// of one offset run while the threads read the previous offset's results and
-// copy operands two offsets ahead.
-constexpr int TCM = 128;       // targets per CTA = MMA M
+// Tiles of 128 targets of one parity class (MMA M = 128).  Per offset, the
+// gathered source multipoles (A: 128 x K, read pre-split as TF32 hi / lo
+// from the upward pass's mult_tc rows) and the deflated operator (B: N x K,
+// N = NP rounded up to 16) sit in shared memory in the K-major core-matrix
+// layout (8 rows x 16 bytes per core matrix, core matrices along K
+// contiguous: LBO = 128 B, SBO = NP/4 * 128 B) and are multiplied by
+// tcgen05.mma kind::tf32 into tensor memory.  Each k-step's three split
+// products (lo.hi, hi.lo, hi.hi) go to their own 32 TMEM columns (the tensor
+// cores truncate their FP32 accumulation); the k-step slots are added in
+// FP32 (round to nearest) and the result into FP64 registers.
+//
+// Persistent and warp specialised, one CTA per SM walking its tiles:
+//   warps 0-3  epilogue: one target row per thread (TMEM lanes 0-127)
+//   warps 4-7  producers: cp.async of the operands into a 3-stage ring
+//   warp 8     lane 0 issues the MMAs
+// and they hand over through mbarriers instead of CTA barriers:
+//   full[s]   stage s loaded        (128 producer arrivals)
+//   sfree[s]  MMAs reading s done   (tcgen05.commit)
+//   mdone[b]  TMEM buffer b written (tcgen05.commit)
+//   tfree[b]  TMEM buffer b read    (128 epilogue arrivals)
+// Use u of the pipeline (a running count of offsets over the CTA's tiles)
+// takes stage u % 3 and buffer u % 2; each barrier's k-th completion has
+// parity k & 1.  Every wait is bounded: one that runs out sets the plan's
+// error flag and the CTA stops, after letting its copies and MMAs land.
+constexpr int TCM = 128;       // targets per tile = MMA M
 constexpr int TC_MAX_NP = 32;  // up to 4 k-steps x 32 TMEM columns per buffer
 constexpr int TC_COLS = 256;   // TMEM columns per CTA (2 buffers x 128)
 constexpr int TC_STAGES = 3;   // operand stages in shared memory
+constexpr int TC_EPI = 128, TC_PROD = 128;
+constexpr int TC_THREADS = TC_EPI + TC_PROD + 32;
 constexpr uint32_t TC_MAX_TRIES = 1u << 20;
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// shared memory of k_m2l_tc: TC_STAGES x (A hi, A lo, B hi, B lo)
+// shared memory of one operand stage: A hi, A lo, B hi, B lo
 size_t m2l_tc_stage_bytes(int np) {
   const size_t ntc = (np + 15) & ~15;
   const size_t a_sz = (size_t(TCM) * np * 4 + 1023) & ~size_t(1023);
@@ -417,39 +430,42 @@ size_t m2l_tc_stage_bytes(int np) {
   return 2 * a_sz + 2 * b_sz;
 }
 
-__global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, int np,
-                                                   const int *__restrict__ rg,
-                                                   const int *__restrict__ il,
-                                                   const LevelOpsDev *__restrict__ ops,
-                                                   const float *__restrict__ mult_tc,
-                                                   const double *__restrict__ msum,
-                                                   double *__restrict__ ple, int *err) {
+__global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int n_tiles, int neq,
+                                                         int np, const int *__restrict__ rg,
+                                                         const int *__restrict__ il,
+                                                         const LevelOpsDev *__restrict__ ops,
+                                                         const float *__restrict__ mult_tc,
+                                                         const double *__restrict__ msum,
+                                                         double *__restrict__ ple, int *err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_sfree[TC_STAGES];
+  __shared__ __align__(8) uint64_t bar_mdone[2], bar_tfree[2], bar_drain;
   __shared__ uint32_t tmem_base;
-  __shared__ int s_src[27][TCM];  // source node per class offset and target
+  __shared__ int s_src[27][TCM];  // source node per class offset and target row
   __shared__ int s_act[27];       // offsets with work, in class order
   __shared__ int s_nact;
   __shared__ unsigned int s_mask;
+  __shared__ volatile int s_abort;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int ntc = (np + 15) & ~15;
   const int nks = np / 8, nk4 = np / 4;
   const uint32_t a_sz = (uint32_t(TCM) * np * 4 + 1023u) & ~1023u;
   const uint32_t b_sz = (uint32_t(ntc) * np * 4 + 1023u) & ~1023u;
-  const uint32_t st_sz = 2 * a_sz + 2 * b_sz;  // one stage: A hi, A lo, B hi, B lo
-  const int warp = threadIdx.x >> 5;
-  int slot = 0;
-  while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= (int)blockIdx.x) ++slot;
-  const int m = slot >> 2, cls = slot & 3;
-  const int q0 = TCM * (blockIdx.x - tiles.tile_start[slot]);
-  const int nloc = min(TCM, tiles.rg_cnt[m] - q0);
-  const int tg = (int)threadIdx.x < nloc ? rg[tiles.rg_lo[m] + q0 + threadIdx.x] + cls : -1;
-  const LevelOpsDev &op = ops[m];
+  const uint32_t st_sz = 2 * a_sz + 2 * b_sz;
   if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_base), TC_COLS);
-  if (threadIdx.x == 0) {
-    tc::mbar_init(tc::smem_u32(&mbar[0]), 1);
-    tc::mbar_init(tc::smem_u32(&mbar[1]), 1);
+  if (tid == 0) {
+    for (int st = 0; st < TC_STAGES; ++st) {
+      tc::mbar_init(tc::smem_u32(&bar_full[st]), TC_PROD);
+      tc::mbar_init(tc::smem_u32(&bar_sfree[st]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(tc::smem_u32(&bar_mdone[b]), 1);
+      tc::mbar_init(tc::smem_u32(&bar_tfree[b]), TC_EPI);
+    }
+    tc::mbar_init(tc::smem_u32(&bar_drain), 1);
     tc::fence_mbar_init();
     s_mask = 0u;
+    s_abort = 0;
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -457,137 +473,165 @@ __global__ void __launch_bounds__(TCM, 1) k_m2l_tc(M2LTilesMx tiles, int neq, in
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = tc::idesc_tf32(TCM, ntc);
   const uint32_t lbo = 128, sbo = uint32_t(nk4) * 128;
-  // the class's offsets that have an operator and a source for some target
-  // of the tile, and every target's source per offset
-  {
-    unsigned int mask = 0;
-    for (int oi = 0; oi < 27; ++oi) {
-      const int o = c_class_off_mx[cls][oi];
-      const int sidx = (tg >= 0 && op.kind[o] != M2L_NULL) ? il[(size_t)tg * N_OFFSETS + o] : -1;
-      s_src[oi][threadIdx.x] = sidx;
-      if (sidx >= 0) mask |= 1u << oi;
-    }
-    mask = __reduce_or_sync(0xffffffffu, mask);
-    if ((threadIdx.x & 31) == 0) atomicOr(&s_mask, mask);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int n = 0;
-    for (int oi = 0; oi < 27; ++oi)
-      if ((s_mask >> oi) & 1u) s_act[n++] = oi;
-    s_nact = n;
-  }
-  __syncthreads();
-  const int nact = s_nact;
   const int units = ntc * nk4;  // 16-byte chunks of one B part
-  // start copying offset ai's operands into stage ai % TC_STAGES; returns the
-  // charge-sum term c_o * msum[src] of this thread's source
-  auto issue = [&](int ai) -> double {
-    const int oi = s_act[ai], o = c_class_off_mx[cls][oi];
-    const int src = s_src[oi][threadIdx.x];
-    unsigned char *st = smraw + (ai % TC_STAGES) * st_sz;
-    const int r = threadIdx.x;
-    unsigned char *ah = st, *al = st + a_sz;
-    if (src >= 0) {
-      const float *row = mult_tc + (size_t)src * 2 * np;
-      for (int k4 = 0; k4 < nk4; ++k4) {
-        const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
-        cp_async16(ah + off, row + 4 * k4);
-        cp_async16(al + off, row + np + 4 * k4);
-      }
-    } else {
-      for (int k4 = 0; k4 < nk4; ++k4) {
-        const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
-        *reinterpret_cast<float4 *>(ah + off) = make_float4(0.f, 0.f, 0.f, 0.f);
-        *reinterpret_cast<float4 *>(al + off) = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-    }
-    for (int u = threadIdx.x; u < 2 * units; u += TCM) {
-      const int part = u >= units, uu = part ? u - units : u;
-      const int n = uu / nk4, k4 = uu - (uu / nk4) * nk4;
-      const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
-      const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
-      cp_async16(st + 2 * a_sz + part * b_sz + off, bsrc + (size_t)n * np + 4 * k4);
-    }
-    return src >= 0 ? op.c_m2l[o] * __ldg(msum + src) : 0.0;
+  auto fail = [&] {
+    s_abort = 1;
+    atomicExch(err, 1);
   };
-  double acc[32];
-#pragma unroll
-  for (int c = 0; c < 32; ++c) acc[c] = 0.0;
-  double r1 = 0.0;
-  int issued = 0, waits0 = 0, waits1 = 0, my_abort = 0;
-  auto epilogue = [&](int b) {
-    const uint32_t parity = uint32_t(b ? waits1 : waits0) & 1u;
-    if (b) ++waits1; else ++waits0;
-    if (!tc::mbar_wait(tc::smem_u32(&mbar[b]), parity, TC_MAX_TRIES)) {
-      my_abort = 1;
-      atomicExch(err, 1);
+  uint32_t gu = 0;  // pipeline uses before the current tile
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    int slot = 0;
+    while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= tile) ++slot;
+    const int m = slot >> 2, cls = slot & 3;
+    const int q0 = TCM * (tile - tiles.tile_start[slot]);
+    const int nloc = min(TCM, tiles.rg_cnt[m] - q0);
+    const LevelOpsDev &op = ops[m];
+    int tg = -1;
+    if (tid < TC_EPI) {
+      // this tile's offsets that have an operator and a source for some
+      // target, and every target's source per offset
+      tg = tid < nloc ? rg[tiles.rg_lo[m] + q0 + tid] + cls : -1;
+      unsigned int mask = 0;
+      for (int oi = 0; oi < 27; ++oi) {
+        const int o = c_class_off_mx[cls][oi];
+        const int sidx = (tg >= 0 && op.kind[o] != M2L_NULL) ? il[(size_t)tg * N_OFFSETS + o] : -1;
+        s_src[oi][tid] = sidx;
+        if (sidx >= 0) mask |= 1u << oi;
+      }
+      mask = __reduce_or_sync(0xffffffffu, mask);
+      if ((tid & 31) == 0) atomicOr(&s_mask, mask);
     }
-    tc::fence_after_sync();
-    float sum[32];
-    for (int ks = 0; ks < nks; ++ks) {
-      float v[32];
-      tc::tmem_ld32(tmem + (uint32_t(32 * warp) << 16) + uint32_t(b * 128 + ks * 32), v);
-#pragma unroll
-      for (int c = 0; c < 32; ++c) sum[c] = ks == 0 ? v[c] : sum[c] + v[c];
+    __syncthreads();
+    if (tid == 0) {
+      int n = 0;
+      for (int oi = 0; oi < 27; ++oi)
+        if ((s_mask >> oi) & 1u) s_act[n++] = oi;
+      s_nact = n;
+      s_mask = 0u;
     }
+    __syncthreads();
+    const int nact = s_nact;
+    if (tid < TC_EPI) {
+      // ---- epilogue: TMEM -> FP32 slot sum -> FP64 ----
+      double acc[32];
 #pragma unroll
-    for (int c = 0; c < 32; ++c) acc[c] += (double)sum[c];
-    tc::fence_before_sync();
-  };
-  // prologue: offsets 0 and 1 in flight (one commit group each, possibly empty)
-  // charge-sum terms of the offsets in flight: pm0 (ai), pm1 (ai + 1)
-  double pm0 = 0.0, pm1 = 0.0;
-  if (nact > 0) pm0 = issue(0);
-  cp_async_commit();
-  if (nact > 1) pm1 = issue(1);
-  cp_async_commit();
-  static_assert(TC_STAGES == 3, "the prologue fills TC_STAGES - 1 = 2 stages");
-  for (int ai = 0; ai < nact; ++ai) {
-    const int buf = issued & 1;
-    // this thread's copies of offset ai done; everyone's after the barrier
-    cp_async_wait_1();
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    if (__syncthreads_or(my_abort)) break;
-    r1 += pm0;
-    if (threadIdx.x == 0) {
-      tc::fence_after_sync();
-      unsigned char *st = smraw + (ai % TC_STAGES) * st_sz;
-      for (int ks = 0; ks < nks; ++ks) {
-        const uint32_t d = tmem + uint32_t(buf * 128 + ks * 32);
+      for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+      double r1 = 0.0;
+      for (int a = 0; a < nact; ++a) {
+        if (__any_sync(0xffffffffu, s_abort)) break;
+        const uint32_t u = gu + a, b = u & 1u;
+        const bool ok = tc::mbar_wait(tc::smem_u32(&bar_mdone[b]), (u >> 1) & 1u, TC_MAX_TRIES);
+        if (!__all_sync(0xffffffffu, ok)) {
+          fail();
+          break;
+        }
+        tc::fence_after_sync();
+        float sum[32];
+        for (int ks = 0; ks < nks; ++ks) {
+          float v[32];
+          tc::tmem_ld32(tmem + (uint32_t(32 * warp) << 16) + b * 128u + uint32_t(ks * 32), v);
 #pragma unroll
-        for (int p = 0; p < 3; ++p) {  // lo.hi, hi.lo, hi.hi
-          const int apart = p == 0 ? 1 : 0, bpart = p == 1 ? 1 : 0;
-          const uint64_t ad = tc::desc_kmajor(tc::smem_u32(st + apart * a_sz) + ks * 256u, lbo, sbo);
-          const uint64_t bd = tc::desc_kmajor(tc::smem_u32(st + 2 * a_sz + bpart * b_sz) + ks * 256u, lbo, sbo);
-          tc::mma_tf32(d, ad, bd, idesc, p > 0 ? 1u : 0u);
+          for (int c = 0; c < 32; ++c) sum[c] = ks == 0 ? v[c] : sum[c] + v[c];
+        }
+        tc::fence_before_sync();
+        tc::mbar_arrive(tc::smem_u32(&bar_tfree[b]));
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] += (double)sum[c];
+        const int oi = s_act[a], src = s_src[oi][tid];
+        if (src >= 0) r1 += op.c_m2l[c_class_off_mx[cls][oi]] * __ldg(msum + src);
+      }
+      if (tg >= 0) {
+        double *o = ple + (size_t)tg * np;
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          if (c < np) o[c] = c < neq ? acc[c] + r1 : 0.0;
+      }
+    } else if (tid < TC_EPI + TC_PROD) {
+      // ---- producers: row r of A (hi, lo) and a share of B per offset ----
+      const int r = tid - TC_EPI;
+      int a = 0;
+      for (; a < nact; ++a) {
+        if (s_abort) break;
+        const uint32_t u = gu + a, st = u % TC_STAGES;
+        if (u >= TC_STAGES &&
+            !tc::mbar_wait(tc::smem_u32(&bar_sfree[st]), ((u / TC_STAGES) - 1) & 1u, TC_MAX_TRIES)) {
+          fail();
+          break;
+        }
+        const int oi = s_act[a], o = c_class_off_mx[cls][oi];
+        const int src = s_src[oi][r];
+        unsigned char *sp = smraw + st * st_sz;
+        unsigned char *ah = sp, *al = sp + a_sz;
+        for (int k4 = 0; k4 < nk4; ++k4) {
+          const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
+          if (src >= 0) {
+            const float *row = mult_tc + (size_t)src * 2 * np;
+            cp_async16(ah + off, row + 4 * k4);
+            cp_async16(al + off, row + np + 4 * k4);
+          } else {
+            *reinterpret_cast<float4 *>(ah + off) = make_float4(0.f, 0.f, 0.f, 0.f);
+            *reinterpret_cast<float4 *>(al + off) = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+        for (int q = r; q < 2 * units; q += TC_PROD) {
+          const int part = q >= units, qq = part ? q - units : q;
+          const int n = qq / nk4, k4 = qq - (qq / nk4) * nk4;
+          const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
+          const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
+          cp_async16(sp + 2 * a_sz + part * b_sz + off, bsrc + (size_t)n * np + 4 * k4);
+        }
+        cp_async_commit();
+        if (a >= 1) {  // the previous offset's copies have landed: announce them
+          cp_async_wait_1();
+          tc::fence_proxy_async();
+          tc::mbar_arrive(tc::smem_u32(&bar_full[(u - 1) % TC_STAGES]));
         }
       }
-      tc::commit(tc::smem_u32(&mbar[buf]));
-    }
-    if (issued >= 1) epilogue(buf ^ 1);  // MMAs of offset ai-1 done: its stage is free
-    ++issued;
-    const int nx = ai + TC_STAGES - 1;  // refill the stage of offset ai - 1
-    pm0 = pm1;
-    pm1 = nx < nact ? issue(nx) : 0.0;
-    cp_async_commit();
-  }
-  const int aborted = __syncthreads_or(my_abort);
-  if (issued >= 1 && !aborted) epilogue((issued - 1) & 1);
-  cp_async_wait_all();
-  if (aborted) {
-    // wait (bounded) for the commits still outstanding before TMEM is freed
-    for (; waits0 < (issued + 1) / 2; ++waits0)
-      tc::mbar_wait(tc::smem_u32(&mbar[0]), uint32_t(waits0) & 1u, TC_MAX_TRIES);
-    for (; waits1 < issued / 2; ++waits1)
-      tc::mbar_wait(tc::smem_u32(&mbar[1]), uint32_t(waits1) & 1u, TC_MAX_TRIES);
-  }
-  if (tg >= 0) {
-    double *o = ple + (size_t)tg * np;
+      cp_async_wait_all();
+      if (a == nact && nact >= 1) {
+        tc::fence_proxy_async();
+        tc::mbar_arrive(tc::smem_u32(&bar_full[(gu + nact - 1) % TC_STAGES]));
+      }
+    } else if (tid == TC_EPI + TC_PROD) {
+      // ---- MMA issue ----
+      for (int a = 0; a < nact; ++a) {
+        if (s_abort) break;
+        const uint32_t u = gu + a, st = u % TC_STAGES, b = u & 1u;
+        if (!tc::mbar_wait(tc::smem_u32(&bar_full[st]), (u / TC_STAGES) & 1u, TC_MAX_TRIES)) {
+          fail();
+          break;
+        }
+        if (u >= 2 &&
+            !tc::mbar_wait(tc::smem_u32(&bar_tfree[b]), ((u >> 1) - 1) & 1u, TC_MAX_TRIES)) {
+          fail();
+          break;
+        }
+        tc::fence_after_sync();
+        unsigned char *sp = smraw + st * st_sz;
+        for (int ks = 0; ks < nks; ++ks) {
+          const uint32_t d = tmem + b * 128u + uint32_t(ks * 32);
 #pragma unroll
-    for (int c = 0; c < 32; ++c)
-      if (c < np) o[c] = c < neq ? acc[c] + r1 : 0.0;
+          for (int p = 0; p < 3; ++p) {  // lo.hi, hi.lo, hi.hi
+            const int apart = p == 0 ? 1 : 0, bpart = p == 1 ? 1 : 0;
+            const uint64_t ad = tc::desc_kmajor(tc::smem_u32(sp + apart * a_sz) + ks * 256u, lbo, sbo);
+            const uint64_t bd =
+                tc::desc_kmajor(tc::smem_u32(sp + 2 * a_sz + bpart * b_sz) + ks * 256u, lbo, sbo);
+            tc::mma_tf32(d, ad, bd, idesc, p > 0 ? 1u : 0u);
+          }
+        }
+        tc::commit(tc::smem_u32(&bar_mdone[b]));
+        tc::commit(tc::smem_u32(&bar_sfree[st]));
+      }
+    }
+    gu += uint32_t(nact);
+    __syncthreads();
+    if (s_abort) break;
+  }
+  // every MMA issued has completed before the tensor memory is freed (the
+  // epilogue waited for each one; after a run-out this drains them)
+  if (tid == TC_EPI + TC_PROD) {
+    tc::commit(tc::smem_u32(&bar_drain));
+    tc::mbar_wait(tc::smem_u32(&bar_drain), 0u, TC_MAX_TRIES);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -1171,8 +1215,7 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc,
     return e && std::string(e) == "mma_sync";
   }();
   if (a.np <= TC_MAX_NP && !force_sync) {
-    // tensor-memory accumulators: 256 columns per CTA, so at most 2 CTAs per
-    // SM (512 columns); the shared-memory request enforces that
+    // tiles of 128 targets per (level, parity class)
     int ctiles = 0;
     M2LTilesMx tc{};
     tc.n_levels = th.L;
@@ -1185,12 +1228,17 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc,
       }
     }
     tc.tile_start[4 * th.L] = ctiles;
-    size_t sm = TC_STAGES * m2l_tc_stage_bytes(a.np);
-    if (sm < 80 * 1024) sm = 80 * 1024;
+    // persistent: one CTA per SM (its shared memory admits no second one),
+    // each walking tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+    const size_t sm = TC_STAGES * m2l_tc_stage_bytes(a.np);
     FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    int dev = 0, sms = 0;
+    FMMB_CUDA(cudaGetDevice(&dev));
+    FMMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PhaseTimer timer(PH_M2L, s);
-    k_m2l_tc<<<ctiles, TCM, sm, s>>>(tc, a.neq, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
-                                     mult_tc, msum, ple, err);
+    k_m2l_tc<<<std::min(ctiles, sms), TC_THREADS, sm, s>>>(tc, ctiles, a.neq, a.np, a.td->rg.get(),
+                                                           a.td->il.get(), a.ops_dev, mult_tc, msum,
+                                                           ple, err);
     FMMB_CUDA(cudaGetLastError());
     return;
   }
