@@ -329,6 +329,8 @@ def measure(args, world, local, d, precision, flush, counts_cache):
     clk = ClockSampler(local).__enter__()
     step(xd, yd, taud, txd, tyd)  # one untimed step with the sampler running
     torch.cuda.synchronize()
+    gc.collect()
+    gc.disable()  # a collector pause inside one timed step is host noise, not the library
     clk.wait_for_sample()
     for _ in range(args.steps):
         flush.fill_(1.0)
@@ -339,6 +341,7 @@ def measure(args, world, local, d, precision, flush, counts_cache):
         e1.record()
         times.append((e0, e1))
     torch.cuda.synchronize()
+    gc.enable()
     barrier(world)
     step_samples = [round(a.elapsed_time(b), 3) for a, b in times]
     ms_step = dist_max(sum(a.elapsed_time(b) for a, b in times) / max(args.steps, 1), world)

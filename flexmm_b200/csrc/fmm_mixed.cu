@@ -400,7 +400,8 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 //
 // Persistent and warp specialised, one CTA per SM walking its tiles:
 //   warps 0-3  epilogue: one target row per thread (TMEM lanes 0-127)
-//   warps 4-7  producers: cp.async of the operands into a 3-stage ring
+//   warps 4-7  producers: cp.async of the operands into a 5-stage ring, a
+//              stage announced once the copies 2 offsets later are issued
 //   warp 8     lane 0 issues the MMAs
 // and they hand over through mbarriers instead of CTA barriers:
 //   full[s]   stage s loaded        (128 producer arrivals)
@@ -408,19 +409,26 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 //   mdone[b]  TMEM buffer b written (tcgen05.commit)
 //   tfree[b]  TMEM buffer b read    (128 epilogue arrivals)
 // Use u of the pipeline (a running count of offsets over the CTA's tiles)
-// takes stage u % 3 and buffer u % 2; each barrier's k-th completion has
+// takes stage u % 5 and buffer u % 2; each barrier's k-th completion has
 // parity k & 1.  Every wait is bounded: one that runs out sets the plan's
 // error flag and the CTA stops, after letting its copies and MMAs land.
 constexpr int TCM = 128;       // targets per tile = MMA M
 constexpr int TC_MAX_NP = 32;  // up to 4 k-steps x 32 TMEM columns per buffer
 constexpr int TC_COLS = 256;   // TMEM columns per CTA (2 buffers x 128)
-constexpr int TC_STAGES = 3;   // operand stages in shared memory
+constexpr int TC_STAGES = 5;   // operand stages in shared memory
+// producer: an offset is announced once the copies TC_LAG offsets later are
+// issued; a stage is refilled TC_STAGES - TC_LAG - 1 offsets after its MMAs
+// could start
+constexpr int TC_LAG = 2;
 constexpr int TC_EPI = 128, TC_PROD = 128;
 constexpr int TC_THREADS = TC_EPI + TC_PROD + 32;
 constexpr uint32_t TC_MAX_TRIES = 1u << 20;
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_lag() {
+  static_assert(TC_LAG == 2, "wait_group takes the lag as an immediate");
+  asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+}
 
 // shared memory of one operand stage: A hi, A lo, B hi, B lo
 size_t m2l_tc_stage_bytes(int np) {
@@ -491,12 +499,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
       // this tile's offsets that have an operator and a source for some
       // target, and every target's source per offset
       tg = tid < nloc ? rg[tiles.rg_lo[m] + q0 + tid] + cls : -1;
-      unsigned int mask = 0;
+      // all 27 (kind, interaction) loads issued together, not one after another
+      int sidx[27];
+#pragma unroll
       for (int oi = 0; oi < 27; ++oi) {
         const int o = c_class_off_mx[cls][oi];
-        const int sidx = (tg >= 0 && op.kind[o] != M2L_NULL) ? il[(size_t)tg * N_OFFSETS + o] : -1;
-        s_src[oi][tid] = sidx;
-        if (sidx >= 0) mask |= 1u << oi;
+        sidx[oi] = (tg >= 0 && __ldg(&op.kind[o]) != M2L_NULL) ? __ldg(il + (size_t)tg * N_OFFSETS + o) : -1;
+      }
+      unsigned int mask = 0;
+#pragma unroll
+      for (int oi = 0; oi < 27; ++oi) {
+        s_src[oi][tid] = sidx[oi];
+        if (sidx[oi] >= 0) mask |= 1u << oi;
       }
       mask = __reduce_or_sync(0xffffffffu, mask);
       if ((tid & 31) == 0) atomicOr(&s_mask, mask);
@@ -516,7 +530,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
       double acc[32];
 #pragma unroll
       for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+      // charge-sum terms c_o * sum(source) first: independent loads, off the
+      // TMEM loop's path
       double r1 = 0.0;
+#pragma unroll 4
+      for (int a = 0; a < nact; ++a) {
+        const int oi = s_act[a], src = s_src[oi][tid];
+        if (src >= 0) r1 += op.c_m2l[c_class_off_mx[cls][oi]] * __ldg(msum + src);
+      }
       for (int a = 0; a < nact; ++a) {
         if (__any_sync(0xffffffffu, s_abort)) break;
         const uint32_t u = gu + a, b = u & 1u;
@@ -537,8 +558,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
         tc::mbar_arrive(tc::smem_u32(&bar_tfree[b]));
 #pragma unroll
         for (int c = 0; c < 32; ++c) acc[c] += (double)sum[c];
-        const int oi = s_act[a], src = s_src[oi][tid];
-        if (src >= 0) r1 += op.c_m2l[c_class_off_mx[cls][oi]] * __ldg(msum + src);
       }
       if (tg >= 0) {
         double *o = ple + (size_t)tg * np;
@@ -581,16 +600,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
           cp_async16(sp + 2 * a_sz + part * b_sz + off, bsrc + (size_t)n * np + 4 * k4);
         }
         cp_async_commit();
-        if (a >= 1) {  // the previous offset's copies have landed: announce them
-          cp_async_wait_1();
+        if (a >= TC_LAG) {  // the copies of offset a - TC_LAG have landed: announce them
+          cp_async_wait_lag();
           tc::fence_proxy_async();
-          tc::mbar_arrive(tc::smem_u32(&bar_full[(u - 1) % TC_STAGES]));
+          tc::mbar_arrive(tc::smem_u32(&bar_full[(u - TC_LAG) % TC_STAGES]));
         }
       }
       cp_async_wait_all();
-      if (a == nact && nact >= 1) {
+      if (a == nact) {  // announce the offsets still unannounced
         tc::fence_proxy_async();
-        tc::mbar_arrive(tc::smem_u32(&bar_full[(gu + nact - 1) % TC_STAGES]));
+        for (int b = max(0, nact - TC_LAG); b < nact; ++b)
+          tc::mbar_arrive(tc::smem_u32(&bar_full[(gu + uint32_t(b)) % TC_STAGES]));
       }
     } else if (tid == TC_EPI + TC_PROD) {
       // ---- MMA issue ----
