@@ -331,7 +331,7 @@ __device__ bool grid_sync(Counters *cnt, unsigned long long *snap) {
           good = 0;
           break;
         }
-        __nanosleep(100);
+        __nanosleep(32);
       }
     }
     __threadfence();
@@ -751,7 +751,8 @@ void exclusive_sum(const T *in, T *out, int64_t n, cudaStream_t s) {
   FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s));
 }
 
-// blocks of a cooperative launch: all co-resident, at most 2 per SM
+// blocks of a cooperative launch: all co-resident, one per SM (the grid
+// barriers' cost grows with the block count; the per-level work is small)
 int cooperative_grid(const void *kernel, int threads) {
   int dev = 0, coop = 0, sms = 0, per = 0;
   FMMB_CUDA(cudaGetDevice(&dev));
@@ -760,7 +761,7 @@ int cooperative_grid(const void *kernel, int threads) {
   FMMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   FMMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0));
   FMMB_CHECK(per >= 1, ERR_CUDA, "cooperative kernel does not fit on an SM");
-  return sms * (per < 2 ? per : 2);
+  return sms;
 }
 
 }  // namespace
