@@ -188,6 +188,18 @@ void retain_pool_memory() {
   if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
     uint64_t keep = ~uint64_t(0);
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    // headroom reserved once: plans built while earlier ones are still
+    // queued (a host running steps ahead) then take memory the pool already
+    // maps, instead of mapping more in the middle of a step (milliseconds)
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const size_t want = std::min<size_t>(size_t(1) << 30, free_b / 8);
+      void *p = nullptr;
+      if (want > 0 && cudaMallocAsync(&p, want, 0) == cudaSuccess) {
+        cudaFreeAsync(p, 0);
+        cudaStreamSynchronize(0);
+      }
+    }
   }
   done_for = dev;
 }
