@@ -906,7 +906,7 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       t_prep.reset();
       run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(),
                        p->mult_tc.get(), s);
-      p->err.alloc(1, s);
+      p->err.alloc(2, s);  // [0] error flag, [1] M2L tile counter
       p->err.zero(s);
       run_m2l_mixed(a, p->mult32.get(), p->mult_tc.get(), p->msum.get(), p->ple.get(),
                     p->err.get(), s);

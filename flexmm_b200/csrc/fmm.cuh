@@ -136,7 +136,7 @@ void node_charge_sums(const PassArgs &a, const double *tau_sorted, double *tsum,
 void run_upward_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum, float *mult32,
                       double *msum, float *mult_tc, cudaStream_t s);
 void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc, const double *msum,
-                   double *ple, int *err, cudaStream_t s);
+                   double *ple, int *err, cudaStream_t s);  // err: 2 zeroed ints (flag, tile counter)
 void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, double *lsum,
                         cudaStream_t s);
 void run_evaluate_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum,

@@ -444,7 +444,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
                                                          const LevelOpsDev *__restrict__ ops,
                                                          const float *__restrict__ mult_tc,
                                                          const double *__restrict__ msum,
-                                                         double *__restrict__ ple, int *err) {
+                                                         double *__restrict__ ple, int *err,
+                                                         int *tile_counter) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_sfree[TC_STAGES];
   __shared__ __align__(8) uint64_t bar_mdone[2], bar_tfree[2], bar_drain;
@@ -454,6 +455,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
   __shared__ int s_nact;
   __shared__ unsigned int s_mask;
   __shared__ volatile int s_abort;
+  __shared__ int s_tile;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int ntc = (np + 15) & ~15;
   const int nks = np / 8, nk4 = np / 4;
@@ -487,7 +489,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
     atomicExch(err, 1);
   };
   uint32_t gu = 0;  // pipeline uses before the current tile
-  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  // tiles handed out dynamically (their offset counts differ): the first
+  // one is blockIdx.x, the next ones come from a counter
+  for (int tile = blockIdx.x; tile < n_tiles;) {
     int slot = 0;
     while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= tile) ++slot;
     const int m = slot >> 2, cls = slot & 3;
@@ -644,8 +648,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
       }
     }
     gu += uint32_t(nact);
+    if (tid == 0) s_tile = int(gridDim.x) + atomicAdd(tile_counter, 1);
     __syncthreads();
     if (s_abort) break;
+    tile = s_tile;
   }
   // every MMA issued has completed before the tensor memory is freed (the
   // epilogue waited for each one; after a run-out this drains them)
@@ -1258,7 +1264,7 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc,
     PhaseTimer timer(PH_M2L, s);
     k_m2l_tc<<<std::min(ctiles, sms), TC_THREADS, sm, s>>>(tc, ctiles, a.neq, a.np, a.td->rg.get(),
                                                            a.td->il.get(), a.ops_dev, mult_tc, msum,
-                                                           ple, err);
+                                                           ple, err, err + 1);
     FMMB_CUDA(cudaGetLastError());
     return;
   }
