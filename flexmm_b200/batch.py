@@ -1,0 +1,134 @@
+"""Many independent Stokes problems at once: forward and charge adjoint.
+
+The reference evaluates one Stokes FMM at a time
+(flexmm/kifmm2d/vector/stokes_fmm.py:592-858).  ``StokesBatch`` holds one
+FMM per problem, all sharing the per-width operators, and spreads them over
+several CUDA streams: every call queues device work only (no host waits), so
+the small problems of a batch overlap on the GPU.
+
+Forward, for each problem's own sources (coincident points skipped):
+``(u, v, p) = A f`` with the reference's Stokeslet (stokes_fmm.py:161-184):
+u = (1/4pi) [(-log(r^2)/2 + dx^2/r^2) fx + (dx dy/r^2) fy], v likewise,
+p = (1/2pi) (dx fx + dy fy) / r^2, (dx, dy) = target - source.
+
+Charge adjoint: the velocity block of the Stokeslet is symmetric under
+exchanging the two points and the two components, so its transpose is the
+same velocity operator; the pressure row p_i = (1/2pi) sum_j (x_i - x_j) .
+f_j / r^2 transposes to d f_j = (1/2pi) sum_i g_p,i (x_i - x_j) / r^2, the
+target-position gradient of the Laplace potential -log(r^2)/(4pi) with
+charges g_p.  So ``A^T (g_u, g_v, g_p)`` = Stokes velocity of (g_u, g_v) plus
+the Laplace gradient of g_p, both at the sources.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .kifmm import KI_FMM, _torch
+from .helpers import KI_Helper
+from .stokes import FMM as StokesFMM
+
+
+class StokesBatch:
+    """``StokesBatch(problems, Nequiv=32, Ncutoff=64, n_streams=8)`` with
+    ``problems`` a list of ``(x, y)`` source arrays; ``forward(forces)`` with
+    ``forces`` a list of ``(fx, fy)`` returns a list of ``(u, v, p)``;
+    ``adjoint(cotangents)`` with a list of ``(gu, gv, gp)`` returns a list of
+    ``(dfx, dfy)``.  Results are CUDA tensors (call ``torch.cuda.synchronize``
+    or read them, which waits, before using them on the host)."""
+
+    def __init__(self, problems, Nequiv=32, Ncutoff=64, n_streams=8, adjoint=True):
+        torch = _torch()
+        self.Nequiv, self.Ncutoff = int(Nequiv), int(Ncutoff)
+        self.streams = [torch.cuda.Stream() for _ in range(max(1, int(n_streams)))]
+        self._pts, self._stokes, self._laplace = [], [], []
+        pre = {}
+        helper = KI_Helper()
+        for k, (x, y) in enumerate(problems):
+            with torch.cuda.stream(self._stream(k)):
+                xd = torch.as_tensor(np.asarray(x, dtype=np.float64)).cuda()
+                yd = torch.as_tensor(np.asarray(y, dtype=np.float64)).cuda()
+                F = StokesFMM(xd, yd, self.Nequiv, self.Ncutoff, None,
+                              precomputations=pre if pre else None)
+                F.precompute()
+                pre = F.precomputations  # operators shared by width across problems
+                self._stokes.append(F)
+                L = None
+                if adjoint:
+                    L = KI_FMM(xd, yd, "Laplace_Eval", self.Ncutoff, self.Nequiv, helper=helper)
+                    L.register_evaluator(None, None, "gradient", 3)  # (u, du/dx, du/dy)
+                self._laplace.append(L)
+                self._pts.append((xd, yd))
+        torch.cuda.synchronize()
+
+    def _stream(self, k):
+        return self.streams[k % len(self.streams)]
+
+    def __len__(self):
+        return len(self._pts)
+
+    def _own_stokes(self, F, n):
+        torch = _torch()
+        out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        _lib.call("fmm_evaluate_sources_outputs", F._plan, _lib.EVALUATORS["stokes"][0], 1,
+                  ctypes.c_void_p(out.data_ptr()), n,
+                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        return out
+
+    def forward(self, forces):
+        """(u, v, p) at every problem's sources for forces [(fx, fy), ...]."""
+        torch = _torch()
+        if len(forces) != len(self):
+            raise ValueError(f"expected {len(self)} force pairs, got {len(forces)}")
+        outs = []
+        for k, (F, (fx, fy)) in enumerate(zip(self._stokes, forces)):
+            with torch.cuda.stream(self._stream(k)):
+                F.build_expansions(_device(fx), _device(fy))
+                o = self._own_stokes(F, F.N)
+                outs.append((o[0], o[1], o[2]))
+        self._join(outs)
+        return outs
+
+    def adjoint(self, cotangents):
+        """(dfx, dfy) = A^T (gu, gv, gp) for every problem."""
+        torch = _torch()
+        if any(L is None for L in self._laplace):
+            raise RuntimeError("built with adjoint=False")
+        if len(cotangents) != len(self):
+            raise ValueError(f"expected {len(self)} cotangent triples, got {len(cotangents)}")
+        outs = []
+        for k, (F, L, (gu, gv, gp), (xd, yd)) in enumerate(
+                zip(self._stokes, self._laplace, cotangents, self._pts)):
+            with torch.cuda.stream(self._stream(k)):
+                F.build_expansions(_device(gu), _device(gv))
+                vel = self._own_stokes(F, F.N)
+                L.build_expansions(_device(gp))
+                grad = L.evaluate_to_points(xd, yd, "gradient", True)
+                outs.append((vel[0] + grad[1], vel[1] + grad[2]))
+        self._join(outs)
+        return outs
+
+    def _join(self, outs):
+        """The caller's stream waits for every batch stream, and the results
+        (made on the batch streams) are marked as used on it."""
+        torch = _torch()
+        cur = torch.cuda.current_stream()
+        for s in self.streams:
+            cur.wait_stream(s)
+        for tup in outs:
+            for t in tup:
+                t.record_stream(cur)
+
+    def status(self):
+        for F in self._stokes:
+            F.status()
+        for L in self._laplace:
+            if L is not None:
+                L.status()
+
+
+def _device(a):
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        return a.to(device="cuda", dtype=torch.float64).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
