@@ -282,22 +282,23 @@ __global__ void k_leaf_targets(int total, int L, const int *__restrict__ off,
     }
     const int lev = lo;
     int b = 0, e = 0;
-    if (flags[g] & NF_LEAF) {
+    if ((flags[g] & NF_LEAF) && m > 0) {
+      // both ends of the leaf's key range: two branchless lower-bound
+      // searches over [0, m) in step (same length, same step count), so each
+      // step's two loads are issued together
       const int sh = 2 * (MAXD - lev);
       const uint64_t c = code[g];
-      int64_t l0 = 0, h0 = m;
       const uint64_t vlo = c << sh, vhi = (c + 1) << sh;
-      while (l0 < h0) {
-        int64_t md = (l0 + h0) >> 1;
-        if (tkeys[md] < vlo) l0 = md + 1; else h0 = md;
+      int64_t b0 = 0, b1 = 0, len = m;
+      while (len > 1) {
+        const int64_t half = len >> 1;
+        const uint64_t k0 = __ldg(tkeys + b0 + half), k1 = __ldg(tkeys + b1 + half);
+        b0 += k0 < vlo ? half : 0;
+        b1 += k1 < vhi ? half : 0;
+        len -= half;
       }
-      b = int(l0);
-      h0 = m;
-      while (l0 < h0) {
-        int64_t md = (l0 + h0) >> 1;
-        if (tkeys[md] < vhi) l0 = md + 1; else h0 = md;
-      }
-      e = int(l0);
+      b = int(b0 + (__ldg(tkeys + b0) < vlo ? 1 : 0));
+      e = int(b1 + (__ldg(tkeys + b1) < vhi ? 1 : 0));
     }
     tb[g] = b;
     te[g] = e;
