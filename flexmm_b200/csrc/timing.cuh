@@ -11,7 +11,7 @@
 namespace fmmb {
 
 enum Phase : int {
-  PH_TREE = 0,      // whole tree build (span, includes host round trips)
+  PH_TREE = 0,      // whole tree build (span, includes its two host waits)
   PH_SORT_TGT = 1,  // target keys + sort + gather
   PH_UPWARD = 2,    // k_upward launches (S2M + M2M + C2E)
   PH_M2L = 3,       // k_m2l launch

@@ -7,11 +7,14 @@
 // colleague four "fake" children (flexmm/tree.py:385-397, 542-553).
 //
 // Here the same tree is computed without sequential partitioning:
-//  1. every point gets a key of 29 quadrant digits by descending from the
-//     root with the reference's own float64 midpoint arithmetic
+//  1. every point gets a key of 29 quadrant digits equal to descending from
+//     the root with the reference's own float64 midpoint arithmetic
 //     (xmid = xmin + half_width, child xmin = xmid - half_width or xmid,
-//     class = 2*(x > xmid) + (y > ymid)), so every comparison is bit-identical;
-//  2. keys are radix-sorted: every box is a contiguous run of sorted keys;
+//     class = 2*(x > xmid) + (y > ymid)): the bits of the fixed-point cell
+//     index where a point is clear of every split line, the descent itself
+//     near one, so every comparison is bit-identical;
+//  2. keys are radix-sorted (on 32-bit prefixes while 16 digits suffice):
+//     every box is a contiguous run of sorted keys;
 //  3. the initially split boxes S0 are the key prefixes with more than `ppl`
 //     points, read off the sorted keys (a run starting at i is longer than
 //     ppl iff key i and key i+ppl share the prefix);
@@ -24,6 +27,9 @@
 //     (level, morton); each contributes 4 consecutive children, so node
 //     arrays, ranges, colleagues and interaction lists follow from binary
 //     searches in sorted arrays.
+// The host waits twice (for the split-box count and depth, then for the
+// balance closure's size); the per-level node counts come back without a
+// wait (finalize_tree).
 #include <cub/cub.cuh>
 
 #include <cmath>
