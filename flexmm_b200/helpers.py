@@ -20,10 +20,14 @@ Two deliberate differences from the reference:
   per (kernel, params, Nequiv) is used, so operators stay warm across objects.
 """
 import ctypes
+import hashlib
+import os
 
 import numpy as np
 
 from . import _lib
+
+CACHE_VERSION = 1      # on-disk operator files: bump when their content changes
 
 SVD_TOL = 1e-14        # M2L compression, flexmm/flexmm2d/helpers.py:197
 C2E_TOL = 1e-15        # SVD_Solver, flexmm/kifmm2d/scalar/helpers.py:241
@@ -96,6 +100,34 @@ class KIPrecomputation:
                 self.m2l_a.append(m)
                 self.m2l_b.append(None)
 
+    def to_arrays(self):
+        """The operators as named arrays (one .npz file of the on-disk cache)."""
+        d = dict(width=np.float64(self.width), c2e_sinv=self.c2e_sinv, c2e_u=self.c2e_u,
+                 c2e_vh=self.c2e_vh, m2mc=self.m2mc, small_x=self.small_x, small_y=self.small_y,
+                 large_x=self.large_x, large_y=self.large_y, m2l_rank=self.m2l_rank)
+        for o, (a, b) in enumerate(zip(self.m2l_a, self.m2l_b)):
+            if a is not None:
+                d[f"m2l_a_{o}"] = a
+            if b is not None:
+                d[f"m2l_b_{o}"] = b
+        return d
+
+    @classmethod
+    def from_arrays(cls, d):
+        """Inverse of to_arrays (no operator is recomputed)."""
+        pre = cls.__new__(cls)
+        pre.width = float(d["width"])
+        for name in ("c2e_sinv", "c2e_u", "c2e_vh", "m2mc", "small_x", "small_y", "large_x",
+                     "large_y"):
+            setattr(pre, name, np.ascontiguousarray(d[name], dtype=np.float64))
+        pre.m2l_rank = np.ascontiguousarray(d["m2l_rank"], dtype=np.int32)
+        pre.m2l_a, pre.m2l_b = [], []
+        for o in range(len(pre.m2l_rank)):
+            a, b = d.get(f"m2l_a_{o}"), d.get(f"m2l_b_{o}")
+            pre.m2l_a.append(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
+            pre.m2l_b.append(None if b is None else np.ascontiguousarray(b, dtype=np.float64))
+        return pre
+
     def upload(self, ops_handle):
         dp = ctypes.POINTER(ctypes.c_double)
 
@@ -134,14 +166,23 @@ class OpsSet:
 
 
 class KI_Helper:
-    """Operator cache for one (kernel, Nequiv) (Helper, flexmm/flexmm2d/helpers.py:35-84)."""
+    """Operator cache for one (kernel, Nequiv) (Helper, flexmm/flexmm2d/helpers.py:35-84).
 
-    def __init__(self, helper=None):
+    ``cache_dir`` (or the environment variable FLEXMM_B200_CACHE) keeps the
+    host operators on disk across processes, one .npz file per width under a
+    directory named by (kernel, parameters, Nequiv, format version): the
+    helper loads them when it is bound to its kernel (so bbox snapping sees
+    those widths, as for a helper that already met them) and writes every
+    width it forms.  Tabulated kernels (``radial``) are not cached on disk:
+    their identity is not in their parameters."""
+
+    def __init__(self, helper=None, cache_dir=None):
         self.kernel = None
         self.nequiv = None
         self.precomputations = {}   # width_key -> KIPrecomputation
         self._level_ids = {}        # width_key -> device operator entry
         self._ops = None
+        self.cache_dir = cache_dir if cache_dir is not None else os.environ.get("FLEXMM_B200_CACHE")
         if helper is not None:      # share the other helper's cache, like the reference
             self.__dict__ = helper.__dict__
 
@@ -149,9 +190,42 @@ class KI_Helper:
         if self.kernel is None:
             self.kernel = kernel
             self.nequiv = nequiv
+            self._load_disk_cache()
         elif self.kernel.key != kernel.key or self.nequiv != nequiv:
             raise ValueError(f"helper holds operators for {self.kernel} with Nequiv={self.nequiv}; "
                              f"got {kernel} with Nequiv={nequiv}")
+
+    def _disk_dir(self):
+        from .kernels import KERNEL_RADIAL_TABLE
+        if not self.cache_dir or self.kernel is None or self.kernel.kernel_id == KERNEL_RADIAL_TABLE:
+            return None
+        tag = repr((self.kernel.key, int(self.nequiv), CACHE_VERSION)).encode()
+        return os.path.join(self.cache_dir, "ki_" + hashlib.sha1(tag).hexdigest()[:20])
+
+    def _load_disk_cache(self):
+        d = self._disk_dir()
+        if d is None or not os.path.isdir(d):
+            return
+        for name in sorted(os.listdir(d)):
+            if not name.endswith(".npz"):
+                continue
+            try:
+                with np.load(os.path.join(d, name)) as z:
+                    pre = KIPrecomputation.from_arrays({k: z[k] for k in z.files})
+            except (OSError, KeyError, ValueError):
+                continue  # a damaged or foreign file: that width is formed again
+            if pre.c2e_u.shape[0] == self.nequiv:
+                self.precomputations.setdefault(width_key(pre.width), pre)
+
+    def _save_disk(self, key, pre):
+        d = self._disk_dir()
+        if d is None:
+            return
+        os.makedirs(d, exist_ok=True)
+        path = os.path.join(d, f"w_{key!r}.npz")
+        tmp = f"{path}.{os.getpid()}.tmp.npz"
+        np.savez(tmp, **pre.to_arrays())
+        os.replace(tmp, path)  # atomic: readers see the whole file or none
 
     def ops_set(self):
         if self._ops is None:
@@ -176,12 +250,21 @@ class KI_Helper:
         cy = (bbox[3] + bbox[2]) / 2
         return [float(cx - width / 2), float(cx + width / 2), float(cy - width / 2), float(cy + width / 2)]
 
-    def level_id(self, width):
+    def precomputation(self, width):
+        """The host operators of a width: from memory, the disk cache, or formed
+        (and then written to the disk cache)."""
         key = width_key(width)
         if key not in self.precomputations:
-            self.precomputations[key] = KIPrecomputation(width, self.nequiv, self.kernel)
+            pre = KIPrecomputation(width, self.nequiv, self.kernel)
+            self.precomputations[key] = pre
+            self._save_disk(key, pre)
+        return self.precomputations[key]
+
+    def level_id(self, width):
+        key = width_key(width)
+        pre = self.precomputation(width)
         if key not in self._level_ids:
-            self._level_ids[key] = self.precomputations[key].upload(self.ops_set().handle)
+            self._level_ids[key] = pre.upload(self.ops_set().handle)
         return self._level_ids[key]
 
     def get_precomputation(self, width):
