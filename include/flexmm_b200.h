@@ -139,7 +139,11 @@ int fmm_ops_add(fmm_ops *ops, const fmm_level_ops *level, int *level_id);
 int fmm_ops_destroy(fmm_ops *ops);
 
 /* Build the quadtree of n sources (device x, y) with at most ncutoff points
- * per leaf over the square bbox = {xmin, xmax, ymin, ymax} (host array). */
+ * per leaf over the square bbox = {xmin, xmax, ymin, ymax} (host array).
+ * Device memory comes from the device's default stream-ordered pool; the
+ * first plan on a device sets that pool to keep freed memory and reserves up
+ * to 1 GiB (at most 1/8 of the free memory) in it, so that later plans do
+ * not map memory while earlier work is still queued. */
 int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
                     const double *bbox, void *stream, fmm_plan **out);
 /* n_levels and, for each level, its box width and node count (host arrays of
