@@ -17,6 +17,8 @@ Differences from the reference, both result-preserving:
   of a previous FMM to reuse them, as the reference's ``precomputations=``).
 """
 import ctypes
+import hashlib
+import os
 
 import numpy as np
 
@@ -134,6 +136,71 @@ class StokesPrecomputation:
         return lid.value
 
 
+    def to_arrays(self):
+        """The operators as named arrays (one .npz file of the on-disk cache)."""
+        d = dict(width=np.float64(self.width), nequiv=np.int64(self.Nequiv),
+                 small_x=self.small_x, small_y=self.small_y, large_x=self.large_x,
+                 large_y=self.large_y, m2mc=self.m2mc, l2lc=self.l2lc, m2l_rank=self.m2l_rank)
+        for name in ("e2c", "c2e"):
+            svd = getattr(self, name)
+            d[f"{name}_U"], d[f"{name}_SI"], d[f"{name}_VH"] = svd.U, svd.SI, svd.VH
+        for o, (a, b) in enumerate(zip(self.m2l_a, self.m2l_b)):
+            if a is not None:
+                d[f"m2l_a_{o}"] = a
+            if b is not None:
+                d[f"m2l_b_{o}"] = b
+        return d
+
+    @classmethod
+    def from_arrays(cls, d):
+        """Inverse of to_arrays (no operator is recomputed)."""
+        pre = cls.__new__(cls)
+        pre.width = float(d["width"])
+        pre.Nequiv = int(d["nequiv"])
+        for name in ("small_x", "small_y", "large_x", "large_y", "m2mc", "l2lc"):
+            setattr(pre, name, np.ascontiguousarray(d[name], dtype=np.float64))
+        for name in ("e2c", "c2e"):
+            svd = _SVD.__new__(_SVD)
+            svd.U, svd.SI, svd.VH = (np.asarray(d[f"{name}_{k}"], dtype=np.float64)
+                                     for k in ("U", "SI", "VH"))
+            setattr(pre, name, svd)
+        pre.m2l_rank = np.ascontiguousarray(d["m2l_rank"], dtype=np.int32)
+        pre.m2l_a, pre.m2l_b = [], []
+        for o in range(len(pre.m2l_rank)):
+            a, b = d.get(f"m2l_a_{o}"), d.get(f"m2l_b_{o}")
+            pre.m2l_a.append(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
+            pre.m2l_b.append(None if b is None else np.ascontiguousarray(b, dtype=np.float64))
+        return pre
+
+
+def stokes_precomputation(width, nequiv, cache_dir=None):
+    """Operators of one width: from the on-disk cache (``cache_dir`` or the
+    environment variable FLEXMM_B200_CACHE) when it holds them, else formed
+    and then written there (one .npz per width under a directory named by
+    Nequiv and the file format's version)."""
+    from .helpers import CACHE_VERSION
+    cache_dir = cache_dir if cache_dir is not None else os.environ.get("FLEXMM_B200_CACHE")
+    path = None
+    if cache_dir:
+        tag = hashlib.sha1(repr(("stokes", int(nequiv), CACHE_VERSION)).encode()).hexdigest()[:20]
+        d = os.path.join(cache_dir, "stokes_" + tag)
+        path = os.path.join(d, f"w_{width_key(width)!r}.npz")
+        try:
+            with np.load(path) as z:
+                pre = StokesPrecomputation.from_arrays({k: z[k] for k in z.files})
+            if pre.Nequiv == nequiv and width_key(pre.width) == width_key(width):
+                return pre
+        except (OSError, KeyError, ValueError):
+            pass  # absent or damaged: formed again below
+    pre = StokesPrecomputation(width, nequiv)
+    if path:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = f"{path}.{os.getpid()}.tmp.npz"
+        np.savez(tmp, **pre.to_arrays())
+        os.replace(tmp, path)  # atomic: readers see the whole file or none
+    return pre
+
+
 class _StokesOps:
     def __init__(self, nequiv):
         h = ctypes.c_void_p()
@@ -212,7 +279,7 @@ class FMM:
         for m, w in enumerate(self._widths):
             key = width_key(w)
             if key not in pre:
-                pre[key] = StokesPrecomputation(w, self.Nequiv)
+                pre[key] = stokes_precomputation(w, self.Nequiv)
             if key not in self._ops.level_ids:
                 self._ops.level_ids[key] = pre[key].upload(self._ops.handle)
             _lib.call("fmm_plan_bind", self._plan, m, self._ops.level_ids[key])

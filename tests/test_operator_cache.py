@@ -63,3 +63,29 @@ def test_disk_cache_keeps_kernels_and_nequiv_apart(tmp_path):
     c.attach(lap, 24)
     assert c.precomputations == {}
     _same(c.precomputation(0.25), KIPrecomputation(0.25, 24, lap))
+
+
+def test_stokes_operators_round_trip_and_disk_cache(tmp_path, monkeypatch):
+    from flexmm_b200 import stokes
+    pre = stokes.StokesPrecomputation(0.25, 16)
+    back = stokes.StokesPrecomputation.from_arrays(pre.to_arrays())
+    for name in ("small_x", "small_y", "large_x", "large_y", "m2mc", "l2lc", "m2l_rank"):
+        np.testing.assert_array_equal(getattr(pre, name), getattr(back, name))
+    for name in ("e2c", "c2e"):
+        for part in ("U", "SI", "VH"):
+            np.testing.assert_array_equal(getattr(getattr(pre, name), part),
+                                          getattr(getattr(back, name), part))
+    for xa, xb in zip(pre.m2l_a + pre.m2l_b, back.m2l_a + back.m2l_b):
+        assert (xa is None) == (xb is None)
+        if xa is not None:
+            np.testing.assert_array_equal(xa, xb)
+    # formed once, then read back from disk without being formed again
+    first = stokes.stokes_precomputation(0.5, 16, cache_dir=str(tmp_path))
+    assert any(f.endswith(".npz") for d in tmp_path.iterdir() for f in os.listdir(d))
+
+    def refuse(*args, **kwargs):
+        raise AssertionError("formed again instead of read from the cache")
+    monkeypatch.setattr(stokes.StokesPrecomputation, "__init__", refuse)
+    again = stokes.stokes_precomputation(0.5, 16, cache_dir=str(tmp_path))
+    np.testing.assert_array_equal(again.m2mc, first.m2mc)
+    np.testing.assert_array_equal(again.c2e.U, first.c2e.U)
