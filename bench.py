@@ -55,7 +55,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched-stokes", action="store_true",
                    help="skip the batched-Stokes (many independent problems) measurement")
-    p.add_argument("--cpu-sample-n", type=int, default=200_000)
+    p.add_argument("--cpu-sample-n", type=int, default=200_000,
+                   help="sources in the bounded reference sample of our arm's cpu_baseline")
+    p.add_argument("--denested-steps", type=int, default=3,
+                   help="reference arm: steps of the de-nested S2M variant (0: none)")
     p.add_argument("--json-only", action="store_true", help=argparse.SUPPRESS)
     p.add_argument("--ncu", action="store_true",
                    help="profiling mode: warm-up and timed steps only (no accuracy, e2e, peaks)")
@@ -443,7 +446,7 @@ def work_counts_gemm(F, neq, c):
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel on the default
-# workload, from one ncu capture of it (profiles/traffic_clustered1M.md)
+# workload (1M clustered sources + 1000^2 grid), from one ncu capture
 NCU_TRAFFIC_BYTES = {("mixed", "evaluate"): 44_016_384, ("fp64", "evaluate"): 53_386_240}
 
 
@@ -471,6 +474,16 @@ def roofline_of(res, precision, peaks, steps, default_workload):
     return {"bound": bound, "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": "measured in bench.py: " + src,
             "flops_per_launch": flops_per_launch, "ms_per_launch": ms_k / max(n_launch, 1)}
+
+
+def workload_config(args, world):
+    """The workload both arms run and report (the same dict in both lines)."""
+    return {"workload": f"clustered Laplace KIFMM, {args.n} sources + {args.grid}^2 grid targets, "
+                        f"self + target evaluation",
+            "n_sources": args.n, "n_targets": args.grid * args.grid,
+            "ncutoff": NCUT, "nequiv": NEQ[args.precision], "precision": args.precision,
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "flushed (256 MB write) between timed GPU steps"}
 
 
 def run_ours(args, world, rank, local):
@@ -510,12 +523,8 @@ def run_ours(args, world, rank, local):
         "dtype": "f32+tf32x3/f64" if args.precision == "mixed" else "f64",
         "precision": args.precision,
         "data": "synthetic: seeded clustered sources and grid targets (no dataset)",
-        "config": {"workload": f"clustered Laplace KIFMM, {n_src} sources + {args.grid}^2 grid targets, "
-                               f"self + target evaluation", "n_sources": n_src, "n_targets": n_tgt,
-                   "ncutoff": NCUT, "nequiv": main["neq"], "precision": args.precision,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "flushed (256 MB write) between timed steps",
-                   "levels": main["F"]._levels, "nodes": int(sum(main["F"]._counts))},
+        "config": workload_config(args, world),
+        "tree": {"levels": main["F"]._levels, "nodes": int(sum(main["F"]._counts))},
         "accuracy": main["accuracy"],
         "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in main["phases"].items() if v[1]},
         "work_per_step": main["counts"],
@@ -580,8 +589,14 @@ def measure_batched_stokes(args, n_problems=256):
 
 
 # ---------------------------------------------------------- reference arm --
-def reference_step_fn(n_src, n_grid, neq):
-    """Closure timing one step of the reference flexmm on the host CPU."""
+def reference_step_fn(n_src, n_grid, neq, denested=False):
+    """Closure timing one step of the reference flexmm on the host CPU.
+
+    denested=True pre-registers a serial kernel_apply in a fresh helper before
+    the FMM is built (KI_Helper.build_s2pM_function keeps a registered one,
+    flexmm/flexmm2d/kifmm.py:83-92): the S2M loop over leaves stays parallel
+    but its inner per-leaf loop no longer opens a nested parallel region.
+    Same arithmetic, so the same results; the as-is form is the baseline."""
     from oracle import refimport  # the reference itself (shimmed copy), checker-only
     from flexmm_b200 import workloads
     refimport.load_reference()
@@ -597,6 +612,28 @@ def reference_step_fn(n_src, n_grid, neq):
 
     d = workloads.clustered(n=n_src, n_grid=n_grid)
     helper = KI_Helper()
+    if denested:
+        @numba.njit(fastmath=True)
+        def kernel_apply_serial(sx, sy, tx, ty, tau, out):
+            for j in range(tx.size):
+                outj = 0.0
+                for i in range(sx.size):
+                    outj += Laplace_Eval(sx[i], sy[i], tx[j], ty[j]) * tau[i]
+                out[j] = outj
+        helper.functions["kernel_eval"] = Laplace_Eval
+        helper.functions["kernel_apply"] = kernel_apply_serial
+
+    # JIT warm-up on a 5,000-point problem (the examples' protocol), with its
+    # own helper so that its box widths do not enter the timed helper's cache
+    w = workloads.clustered(n=5000, n_grid=20)
+    wh = KI_Helper()
+    if denested:
+        wh.functions.update(helper.functions)
+    Fw = KI_FMM(w["x"], w["y"], Laplace_Eval, NCUT, neq, bbox=w["bbox"], helper=wh)
+    Fw.build_expansions(w["tau"])
+    Fw.source_evaluation(w["x"], w["y"])
+    Fw.target_evaluation(w["tx"], w["ty"])
+    helper.functions.update({k: v for k, v in wh.functions.items() if k not in helper.functions})
 
     def step():
         t0 = time.perf_counter()
@@ -615,12 +652,15 @@ def reference_available():
 
 
 def cpu_baseline_subprocess(args):
-    """Time the reference on the host in a fresh process (all cores)."""
+    """Time the reference on the host in a fresh process (all cores) on a
+    bounded sample of the workload (--cpu-sample-n sources, a grid of about
+    as many targets): best and mean of 3 steps, as-is and de-nested."""
     cores = os.cpu_count() or 1
     env = dict(os.environ, NUMBA_NUM_THREADS=str(cores), CUDA_VISIBLE_DEVICES="")
-    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "2",
-           "--warmup", "1", "--precision", args.precision, "--cpu-sample-n",
-           str(args.cpu_sample_n), "--json-only"]
+    grid = int(round(np.sqrt(args.cpu_sample_n)))
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "3",
+           "--warmup", "1", "--precision", args.precision, "--n", str(args.cpu_sample_n),
+           "--grid", str(grid), "--denested-steps", "3", "--json-only"]
     try:
         r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
         line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
@@ -631,34 +671,49 @@ def cpu_baseline_subprocess(args):
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference flexmm's own KI_FMM (numba, all host
+    threads) on this bench's workload -- by default the full 1M-source /
+    1000^2-grid configuration, the same one the GPU line reports -- one full
+    problem per step (tree + build_expansions + source_evaluation +
+    target_evaluation, operators warm), W warm-up and K timed steps."""
     if rank != 0:
         return
     neq = NEQ[args.precision]
-    grid = int(round(np.sqrt(args.cpu_sample_n)))
     base = {"impl": "reference", "metric": METRIC, "unit": "Mpts/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded clustered sources and grid targets (no dataset)",
-            "config": {"workload": f"clustered Laplace KIFMM, {args.n} sources + {args.grid}^2 grid "
-                                   f"targets, self + target evaluation", "ncutoff": NCUT,
-                       "nequiv": neq, "precision": args.precision}}
+            "config": workload_config(args, world)}
     if not reference_available():
         base["unavailable"] = "reference copy oracle/_ref not built (needs the reference checkout)"
         print(json.dumps(base), flush=True)
         return
     cores = int(os.environ.get("NUMBA_NUM_THREADS", os.cpu_count() or 1))
-    step, pts = reference_step_fn(args.cpu_sample_n, grid, neq)
+    step, pts = reference_step_fn(args.n, args.grid, neq)
     for _ in range(max(args.warmup, 1)):
         step()
     ts = [step() for _ in range(max(args.steps, 1))]
     sec = statistics.mean(ts)
     value = pts / sec / 1e6
-    sample = (f"reference flexmm KI_FMM (numba, {cores} threads), clustered {args.cpu_sample_n} "
-              f"sources + {grid}^2 grid targets, Nequiv {neq}, warm JIT and operators; per step: "
-              f"tree + build_expansions + source_evaluation + target_evaluation")
-    base.update({"value": value, "ms_per_step": sec * 1e3,
-                 "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores,
-                                  "kind": "reference", "sample": sample},
+    scope = ("a bounded sample of the 1M-source / 1000^2-grid workload" if args.json_only
+             else "the full workload")
+    sample = (f"{scope}: reference flexmm KI_FMM as-is (numba, {cores} threads), "
+              f"clustered {args.n} sources + {args.grid}^2 grid targets, Nequiv {neq}, warm JIT "
+              f"(5,000-point problem) and operators (helper reuse); per step: tree + "
+              f"build_expansions + source_evaluation + target_evaluation; value = mean of "
+              f"{len(ts)} steps")
+    cpu = {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "reference",
+           "sample": sample, "best_of_steps": pts / min(ts) / 1e6,
+           "s_per_step": [round(t, 3) for t in ts]}
+    if args.denested_steps > 0:
+        dstep, _ = reference_step_fn(args.n, args.grid, neq, denested=True)
+        dstep()  # operators of this helper
+        dts = [dstep() for _ in range(args.denested_steps)]
+        cpu["denested_s2m"] = {"value": pts / statistics.mean(dts) / 1e6,
+                               "best": pts / min(dts) / 1e6, "steps": len(dts),
+                               "note": "serial kernel_apply pre-registered in the helper: S2M "
+                                       "without the nested parallel region; same results"}
+    base.update({"value": value, "ms_per_step": sec * 1e3, "cpu_baseline": cpu,
                  "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0,
                          "d2h_bytes_per_step": 0}})
     print(json.dumps(base), flush=True)

@@ -27,7 +27,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_COPY = os.path.join(HERE, "_ref")
-REFERENCE_CHECKOUT = "/root/reference"
+# the read-only reference checkout; FLEXMM_REFERENCE overrides where it lies
+REFERENCE_CHECKOUT = os.environ.get("FLEXMM_REFERENCE", "/root/reference")
 
 
 def build_ref(src=REFERENCE_CHECKOUT, dst=REF_COPY):

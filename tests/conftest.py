@@ -31,8 +31,9 @@ def load_golden(name):
     import json
     d = dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
     d["meta"] = json.loads(str(d["meta"]))
-    if "tree_sha" in d:
-        d["tree_sha"] = json.loads(str(d["tree_sha"]))
+    for k in ("tree_sha", "tree_sha_nonempty"):
+        if k in d:
+            d[k] = json.loads(str(d[k]))
     return d
 
 

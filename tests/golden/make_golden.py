@@ -5,6 +5,7 @@ Run in a container that has the reference checkout (it is copied into
 
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py small      # only the quick ones
+    python tests/golden/make_golden.py tree-digests   # reference tree digests of the large cases
 
 For every case the inputs are regenerated from ``flexmm_b200.workloads``
 recipes (seeded numpy), the reference ``KI_FMM`` is built with a fresh
@@ -17,6 +18,8 @@ recipes (seeded numpy), the reference ``KI_FMM`` is built with a fresh
 * ``direct_src`` / ``direct_tgt`` FP64 direct sums at the sampled points
 * ``tree_sha``  sha256 of every canonical tree array of the reference tree
   (``tests/canon.py``), for cases small enough to canonicalise quickly
+* ``tree_sha_nonempty`` (the sampled 100k / 1M cases) the same digests of the
+  reference's tree with interactions from empty source boxes left out
 
 Gradient cases (``grad_*``) run the reference's kifmm2d FMM with the
 gradient evaluator of examples/pure_kifmm_laplace_gradient.py
@@ -348,7 +351,34 @@ def run_stokes_case(name, meta, ref):
           flush=True)
 
 
+def add_tree_digests(name, meta, ref):
+    """Canonical digests of the reference's own tree for a large (sampled)
+    case, added to its existing fixture: the reference Tree alone
+    (flexmm/tree.py:451-518) on the case's inputs and the bbox the reference
+    FMM used.  ``tree_sha_nonempty`` keeps only interactions whose source box
+    holds points (the form the device tree's lists take)."""
+    from flexmm.tree import Tree
+    path = os.path.join(HERE, name + ".npz")
+    old = dict(np.load(path, allow_pickle=False))
+    d = case_inputs(meta)
+    t0 = time.time()
+    T = Tree(d["x"], d["y"], meta["ncut"], list(old["bbox_used"]))
+    t1 = time.time()
+    assert T.levels == int(old["levels"])
+    c = canon.canonical(T, nonempty_sources=True)
+    old["tree_sha_nonempty"] = json.dumps({k: sha(np.asarray(v, dtype=np.int64)) for k, v in c.items()})
+    np.savez_compressed(path, **old)
+    print(f"{name}: reference tree {t1 - t0:.1f}s, {T.levels} levels, digests added", flush=True)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "tree-digests":
+        refimport.build_ref()
+        ref = refimport.load_reference()
+        for name, (meta, small) in CASES.items():
+            if "sample" in meta and meta.get("method") is None:
+                add_tree_digests(name, meta, ref)
+        return
     only_small = len(sys.argv) > 1 and sys.argv[1] == "small"
     names = [a for a in sys.argv[1:] if a in CASES]
     refimport.build_ref()

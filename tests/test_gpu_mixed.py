@@ -32,6 +32,26 @@ def test_mixed_error_vs_direct_sum(built_lib, recipe, n, neq):
     assert es < BAR and et < BAR, (es, et)
 
 
+def test_mixed_headline_config_vs_direct_sum(built_lib):
+    """The headline configuration: 1M sources in 20 Gaussian clusters plus a
+    1000^2 grid, Nequiv 24, mixed form -- against the FP64 direct sums at the
+    fixture's 2,000 sampled sources and 2,000 grid targets (bar 1e-6), and
+    against the reference's own FP64 Nequiv-24 outputs there."""
+    from conftest import golden_inputs, load_golden
+    g = load_golden("clustered_1M_q24")
+    meta = g["meta"]
+    d = golden_inputs(meta)
+    F, us, ut = _run(d, meta["ncut"], meta["neq"], "mixed", d["tx"], d["ty"])
+    F.status()
+    assert np.isfinite(us).all() and np.isfinite(ut).all()
+    es = rel_l2(us[g["src_idx"]], g["direct_src"])
+    et = rel_l2(ut[g["tgt_idx"]], g["direct_tgt"])
+    assert es < BAR and et < BAR, (es, et)
+    # the reference at Nequiv 24 is itself ~2e-7 from the direct sum
+    assert rel_l2(us[g["src_idx"]], g["src_val"]) < BAR
+    assert rel_l2(ut[g["tgt_idx"]], g["tgt_val"]) < BAR
+
+
 def test_mixed_coincident_points_are_skipped_exactly(built_lib):
     """Duplicated sources: the FP32 path must still skip exactly the coincident pairs."""
     from conftest import golden_inputs, load_golden

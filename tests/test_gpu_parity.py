@@ -46,6 +46,46 @@ def test_tree_matches_oracle(built_lib, case):
     assert canon.compare(a, b) == []
 
 
+@pytest.mark.parametrize("case", [c for c in golden_cases() if "tree_sha_nonempty" in load_golden(c)])
+def test_tree_matches_reference_at_scale(built_lib, case):
+    """100k uniform and 1M clustered sources: the device tree, canonically,
+    against digests of the reference's own tree (flexmm/tree.py:451-518) --
+    box positions and flags, the leaf of every source, colleague sets and
+    interaction lists, level by level."""
+    import hashlib
+    g = load_golden(case)
+    meta = g["meta"]
+    d = golden_inputs(meta)
+    F = _fmm(d, meta)
+    assert np.array_equal(np.array(F.bbox), g["bbox_used"])
+    assert F.tree.levels == int(g["levels"])
+    c = canon.canonical(F.tree, triples_fn=canon.gpu_triples, nonempty_sources=True)
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(np.asarray(a, dtype=np.int64)).tobytes()).hexdigest()
+    got = {k: sha(v) for k, v in c.items()}
+    ref = g["tree_sha_nonempty"]
+    assert set(got) == set(ref)
+    bad = [k for k in ref if got[k] != ref[k]]
+    assert not bad, f"device tree differs from the reference's: {bad}"
+
+
+def test_direct_sum_matches_c_oracle(built_lib):
+    """The library's FP64 direct sum (the accuracy yardstick of the mixed
+    tests) against the oracle's C direct sum, with and without the
+    coincident-pair check, on clustered points with duplicates."""
+    from flexmm_b200 import direct_evaluation, workloads
+    from oracle.direct import direct_laplace
+    d = workloads.clustered(n=30000, n_grid=40, seed=8)
+    x, y, tau = d["x"].copy(), d["y"].copy(), d["tau"]
+    x[1::7], y[1::7] = x[0::7][: x[1::7].size], y[0::7][: y[1::7].size]
+    rng = np.random.default_rng(2)
+    si = rng.choice(x.size, 1500, replace=False)
+    for tx, ty, check in ((x[si], y[si], True), (d["tx"], d["ty"], False)):
+        got = np.asarray(direct_evaluation("Laplace_Eval", x, y, tau, tx, ty, check=check))
+        ref = direct_laplace(x, y, tau, tx, ty, check)
+        assert np.isfinite(got).all()
+        assert rel_l2(got, ref) < 1e-13
+
+
 def _descent_lines(p, x0, w0, levels):
     """The midpoints the reference's descent compares point p with, level by
     level (FP64, the same recurrence: xm = xmin + w/2)."""

@@ -31,6 +31,24 @@ def test_oracle_tree_matches_reference_tree(case):
     assert not bad, f"canonical tree fields differ from the reference: {bad}"
 
 
+LARGE = [c for c in golden_cases() if "tree_sha_nonempty" in load_golden(c)]
+
+
+@pytest.mark.parametrize("case", LARGE)
+def test_oracle_tree_matches_reference_tree_at_scale(case):
+    """100k uniform and 1M clustered: the oracle's tree against the digests
+    of the reference's own tree (interactions from empty boxes left out)."""
+    g = load_golden(case)
+    d = golden_inputs(g["meta"])
+    t = Tree(d["x"], d["y"], g["meta"]["ncut"], list(g["bbox_used"]))
+    assert t.levels == int(g["levels"])
+    got = {k: sha(v) for k, v in canon.canonical(t, nonempty_sources=True).items()}
+    ref = g["tree_sha_nonempty"]
+    assert set(got) == set(ref)
+    bad = [k for k in ref if got[k] != ref[k]]
+    assert not bad, f"canonical tree fields differ from the reference: {bad}"
+
+
 @pytest.mark.parametrize("case", [c for c in SMALL if load_golden(c)["meta"].get("method") != "bb"])
 def test_oracle_results_match_reference(case):
     g = load_golden(case)
