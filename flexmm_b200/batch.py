@@ -80,10 +80,12 @@ class StokesBatch:
         torch = _torch()
         if len(forces) != len(self):
             raise ValueError(f"expected {len(self)} force pairs, got {len(forces)}")
+        self._enter()
         outs = []
         for k, (F, (fx, fy)) in enumerate(zip(self._stokes, forces)):
-            with torch.cuda.stream(self._stream(k)):
-                F.build_expansions(_device(fx), _device(fy))
+            s = self._stream(k)
+            with torch.cuda.stream(s):
+                F.build_expansions(_device(fx, s), _device(fy, s))
                 o = self._own_stokes(F, F.N)
                 outs.append((o[0], o[1], o[2]))
         self._join(outs)
@@ -96,17 +98,28 @@ class StokesBatch:
             raise RuntimeError("built with adjoint=False")
         if len(cotangents) != len(self):
             raise ValueError(f"expected {len(self)} cotangent triples, got {len(cotangents)}")
+        self._enter()
         outs = []
         for k, (F, L, (gu, gv, gp), (xd, yd)) in enumerate(
                 zip(self._stokes, self._laplace, cotangents, self._pts)):
-            with torch.cuda.stream(self._stream(k)):
-                F.build_expansions(_device(gu), _device(gv))
+            s = self._stream(k)
+            with torch.cuda.stream(s):
+                F.build_expansions(_device(gu, s), _device(gv, s))
                 vel = self._own_stokes(F, F.N)
-                L.build_expansions(_device(gp))
+                L.build_expansions(_device(gp, s))
                 grad = L.evaluate_to_points(xd, yd, "gradient", True)
                 outs.append((vel[0] + grad[1], vel[1] + grad[2]))
         self._join(outs)
         return outs
+
+    def _enter(self):
+        """Every batch stream waits for the caller's stream, so inputs the
+        caller produced on the GPU just before the call are complete when the
+        batch streams read them."""
+        torch = _torch()
+        cur = torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(cur)
 
     def _join(self, outs):
         """The caller's stream waits for every batch stream, and the results
@@ -127,8 +140,16 @@ class StokesBatch:
                 L.status()
 
 
-def _device(a):
+def _device(a, stream):
+    """A contiguous float64 CUDA tensor of ``a`` for use on ``stream`` (the
+    current stream inside the caller's ``torch.cuda.stream`` block).  A CUDA
+    tensor the caller passed in is marked as used on that stream, so the
+    caching allocator does not hand its memory out again before the batch
+    stream has read it, even if the caller drops it right after the call."""
     torch = _torch()
     if isinstance(a, torch.Tensor):
-        return a.to(device="cuda", dtype=torch.float64).contiguous()
+        t = a.to(device="cuda", dtype=torch.float64).contiguous()
+        if t.is_cuda and a.is_cuda:
+            t.record_stream(stream)
+        return t
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()

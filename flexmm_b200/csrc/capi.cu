@@ -1229,9 +1229,13 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
     a.ops_dev = p->ops_dev.get();
     const uint64_t *tkeys = nullptr;
     const int *tperm = nullptr;
-    sort_points_scratch(tx, ty, m, p->th, k0, k1, i0, i1, sort_tmp, sort_bytes, &tkeys, &tperm, s);
-    gather_sorted(tx, tperm, m, txs, s);
-    gather_sorted(ty, tperm, m, tys, s);
+    {
+      PhaseTimer timer(PH_SORT_TGT, s);
+      sort_points_scratch(tx, ty, m, p->th, k0, k1, i0, i1, sort_tmp, sort_bytes, &tkeys, &tperm,
+                          s);
+      gather_sorted(tx, tperm, m, txs, s);
+      gather_sorted(ty, tperm, m, tys, s);
+    }
     run_evaluate_scratch(a, p->tau_s.get(), p->loc.get(), txs, tys, tkeys, tperm, m, check, out, tb,
                          te, nch, choff, items, n_items, scan_tmp, scan_bytes, s);
   });

@@ -35,6 +35,8 @@ constexpr int TN = 32;      // nodes per upward / downward tile
 constexpr int TM = 64;      // targets per M2L tile
 constexpr int NT = 256;     // threads per tile CTA
 constexpr int TCH = 128;    // targets per evaluation work item (= threads)
+// callers size the work-item array as total + m / EVAL_CHUNK + 1 entries
+static_assert(TCH == EVAL_CHUNK, "evaluation work items hold EVAL_CHUNK targets");
 constexpr int SMAX = 1024;  // sources staged per evaluation pass
 
 // the 27 offsets a target can see, by its parity class 2*(ix&1) + (iy&1)
@@ -839,13 +841,16 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), tb, te, nch, choff,
                                                     items, n_items);
   FMMB_CUDA(cudaGetLastError());
+  PhaseTimer timer(PH_EVAL, s);
+  auto launch = [&](auto kern) {
+    kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(),
+                                 td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
+                                 td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0);
+  };
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE:
-      k_evaluate<LaplaceF64, 1><<<148 * 8, TCH, 0, s>>>(
-          a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(), td.top.get(),
-          td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc, txs, tys,
-          tperm, check, out, 0);
-      break;
+    case KERNEL_LAPLACE: launch(k_evaluate<LaplaceF64, 1>); break;
+    case KERNEL_MOD_HELMHOLTZ: launch(k_evaluate<ModHelmholtzF64, 1>); break;
+    case KERNEL_RADIAL_TABLE: launch(k_evaluate<RadialTableF64, 1>); break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
   FMMB_CUDA(cudaGetLastError());

@@ -170,11 +170,13 @@ class KI_Helper:
 
     ``cache_dir`` (or the environment variable FLEXMM_B200_CACHE) keeps the
     host operators on disk across processes, one .npz file per width under a
-    directory named by (kernel, parameters, Nequiv, format version): the
-    helper loads them when it is bound to its kernel (so bbox snapping sees
-    those widths, as for a helper that already met them) and writes every
-    width it forms.  Tabulated kernels (``radial``) are not cached on disk:
-    their identity is not in their parameters."""
+    directory named by (kernel, parameters, Nequiv, format version): a width
+    the helper needs is read from there instead of formed, and every width it
+    forms is written there.  Files are read only when their width is asked
+    for, so bbox snapping sees the widths met in this process alone, as in
+    the reference (the tree, and so the results, never depend on what an
+    earlier run left on disk).  Tabulated kernels (``radial``) are not cached
+    on disk: their identity is not in their parameters."""
 
     def __init__(self, helper=None, cache_dir=None):
         self.kernel = None
@@ -190,7 +192,6 @@ class KI_Helper:
         if self.kernel is None:
             self.kernel = kernel
             self.nequiv = nequiv
-            self._load_disk_cache()
         elif self.kernel.key != kernel.key or self.nequiv != nequiv:
             raise ValueError(f"helper holds operators for {self.kernel} with Nequiv={self.nequiv}; "
                              f"got {kernel} with Nequiv={nequiv}")
@@ -202,30 +203,29 @@ class KI_Helper:
         tag = repr((self.kernel.key, int(self.nequiv), CACHE_VERSION)).encode()
         return os.path.join(self.cache_dir, "ki_" + hashlib.sha1(tag).hexdigest()[:20])
 
-    def _load_disk_cache(self):
+    def _disk_path(self, key):
         d = self._disk_dir()
-        if d is None or not os.path.isdir(d):
-            return
-        for name in sorted(os.listdir(d)):
-            if not name.endswith(".npz"):
-                continue
-            try:
-                with np.load(os.path.join(d, name)) as z:
-                    pre = KIPrecomputation.from_arrays({k: z[k] for k in z.files})
-            except (OSError, KeyError, ValueError):
-                continue  # a damaged or foreign file: that width is formed again
-            if pre.c2e_u.shape[0] == self.nequiv:
-                self.precomputations.setdefault(width_key(pre.width), pre)
+        return None if d is None else os.path.join(d, f"w_{key!r}.npz")
+
+    def _load_disk(self, key):
+        """The operators of one width from the disk cache, or None (absent,
+        damaged, half-written by a crashed writer, or for another Nequiv)."""
+        path = self._disk_path(key)
+        if path is None or not os.path.isfile(path):
+            return None
+        try:
+            with np.load(path) as z:
+                pre = KIPrecomputation.from_arrays({k: z[k] for k in z.files})
+        except Exception:
+            return None  # that width is formed again
+        if pre.c2e_u.shape[0] != self.nequiv or width_key(pre.width) != key:
+            return None
+        return pre
 
     def _save_disk(self, key, pre):
-        d = self._disk_dir()
-        if d is None:
-            return
-        os.makedirs(d, exist_ok=True)
-        path = os.path.join(d, f"w_{key!r}.npz")
-        tmp = f"{path}.{os.getpid()}.tmp.npz"
-        np.savez(tmp, **pre.to_arrays())
-        os.replace(tmp, path)  # atomic: readers see the whole file or none
+        path = self._disk_path(key)
+        if path is not None:
+            save_npz_atomic(path, pre.to_arrays())
 
     def ops_set(self):
         if self._ops is None:
@@ -255,9 +255,11 @@ class KI_Helper:
         (and then written to the disk cache)."""
         key = width_key(width)
         if key not in self.precomputations:
-            pre = KIPrecomputation(width, self.nequiv, self.kernel)
+            pre = self._load_disk(key)
+            if pre is None:
+                pre = KIPrecomputation(width, self.nequiv, self.kernel)
+                self._save_disk(key, pre)
             self.precomputations[key] = pre
-            self._save_disk(key, pre)
         return self.precomputations[key]
 
     def level_id(self, width):
@@ -269,6 +271,27 @@ class KI_Helper:
 
     def get_precomputation(self, width):
         return self.precomputations[width_key(width)]
+
+
+def save_npz_atomic(path, arrays):
+    """Write ``arrays`` to ``path`` (.npz) so that readers see the whole file or
+    none: the data goes to a uniquely named temporary file in the same
+    directory (a name no reader takes for a cache file), then replaces the
+    target in one rename."""
+    import tempfile
+    d = os.path.dirname(path)
+    os.makedirs(d, exist_ok=True)
+    fd, tmp = tempfile.mkstemp(dir=d, prefix=".w_", suffix=".tmp")
+    try:
+        with os.fdopen(fd, "wb") as f:
+            np.savez(f, **arrays)
+        os.replace(tmp, path)
+    except BaseException:
+        try:
+            os.unlink(tmp)
+        except OSError:
+            pass
+        raise
 
 
 _DEFAULT_HELPERS = {}

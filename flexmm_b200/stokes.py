@@ -190,14 +190,12 @@ def stokes_precomputation(width, nequiv, cache_dir=None):
                 pre = StokesPrecomputation.from_arrays({k: z[k] for k in z.files})
             if pre.Nequiv == nequiv and width_key(pre.width) == width_key(width):
                 return pre
-        except (OSError, KeyError, ValueError):
-            pass  # absent or damaged: formed again below
+        except Exception:
+            pass  # absent, damaged or half-written: formed again below
     pre = StokesPrecomputation(width, nequiv)
     if path:
-        os.makedirs(os.path.dirname(path), exist_ok=True)
-        tmp = f"{path}.{os.getpid()}.tmp.npz"
-        np.savez(tmp, **pre.to_arrays())
-        os.replace(tmp, path)  # atomic: readers see the whole file or none
+        from .helpers import save_npz_atomic
+        save_npz_atomic(path, pre.to_arrays())
     return pre
 
 

@@ -246,8 +246,12 @@ int fmm_timing_read(double *ms /* [FMM_N_PHASES] */, int64_t *launches /* [FMM_N
 /* Allocation-free fmm_evaluate, for callers that cannot allocate device
  * memory at evaluation time: e.g. an application that has reserved the whole
  * GPU for its own pool, or a loop that must not touch the allocator.  It has
- * no counterpart in the reference.  It computes exactly what fmm_evaluate
- * computes, with the plan built and expanded beforehand; its scratch is a
+ * no counterpart in the reference.  It serves FP64 KIFMM plans (Laplace,
+ * modified Helmholtz and tabulated radial kernels; the potential, one value
+ * per target) and refuses mixed-precision, black-box and Stokes plans with
+ * FMM_ERR_UNSUPPORTED before queueing any work.  For the plans it serves it
+ * computes what fmm_evaluate computes, with the plan built and expanded
+ * beforehand; its scratch is a
  * 24 MiB array inside the library (held on every GPU that loads it until
  * exit), shared by all calls and keeping the last call's contents.  Calls
  * that overlap on the GPU race on it: serialise them.  The first call on a

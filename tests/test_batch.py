@@ -90,3 +90,29 @@ def test_stokes_batch_adjoint_matches_direct_adjoint(built_lib):
     again = B.forward(forces)
     torch.cuda.synchronize()
     assert all(np.isfinite(t.cpu().numpy()).all() for tup in again for t in tup)
+
+
+@pytest.mark.gpu
+def test_stokes_batch_reads_forces_made_on_the_callers_stream(built_lib):
+    """Forces produced by GPU kernels on the caller's stream immediately before
+    the call (and dropped right after it): the batch streams wait for them."""
+    import torch
+    from flexmm_b200.batch import StokesBatch
+    probs, forces, _ = _problems(seed=5)
+    B = StokesBatch(probs, Nequiv=32, Ncutoff=64, n_streams=4)
+    ref = B.forward(forces)
+    torch.cuda.synchronize()
+    ref = [[t.cpu().numpy() for t in tup] for tup in ref]
+    big = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")
+    dev = []
+    for fx, fy in forces:
+        big.normal_()  # keeps the caller's stream busy ahead of the copies below
+        a = torch.from_numpy(fx).cuda(non_blocking=True) * 2.0 - torch.from_numpy(fx).cuda()
+        b = torch.from_numpy(fy).cuda() + 0.0
+        dev.append((a, b))
+    outs = B.forward(dev)
+    del dev
+    torch.cuda.synchronize()
+    for k in range(len(probs)):
+        for r in range(3):
+            assert rel_l2(outs[k][r].cpu().numpy(), ref[k][r]) < 1e-14, (k, r)

@@ -35,15 +35,48 @@ def test_disk_cache_is_written_and_loaded_by_a_new_helper(tmp_path):
     formed = [h1.precomputation(w) for w in widths]
     files = [f for d in os.listdir(tmp_path) for f in os.listdir(tmp_path / d)]
     assert len(files) == len(widths) and all(f.endswith(".npz") for f in files)
-    # a new helper (a new process, say) loads them when bound to the kernel
+    # a new helper (a new process, say) snaps a bbox like a fresh reference
+    # helper -- the widths on disk play no part -- and reads a width from
+    # disk when it needs it, without forming it
     h2 = KI_Helper(cache_dir=str(tmp_path))
     h2.attach(k, 24)
-    assert sorted(h2.precomputations) == sorted(width_key(w) for w in widths)
-    for w, pre in zip(widths, formed):
-        _same(h2.precomputation(w), pre)
-    # and snaps a bbox to those widths like the helper that formed them
+    assert h2.precomputations == {}
     bb = [-0.9, 0.8, -0.7, 0.95]
+    assert h2.get_bbox(None, None, bb) == KI_Helper().get_bbox(None, None, bb)
+    real_init = KIPrecomputation.__init__
+
+    def refuse(*args, **kwargs):
+        raise AssertionError("formed again instead of read from the cache")
+    KIPrecomputation.__init__ = refuse
+    try:
+        for w, pre in zip(widths, formed):
+            _same(h2.precomputation(w), pre)
+    finally:
+        KIPrecomputation.__init__ = real_init
+    assert sorted(h2.precomputations) == sorted(width_key(w) for w in widths)
+    # and then snaps like the helper that formed them
     assert h2.get_bbox(None, None, bb) == h1.get_bbox(None, None, bb)
+
+
+def test_disk_cache_skips_temporary_and_truncated_files(tmp_path):
+    """A writer's temporary file, or a truncated cache file left by a crash,
+    never breaks a helper: the width is formed again."""
+    k = resolve("Laplace_Eval")
+    h1 = KI_Helper(cache_dir=str(tmp_path))
+    h1.attach(k, 24)
+    good = h1.precomputation(0.25)
+    d = next(tmp_path.iterdir())
+    f = next(p for p in d.iterdir() if p.name.endswith(".npz"))
+    data = f.read_bytes()
+    (d / ".w_123.tmp").write_bytes(data[: len(data) // 2])
+    f.write_bytes(data[: len(data) // 3])   # a truncated zip
+    h2 = KI_Helper(cache_dir=str(tmp_path))
+    h2.attach(k, 24)
+    _same(h2.precomputation(0.25), good)
+    # the width formed again is written back whole
+    h3 = KI_Helper(cache_dir=str(tmp_path))
+    h3.attach(k, 24)
+    assert h3._load_disk(width_key(0.25)) is not None
 
 
 def test_disk_cache_keeps_kernels_and_nequiv_apart(tmp_path):
@@ -54,14 +87,14 @@ def test_disk_cache_keeps_kernels_and_nequiv_apart(tmp_path):
     for kern, neq in ((lap, 32), (mh, 24)):
         b = KI_Helper(cache_dir=str(tmp_path))
         b.attach(kern, neq)
-        assert b.precomputations == {}
+        assert b._load_disk(width_key(0.25)) is None
     # a damaged file is skipped, and that width is formed again
     d = next(tmp_path.iterdir())
     f = next(d.iterdir())
     f.write_bytes(b"not an npz file")
     c = KI_Helper(cache_dir=str(tmp_path))
     c.attach(lap, 24)
-    assert c.precomputations == {}
+    assert c._load_disk(width_key(0.25)) is None
     _same(c.precomputation(0.25), KIPrecomputation(0.25, 24, lap))
 
 

@@ -54,6 +54,34 @@ def test_noalloc_matches_fmm_evaluate_twice(built_lib):
         assert rel_l2(got, want) < TOL
 
 
+def test_noalloc_modified_helmholtz_and_refused_forms(built_lib):
+    """Every FP64 KIFMM kernel goes through the allocation-free route (here
+    the modified Helmholtz kernel, two calls in a row); a mixed-precision plan
+    is refused before any work, with status 5 (unsupported)."""
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, _lib, workloads
+    lib = _lib.load()
+    d = workloads.uniform(n=30_000, n_grid=10, seed=33)
+    F = KI_FMM(d["x"], d["y"], "Modified_Helmholtz_Eval", 64, 24, bbox=d["bbox"],
+               helper=KI_Helper(), helmholtz_k=5.0)
+    F.build_expansions(d["tau"])
+    rng = np.random.default_rng(8)
+    for n in (20_000, 7_000):
+        txd = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+        tyd = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+        want = _eval(lib, "fmm_evaluate", F._plan, txd, tyd, 0)
+        got = _eval(lib, "fmm_evaluate_noalloc", F._plan, txd, tyd, 0)
+        assert np.isfinite(got).all()
+        assert rel_l2(got, want) < TOL
+    M = KI_FMM(d["x"], d["y"], "Laplace_Eval", 64, 24, bbox=d["bbox"], helper=KI_Helper(),
+               precision="mixed")
+    M.build_expansions(d["tau"])
+    t = torch.zeros(4, dtype=torch.float64, device="cuda")
+    rc = lib.fmm_evaluate_noalloc(M._plan, ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(t.data_ptr()),
+                                  4, 0, ctypes.c_void_p(t.data_ptr()), None)
+    assert rc == 5 and b"FP64" in lib.fmm_last_error()
+
+
 def test_noalloc_refuses_oversized_requests(built_lib):
     import torch
     from flexmm_b200 import KI_FMM, KI_Helper, _lib, workloads
