@@ -1103,6 +1103,16 @@ int fmm_direct(int kernel_id, const double *kparams, const double *sx, const dou
   });
 }
 
+int fmm_diag_log2(const double *x, int64_t n, double *out_table, double *out_library,
+                  void *stream) {
+  return guarded([&] {
+    FMMB_CHECK(n >= 0, ERR_INVALID_ARGUMENT, "negative size");
+    if (n == 0) return;
+    FMMB_CHECK(x && out_table && out_library, ERR_INVALID_ARGUMENT, "NULL argument");
+    run_diag_log2(x, n, out_table, out_library, (cudaStream_t)stream);
+  });
+}
+
 int fmm_timing_enable(int on) {
   return guarded([&] {
     auto &R = TimingRegistry::get();

@@ -37,7 +37,8 @@ constexpr int NT = 256;     // threads per tile CTA
 constexpr int TCH = 128;    // targets per evaluation work item (= threads)
 // callers size the work-item array as total + m / EVAL_CHUNK + 1 entries
 static_assert(TCH == EVAL_CHUNK, "evaluation work items hold EVAL_CHUNK targets");
-constexpr int SMAX = 1024;  // sources staged per evaluation pass
+constexpr int SMAX = 896;   // sources staged per evaluation pass (8 blocks of 128 per SM
+                            // with the log2 table beside them)
 
 // the 27 offsets a target can see, by its parity class 2*(ix&1) + (iy&1)
 // (offset ids walk ox = -3..3 outer, oy = -3..3 inner, skipping (-1..1)^2)
@@ -46,6 +47,15 @@ __constant__ int8_t c_class_off[4][27] = {
     {7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31, 33, 34, 35, 36, 37, 38},
     {1, 2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32},
     {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31}};
+
+// the factor a kernel's loops fold into their staged charges and locals
+template <class KF, bool kFolded>
+__device__ __forceinline__ double fold_of() {
+  if constexpr (kFolded)
+    return KF::kFold;
+  else
+    return 1.0;
+}
 
 // ---------------------------------------------------------------- upward ----
 // One tile = 32 consecutive nodes of level m.
@@ -67,7 +77,9 @@ __global__ void __launch_bounds__(NT) k_upward(int m, KernelParams kp, int neq, 
   double *P = smem;           // [TN][ldp]  check potentials
   double *A = P + TN * ldp;   // [TN][lda]  children multipoles; later C2E scratch
   __shared__ double *orow[TN];
-  const KF K(kp);
+  __shared__ FunctorSmem<KF> fsm;
+  KF K(kp);
+  fsm.bind(K);
   const LevelOpsDev &op = ops[m];
   const int g0 = g_begin + blockIdx.x * TN;
   const int nloc = min(TN, g_end - g0);
@@ -357,7 +369,13 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
   __shared__ double ssx[SMAX], ssy[SMAX], stau[SMAX];
   __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
   __shared__ double red[NOUT][TCH / 32];
-  const KF K(kp);
+  __shared__ FunctorSmem<KF> fsm;
+  KF K(kp);
+  fsm.bind(K);
+  // table-driven Laplace (potential only): the kernel's constant factor is
+  // folded into the staged locals and charges, the loops sum raw log2 values
+  constexpr bool kFolded = KF::kLogTable && NOUT == 1;
+  const double fold = fold_of<KF, kFolded>();
   const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int4 it = items[item];
@@ -376,7 +394,7 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     // L2T (flexmm/flexmm2d/kifmm.py:106-120); locals of levels 0-1 are zero
     if (lev >= 2)
       for (int k = threadIdx.x; k < neq; k += TCH) {
-        Ls[k] = loc[(size_t)g * np + k];
+        Ls[k] = loc[(size_t)g * np + k] * fold;
         lxs[k] = ops[lev].lx[k];
         lys[k] = ops[lev].ly[k];
       }
@@ -388,14 +406,20 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     if (lev >= 2 && valid) {
       const double dx = x - xmid[g], dy = y - ymid[g];
       if constexpr (NOUT == 1) {
+        auto kv = [&](int k) -> double {
+          if constexpr (kFolded)
+            return K.raw(dx - lxs[k], dy - lys[k]);
+          else
+            return K(lxs[k], lys[k], dx, dy);
+        };
         int k = sub;
         for (; k + 3 * G < neq; k += 4 * G) {
-          u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
-          u1 = fma(K(lxs[k + G], lys[k + G], dx, dy), Ls[k + G], u1);
-          u2 = fma(K(lxs[k + 2 * G], lys[k + 2 * G], dx, dy), Ls[k + 2 * G], u2);
-          u3 = fma(K(lxs[k + 3 * G], lys[k + 3 * G], dx, dy), Ls[k + 3 * G], u3);
+          u0 = fma(kv(k), Ls[k], u0);
+          u1 = fma(kv(k + G), Ls[k + G], u1);
+          u2 = fma(kv(k + 2 * G), Ls[k + 2 * G], u2);
+          u3 = fma(kv(k + 3 * G), Ls[k + 3 * G], u3);
         }
-        for (; k < neq; k += G) u0 = fma(K(lxs[k], lys[k], dx, dy), Ls[k], u0);
+        for (; k < neq; k += G) u0 = fma(kv(k), Ls[k], u0);
       } else {
         for (int k = sub; k < neq; k += G) K.grad(lxs[k], lys[k], dx, dy, Ls[k], gu, gx, gy);
       }
@@ -405,8 +429,12 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     // a coincident pair is skipped when check is set (helpers.py:99-107)
     auto pair = [&](int j) -> double {
       const double qx = ssx[j], qy = ssy[j];
-      const double v = K(qx, qy, x, y) * stau[j];
-      return (check && x - qx == 0.0 && y - qy == 0.0) ? 0.0 : v;
+      if constexpr (kFolded) {
+        return K.raw_checked(qx, qy, x, y, check) * stau[j];
+      } else {
+        const double v = K(qx, qy, x, y) * stau[j];
+        return (check && x - qx == 0.0 && y - qy == 0.0) ? 0.0 : v;
+      }
     };
     const int ns = rs[9];
     for (int base = 0; base < ns; base += SMAX) {
@@ -418,7 +446,7 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
         const int j = rb[c] + (idx - rs[c]);
         ssx[i] = sx[j];
         ssy[i] = sy[j];
-        stau[i] = tau[j];
+        stau[i] = tau[j] * fold;
       }
       __syncthreads();
       if (valid) {
@@ -496,7 +524,9 @@ __global__ void __launch_bounds__(TCH) k_evaluate_multi(KernelParams kp, int neq
   __shared__ double ssx[SMAX_MR], ssy[SMAX_MR], stau[R][SMAX_MR];
   __shared__ int rb[9], rs[10];
   __shared__ double red[R][TCH / 32];
-  const KF K(kp);
+  __shared__ FunctorSmem<KF> fsm;
+  KF K(kp);
+  fsm.bind(K);
   const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int4 it = items[item];
@@ -683,7 +713,7 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
 
 void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s) {
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE: upward_impl<LaplaceF64>(a, tau_s, mult, s); break;
+    case KERNEL_LAPLACE: upward_impl<LaplaceF64T>(a, tau_s, mult, s); break;
     case KERNEL_MOD_HELMHOLTZ: upward_impl<ModHelmholtzF64>(a, tau_s, mult, s); break;
     case KERNEL_RADIAL_TABLE: upward_impl<RadialTableF64>(a, tau_s, mult, s); break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
@@ -736,7 +766,8 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
   if (m == 0) return;
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
-      evaluate_impl<LaplaceF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out, ld_out, s);
+      evaluate_impl<LaplaceF64T>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out, ld_out,
+                                 s);
       break;
     case KERNEL_MOD_HELMHOLTZ:
       evaluate_impl<ModHelmholtzF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
@@ -781,7 +812,7 @@ void run_evaluate_multi(const PassArgs &a, const double *tau_s, int64_t n_src, i
   if (m == 0 || n_rhs == 0) return;
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
-      evaluate_multi_impl<LaplaceF64>(a, tau_s, n_src, n_rhs, loc, col_stride, txs, tys, tkeys,
+      evaluate_multi_impl<LaplaceF64T>(a, tau_s, n_src, n_rhs, loc, col_stride, txs, tys, tkeys,
                                       tperm, m, check, out, ld_out, s);
       break;
     case KERNEL_MOD_HELMHOLTZ:
@@ -848,11 +879,32 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
                                  td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0);
   };
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE: launch(k_evaluate<LaplaceF64, 1>); break;
+    case KERNEL_LAPLACE: launch(k_evaluate<LaplaceF64T, 1>); break;
     case KERNEL_MOD_HELMHOLTZ: launch(k_evaluate<ModHelmholtzF64, 1>); break;
     case KERNEL_RADIAL_TABLE: launch(k_evaluate<RadialTableF64, 1>); break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
+  FMMB_CUDA(cudaGetLastError());
+}
+
+namespace {
+__global__ void k_diag_log2(const double *__restrict__ x, int64_t n, double *__restrict__ out_tab,
+                            double *__restrict__ out_lib) {
+  __shared__ FunctorSmem<LaplaceF64T> fsm;
+  LaplaceF64T K(KernelParams{});
+  fsm.bind(K);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double d = x[i];
+    out_tab[i] = log2_tab_rare(d) ? log2(d) : log2_tab(d, K.lt);
+    out_lib[i] = log2(d);
+  }
+}
+}  // namespace
+
+void run_diag_log2(const double *x, int64_t n, double *out_tab, double *out_lib, cudaStream_t s) {
+  if (n == 0) return;
+  k_diag_log2<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(x, n, out_tab, out_lib);
   FMMB_CUDA(cudaGetLastError());
 }
 

@@ -114,6 +114,8 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
                 const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
                 int check, double *out, cudaStream_t s);
 void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaStream_t s);
+// the FP64 passes' table-driven log2 and the library log2 at n device points
+void run_diag_log2(const double *x, int64_t n, double *out_tab, double *out_lib, cudaStream_t s);
 // nout = 1: potential into out[m]; nout = 3: potential and its gradient in the
 // target position into out[0..2][m] (row stride ld_out)
 void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc,

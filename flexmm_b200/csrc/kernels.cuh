@@ -28,7 +28,71 @@ struct KernelParams {
   const double *table;
 };
 
+// ---------------------------------------------------------------------------
+// Table-driven FP64 log2, after P. T. P. Tang, "Table-driven implementation
+// of the logarithm function in IEEE floating-point arithmetic", ACM TOMS 16
+// (1990): d = 2^e m, m in [1, 2); F = 1 + j/256 is the table point nearest m,
+// so r = (m - F) / F has |r| <= 2^-9 and
+//   log2 d = e + log2 F + log2(1 + r),
+//   log2(1 + r) = r (c1 + r (c2 + r (c3 + r (c4 + r c5)))),  c_k = (-1)^(k+1) / (k ln 2),
+// the Taylor series of log(1 + r) / ln 2 cut after r^5 (the first dropped
+// term, r^6 / (6 ln 2), is below 1.3e-17).  m - F is exact; the table holds
+// 1/F (IEEE division) and log2 F (CUDA's log2) for j = 0..256, filled in
+// shared memory by each block.  Absolute error about one ulp of the result
+// (~1e-16 relative to max(1, |log2 d|)): far inside the 1e-12 parity bar,
+// at about a third of the FP64 instructions of the library log.  Zero,
+// subnormal, infinite and NaN arguments take the library log2 instead.
+constexpr int LOG2_TAB_N = 256;
+struct Log2Table {
+  double2 t[LOG2_TAB_N + 1];
+  __device__ void fill() {
+    for (int i = threadIdx.x; i <= LOG2_TAB_N; i += blockDim.x) {
+      const double F = 1.0 + i * (1.0 / LOG2_TAB_N);
+      t[i] = make_double2(1.0 / F, log2(F));
+    }
+  }
+};
+
+// true for arguments outside the table path: zero, subnormal, negative,
+// infinite or NaN (one unsigned compare of the high word)
+__device__ __forceinline__ bool log2_tab_rare(double d) {
+  return (unsigned)(__double2hiint(d) - 0x00100000) >= 0x7FE00000u;
+}
+
+// log2 of a positive normal finite d (callers route log2_tab_rare arguments
+// elsewhere)
+__device__ __forceinline__ double log2_tab(double d, const double2 *__restrict__ tab) {
+  constexpr double LN2 = 0.69314718055994530942;
+  constexpr double C1 = 1.0 / LN2, C2 = -1.0 / (2.0 * LN2), C3 = 1.0 / (3.0 * LN2),
+                   C4 = -1.0 / (4.0 * LN2), C5 = 1.0 / (5.0 * LN2);
+  const int hi = __double2hiint(d), lo = __double2loint(d);
+  const int mh = hi & 0x000FFFFF;
+  const int j = (mh + (1 << 11)) >> 12;                           // nearest 1/256 step: 0..256
+  const double m = __hiloint2double(mh | 0x3FF00000, lo);         // [1, 2)
+  const double F = __hiloint2double(0x3FF00000 + (j << 12), 0);   // 1 + j/256 (j = 256: 2)
+  const double2 tj = tab[j];
+  const double r = (m - F) * tj.x;
+  // the exponent as a double without a conversion instruction:
+  // bits (0x43300000, e + 2^31) are 2^52 + 2^31 + e
+  const double e = __hiloint2double(0x43300000, ((hi >> 20) - 1023) ^ (int)0x80000000) -
+                   4503601774854144.0;
+  double q = fma(r, C5, C4);
+  q = fma(r, q, C3);
+  q = fma(r, q, C2);
+  q = fma(r, q, C1);
+  return fma(r, q, e + tj.y);
+}
+
+// Shared-memory state a functor needs inside a kernel (the log2 table of
+// LaplaceF64T); empty for the other functors.  bind() is called by every
+// thread of the block before the functor's first use.
+template <class KF, bool = KF::kLogTable>
+struct FunctorSmem {
+  __device__ void bind(KF &) {}
+};
+
 struct LaplaceF64 {
+  static constexpr bool kLogTable = false;
   __host__ __device__ explicit LaplaceF64(const KernelParams &) {}
   __device__ __forceinline__ double operator()(double sx, double sy, double tx, double ty) const {
     const double dx = tx - sx, dy = ty - sy;
@@ -46,7 +110,52 @@ struct LaplaceF64 {
   }
 };
 
+// The Laplace kernel of the FP64 passes: LaplaceF64 with the table-driven
+// log2 above.  raw(dx, dy) = log2(dx^2 + dy^2), so K = kFold * raw; the P2P
+// and L2T loops fold kFold into their staged charges / locals.
+struct LaplaceF64T {
+  static constexpr bool kLogTable = true;
+  static constexpr double kFold = -0.69314718055994530942 / (4.0 * M_PI);  // -ln2 / (4 pi)
+  const double2 *lt = nullptr;  // the block's table (FunctorSmem::bind)
+  __host__ __device__ explicit LaplaceF64T(const KernelParams &) {}
+  __device__ __forceinline__ double raw(double dx, double dy) const {
+    const double d2 = dx * dx + dy * dy;
+    return log2_tab_rare(d2) ? log2(d2) : log2_tab(d2, lt);
+  }
+  // raw value of a P2P pair, 0 for a coincident pair when check is set
+  // (flexmm/flexmm2d/helpers.py:99-107): a coincident pair has d2 = 0, so
+  // the test only runs on the rare path
+  __device__ __forceinline__ double raw_checked(double sx, double sy, double tx, double ty,
+                                                int check) const {
+    const double dx = tx - sx, dy = ty - sy, d2 = dx * dx + dy * dy;
+    if (!log2_tab_rare(d2)) return log2_tab(d2, lt);
+    return (check && dx == 0.0 && dy == 0.0) ? 0.0 : log2(d2);
+  }
+  __device__ __forceinline__ double operator()(double sx, double sy, double tx, double ty) const {
+    return kFold * raw(tx - sx, ty - sy);
+  }
+  __device__ __forceinline__ void grad(double sx, double sy, double tx, double ty, double q,
+                                       double &u, double &ux, double &uy) const {
+    const double dx = tx - sx, dy = ty - sy, d2 = dx * dx + dy * dy;
+    const double s = -(1.0 / (2.0 * M_PI)) / d2 * q;
+    u += kFold * raw(dx, dy) * q;
+    ux += s * dx;
+    uy += s * dy;
+  }
+};
+
+template <class KF>
+struct FunctorSmem<KF, true> {
+  Log2Table tab;
+  __device__ void bind(KF &k) {
+    tab.fill();
+    __syncthreads();
+    k.lt = tab.t;
+  }
+};
+
 struct ModHelmholtzF64 {
+  static constexpr bool kLogTable = false;
   double k;
   const double *tab;
   __host__ __device__ explicit ModHelmholtzF64(const KernelParams &kp) : k(kp.p[0]), tab(kp.table) {}
@@ -76,6 +185,7 @@ struct ModHelmholtzF64 {
 // host from any function; the octave grid resolves power-law and log
 // behaviour at 0).  Distances outside the tabulated range are clamped to it.
 struct RadialTableF64 {
+  static constexpr bool kLogTable = false;
   const double *tab;
   int j0, noct, ncheb;
   __host__ __device__ explicit RadialTableF64(const KernelParams &kp)

@@ -264,6 +264,13 @@ int fmm_timing_read(double *ms /* [FMM_N_PHASES] */, int64_t *launches /* [FMM_N
 int fmm_evaluate_noalloc(fmm_plan *plan, const double *tx, const double *ty, int64_t m, int check,
                          double *out, void *stream);
 
+/* Diagnostic: the table-driven log2 that the FP64 passes use for the
+ * Laplace kernel (exponent split, a 257-entry table of 1/F and log2 F,
+ * degree-5 series; Tang, ACM TOMS 16, 1990) and CUDA's log2, at n device
+ * points x, into out_table and out_library.  For tests of its accuracy. */
+int fmm_diag_log2(const double *x, int64_t n, double *out_table, double *out_library,
+                  void *stream);
+
 const char *fmm_last_error(void);
 
 #ifdef __cplusplus
