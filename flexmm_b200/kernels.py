@@ -18,6 +18,8 @@ import numpy as np
 
 
 class Kernel:
+    vector = False   # vector-valued kernels (Stokes) have their own FMM class
+
     def __init__(self, name, kernel_id, params, host):
         self.name = name
         self.kernel_id = kernel_id
@@ -164,8 +166,75 @@ def ModifiedHelmholtz(helmholtz_k):
                   _mod_helmholtz_host)
 
 
+def struve_gf(x):
+    """The Struve Green's function GF(r) = (r (Y1(r) - H_-3(r)) - 4 H_-2(r)) / r^2
+    of examples/bbfmm_struve.py:29-33, from scipy's Bessel and Struve
+    functions.  scipy's struve returns NaN on a few ~3e-5-wide intervals
+    (order -2 near r = 25.8463 and 28.995, order -3 near 27.329); there GF is
+    taken from the cubic through its values at r +- 1e-4 and r +- 2e-4."""
+    from scipy.special import struve, yn
+
+    def gf(v):
+        return (v * (yn(1, v) - struve(-3, v)) - 4 * struve(-2, v)) / v ** 2
+    x = np.asarray(x, dtype=np.float64)
+    out = np.asarray(gf(x), dtype=np.float64)
+    bad = ~np.isfinite(out)
+    if np.any(bad):
+        xb = x[bad]
+        h = 1e-4
+        f = [gf(xb + k * h) for k in (-2, -1, 1, 2)]
+        out[bad] = (-f[0] + 4 * f[1] + 4 * f[2] - f[3]) / 6.0
+    return out
+
+
+_STRUVE = {}
+
+
+def Struve(b=256.0):
+    """The Struve example's kernel ``Kernel`` (examples/bbfmm_struve.py:29-46):
+    GF(|t - s|) tabulated on [1e-30, b] as the example tabulates it with
+    function_generator (there b = 1000; here 256 by default: beyond it scipy's
+    GF loses most of its relative digits to cancellation, |GF| < 1e-11 there,
+    and distances above b are clamped to b).  One table per process and b."""
+    b = float(b)
+    if b not in _STRUVE:
+        _STRUVE[b] = radial(struve_gf, 1e-30, b, tol=1e-5, name="Kernel")
+    return _STRUVE[b]
+
+
+KERNEL_STOKES = 3
+
+
+def _stokes_host(p, sx, sy, tx, ty):
+    """The Stokeslet (u, v, p) rows for unit forces in x and y
+    (kifmm2d/vector/stokes_fmm.py:161-184): [3, 2, ...] = rows (u, v, p) by
+    force component (fx, fy)."""
+    dx = tx - sx
+    dy = ty - sy
+    d2 = dx * dx + dy * dy
+    il = 1.0 / d2
+    lg = -0.5 * np.log(d2)
+    f4 = 1.0 / (4 * np.pi)
+    f2 = 1.0 / (2 * np.pi)
+    return np.array([[f4 * (lg + dx * dx * il), f4 * dx * dy * il],
+                     [f4 * dx * dy * il, f4 * (lg + dy * dy * il)],
+                     [f2 * dx * il, f2 * dy * il]])
+
+
+def Stokes():
+    """The 2D Stokeslet of the reference's Stokes FMM (vector valued: forces
+    (fx, fy) in, (u, v, p) out; kifmm2d/vector/stokes_fmm.py:100-187).  Its
+    FMM is ``flexmm_b200.stokes.FMM``, as in the reference; the scalar FMM
+    classes refuse it."""
+    k = Kernel("Stokes", KERNEL_STOKES, (), _stokes_host)
+    k.vector = True
+    return k
+
+
 _BY_NAME = {"Laplace_Eval": Laplace, "Laplace": Laplace,
-            "Modified_Helmholtz_Eval": ModifiedHelmholtz, "ModifiedHelmholtz": ModifiedHelmholtz}
+            "Modified_Helmholtz_Eval": ModifiedHelmholtz, "ModifiedHelmholtz": ModifiedHelmholtz,
+            "Kernel": Struve, "Struve": Struve,
+            "Stokes": Stokes, "Stokes_Kernel_Form": Stokes}
 # parameters a reference-style kernel function reads from its module's globals
 _GLOBAL_PARAMS = {"Modified_Helmholtz_Eval": ("helmholtz_k",)}
 

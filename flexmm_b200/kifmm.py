@@ -151,6 +151,9 @@ class KI_FMM:
         self.precision = precision
         _lib.load()
         self.kernel = resolve(kernel_eval, **kernel_params)
+        if self.kernel.vector:
+            raise ValueError(f"{self.kernel.name} is vector valued: its FMM is "
+                             "flexmm_b200.stokes.FMM (kifmm2d/vector/stokes_fmm.py)")
         self.Ncutoff = int(Ncutoff)
         self.Nequiv = int(Nequiv)
         self.dtype = dtype

@@ -224,6 +224,8 @@ class FMM:
         if Nequiv > _lib.MAX_NEQUIV:
             raise ValueError(f"Nequiv must be <= {_lib.MAX_NEQUIV}")
         _lib.load()
+        from .kernels import Stokes
+        self.kernel = Stokes()   # the registered "Stokes" kernel
         self.Nequiv = int(Nequiv)
         self.Ncutoff = int(Ncutoff)
         self.verbose = verbose

@@ -78,3 +78,25 @@ def test_helper_rejects_other_kernel_or_nequiv():
     h.attach(kernels.Laplace(), 24)
     with pytest.raises(ValueError):
         h.attach(kernels.Laplace(), 32)
+
+
+def test_registered_kernel_names_of_the_reference():
+    """Every kernel of the reference's examples resolves by its name:
+    Laplace_Eval, Modified_Helmholtz_Eval, the Struve example's Kernel, and
+    the Stokeslet (whose FMM is the Stokes FMM class)."""
+    import numpy as np
+    from flexmm_b200.kernels import KERNEL_STOKES, _BY_NAME, resolve, struve_gf
+    assert resolve("Laplace_Eval").name == "Laplace_Eval"
+    assert resolve("Modified_Helmholtz_Eval", helmholtz_k=10.0).params[0] == 10.0
+    assert {"Laplace_Eval", "Modified_Helmholtz_Eval", "Kernel", "Stokes"} <= set(_BY_NAME)
+    st = resolve("Stokes")
+    assert st.vector and st.kernel_id == KERNEL_STOKES
+    # the Stokeslet's host rows against the reference's formulas at one pair
+    dx, dy = 0.3, -0.7
+    d2 = dx * dx + dy * dy
+    rows = st.host(0.0, 0.0, dx, dy)
+    assert np.isclose(rows[0, 0], (-0.5 * np.log(d2) + dx * dx / d2) / (4 * np.pi))
+    assert np.isclose(rows[2, 1], dy / d2 / (2 * np.pi))
+    # GF through scipy bridges scipy's NaN intervals
+    r = np.array([0.5, 25.8463, 27.329, 28.995, 100.0])
+    assert np.all(np.isfinite(struve_gf(r)))
