@@ -541,51 +541,70 @@ def run_ours(args, world, rank, local):
         out[p] = summary(p, res[p])
     if "fp64" in res and "mixed" in res:
         out["mixed_over_fp64"] = res["fp64"]["ms_step"] / res["mixed"]["ms_step"]
-    if world == 1 and not args.no_batched_stokes:
-        out["batched_stokes"] = measure_batched_stokes(args)
+    if not args.no_batched_stokes:
+        out["batched_stokes"] = measure_batched_stokes(args, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_subprocess(args)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-def measure_batched_stokes(args, n_problems=256):
+def measure_batched_stokes(args, world=1, n_problems=256):
     """The batching form: 256 independent FP64 Stokes problems (sizes
     log-uniform in [2,000, 200,000], sources uniform in [-1,1]^2, forces
     N(0,1)), self-evaluation, Nequiv 32, Ncutoff 64; forward and charge
     adjoint through StokesBatch, inputs resident, timed with CUDA events on
-    the caller's stream (the batch streams are joined into it)."""
+    the caller's stream (the batch streams are joined into it).  With N > 1
+    ranks the problems are partitioned by cost over the ranks
+    (ShardedStokesBatch: no exchange while computing): each rank times its
+    own share, the slowest rank's time counts, and one all-gather afterwards
+    (untimed) hands every rank all results."""
     import torch
     from flexmm_b200.batch import StokesBatch
+    from flexmm_b200.shard import partition_by_cost
     rng = np.random.default_rng(4)
     sizes = np.round(np.exp(rng.uniform(np.log(2000), np.log(200000), n_problems))).astype(int)
     probs = [(rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)) for n in sizes]
+    forces = [(rng.standard_normal(n), rng.standard_normal(n)) for n in sizes]
+    cots = [tuple(rng.standard_normal(n) for _ in range(3)) for n in sizes]
+    rank = int(os.environ.get("RANK", "0"))
+    mine = partition_by_cost(sizes, world)[rank]
     dev = lambda a: torch.from_numpy(a).cuda()
-    forces = [(dev(rng.standard_normal(n)), dev(rng.standard_normal(n))) for n in sizes]
-    cots = [tuple(dev(rng.standard_normal(n)) for _ in range(3)) for n in sizes]
-    B = StokesBatch(probs, Nequiv=32, Ncutoff=64, n_streams=8)
+    B = StokesBatch([probs[i] for i in mine], Nequiv=32, Ncutoff=64, n_streams=8)
+    f_loc = [(dev(forces[i][0]), dev(forces[i][1])) for i in mine]
+    c_loc = [tuple(dev(v) for v in cots[i]) for i in mine]
     total = int(sizes.sum())
 
     def timed(fn, reps=3):
         fn()
         torch.cuda.synchronize()
+        barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(reps):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+        barrier(world)
+        return dist_max(e0.elapsed_time(e1) / reps, world)
 
-    ms_f = timed(lambda: B.forward(forces))
-    ms_a = timed(lambda: B.adjoint(cots))
+    ms_f = timed(lambda: B.forward(f_loc))
+    ms_a = timed(lambda: B.adjoint(c_loc))
     B.status()
-    return {"workload": f"{n_problems} independent Stokes problems, N_i log-uniform in "
-                        f"[2000, 200000] (sum {total}), self-evaluation, Nequiv 32, Ncutoff 64, FP64",
-            "metric": "sum N_i / T", "unit": "Mpts/s", "dtype": "f64", "streams": len(B.streams),
-            "forward": {"value": total / (ms_f * 1e-3) / 1e6, "ms": ms_f},
-            "adjoint": {"value": total / (ms_a * 1e-3) / 1e6, "ms": ms_a},
-            "note": "concurrent per-problem plans on CUDA streams (trees built once, outside the timing)"}
+    res = {"workload": f"{n_problems} independent Stokes problems, N_i log-uniform in "
+                       f"[2000, 200000] (sum {total}), self-evaluation, Nequiv 32, Ncutoff 64, FP64",
+           "metric": "sum N_i / T", "unit": "Mpts/s", "dtype": "f64", "streams": len(B.streams),
+           "forward": {"value": total / (ms_f * 1e-3) / 1e6, "ms": ms_f},
+           "adjoint": {"value": total / (ms_a * 1e-3) / 1e6, "ms": ms_a},
+           "note": "concurrent per-problem plans on CUDA streams (trees built once, outside the timing)"}
+    if world > 1:
+        from flexmm_b200.shard import ShardedStokesBatch
+        S = ShardedStokesBatch(probs, Nequiv=32, Ncutoff=64, n_streams=8)
+        S.forward(forces)   # the gather path, once, untimed
+        res.update(scaling="strong", ranks=world,
+                   note="problems partitioned by points over the ranks (no exchange while "
+                        "computing); slowest rank's device time; trees built outside the timing")
+    return res
 
 
 # ---------------------------------------------------------- reference arm --

@@ -94,6 +94,8 @@ SIGNATURES = [
     ("fmm_evaluate_sources_outputs", ctypes.c_int,
      [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
     ("fmm_plan_destroy", ctypes.c_int, [_vp]),
+    ("fmm_plan_drop_expansions", ctypes.c_int, [_vp]),
+    ("fmm_plan_move_sources", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("fmm_plan_status", ctypes.c_int, [_vp]),
     ("fmm_tree_export", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("fmm_direct", ctypes.c_int, [ctypes.c_int, _dp, _vp, _vp, _vp, ctypes.c_int64, _vp, _vp,

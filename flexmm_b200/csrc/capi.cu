@@ -1058,6 +1058,41 @@ int fmm_plan_status(fmm_plan *p) {
   });
 }
 
+int fmm_plan_drop_expansions(fmm_plan *p) {
+  return guarded([&] {
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    // device memory returns to the pool in the plan stream's order
+    p->tau_s.release();
+    p->tau2_s.release();
+    p->mult.release();
+    p->ple.release();
+    p->loc.release();
+    p->mult32.release();
+    p->loc32.release();
+    p->mult_tc.release();
+    p->msum.release();
+    p->lsum.release();
+    p->tsum.release();
+    p->partial.release();
+    p->have_expansions = false;
+  });
+}
+
+int fmm_plan_move_sources(fmm_plan *p, const double *x, const double *y, void *stream) {
+  return guarded([&] {
+    tree_ready(p);
+    FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
+    const int64_t n = p->th.n_points;
+    if (n == 0) return;
+    FMMB_CHECK(x && y, ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    // the tree's sorted copy, in the tree's own order (sorted -> original)
+    gather_sorted(x, p->td.ordv.get(), n, p->td.sx.get(), s);
+    gather_sorted(y, p->td.ordv.get(), n, p->td.sy.get(), s);
+    p->have_expansions = false;
+  });
+}
+
 int fmm_plan_destroy(fmm_plan *p) {
   // no host wait: the plan's device buffers go back to the pool with
   // cudaFreeAsync on the stream they were allocated on, after the work

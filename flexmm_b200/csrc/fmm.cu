@@ -58,78 +58,166 @@ __device__ __forceinline__ double fold_of() {
 }
 
 // ---------------------------------------------------------------- upward ----
-// One tile = 32 consecutive nodes of level m.
+__device__ __forceinline__ int level_of_node(const int *__restrict__ off, int L, int g) {
+  int lo = 0, hi = L;  // largest l with off[l] <= g
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// kernel value at the difference (ax, ay) = target - source; raw log2 for
+// the table-driven Laplace functor (its factor folded into the charges)
 template <class KF>
-__global__ void __launch_bounds__(NT) k_upward(int m, KernelParams kp, int neq, int np, int g_begin,
-                                               int g_end, const uint8_t *__restrict__ flags,
-                                               const int *__restrict__ bot,
-                                               const int *__restrict__ top,
-                                               const int *__restrict__ child,
-                                               const double *__restrict__ xmid,
-                                               const double *__restrict__ ymid,
-                                               const double *__restrict__ sx,
-                                               const double *__restrict__ sy,
-                                               const double *__restrict__ tau,
-                                               const LevelOpsDev *__restrict__ ops,
-                                               double *__restrict__ mult) {
+__device__ __forceinline__ double kernel_at(const KF &K, double ax, double ay) {
+  if constexpr (KF::kLogTable)
+    return K.raw(ax, ay);
+  else
+    return K(0.0, 0.0, ax, ay);
+}
+
+// S2M + C2E of every S2M node (leaves holding points, levels >= 2) of every
+// level in one launch (flexmm/flexmm2d/kifmm.py:96-105, then fmm.py:86-90):
+// a tile is TN consecutive entries of the level-major S2M node list, a warp
+// sums one node's sources into its check potentials (lanes over check
+// points, the node's sources staged 32 at a time, four independent sums
+// per lane); C2E runs once for each level the tile holds.
+template <class KF>
+__global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, int L,
+                                            const int *__restrict__ off,
+                                            const int *__restrict__ uplist,
+                                            const int *__restrict__ n_up_ptr,
+                                            const int *__restrict__ bot,
+                                            const int *__restrict__ top,
+                                            const double *__restrict__ xmid,
+                                            const double *__restrict__ ymid,
+                                            const double *__restrict__ sx,
+                                            const double *__restrict__ sy,
+                                            const double *__restrict__ tau,
+                                            const LevelOpsDev *__restrict__ ops,
+                                            double *__restrict__ mult) {
   extern __shared__ double smem[];
-  const int ldp = pad_ld(np), lda = pad_ld(4 * np);
-  double *P = smem;           // [TN][ldp]  check potentials
-  double *A = P + TN * ldp;   // [TN][lda]  children multipoles; later C2E scratch
+  const int ldp = pad_ld(np);
+  double *P = smem;          // [TN][ldp] check potentials
+  double *T = P + TN * ldp;  // [TN][ldp] C2E scratch
+  __shared__ double srcx[NT / 32][32], srcy[NT / 32][32], srct[NT / 32][32];
+  __shared__ int node[TN], nlev[TN];
   __shared__ double *orow[TN];
   __shared__ FunctorSmem<KF> fsm;
   KF K(kp);
   fsm.bind(K);
-  const LevelOpsDev &op = ops[m];
-  const int g0 = g_begin + blockIdx.x * TN;
-  const int nloc = min(TN, g_end - g0);
-  for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = 0.0;
-  for (int i = threadIdx.x; i < TN * lda; i += NT) A[i] = 0.0;
-  if (threadIdx.x < TN) orow[threadIdx.x] = threadIdx.x < nloc ? mult + (size_t)(g0 + threadIdx.x) * np : nullptr;
-  __syncthreads();
+  const double fold = fold_of<KF, KF::kLogTable>();
+  const int n_up = *n_up_ptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // S2M (flexmm/flexmm2d/kifmm.py:96-105) for leaves and fake leaves holding
-  // points; children multipoles for boxes with children (M2M)
-  for (int t = warp; t < nloc; t += NT / 32) {
-    const int g = g0 + t;
-    const uint8_t f = flags[g];
-    const int b = bot[g], e = top[g];
-    const bool up = (((f & NF_LEAF) && !(f & NF_XLIST)) || (f & NF_FAKE)) && e > b;
-    if (up) {
-      const double cx = xmid[g], cy = ymid[g];
-      for (int k = lane; k < neq; k += 32) {
-        const double lxk = op.lx[k], lyk = op.ly[k];
-        double acc = 0.0;
-        for (int j = b; j < e; ++j) acc = fma(K(sx[j] - cx, sy[j] - cy, lxk, lyk), tau[j], acc);
-        P[t * ldp + k] = acc;
-      }
-    } else if (f & NF_CHILDREN) {
-      const double *src = mult + (size_t)child[g] * np;  // 4 consecutive children rows
-      for (int qd = lane; qd < 4 * np; qd += 32) A[t * lda + qd] = src[qd];
+  for (int tile = blockIdx.x; tile * TN < n_up; tile += gridDim.x) {
+    const int i0 = tile * TN, nloc = min(TN, n_up - i0);
+    for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = 0.0;
+    if (threadIdx.x < TN) {
+      const int g = (int)threadIdx.x < nloc ? uplist[i0 + threadIdx.x] : -1;
+      node[threadIdx.x] = g;
+      nlev[threadIdx.x] = g >= 0 ? level_of_node(off, L, g) : -1;
     }
+    __syncthreads();
+    const int mlo = nlev[0], mhi = nlev[nloc - 1];
+    for (int t = warp; t < nloc; t += NT / 32) {
+      const int g = node[t];
+      const LevelOpsDev &op = ops[nlev[t]];
+      const int b = bot[g], e = top[g];
+      const double cx = xmid[g], cy = ymid[g];
+      const bool k0 = lane < neq, k1 = lane + 32 < neq;
+      const double lx0 = k0 ? op.lx[lane] : 0.0, ly0 = k0 ? op.ly[lane] : 0.0;
+      const double lx1 = k1 ? op.lx[lane + 32] : 0.0, ly1 = k1 ? op.ly[lane + 32] : 0.0;
+      double a0 = 0.0, b0 = 0.0, a1 = 0.0, b1 = 0.0;
+      for (int j0 = b; j0 < e; j0 += 32) {
+        const int nj = min(32, e - j0);
+        if (lane < nj) {
+          srcx[warp][lane] = sx[j0 + lane] - cx;
+          srcy[warp][lane] = sy[j0 + lane] - cy;
+          srct[warp][lane] = tau[j0 + lane] * fold;
+        } else {  // padding pairs: zero charge at a harmless distance
+          srcx[warp][lane] = 0.0;
+          srcy[warp][lane] = 0.0;
+          srct[warp][lane] = 0.0;
+        }
+        __syncwarp();
+        const int nj2 = (nj + 1) & ~1;
+        if (k0)
+          for (int j = 0; j < nj2; j += 2) {
+            a0 = fma(kernel_at(K, lx0 - srcx[warp][j], ly0 - srcy[warp][j]), srct[warp][j], a0);
+            b0 = fma(kernel_at(K, lx0 - srcx[warp][j + 1], ly0 - srcy[warp][j + 1]),
+                     srct[warp][j + 1], b0);
+          }
+        if (k1)
+          for (int j = 0; j < nj2; j += 2) {
+            a1 = fma(kernel_at(K, lx1 - srcx[warp][j], ly1 - srcy[warp][j]), srct[warp][j], a1);
+            b1 = fma(kernel_at(K, lx1 - srcx[warp][j + 1], ly1 - srcy[warp][j + 1]),
+                     srct[warp][j + 1], b1);
+          }
+        __syncwarp();
+      }
+      if (k0) P[t * ldp + lane] = a0 + b0;
+      if (k1) P[t * ldp + lane + 32] = a1 + b1;
+    }
+    for (int m = mlo; m <= mhi; ++m) {
+      __syncthreads();
+      if (threadIdx.x < TN)
+        orow[threadIdx.x] = nlev[threadIdx.x] == m ? mult + (size_t)node[threadIdx.x] * np : nullptr;
+      __syncthreads();
+      c2e_tile(ops[m], np, P, T, orow);
+    }
+    __syncthreads();
   }
+}
+
+// M2M + C2E of the parent boxes of level m (flexmm/flexmm2d/fmm.py:91-98):
+// TN parent groups per tile; their children are the contiguous node rows
+// c_first + 4e .. c_first + 4e + 3 of level m+1.  P[t] = M2MC . children.
+__global__ void __launch_bounds__(NT) k_m2m(int m, int np, int c_first, int n_groups,
+                                            const int *__restrict__ parent,
+                                            const LevelOpsDev *__restrict__ ops,
+                                            double *__restrict__ mult) {
+  extern __shared__ double smem[];
+  const int ldp = pad_ld(np), lda = pad_ld(4 * np);
+  double *P = smem;           // [TN][ldp] check potentials
+  double *T = P + TN * ldp;   // [TN][ldp] C2E scratch
+  double *A = T + TN * ldp;   // [TN][lda] children multipoles
+  __shared__ double *orow[TN];
+  const LevelOpsDev &op = ops[m];
+  const int e0 = blockIdx.x * TN, nloc = min(TN, n_groups - e0);
+  for (int i = threadIdx.x; i < TN * ldp; i += NT) P[i] = T[i] = 0.0;
+  for (int i = threadIdx.x + nloc * lda; i < TN * lda; i += NT) A[i] = 0.0;
+  pdl_wait();  // the children's multipoles come from the kernels before
+  pdl_trigger();
+  stage_rows(A, lda, mult + (size_t)(c_first + 4 * e0) * np, nloc, 4 * np);
+  if (threadIdx.x < TN) {
+    const int t = threadIdx.x;
+    orow[t] = t < nloc ? mult + (size_t)parent[c_first + 4 * (e0 + t)] * np : nullptr;
+  }
+  cp_async_wait_all();
   __syncthreads();
-  // M2M: P[t] = M2MC . [children]  (flexmm/flexmm2d/fmm.py:93-96)
   {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const int r0 = 8 * (warp & 3), c0 = 8 * (warp >> 2);
     double acc[1][4][2];
     zero_acc(acc);
     warp_gemm<1, 4>(A, lda, op.m2mct, np, 4 * np, r0, c0, 2, np, acc);
     const int t = r0 + g;
-    if (t < nloc && (flags[g0 + t] & NF_CHILDREN)) {
 #pragma unroll
-      for (int cb = 0; cb < 4; ++cb) {
-        const int col = c0 + 16 * cb + 2 * q;
-        if (col < np) {
-          P[t * ldp + col] = acc[0][cb][0];
-          P[t * ldp + col + 1] = acc[0][cb][1];
-        }
+    for (int cb = 0; cb < 4; ++cb) {
+      const int col = c0 + 16 * cb + 2 * q;
+      if (col < np) {
+        P[t * ldp + col] = acc[0][cb][0];
+        P[t * ldp + col + 1] = acc[0][cb][1];
       }
     }
   }
   __syncthreads();
-  c2e_tile(op, np, P, A, orow);
+  c2e_tile(op, np, P, T, orow);
 }
 
 // ------------------------------------------------------------------- M2L ----
@@ -244,6 +332,8 @@ __global__ void __launch_bounds__(NT) k_downward(int m, int np, int rg_lo, int r
     node[threadIdx.x] = n;
     orow[threadIdx.x] = n >= 0 ? loc + (size_t)n * np : nullptr;
   }
+  pdl_wait();  // partial locals (M2L) and the parents' locals come from the kernels before
+  pdl_trigger();
   __syncthreads();
   for (int i = threadIdx.x; i < TN * np; i += NT) {
     const int t = i / np, k = i % np;
@@ -647,17 +737,25 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int np = a.np;
-  const size_t sm = sizeof(double) * (size_t)TN * (pad_ld(np) + pad_ld(4 * np));
-  FMMB_CUDA(cudaFuncSetAttribute(k_upward<KF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(double) * TN * (pad_ld(64) + pad_ld(256)))));
-  for (int m = th.L - 1; m >= 2; --m) {
-    const int gb = th.off[m], ge = th.off[m + 1];
-    const int tiles = (ge - gb + TN - 1) / TN;
-    PhaseTimer timer(PH_UPWARD, s);
-    k_upward<KF><<<tiles, NT, sm, s>>>(m, a.kp, a.neq, np, gb, ge, td.flags.get(), td.bot.get(),
-                                       td.top.get(), td.child.get(), td.xmid.get(), td.ymid.get(),
-                                       td.sx.get(), td.sy.get(), tau_s, a.ops_dev, mult);
-    FMMB_CUDA(cudaGetLastError());
+  if (th.L < 3) return;
+  const size_t s2m_bytes = sizeof(double) * (size_t)TN * pad_ld(np) * 2;
+  FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(s2m_bytes)));
+  PhaseTimer timer(PH_UPWARD, s);
+  k_s2m<KF><<<148 * 4, NT, s2m_bytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
+                                           td.uplist.get(), td.n_up.get(), td.bot.get(),
+                                           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
+                                           td.sy.get(), tau_s, a.ops_dev, mult);
+  FMMB_CUDA(cudaGetLastError());
+  const size_t m2m_bytes = sizeof(double) * (size_t)TN * (2 * pad_ld(np) + pad_ld(4 * np));
+  FMMB_CUDA(cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(m2m_bytes)));
+  for (int m = th.L - 2; m >= 2; --m) {
+    const int c_first = th.off[m + 1];
+    const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
+    if (n_groups == 0) continue;
+    launch_pdl(k_m2m, dim3((n_groups + TN - 1) / TN), dim3(NT), m2m_bytes, s, m, np, c_first,
+               n_groups, td.parent.get(), a.ops_dev, mult);
   }
 }
 
@@ -754,8 +852,8 @@ void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_
     if (cnt <= 0) continue;
     const int tiles = (cnt + 7) / 8;
     PhaseTimer timer(PH_DOWNWARD, s);
-    k_downward<<<tiles, NT, sm, s>>>(m, a.np, lo, cnt, td.rg.get(), td.parent.get(), a.ops_dev, ple,
-                                     loc);
+    launch_pdl(k_downward, dim3(tiles), dim3(NT), sm, s, m, a.np, lo, cnt, td.rg.get(),
+               td.parent.get(), a.ops_dev, ple, loc);
     FMMB_CUDA(cudaGetLastError());
   }
 }

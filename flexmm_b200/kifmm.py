@@ -246,6 +246,28 @@ class KI_FMM:
             _torch().cuda.synchronize()
             print("....Time for expansions:        {:0.2f}".format(1000 * (time.time() - st)))
 
+    def drop_expansions(self):
+        """Release the expansions, keep the tree; build_expansions forms them again."""
+        _lib.call("fmm_plan_drop_expansions", self._plan)
+        self._expanded = False
+        self._tau = None
+
+    def move_sources(self, x, y):
+        """New source coordinates on the same (frozen) tree: every source keeps
+        the leaf it was sorted into; expansions must be built again."""
+        xd, _ = _device_f64(x)
+        yd, _ = _device_f64(y)
+        if xd.numel() != self.N or yd.numel() != self.N:
+            raise ValueError(f"expected {self.N} source coordinates")
+        _lib.call("fmm_plan_move_sources", self._plan, ctypes.c_void_p(xd.data_ptr()),
+                  ctypes.c_void_p(yd.data_ptr()), _stream())
+        self._x, self._y = xd, yd
+        torch = _torch()
+        self._src_in = ((x, y, x._version, y._version)
+                        if isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor) else None)
+        self._expanded = False
+        self._tau = None
+
     def register_evaluator(self, KAS1, KAS2, name, outputs):
         """Name an evaluator (kifmm2d FMM.register_evaluator, flexmm/kifmm2d/scalar/fmm.py:172-173).
 

@@ -207,6 +207,19 @@ int fmm_evaluate_outputs(fmm_plan *plan, int evaluator, const double *tx, const 
 /* The same at the plan's own source points (see fmm_evaluate_sources). */
 int fmm_evaluate_sources_outputs(fmm_plan *plan, int evaluator, int check, double *out,
                                  int64_t ld_out, void *stream);
+/* Release the plan's expansions (and its sorted charges), keeping the tree:
+ * a later fmm_build_expansions forms them again.  The differentiation form
+ * (torch.autograd) uses it to recompute expansions in its backward pass
+ * instead of holding them between forward and backward.  No counterpart in
+ * the reference, whose FMM objects hold their expansions. */
+int fmm_plan_drop_expansions(fmm_plan *plan);
+/* Move the plan's sources to new coordinates (device x, y in the caller's
+ * original order) without rebuilding the tree: every source keeps the leaf
+ * the tree gave it ("frozen tree"; points may leave their box slightly).
+ * Expansions must be built again afterwards.  For finite-difference checks
+ * and optimisation loops over slowly moving points; no counterpart in the
+ * reference, whose Tree copies the points once (flexmm/tree.py:459-460). */
+int fmm_plan_move_sources(fmm_plan *plan, const double *x, const double *y, void *stream);
 /* Releases the plan without waiting for the GPU: its device memory returns to
  * the pool in stream order on the plan's stream (one stream per plan), so a
  * loop that builds a plan per step keeps the host ahead of the GPU. */

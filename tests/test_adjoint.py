@@ -17,10 +17,12 @@ def _problem(n=6000, m=2500, seed=3):
 
 @pytest.mark.parametrize("method", ["bb", "kifmm"])
 def test_adjoint_gradients_match_direct_sum(built_lib, method):
+    """N = 20,000 sources, 10,000 targets: every gradient against its FP64
+    direct-sum value (bar 1e-8 relative L2)."""
     import torch
     from flexmm_b200.autograd import fmm_potential
     from oracle.direct import direct_laplace, direct_laplace_grad
-    sx, sy, tau, tx, ty, uref = _problem()
+    sx, sy, tau, tx, ty, uref = _problem(n=20_000, m=10_000)
     T = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda", requires_grad=True)
     vs = [T(a) for a in (sx, sy, tau, tx, ty)]
     kw = dict(method=method, Ncutoff=64, p=16, Nequiv=60, bbox=[-1, 1, -1, 1])
@@ -39,31 +41,58 @@ def test_adjoint_gradients_match_direct_sum(built_lib, method):
         assert rel_l2(a, b) < 1e-8, (name, rel_l2(a, b))
 
 
-def test_adjoint_matches_central_differences(built_lib):
-    """Central differences h = 1e-6 on a few source and target coordinates
-    (the tree is rebuilt at each perturbed point; no point crosses a box
-    boundary at this h for this seed)."""
+def test_adjoint_matches_central_differences_frozen_tree(built_lib):
+    """Central differences h = 1e-6 on 50 random coordinates (sources,
+    charges, targets), the trees frozen (FMMPotential: perturbed points are
+    moved inside the trees built at the start).  Bar per coordinate:
+    1e-5 max(1, |g|) plus the difference quotient's own rounding,
+    4 eps L / h."""
     import torch
-    from flexmm_b200.autograd import fmm_potential
-    sx, sy, tau, tx, ty, uref = _problem(n=3000, m=1000, seed=4)
+    from flexmm_b200.autograd import FMMPotential
+    sx, sy, tau, tx, ty, uref = _problem(n=20_000, m=10_000, seed=4)
     kw = dict(method="bb", Ncutoff=64, p=16, bbox=[-1, 1, -1, 1])
     ur = torch.tensor(uref, device="cuda")
+    D = lambda a, g=False: torch.tensor(a, dtype=torch.float64, device="cuda", requires_grad=g)
+    P = FMMPotential(D(sx), D(sy), D(tx), D(ty), **kw)
 
     def loss_of(a):
-        u = fmm_potential(*[torch.tensor(v, dtype=torch.float64, device="cuda") for v in a], **kw)
+        u = P(*[D(v) for v in a])
         return 0.5 * float(((u - ur) ** 2).sum())
-    vs = [torch.tensor(v, dtype=torch.float64, device="cuda", requires_grad=True) for v in (sx, sy, tau, tx, ty)]
-    u = fmm_potential(*vs, **kw)
-    (0.5 * ((u - ur) ** 2).sum()).backward()
+    vs = [D(v, True) for v in (sx, sy, tau, tx, ty)]
+    u = P(*vs)
+    L = 0.5 * ((u - ur) ** 2).sum()
+    L.backward()
+    L = float(L)
     rng = np.random.default_rng(0)
     h = 1e-6
-    for which in (0, 1, 2, 3, 4):
-        base = [v.copy() for v in (sx, sy, tau, tx, ty)]
-        for k in rng.choice(base[which].size, 4, replace=False):
-            plus = [v.copy() for v in base]
-            minus = [v.copy() for v in base]
-            plus[which][k] += h
-            minus[which][k] -= h
-            fd = (loss_of(plus) - loss_of(minus)) / (2 * h)
-            an = float(vs[which].grad[k])
-            assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)), (which, k, fd, an)
+    eps = np.finfo(np.float64).eps
+    base = [v.copy() for v in (sx, sy, tau, tx, ty)]
+    picks = [(int(w), int(rng.integers(base[w].size))) for w in rng.integers(0, 5, 50)]
+    assert len(picks) == 50
+    for which, k in picks:
+        plus = [v.copy() for v in base]
+        minus = [v.copy() for v in base]
+        plus[which][k] += h
+        minus[which][k] -= h
+        fd = (loss_of(plus) - loss_of(minus)) / (2 * h)
+        an = float(vs[which].grad[k])
+        assert abs(fd - an) <= 1e-5 * max(1.0, abs(an)) + 4 * eps * L / h, (which, k, fd, an)
+
+
+def test_backward_recomputes_expansions(built_lib):
+    """The forward FMM keeps its tree and releases its expansions; the
+    backward forms them again (the gradients stay those of the direct sum)."""
+    import torch
+    from flexmm_b200.autograd import _FMMPotential, _Trees, _make
+    sx, sy, tau, tx, ty, uref = _problem(n=5000, m=2000, seed=6)
+    T = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda", requires_grad=True)
+    vs = [T(a) for a in (sx, sy, tau, tx, ty)]
+    trees = _Trees(_make("bb", "Laplace_Eval", 64, 32, 16, [-1, 1, -1, 1], {}))
+    u = _FMMPotential.apply(*vs, trees)
+    assert trees.F is not None and not trees.F._expanded   # tree kept, expansions released
+    assert trees.A is None                                 # the adjoint tree comes in backward
+    (u * torch.tensor(uref, device="cuda")).sum().backward()
+    assert not trees.F._expanded and not trees.A._expanded
+    from oracle.direct import direct_laplace_grad
+    Gt = direct_laplace_grad(sx, sy, tau, tx, ty, False)
+    assert rel_l2(vs[3].grad.cpu().numpy(), uref * Gt[1]) < 1e-8
