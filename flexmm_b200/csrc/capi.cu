@@ -235,10 +235,44 @@ struct fmm_plan {
   DevBuf<double> tau2_s, partial;  // Stokes FMM: sorted fy; partial multipoles
   int n_rhs = 1;                   // charge columns of the last build (multi-RHS)
   cublasHandle_t blas = nullptr;  // black-box and Stokes FMM translations
+  // split own-source evaluation (near field on a side stream, see SplitEval):
+  // `ready` is recorded once a single-column KIFMM build has sorted its charges
+  cudaStream_t side = nullptr;  // from the device's pool, not owned
+  cudaEvent_t ev_ready = nullptr, ev_near = nullptr, ev_far = nullptr;
+  bool ready_recorded = false;
   ~fmm_plan() {
     if (blas) cublasDestroy(blas);
+    for (cudaEvent_t e : {ev_ready, ev_near, ev_far})
+      if (e) cudaEventDestroy(e);
   }
 };
+
+namespace {
+// Side streams for the split evaluation: a few non-blocking streams per
+// device, handed to plans round-robin (created once, kept until exit).
+constexpr int SIDE_STREAMS = 8;
+constexpr int SIDE_MAX_DEVICES = 64;
+std::mutex g_side_mu;
+cudaStream_t g_side[SIDE_MAX_DEVICES][SIDE_STREAMS] = {};
+int g_side_next[SIDE_MAX_DEVICES] = {};
+
+cudaStream_t side_stream() {
+  int dev = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  FMMB_CHECK(dev >= 0 && dev < SIDE_MAX_DEVICES, ERR_UNSUPPORTED, "device ordinal too large");
+  std::lock_guard<std::mutex> g(g_side_mu);
+  const int k = g_side_next[dev]++ % SIDE_STREAMS;
+  if (!g_side[dev][k]) FMMB_CUDA(cudaStreamCreateWithFlags(&g_side[dev][k], cudaStreamNonBlocking));
+  return g_side[dev][k];
+}
+
+// the plan's split-evaluation events (created on first use) and side stream
+void split_prepare(fmm_plan *p) {
+  if (!p->side) p->side = side_stream();
+  for (cudaEvent_t *e : {&p->ev_ready, &p->ev_near, &p->ev_far})
+    if (!*e) FMMB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+}
+}  // namespace
 
 extern "C" {
 
@@ -805,6 +839,7 @@ int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_
       run_downward(a, p->ple.get() + (size_t)r * cs, p->loc.get() + (size_t)r * cs, s);
     }
     p->n_rhs = n_rhs;
+    p->ready_recorded = false;  // the split evaluation serves single-column builds
     p->have_expansions = true;
   });
 }
@@ -885,6 +920,8 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
     }
     std::unique_ptr<PhaseTimer> t_prep(new PhaseTimer(PH_PREP, s));
     upload_level_ops(p, s);
+    split_prepare(p);
+    p->ready_recorded = false;
     PassArgs a = pass_args(p);
     p->tau_s.alloc(th.n_points, s);
     gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
@@ -903,6 +940,9 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       p->lsum.zero(s);
       p->tsum.alloc(total, s);
       node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
+      // sorted charges and box charge sums are all the near field reads
+      FMMB_CUDA(cudaEventRecord(p->ev_ready, s));
+      p->ready_recorded = true;
       t_prep.reset();
       run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(),
                        p->mult_tc.get(), s);
@@ -916,6 +956,8 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       p->loc.alloc(total * np, s);
       p->mult.zero(s);
       p->loc.zero(s);
+      FMMB_CUDA(cudaEventRecord(p->ev_ready, s));  // sorted charges: all the near field reads
+      p->ready_recorded = true;
       t_prep.reset();
       run_upward(a, p->tau_s.get(), p->mult.get(), s);
       run_m2l(a, p->mult.get(), p->ple.get(), s);
@@ -979,6 +1021,16 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
                  m, check, nout, out, ld_out, s);
 }
 
+// FLEXMM_B200_SPLIT_EVAL=0 evaluates own sources in one pass on the plan
+// stream (near and far field together), for comparison
+bool split_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("FLEXMM_B200_SPLIT_EVAL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t ld_out,
                           cudaStream_t s) {
   FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
@@ -997,7 +1049,15 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
   else if (p->ops->method == METHOD_BBFMM)
     run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), td.sx.get(), td.sy.get(),
                     td.pkeys.get(), td.ordv.get(), m, check, nout, out, ld_out, s);
-  else if (p->precision == PREC_MIXED)
+  else if (nout == 1 && p->ready_recorded && p->n_rhs == 1 && split_enabled()) {
+    // near field on the side stream, started when the charges were sorted
+    const SplitEval se{p->side, p->ev_ready, p->ev_near, p->ev_far};
+    if (p->precision == PREC_MIXED)
+      run_evaluate_sources_split_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(),
+                                       p->lsum.get(), check, out, s, se);
+    else
+      run_evaluate_sources_split(a, p->tau_s.get(), p->loc.get(), check, out, s, se);
+  } else if (p->precision == PREC_MIXED)
     run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(),
                        td.sx.get(), td.sy.get(), td.pkeys.get(), td.ordv.get(), m, check, nout,
                        out, ld_out, s);
@@ -1075,6 +1135,7 @@ int fmm_plan_drop_expansions(fmm_plan *p) {
     p->tsum.release();
     p->partial.release();
     p->have_expansions = false;
+    p->ready_recorded = false;
   });
 }
 
@@ -1090,6 +1151,7 @@ int fmm_plan_move_sources(fmm_plan *p, const double *x, const double *y, void *s
     gather_sorted(x, p->td.ordv.get(), n, p->td.sx.get(), s);
     gather_sorted(y, p->td.ordv.get(), n, p->td.sy.get(), s);
     p->have_expansions = false;
+    p->ready_recorded = false;
   });
 }
 

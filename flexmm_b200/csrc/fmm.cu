@@ -437,7 +437,9 @@ __global__ void k_make_items(int total, int L, const int *__restrict__ off, cons
 // warp shuffles (and shared memory when G > 32).
 // NOUT = 1: potential; NOUT = 3: potential and its gradient in the target
 // position (rows of out, stride ld_out).
-template <class KF, int NOUT>
+// PART: EVAL_FULL (L2T + P2P), EVAL_NEAR (P2P only, into near[], caller's
+// point order) or EVAL_FAR (L2T only, plus near[]: out = far + near).
+template <class KF, int NOUT, int PART = EVAL_FULL>
 __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np,
                                                   const int4 *__restrict__ items,
                                                   const int *__restrict__ n_items_ptr,
@@ -454,7 +456,9 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
                                                   const double *__restrict__ txs,
                                                   const double *__restrict__ tys,
                                                   const int *__restrict__ tperm, int check,
-                                                  double *__restrict__ out, int64_t ld_out) {
+                                                  double *__restrict__ out, int64_t ld_out,
+                                                  double *__restrict__ near = nullptr) {
+  static_assert(PART == EVAL_FULL || NOUT == 1, "split evaluation: potential only");
   __shared__ double Ls[64], lxs[64], lys[64];
   __shared__ double ssx[SMAX], ssy[SMAX], stau[SMAX];
   __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
@@ -476,13 +480,14 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     const bool valid = t < cnt;
     const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
     if (threadIdx.x < 9) {
-      const int cg = coll[(size_t)g * 9 + threadIdx.x];
+      const int cg = PART == EVAL_FAR ? -1 : coll[(size_t)g * 9 + threadIdx.x];
       rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
       rs[threadIdx.x + 1] = cg >= 0 ? top[cg] - bot[cg] : 0;
     }
     if (threadIdx.x == 0) rs[0] = 0;
     // L2T (flexmm/flexmm2d/kifmm.py:106-120); locals of levels 0-1 are zero
-    if (lev >= 2)
+    const bool l2t = lev >= 2 && PART != EVAL_NEAR;
+    if (l2t)
       for (int k = threadIdx.x; k < neq; k += TCH) {
         Ls[k] = loc[(size_t)g * np + k] * fold;
         lxs[k] = ops[lev].lx[k];
@@ -493,7 +498,7 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
       for (int c = 1; c <= 9; ++c) rs[c] += rs[c - 1];
     double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
     double gu = 0.0, gx = 0.0, gy = 0.0;  // NOUT = 3
-    if (lev >= 2 && valid) {
+    if (l2t && valid) {
       const double dx = x - xmid[g], dy = y - ymid[g];
       if constexpr (NOUT == 1) {
         auto kv = [&](int k) -> double {
@@ -579,7 +584,15 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
           for (int w = 0; w < G / 32; ++w) u += red[o][(threadIdx.x >> 5) + w];
         }
       }
-      if (valid && sub == 0) out[o * ld_out + tperm[t0 + t]] = u;
+      if (valid && sub == 0) {
+        const int i = tperm[t0 + t];
+        if constexpr (PART == EVAL_NEAR)
+          near[i] = u;
+        else if constexpr (PART == EVAL_FAR)
+          out[i] = u + near[i];
+        else
+          out[o * ld_out + i] = u;
+      }
     }
     __syncthreads();
   }
@@ -804,7 +817,7 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
   kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(),
                                td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
                                td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out,
-                               ld_out);
+                               ld_out, nullptr);
   FMMB_CUDA(cudaGetLastError());
 }
 }  // namespace
@@ -882,6 +895,40 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
 
 namespace {
 template <class KF>
+void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *loc, int check,
+                         double *out, cudaStream_t s, const SplitEval &se) {
+  const TreeDev &td = *a.td;
+  const int64_t m = a.th->n_points;
+  FMMB_CUDA(cudaStreamWaitEvent(se.side, se.ready, 0));
+  EvalItems it;
+  eval_items(a, td.pkeys.get(), m, it, se.side);
+  DevBuf<double> near;
+  near.alloc(m, se.side);
+  {
+    PhaseTimer timer(PH_EVAL, se.side);
+    k_evaluate<KF, 1, EVAL_NEAR><<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
+        a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+        td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+        loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
+  FMMB_CUDA(cudaEventRecord(se.near_done, se.side));
+  FMMB_CUDA(cudaStreamWaitEvent(s, se.near_done, 0));
+  {
+    PhaseTimer timer(PH_EVAL, s);
+    k_evaluate<KF, 1, EVAL_FAR><<<148 * 8, TCH, 0, s>>>(
+        a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+        td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+        loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
+  // the scratch (allocated on the side stream) is freed there once the plan
+  // stream is done with it
+  FMMB_CUDA(cudaEventRecord(se.far_done, s));
+  FMMB_CUDA(cudaStreamWaitEvent(se.side, se.far_done, 0));
+}
+
+template <class KF>
 void evaluate_multi_impl(const PassArgs &a, const double *tau_s, int64_t n_src, int n_rhs,
                          const double *loc, int64_t col_stride, const double *txs,
                          const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
@@ -920,6 +967,21 @@ void run_evaluate_multi(const PassArgs &a, const double *tau_s, int64_t n_src, i
     case KERNEL_RADIAL_TABLE:
       evaluate_multi_impl<RadialTableF64>(a, tau_s, n_src, n_rhs, loc, col_stride, txs, tys, tkeys,
                                           tperm, m, check, out, ld_out, s);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+}
+
+void run_evaluate_sources_split(const PassArgs &a, const double *tau_s, const double *loc,
+                                int check, double *out, cudaStream_t s, const SplitEval &se) {
+  if (a.th->n_points == 0) return;
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE: evaluate_split_impl<LaplaceF64T>(a, tau_s, loc, check, out, s, se); break;
+    case KERNEL_MOD_HELMHOLTZ:
+      evaluate_split_impl<ModHelmholtzF64>(a, tau_s, loc, check, out, s, se);
+      break;
+    case KERNEL_RADIAL_TABLE:
+      evaluate_split_impl<RadialTableF64>(a, tau_s, loc, check, out, s, se);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
@@ -974,7 +1036,8 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   auto launch = [&](auto kern) {
     kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(),
                                  td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
-                                 td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0);
+                                 td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0,
+                                 nullptr);
   };
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: launch(k_evaluate<LaplaceF64T, 1>); break;

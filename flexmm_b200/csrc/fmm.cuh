@@ -106,6 +106,22 @@ void run_evaluate_multi(const PassArgs &a, const double *tau_sorted, int64_t n_s
                         const double *loc, int64_t col_stride, const double *txs, const double *tys,
                         const uint64_t *tkeys, const int *tperm, int64_t m, int check, double *out,
                         int64_t ld_out, cudaStream_t s);
+// Split own-source evaluation: the near field (P2P) runs on `side` as soon
+// as `ready` (recorded on the plan stream once the charges are sorted) has
+// passed, beside the level passes still queued on the plan stream; the far
+// field (L2T) runs on the plan stream after them and adds the near field.
+// near_done / far_done are scratch events of the plan.  Scratch lives on the
+// side stream and is released there after the plan stream has used it.
+struct SplitEval {
+  cudaStream_t side;
+  cudaEvent_t ready, near_done, far_done;
+};
+constexpr int NEAR_BLOCKS_PER_SM = 4;  // near-field blocks per SM, leaving room for the level passes
+void run_evaluate_sources_split(const PassArgs &a, const double *tau_sorted, const double *loc,
+                                int check, double *out, cudaStream_t s, const SplitEval &se);
+void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_sorted,
+                                      const double *tsum, const float *loc32, const double *lsum,
+                                      int check, double *out, cudaStream_t s, const SplitEval &se);
 void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaStream_t s);
 void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s);
 void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s);
@@ -130,6 +146,8 @@ struct EvalItems {
   DevBuf<int> n_items;  // device count of items
 };
 constexpr int EVAL_CHUNK = 128;  // targets per evaluation work item
+// parts of an evaluation: both, the near field (P2P) alone, the far field (L2T) alone
+constexpr int EVAL_FULL = 0, EVAL_NEAR = 1, EVAL_FAR = 2;
 void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s);
 
 // Mixed precision (fmm_mixed.cu): FP32 multipoles / locals with FP64 sums.

@@ -810,7 +810,10 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // NOUT = 3: potential and its gradient in the target position (rows of out,
 // stride ld_out); the gradient is summed on width-scaled coordinates and
 // scaled by 1/w in FP64.
-template <class KF32, class KF64, int NOUT>
+// PART: EVAL_FULL (L2T + P2P), EVAL_NEAR (P2P and its kernel-offset term
+// only, into near[], caller's point order) or EVAL_FAR (L2T and its offset
+// term only, plus near[]: out = far + near).
+template <class KF32, class KF64, int NOUT, int PART = EVAL_FULL>
 __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
     k_evaluate_mx(KernelParams kp, int neq, int np, const EvalDesc *__restrict__ desc,
                   const int *__restrict__ n_items_ptr, const double *__restrict__ sx,
@@ -819,7 +822,8 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
                   const double *__restrict__ lsum, const double *__restrict__ txs,
                   const double *__restrict__ tys, const int *__restrict__ tperm, int check,
                   int self_eval, double *__restrict__ out, int64_t ld_out,
-                  int *__restrict__ next_item) {
+                  int *__restrict__ next_item, double *__restrict__ near = nullptr) {
+  static_assert(PART == EVAL_FULL || NOUT == 1, "split evaluation: potential only");
   __shared__ EvalDesc D;
   __shared__ float4 src[SMAX];  // (x, y, charge, sorted index) in width units of the leaf
   // NOUT = 3: the low parts of the source coordinates (x = hi + lo): the
@@ -843,7 +847,8 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
     if (nxt < n_items && threadIdx.x < 32) nextw = __ldg(dw + (size_t)nxt * 32 + threadIdx.x);
     int after = 0;
     if (threadIdx.x == 0) after = atomicAdd(next_item, 1) + 2 * gridDim.x;
-    const int g = D.g, lev = D.lev, t0 = D.t0, cnt = D.cnt, ns = D.rs[9];
+    const int g = D.g, lev = D.lev, t0 = D.t0, cnt = D.cnt;
+    const int ns = PART == EVAL_FAR ? 0 : D.rs[9];
     int G = 1;
     while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
@@ -855,7 +860,7 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
     const float tx = (float)txd, ty = (float)tyd;
     const float tx_lo = (float)(txd - (double)tx), ty_lo = (float)(tyd - (double)ty);
     double acc = 0.0, accx = 0.0, accy = 0.0;  // accx, accy: kScale * (dx, dy) / d2 sums
-    if (lev >= 2 && valid) {  // L2T (flexmm/flexmm2d/kifmm.py:106-120), operands through L1
+    if (lev >= 2 && valid && PART != EVAL_NEAR) {  // L2T (flexmm/flexmm2d/kifmm.py:106-120), operands through L1
       const float *Lg = loc32 + (size_t)g * np;
       const float *lx = ops[lev].lx32, *ly = ops[lev].ly32;
       if constexpr (NOUT == 1) {
@@ -1126,7 +1131,11 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
     }
     double r[NOUT];
     r[0] = acc + exact;
-    if (sub == 0) r[0] += kofs * (D.csrc + (lev >= 2 ? lsum[g] : 0.0));  // FP64 kernel-offset terms
+    if (sub == 0) {  // FP64 kernel-offset terms: colleagues' charges (P2P), locals' sum (L2T)
+      const double cterm = PART == EVAL_FAR ? 0.0 : D.csrc;
+      const double lterm = (PART == EVAL_NEAR || lev < 2) ? 0.0 : lsum[g];
+      r[0] += kofs * (cterm + lterm);
+    }
     if constexpr (NOUT == 3) {
       const double gs = KF32::kGradScale / (double)KF32::kScale * iw;
       r[1] = accx * gs + exact_x;
@@ -1144,7 +1153,15 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
           for (int w = 0; w < G / 32; ++w) u += red[o][(threadIdx.x >> 5) + w];
         }
       }
-      if (valid && sub == 0) out[o * ld_out + tperm[t0 + t]] = u;
+      if (valid && sub == 0) {
+        const int i = tperm[t0 + t];
+        if constexpr (PART == EVAL_NEAR)
+          near[i] = u;
+        else if constexpr (PART == EVAL_FAR)
+          out[i] = u + near[i];
+        else
+          out[o * ld_out + i] = u;
+      }
     }
     if (threadIdx.x == 0) s_next = after;
     __syncthreads();  // D and src are rewritten by the next item
@@ -1296,6 +1313,52 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
   }
 }
 
+void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
+                                      const double *tsum, const float *loc32, const double *lsum,
+                                      int check, double *out, cudaStream_t s, const SplitEval &se) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const int64_t m = th.n_points;
+  if (m == 0) return;
+  FMMB_CHECK(a.kernel_id == KERNEL_LAPLACE, ERR_UNSUPPORTED, "unknown kernel id");
+  const int total = th.n_total();
+  FMMB_CUDA(cudaStreamWaitEvent(se.side, se.ready, 0));
+  EvalItems it;
+  eval_items(a, td.pkeys.get(), m, it, se.side);
+  DevBuf<EvalDesc> desc;
+  desc.alloc(total + m / TCH + 1, se.side);
+  DevBuf<int> next_item;  // [0] near-field, [1] far-field hand-out counters
+  next_item.alloc(2, se.side);
+  next_item.zero(se.side);
+  DevBuf<double> near;
+  near.alloc(m, se.side);
+  k_eval_desc<<<grid_for(total + m / TCH + 1, 256), 256, 0, se.side>>>(
+      it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+      td.ymid.get(), tsum, desc.get());
+  FMMB_CUDA(cudaGetLastError());
+  {
+    PhaseTimer timer(PH_EVAL, se.side);
+    k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>
+        <<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
+            a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
+            a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
+            next_item.get(), near.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
+  FMMB_CUDA(cudaEventRecord(se.near_done, se.side));
+  FMMB_CUDA(cudaStreamWaitEvent(s, se.near_done, 0));
+  {
+    PhaseTimer timer(PH_EVAL, s);
+    k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_FAR><<<148 * EVAL_BLOCKS_PER_SM, TCH, 0, s>>>(
+        a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
+        a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
+        next_item.get() + 1, near.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
+  FMMB_CUDA(cudaEventRecord(se.far_done, s));
+  FMMB_CUDA(cudaStreamWaitEvent(se.side, se.far_done, 0));
+}
+
 void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *tsum,
                         const float *loc32, const double *lsum, const double *txs,
                         const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
@@ -1327,7 +1390,7 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
       kern<<<148 * per_sm, TCH, 0, s>>>(a.kp, a.neq, a.np, desc.get(), it.n_items.get(),
                                         td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc32, lsum,
                                         txs, tys, tperm, check, self_eval, out, ld_out,
-                                        next_item.get());
+                                        next_item.get(), nullptr);
       break;
     }
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");

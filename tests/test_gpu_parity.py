@@ -287,3 +287,46 @@ def test_radial_table_kernel_device_matches_host_table(built_lib):
     np.testing.assert_allclose(got, k.table(r), rtol=1e-13)
     near = r < 10
     np.testing.assert_allclose(got[near], struve_gf(r[near]), rtol=5e-12)
+
+
+_UNSPLIT_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, {repo!r})
+from flexmm_b200 import KI_FMM, KI_Helper, workloads
+import torch
+d = workloads.clustered(n=120_000, n_grid=10, seed=44)
+x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
+out = {{}}
+for prec, neq in (("fp64", 40), ("mixed", 24)):
+    F = KI_FMM(x, y, "Laplace_Eval", 64, neq, bbox=d["bbox"], helper=KI_Helper(), precision=prec)
+    F.build_expansions(d["tau"])
+    out[prec] = F.source_evaluation(x, y).cpu().numpy()
+np.savez({path!r}, **out)
+"""
+
+
+def test_split_source_evaluation_equals_one_pass(built_lib, tmp_path):
+    """Own-source evaluation runs its near field on a side stream (from the
+    moment the charges are sorted) and adds the far field on the plan stream;
+    it equals the one-pass evaluation (FLEXMM_B200_SPLIT_EVAL=0, another
+    process) up to the order of the two sums, in both forms."""
+    import os
+    import subprocess
+    import sys
+    import torch
+    from conftest import REPO
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    path = str(tmp_path / "one_pass.npz")
+    env = dict(os.environ, FLEXMM_B200_SPLIT_EVAL="0")
+    subprocess.run([sys.executable, "-c", _UNSPLIT_SCRIPT.format(repo=REPO, path=path)], env=env,
+                   check=True, timeout=600)
+    ref = np.load(path)
+    d = workloads.clustered(n=120_000, n_grid=10, seed=44)
+    x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
+    for prec, neq in (("fp64", 40), ("mixed", 24)):
+        F = KI_FMM(x, y, "Laplace_Eval", 64, neq, bbox=d["bbox"], helper=KI_Helper(), precision=prec)
+        F.build_expansions(d["tau"])
+        got = F.source_evaluation(x, y).cpu().numpy()
+        F.status()
+        assert np.isfinite(got).all()
+        assert rel_l2(got, ref[prec]) < (1e-14 if prec == "fp64" else 1e-9), prec
