@@ -1021,14 +1021,19 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
                  m, check, nout, out, ld_out, s);
 }
 
-// FLEXMM_B200_SPLIT_EVAL=0 evaluates own sources in one pass on the plan
-// stream (near and far field together), for comparison
-bool split_enabled() {
-  static const bool on = [] {
+// Whether own-source evaluation runs split (near field beside the level
+// passes).  Measured at 1M clustered sources: the FP64 form gains ~0.6 ms
+// (its level passes are DMMA tiles that share SMs well); the mixed form
+// loses (its persistent tcgen05 M2L and smem-staged level kernels slow down
+// more beside the near field than the near field saves), so it evaluates in
+// one pass unless FLEXMM_B200_SPLIT_EVAL=1.  FLEXMM_B200_SPLIT_EVAL=0 turns
+// the split off for both forms.
+bool split_enabled(int precision) {
+  static const int mode = [] {
     const char *e = getenv("FLEXMM_B200_SPLIT_EVAL");
-    return !(e && e[0] == '0');
+    return e ? (e[0] == '0' ? 0 : 1) : -1;
   }();
-  return on;
+  return mode < 0 ? precision == PREC_FP64 : mode == 1;
 }
 
 void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t ld_out,
@@ -1049,7 +1054,7 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
   else if (p->ops->method == METHOD_BBFMM)
     run_bb_evaluate(bb_args(p, s), p->tau_s.get(), p->ple.get(), td.sx.get(), td.sy.get(),
                     td.pkeys.get(), td.ordv.get(), m, check, nout, out, ld_out, s);
-  else if (nout == 1 && p->ready_recorded && p->n_rhs == 1 && split_enabled()) {
+  else if (nout == 1 && p->ready_recorded && p->n_rhs == 1 && split_enabled(p->precision)) {
     // near field on the side stream, started when the charges were sorted
     const SplitEval se{p->side, p->ev_ready, p->ev_near, p->ev_far};
     if (p->precision == PREC_MIXED)

@@ -905,6 +905,15 @@ void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *l
   DevBuf<double> near;
   near.alloc(m, se.side);
   {
+    // the SMs keep their largest shared-memory carveout while near-field
+    // blocks sit on them, so the level passes' CTAs still fit beside them
+    static const bool carveout_set = [] {
+      FMMB_CUDA(cudaFuncSetAttribute(k_evaluate<KF, 1, EVAL_NEAR>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
+      return true;
+    }();
+    (void)carveout_set;
     PhaseTimer timer(PH_EVAL, se.side);
     k_evaluate<KF, 1, EVAL_NEAR><<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
         a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),

@@ -116,7 +116,11 @@ struct SplitEval {
   cudaStream_t side;
   cudaEvent_t ready, near_done, far_done;
 };
-constexpr int NEAR_BLOCKS_PER_SM = 4;  // near-field blocks per SM, leaving room for the level passes
+// near-field blocks per SM, leaving room for the level passes: FP64 (28 KB of
+// shared memory each) beside the DMMA M2L tiles; mixed (17 KB each) beside
+// one persistent tcgen05 M2L CTA (154 KB at Nequiv 24)
+constexpr int NEAR_BLOCKS_PER_SM = 4;
+constexpr int NEAR_BLOCKS_PER_SM_MIXED = 3;
 void run_evaluate_sources_split(const PassArgs &a, const double *tau_sorted, const double *loc,
                                 int check, double *out, cudaStream_t s, const SplitEval &se);
 void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_sorted,

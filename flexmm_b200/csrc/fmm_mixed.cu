@@ -1337,9 +1337,18 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
       td.ymid.get(), tsum, desc.get());
   FMMB_CUDA(cudaGetLastError());
   {
+    // the SMs keep their largest shared-memory carveout while near-field
+    // blocks sit on them, so the level passes' CTAs still fit beside them
+    static const bool carveout_set = [] {
+      FMMB_CUDA(cudaFuncSetAttribute(k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared));
+      return true;
+    }();
+    (void)carveout_set;
     PhaseTimer timer(PH_EVAL, se.side);
     k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>
-        <<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
+        <<<148 * NEAR_BLOCKS_PER_SM_MIXED, TCH, 0, se.side>>>(
             a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
             a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
             next_item.get(), near.get());

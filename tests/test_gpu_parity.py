@@ -306,10 +306,24 @@ np.savez({path!r}, **out)
 
 
 def test_split_source_evaluation_equals_one_pass(built_lib, tmp_path):
-    """Own-source evaluation runs its near field on a side stream (from the
-    moment the charges are sorted) and adds the far field on the plan stream;
-    it equals the one-pass evaluation (FLEXMM_B200_SPLIT_EVAL=0, another
-    process) up to the order of the two sums, in both forms."""
+    import os
+    if os.environ.get("FLEXMM_B200_SPLIT_EVAL") != "1":   # the mode is read once per process
+        import subprocess
+        import sys
+        env = dict(os.environ, FLEXMM_B200_SPLIT_EVAL="1")
+        r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", __file__ + "::"
+                            "test_split_source_evaluation_equals_one_pass"], env=env, timeout=900)
+        assert r.returncode == 0
+        return
+    _split_vs_one_pass(tmp_path)
+
+
+def _split_vs_one_pass(tmp_path):
+    """Own-source evaluation split in two -- the near field on a side stream
+    from the moment the charges are sorted, the far field on the plan stream
+    adding it -- equals the one-pass evaluation up to the order of the two
+    sums, in both forms (this process: FLEXMM_B200_SPLIT_EVAL=1, split in
+    both forms; the other process: =0, one pass)."""
     import os
     import subprocess
     import sys
