@@ -237,6 +237,8 @@ struct fmm_plan {
   cublasHandle_t blas = nullptr;  // black-box and Stokes FMM translations
   // split own-source evaluation (near field on a side stream, see SplitEval):
   // `ready` is recorded once a single-column KIFMM build has sorted its charges
+  DevBuf<double> dvx, dvy;  // dipole sources: strength * normal, sorted (see PassArgs)
+  bool has_dipoles = false;
   cudaStream_t side = nullptr;  // from the device's pool, not owned
   cudaEvent_t ev_ready = nullptr, ev_near = nullptr, ev_far = nullptr;
   bool ready_recorded = false;
@@ -713,7 +715,22 @@ static PassArgs pass_args(fmm_plan *p) {
   a.td = &p->td;
   a.th = &p->th;
   a.ops_dev = p->ops_dev.get();
+  if (p->has_dipoles) {
+    a.dvx = p->dvx.get();
+    a.dvy = p->dvy.get();
+  }
   return a;
+}
+
+__global__ void k_gather_dipoles(const double *__restrict__ str, const double *__restrict__ nx,
+                                 const double *__restrict__ ny, const int *__restrict__ ordv,
+                                 int64_t n, double *__restrict__ dvx, double *__restrict__ dvy) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int o = ordv[i];
+    dvx[i] = str[o] * nx[o];
+    dvy[i] = str[o] * ny[o];
+  }
 }
 
 // The plan's per-level operator table, gathered on the device from the
@@ -839,6 +856,7 @@ int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_
       run_downward(a, p->ple.get() + (size_t)r * cs, p->loc.get() + (size_t)r * cs, s);
     }
     p->n_rhs = n_rhs;
+    p->has_dipoles = false;
     p->ready_recorded = false;  // the split evaluation serves single-column builds
     p->have_expansions = true;
   });
@@ -892,12 +910,46 @@ int fmm_evaluate_sources_multi(fmm_plan *p, int check, double *out, int64_t ld_o
   });
 }
 
+static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream);
+
 int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
   return guarded([&] {
     tree_ready(p);
     FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(p->ops->method != METHOD_STOKES, ERR_INVALID_ARGUMENT,
                "Stokes plans take fmm_build_expansions2 (two force components)");
+    p->has_dipoles = false;
+    build_expansions_impl(p, tau, stream);
+  });
+}
+
+int fmm_build_expansions_dipole(fmm_plan *p, const double *tau, const double *dip_str,
+                                const double *dip_nx, const double *dip_ny, void *stream) {
+  return guarded([&] {
+    tree_ready(p);
+    FMMB_CHECK(p && dip_str && dip_nx && dip_ny, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(p->ops->method == METHOD_KIFMM && p->ops->kernel_id == KERNEL_LAPLACE,
+               ERR_UNSUPPORTED, "dipole sources: KIFMM plans of the Laplace kernel");
+    FMMB_CHECK(p->precision == PREC_FP64, ERR_UNSUPPORTED, "dipole sources: FP64 form only");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = p->th.n_points;
+    p->dvx.alloc(n, s);
+    p->dvy.alloc(n, s);
+    if (n > 0) {
+      k_gather_dipoles<<<grid_for(n, 256), 256, 0, s>>>(dip_str, dip_nx, dip_ny,
+                                                         p->td.ordv.get(), n, p->dvx.get(),
+                                                         p->dvy.get());
+      FMMB_CUDA(cudaGetLastError());
+    }
+    p->has_dipoles = true;
+    build_expansions_impl(p, tau, stream);
+  });
+}
+
+// the build itself (FP64 / mixed KIFMM or black-box), after the entry's checks;
+// tau = NULL: zero charges
+static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream) {
+  {
     p->n_rhs = 1;
     cudaStream_t s = (cudaStream_t)stream;
     const TreeHost &th = p->th;
@@ -924,7 +976,10 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
     p->ready_recorded = false;
     PassArgs a = pass_args(p);
     p->tau_s.alloc(th.n_points, s);
-    gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
+    if (tau)
+      gather_sorted(tau, p->td.ordv.get(), th.n_points, p->tau_s.get(), s);
+    else
+      p->tau_s.zero(s);
     p->ple.alloc(total * np, s);
     p->ple.zero(s);
     if (p->precision == PREC_MIXED) {
@@ -964,7 +1019,7 @@ int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {
       run_downward(a, p->ple.get(), p->loc.get(), s);
     }
     p->have_expansions = true;
-  });
+  }
 }
 
 namespace {
@@ -1139,6 +1194,9 @@ int fmm_plan_drop_expansions(fmm_plan *p) {
     p->lsum.release();
     p->tsum.release();
     p->partial.release();
+    p->dvx.release();
+    p->dvy.release();
+    p->has_dipoles = false;
     p->have_expansions = false;
     p->ready_recorded = false;
   });
@@ -1295,6 +1353,8 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
                "fmm_evaluate_noalloc evaluates FP64 plans only");
     FMMB_CHECK(p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
                "fmm_evaluate_noalloc evaluates KIFMM plans only");
+    FMMB_CHECK(!p->has_dipoles, ERR_UNSUPPORTED,
+               "fmm_evaluate_noalloc evaluates charge sources only (no dipoles)");
     FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
     FMMB_CHECK(m <= FMM_NOALLOC_MAX_TARGETS, ERR_CAPACITY,
                "fmm_evaluate_noalloc: more than FMM_NOALLOC_MAX_TARGETS targets");

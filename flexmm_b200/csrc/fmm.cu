@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fmm.cuh"
 #include "gemm.cuh"
@@ -86,7 +87,16 @@ __device__ __forceinline__ double kernel_at(const KF &K, double ax, double ay) {
 // sums one node's sources into its check potentials (lanes over check
 // points, the node's sources staged 32 at a time, four independent sums
 // per lane); C2E runs once for each level the tile holds.
-template <class KF>
+constexpr double INV_2PI = 1.0 / (2.0 * M_PI);
+
+// double-layer kernel of the Laplace kernel -log(r^2)/(4 pi): the field at
+// offset (ax, ay) = target - source of a dipole (dx, dy) = strength * normal,
+// (d . a) / (2 pi |a|^2) (Laplace_Both_Eval, examples/pure_kifmm_laplace_dipoles.py:31-40)
+__device__ __forceinline__ double dipole_at(double dx, double dy, double ax, double ay) {
+  return fma(dx, ax, dy * ay) / fma(ax, ax, ay * ay) * INV_2PI;
+}
+
+template <class KF, bool DIP = false>
 __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, int L,
                                             const int *__restrict__ off,
                                             const int *__restrict__ uplist,
@@ -99,12 +109,15 @@ __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, in
                                             const double *__restrict__ sy,
                                             const double *__restrict__ tau,
                                             const LevelOpsDev *__restrict__ ops,
-                                            double *__restrict__ mult) {
+                                            double *__restrict__ mult,
+                                            const double *__restrict__ dvx = nullptr,
+                                            const double *__restrict__ dvy = nullptr) {
   extern __shared__ double smem[];
   const int ldp = pad_ld(np);
   double *P = smem;          // [TN][ldp] check potentials
   double *T = P + TN * ldp;  // [TN][ldp] C2E scratch
   __shared__ double srcx[NT / 32][32], srcy[NT / 32][32], srct[NT / 32][32];
+  __shared__ double srcdx[DIP ? NT / 32 : 1][32], srcdy[DIP ? NT / 32 : 1][32];
   __shared__ int node[TN], nlev[TN];
   __shared__ double *orow[TN];
   __shared__ FunctorSmem<KF> fsm;
@@ -138,24 +151,37 @@ __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, in
           srcx[warp][lane] = sx[j0 + lane] - cx;
           srcy[warp][lane] = sy[j0 + lane] - cy;
           srct[warp][lane] = tau[j0 + lane] * fold;
+          if constexpr (DIP) {
+            srcdx[warp][lane] = dvx[j0 + lane];
+            srcdy[warp][lane] = dvy[j0 + lane];
+          }
         } else {  // padding pairs: zero charge at a harmless distance
           srcx[warp][lane] = 0.0;
           srcy[warp][lane] = 0.0;
           srct[warp][lane] = 0.0;
+          if constexpr (DIP) {
+            srcdx[warp][lane] = 0.0;
+            srcdy[warp][lane] = 0.0;
+          }
         }
         __syncwarp();
         const int nj2 = (nj + 1) & ~1;
+        // one source's contribution at check point (lx, ly)
+        auto term = [&](double lx, double ly, int j) -> double {
+          const double ax = lx - srcx[warp][j], ay = ly - srcy[warp][j];
+          double v = kernel_at(K, ax, ay) * srct[warp][j];
+          if constexpr (DIP) v += dipole_at(srcdx[warp][j], srcdy[warp][j], ax, ay);
+          return v;
+        };
         if (k0)
           for (int j = 0; j < nj2; j += 2) {
-            a0 = fma(kernel_at(K, lx0 - srcx[warp][j], ly0 - srcy[warp][j]), srct[warp][j], a0);
-            b0 = fma(kernel_at(K, lx0 - srcx[warp][j + 1], ly0 - srcy[warp][j + 1]),
-                     srct[warp][j + 1], b0);
+            a0 += term(lx0, ly0, j);
+            b0 += term(lx0, ly0, j + 1);
           }
         if (k1)
           for (int j = 0; j < nj2; j += 2) {
-            a1 = fma(kernel_at(K, lx1 - srcx[warp][j], ly1 - srcy[warp][j]), srct[warp][j], a1);
-            b1 = fma(kernel_at(K, lx1 - srcx[warp][j + 1], ly1 - srcy[warp][j + 1]),
-                     srct[warp][j + 1], b1);
+            a1 += term(lx1, ly1, j);
+            b1 += term(lx1, ly1, j + 1);
           }
         __syncwarp();
       }
@@ -439,7 +465,9 @@ __global__ void k_make_items(int total, int L, const int *__restrict__ off, cons
 // position (rows of out, stride ld_out).
 // PART: EVAL_FULL (L2T + P2P), EVAL_NEAR (P2P only, into near[], caller's
 // point order) or EVAL_FAR (L2T only, plus near[]: out = far + near).
-template <class KF, int NOUT, int PART = EVAL_FULL>
+// DIP: the sources also carry dipoles (dvx, dvy: strength * normal, sorted);
+// Laplace (table-driven functor), potential only.
+template <class KF, int NOUT, int PART = EVAL_FULL, bool DIP = false>
 __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np,
                                                   const int4 *__restrict__ items,
                                                   const int *__restrict__ n_items_ptr,
@@ -457,10 +485,14 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
                                                   const double *__restrict__ tys,
                                                   const int *__restrict__ tperm, int check,
                                                   double *__restrict__ out, int64_t ld_out,
-                                                  double *__restrict__ near = nullptr) {
+                                                  double *__restrict__ near = nullptr,
+                                                  const double *__restrict__ dvx = nullptr,
+                                                  const double *__restrict__ dvy = nullptr) {
   static_assert(PART == EVAL_FULL || NOUT == 1, "split evaluation: potential only");
+  static_assert(!DIP || (KF::kLogTable && NOUT == 1), "dipoles: table Laplace, potential only");
   __shared__ double Ls[64], lxs[64], lys[64];
   __shared__ double ssx[SMAX], ssy[SMAX], stau[SMAX];
+  __shared__ double sdx[DIP ? SMAX : 1], sdy[DIP ? SMAX : 1];
   __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
   __shared__ double red[NOUT][TCH / 32];
   __shared__ FunctorSmem<KF> fsm;
@@ -524,7 +556,11 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     // a coincident pair is skipped when check is set (helpers.py:99-107)
     auto pair = [&](int j) -> double {
       const double qx = ssx[j], qy = ssy[j];
-      if constexpr (kFolded) {
+      if constexpr (DIP) {  // single plus double layer; coincident pairs skipped when check
+        const double ax = x - qx, ay = y - qy;
+        if (check && ax == 0.0 && ay == 0.0) return 0.0;
+        return K.raw(ax, ay) * stau[j] + dipole_at(sdx[j], sdy[j], ax, ay);
+      } else if constexpr (kFolded) {
         return K.raw_checked(qx, qy, x, y, check) * stau[j];
       } else {
         const double v = K(qx, qy, x, y) * stau[j];
@@ -542,6 +578,10 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
         ssx[i] = sx[j];
         ssy[i] = sy[j];
         stau[i] = tau[j] * fold;
+        if constexpr (DIP) {
+          sdx[i] = dvx[j];
+          sdy[i] = dvy[j];
+        }
       }
       __syncthreads();
       if (valid) {
@@ -755,10 +795,24 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(s2m_bytes)));
   PhaseTimer timer(PH_UPWARD, s);
-  k_s2m<KF><<<148 * 4, NT, s2m_bytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
-                                           td.uplist.get(), td.n_up.get(), td.bot.get(),
-                                           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
-                                           td.sy.get(), tau_s, a.ops_dev, mult);
+  if (a.dvx) {
+    if constexpr (std::is_same<KF, LaplaceF64T>::value) {
+      FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(s2m_bytes)));
+      k_s2m<KF, true><<<148 * 4, NT, s2m_bytes, s>>>(
+          a.kp, a.neq, np, th.L, td.dev_off.get(), td.uplist.get(), td.n_up.get(), td.bot.get(),
+          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+          mult, a.dvx, a.dvy);
+    } else {
+      throw Error(ERR_UNSUPPORTED, "dipole sources: Laplace kernel only");
+    }
+  } else {
+    k_s2m<KF><<<148 * 4, NT, s2m_bytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
+                                             td.uplist.get(), td.n_up.get(), td.bot.get(),
+                                             td.top.get(), td.xmid.get(), td.ymid.get(),
+                                             td.sx.get(), td.sy.get(), tau_s, a.ops_dev, mult,
+                                             nullptr, nullptr);
+  }
   FMMB_CUDA(cudaGetLastError());
   const size_t m2m_bytes = sizeof(double) * (size_t)TN * (2 * pad_ld(np) + pad_ld(4 * np));
   FMMB_CUDA(cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -813,11 +867,23 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
   EvalItems it;
   eval_items(a, tkeys, m, it, s);
   PhaseTimer timer(PH_EVAL, s);
-  auto kern = nout == 3 ? k_evaluate<KF, 3> : k_evaluate<KF, 1>;
-  kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(),
-                               td.bot.get(), td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
-                               td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out,
-                               ld_out, nullptr);
+  if (a.dvx) {
+    FMMB_CHECK(nout == 1, ERR_UNSUPPORTED, "dipole sources: potential only");
+    if constexpr (std::is_same<KF, LaplaceF64T>::value) {
+      k_evaluate<KF, 1, EVAL_FULL, true><<<148 * 5, TCH, 0, s>>>(
+          a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+          td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+          loc, txs, tys, tperm, check, out, ld_out, nullptr, a.dvx, a.dvy);
+    } else {
+      throw Error(ERR_UNSUPPORTED, "dipole sources: Laplace kernel only");
+    }
+  } else {
+    auto kern = nout == 3 ? k_evaluate<KF, 3> : k_evaluate<KF, 1>;
+    kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(),
+                                 td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
+                                 td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc,
+                                 txs, tys, tperm, check, out, ld_out, nullptr, nullptr, nullptr);
+  }
   FMMB_CUDA(cudaGetLastError());
 }
 }  // namespace
@@ -894,7 +960,7 @@ void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, con
 }
 
 namespace {
-template <class KF>
+template <class KF, bool DIP>
 void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *loc, int check,
                          double *out, cudaStream_t s, const SplitEval &se) {
   const TreeDev &td = *a.td;
@@ -908,17 +974,17 @@ void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *l
     // the SMs keep their largest shared-memory carveout while near-field
     // blocks sit on them, so the level passes' CTAs still fit beside them
     static const bool carveout_set = [] {
-      FMMB_CUDA(cudaFuncSetAttribute(k_evaluate<KF, 1, EVAL_NEAR>,
+      FMMB_CUDA(cudaFuncSetAttribute(k_evaluate<KF, 1, EVAL_NEAR, DIP>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
       return true;
     }();
     (void)carveout_set;
     PhaseTimer timer(PH_EVAL, se.side);
-    k_evaluate<KF, 1, EVAL_NEAR><<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
+    k_evaluate<KF, 1, EVAL_NEAR, DIP><<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
         a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
         td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
-        loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get());
+        loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get(), a.dvx, a.dvy);
     FMMB_CUDA(cudaGetLastError());
   }
   FMMB_CUDA(cudaEventRecord(se.near_done, se.side));
@@ -928,7 +994,8 @@ void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *l
     k_evaluate<KF, 1, EVAL_FAR><<<148 * 8, TCH, 0, s>>>(
         a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
         td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
-        loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get());
+        loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get(), nullptr,
+        nullptr);
     FMMB_CUDA(cudaGetLastError());
   }
   // the scratch (allocated on the side stream) is freed there once the plan
@@ -985,12 +1052,19 @@ void run_evaluate_sources_split(const PassArgs &a, const double *tau_s, const do
                                 int check, double *out, cudaStream_t s, const SplitEval &se) {
   if (a.th->n_points == 0) return;
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE: evaluate_split_impl<LaplaceF64T>(a, tau_s, loc, check, out, s, se); break;
+    case KERNEL_LAPLACE:
+      if (a.dvx)
+        evaluate_split_impl<LaplaceF64T, true>(a, tau_s, loc, check, out, s, se);
+      else
+        evaluate_split_impl<LaplaceF64T, false>(a, tau_s, loc, check, out, s, se);
+      break;
     case KERNEL_MOD_HELMHOLTZ:
-      evaluate_split_impl<ModHelmholtzF64>(a, tau_s, loc, check, out, s, se);
+      FMMB_CHECK(!a.dvx, ERR_UNSUPPORTED, "dipole sources: Laplace kernel only");
+      evaluate_split_impl<ModHelmholtzF64, false>(a, tau_s, loc, check, out, s, se);
       break;
     case KERNEL_RADIAL_TABLE:
-      evaluate_split_impl<RadialTableF64>(a, tau_s, loc, check, out, s, se);
+      FMMB_CHECK(!a.dvx, ERR_UNSUPPORTED, "dipole sources: Laplace kernel only");
+      evaluate_split_impl<RadialTableF64, false>(a, tau_s, loc, check, out, s, se);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
@@ -1046,7 +1120,7 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
     kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(),
                                  td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
                                  td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0,
-                                 nullptr);
+                                 nullptr, nullptr, nullptr);
   };
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: launch(k_evaluate<LaplaceF64T, 1>); break;

@@ -49,6 +49,9 @@ struct PassArgs {
   const TreeDev *td;
   const TreeHost *th;
   const LevelOpsDev *ops_dev;   // device array indexed by level
+  // dipole sources (Laplace double layer): per sorted source the dipole
+  // vector strength * normal; null when the sources carry charges only
+  const double *dvx = nullptr, *dvy = nullptr;
 };
 
 // Black-box (Chebyshev) FMM (bbfmm.cu): p x p coefficients per box, NQ = p^2

@@ -165,7 +165,20 @@ class OpsSet:
         self.handle = None
 
 
+class _NamedForm:
+    """A placeholder for one of the reference helper's compiled functions
+    (helper.functions[...]): only its name matters here, the device forms are
+    built in (register_evaluator / register_upwardor match it by name)."""
+
+    def __init__(self, name):
+        self.__name__ = name
+
+    def __repr__(self):
+        return f"<built-in {self.__name__}>"
+
+
 class KI_Helper:
+
     """Operator cache for one (kernel, Nequiv) (Helper, flexmm/flexmm2d/helpers.py:35-84).
 
     ``cache_dir`` (or the environment variable FLEXMM_B200_CACHE) keeps the
@@ -177,6 +190,11 @@ class KI_Helper:
     the reference (the tree, and so the results, never depend on what an
     earlier run left on disk).  Tabulated kernels (``radial``) are not cached
     on disk: their identity is not in their parameters."""
+
+    # the names of the reference helper's base functions that scripts pass
+    # back to register_evaluator / register_upwardor
+    # (flexmm/kifmm2d/scalar/helpers.py:113-124)
+    functions = {n: _NamedForm(n) for n in ("kernel_app", "extra_kernel_app")}
 
     def __init__(self, helper=None, cache_dir=None):
         self.kernel = None

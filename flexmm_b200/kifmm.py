@@ -203,6 +203,8 @@ class KI_FMM:
         self._expanded = False
         # named evaluators (kifmm2d FMM.__init__ registers 'potential_evaluation')
         self._evaluators = {"potential_evaluation": "potential"}
+        # named upwardors (kifmm2d FMM.__init__ registers 'slp')
+        self._upwardors = {"slp": "slp"}
 
     @property
     def _counts(self):
@@ -217,10 +219,42 @@ class KI_FMM:
             self._tree = TreeView(self)
         return self._tree
 
-    def build_expansions(self, tau):
+    # device upwardors: the reference compiles a user's numba source function
+    # (KAS(sx, sy, tx, ty, tau, extras)) into its S2M loop; here a function is
+    # mapped by its name to the built-in device form of the same sum
+    _UPWARDOR_KINDS = {"slp": "slp", "extra_kernel_app": "slp", "kernel_app": "slp",
+                       "slp+dlp": "slp+dlp", "Laplace_Both_Eval": "slp+dlp"}
+
+    def register_upwardor(self, KAS, name):
+        """Name a source-to-multipole form (kifmm2d FMM.register_upwardor,
+        flexmm/kifmm2d/scalar/fmm.py:174-176, helpers.py:155-173).  Built in:
+        'slp' (charges) and 'slp+dlp' (charges and dipoles: the reference
+        example's Laplace_Both_Eval, examples/pure_kifmm_laplace_dipoles.py:31-40,
+        with tau = [charge, dipole strength] and extras = normals [nx, ny]).
+        KAS is that function (matched by its name) or one of those names."""
+        key = KAS if isinstance(KAS, str) else getattr(getattr(KAS, "py_func", KAS), "__name__", None)
+        kind = self._UPWARDOR_KINDS.get(key)
+        if kind is None:
+            raise NotImplementedError(f"no device form of upwardor {key!r}; built in: "
+                                      f"{sorted(self._UPWARDOR_KINDS)}")
+        if kind == "slp+dlp" and self.kernel.kernel_id != 0:
+            raise NotImplementedError("the double layer is built in for Laplace_Eval only")
+        self._upwardors[name] = kind
+
+    def build_expansions(self, tau, name=None, extras=None):
         """Charges in the caller's source order: [N], or [k, N] for k charge
-        columns on one tree (kifmm2d's tau layout, flexmm/kifmm2d/scalar/fmm.py:71-87;
-        FP64 form), whose evaluations then return [k, M]."""
+        columns on one tree (FP64 form), whose evaluations then return [k, M].
+
+        ``name`` selects a registered upwardor (kifmm2d's
+        build_expansions(tau, name, extras), flexmm/kifmm2d/scalar/fmm.py:168-170):
+        with an 'slp+dlp' upwardor tau is [2, N] (charge, dipole strength)
+        and ``extras`` [2, N] the dipole normals, and every later evaluation
+        includes both layers."""
+        kind = "slp" if name is None else self._upwardors.get(name)
+        if kind is None:
+            raise KeyError(f"upwardor {name!r} is not registered; registered: {sorted(self._upwardors)}")
+        if kind == "slp+dlp":
+            return self._build_dipole(tau, extras)
         self._n_rhs = None
         if np.ndim(tau) == 2:
             torch = _torch()
@@ -245,6 +279,23 @@ class KI_FMM:
         if self.verbose:
             _torch().cuda.synchronize()
             print("....Time for expansions:        {:0.2f}".format(1000 * (time.time() - st)))
+
+    def _build_dipole(self, tau, extras):
+        if extras is None:
+            raise ValueError("the 'slp+dlp' upwardor needs extras = [nx, ny] (dipole normals)")
+        torch = _torch()
+        dev = lambda a: (a if isinstance(a, torch.Tensor)
+                         else torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)))
+        t = dev(tau).to(device="cuda", dtype=torch.float64).contiguous()
+        e = dev(extras).to(device="cuda", dtype=torch.float64).contiguous()
+        if t.shape != (2, self.N) or e.shape != (2, self.N):
+            raise ValueError(f"'slp+dlp' takes tau [2, {self.N}] and extras [2, {self.N}]")
+        self._n_rhs = None
+        p = lambda a: ctypes.c_void_p(a.data_ptr())
+        _lib.call("fmm_build_expansions_dipole", self._plan, p(t[0]), p(t[1]), p(e[0]), p(e[1]),
+                  _stream())
+        self._tau, self._extras = t, e   # kept alive until the stream has consumed them
+        self._expanded = True
 
     def drop_expansions(self):
         """Release the expansions, keep the tree; build_expansions forms them again."""

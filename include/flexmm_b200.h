@@ -180,6 +180,19 @@ int fmm_evaluate(fmm_plan *plan, const double *tx, const double *ty, int64_t m, 
  * the FMM's own sources (flexmm/flexmm2d/fmm.py:158-159, 162-176). */
 int fmm_evaluate_sources(fmm_plan *plan, int check, double *out, void *stream);
 
+/* Charges and dipoles: the Laplace single plus double layer of the
+ * reference's kifmm2d FMM with the example's upwardor Laplace_Both_Eval
+ * (build_expansions(tau, 'slp+dlp', extras), flexmm/kifmm2d/scalar/fmm.py:73-124,
+ * 168-176; examples/pure_kifmm_laplace_dipoles.py:31-40, 94-98): source j
+ * carries the charge tau[j] (NULL: none) and the dipole of strength
+ * dip_str[j] along the normal (dip_nx[j], dip_ny[j]), all device arrays in the
+ * caller's source order.  The field at t of a source at s is
+ *   -log|t - s|^2 / (4 pi) tau + (n . (t - s)) / |t - s|^2 / (2 pi) str.
+ * FP64 KIFMM plans of the Laplace kernel.  Evaluations after it (potential
+ * only) include both layers in the near field; the expansions carry both. */
+int fmm_build_expansions_dipole(fmm_plan *plan, const double *tau, const double *dip_str,
+                                const double *dip_nx, const double *dip_ny, void *stream);
+
 /* Several charge columns on one tree (multi-RHS; the reference's kifmm2d
  * FMM takes tau [k, N], flexmm/kifmm2d/scalar/fmm.py:71-87): column r is
  * tau[r * ld_tau .. + n), caller's source order.  FP64 KIFMM plans.  The

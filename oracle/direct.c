@@ -86,3 +86,28 @@ void oracle_direct_stokes(const double *sx, const double *sy, const double *fx,
         out[2 * nt + j] = p * ps;
     }
 }
+
+/* Laplace single plus double layer: the reference example's
+ * Laplace_Both_Eval (examples/pure_kifmm_laplace_dipoles.py:31-40),
+ *   -log(d^2)/(4 pi) slp + (n . d)/d^2 / (2 pi) dlp,  d = target - source,
+ * summed over all sources (normal (nx, ny) per source), coincident pairs
+ * skipped when check (flexmm/kifmm2d/scalar/helpers.py:200-205). */
+void oracle_direct_laplace_dipole(const double *sx, const double *sy, const double *slp,
+                                  const double *dlp, const double *nx, const double *ny,
+                                  int64_t ns, const double *tx, const double *ty, int64_t nt,
+                                  int check, double *out)
+{
+    const double c = 1.0 / (4.0 * M_PI), g = 1.0 / (2.0 * M_PI);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t j = 0; j < nt; ++j) {
+        double acc = 0.0;
+        const double x = tx[j], y = ty[j];
+        for (int64_t i = 0; i < ns; ++i) {
+            double dx = x - sx[i], dy = y - sy[i];
+            if (check && dx == 0.0 && dy == 0.0) continue;
+            double d2 = dx * dx + dy * dy;
+            acc += -log(d2) * c * slp[i] + (nx[i] * dx + ny[i] * dy) / d2 * g * dlp[i];
+        }
+        out[j] = acc;
+    }
+}

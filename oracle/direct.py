@@ -29,6 +29,9 @@ def _load():
         g = _lib.oracle_direct_laplace_grad
         g.argtypes = f.argtypes
         g.restype = None
+        dd = _lib.oracle_direct_laplace_dipole
+        dd.argtypes = [dp, dp, dp, dp, dp, dp, ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
+        dd.restype = None
         h = _lib.oracle_direct_stokes
         h.argtypes = [dp, dp, dp, dp, ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
         h.restype = None
@@ -45,6 +48,17 @@ def direct_laplace(sx, sy, tau, tx, ty, check):
     out = np.empty(tx.size)
     lib.oracle_direct_laplace(_p(sx), _p(sy), _p(tau), sx.size, _p(tx), _p(ty), tx.size,
                               1 if check else 0, _p(out))
+    return out
+
+
+def direct_laplace_dipole(sx, sy, slp, dlp, nx, ny, tx, ty, check):
+    """FP64 direct sum of the Laplace single + double layer
+    (examples/pure_kifmm_laplace_dipoles.py:31-40)."""
+    lib = _load()
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, slp, dlp, nx, ny, tx, ty)]
+    out = np.empty(a[6].size)
+    lib.oracle_direct_laplace_dipole(*[_p(v) for v in a[:6]], a[0].size, _p(a[6]), _p(a[7]),
+                                     a[6].size, 1 if check else 0, _p(out))
     return out
 
 

@@ -17,14 +17,18 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
-def golden_cases(gradient=False, stokes=False):
+def golden_cases(gradient=False, stokes=False, dipole=False):
     """Fixture names: potential cases; (gradient=True) the grad_* cases whose
     results are [3, n] rows (u, du/dx, du/dy); (stokes=True) the stokes_*
-    cases, rows (u, v, p)."""
+    cases, rows (u, v, p); (dipole=True) the dip_* cases (single plus
+    double layer through kifmm2d's upwardor / evaluator)."""
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
     if stokes:
         return [n for n in names if n.startswith("stokes_")]
-    return [n for n in names if n.startswith("grad_") == gradient and not n.startswith("stokes_")]
+    if dipole:
+        return [n for n in names if n.startswith("dip_")]
+    return [n for n in names if n.startswith("grad_") == gradient
+            and not n.startswith(("stokes_", "dip_"))]
 
 
 def load_golden(name):

@@ -91,6 +91,11 @@ def case_inputs(meta):
         d["bbox"] = None
     if meta.get("method") == "stokes":  # second force component
         d["tau2"] = np.random.default_rng(meta["seed"] + 1000).standard_normal(d["x"].size)
+    if meta.get("dipole"):  # double-layer strengths and unit normals
+        r2 = np.random.default_rng(meta["seed"] + 2000)
+        d["dlp"] = r2.standard_normal(d["x"].size)
+        th = r2.uniform(0, 2 * np.pi, d["x"].size)
+        d["nx"], d["ny"] = np.cos(th), np.sin(th)
     return d
 
 
@@ -133,6 +138,12 @@ CASES = {
                                       neq=32, method="stokes"), True),
     "stokes_duplicates_5k_q24": (dict(recipe="duplicates", seed=30, n=5000, n_grid=33, ncut=16,
                                       neq=24, method="stokes"), True),
+    "dip_uniform_5k_q24": (dict(recipe="uniform", seed=31, n=5000, n_grid=41, ncut=32, neq=24,
+                                dipole=True), True),
+    "dip_clustered_20k_q32": (dict(recipe="clustered", seed=32, n=20000, n_grid=64, ncut=64,
+                                   neq=32, dipole=True), True),
+    "dip_duplicates_5k_q24": (dict(recipe="duplicates", seed=33, n=5000, n_grid=33, ncut=16,
+                                   neq=24, dipole=True), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -322,6 +333,54 @@ def run_gradient_case(name, meta, ref):
           flush=True)
 
 
+def run_dipole_case(name, meta, ref):
+    """Single plus double layer through the reference's kifmm2d FMM, as
+    examples/pure_kifmm_laplace_dipoles.py:94-98 drives it: the upwardor and
+    the evaluator Laplace_Both_Eval, tau = [slp, dlp], extras = normals."""
+    import numba
+    from flexmm.kifmm2d.scalar.fmm import FMM
+    Laplace_Eval = reference_kernel(meta)
+
+    # examples/pure_kifmm_laplace_dipoles.py:31-40
+    @numba.njit(fastmath=True)
+    def Laplace_Both_Eval(sx, sy, tx, ty, tau, extras):
+        nx = extras[0]
+        ny = extras[1]
+        dx = tx - sx
+        dy = ty - sy
+        n_dot_d = nx * dx + ny * dy
+        d2 = dx * dx + dy * dy
+        return (-np.log(d2) / (4 * np.pi) * tau[0] + n_dot_d / d2 / (2 * np.pi) * tau[1],)
+
+    d = case_inputs(meta)
+    tau = np.vstack([d["tau"], d["dlp"]])
+    dipvec = np.vstack([d["nx"], d["ny"]])
+    t0 = time.time()
+    F = FMM(d["x"], d["y"], Laplace_Eval, meta["ncut"], meta["neq"], bbox=d["bbox"])
+    F.register_upwardor(Laplace_Both_Eval, "slp+dlp")
+    F.register_evaluator(F.helper.functions["kernel_app"], Laplace_Both_Eval, "slp+dlp->u", 1)
+    F.build_expansions(tau, "slp+dlp", dipvec)
+    us = F.evaluate_to_points(d["x"], d["y"], "slp+dlp->u", True)[0]
+    ut = F.evaluate_to_points(d["tx"], d["ty"], "slp+dlp->u", False)[0]
+    t1 = time.time()
+    from oracle.direct import direct_laplace_dipole
+    ds = direct_laplace_dipole(d["x"], d["y"], d["tau"], d["dlp"], d["nx"], d["ny"], d["x"], d["y"], True)
+    dt = direct_laplace_dipole(d["x"], d["y"], d["tau"], d["dlp"], d["nx"], d["ny"], d["tx"], d["ty"],
+                               False)
+    out = dict(
+        meta=json.dumps(meta),
+        inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"], d["dlp"], d["nx"], d["ny"]),
+        bbox_used=np.array(F.bbox, dtype=np.float64),
+        levels=np.int64(F.tree.levels),
+        src_idx=np.arange(d["x"].size), src_val=us, tgt_idx=np.arange(d["tx"].size), tgt_val=ut,
+        direct_src=ds, direct_tgt=dt,
+    )
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"{name}: levels {F.tree.levels} ref {t1 - t0:.1f}s  err vs direct src {rel(us, ds):.2e} "
+          f"tgt {rel(ut, dt):.2e}", flush=True)
+
+
 def run_stokes_case(name, meta, ref):
     """The reference's Stokes FMM (flexmm/kifmm2d/vector/stokes_fmm.py:592-858):
     src_val / tgt_val are [3, n] rows (u, v, p)."""
@@ -390,6 +449,8 @@ def main():
             continue
         if meta.get("method") == "stokes":
             run_stokes_case(name, meta, ref)
+        elif meta.get("dipole"):
+            run_dipole_case(name, meta, ref)
         else:
             (run_gradient_case if meta.get("gradient") else run_case)(name, meta, ref)
 

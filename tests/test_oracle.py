@@ -69,6 +69,20 @@ def test_golden_inputs_regenerate_bitwise():
         g = load_golden(case)
         d = golden_inputs(g["meta"])
         assert make_golden.sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]) == str(g["inputs_sha"]), case
+    for case in golden_cases(dipole=True):
+        g = load_golden(case)
+        d = golden_inputs(g["meta"])
+        got = make_golden.sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"], d["dlp"], d["nx"], d["ny"])
+        assert got == str(g["inputs_sha"]), case
+
+
+@pytest.mark.parametrize("case", golden_cases(dipole=True))
+def test_dipole_fixtures_against_direct_sum(case):
+    """The reference's single + double layer FMM (kifmm2d upwardor) is close
+    to the oracle's direct sum at its Nequiv (a check of the fixture)."""
+    g = load_golden(case)
+    assert rel_l2(g["src_val"], g["direct_src"]) < 1e-5
+    assert rel_l2(g["tgt_val"], g["direct_tgt"]) < 1e-5
 
 
 def test_direct_sum_oracle_small():
