@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched-stokes", action="store_true",
                    help="skip the batched-Stokes (many independent problems) measurement")
+    p.add_argument("--no-multi-rhs", action="store_true",
+                   help="skip the multi-RHS (64 charge columns, modified Helmholtz) measurement")
     p.add_argument("--cpu-sample-n", type=int, default=200_000,
                    help="sources in the bounded reference sample of our arm's cpu_baseline")
     p.add_argument("--denested-steps", type=int, default=3,
@@ -543,10 +545,69 @@ def run_ours(args, world, rank, local):
         out["mixed_over_fp64"] = res["fp64"]["ms_step"] / res["mixed"]["ms_step"]
     if not args.no_batched_stokes:
         out["batched_stokes"] = measure_batched_stokes(args, world)
+    if not args.no_multi_rhs:
+        out["multi_rhs"] = measure_multi_rhs(args, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_subprocess(args)
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def measure_multi_rhs(args, world=1, n=1_000_000, n_rhs=64, steps=3):
+    """The multi-RHS batching form: 1,000,000 sources at uniform angles on a
+    circle of radius 0.5 (radial jitter U(-1e-3, 1e-3)), 64 charge columns
+    N(0,1) on one tree, the modified Helmholtz kernel K0(10 r)/(2 pi), Nequiv
+    40, Ncutoff 64, bbox from the points, self-evaluation of every column.
+    A step: tree + expansions of all 64 columns (one launch per level for all
+    columns) + source evaluation (each kernel value applied to 8 columns).
+    Metric: point-RHS per second, 64 N / T.  Inputs resident; CUDA events.
+    With N > 1 ranks the columns are split into blocks over the ranks
+    (flexmm_b200.shard, no exchange while computing)."""
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    from flexmm_b200.shard import column_blocks
+    rank = int(os.environ.get("RANK", "0"))
+    d = workloads.circle(n=n, n_rhs=n_rhs)
+    lo, hi = column_blocks(n_rhs, world)[rank]
+    x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
+    tau = torch.from_numpy(np.ascontiguousarray(d["tau"][lo:hi])).cuda()
+    helper = KI_Helper()
+
+    def step():
+        F = KI_FMM(x, y, "Modified_Helmholtz_Eval", NCUT, 40, helper=helper, helmholtz_k=10.0)
+        F.build_expansions(tau)
+        return F, F.source_evaluation(x, y)
+    F, u = step()
+    torch.cuda.synchronize()
+    # accuracy: two columns at 1000 sampled sources against the FP64 direct sum
+    from flexmm_b200 import direct_evaluation
+    rng = np.random.default_rng(5)
+    si = np.sort(rng.choice(n, 1000, replace=False))
+    errs = []
+    for r in (0, hi - lo - 1):
+        ds = direct_evaluation("Modified_Helmholtz_Eval", x, y, tau[r], x[si], y[si], check=True,
+                               helmholtz_k=10.0).cpu().numpy()
+        errs.append(float(np.linalg.norm(u[r].cpu().numpy()[si] - ds) / np.linalg.norm(ds)))
+    del F, u
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = dist_max(e0.elapsed_time(e1) / steps, world)
+    return {"workload": f"{n} sources on a circle (r = 0.5 +- 1e-3), {n_rhs} charge columns, "
+                        f"K0(10 r)/(2 pi), Nequiv 40, Ncutoff 64, self-evaluation, FP64",
+            "metric": "point-RHS / s", "unit": "M point-RHS/s", "dtype": "f64",
+            "value": n * n_rhs / (ms * 1e-3) / 1e6, "ms_per_step": ms, "steps": steps,
+            "rel_l2_vs_direct": max(errs),
+            "accuracy_sample": "columns 0 and last of this rank, 1000 sources, FP64 direct sum",
+            "note": "one launch per level for all columns (column = blockIdx.y); evaluation "
+                    "shares each kernel value across 8 columns; inputs resident"
+                    + (f"; columns split over {world} ranks, slowest rank's time" if world > 1 else "")}
 
 
 def measure_batched_stokes(args, world=1, n_problems=256):

@@ -840,6 +840,7 @@ int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_
     const int np = p->ops->np;
     const int64_t total = th.n_total(), n = th.n_points, cs = total * np;
     upload_level_ops(p, s);
+    p->has_dipoles = false;
     PassArgs a = pass_args(p);
     p->tau_s.alloc((size_t)n_rhs * n, s);
     p->mult.alloc((size_t)n_rhs * cs, s);
@@ -848,15 +849,13 @@ int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_
     p->mult.zero(s);
     p->ple.zero(s);
     p->loc.zero(s);
-    for (int r = 0; r < n_rhs; ++r) {
-      double *tr = p->tau_s.get() + (size_t)r * n;
-      gather_sorted(tau + (size_t)r * ld_tau, p->td.ordv.get(), n, tr, s);
-      run_upward(a, tr, p->mult.get() + (size_t)r * cs, s);
-      run_m2l(a, p->mult.get() + (size_t)r * cs, p->ple.get() + (size_t)r * cs, s);
-      run_downward(a, p->ple.get() + (size_t)r * cs, p->loc.get() + (size_t)r * cs, s);
-    }
+    for (int r = 0; r < n_rhs; ++r)
+      gather_sorted(tau + (size_t)r * ld_tau, p->td.ordv.get(), n, p->tau_s.get() + (size_t)r * n, s);
+    // every pass once per level for all columns (column = blockIdx.y)
+    run_upward(a, p->tau_s.get(), p->mult.get(), s, n_rhs, n, cs);
+    run_m2l(a, p->mult.get(), p->ple.get(), s, n_rhs, cs);
+    run_downward(a, p->ple.get(), p->loc.get(), s, n_rhs, cs);
     p->n_rhs = n_rhs;
-    p->has_dipoles = false;
     p->ready_recorded = false;  // the split evaluation serves single-column builds
     p->have_expansions = true;
   });

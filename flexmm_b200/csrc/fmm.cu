@@ -111,7 +111,11 @@ __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, in
                                             const LevelOpsDev *__restrict__ ops,
                                             double *__restrict__ mult,
                                             const double *__restrict__ dvx = nullptr,
-                                            const double *__restrict__ dvy = nullptr) {
+                                            const double *__restrict__ dvy = nullptr,
+                                            int64_t tstride = 0, int64_t cstride = 0) {
+  // charge column blockIdx.y (multi-RHS: column strides tstride / cstride)
+  tau += blockIdx.y * tstride;
+  mult += blockIdx.y * cstride;
   extern __shared__ double smem[];
   const int ldp = pad_ld(np);
   double *P = smem;          // [TN][ldp] check potentials
@@ -205,7 +209,8 @@ __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, in
 __global__ void __launch_bounds__(NT) k_m2m(int m, int np, int c_first, int n_groups,
                                             const int *__restrict__ parent,
                                             const LevelOpsDev *__restrict__ ops,
-                                            double *__restrict__ mult) {
+                                            double *__restrict__ mult, int64_t cstride) {
+  mult += blockIdx.y * cstride;  // charge column blockIdx.y
   extern __shared__ double smem[];
   const int ldp = pad_ld(np), lda = pad_ld(4 * np);
   double *P = smem;           // [TN][ldp] check potentials
@@ -258,7 +263,9 @@ __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *_
                                             const int *__restrict__ il,
                                             const LevelOpsDev *__restrict__ ops,
                                             const double *__restrict__ mult,
-                                            double *__restrict__ ple) {
+                                            double *__restrict__ ple, int64_t cstride) {
+  mult += blockIdx.y * cstride;  // charge column blockIdx.y
+  ple += blockIdx.y * cstride;
   extern __shared__ double smem[];
   const int ldp = pad_ld(np), ldw = pad_ld(32);
   double *G = smem;            // [TM][ldp] gathered source multipoles
@@ -342,7 +349,9 @@ __global__ void __launch_bounds__(NT) k_downward(int m, int np, int rg_lo, int r
                                                  const int *__restrict__ parent,
                                                  const LevelOpsDev *__restrict__ ops,
                                                  const double *__restrict__ ple,
-                                                 double *__restrict__ loc) {
+                                                 double *__restrict__ loc, int64_t cstride) {
+  ple += blockIdx.y * cstride;  // charge column blockIdx.y
+  loc += blockIdx.y * cstride;
   extern __shared__ double smem[];
   const int ldp = pad_ld(np);
   double *P = smem;           // [32][ldp] partial locals
@@ -786,7 +795,8 @@ __global__ void k_gather_sorted(const double *__restrict__ v, const int *__restr
 }
 
 template <class KF>
-void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s) {
+void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s, int n_rhs,
+                 int64_t tstride, int64_t cstride) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int np = a.np;
@@ -799,19 +809,18 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
     if constexpr (std::is_same<KF, LaplaceF64T>::value) {
       FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(s2m_bytes)));
-      k_s2m<KF, true><<<148 * 4, NT, s2m_bytes, s>>>(
+      k_s2m<KF, true><<<dim3(148 * 4, n_rhs), NT, s2m_bytes, s>>>(
           a.kp, a.neq, np, th.L, td.dev_off.get(), td.uplist.get(), td.n_up.get(), td.bot.get(),
           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
-          mult, a.dvx, a.dvy);
+          mult, a.dvx, a.dvy, tstride, cstride);
     } else {
       throw Error(ERR_UNSUPPORTED, "dipole sources: Laplace kernel only");
     }
   } else {
-    k_s2m<KF><<<148 * 4, NT, s2m_bytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
-                                             td.uplist.get(), td.n_up.get(), td.bot.get(),
-                                             td.top.get(), td.xmid.get(), td.ymid.get(),
-                                             td.sx.get(), td.sy.get(), tau_s, a.ops_dev, mult,
-                                             nullptr, nullptr);
+    k_s2m<KF><<<dim3(148 * 4, n_rhs), NT, s2m_bytes, s>>>(
+        a.kp, a.neq, np, th.L, td.dev_off.get(), td.uplist.get(), td.n_up.get(), td.bot.get(),
+        td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+        mult, nullptr, nullptr, tstride, cstride);
   }
   FMMB_CUDA(cudaGetLastError());
   const size_t m2m_bytes = sizeof(double) * (size_t)TN * (2 * pad_ld(np) + pad_ld(4 * np));
@@ -821,8 +830,8 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
     const int c_first = th.off[m + 1];
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
     if (n_groups == 0) continue;
-    launch_pdl(k_m2m, dim3((n_groups + TN - 1) / TN), dim3(NT), m2m_bytes, s, m, np, c_first,
-               n_groups, td.parent.get(), a.ops_dev, mult);
+    launch_pdl(k_m2m, dim3((n_groups + TN - 1) / TN, n_rhs), dim3(NT), m2m_bytes, s, m, np,
+               c_first, n_groups, td.parent.get(), a.ops_dev, mult, cstride);
   }
 }
 
@@ -888,16 +897,23 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
 }
 }  // namespace
 
-void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s) {
+void run_upward(const PassArgs &a, const double *tau_s, double *mult, cudaStream_t s, int n_rhs,
+                int64_t tstride, int64_t cstride) {
+  FMMB_CHECK(n_rhs >= 1 && n_rhs <= 65535, ERR_INVALID_ARGUMENT, "1..65535 charge columns");
   switch (a.kernel_id) {
-    case KERNEL_LAPLACE: upward_impl<LaplaceF64T>(a, tau_s, mult, s); break;
-    case KERNEL_MOD_HELMHOLTZ: upward_impl<ModHelmholtzF64>(a, tau_s, mult, s); break;
-    case KERNEL_RADIAL_TABLE: upward_impl<RadialTableF64>(a, tau_s, mult, s); break;
+    case KERNEL_LAPLACE: upward_impl<LaplaceF64T>(a, tau_s, mult, s, n_rhs, tstride, cstride); break;
+    case KERNEL_MOD_HELMHOLTZ:
+      upward_impl<ModHelmholtzF64>(a, tau_s, mult, s, n_rhs, tstride, cstride);
+      break;
+    case KERNEL_RADIAL_TABLE:
+      upward_impl<RadialTableF64>(a, tau_s, mult, s, n_rhs, tstride, cstride);
+      break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
 
-void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s) {
+void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s, int n_rhs,
+             int64_t cstride) {
   const TreeHost &th = *a.th;
   if (th.L < 3) return;
   FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
@@ -918,11 +934,13 @@ void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s)
   FMMB_CUDA(cudaFuncSetAttribute(k_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sizeof(double) * TM * (pad_ld(64) + pad_ld(32)))));
   PhaseTimer timer(PH_M2L, s);
-  k_m2l<<<tiles, NT, sm, s>>>(tl, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev, mult, ple);
+  k_m2l<<<dim3(tiles, n_rhs), NT, sm, s>>>(tl, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
+                                           mult, ple, cstride);
   FMMB_CUDA(cudaGetLastError());
 }
 
-void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s) {
+void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s, int n_rhs,
+                  int64_t cstride) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const size_t sm = sizeof(double) * (size_t)TN * pad_ld(a.np) * 2;
@@ -931,8 +949,8 @@ void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_
     if (cnt <= 0) continue;
     const int tiles = (cnt + 7) / 8;
     PhaseTimer timer(PH_DOWNWARD, s);
-    launch_pdl(k_downward, dim3(tiles), dim3(NT), sm, s, m, a.np, lo, cnt, td.rg.get(),
-               td.parent.get(), a.ops_dev, ple, loc);
+    launch_pdl(k_downward, dim3(tiles, n_rhs), dim3(NT), sm, s, m, a.np, lo, cnt, td.rg.get(),
+               td.parent.get(), a.ops_dev, ple, loc, cstride);
     FMMB_CUDA(cudaGetLastError());
   }
 }

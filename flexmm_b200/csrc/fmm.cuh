@@ -129,9 +129,15 @@ void run_evaluate_sources_split(const PassArgs &a, const double *tau_sorted, con
 void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_sorted,
                                       const double *tsum, const float *loc32, const double *lsum,
                                       int check, double *out, cudaStream_t s, const SplitEval &se);
-void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaStream_t s);
-void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s);
-void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s);
+// The FP64 passes; n_rhs charge columns at once (multi-RHS: column r's
+// charges at tau_sorted + r * tstride, its expansions at + r * cstride),
+// one launch per level for all columns.
+void run_upward(const PassArgs &a, const double *tau_sorted, double *mult, cudaStream_t s,
+                int n_rhs = 1, int64_t tstride = 0, int64_t cstride = 0);
+void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s, int n_rhs = 1,
+             int64_t cstride = 0);
+void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_t s,
+                  int n_rhs = 1, int64_t cstride = 0);
 // targets: sorted coordinates, sorted keys, permutation sorted -> original
 void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const double *sy,
                 const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
