@@ -63,7 +63,10 @@ def test_sixty_four_columns_in_one_pass_per_level(built_lib):
     assert u.shape == (64, 30000) and np.isfinite(u).all()
     idx = np.arange(0, 30000, 151)
     for r in (0, 17, 40, 63):
-        S = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, helper=helper, helmholtz_k=10.0)
+        # the same box (and so the same tree): without it the helper's cached
+        # widths would snap a fresh bbox differently, as the reference's get_bbox does
+        S = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, bbox=F.bbox, helper=helper,
+                   helmholtz_k=10.0)
         S.build_expansions(d["tau"][r])
         one = S.source_evaluation(x, y).cpu().numpy()
         assert rel_l2(u[r], one) < 1e-13, r
