@@ -55,18 +55,21 @@ def test_sixty_four_columns_in_one_pass_per_level(built_lib):
     from oracle.direct import direct_mod_helmholtz
     d = workloads.circle(n=30000, n_rhs=64, seed=7)
     x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
-    helper = KI_Helper()
-    F = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, helper=helper, helmholtz_k=10.0)
+    # one box for every object, each with a fresh helper: a helper that has
+    # cached widths snaps a box to them (the reference's get_bbox), which
+    # would give a different tree
+    bb = [-0.51, 0.51, -0.51, 0.51]
+    F = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, bbox=bb, helper=KI_Helper(),
+               helmholtz_k=10.0)
     F.build_expansions(d["tau"])
     u = F.source_evaluation(x, y).cpu().numpy()
     F.status()
     assert u.shape == (64, 30000) and np.isfinite(u).all()
     idx = np.arange(0, 30000, 151)
     for r in (0, 17, 40, 63):
-        # the same box (and so the same tree): without it the helper's cached
-        # widths would snap a fresh bbox differently, as the reference's get_bbox does
-        S = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, bbox=F.bbox, helper=helper,
+        S = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, bbox=bb, helper=KI_Helper(),
                    helmholtz_k=10.0)
+        assert S.bbox == F.bbox
         S.build_expansions(d["tau"][r])
         one = S.source_evaluation(x, y).cpu().numpy()
         assert rel_l2(u[r], one) < 1e-13, r
