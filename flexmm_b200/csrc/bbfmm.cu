@@ -270,7 +270,7 @@ void run_bb_upward(const BBArgs &b, const double *tau_s, double *mult, cudaStrea
   const int np = b.np;
   const BBScale sc = bb_scale(th);
   PhaseTimer timer(PH_UPWARD, s);
-  k_bb_s2m<<<148 * 8, 128, 0, s>>>(b.p, np, th.L, sc, td.dev_off.get(), td.uplist.get(),
+  k_bb_s2m<<<work_grid(th.n_total(), 8), 128, 0, s>>>(b.p, np, th.L, sc, td.dev_off.get(), td.uplist.get(),
                                    td.n_up.get(), td.bot.get(), td.top.get(), td.xmid.get(),
                                    td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, mult);
   FMMB_CUDA(cudaGetLastError());
@@ -354,7 +354,8 @@ void run_bb_evaluate(const BBArgs &b, const double *tau_s, const double *loc, co
   const BBScale sc = bb_scale(*b.th);
   PhaseTimer timer(PH_EVAL, s);
   auto launch = [&](auto kern) {
-    kern<<<148 * 8, TCH_BB, 0, s>>>(b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(),
+    kern<<<work_grid(b.th->n_total() + m / TCH_BB + 1, 8), TCH_BB, 0, s>>>(
+        b.kp, b.p, b.np, sc, it.items.get(), it.n_items.get(),
                                     td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
                                     td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, loc, txs, tys,
                                     tperm, check, out, ld_out);

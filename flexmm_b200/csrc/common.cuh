@@ -126,6 +126,15 @@ void launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, c
   FMMB_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...));
 }
 
+// blocks for a persistent or grid-stride kernel over `units` work units (at
+// most one block per unit): per_sm blocks per SM on a large problem, fewer
+// on a small one (a batch of small problems then does not launch thousands
+// of idle blocks per kernel)
+inline int work_grid(int64_t units, int per_sm) {
+  const int64_t cap = 148 * int64_t(per_sm);
+  return int(units < 1 ? 1 : (units < cap ? units : cap));
+}
+
 inline int grid_for(int64_t n, int threads, int cap = 148 * 16) {
   int64_t g = (n + threads - 1) / threads;
   if (g < 1) g = 1;

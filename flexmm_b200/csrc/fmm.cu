@@ -804,12 +804,15 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   const size_t s2m_bytes = sizeof(double) * (size_t)TN * pad_ld(np) * 2;
   FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(s2m_bytes)));
+  // persistent over the S2M nodes; at most one block per TN nodes of the tree
+  // (small trees launch small grids)
+  const int s2m_grid = std::max(1, std::min(148 * 4, (th.n_total() + TN - 1) / TN));
   PhaseTimer timer(PH_UPWARD, s);
   if (a.dvx) {
     if constexpr (std::is_same<KF, LaplaceF64T>::value) {
       FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(s2m_bytes)));
-      k_s2m<KF, true><<<dim3(148 * 4, n_rhs), NT, s2m_bytes, s>>>(
+      k_s2m<KF, true><<<dim3(s2m_grid, n_rhs), NT, s2m_bytes, s>>>(
           a.kp, a.neq, np, th.L, td.dev_off.get(), td.uplist.get(), td.n_up.get(), td.bot.get(),
           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
           mult, a.dvx, a.dvy, tstride, cstride);
@@ -817,7 +820,7 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
       throw Error(ERR_UNSUPPORTED, "dipole sources: Laplace kernel only");
     }
   } else {
-    k_s2m<KF><<<dim3(148 * 4, n_rhs), NT, s2m_bytes, s>>>(
+    k_s2m<KF><<<dim3(s2m_grid, n_rhs), NT, s2m_bytes, s>>>(
         a.kp, a.neq, np, th.L, td.dev_off.get(), td.uplist.get(), td.n_up.get(), td.bot.get(),
         td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
         mult, nullptr, nullptr, tstride, cstride);
@@ -875,11 +878,12 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
   const TreeDev &td = *a.td;
   EvalItems it;
   eval_items(a, tkeys, m, it, s);
+  const int64_t units = a.th->n_total() + m / TCH + 1;  // work items, upper bound
   PhaseTimer timer(PH_EVAL, s);
   if (a.dvx) {
     FMMB_CHECK(nout == 1, ERR_UNSUPPORTED, "dipole sources: potential only");
     if constexpr (std::is_same<KF, LaplaceF64T>::value) {
-      k_evaluate<KF, 1, EVAL_FULL, true><<<148 * 5, TCH, 0, s>>>(
+      k_evaluate<KF, 1, EVAL_FULL, true><<<work_grid(units, 5), TCH, 0, s>>>(
           a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
           loc, txs, tys, tperm, check, out, ld_out, nullptr, a.dvx, a.dvy);
@@ -888,7 +892,7 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
     }
   } else {
     auto kern = nout == 3 ? k_evaluate<KF, 3> : k_evaluate<KF, 1>;
-    kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(),
+    kern<<<work_grid(units, 8), TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(),
                                  td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
                                  td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc,
                                  txs, tys, tperm, check, out, ld_out, nullptr, nullptr, nullptr);
@@ -988,6 +992,7 @@ void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *l
   eval_items(a, td.pkeys.get(), m, it, se.side);
   DevBuf<double> near;
   near.alloc(m, se.side);
+  const int64_t units = a.th->n_total() + m / TCH + 1;  // work items, upper bound
   {
     // the SMs keep their largest shared-memory carveout while near-field
     // blocks sit on them, so the level passes' CTAs still fit beside them
@@ -999,7 +1004,7 @@ void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *l
     }();
     (void)carveout_set;
     PhaseTimer timer(PH_EVAL, se.side);
-    k_evaluate<KF, 1, EVAL_NEAR, DIP><<<148 * NEAR_BLOCKS_PER_SM, TCH, 0, se.side>>>(
+    k_evaluate<KF, 1, EVAL_NEAR, DIP><<<work_grid(units, NEAR_BLOCKS_PER_SM), TCH, 0, se.side>>>(
         a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
         td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
         loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get(), a.dvx, a.dvy);
@@ -1009,7 +1014,7 @@ void evaluate_split_impl(const PassArgs &a, const double *tau_s, const double *l
   FMMB_CUDA(cudaStreamWaitEvent(s, se.near_done, 0));
   {
     PhaseTimer timer(PH_EVAL, s);
-    k_evaluate<KF, 1, EVAL_FAR><<<148 * 8, TCH, 0, s>>>(
+    k_evaluate<KF, 1, EVAL_FAR><<<work_grid(units, 8), TCH, 0, s>>>(
         a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
         td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
         loc, td.sx.get(), td.sy.get(), td.ordv.get(), check, out, 0, near.get(), nullptr,
@@ -1034,7 +1039,7 @@ void evaluate_multi_impl(const PassArgs &a, const double *tau_s, int64_t n_src, 
   constexpr int R = 8;
   for (int r0 = 0; r0 < n_rhs; r0 += R) {
     const int ncol = std::min(R, n_rhs - r0);
-    k_evaluate_multi<KF, R><<<148 * 8, TCH, 0, s>>>(
+    k_evaluate_multi<KF, R><<<work_grid(a.th->n_total() + m / TCH + 1, 8), TCH, 0, s>>>(
         a.kp, a.neq, a.np, ncol, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
         td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s + r0 * n_src,
         n_src, a.ops_dev, loc + r0 * col_stride, col_stride, txs, tys, tperm, check,
@@ -1135,7 +1140,8 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   FMMB_CUDA(cudaGetLastError());
   PhaseTimer timer(PH_EVAL, s);
   auto launch = [&](auto kern) {
-    kern<<<148 * 8, TCH, 0, s>>>(a.kp, a.neq, a.np, items, n_items, td.coll.get(), td.bot.get(),
+    kern<<<work_grid(total + m / TCH + 1, 8), TCH, 0, s>>>(a.kp, a.neq, a.np, items, n_items,
+                                                             td.coll.get(), td.bot.get(),
                                  td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
                                  td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0,
                                  nullptr, nullptr, nullptr);

@@ -1188,7 +1188,7 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
   FMMB_CUDA(cudaFuncSetAttribute(k_s2m_mx<KF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(pbytes)));
   PhaseTimer timer(PH_UPWARD, s);
-  k_s2m_mx<KF32><<<148 * 4, NT, pbytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
+  k_s2m_mx<KF32><<<work_grid((th.n_total() + TN - 1) / TN, 4), NT, pbytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
                                               td.uplist.get(), td.n_up.get(), td.bot.get(),
                                               td.top.get(), td.xmid.get(), td.ymid.get(),
                                               td.sx.get(), td.sy.get(), tau_s, tsum, a.ops_dev,
@@ -1348,7 +1348,7 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
     (void)carveout_set;
     PhaseTimer timer(PH_EVAL, se.side);
     k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>
-        <<<148 * NEAR_BLOCKS_PER_SM_MIXED, TCH, 0, se.side>>>(
+        <<<work_grid(total + m / TCH + 1, NEAR_BLOCKS_PER_SM_MIXED), TCH, 0, se.side>>>(
             a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
             a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
             next_item.get(), near.get());
@@ -1358,7 +1358,8 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
   FMMB_CUDA(cudaStreamWaitEvent(s, se.near_done, 0));
   {
     PhaseTimer timer(PH_EVAL, s);
-    k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_FAR><<<148 * EVAL_BLOCKS_PER_SM, TCH, 0, s>>>(
+    k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_FAR>
+        <<<work_grid(total + m / TCH + 1, EVAL_BLOCKS_PER_SM), TCH, 0, s>>>(
         a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
         a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
         next_item.get() + 1, near.get());
@@ -1396,7 +1397,8 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
       auto kern = nout == 3 ? k_evaluate_mx<LaplaceF32, LaplaceF64, 3>
                             : k_evaluate_mx<LaplaceF32, LaplaceF64, 1>;
       const int per_sm = nout == 3 ? 6 : EVAL_BLOCKS_PER_SM;
-      kern<<<148 * per_sm, TCH, 0, s>>>(a.kp, a.neq, a.np, desc.get(), it.n_items.get(),
+      kern<<<work_grid(total + m / TCH + 1, per_sm), TCH, 0, s>>>(a.kp, a.neq, a.np, desc.get(),
+                                                                it.n_items.get(),
                                         td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc32, lsum,
                                         txs, tys, tperm, check, self_eval, out, ld_out,
                                         next_item.get(), nullptr);

@@ -213,7 +213,7 @@ void run_stokes_upward(const StokesArgs &a, const double *fx, const double *fy, 
   FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
   const int np = a.np;
   PhaseTimer timer(PH_UPWARD, s);
-  k_stokes_s2m<<<148 * 8, 128, 0, s>>>(a.neq, np, th.L, circles(a), td.dev_off.get(),
+  k_stokes_s2m<<<work_grid(th.n_total(), 8), 128, 0, s>>>(a.neq, np, th.L, circles(a), td.dev_off.get(),
                                        td.uplist.get(), td.n_up.get(), td.bot.get(), td.top.get(),
                                        td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), fx, fy,
                                        partial);
@@ -308,7 +308,7 @@ void run_stokes_evaluate(const StokesArgs &a, const double *fx, const double *fy
   EvalItems it;
   eval_items(pa, tkeys, m, it, s);
   PhaseTimer timer(PH_EVAL, s);
-  k_stokes_evaluate<<<148 * 8, TCH_ST, 0, s>>>(
+  k_stokes_evaluate<<<work_grid(a.th->n_total() + m / TCH_ST + 1, 8), TCH_ST, 0, s>>>(
       a.neq, a.np, circles(a), it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
       td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), fx, fy, loc, txs, tys,
       tperm, check, out, ld_out);
