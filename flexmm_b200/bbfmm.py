@@ -14,8 +14,8 @@ the reference forms them, are:
   compressed by the same SVD rule as the KIFMM operators (bbfmm.py:101-122,
   flexmm/flexmm2d/helpers.py:5-33).
 
-The device runs S2M (Chebyshev moments), M2M, M2L, L2L (cuBLAS DGEMMs over
-contiguous child rows and offset-concatenated operators), L2T (2-D Chebyshev
+The device runs S2M (Chebyshev moments), M2M, M2L, L2L (FP64 tensor-core
+row GEMMs with fused gathers, ``csrc/rowgemm.cuh``), L2T (2-D Chebyshev
 series) and P2P in FP64 (``csrc/bbfmm.cu``).
 """
 import ctypes

@@ -22,8 +22,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
-# cuBLAS for the black-box FMM's translation GEMMs
-LINK = ["-lcublas", "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
+LINK = []
 
 
 def sources():

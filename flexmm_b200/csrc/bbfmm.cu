@@ -8,20 +8,22 @@
 //  * M2M / L2L: the level-independent M2MC [NQ x 4NQ] and its transpose
 //    (bbfmm.py:145-161) on the contiguous child rows of each parent group;
 //  * M2L: per level and offset VI K VI^T (bbfmm.py:101-122), the 40 offsets
-//    of a level applied as ONE GEMM over the offset-concatenated operator
-//    [NQ x 40 NQ] and a gathered [targets x 40 NQ] block (a missing source
-//    is a zero block);
+//    of a level applied in one row-GEMM launch (rowgemm.cuh) over the
+//    stacked operators: each tile of 64 target boxes of one parity class
+//    reads the source multipole of each offset it meets, and skips the
+//    offsets absent for the whole tile;
 //  * L2T: the local coefficients evaluated as a 2-D Chebyshev series
 //    (chebeval2d1, bbfmm.py:25-31, L2targets, bbfmm.py:198-210);
 //  * P2P: the same colleague sweep as the KIFMM evaluation.
-// The GEMMs are cuBLAS DGEMMs on the plan's stream; gathers, scatters,
-// moments and evaluation are the kernels below.
-#include <cublas_v2.h>
+// M2M, L2L and M2L are FP64 tensor-core row GEMMs (rowgemm.cuh) with their
+// gathers and scatters fused into the loads and stores; moments and
+// evaluation are the kernels below.
 
 #include <algorithm>
 #include <string>
 
 #include "dense.cuh"
+#include "rowgemm.cuh"
 #include "fmm.cuh"
 #include "timing.cuh"
 
@@ -274,25 +276,14 @@ void run_bb_upward(const BBArgs &b, const double *tau_s, double *mult, cudaStrea
                                    td.n_up.get(), td.bot.get(), td.top.get(), td.xmid.get(),
                                    td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, mult);
   FMMB_CUDA(cudaGetLastError());
-  int max_groups = 0;
-  for (int m = th.L - 2; m >= 2; --m)
-    max_groups = std::max(max_groups, (th.off[m + 2] - th.off[m + 1]) / 4);
-  if (max_groups == 0) return;
-  DevBuf<double> rows;
-  rows.alloc((size_t)max_groups * np, s);
-  FMMB_BLAS(cublasSetStream(b.blas, s));
-  const double one = 1.0, zero = 0.0;
   for (int m = th.L - 2; m >= 2; --m) {
     const int c_first = th.off[m + 1];
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
     if (n_groups == 0) continue;
-    // rows[e] = M2MC . (children of group e): column-major rows^T (np x n) =
-    // M2MC (np x 4np) . children^T (4np x n); M2MC row-major = its transpose column-major
-    FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n_groups, 4 * np, &one, b.m2mc,
-                          4 * np, mult + (size_t)c_first * np, 4 * np, &zero, rows.get(), np));
-    k_rows_to_parents<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
-        n_groups, np, c_first, td.parent.get(), rows.get(), mult);
-    FMMB_CUDA(cudaGetLastError());
+    // parent rows = children rows (contiguous, 4np wide) . M2MC^T (fmm.py:93-96)
+    rowgemm(RowsContig{mult + (size_t)c_first * np, 4 * (int64_t)np, n_groups, 4 * np},
+            StoreParents{td.parent.get(), mult, c_first, np}, row_tiles(n_groups), b.m2mct, np, np,
+            4 * np, s);
   }
 }
 
@@ -301,42 +292,20 @@ void run_bb_downward(const BBArgs &b, const double *mult, double *ple, cudaStrea
   const TreeDev &td = *b.td;
   if (th.L < 3) return;
   const int np = b.np;
-  int max_groups = 0;
-  for (int m = 2; m < th.L; ++m) max_groups = std::max(max_groups, th.rg_hi[m] - th.rg_lo[m]);
-  if (max_groups == 0) return;
-  DevBuf<double> sbig, y, lp, c;
-  sbig.alloc((size_t)max_groups * 4 * N_OFFSETS * np, s);
-  y.alloc((size_t)max_groups * 4 * np, s);
-  lp.alloc((size_t)max_groups * np, s);
-  c.alloc((size_t)max_groups * 4 * np, s);
-  FMMB_BLAS(cublasSetStream(b.blas, s));
-  const double one = 1.0, zero = 0.0;
   for (int m = 2; m < th.L; ++m) {
     const int lo = th.rg_lo[m], n_groups = th.rg_hi[m] - th.rg_lo[m];
     if (n_groups == 0) continue;
-    const int n = 4 * n_groups;
     if (m >= 3) {  // L2L from level m-1: children += parent local . M2MC (bbfmm.py:161, fmm.py:140-147)
       PhaseTimer timer(PH_DOWNWARD, s);
-      k_gather_parent_rows<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
-          n_groups, np, td.rg.get(), lo, td.parent.get(), ple, lp.get());
-      FMMB_CUDA(cudaGetLastError());
-      FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_N, CUBLAS_OP_N, 4 * np, n_groups, np, &one, b.m2mc,
-                            4 * np, lp.get(), np, &zero, c.get(), 4 * np));
-      k_add_child_rows<<<grid_for((int64_t)n_groups * 4 * np, 256), 256, 0, s>>>(
-          n_groups, np, td.rg.get(), lo, c.get(), ple);
-      FMMB_CUDA(cudaGetLastError());
+      rowgemm(ParentRows{td.rg.get(), td.parent.get(), ple, lo, n_groups, np},
+              AddChildRows{td.rg.get(), ple, lo, np}, row_tiles(n_groups), b.m2mc, 4 * np, 4 * np,
+              np, s);
     }
-    {  // M2L of level m: all 40 offsets in one GEMM (fmm.py:118-131)
+    {  // M2L of level m: tiles of one parity class, absent offsets skipped (fmm.py:118-131)
       PhaseTimer timer(PH_M2L, s);
-      k_m2l_gather_cat<<<grid_for((int64_t)n * N_OFFSETS * np, 256, 148 * 64), 256, 0, s>>>(
-          n_groups, np, td.rg.get(), lo, td.il.get(), mult, sbig.get());
-      FMMB_CUDA(cudaGetLastError());
-      FMMB_BLAS(cublasDgemm(b.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, N_OFFSETS * np, &one,
-                            b.m2l_cat[m], N_OFFSETS * np, sbig.get(), N_OFFSETS * np, &zero, y.get(),
-                            np));
-      k_add_group_rows<<<grid_for((int64_t)n * np, 256), 256, 0, s>>>(n_groups, np, td.rg.get(), lo,
-                                                                    y.get(), ple);
-      FMMB_CUDA(cudaGetLastError());
+      const int tpc = row_tiles(n_groups);
+      rowgemm(M2LRows{td.rg.get(), td.il.get(), mult, lo, n_groups, np, tpc},
+              AddGroupRows{td.rg.get(), ple, lo, np}, 4 * tpc, b.m2l_cat[m], np, np, np, s);
     }
   }
 }

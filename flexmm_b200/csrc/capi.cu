@@ -214,6 +214,7 @@ struct fmm_ops {
   int method = METHOD_KIFMM;
   int p = 0;                  // black-box FMM: Chebyshev order
   DevBuf<double> bb_m2mc;     // black-box FMM: M2MC [np x 4np]
+  DevBuf<double> bb_m2mct;    // and its transpose [4np x np]
   std::vector<std::unique_ptr<LevelEntry>> levels;
 };
 
@@ -234,7 +235,6 @@ struct fmm_plan {
   bool have_expansions = false;
   DevBuf<double> tau2_s, partial;  // Stokes FMM: sorted fy; partial multipoles
   int n_rhs = 1;                   // charge columns of the last build (multi-RHS)
-  cublasHandle_t blas = nullptr;  // black-box and Stokes FMM translations
   // split own-source evaluation (near field on a side stream, see SplitEval):
   // `ready` is recorded once a single-column KIFMM build has sorted its charges
   DevBuf<double> dvx, dvy;  // dipole sources: strength * normal, sorted (see PassArgs)
@@ -243,7 +243,6 @@ struct fmm_plan {
   cudaEvent_t ev_ready = nullptr, ev_near = nullptr, ev_far = nullptr;
   bool ready_recorded = false;
   ~fmm_plan() {
-    if (blas) cublasDestroy(blas);
     for (cudaEvent_t e : {ev_ready, ev_near, ev_far})
       if (e) cudaEventDestroy(e);
   }
@@ -493,6 +492,12 @@ int fmm_bb_ops_create(int kernel_id, const double *kparams, int p, const double 
     o->p = p;
     o->bb_m2mc.alloc(h.size(), 0);
     FMMB_CUDA(cudaMemcpy(o->bb_m2mc.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> ht(h.size(), 0.0);  // [4np x np]: the M2M row GEMM's operator
+    for (int i = 0; i < np; ++i)
+      for (int k = 0; k < 4 * np; ++k) ht[size_t(k) * np + i] = h[size_t(i) * 4 * np + k];
+    o->bb_m2mct.alloc(ht.size(), 0);
+    FMMB_CUDA(cudaMemcpy(o->bb_m2mct.get(), ht.data(), ht.size() * sizeof(double),
+                         cudaMemcpyHostToDevice));
     *out = o.release();
   });
 }
@@ -509,16 +514,18 @@ int fmm_bb_ops_add(fmm_ops *ops, const fmm_bb_level_ops *lv, int *level_id) {
       const int r = lv->m2l_rank[o];
       if (r == 0) continue;
       FMMB_CHECK(lv->m2l_a[o], ERR_INVALID_ARGUMENT, "missing M2L operator");
+      // stored transposed, [40 np x np]: row o np + k holds column k of
+      // offset o's operator (the M2L row GEMM's W)
       if (r < 0) {  // dense [n x n]
         for (int i = 0; i < n; ++i)
-          for (int k = 0; k < n; ++k) h[size_t(i) * ld + size_t(o) * np + k] = lv->m2l_a[o][size_t(i) * n + k];
+          for (int k = 0; k < n; ++k) h[(size_t(o) * np + k) * np + i] = lv->m2l_a[o][size_t(i) * n + k];
       } else {  // the truncated operator M2 . M1 ([n x r] . [r x n]), as the reference applies it
         FMMB_CHECK(r <= n && lv->m2l_b[o], ERR_INVALID_ARGUMENT, "bad M2L factors");
         for (int i = 0; i < n; ++i)
           for (int k = 0; k < n; ++k) {
             double acc = 0.0;
             for (int q = 0; q < r; ++q) acc += lv->m2l_a[o][size_t(i) * r + q] * lv->m2l_b[o][size_t(q) * n + k];
-            h[size_t(i) * ld + size_t(o) * np + k] = acc;
+            h[(size_t(o) * np + k) * np + i] = acc;
           }
       }
     }
@@ -614,7 +621,7 @@ int fmm_stokes_ops_add(fmm_ops *ops, const fmm_stokes_level_ops *lv, int *level_
             v = 0.0;
             for (int q = 0; q < r; ++q) v += lv->m2l_a[o][size_t(i) * r + q] * lv->m2l_b[o][size_t(q) * n2 + k];
           }
-          h[o_cat + size_t(i) * ld + size_t(o) * np + k] = v;
+          h[o_cat + (size_t(o) * np + k) * np + i] = v;  // transposed [40 np x np]
         }
     }
     auto e = std::make_unique<LevelEntry>();
@@ -759,30 +766,18 @@ static void upload_level_ops(fmm_plan *p, cudaStream_t s) {
   FMMB_CUDA(cudaGetLastError());
 }
 
-static void ensure_blas(fmm_plan *p, cudaStream_t s) {
-  if (!p->blas) {
-    FMMB_CHECK(cublasCreate(&p->blas) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasCreate failed");
-    // no TF32 / reduced-precision paths: these forms are FP64 end to end
-    FMMB_CHECK(cublasSetMathMode(p->blas, CUBLAS_PEDANTIC_MATH) == CUBLAS_STATUS_SUCCESS, ERR_CUDA,
-               "cublasSetMathMode failed");
-  }
-  FMMB_CHECK(cublasSetStream(p->blas, s) == CUBLAS_STATUS_SUCCESS, ERR_CUDA, "cublasSetStream failed");
-}
-
-static StokesArgs stokes_args(fmm_plan *p, cudaStream_t s) {
-  ensure_blas(p, s);
+static StokesArgs stokes_args(fmm_plan *p, cudaStream_t) {
   StokesArgs a{};
   a.neq = p->ops->neq;
   a.np = p->ops->np;
   a.td = &p->td;
   a.th = &p->th;
-  a.blas = p->blas;
   for (int m = 0; m < p->th.L && m < FMM_MAX_LEVELS_DEV; ++m)
     if (p->bound[m] >= 0) a.lev[m] = p->ops->levels[p->bound[m]]->st_lev;
   return a;
 }
 
-static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
+static BBArgs bb_args(fmm_plan *p, cudaStream_t) {
   BBArgs b{};
   b.kernel_id = p->ops->kernel_id;
   b.kp = p->ops->kp;
@@ -790,9 +785,8 @@ static BBArgs bb_args(fmm_plan *p, cudaStream_t s) {
   b.np = p->ops->np;
   b.td = &p->td;
   b.th = &p->th;
-  ensure_blas(p, s);
-  b.blas = p->blas;
   b.m2mc = p->ops->bb_m2mc.get();
+  b.m2mct = p->ops->bb_m2mct.get();
   for (int m = 0; m < p->th.L && m < FMM_MAX_LEVELS_DEV; ++m)
     b.m2l_cat[m] = p->bound[m] >= 0 ? p->ops->levels[p->bound[m]]->bb_m2l.get() : nullptr;
   return b;

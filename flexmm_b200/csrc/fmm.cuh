@@ -3,7 +3,6 @@
 // circle), partial locals from M2L, and locals (equivalent densities on the
 // large circle).
 #pragma once
-#include <cublas_v2.h>
 
 #include "kernels.cuh"
 #include "tree.cuh"
@@ -56,16 +55,16 @@ struct PassArgs {
 
 // Black-box (Chebyshev) FMM (bbfmm.cu): p x p coefficients per box, NQ = p^2
 // padded to np columns; M2MC [np x 4np] row-major (level independent);
-// m2l_cat[m]: level m's 40 M2L operators side by side, [np x 40 np] row-major,
-// block o holding VI K VI^T of offset o (zero for a null offset).
+// m2l_cat[m]: level m's 40 M2L operators stacked transposed, [40 np x np]
+// row-major, rows o np .. o np + np - 1 holding (VI K VI^T)^T of offset o
+// (zero for a null offset); m2mct = M2MC^T [4np x np].
 struct BBArgs {
   int kernel_id;
   KernelParams kp;
   int p, np;
   const TreeDev *td;
   const TreeHost *th;
-  cublasHandle_t blas;
-  const double *m2mc;
+  const double *m2mc, *m2mct;
   const double *m2l_cat[FMM_MAX_LEVELS_DEV];
 };
 void run_bb_upward(const BBArgs &b, const double *tau_sorted, double *mult, cudaStream_t s);
@@ -82,12 +81,11 @@ void run_bb_evaluate(const BBArgs &b, const double *tau_sorted, const double *lo
 //   c2e_u, c2e_vhs [np x np]: C2E solve, the extra unknown's column zeroed;
 //   m2mc [4np x np]: parent check row = children rows . m2mc;
 //   l2lc [np x 4np]: children partial-local rows = local row . l2lc;
-//   m2l_cat [np x 40np]: the 40 M2L operators side by side.
+//   m2l_cat [40np x np]: the 40 M2L operators stacked, each transposed.
 struct StokesArgs {
   int neq, np;
   const TreeDev *td;
   const TreeHost *th;
-  cublasHandle_t blas;
   struct Level {
     const double *lx, *ly;
     const double *e2c_u, *e2c_vhs, *c2e_u, *c2e_vhs, *m2mc, *l2lc, *m2l_cat;

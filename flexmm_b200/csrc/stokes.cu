@@ -10,18 +10,19 @@
 //    the factored-SVD solve of the corrected equivalent-to-check form
 //    (E2C_SVD, stokes_fmm.py:553-558);
 //  * downward: partial locals += L2LC . parent local (real sibling groups) and
-//    += M2L . source multipoles (the 40 offsets as one offset-concatenated
-//    GEMM, a missing source a zero block), then the C2E solve, extra unknown
-//    dropped (stokes_fmm.py:712-733);
+//    += M2L . source multipoles (the 40 offsets in one row-GEMM launch,
+//    tiles of one parity class skipping absent offsets), then the C2E solve,
+//    extra unknown dropped (stokes_fmm.py:712-733);
 //  * evaluation: (u, v, p) from the leaf's local forces on the large circle
 //    (local_expansion_evaluation, stokes_fmm.py:331-360) plus the colleagues'
 //    sources (neighbor_evaluation, stokes_fmm.py:361-396).
-// Solves and translations are cuBLAS DGEMMs on the plan's stream.
-#include <cublas_v2.h>
+// Solves and translations are FP64 tensor-core row GEMMs (rowgemm.cuh) on
+// the plan's stream, gathers and scatters fused into their loads and stores.
 
 #include <algorithm>
 
 #include "dense.cuh"
+#include "rowgemm.cuh"
 #include "fmm.cuh"
 #include "timing.cuh"
 
@@ -194,13 +195,12 @@ StokesCircles circles(const StokesArgs &a) {
   return c;
 }
 
-// rows [r0, r0 + n) of x := ((b . U) . VHs), row-major np x np operators
+// rows of x := ((b . U) . VHs), row-major np x np operators, n contiguous rows
 void solve_rows(const StokesArgs &a, const double *u, const double *vhs, const double *b, double *x,
-                double *tmp, int n) {
-  const double one = 1.0, zero = 0.0;
+                double *tmp, int n, cudaStream_t s) {
   const int np = a.np;
-  FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, np, n, np, &one, u, np, b, np, &zero, tmp, np));
-  FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, np, n, np, &one, vhs, np, tmp, np, &zero, x, np));
+  rowgemm(RowsContig{b, np, n, np}, StoreRows{tmp, np}, row_tiles(n), u, np, np, np, s);
+  rowgemm(RowsContig{tmp, np, n, np}, StoreRows{x, np}, row_tiles(n), vhs, np, np, np, s);
 }
 
 }  // namespace
@@ -222,25 +222,19 @@ void run_stokes_upward(const StokesArgs &a, const double *fx, const double *fy, 
   for (int m = 2; m < th.L; ++m) max_rows = std::max(max_rows, th.off[m + 1] - th.off[m]);
   DevBuf<double> tmp;
   tmp.alloc((size_t)max_rows * np, s);
-  FMMB_BLAS(cublasSetStream(a.blas, s));
-  const double one = 1.0, zero = 0.0;
   for (int m = th.L - 1; m >= 2; --m) {
-    if (m <= th.L - 2) {  // partial of level m's parents += M2MC . children
+    if (m <= th.L - 2) {  // partial of level m's parents = children . M2MC
       const int c_first = th.off[m + 1];
       const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
-      if (n_groups > 0) {
-        FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, np, n_groups, 4 * np, &one,
-                              a.lev[m].m2mc, np, mult + (size_t)c_first * np, 4 * np, &zero,
-                              tmp.get(), np));
-        k_rows_to_parents<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
-            n_groups, np, c_first, td.parent.get(), tmp.get(), partial);
-        FMMB_CUDA(cudaGetLastError());
-      }
+      if (n_groups > 0)
+        rowgemm(RowsContig{mult + (size_t)c_first * np, 4 * (int64_t)np, n_groups, 4 * np},
+                StoreParents{td.parent.get(), partial, c_first, np}, row_tiles(n_groups),
+                a.lev[m].m2mc, np, np, 4 * np, s);
     }
     const int r0 = th.off[m], n = th.off[m + 1] - th.off[m];
     if (n > 0)
       solve_rows(a, a.lev[m].e2c_u, a.lev[m].e2c_vhs, partial + (size_t)r0 * np,
-                 mult + (size_t)r0 * np, tmp.get(), n);
+                 mult + (size_t)r0 * np, tmp.get(), n, s);
   }
 }
 
@@ -255,44 +249,27 @@ void run_stokes_downward(const StokesArgs &a, const double *mult, double *ple, d
     max_groups = std::max(max_groups, th.rg_hi[m] - th.rg_lo[m]);
     max_rows = std::max(max_rows, th.off[m + 1] - th.off[m]);
   }
-  DevBuf<double> sbig, y, lp, c, tmp;
-  sbig.alloc((size_t)std::max(max_groups, 1) * 4 * N_OFFSETS * np, s);
-  y.alloc((size_t)std::max(max_groups, 1) * 4 * np, s);
-  lp.alloc((size_t)std::max(max_groups, 1) * np, s);
-  c.alloc((size_t)std::max(max_groups, 1) * 4 * np, s);
+  DevBuf<double> tmp;
   tmp.alloc((size_t)std::max(max_rows, 1) * np, s);
-  FMMB_BLAS(cublasSetStream(a.blas, s));
-  const double one = 1.0, zero = 0.0;
   for (int m = 2; m < th.L; ++m) {
     const int lo = th.rg_lo[m], n_groups = th.rg_hi[m] - th.rg_lo[m];
     if (n_groups > 0) {
-      const int n = 4 * n_groups;
       if (m >= 3) {  // L2L from level m-1 (stokes_fmm.py:726-733)
         PhaseTimer timer(PH_DOWNWARD, s);
-        k_gather_parent_rows<<<grid_for((int64_t)n_groups * np, 256), 256, 0, s>>>(
-            n_groups, np, td.rg.get(), lo, td.parent.get(), loc, lp.get());
-        FMMB_CUDA(cudaGetLastError());
-        FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_N, CUBLAS_OP_N, 4 * np, n_groups, np, &one,
-                              a.lev[m - 1].l2lc, 4 * np, lp.get(), np, &zero, c.get(), 4 * np));
-        k_add_child_rows<<<grid_for((int64_t)n_groups * 4 * np, 256), 256, 0, s>>>(
-            n_groups, np, td.rg.get(), lo, c.get(), ple);
-        FMMB_CUDA(cudaGetLastError());
+        rowgemm(ParentRows{td.rg.get(), td.parent.get(), loc, lo, n_groups, np},
+                AddChildRows{td.rg.get(), ple, lo, np}, row_tiles(n_groups), a.lev[m - 1].l2lc,
+                4 * np, 4 * np, np, s);
       }
+      // M2L: tiles of one parity class, absent offsets skipped
       PhaseTimer timer(PH_M2L, s);
-      k_m2l_gather_cat<<<grid_for((int64_t)n * N_OFFSETS * np, 256, 148 * 64), 256, 0, s>>>(
-          n_groups, np, td.rg.get(), lo, td.il.get(), mult, sbig.get());
-      FMMB_CUDA(cudaGetLastError());
-      FMMB_BLAS(cublasDgemm(a.blas, CUBLAS_OP_T, CUBLAS_OP_N, np, n, N_OFFSETS * np, &one,
-                            a.lev[m].m2l_cat, N_OFFSETS * np, sbig.get(), N_OFFSETS * np, &zero,
-                            y.get(), np));
-      k_add_group_rows<<<grid_for((int64_t)n * np, 256), 256, 0, s>>>(n_groups, np, td.rg.get(),
-                                                                       lo, y.get(), ple);
-      FMMB_CUDA(cudaGetLastError());
+      const int tpc = row_tiles(n_groups);
+      rowgemm(M2LRows{td.rg.get(), td.il.get(), mult, lo, n_groups, np, tpc},
+              AddGroupRows{td.rg.get(), ple, lo, np}, 4 * tpc, a.lev[m].m2l_cat, np, np, np, s);
     }
     const int r0 = th.off[m], nr = th.off[m + 1] - th.off[m];
     if (nr > 0)
       solve_rows(a, a.lev[m].c2e_u, a.lev[m].c2e_vhs, ple + (size_t)r0 * np, loc + (size_t)r0 * np,
-                 tmp.get(), nr);
+                 tmp.get(), nr, s);
   }
 }
 
