@@ -132,6 +132,18 @@ class StokesBatch:
             for t in tup:
                 t.record_stream(cur)
 
+    def graph(self, kind="forward"):
+        """A CUDA graph of one batch call (kind "forward" or "adjoint") over
+        static input tensors: ``g.replay(inputs)`` copies the inputs into the
+        graph's buffers, launches the whole batch -- every problem's S2M,
+        level passes and evaluation on its stream -- as ONE graph launch, and
+        returns the outputs (tensors owned by the graph, overwritten by the
+        next replay).  The trees and operators stay those of this batch;
+        capture runs one warm-up call first so that every plan's expansion
+        buffers exist before capture (memory allocated inside the graph is
+        only its per-call scratch)."""
+        return _BatchGraph(self, kind)
+
     def status(self):
         for F in self._stokes:
             F.status()
@@ -149,7 +161,42 @@ def _device(a, stream):
     torch = _torch()
     if isinstance(a, torch.Tensor):
         t = a.to(device="cuda", dtype=torch.float64).contiguous()
-        if t.is_cuda and a.is_cuda:
+        if t.is_cuda and a.is_cuda and stream is not None:
             t.record_stream(stream)
         return t
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+class _BatchGraph:
+    def __init__(self, batch, kind):
+        torch = _torch()
+        if kind not in ("forward", "adjoint"):
+            raise ValueError("kind must be 'forward' or 'adjoint'")
+        self.batch, self.kind = batch, kind
+        width = 2 if kind == "forward" else 3
+        self.inputs = [tuple(torch.zeros(int(xd.numel()), dtype=torch.float64, device="cuda")
+                             for _ in range(width)) for xd, _ in batch._pts]
+        fn = batch.forward if kind == "forward" else batch.adjoint
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            fn(self.inputs)          # warm-up: plan buffers, side streams, kernel attributes
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        self.g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g):
+            self.outputs = fn(self.inputs)
+        torch.cuda.synchronize()
+
+    def replay(self, inputs=None):
+        """Copy ``inputs`` (same structure as the batch call's) into the graph's
+        buffers (None: keep the current ones), launch the graph, return the
+        outputs."""
+        if inputs is not None:
+            if len(inputs) != len(self.inputs):
+                raise ValueError(f"expected {len(self.inputs)} problems")
+            for dst, src in zip(self.inputs, inputs):
+                for d, v in zip(dst, src):
+                    d.copy_(_device(v, None) if not hasattr(v, "is_cuda") else v, non_blocking=True)
+        self.g.replay()
+        return self.outputs

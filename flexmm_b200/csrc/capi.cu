@@ -61,6 +61,22 @@ float tf32_rna(float x) {
 
 int pad8(int n) { return (n + 7) & ~7; }
 
+}  // namespace
+
+void smem_limit_impl(const void *kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> done;
+  int dev = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  size_t &have = done[{kernel, dev}];
+  if (have >= bytes) return;
+  FMMB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  have = bytes;
+}
+
+namespace {
+
 // sqrt(x) e^x K_n(x), n = 0, 1, for x >= 1: trapezoidal rule on
 // int_0^inf exp(-2x sinh^2(t/2)) cosh^n(t) dt (exponent without cancellation;
 // step below the integrand's width 1/sqrt(x); summed from the small terms up)

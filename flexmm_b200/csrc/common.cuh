@@ -126,6 +126,16 @@ void launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, c
   FMMB_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...));
 }
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device.  The attribute is set once per (kernel, device) and size
+// (later calls that need no more are no-ops), so launches inside a CUDA
+// graph capture make no attribute calls once the kernel has run before.
+void smem_limit_impl(const void *kernel, size_t bytes);
+template <class F>
+inline void smem_limit(F *kernel, size_t bytes) {
+  smem_limit_impl(reinterpret_cast<const void *>(kernel), bytes);
+}
+
 // blocks for a persistent or grid-stride kernel over `units` work units (at
 // most one block per unit): per_sm blocks per SM on a large problem, fewer
 // on a small one (a batch of small problems then does not launch thousands

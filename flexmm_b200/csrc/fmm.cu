@@ -802,16 +802,14 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   const int np = a.np;
   if (th.L < 3) return;
   const size_t s2m_bytes = sizeof(double) * (size_t)TN * pad_ld(np) * 2;
-  FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(s2m_bytes)));
+  smem_limit(k_s2m<KF>, s2m_bytes);
   // persistent over the S2M nodes; at most one block per TN nodes of the tree
   // (small trees launch small grids)
   const int s2m_grid = std::max(1, std::min(148 * 4, (th.n_total() + TN - 1) / TN));
   PhaseTimer timer(PH_UPWARD, s);
   if (a.dvx) {
     if constexpr (std::is_same<KF, LaplaceF64T>::value) {
-      FMMB_CUDA(cudaFuncSetAttribute(k_s2m<KF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(s2m_bytes)));
+      smem_limit(k_s2m<KF, true>, s2m_bytes);
       k_s2m<KF, true><<<dim3(s2m_grid, n_rhs), NT, s2m_bytes, s>>>(
           a.kp, a.neq, np, th.L, td.dev_off.get(), td.uplist.get(), td.n_up.get(), td.bot.get(),
           td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
@@ -827,8 +825,7 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   }
   FMMB_CUDA(cudaGetLastError());
   const size_t m2m_bytes = sizeof(double) * (size_t)TN * (2 * pad_ld(np) + pad_ld(4 * np));
-  FMMB_CUDA(cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(m2m_bytes)));
+  smem_limit(k_m2m, m2m_bytes);
   for (int m = th.L - 2; m >= 2; --m) {
     const int c_first = th.off[m + 1];
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
@@ -935,8 +932,7 @@ void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s,
   tl.tile_start[4 * th.L] = tiles;
   if (tiles == 0) return;
   const size_t sm = sizeof(double) * (size_t)TM * (pad_ld(a.np) + pad_ld(32));
-  FMMB_CUDA(cudaFuncSetAttribute(k_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(double) * TM * (pad_ld(64) + pad_ld(32)))));
+  smem_limit(k_m2l, sizeof(double) * TM * (pad_ld(64) + pad_ld(32)));
   PhaseTimer timer(PH_M2L, s);
   k_m2l<<<dim3(tiles, n_rhs), NT, sm, s>>>(tl, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
                                            mult, ple, cstride);

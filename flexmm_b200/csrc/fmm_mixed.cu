@@ -1185,8 +1185,7 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
   const int np = a.np;
   if (th.L < 3) return;
   const size_t pbytes = sizeof(double) * ((size_t)TN * pad_ld(np) * 2 + c2e_stage_doubles(np));
-  FMMB_CUDA(cudaFuncSetAttribute(k_s2m_mx<KF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(pbytes)));
+  smem_limit(k_s2m_mx<KF32>, pbytes);
   PhaseTimer timer(PH_UPWARD, s);
   k_s2m_mx<KF32><<<work_grid((th.n_total() + TN - 1) / TN, 4), NT, pbytes, s>>>(a.kp, a.neq, np, th.L, td.dev_off.get(),
                                               td.uplist.get(), td.n_up.get(), td.bot.get(),
@@ -1198,7 +1197,7 @@ void upward_mx_impl(const PassArgs &a, const double *tau_s, const double *tsum, 
   const bool stage_b = m2m_mx_smem(np, true) + 4096 <= smem_optin();
   const size_t mbytes = m2m_mx_smem(np, stage_b);
   auto kern = stage_b ? k_m2m_mx<true> : k_m2m_mx<false>;
-  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(mbytes)));
+  smem_limit(kern, mbytes);
   for (int m = th.L - 2; m >= 2; --m) {
     const int c_first = th.off[m + 1];
     const int n_groups = (th.off[m + 2] - th.off[m + 1]) / 4;
@@ -1274,7 +1273,7 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc,
     // persistent: one CTA per SM (its shared memory admits no second one),
     // each walking tiles blockIdx.x, blockIdx.x + gridDim.x, ...
     const size_t sm = TC_STAGES * m2l_tc_stage_bytes(a.np);
-    FMMB_CUDA(cudaFuncSetAttribute(k_m2l_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    smem_limit(k_m2l_tc, sm);
     int dev = 0, sms = 0;
     FMMB_CUDA(cudaGetDevice(&dev));
     FMMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1303,7 +1302,7 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
   const bool stage_b = bytes(true) + 4096 <= smem_optin();
   const size_t sm = bytes(stage_b);
   auto kern = stage_b ? k_downward_mx<true> : k_downward_mx<false>;
-  FMMB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  smem_limit(kern, sm);
   for (int m = 2; m < th.L; ++m) {
     const int lo = th.rg_lo[m], cnt = th.rg_hi[m] - th.rg_lo[m];
     if (cnt <= 0) continue;

@@ -116,3 +116,33 @@ def test_stokes_batch_reads_forces_made_on_the_callers_stream(built_lib):
     for k in range(len(probs)):
         for r in range(3):
             assert rel_l2(outs[k][r].cpu().numpy(), ref[k][r]) < 1e-14, (k, r)
+
+
+@pytest.mark.gpu
+def test_stokes_batch_graph_replay_equals_eager(built_lib):
+    """The whole batch captured as one CUDA graph (forward and adjoint):
+    replays with new inputs equal the eager calls."""
+    import torch
+    from flexmm_b200.batch import StokesBatch
+    probs, forces, cots = _problems(seed=21)
+    B = StokesBatch(probs, Nequiv=24, Ncutoff=64, n_streams=4)
+    gf = B.graph("forward")
+    ga = B.graph("adjoint")
+    for seed in (1, 2):
+        rng = np.random.default_rng(seed)
+        f = [(rng.standard_normal(x.size), rng.standard_normal(x.size)) for x, _ in probs]
+        c = [tuple(rng.standard_normal(x.size) for _ in range(3)) for x, _ in probs]
+        want_f = [[t.cpu().numpy() for t in tup] for tup in B.forward(f)]
+        want_a = [[t.cpu().numpy() for t in tup] for tup in B.adjoint(c)]
+        dev = lambda a: torch.from_numpy(a).cuda()
+        got_f = gf.replay([tuple(dev(v) for v in tup) for tup in f])
+        got_f = [[t.cpu().numpy() for t in tup] for tup in got_f]
+        got_a = ga.replay([tuple(dev(v) for v in tup) for tup in c])
+        got_a = [[t.cpu().numpy() for t in tup] for tup in got_a]
+        torch.cuda.synchronize()
+        B.status()
+        for k in range(len(probs)):
+            for r in range(3):
+                assert rel_l2(got_f[k][r], want_f[k][r]) < 1e-14, (seed, k, r)
+            for r in range(2):
+                assert rel_l2(got_a[k][r], want_a[k][r]) < 1e-14, (seed, k, r)
