@@ -720,7 +720,8 @@ def measure_batched_stokes(args, world=1, n_problems=256):
     tree_probs = [probs[i] for i in mine]
 
     def with_trees():
-        Bt = StokesBatch(tree_probs, Nequiv=32, Ncutoff=64, n_streams=8, adjoint=False)
+        Bt = StokesBatch(tree_probs, Nequiv=32, Ncutoff=64, n_streams=8, adjoint=False,
+                         precomputations=B.precomputations)
         Bt.forward(f_loc)
     ms_t = timed(with_trees, reps=1)
     res = {"workload": f"{n_problems} independent Stokes problems, N_i log-uniform in "

@@ -37,12 +37,16 @@ class StokesBatch:
     ``(dfx, dfy)``.  Results are CUDA tensors (call ``torch.cuda.synchronize``
     or read them, which waits, before using them on the host)."""
 
-    def __init__(self, problems, Nequiv=32, Ncutoff=64, n_streams=8, adjoint=True):
+    def __init__(self, problems, Nequiv=32, Ncutoff=64, n_streams=8, adjoint=True,
+                 precomputations=None):
+        """``precomputations``: the operators of an earlier batch with the same
+        Nequiv (``batch.precomputations``), so that widths it met are not
+        formed again."""
         torch = _torch()
         self.Nequiv, self.Ncutoff = int(Nequiv), int(Ncutoff)
         self.streams = [torch.cuda.Stream() for _ in range(max(1, int(n_streams)))]
         self._pts, self._stokes, self._laplace = [], [], []
-        pre = {}
+        pre = dict(precomputations) if precomputations else {}
         helper = KI_Helper()
         for k, (x, y) in enumerate(problems):
             with torch.cuda.stream(self._stream(k)):
@@ -59,6 +63,7 @@ class StokesBatch:
                     L.register_evaluator(None, None, "gradient", 3)  # (u, du/dx, du/dy)
                 self._laplace.append(L)
                 self._pts.append((xd, yd))
+        self.precomputations = pre
         torch.cuda.synchronize()
 
     def _stream(self, k):

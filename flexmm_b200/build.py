@@ -74,7 +74,8 @@ def build(force=False, verbose=False):
         with ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 4)) as ex:
             list(ex.map(compile_one, todo))
     tmp = LIB + ".tmp"
-    cmd = [nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + \
+    # -z defs: an unresolved symbol fails the build instead of the first load
+    cmd = [nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-Xlinker", "-z,defs"] + \
         [_obj(s) for s in sources()] + ["-o", tmp] + LINK
     if verbose:
         print(" ".join(cmd), flush=True)

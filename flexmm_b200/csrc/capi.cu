@@ -63,7 +63,7 @@ int pad8(int n) { return (n + 7) & ~7; }
 
 }  // namespace
 
-void smem_limit_impl(const void *kernel, size_t bytes) {
+void fmmb::smem_limit_impl(const void *kernel, size_t bytes) {
   static std::mutex mu;
   static std::map<std::pair<const void *, int>, size_t> done;
   int dev = 0;
