@@ -343,7 +343,9 @@ def _split_vs_one_pass(tmp_path):
         got = F.source_evaluation(x, y).cpu().numpy()
         F.status()
         assert np.isfinite(got).all()
-        assert rel_l2(got, ref[prec]) < (1e-14 if prec == "fp64" else 1e-9), prec
+        # mixed: FP32 partial sums grouped differently (L2T and P2P apart),
+        # ~1e-9 apart, against the form's ~1e-7 error
+        assert rel_l2(got, ref[prec]) < (1e-14 if prec == "fp64" else 2e-8), prec
 
 
 @pytest.mark.parametrize("case", golden_cases(dipole=True))
