@@ -47,22 +47,51 @@ class StokesBatch:
         self.streams = [torch.cuda.Stream() for _ in range(max(1, int(n_streams)))]
         self._pts, self._stokes, self._laplace = [], [], []
         pre = dict(precomputations) if precomputations else {}
-        helper = KI_Helper()
-        for k, (x, y) in enumerate(problems):
+        problems = list(problems)
+        n = len(problems)
+        # Trees: problem 0 first; its level widths fix the dyadic family every
+        # later box snaps to (Stokes FMM adjust_bbox, stokes_fmm.py:608-637),
+        # whatever deeper widths later problems add, so the other trees can be
+        # built concurrently (each on its stream, from a pool of host threads:
+        # the tree build's host waits then overlap) with their snapped boxes
+        # computed up front.  Operators are bound afterwards, in problem order.
+        def build(k, bbox, pre_k):
+            x, y = problems[k]
             with torch.cuda.stream(self._stream(k)):
                 xd = torch.as_tensor(np.asarray(x, dtype=np.float64)).cuda()
                 yd = torch.as_tensor(np.asarray(y, dtype=np.float64)).cuda()
-                F = StokesFMM(xd, yd, self.Nequiv, self.Ncutoff, None,
-                              precomputations=pre if pre else None)
-                F.precompute()
+                return StokesFMM(xd, yd, self.Nequiv, self.Ncutoff, bbox,
+                                 precomputations=pre_k if pre_k else None), xd, yd
+        fmms = [None] * n
+        if n:
+            fmms[0] = build(0, None, pre)
+            with torch.cuda.stream(self._stream(0)):
+                fmms[0][0].precompute()
+            pre = fmms[0][0].precomputations
+        if n > 1:
+            from concurrent.futures import ThreadPoolExecutor
+            boxes = [None] + [[float(np.min(x)), float(np.max(x)), float(np.min(y)), float(np.max(y))]
+                              for x, y in (map(np.asarray, problems[k]) for k in range(1, n))]
+            with ThreadPoolExecutor(max_workers=len(self.streams)) as ex:
+                for k, r in zip(range(1, n), ex.map(lambda k: build(k, boxes[k], pre), range(1, n))):
+                    fmms[k] = r
+            for k in range(1, n):
+                F = fmms[k][0]
+                F.input_precomputations = pre   # every width met so far
+                with torch.cuda.stream(self._stream(k)):
+                    F.precompute()
                 pre = F.precomputations  # operators shared by width across problems
-                self._stokes.append(F)
-                L = None
-                if adjoint:
+        helper = KI_Helper()
+        for k in range(n):
+            F, xd, yd = fmms[k]
+            self._stokes.append(F)
+            L = None
+            if adjoint:
+                with torch.cuda.stream(self._stream(k)):
                     L = KI_FMM(xd, yd, "Laplace_Eval", self.Ncutoff, self.Nequiv, helper=helper)
-                    L.register_evaluator(None, None, "gradient", 3)  # (u, du/dx, du/dy)
-                self._laplace.append(L)
-                self._pts.append((xd, yd))
+                L.register_evaluator(None, None, "gradient", 3)  # (u, du/dx, du/dy)
+            self._laplace.append(L)
+            self._pts.append((xd, yd))
         self.precomputations = pre
         torch.cuda.synchronize()
 

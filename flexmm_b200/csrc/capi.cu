@@ -919,6 +919,69 @@ int fmm_evaluate_sources_multi(fmm_plan *p, int check, double *out, int64_t ld_o
   });
 }
 
+int fmm_plan_create_local(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
+                          double min_width, const double *bbox, void *stream, fmm_plan **out) {
+  return guarded([&] {
+    FMMB_CHECK(ops && x && y && bbox && out, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(ops->method == METHOD_KIFMM && ops->kernel_id >= 0, ERR_INVALID_ARGUMENT,
+               "a local plan takes a kernel operator set (fmm_ops_create)");
+    FMMB_CHECK(min_width >= 0.0, ERR_INVALID_ARGUMENT, "negative minimum width");
+    // a box of level m (width w0 / 2^m, halved level by level as the
+    // reference does) splits only while its width exceeds 2 min_width
+    const double w0 = bbox[1] - bbox[0];
+    int max_split = 0;
+    for (double w = w0; max_split < 64 && w > 2.0 * min_width; w *= 0.5) ++max_split;
+    retain_pool_memory();
+    auto p = std::make_unique<fmm_plan>();
+    p->ops = ops;
+    p->stream = (cudaStream_t)stream;
+    {
+      PhaseTimer timer(PH_TREE, p->stream);
+      build_tree(p->td, p->th, x, y, n, ncutoff, bbox, p->stream, max_split);
+    }
+    p->bound.assign(p->th.L, -1);
+    *out = p.release();
+  });
+}
+
+int fmm_local_evaluate(fmm_plan *p, const double *tau, const double *tx, const double *ty,
+                       int64_t m, int check, const int64_t *src_cat, const int64_t *tgt_cat,
+                       double *out, void *stream) {
+  return guarded([&] {
+    tree_ready(p);
+    FMMB_CHECK(p && tau, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(p->ops->method == METHOD_KIFMM, ERR_INVALID_ARGUMENT, "not a local plan");
+    FMMB_CHECK((src_cat == nullptr) == (tgt_cat == nullptr), ERR_INVALID_ARGUMENT,
+               "source and target categories go together");
+    FMMB_CHECK(m >= 0, ERR_INVALID_ARGUMENT, "negative target count");
+    if (m == 0) return;
+    FMMB_CHECK(tx && ty && out, ERR_INVALID_ARGUMENT, "NULL argument");
+    FMMB_CHECK(m < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 targets");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = p->th.n_points;
+    p->tau_s.alloc(n, s);
+    gather_sorted(tau, p->td.ordv.get(), n, p->tau_s.get(), s);
+    DevBuf<int64_t> scat;
+    if (src_cat) {
+      scat.alloc(n, s);
+      gather_sorted_i64(src_cat, p->td.ordv.get(), n, scat.get(), s);
+    }
+    PassArgs a = pass_args(p);
+    DevBuf<uint64_t> tkeys;
+    DevBuf<int> tperm;
+    DevBuf<double> txs, tys;
+    {
+      PhaseTimer timer(PH_SORT_TGT, s);
+      txs.alloc(m, s);
+      tys.alloc(m, s);
+      sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
+                  tys.get());
+    }
+    run_local_evaluate(a, p->tau_s.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(), m,
+                       check, src_cat ? scat.get() : nullptr, tgt_cat, out, s);
+  });
+}
+
 static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream);
 
 int fmm_build_expansions(fmm_plan *p, const double *tau, void *stream) {

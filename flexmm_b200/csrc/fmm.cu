@@ -476,7 +476,10 @@ __global__ void k_make_items(int total, int L, const int *__restrict__ off, cons
 // point order) or EVAL_FAR (L2T only, plus near[]: out = far + near).
 // DIP: the sources also carry dipoles (dvx, dvy: strength * normal, sorted);
 // Laplace (table-driven functor), potential only.
-template <class KF, int NOUT, int PART = EVAL_FULL, bool DIP = false>
+// CAT (near field only): a source whose category scat[] (sorted order)
+// equals the target's tcat[] (caller's order) is left out
+// (flexmm/flexmm2d/local_evaluator_category.py:33-38).
+template <class KF, int NOUT, int PART = EVAL_FULL, bool DIP = false, bool CAT = false>
 __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int np,
                                                   const int4 *__restrict__ items,
                                                   const int *__restrict__ n_items_ptr,
@@ -496,12 +499,16 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
                                                   double *__restrict__ out, int64_t ld_out,
                                                   double *__restrict__ near = nullptr,
                                                   const double *__restrict__ dvx = nullptr,
-                                                  const double *__restrict__ dvy = nullptr) {
+                                                  const double *__restrict__ dvy = nullptr,
+                                                  const int64_t *__restrict__ scat = nullptr,
+                                                  const int64_t *__restrict__ tcat = nullptr) {
   static_assert(PART == EVAL_FULL || NOUT == 1, "split evaluation: potential only");
+  static_assert(!CAT || (PART == EVAL_NEAR && !DIP), "categories: near field of charges only");
   static_assert(!DIP || (KF::kLogTable && NOUT == 1), "dipoles: table Laplace, potential only");
   __shared__ double Ls[64], lxs[64], lys[64];
   __shared__ double ssx[SMAX], ssy[SMAX], stau[SMAX];
   __shared__ double sdx[DIP ? SMAX : 1], sdy[DIP ? SMAX : 1];
+  __shared__ long long scs[CAT ? SMAX : 1];
   __shared__ int rb[9], rs[10];  // colleague range begins and prefix sizes
   __shared__ double red[NOUT][TCH / 32];
   __shared__ FunctorSmem<KF> fsm;
@@ -520,6 +527,8 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
     const bool valid = t < cnt;
     const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
+    long long tc = 0;
+    if constexpr (CAT) tc = valid ? (long long)tcat[tperm[t0 + t]] : 0;
     if (threadIdx.x < 9) {
       const int cg = PART == EVAL_FAR ? -1 : coll[(size_t)g * 9 + threadIdx.x];
       rb[threadIdx.x] = cg >= 0 ? bot[cg] : 0;
@@ -569,6 +578,14 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
         const double ax = x - qx, ay = y - qy;
         if (check && ax == 0.0 && ay == 0.0) return 0.0;
         return K.raw(ax, ay) * stau[j] + dipole_at(sdx[j], sdy[j], ax, ay);
+      } else if constexpr (CAT) {  // a source of the target's own category adds nothing
+        if (scs[j] == tc) return 0.0;
+        if constexpr (kFolded) {
+          return K.raw_checked(qx, qy, x, y, check) * stau[j];
+        } else {
+          const double v = K(qx, qy, x, y) * stau[j];
+          return (check && x - qx == 0.0 && y - qy == 0.0) ? 0.0 : v;
+        }
       } else if constexpr (kFolded) {
         return K.raw_checked(qx, qy, x, y, check) * stau[j];
       } else {
@@ -591,6 +608,7 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
           sdx[i] = dvx[j];
           sdy[i] = dvy[j];
         }
+        if constexpr (CAT) scs[i] = (long long)scat[j];
       }
       __syncthreads();
       if (valid) {
@@ -892,7 +910,8 @@ void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, co
     kern<<<work_grid(units, 8), TCH, 0, s>>>(a.kp, a.neq, a.np, it.items.get(), it.n_items.get(),
                                  td.coll.get(), td.bot.get(), td.top.get(), td.xmid.get(),
                                  td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc,
-                                 txs, tys, tperm, check, out, ld_out, nullptr, nullptr, nullptr);
+                                 txs, tys, tperm, check, out, ld_out, nullptr, nullptr, nullptr,
+                                 nullptr, nullptr);
   }
   FMMB_CUDA(cudaGetLastError());
 }
@@ -1089,6 +1108,62 @@ void run_evaluate_sources_split(const PassArgs &a, const double *tau_s, const do
   }
 }
 
+namespace {
+template <class KF>
+void local_impl(const PassArgs &a, const double *tau_s, const double *txs, const double *tys,
+                const uint64_t *tkeys, const int *tperm, int64_t m, int check,
+                const int64_t *scat, const int64_t *tcat, double *out, cudaStream_t s) {
+  const TreeDev &td = *a.td;
+  EvalItems it;
+  eval_items(a, tkeys, m, it, s);
+  const int grid = work_grid(a.th->n_total() + m / TCH + 1, 8);
+  PhaseTimer timer(PH_EVAL, s);
+  if (scat)
+    k_evaluate<KF, 1, EVAL_NEAR, false, true><<<grid, TCH, 0, s>>>(
+        a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+        td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+        nullptr, txs, tys, tperm, check, out, 0, out, nullptr, nullptr, scat, tcat);
+  else
+    k_evaluate<KF, 1, EVAL_NEAR><<<grid, TCH, 0, s>>>(
+        a.kp, a.neq, a.np, it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
+        td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), tau_s, a.ops_dev,
+        nullptr, txs, tys, tperm, check, out, 0, out, nullptr, nullptr, nullptr, nullptr);
+  FMMB_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void run_local_evaluate(const PassArgs &a, const double *tau_s, const double *txs,
+                        const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
+                        int check, const int64_t *scat, const int64_t *tcat, double *out,
+                        cudaStream_t s) {
+  if (m == 0) return;
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE:
+      local_impl<LaplaceF64T>(a, tau_s, txs, tys, tkeys, tperm, m, check, scat, tcat, out, s);
+      break;
+    case KERNEL_MOD_HELMHOLTZ:
+      local_impl<ModHelmholtzF64>(a, tau_s, txs, tys, tkeys, tperm, m, check, scat, tcat, out, s);
+      break;
+    case KERNEL_RADIAL_TABLE:
+      local_impl<RadialTableF64>(a, tau_s, txs, tys, tkeys, tperm, m, check, scat, tcat, out, s);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
+}
+
+__global__ void k_gather_i64(const int64_t *__restrict__ v, const int *__restrict__ perm, int64_t n,
+                             int64_t *__restrict__ o) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    o[i] = v[perm[i]];
+}
+
+void gather_sorted_i64(const int64_t *v, const int *perm, int64_t n, int64_t *o, cudaStream_t s) {
+  if (n == 0) return;
+  k_gather_i64<<<grid_for(n, 256), 256, 0, s>>>(v, perm, n, o);
+  FMMB_CUDA(cudaGetLastError());
+}
+
 void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const double *sy,
                 const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
                 int check, double *out, cudaStream_t s) {
@@ -1140,7 +1215,7 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
                                                              td.coll.get(), td.bot.get(),
                                  td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(),
                                  td.sy.get(), tau_s, a.ops_dev, loc, txs, tys, tperm, check, out, 0,
-                                 nullptr, nullptr, nullptr);
+                                 nullptr, nullptr, nullptr, nullptr, nullptr);
   };
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: launch(k_evaluate<LaplaceF64T, 1>); break;

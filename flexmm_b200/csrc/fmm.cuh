@@ -141,6 +141,13 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
                 const double *tau, int64_t ns, const double *tx, const double *ty, int64_t nt,
                 int check, double *out, cudaStream_t s);
 void gather_sorted(const double *v, const int *perm, int64_t n, double *o, cudaStream_t s);
+void gather_sorted_i64(const int64_t *v, const int *perm, int64_t n, int64_t *o, cudaStream_t s);
+// near field only (local evaluator): out[i] = sum over the target's
+// colleagues' sources; scat (sorted) / tcat (caller's order) categories, or null
+void run_local_evaluate(const PassArgs &a, const double *tau_sorted, const double *txs,
+                        const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
+                        int check, const int64_t *scat, const int64_t *tcat, double *out,
+                        cudaStream_t s);
 // the FP64 passes' table-driven log2 and the library log2 at n device points
 void run_diag_log2(const double *x, int64_t n, double *out_tab, double *out_lib, cudaStream_t s);
 // nout = 1: potential into out[m]; nout = 3: potential and its gradient in the

@@ -239,23 +239,26 @@ __global__ void k_gather_xy(const double *__restrict__ x, const double *__restri
 // With keys sorted on their top `sorted_digits` digits, point i starts a box
 // of every level in (cprev, cnext] that holds more than ppl points: the run
 // from i is longer than ppl iff key i and key i+ppl share that prefix.
+// Boxes of levels >= max_split stay leaves whatever their point count (the
+// local evaluator's width floor, flexmm/local_tree.py:191-222).
 __device__ __forceinline__ void split_range(const uint64_t *__restrict__ keys, int64_t n, int ppl,
-                                            int64_t i, int &cprev, int &cnext) {
+                                            int64_t i, int &cprev, int &cnext, int max_split) {
   const uint64_t k = keys[i];
   cprev = (i == 0) ? -1 : common_digits(keys[i - 1], k);
   cnext = (i + ppl < n) ? common_digits(k, keys[i + ppl]) : -1;
+  if (cnext >= max_split) cnext = max_split - 1;
 }
 
 // number of split boxes each point starts; flags trees too deep for the key
 // or for the partial sort; deepest split level
 __global__ void k_split_counts(const uint64_t *__restrict__ keys, int64_t n, int ppl,
                                int sorted_digits, unsigned long long *__restrict__ counts,
-                               Counters *cnt) {
+                               Counters *cnt, int max_split) {
   int lmax = -1;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int cprev, cnext;
-    split_range(keys, n, ppl, i, cprev, cnext);
+    split_range(keys, n, ppl, i, cprev, cnext, max_split);
     unsigned long long c = 0;
     if (cnext > cprev) {
       if (cnext >= MAXD) {
@@ -278,13 +281,13 @@ __global__ void k_split_counts(const uint64_t *__restrict__ keys, int64_t n, int
 __global__ void k_split_emit(const uint64_t *__restrict__ keys, int64_t n, int ppl,
                              const unsigned long long *__restrict__ counts,
                              const unsigned long long *__restrict__ pos, uint64_t *__restrict__ out,
-                             unsigned long long cap, Counters *cnt) {
+                             unsigned long long cap, Counters *cnt, int max_split) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     if (i == n - 1) cnt->s0_count = pos[i] + counts[i];
     if (!counts[i]) continue;
     int cprev, cnext;
-    split_range(keys, n, ppl, i, cprev, cnext);
+    split_range(keys, n, ppl, i, cprev, cnext, max_split);
     const uint64_t k = keys[i];
     for (int m = cprev + 1; m <= cnext; ++m) {
       const unsigned long long p = pos[i] + (unsigned long long)(m - cprev - 1);
@@ -911,7 +914,7 @@ void sort_points_scratch(const double *x, const double *y, int64_t n, const Tree
 }
 
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
-                const double bbox[4], cudaStream_t s) {
+                const double bbox[4], cudaStream_t s, int max_split) {
   FMMB_CHECK(n > 0, ERR_INVALID_ARGUMENT, "tree needs at least one point");
   FMMB_CHECK(ppl >= 1, ERR_INVALID_ARGUMENT, "Ncutoff must be >= 1");
   FMMB_CHECK(n < (int64_t(1) << 31) - 1, ERR_INVALID_ARGUMENT, "more than 2^31-2 points");
@@ -939,11 +942,11 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits, td.sx.get(), td.sy.get());
     cnt.zero(s);
     k_split_counts<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, scount.get(),
-                                                     cnt.get());
+                                                     cnt.get(), max_split);
     FMMB_CUDA(cudaGetLastError());
     exclusive_sum(scount.get(), spos.get(), n, s);
     k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
-                                                   s0raw.get(), cap0, cnt.get());
+                                                   s0raw.get(), cap0, cnt.get(), max_split);
     FMMB_CUDA(cudaGetLastError());
     FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));

@@ -78,9 +78,10 @@ struct TreeHost {
 // after build_tree comes after this.
 void finalize_tree(TreeHost &th);
 
-// Build the tree over device coordinates x, y (n points) on `stream`.
+// Build the tree over device coordinates x, y (n points) on `stream`;
+// boxes of levels >= max_split are never split (default: no floor).
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
-                const double bbox[4], cudaStream_t stream);
+                const double bbox[4], cudaStream_t stream, int max_split = 64);
 
 // Sort arbitrary points by the same descent key on its top `sorted_digits`
 // quadrant digits (enough to place them in boxes of levels <= sorted_digits);

@@ -146,6 +146,24 @@ int fmm_ops_destroy(fmm_ops *ops);
  * not map memory while earlier work is still queued. */
 int fmm_plan_create(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
                     const double *bbox, void *stream, fmm_plan **out);
+/* Near-field-only evaluation, the LocalEvaluator family
+ * (flexmm/flexmm2d/local_evaluator.py, local_evaluator_category.py,
+ * periodic_local_evaluator_category.py; LocalTree, flexmm/local_tree.py):
+ * fmm_plan_create_local builds the tree of fmm_plan_create except that a box
+ * splits only while it holds more than ncutoff points AND its width exceeds
+ * 2 min_width (local_tree.py:191-222), on an operator set of the kernel
+ * (fmm_ops_create; no levels need binding).  fmm_local_evaluate sums, at m
+ * device points, the kernel over the sources of the target leaf's
+ * colleagues only -- no far field -- with charges tau (caller's source
+ * order); check != 0 skips coincident sources; src_cat / tgt_cat (device
+ * int64, both or neither) leave out sources whose category equals the
+ * target's (local_evaluator_category.py:33-38).  out[m] is overwritten. */
+int fmm_plan_create_local(fmm_ops *ops, const double *x, const double *y, int64_t n, int ncutoff,
+                          double min_width, const double *bbox, void *stream, fmm_plan **out);
+int fmm_local_evaluate(fmm_plan *plan, const double *tau, const double *tx, const double *ty,
+                       int64_t m, int check, const int64_t *src_cat, const int64_t *tgt_cat,
+                       double *out, void *stream);
+
 /* n_levels and, for each level, its box width and node count (host arrays of
  * FMM_MAX_LEVELS entries). */
 int fmm_plan_info(fmm_plan *plan, int *n_levels, double *widths, int *n_nodes);

@@ -91,6 +91,10 @@ def case_inputs(meta):
         d["bbox"] = None
     if meta.get("method") == "stokes":  # second force component
         d["tau2"] = np.random.default_rng(meta["seed"] + 1000).standard_normal(d["x"].size)
+    if meta.get("local") in ("category", "periodic"):  # source and target categories
+        r3 = np.random.default_rng(meta["seed"] + 3000)
+        d["cat"] = r3.integers(0, meta["ncat"], d["x"].size)
+        d["tcat"] = r3.integers(0, meta["ncat"], d["tx"].size)
     if meta.get("dipole"):  # double-layer strengths and unit normals
         r2 = np.random.default_rng(meta["seed"] + 2000)
         d["dlp"] = r2.standard_normal(d["x"].size)
@@ -144,6 +148,12 @@ CASES = {
                                    neq=32, dipole=True), True),
     "dip_duplicates_5k_q24": (dict(recipe="duplicates", seed=33, n=5000, n_grid=33, ncut=16,
                                    neq=24, dipole=True), True),
+    "local_uniform_20k": (dict(recipe="uniform", seed=34, n=20000, n_grid=64, ncut=20,
+                               local="plain", delta=2.0 ** -5), True),
+    "local_cat_clustered_20k": (dict(recipe="clustered", seed=35, n=20000, n_grid=64, ncut=20,
+                                     local="category", delta=2.0 ** -5, ncat=7), True),
+    "local_periodic_10k": (dict(recipe="uniform", seed=36, n=10000, n_grid=50, ncut=20,
+                                local="periodic", delta=2.0 ** -4, ncat=5), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -381,6 +391,101 @@ def run_dipole_case(name, meta, ref):
           f"tgt {rel(ut, dt):.2e}", flush=True)
 
 
+def local_bump(delta):
+    """The test kernel of the local evaluators: (1 - r^2/delta^2)^3 for
+    r < delta, else 0 (compact support of radius delta)."""
+    def f(r):
+        r = np.asarray(r, dtype=np.float64)
+        q = 1.0 - (r / delta) ** 2
+        return np.where(r < delta, q * q * q, 0.0)
+    return f
+
+
+def local_direct(meta, sx, sy, tau, tx, ty, check, scat=None, tcat=None):
+    """FP64 direct sum of the compact bump (numpy): every source within delta."""
+    f = local_bump(meta["delta"])
+    out = np.zeros(tx.size)
+    step = max(1, 2_000_000 // max(sx.size, 1))
+    for a in range(0, tx.size, step):
+        b = min(tx.size, a + step)
+        dx = tx[a:b, None] - sx[None, :]
+        dy = ty[a:b, None] - sy[None, :]
+        w = f(np.sqrt(dx * dx + dy * dy)) * tau[None, :]
+        if check:
+            w = np.where((dx == 0) & (dy == 0), 0.0, w)
+        if scat is not None:
+            w = np.where(scat[None, :] == tcat[a:b, None], 0.0, w)
+        out[a:b] = w.sum(1)
+    return out
+
+
+def run_local_case(name, meta, ref):
+    """The reference's local evaluators (flexmm/flexmm2d/local_evaluator.py,
+    local_evaluator_category.py, periodic_local_evaluator_category.py) with
+    the compact bump as Kernel_Add, ncutoff and min_distance from meta."""
+    import numba
+    D2 = float(meta["delta"]) ** 2
+
+    @numba.njit(fastmath=True)
+    def Kernel_Add(sx, sy, tx, ty, tau, out):
+        dx = tx - sx
+        dy = ty - sy
+        d2 = dx * dx + dy * dy
+        if d2 < D2:
+            q = 1.0 - d2 / D2
+            out[0] += q * q * q * tau
+
+    d = case_inputs(meta)
+    n, m = d["x"].size, d["tx"].size
+    kind = meta["local"]
+    out_s = np.zeros((n, 1))
+    out_t = np.zeros((m, 1))
+    t0 = time.time()
+    if kind == "plain":
+        from flexmm.flexmm2d.local_evaluator import LocalEvaluator
+        E = LocalEvaluator(d["x"], d["y"], Kernel_Add, meta["delta"], ncutoff=meta["ncut"])
+        E.load_tau(d["tau"])
+        E.source_evaluation(d["x"], d["y"], out_s)
+        E.target_evaluation(d["tx"], d["ty"], out_t)
+        ds = local_direct(meta, d["x"], d["y"], d["tau"], d["x"], d["y"], True)
+        dt = local_direct(meta, d["x"], d["y"], d["tau"], d["tx"], d["ty"], False)
+    elif kind == "category":
+        from flexmm.flexmm2d.local_evaluator_category import LocalEvaluator
+        E = LocalEvaluator(d["x"], d["y"], d["cat"], Kernel_Add, meta["delta"], ncutoff=meta["ncut"])
+        E.load_tau(d["tau"])
+        E.target_evaluation(d["x"], d["y"], d["cat"], out_s)
+        E.target_evaluation(d["tx"], d["ty"], d["tcat"], out_t)
+        ds = local_direct(meta, d["x"], d["y"], d["tau"], d["x"], d["y"], False, d["cat"], d["cat"])
+        dt = local_direct(meta, d["x"], d["y"], d["tau"], d["tx"], d["ty"], False, d["cat"], d["tcat"])
+    else:
+        from flexmm.flexmm2d.periodic_local_evaluator_category import PeriodicLocalEvaluator
+        bounds = [-1.0, 1.0, -1.0, 1.0]
+        E = PeriodicLocalEvaluator(d["x"], d["y"], d["cat"], Kernel_Add, meta["delta"], bounds,
+                                   ncutoff=meta["ncut"])
+        E.load_tau(d["tau"])
+        E.target_evaluation(d["x"], d["y"], d["cat"], out_s)
+        E.target_evaluation(d["tx"], d["ty"], d["tcat"], out_t)
+        # direct sum over the 3 x 3 periodic copies of the sources
+        sx = np.concatenate([d["x"] + 2 * a for a in (-1, 0, 1) for b in (-1, 0, 1)])
+        sy = np.concatenate([d["y"] + 2 * b for a in (-1, 0, 1) for b in (-1, 0, 1)])
+        st, sc = np.tile(d["tau"], 9), np.tile(d["cat"], 9)
+        ds = local_direct(meta, sx, sy, st, d["x"], d["y"], False, sc, d["cat"])
+        dt = local_direct(meta, sx, sy, st, d["tx"], d["ty"], False, sc, d["tcat"])
+    t1 = time.time()
+    out = dict(
+        meta=json.dumps(meta),
+        inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),
+        bbox_used=np.array(E.bbox, dtype=np.float64),
+        levels=np.int64(getattr(getattr(E, "tree", None), "levels", 0)),
+        src_idx=np.arange(n), src_val=out_s[:, 0], tgt_idx=np.arange(m), tgt_val=out_t[:, 0],
+        direct_src=ds, direct_tgt=dt,
+    )
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"{name}: ref {t1 - t0:.1f}s  vs direct src {rel(out_s[:, 0], ds):.2e} "
+          f"tgt {rel(out_t[:, 0], dt):.2e}", flush=True)
+
+
 def run_stokes_case(name, meta, ref):
     """The reference's Stokes FMM (flexmm/kifmm2d/vector/stokes_fmm.py:592-858):
     src_val / tgt_val are [3, n] rows (u, v, p)."""
@@ -451,6 +556,8 @@ def main():
             run_stokes_case(name, meta, ref)
         elif meta.get("dipole"):
             run_dipole_case(name, meta, ref)
+        elif meta.get("local"):
+            run_local_case(name, meta, ref)
         else:
             (run_gradient_case if meta.get("gradient") else run_case)(name, meta, ref)
 

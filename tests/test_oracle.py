@@ -65,7 +65,8 @@ def test_oracle_results_match_reference(case):
 
 def test_golden_inputs_regenerate_bitwise():
     import make_golden
-    for case in golden_cases() + golden_cases(gradient=True) + golden_cases(stokes=True):
+    for case in (golden_cases() + golden_cases(gradient=True) + golden_cases(stokes=True)
+                 + golden_cases(local=True)):
         g = load_golden(case)
         d = golden_inputs(g["meta"])
         assert make_golden.sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]) == str(g["inputs_sha"]), case
