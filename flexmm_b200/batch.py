@@ -75,12 +75,16 @@ class StokesBatch:
             with ThreadPoolExecutor(max_workers=len(self.streams)) as ex:
                 for k, r in zip(range(1, n), ex.map(lambda k: build(k, boxes[k], pre), range(1, n))):
                     fmms[k] = r
+            pre0 = pre   # the widths every later box was snapped to
             for k in range(1, n):
                 F = fmms[k][0]
-                F.input_precomputations = pre   # every width met so far
+                F.input_precomputations = pre   # every width met so far: none formed twice
                 with torch.cuda.stream(self._stream(k)):
                     F.precompute()
                 pre = F.precomputations  # operators shared by width across problems
+                # the operators this problem's box was snapped with (the same
+                # problem built alone with them gets the same box and tree)
+                F.input_precomputations = pre0
         helper = KI_Helper()
         for k in range(n):
             F, xd, yd = fmms[k]
