@@ -98,6 +98,7 @@ SIGNATURES = [
                                              ctypes.c_double, _dp, _vp, ctypes.POINTER(_vp)]),
     ("fmm_local_evaluate", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp,
                                           _vp, _vp, _vp]),
+    ("fmm_build_expansions2_dipole", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("fmm_plan_destroy", ctypes.c_int, [_vp]),
     ("fmm_plan_drop_expansions", ctypes.c_int, [_vp]),
     ("fmm_plan_move_sources", ctypes.c_int, [_vp, _vp, _vp, _vp]),

@@ -255,6 +255,8 @@ struct fmm_plan {
   // `ready` is recorded once a single-column KIFMM build has sorted its charges
   DevBuf<double> dvx, dvy;  // dipole sources: strength * normal, sorted (see PassArgs)
   bool has_dipoles = false;
+  DevBuf<double> st_dip;    // Stokes stresslets: sigma_x, sigma_y, n_x, n_y, sorted ([4][n])
+  bool has_st_dipoles = false;
   cudaStream_t side = nullptr;  // from the device's pool, not owned
   cudaEvent_t ev_ready = nullptr, ev_near = nullptr, ev_far = nullptr;
   bool ready_recorded = false;
@@ -790,6 +792,14 @@ static StokesArgs stokes_args(fmm_plan *p, cudaStream_t) {
   a.th = &p->th;
   for (int m = 0; m < p->th.L && m < FMM_MAX_LEVELS_DEV; ++m)
     if (p->bound[m] >= 0) a.lev[m] = p->ops->levels[p->bound[m]]->st_lev;
+  if (p->has_st_dipoles) {
+    const size_t n = size_t(p->th.n_points);
+    double *d = p->st_dip.get();
+    a.sgx = d;
+    a.sgy = d + n;
+    a.dnx = d + 2 * n;
+    a.dny = d + 3 * n;
+  }
   return a;
 }
 
@@ -808,13 +818,37 @@ static BBArgs bb_args(fmm_plan *p, cudaStream_t) {
   return b;
 }
 
+static void build_stokes(fmm_plan *p, const double *fx, const double *fy, const double *sgx,
+                         const double *sgy, const double *nx, const double *ny, void *stream);
+
 int fmm_build_expansions2(fmm_plan *p, const double *fx, const double *fy, void *stream) {
+  return guarded([&] { build_stokes(p, fx, fy, nullptr, nullptr, nullptr, nullptr, stream); });
+}
+
+int fmm_build_expansions2_dipole(fmm_plan *p, const double *fx, const double *fy,
+                                 const double *sigma_x, const double *sigma_y, const double *dip_nx,
+                                 const double *dip_ny, void *stream) {
   return guarded([&] {
+    FMMB_CHECK(sigma_x && sigma_y && dip_nx && dip_ny, ERR_INVALID_ARGUMENT, "NULL argument");
+    build_stokes(p, fx, fy, sigma_x, sigma_y, dip_nx, dip_ny, stream);
+  });
+}
+
+static void build_stokes(fmm_plan *p, const double *fx, const double *fy, const double *sgx,
+                         const double *sgy, const double *nx, const double *ny, void *stream) {
+  {
     tree_ready(p);
     FMMB_CHECK(p && fx && fy, ERR_INVALID_ARGUMENT, "NULL argument");
     FMMB_CHECK(p->ops->method == METHOD_STOKES, ERR_INVALID_ARGUMENT,
                "fmm_build_expansions2 takes Stokes plans (two force components)");
     cudaStream_t s = (cudaStream_t)stream;
+    p->has_st_dipoles = sgx != nullptr;
+    if (sgx) {  // stresslet strengths and normals in the tree's order
+      const int64_t n = p->th.n_points;
+      p->st_dip.alloc(4 * size_t(n), s);
+      const double *src[4] = {sgx, sgy, nx, ny};
+      for (int c = 0; c < 4; ++c) gather_sorted(src[c], p->td.ordv.get(), n, p->st_dip.get() + c * n, s);
+    }
     const TreeHost &th = p->th;
     for (int m = 2; m < th.L; ++m)
       FMMB_CHECK(p->bound[m] >= 0, ERR_NOT_READY, "operators not bound for every level >= 2");
@@ -832,7 +866,7 @@ int fmm_build_expansions2(fmm_plan *p, const double *fx, const double *fy, void 
     run_stokes_upward(a, p->tau_s.get(), p->tau2_s.get(), p->partial.get(), p->mult.get(), s);
     run_stokes_downward(a, p->mult.get(), p->ple.get(), p->loc.get(), s);
     p->have_expansions = true;
-  });
+  }
 }
 
 int fmm_build_expansions_multi(fmm_plan *p, const double *tau, int n_rhs, int64_t ld_tau,
@@ -1269,6 +1303,8 @@ int fmm_plan_drop_expansions(fmm_plan *p) {
     p->dvx.release();
     p->dvy.release();
     p->has_dipoles = false;
+    p->st_dip.release();
+    p->has_st_dipoles = false;
     p->have_expansions = false;
     p->ready_recorded = false;
   });

@@ -86,6 +86,10 @@ struct StokesArgs {
   int neq, np;
   const TreeDev *td;
   const TreeHost *th;
+  // double-layer (stresslet) sources: strengths (sigma) and normals, sorted;
+  // null when the sources carry forces only (build_expansions_dipole,
+  // stokes_fmm.py:738-826)
+  const double *sgx = nullptr, *sgy = nullptr, *dnx = nullptr, *dny = nullptr;
   struct Level {
     const double *lx, *ly;
     const double *e2c_u, *e2c_vhs, *c2e_u, *c2e_vhs, *m2mc, *l2lc, *m2l_cat;

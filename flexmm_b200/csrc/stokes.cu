@@ -48,8 +48,26 @@ __device__ __forceinline__ void stokeslet(double dx, double dy, double fx, doubl
   p += (fx * dx + fy * dy) * id2;
 }
 
+// one stresslet (double-layer) pair, unscaled like stokeslet: strength
+// (sgx, sgy) along the normal (nx, ny), d = (dx, dy) target - source
+// (kernel_apply_single_with_dipole, stokes_fmm.py:187-235):
+//   u_a += 4 (d.n) d_a d_b / r^4 sigma_b,
+//   p   += 2 (-n_b / r^2 + 2 d_b (d.n) / r^4) sigma_b
+__device__ __forceinline__ void stresslet(double dx, double dy, double sgx, double sgy, double nx,
+                                          double ny, double &u, double &v, double &p) {
+  const double id2 = 1.0 / (dx * dx + dy * dy);
+  const double dn = dx * nx + dy * ny;
+  const double c = 4.0 * dn * id2 * id2;
+  const double gxy = c * dx * dy;
+  u += c * dx * dx * sgx + gxy * sgy;
+  v += gxy * sgx + c * dy * dy * sgy;
+  p += 2.0 * (-nx * id2 + 0.5 * dx * c) * sgx + 2.0 * (-ny * id2 + 0.5 * dy * c) * sgy;
+}
+
 // S2M: velocities at the large circle's points from the box's sources; one
-// warp per S2M node, lane k owns check points k and k + 32
+// warp per S2M node, lane k owns check points k and k + 32.  DIP: the
+// sources also carry stresslets (upwards_pass_dipole, stokes_fmm.py:294-322).
+template <bool DIP>
 __global__ void __launch_bounds__(128) k_stokes_s2m(int neq, int np, int L, StokesCircles cir,
                                                     const int *__restrict__ off,
                                                     const int *__restrict__ uplist,
@@ -62,8 +80,14 @@ __global__ void __launch_bounds__(128) k_stokes_s2m(int neq, int np, int L, Stok
                                                     const double *__restrict__ sy,
                                                     const double *__restrict__ fx,
                                                     const double *__restrict__ fy,
-                                                    double *__restrict__ partial) {
+                                                    double *__restrict__ partial,
+                                                    const double *__restrict__ sgx,
+                                                    const double *__restrict__ sgy,
+                                                    const double *__restrict__ dnx,
+                                                    const double *__restrict__ dny) {
   __shared__ double qx[4][32], qy[4][32], qf[4][32], qg[4][32];
+  __shared__ double qs[DIP ? 4 : 1][32], qt[DIP ? 4 : 1][32], qn[DIP ? 4 : 1][32],
+      qm[DIP ? 4 : 1][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_up = *n_up_ptr;
   for (int i = blockIdx.x * 4 + warp; i < n_up; i += gridDim.x * 4) {
@@ -85,14 +109,24 @@ __global__ void __launch_bounds__(128) k_stokes_s2m(int neq, int np, int L, Stok
         qy[warp][lane] = sy[j0 + lane] - cy;
         qf[warp][lane] = fx[j0 + lane];
         qg[warp][lane] = fy[j0 + lane];
+        if constexpr (DIP) {
+          qs[warp][lane] = sgx[j0 + lane];
+          qt[warp][lane] = sgy[j0 + lane];
+          qn[warp][lane] = dnx[j0 + lane];
+          qm[warp][lane] = dny[j0 + lane];
+        }
       }
       __syncwarp();
 #pragma unroll
       for (int h = 0; h < 2; ++h)
         if (lane + 32 * h < neq)
-          for (int j = 0; j < nj; ++j)
-            stokeslet(ex[h] - qx[warp][j], ey[h] - qy[warp][j], qf[warp][j], qg[warp][j], u[h],
-                      v[h], p[h]);
+          for (int j = 0; j < nj; ++j) {
+            const double dx = ex[h] - qx[warp][j], dy = ey[h] - qy[warp][j];
+            stokeslet(dx, dy, qf[warp][j], qg[warp][j], u[h], v[h], p[h]);
+            if constexpr (DIP)
+              stresslet(dx, dy, qs[warp][j], qt[warp][j], qn[warp][j], qm[warp][j], u[h], v[h],
+                        p[h]);
+          }
       __syncwarp();
     }
     const double us = 0.25 / M_PI;
@@ -108,7 +142,10 @@ __global__ void __launch_bounds__(128) k_stokes_s2m(int neq, int np, int L, Stok
 }
 
 // Evaluation: (u, v, p) rows of out (stride ld_out).  One work item = (leaf,
-// up to 128 of its targets); G threads share a target.
+// up to 128 of its targets); G threads share a target.  DIP: the near field
+// adds the sources' stresslets (neighbor_evaluation_dipole,
+// stokes_fmm.py:399-441); the far field is the same local expansion.
+template <bool DIP>
 __global__ void __launch_bounds__(TCH_ST) k_stokes_evaluate(
     int neq, int np, StokesCircles cir, const int4 *__restrict__ items,
     const int *__restrict__ n_items_ptr, const int *__restrict__ coll, const int *__restrict__ bot,
@@ -116,8 +153,12 @@ __global__ void __launch_bounds__(TCH_ST) k_stokes_evaluate(
     const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ fx,
     const double *__restrict__ fy, const double *__restrict__ loc, const double *__restrict__ txs,
     const double *__restrict__ tys, const int *__restrict__ tperm, int check,
-    double *__restrict__ out, int64_t ld_out) {
-  __shared__ double ssx[SMAX_ST], ssy[SMAX_ST], sfx[SMAX_ST], sfy[SMAX_ST];
+    double *__restrict__ out, int64_t ld_out, const double *__restrict__ sgx,
+    const double *__restrict__ sgy, const double *__restrict__ dnx,
+    const double *__restrict__ dny) {
+  constexpr int SM = DIP ? SMAX_ST / 2 : SMAX_ST;  // 48 KB of static shared memory at most
+  __shared__ double ssx[SM], ssy[SM], sfx[SM], sfy[SM];
+  __shared__ double ssg[DIP ? SM : 1], stg[DIP ? SM : 1], snx[DIP ? SM : 1], sny[DIP ? SM : 1];
   __shared__ int rb[9], rs[10];
   __shared__ double red[3][TCH_ST / 32];
   const int n_items = *n_items_ptr;
@@ -147,8 +188,8 @@ __global__ void __launch_bounds__(TCH_ST) k_stokes_evaluate(
     }
     __syncthreads();
     const int ns = rs[9];
-    for (int base = 0; base < ns; base += SMAX_ST) {
-      const int nb = min(SMAX_ST, ns - base);
+    for (int base = 0; base < ns; base += SM) {
+      const int nb = min(SM, ns - base);
       for (int i = threadIdx.x; i < nb; i += TCH_ST) {
         const int idx = base + i;
         int c = 0;
@@ -158,12 +199,20 @@ __global__ void __launch_bounds__(TCH_ST) k_stokes_evaluate(
         ssy[i] = sy[j];
         sfx[i] = fx[j];
         sfy[i] = fy[j];
+        if constexpr (DIP) {
+          ssg[i] = sgx[j];
+          stg[i] = sgy[j];
+          snx[i] = dnx[j];
+          sny[i] = dny[j];
+        }
       }
       __syncthreads();
       if (valid)
         for (int j = sub; j < nb; j += G) {
           const double dx = x - ssx[j], dy = y - ssy[j];
-          if (!(check && dx == 0.0 && dy == 0.0)) stokeslet(dx, dy, sfx[j], sfy[j], u, v, p);
+          if (check && dx == 0.0 && dy == 0.0) continue;
+          stokeslet(dx, dy, sfx[j], sfy[j], u, v, p);
+          if constexpr (DIP) stresslet(dx, dy, ssg[j], stg[j], snx[j], sny[j], u, v, p);
         }
       __syncthreads();
     }
@@ -213,10 +262,12 @@ void run_stokes_upward(const StokesArgs &a, const double *fx, const double *fy, 
   FMMB_CHECK(th.L <= FMM_MAX_LEVELS_DEV, ERR_INVALID_ARGUMENT, "too many levels");
   const int np = a.np;
   PhaseTimer timer(PH_UPWARD, s);
-  k_stokes_s2m<<<work_grid(th.n_total(), 8), 128, 0, s>>>(a.neq, np, th.L, circles(a), td.dev_off.get(),
-                                       td.uplist.get(), td.n_up.get(), td.bot.get(), td.top.get(),
-                                       td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), fx, fy,
-                                       partial);
+  auto s2m = a.sgx ? k_stokes_s2m<true> : k_stokes_s2m<false>;
+  s2m<<<work_grid(th.n_total(), 8), 128, 0, s>>>(a.neq, np, th.L, circles(a), td.dev_off.get(),
+                                                 td.uplist.get(), td.n_up.get(), td.bot.get(),
+                                                 td.top.get(), td.xmid.get(), td.ymid.get(),
+                                                 td.sx.get(), td.sy.get(), fx, fy, partial, a.sgx,
+                                                 a.sgy, a.dnx, a.dny);
   FMMB_CUDA(cudaGetLastError());
   int max_rows = 0;
   for (int m = 2; m < th.L; ++m) max_rows = std::max(max_rows, th.off[m + 1] - th.off[m]);
@@ -285,10 +336,11 @@ void run_stokes_evaluate(const StokesArgs &a, const double *fx, const double *fy
   EvalItems it;
   eval_items(pa, tkeys, m, it, s);
   PhaseTimer timer(PH_EVAL, s);
-  k_stokes_evaluate<<<work_grid(a.th->n_total() + m / TCH_ST + 1, 8), TCH_ST, 0, s>>>(
+  auto ev = a.sgx ? k_stokes_evaluate<true> : k_stokes_evaluate<false>;
+  ev<<<work_grid(a.th->n_total() + m / TCH_ST + 1, 8), TCH_ST, 0, s>>>(
       a.neq, a.np, circles(a), it.items.get(), it.n_items.get(), td.coll.get(), td.bot.get(),
       td.top.get(), td.xmid.get(), td.ymid.get(), td.sx.get(), td.sy.get(), fx, fy, loc, txs, tys,
-      tperm, check, out, ld_out);
+      tperm, check, out, ld_out, a.sgx, a.sgy, a.dnx, a.dny);
   FMMB_CUDA(cudaGetLastError());
 }
 

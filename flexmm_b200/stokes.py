@@ -296,6 +296,24 @@ class FMM:
                   ctypes.c_void_p(fy.data_ptr()), _stream())
         self._tau = (fx, fy)
 
+    def build_expansions_dipole(self, taux, tauy, sigmax, sigmay, dipx, dipy):
+        """Forces plus stresslets (double layer of strength (sigmax, sigmay)
+        along the normals (dipx, dipy)): build_expansions_dipole,
+        stokes_fmm.py:738-826.  Later evaluations include the stresslets."""
+        if self.precomputations is None:
+            self.precompute()
+        arrs = [_device_f64(a)[0] for a in (taux, tauy, sigmax, sigmay, dipx, dipy)]
+        if any(a.numel() != self.N for a in arrs):
+            raise ValueError(f"every array must have {self.N} entries")
+        _lib.call("fmm_build_expansions2_dipole", self._plan,
+                  *[ctypes.c_void_p(a.data_ptr()) for a in arrs], _stream())
+        self._tau = tuple(arrs)
+
+    def evaluate_to_points_dipole(self, x, y, check_self=False):
+        """(u, v, p) at (x, y) after build_expansions_dipole
+        (evaluate_to_points_dipole, stokes_fmm.py:844-858)."""
+        return self.evaluate_to_points(x, y, check_self)
+
     def evaluate_to_points(self, x, y, check_self=False):
         """(u, v, p) at (x, y); ``check_self`` skips coincident sources."""
         torch = _torch()

@@ -97,6 +97,15 @@ int fmm_stokes_ops_add(fmm_ops *ops, const fmm_stokes_level_ops *lv, int *level_
 /* FMM.build_expansions(taux, tauy) of the Stokes FMM (stokes_fmm.py:642-735):
  * device forces in the caller's source order. */
 int fmm_build_expansions2(fmm_plan *plan, const double *fx, const double *fy, void *stream);
+/* The Stokes FMM's build_expansions_dipole(taux, tauy, sigmax, sigmay, dipx,
+ * dipy) (stokes_fmm.py:738-826): forces plus stresslets of strength
+ * (sigma_x, sigma_y) along the normals (dip_nx, dip_ny), device arrays in the
+ * caller's source order.  Its evaluations (FMM_EVAL_STOKES) add the
+ * stresslets' near field (evaluate_to_points_dipole, stokes_fmm.py:844-858);
+ * the expansions carry both. */
+int fmm_build_expansions2_dipole(fmm_plan *plan, const double *fx, const double *fy,
+                                 const double *sigma_x, const double *sigma_y,
+                                 const double *dip_nx, const double *dip_ny, void *stream);
 
 /* Kernel ids: 0 Laplace -log(r^2)/(4 pi) (examples/kifmm_laplace.py:24-29);
  * 1 modified Helmholtz K0(k r)/(2 pi), kparams[0] = k

@@ -111,3 +111,37 @@ void oracle_direct_laplace_dipole(const double *sx, const double *sy, const doub
         out[j] = acc;
     }
 }
+
+/* Stokeslets plus stresslets: the reference's
+ * kernel_apply_single(_check)_with_dipole (flexmm/kifmm2d/vector/stokes_fmm.py:
+ * 128-235) summed over all sources: forces (fx, fy), double-layer strengths
+ * (sx_, sy_) along the normals (nx, ny); rows (u, v, p). */
+void oracle_direct_stokes_dipole(const double *sx, const double *sy, const double *fx,
+                                 const double *fy, const double *gx, const double *gy,
+                                 const double *nx, const double *ny, int64_t ns,
+                                 const double *tx, const double *ty, int64_t nt, int check,
+                                 double *out)
+{
+    const double us = 0.25 / M_PI, ps = 0.5 / M_PI;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t j = 0; j < nt; ++j) {
+        double u = 0.0, v = 0.0, p = 0.0;
+        const double x = tx[j], y = ty[j];
+        for (int64_t i = 0; i < ns; ++i) {
+            double dx = x - sx[i], dy = y - sy[i];
+            if (check && dx == 0.0 && dy == 0.0) continue;
+            double id2 = 1.0 / (dx * dx + dy * dy);
+            double logid = 0.5 * log(id2);
+            double dxdy = dx * dy * id2;
+            double dn = dx * nx[i] + dy * ny[i];
+            double c = 4.0 * dn * id2 * id2;
+            u += (logid + dx * dx * id2) * fx[i] + dxdy * fy[i] + c * dx * dx * gx[i] + c * dx * dy * gy[i];
+            v += dxdy * fx[i] + (logid + dy * dy * id2) * fy[i] + c * dx * dy * gx[i] + c * dy * dy * gy[i];
+            p += (fx[i] * dx + fy[i] * dy) * id2;
+            p += 2.0 * (-nx[i] * id2 + 0.5 * dx * c) * gx[i] + 2.0 * (-ny[i] * id2 + 0.5 * dy * c) * gy[i];
+        }
+        out[j] = u * us;
+        out[nt + j] = v * us;
+        out[2 * nt + j] = p * ps;
+    }
+}

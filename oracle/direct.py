@@ -32,6 +32,9 @@ def _load():
         dd = _lib.oracle_direct_laplace_dipole
         dd.argtypes = [dp, dp, dp, dp, dp, dp, ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
         dd.restype = None
+        sd = _lib.oracle_direct_stokes_dipole
+        sd.argtypes = [dp] * 8 + [ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
+        sd.restype = None
         h = _lib.oracle_direct_stokes
         h.argtypes = [dp, dp, dp, dp, ctypes.c_int64, dp, dp, ctypes.c_int64, ctypes.c_int, dp]
         h.restype = None
@@ -154,4 +157,15 @@ def direct_stokes(sx, sy, fx, fy, tx, ty, check):
     out = np.empty((3, tx.size))
     lib.oracle_direct_stokes(_p(sx), _p(sy), _p(fx), _p(fy), sx.size, _p(tx), _p(ty), tx.size,
                              1 if check else 0, _p(out))
+    return out
+
+
+def direct_stokes_dipole(sx, sy, fx, fy, gx, gy, nx, ny, tx, ty, check):
+    """FP64 direct sum of Stokeslets plus stresslets -> [3, nt] rows (u, v, p)
+    (flexmm/kifmm2d/vector/stokes_fmm.py:128-235)."""
+    lib = _load()
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, fx, fy, gx, gy, nx, ny, tx, ty)]
+    out = np.empty((3, a[8].size))
+    lib.oracle_direct_stokes_dipole(*[_p(v) for v in a[:8]], a[0].size, _p(a[8]), _p(a[9]),
+                                    a[8].size, 1 if check else 0, _p(out))
     return out

@@ -17,7 +17,7 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
-def golden_cases(gradient=False, stokes=False, dipole=False, local=False):
+def golden_cases(gradient=False, stokes=False, dipole=False, local=False, stresslet=False):
     """Fixture names: potential cases; (gradient=True) the grad_* cases whose
     results are [3, n] rows (u, du/dx, du/dy); (stokes=True) the stokes_*
     cases, rows (u, v, p); (dipole=True) the dip_* cases (single plus
@@ -29,8 +29,10 @@ def golden_cases(gradient=False, stokes=False, dipole=False, local=False):
         return [n for n in names if n.startswith("dip_")]
     if local:   # the local evaluators (near field only)
         return [n for n in names if n.startswith("local_")]
+    if stresslet:  # the Stokes FMM with stresslets (build_expansions_dipole)
+        return [n for n in names if n.startswith("sdip_")]
     return [n for n in names if n.startswith("grad_") == gradient
-            and not n.startswith(("stokes_", "dip_", "local_"))]
+            and not n.startswith(("stokes_", "dip_", "local_", "sdip_"))]
 
 
 def load_golden(name):

@@ -91,6 +91,11 @@ def case_inputs(meta):
         d["bbox"] = None
     if meta.get("method") == "stokes":  # second force component
         d["tau2"] = np.random.default_rng(meta["seed"] + 1000).standard_normal(d["x"].size)
+    if meta.get("stresslet"):  # double-layer strengths and unit normals of the Stokes FMM
+        r4 = np.random.default_rng(meta["seed"] + 4000)
+        d["sgx"], d["sgy"] = r4.standard_normal(d["x"].size), r4.standard_normal(d["x"].size)
+        th = r4.uniform(0, 2 * np.pi, d["x"].size)
+        d["nx"], d["ny"] = np.cos(th), np.sin(th)
     if meta.get("local") in ("category", "periodic"):  # source and target categories
         r3 = np.random.default_rng(meta["seed"] + 3000)
         d["cat"] = r3.integers(0, meta["ncat"], d["x"].size)
@@ -154,6 +159,10 @@ CASES = {
                                      local="category", delta=2.0 ** -5, ncat=7), True),
     "local_periodic_10k": (dict(recipe="uniform", seed=36, n=10000, n_grid=50, ncut=20,
                                 local="periodic", delta=2.0 ** -4, ncat=5), True),
+    "sdip_uniform_3k_q16": (dict(recipe="uniform", seed=37, n=3000, n_grid=41, ncut=16, neq=16,
+                                 method="stokes", stresslet=True), True),
+    "sdip_clustered_20k_q32": (dict(recipe="clustered", seed=38, n=20000, n_grid=64, ncut=64,
+                                    neq=32, method="stokes", stresslet=True), True),
     "uniform_100k_q32": (dict(recipe="uniform", seed=0, n=100000, n_grid=316, ncut=64, neq=32,
                               sample=2000), False),
     "clustered_1M_q60": (dict(recipe="clustered", seed=1, n=1000000, n_grid=1000, ncut=64, neq=60,
@@ -494,12 +503,22 @@ def run_stokes_case(name, meta, ref):
     t0 = time.time()
     F = FMM(d["x"], d["y"], meta["neq"], meta["ncut"], bbox=d["bbox"])
     F.precompute()
-    F.build_expansions(d["tau"], d["tau2"])
-    us = np.array(F.evaluate_to_points(d["x"], d["y"], True))
-    ut = np.array(F.evaluate_to_points(d["tx"], d["ty"], False))
-    t1 = time.time()
-    ds = direct_stokes(d["x"], d["y"], d["tau"], d["tau2"], d["x"], d["y"], True)
-    dt = direct_stokes(d["x"], d["y"], d["tau"], d["tau2"], d["tx"], d["ty"], False)
+    if meta.get("stresslet"):  # build_expansions_dipole / evaluate_to_points_dipole
+        from oracle.direct import direct_stokes_dipole
+        F.build_expansions_dipole(d["tau"], d["tau2"], d["sgx"], d["sgy"], d["nx"], d["ny"])
+        us = np.array(F.evaluate_to_points_dipole(d["x"], d["y"], True))
+        ut = np.array(F.evaluate_to_points_dipole(d["tx"], d["ty"], False))
+        t1 = time.time()
+        srcs = (d["x"], d["y"], d["tau"], d["tau2"], d["sgx"], d["sgy"], d["nx"], d["ny"])
+        ds = direct_stokes_dipole(*srcs, d["x"], d["y"], True)
+        dt = direct_stokes_dipole(*srcs, d["tx"], d["ty"], False)
+    else:
+        F.build_expansions(d["tau"], d["tau2"])
+        us = np.array(F.evaluate_to_points(d["x"], d["y"], True))
+        ut = np.array(F.evaluate_to_points(d["tx"], d["ty"], False))
+        t1 = time.time()
+        ds = direct_stokes(d["x"], d["y"], d["tau"], d["tau2"], d["x"], d["y"], True)
+        dt = direct_stokes(d["x"], d["y"], d["tau"], d["tau2"], d["tx"], d["ty"], False)
     out = dict(
         meta=json.dumps(meta),
         inputs_sha=sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]),

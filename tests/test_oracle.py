@@ -70,6 +70,10 @@ def test_golden_inputs_regenerate_bitwise():
         g = load_golden(case)
         d = golden_inputs(g["meta"])
         assert make_golden.sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]) == str(g["inputs_sha"]), case
+    for case in golden_cases(stresslet=True):
+        g = load_golden(case)
+        d = golden_inputs(g["meta"])
+        assert make_golden.sha(d["x"], d["y"], d["tau"], d["tx"], d["ty"]) == str(g["inputs_sha"]), case
     for case in golden_cases(dipole=True):
         g = load_golden(case)
         d = golden_inputs(g["meta"])
