@@ -14,9 +14,9 @@ sm_100a CUDA behind the C ABI in ``include/flexmm_b200.h``); build it with
 from .bbfmm import BB_FMM, BB_Helper
 from .helpers import KI_Helper
 from .kernels import Kernel, Laplace, resolve
-from .kifmm import KI_FMM, direct_evaluation, enable_timing, read_timing
+from .kifmm import KI_FMM, direct_evaluation, enable_timing, read_timing, set_split_evaluation
 
 Laplace_Eval = Laplace()
 
 __all__ = ["KI_FMM", "KI_Helper", "BB_FMM", "BB_Helper", "Kernel", "Laplace", "Laplace_Eval", "resolve",
-           "direct_evaluation", "enable_timing", "read_timing"]
+           "direct_evaluation", "enable_timing", "read_timing", "set_split_evaluation"]

@@ -108,6 +108,7 @@ SIGNATURES = [
                                   ctypes.c_int64, ctypes.c_int, _vp, _vp]),
     ("fmm_diag_log2", ctypes.c_int, [_vp, ctypes.c_int64, _vp, _vp, _vp]),
     ("fmm_timing_enable", ctypes.c_int, [ctypes.c_int]),
+    ("fmm_set_split_evaluation", ctypes.c_int, [ctypes.c_int]),
     ("fmm_timing_read", ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int64)]),
     ("fmm_evaluate_noalloc", ctypes.c_int,
      [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, _vp, _vp]),

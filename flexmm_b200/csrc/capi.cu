@@ -5,6 +5,7 @@
 #include <cmath>
 
 #include <map>
+#include <atomic>
 #include <mutex>
 
 #include <memory>
@@ -280,9 +281,10 @@ cudaStream_t side_stream() {
   FMMB_CUDA(cudaGetDevice(&dev));
   FMMB_CHECK(dev >= 0 && dev < SIDE_MAX_DEVICES, ERR_UNSUPPORTED, "device ordinal too large");
   std::lock_guard<std::mutex> g(g_side_mu);
-  const int k = g_side_next[dev]++ % SIDE_STREAMS;
-  if (!g_side[dev][k]) FMMB_CUDA(cudaStreamCreateWithFlags(&g_side[dev][k], cudaStreamNonBlocking));
-  return g_side[dev][k];
+  if (!g_side[dev][0])  // all at once: no plan after the first pays for a stream
+    for (int k = 0; k < SIDE_STREAMS; ++k)
+      FMMB_CUDA(cudaStreamCreateWithFlags(&g_side[dev][k], cudaStreamNonBlocking));
+  return g_side[dev][g_side_next[dev]++ % SIDE_STREAMS];
 }
 
 // the plan's split-evaluation events (created on first use) and side stream
@@ -1189,11 +1191,16 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
 // more beside the near field than the near field saves), so it evaluates in
 // one pass unless FLEXMM_B200_SPLIT_EVAL=1.  FLEXMM_B200_SPLIT_EVAL=0 turns
 // the split off for both forms.
+std::atomic<int> g_split_mode{-2};  // -2: not yet read from the environment
+
 bool split_enabled(int precision) {
-  static const int mode = [] {
+  int mode = g_split_mode.load(std::memory_order_relaxed);
+  if (mode == -2) {
     const char *e = getenv("FLEXMM_B200_SPLIT_EVAL");
-    return e ? (e[0] == '0' ? 0 : 1) : -1;
-  }();
+    int env = e ? (e[0] == '0' ? 0 : 1) : -1;
+    g_split_mode.compare_exchange_strong(mode, env);
+    mode = g_split_mode.load(std::memory_order_relaxed);
+  }
   return mode < 0 ? precision == PREC_FP64 : mode == 1;
 }
 
@@ -1378,6 +1385,17 @@ int fmm_diag_log2(const double *x, int64_t n, double *out_table, double *out_lib
     if (n == 0) return;
     FMMB_CHECK(x && out_table && out_library, ERR_INVALID_ARGUMENT, "NULL argument");
     run_diag_log2(x, n, out_table, out_library, (cudaStream_t)stream);
+  });
+}
+
+int fmm_set_split_evaluation(int mode) {
+  return guarded([&] {
+    FMMB_CHECK(mode >= -1 && mode <= 1, ERR_INVALID_ARGUMENT, "mode must be -1, 0 or 1");
+    if (mode == -1) {
+      const char *e = getenv("FLEXMM_B200_SPLIT_EVAL");
+      mode = e ? (e[0] == '0' ? 0 : 1) : -1;
+    }
+    g_split_mode.store(mode);
   });
 }
 

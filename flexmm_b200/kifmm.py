@@ -450,6 +450,14 @@ def direct_evaluation(kernel, sx, sy, tau, tx, ty, check=False, **kernel_params)
     return _as_kind(out, kind, np.shape(tx))
 
 
+def set_split_evaluation(mode=None):
+    """Own-source evaluation split into a near-field kernel beside the level
+    passes and a far-field kernel after them: True / False, or None for the
+    default (on for the FP64 form, off for the mixed form)."""
+    _lib.load()
+    _lib.call("fmm_set_split_evaluation", -1 if mode is None else int(bool(mode)))
+
+
 def enable_timing(on=True):
     """Per-kernel CUDA-event timing inside the library (off by default)."""
     _lib.load()

@@ -289,63 +289,31 @@ def test_radial_table_kernel_device_matches_host_table(built_lib):
     np.testing.assert_allclose(got[near], struve_gf(r[near]), rtol=5e-12)
 
 
-_UNSPLIT_SCRIPT = r"""
-import sys, numpy as np
-sys.path.insert(0, {repo!r})
-from flexmm_b200 import KI_FMM, KI_Helper, workloads
-import torch
-d = workloads.clustered(n=120_000, n_grid=10, seed=44)
-x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
-out = {{}}
-for prec, neq in (("fp64", 40), ("mixed", 24)):
-    F = KI_FMM(x, y, "Laplace_Eval", 64, neq, bbox=d["bbox"], helper=KI_Helper(), precision=prec)
-    F.build_expansions(d["tau"])
-    out[prec] = F.source_evaluation(x, y).cpu().numpy()
-np.savez({path!r}, **out)
-"""
-
-
-def test_split_source_evaluation_equals_one_pass(built_lib, tmp_path):
-    import os
-    if os.environ.get("FLEXMM_B200_SPLIT_EVAL") != "1":   # the mode is read once per process
-        import subprocess
-        import sys
-        env = dict(os.environ, FLEXMM_B200_SPLIT_EVAL="1")
-        r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", __file__ + "::"
-                            "test_split_source_evaluation_equals_one_pass"], env=env, timeout=900)
-        assert r.returncode == 0
-        return
-    _split_vs_one_pass(tmp_path)
-
-
-def _split_vs_one_pass(tmp_path):
+def test_split_source_evaluation_equals_one_pass(built_lib):
     """Own-source evaluation split in two -- the near field on a side stream
     from the moment the charges are sorted, the far field on the plan stream
     adding it -- equals the one-pass evaluation up to the order of the two
-    sums, in both forms (this process: FLEXMM_B200_SPLIT_EVAL=1, split in
-    both forms; the other process: =0, one pass)."""
-    import os
-    import subprocess
-    import sys
+    sums, in both forms (fmm_set_split_evaluation on, then off)."""
     import torch
-    from conftest import REPO
-    from flexmm_b200 import KI_FMM, KI_Helper, workloads
-    path = str(tmp_path / "one_pass.npz")
-    env = dict(os.environ, FLEXMM_B200_SPLIT_EVAL="0")
-    subprocess.run([sys.executable, "-c", _UNSPLIT_SCRIPT.format(repo=REPO, path=path)], env=env,
-                   check=True, timeout=600)
-    ref = np.load(path)
+    from flexmm_b200 import KI_FMM, KI_Helper, set_split_evaluation, workloads
     d = workloads.clustered(n=120_000, n_grid=10, seed=44)
     x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
-    for prec, neq in (("fp64", 40), ("mixed", 24)):
-        F = KI_FMM(x, y, "Laplace_Eval", 64, neq, bbox=d["bbox"], helper=KI_Helper(), precision=prec)
-        F.build_expansions(d["tau"])
-        got = F.source_evaluation(x, y).cpu().numpy()
-        F.status()
-        assert np.isfinite(got).all()
-        # mixed: FP32 partial sums grouped differently (L2T and P2P apart),
-        # ~1e-9 apart, against the form's ~1e-7 error
-        assert rel_l2(got, ref[prec]) < (1e-14 if prec == "fp64" else 2e-8), prec
+    try:
+        for prec, neq in (("fp64", 40), ("mixed", 24)):
+            got = {}
+            for mode in (True, False):
+                set_split_evaluation(mode)
+                F = KI_FMM(x, y, "Laplace_Eval", 64, neq, bbox=d["bbox"], helper=KI_Helper(),
+                           precision=prec)
+                F.build_expansions(d["tau"])
+                got[mode] = F.source_evaluation(x, y).cpu().numpy()
+                F.status()
+                assert np.isfinite(got[mode]).all()
+            # mixed: FP32 partial sums grouped differently (L2T and P2P apart),
+            # ~1e-9 apart, against the form's ~1e-7 error
+            assert rel_l2(got[True], got[False]) < (1e-14 if prec == "fp64" else 2e-8), prec
+    finally:
+        set_split_evaluation(None)
 
 
 @pytest.mark.parametrize("case", golden_cases(dipole=True))
