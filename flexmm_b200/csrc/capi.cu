@@ -929,7 +929,7 @@ int fmm_evaluate_multi(fmm_plan *p, const double *tx, const double *ty, int64_t 
       txs.alloc(m, s);
       tys.alloc(m, s);
       sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
-                  tys.get());
+                  tys.get(), p->td.sort_fail.get());
     }
     run_evaluate_multi(a, p->tau_s.get(), p->th.n_points, p->n_rhs, p->loc.get(),
                        (int64_t)p->th.n_total() * p->ops->np, txs.get(), tys.get(), tkeys.get(),
@@ -1011,7 +1011,7 @@ int fmm_local_evaluate(fmm_plan *p, const double *tau, const double *tx, const d
       txs.alloc(m, s);
       tys.alloc(m, s);
       sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
-                  tys.get());
+                  tys.get(), p->td.sort_fail.get());
     }
     run_local_evaluate(a, p->tau_s.get(), txs.get(), tys.get(), tkeys.get(), tperm.get(), m,
                        check, src_cat ? scat.get() : nullptr, tgt_cat, out, s);
@@ -1168,7 +1168,7 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
     txs.alloc(m, s);
     tys.alloc(m, s);
     sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
-                tys.get());
+                tys.get(), p->td.sort_fail.get());
   }
   if (p->ops->method == METHOD_STOKES)
     run_stokes_evaluate(stokes_args(p, s), p->tau_s.get(), p->tau2_s.get(), p->loc.get(), txs.get(),
@@ -1287,6 +1287,11 @@ int fmm_plan_status(fmm_plan *p) {
       int h = 0;
       FMMB_CUDA(cudaMemcpy(&h, p->err.get(), sizeof(int), cudaMemcpyDeviceToHost));
       FMMB_CHECK(h == 0, ERR_CUDA, "a tensor-core wait ran out of time; results are invalid");
+    }
+    if (p->td.sort_fail.get()) {
+      int h = 0;
+      FMMB_CUDA(cudaMemcpy(&h, p->td.sort_fail.get(), sizeof(int), cudaMemcpyDeviceToHost));
+      FMMB_CHECK(h == 0, ERR_CUDA, "a radix sort's grid barrier wait ran out of time; results are invalid");
     }
   });
 }
@@ -1492,7 +1497,8 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char *base = static_cast<unsigned char *>(noalloc_scratch_for_current_device());
     // carve the scratch
-    const size_t sort_bytes = round256(sort_points_scratch_bytes(m));
+    const int digits = p->th.L > 1 ? p->th.L - 1 : 1;
+    const size_t sort_bytes = round256(sort_points_scratch_bytes(m, digits));
     const size_t scan_bytes = round256(evaluate_scratch_bytes(total));
     size_t at = 0;
     auto carve = [&](size_t bytes) {
@@ -1500,10 +1506,8 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
       at += round256(bytes);
       return q;
     };
-    uint64_t *k0 = (uint64_t *)carve(m * sizeof(uint64_t));
-    uint64_t *k1 = (uint64_t *)carve(m * sizeof(uint64_t));
-    int *i0 = (int *)carve(m * sizeof(int));
-    int *i1 = (int *)carve(m * sizeof(int));
+    uint64_t *tkeys = (uint64_t *)carve(m * sizeof(uint64_t));
+    int *tperm = (int *)carve(m * sizeof(int));
     double *txs = (double *)carve(m * sizeof(double));
     double *tys = (double *)carve(m * sizeof(double));
     int *tb = (int *)carve(total * sizeof(int));
@@ -1525,14 +1529,10 @@ extern "C" int fmm_evaluate_noalloc(fmm_plan *p, const double *tx, const double 
     a.td = &p->td;
     a.th = &p->th;
     a.ops_dev = p->ops_dev.get();
-    const uint64_t *tkeys = nullptr;
-    const int *tperm = nullptr;
     {
       PhaseTimer timer(PH_SORT_TGT, s);
-      sort_points_scratch(tx, ty, m, p->th, k0, k1, i0, i1, sort_tmp, sort_bytes, &tkeys, &tperm,
-                          s);
-      gather_sorted(tx, tperm, m, txs, s);
-      gather_sorted(ty, tperm, m, tys, s);
+      sort_points_scratch(tx, ty, m, p->th, digits, tkeys, tperm, txs, tys, sort_tmp, sort_bytes,
+                          p->td.sort_fail.get(), s);
     }
     run_evaluate_scratch(a, p->tau_s.get(), p->loc.get(), txs, tys, tkeys, tperm, m, check, out, tb,
                          te, nch, choff, items, n_items, scan_tmp, scan_bytes, s);

@@ -37,6 +37,7 @@
 #include <memory>
 #include <mutex>
 
+#include "radix.cuh"
 #include "timing.cuh"
 #include "tree.cuh"
 
@@ -167,50 +168,56 @@ __device__ __forceinline__ uint64_t point_key(double px, double py, double x0, d
   return (spread_bits(uint64_t(fx)) << 1) | spread_bits(uint64_t(fy));
 }
 
-__global__ void k_point_keys(const double *__restrict__ x, const double *__restrict__ y,
-                             int64_t n, double x0, double y0, double w0, double scale,
-                             double margin, uint64_t *__restrict__ keys, int *__restrict__ idx) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    keys[i] = point_key(x[i], y[i], x0, y0, w0, scale, margin);
-    idx[i] = int(i);
-  }
-}
-
 // The top KEY32_DIGITS digits of the key as a 32-bit sort key: a sort on at
 // most that many digits moves 8-byte pairs instead of 12-byte ones.
 constexpr int KEY32_DIGITS = 16;
 
-__global__ void k_point_keys32(const double *__restrict__ x, const double *__restrict__ y,
-                               int64_t n, double x0, double y0, double w0, double scale,
-                               double margin, uint32_t *__restrict__ keys, int *__restrict__ idx) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    keys[i] = uint32_t(point_key(x[i], y[i], x0, y0, w0, scale, margin) >> (2 * (MAXD - KEY32_DIGITS)));
-    idx[i] = int(i);
+// Radix sort source of the point sort: the key of point i computed from its
+// coordinates (its top KEY32_DIGITS digits for 32-bit sort keys), value i.
+template <class K>
+struct SrcPoints {
+  const double *x, *y;
+  double x0, y0, w0, scale, margin;
+  __device__ K key(int i) const {
+    const uint64_t k = point_key(__ldg(x + i), __ldg(y + i), x0, y0, w0, scale, margin);
+    if constexpr (sizeof(K) == 8)
+      return k;
+    else
+      return K(k >> (2 * (MAXD - KEY32_DIGITS)));
   }
-}
+  __device__ int val(int i) const { return int(i); }
+};
 
-// sorted order: the full keys (recomputed from the points) and, if sx is
-// given, the coordinates
-__global__ void k_gather_keyed(const double *__restrict__ x, const double *__restrict__ y,
-                               const int *__restrict__ perm, int64_t n, double x0, double y0,
-                               double w0, double scale, double margin, double *__restrict__ sx,
-                               double *__restrict__ sy, uint64_t *__restrict__ keys) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int j = perm[i];
-    const double px = x[j], py = y[j];
+// Radix sort emit of the point sort: the permutation (sorted -> input), the
+// full 64-bit keys (computed again from the point for 32-bit sort keys) and,
+// if sx is given, the coordinates in sorted order.
+template <class K>
+struct EmitPoints {
+  struct Pre {
+    double x, y;
+  };
+  const double *x, *y;
+  double x0, y0, w0, scale, margin;
+  uint64_t *keys;
+  int *perm;
+  double *sx, *sy;
+  __device__ void init(int i) const { perm[i] = int(i); }
+  __device__ Pre fetch(int v) const { return Pre{__ldg(x + v), __ldg(y + v)}; }
+  __device__ void operator()(int pos, K k, int v, Pre q) const {
+    perm[pos] = v;
     if (sx) {
-      sx[i] = px;
-      sy[i] = py;
+      sx[pos] = q.x;
+      sy[pos] = q.y;
     }
-    keys[i] = point_key(px, py, x0, y0, w0, scale, margin);
+    if constexpr (sizeof(K) == 8)
+      keys[pos] = k;
+    else
+      keys[pos] = point_key(q.x, q.y, x0, y0, w0, scale, margin);
   }
-}
+};
 
 namespace {
-// scale and margin of k_point_keys for a tree box (x0, y0, w0)
+// scale and margin of point_key for a tree box (x0, y0, w0)
 void key_params(double x0, double y0, double w0, double &scale, double &margin) {
   scale = std::ldexp(1.0, MAXD) / w0;
   // A descent midpoint is off its line by at most two roundings per level,
@@ -223,17 +230,6 @@ void key_params(double x0, double y0, double w0, double &scale, double &margin) 
   margin = std::ldexp(1.0, -14) * std::fmax(1.0, big / w0);
 }
 }  // namespace
-
-__global__ void k_gather_xy(const double *__restrict__ x, const double *__restrict__ y,
-                            const int *__restrict__ perm, int64_t n, double *__restrict__ sx,
-                            double *__restrict__ sy) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int j = perm[i];
-    sx[i] = x[j];
-    sy[i] = y[j];
-  }
-}
 
 // --- 3. initially split boxes ------------------------------------------------
 // With keys sorted on their top `sorted_digits` digits, point i starts a box
@@ -727,27 +723,12 @@ uint64_t next_pow2(uint64_t v) {
   return p;
 }
 
-template <class K, class V>
-void radix_sort_pairs(const K *kin, K *kout, const V *vin, V *vout, int64_t n, int begin_bit,
-                      int end_bit, cudaStream_t s) {
-  if (n <= 0) return;
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, begin_bit,
-                                            end_bit, s));
-  DevBuf<uint8_t> tmp;
-  tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, kin, kout, vin, vout, n, begin_bit,
-                                            end_bit, s));
-}
-
+// stable sort of keys on bits [begin_bit, end_bit)
 template <class K>
-void sort_keys(const K *kin, K *kout, int64_t n, int begin_bit, int end_bit, cudaStream_t s) {
-  if (n <= 0) return;
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, kin, kout, n, begin_bit, end_bit, s));
-  DevBuf<uint8_t> tmp;
-  tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), bytes, kin, kout, n, begin_bit, end_bit, s));
+void sort_keys(const K *kin, K *kout, int64_t n, int begin_bit, int end_bit, int *fail,
+               cudaStream_t s) {
+  radix_sort<K, false>(SrcKeys<K>{kin, nullptr}, EmitPairs<K>{kout, nullptr}, n, begin_bit, end_bit,
+                       fail, s);
 }
 
 template <class T>
@@ -778,7 +759,7 @@ int cooperative_grid(const void *kernel, int threads) {
 // Small pinned host blocks for the per-level counts, kept for reuse: pinned
 // allocation is slow, and a plan is built per step in many loops.
 namespace {
-constexpr int PINNED_INTS = 64;  // >= 2 (MAXD + 2)
+constexpr int PINNED_INTS = 64;  // >= 2 (MAXD + 2) + 1
 std::mutex g_pinned_mu;
 std::vector<int *> g_pinned_free;
 
@@ -806,11 +787,15 @@ void pinned_release(int *p) {
   g_pinned_free.push_back(p);
 }
 
-void begin_pending_counts(TreeHost &th, const int *dev_counts, int count, cudaStream_t s) {
-  FMMB_CHECK(count <= PINNED_INTS, ERR_INVALID_ARGUMENT, "too many levels");
+// the counts and, after them, the tree's sort failure flag
+void begin_pending_counts(TreeHost &th, const int *dev_counts, int count, const int *dev_fail,
+                          cudaStream_t s) {
+  FMMB_CHECK(count + 1 <= PINNED_INTS, ERR_INVALID_ARGUMENT, "too many levels");
   if (!th.pending_counts) th.pending_counts = pinned_acquire();
   if (!th.ready) FMMB_CUDA(cudaEventCreateWithFlags(&th.ready, cudaEventDisableTiming));
   FMMB_CUDA(cudaMemcpyAsync(th.pending_counts, dev_counts, count * sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
+  FMMB_CUDA(cudaMemcpyAsync(th.pending_counts + count, dev_fail, sizeof(int),
                             cudaMemcpyDeviceToHost, s));
   FMMB_CUDA(cudaEventRecord(th.ready, s));
   th.pending = true;
@@ -825,6 +810,8 @@ void finalize_tree(TreeHost &th) {
   FMMB_CUDA(cudaEventSynchronize(th.ready));
   const int L = th.L;
   const int *hpb = th.pending_counts;  // [0, L]: parent-box bounds; [L+1, 2L+1]: real groups
+  // (stays pending: every later use reports the failure again)
+  FMMB_CHECK(!hpb[2 * (L + 1)], ERR_CUDA, "tree sort: a grid barrier wait ran out of time");
   th.off.assign(L + 1, 0);
   if (L >= 1) th.off[1] = 1;
   for (int m = 1; m < L; ++m) th.off[m + 1] = th.off[m] + 4 * (hpb[m] - hpb[m - 1]);
@@ -844,73 +831,81 @@ TreeHost::~TreeHost() {
   pinned_release(pending_counts);
 }
 
-void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
-                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s, int sorted_digits,
-                 double *sx, double *sy) {
-  keys.alloc(n, s);
-  perm.alloc(n, s);
-  if (n == 0) return;
-  double scale, margin;
-  key_params(th.x0, th.y0, th.w0, scale, margin);
-  const int digits = sorted_digits < 1 ? 1 : (sorted_digits > MAXD ? MAXD : sorted_digits);
+namespace {
+int clamp_digits(int d) { return d < 1 ? 1 : (d > MAXD ? MAXD : d); }
+
+template <class K>
+using PointSortKernel = decltype(&k_radix_sort<K, SrcPoints<K>, EmitPoints<K>, true>);
+
+template <class K>
+PointSortKernel<K> point_sort_kernel() {
+  return &k_radix_sort<K, SrcPoints<K>, EmitPoints<K>, true>;
+}
+
+// bit range of the sort keys for `digits` top digits
+void point_sort_bits(int digits, int &begin_bit, int &end_bit) {
   if (digits <= KEY32_DIGITS) {
-    // 32-bit sort keys; the 64-bit keys follow in sorted order (a stable
-    // sort on the same top digits: the same permutation)
-    DevBuf<uint32_t> k0, k1;
-    DevBuf<int> i0;
-    k0.alloc(n, s);
-    k1.alloc(n, s);
-    i0.alloc(n, s);
-    k_point_keys32<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin,
-                                                     k0.get(), i0.get());
-    FMMB_CUDA(cudaGetLastError());
-    radix_sort_pairs(k0.get(), k1.get(), i0.get(), perm.get(), n, 2 * (KEY32_DIGITS - digits),
-                     2 * KEY32_DIGITS, s);
-    k_gather_keyed<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, perm.get(), n, th.x0, th.y0, th.w0, scale,
-                                                     margin, sx, sy, keys.get());
-    FMMB_CUDA(cudaGetLastError());
-    return;
-  }
-  DevBuf<uint64_t> k0;
-  DevBuf<int> i0;
-  k0.alloc(n, s);
-  i0.alloc(n, s);
-  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin,
-                                                 k0.get(), i0.get());
-  FMMB_CUDA(cudaGetLastError());
-  radix_sort_pairs(k0.get(), keys.get(), i0.get(), perm.get(), n, 2 * (MAXD - digits), 2 * MAXD, s);
-  if (sx) {
-    k_gather_xy<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, perm.get(), n, sx, sy);
-    FMMB_CUDA(cudaGetLastError());
+    begin_bit = 2 * (KEY32_DIGITS - digits);
+    end_bit = 2 * KEY32_DIGITS;
+  } else {
+    begin_bit = 2 * (MAXD - digits);
+    end_bit = 2 * MAXD;
   }
 }
 
-size_t sort_points_scratch_bytes(int64_t n) {
-  size_t bytes = 0;
-  cub::DoubleBuffer<uint64_t> kb(nullptr, nullptr);
-  cub::DoubleBuffer<int> vb(nullptr, nullptr);
-  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, n, 0, 2 * MAXD));
-  return bytes;
+template <class K>
+size_t point_sort_bytes(int64_t n, int digits) {
+  int b0, b1;
+  point_sort_bits(digits, b0, b1);
+  return radix_scratch_bytes<K, true>(n, (b1 - b0 + 7) / 8);
+}
+
+template <class K>
+void point_sort_run(const double *x, const double *y, int64_t n, const TreeHost &th, int digits,
+                    uint64_t *keys, int *perm, double *sx, double *sy, void *scratch,
+                    size_t bytes, int *fail, cudaStream_t s) {
+  double scale, margin;
+  key_params(th.x0, th.y0, th.w0, scale, margin);
+  int b0, b1;
+  point_sort_bits(digits, b0, b1);
+  const SrcPoints<K> src{x, y, th.x0, th.y0, th.w0, scale, margin};
+  const EmitPoints<K> emit{x, y, th.x0, th.y0, th.w0, scale, margin, keys, perm, sx, sy};
+  radix_sort_run<K, true>(src, emit, n, b0, b1, scratch, bytes,
+                          radix_grid<K, true>(point_sort_kernel<K>(), n), fail, s);
+}
+}  // namespace
+
+size_t sort_points_scratch_bytes(int64_t n, int sorted_digits) {
+  if (n <= 0) return 0;
+  const int digits = clamp_digits(sorted_digits);
+  return digits <= KEY32_DIGITS ? point_sort_bytes<uint32_t>(n, digits)
+                                : point_sort_bytes<uint64_t>(n, digits);
 }
 
 void sort_points_scratch(const double *x, const double *y, int64_t n, const TreeHost &th,
-                         uint64_t *k0, uint64_t *k1, int *i0, int *i1, void *temp,
-                         size_t temp_bytes, const uint64_t **keys, const int **perm,
-                         cudaStream_t s) {
-  *keys = k0;
-  *perm = i0;
+                         int sorted_digits, uint64_t *keys, int *perm, double *sx, double *sy,
+                         void *scratch, size_t scratch_bytes, int *fail, cudaStream_t s) {
+  if (n <= 0) return;
+  const int digits = clamp_digits(sorted_digits);
+  if (digits <= KEY32_DIGITS)
+    point_sort_run<uint32_t>(x, y, n, th, digits, keys, perm, sx, sy, scratch, scratch_bytes, fail,
+                             s);
+  else
+    point_sort_run<uint64_t>(x, y, n, th, digits, keys, perm, sx, sy, scratch, scratch_bytes, fail,
+                             s);
+}
+
+void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
+                 DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t s, int sorted_digits,
+                 double *sx, double *sy, int *fail) {
+  keys.alloc(n, s);
+  perm.alloc(n, s);
   if (n == 0) return;
-  double scale, margin;
-  key_params(th.x0, th.y0, th.w0, scale, margin);
-  k_point_keys<<<grid_for(n, TPB), TPB, 0, s>>>(x, y, n, th.x0, th.y0, th.w0, scale, margin, k0,
-                                                 i0);
-  FMMB_CUDA(cudaGetLastError());
-  cub::DoubleBuffer<uint64_t> kb(k0, k1);
-  cub::DoubleBuffer<int> vb(i0, i1);
-  size_t bytes = temp_bytes;
-  FMMB_CUDA(cub::DeviceRadixSort::SortPairs(temp, bytes, kb, vb, n, 0, 2 * MAXD, s));
-  *keys = kb.Current();
-  *perm = vb.Current();
+  const size_t bytes = sort_points_scratch_bytes(n, sorted_digits);
+  DevBuf<unsigned char> tmp;
+  tmp.alloc(bytes, s);
+  sort_points_scratch(x, y, n, th, sorted_digits, keys.get(), perm.get(), sx, sy, tmp.get(), bytes,
+                      fail, s);
 }
 
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
@@ -938,8 +933,12 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   std::unique_ptr<PhaseTimer> t_split(new PhaseTimer(PH_TREE_SPLITS, s));
   td.sx.alloc(n, s);
   td.sy.alloc(n, s);
+  td.sort_fail.alloc(1, s);
+  td.sort_fail.zero(s);
+  int hfail = 0;
   for (int digits = SORT_DIGITS;; digits = MAXD) {
-    sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits, td.sx.get(), td.sy.get());
+    sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits, td.sx.get(), td.sy.get(),
+                td.sort_fail.get());
     cnt.zero(s);
     k_split_counts<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, scount.get(),
                                                      cnt.get(), max_split);
@@ -949,7 +948,9 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
                                                    s0raw.get(), cap0, cnt.get(), max_split);
     FMMB_CUDA(cudaGetLastError());
     FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaMemcpyAsync(&hfail, td.sort_fail.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
+    FMMB_CHECK(!hfail, ERR_CUDA, "point sort: a grid barrier wait ran out of time");
     FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
                "more than Ncutoff points share a box of width bbox/2^29 (coincident points?)");
     FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
@@ -971,7 +972,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     // split boxes by (level, morton): a stable sort on the level bits keeps
     // the morton order every level already has
     s0.alloc(n0, s);
-    sort_keys(s0raw.get(), s0.get(), n0, LEVEL_SHIFT, LEVEL_SHIFT + 5, s);
+    sort_keys(s0raw.get(), s0.get(), n0, LEVEL_SHIFT, LEVEL_SHIFT + 5, td.sort_fail.get(), s);
     DevBuf<int> s0b;
     s0b.alloc(L + 2, s);
     k_level_starts<<<grid_for(n0, TPB), TPB, 0, s>>>(s0.get(), n0, L + 1, s0b.get());
@@ -1007,8 +1008,10 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
                                               TPB, args, 0, s));
       }
       FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+      FMMB_CUDA(cudaMemcpyAsync(&hfail, td.sort_fail.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
       FMMB_CUDA(cudaStreamSynchronize(s));
       FMMB_CHECK(!hc.bar_timeout, ERR_CUDA, "tree balance: a grid barrier wait ran out of time");
+      FMMB_CHECK(!hfail, ERR_CUDA, "split-box sort: a grid barrier wait ran out of time");
       if (hc.overflow) {
         FMMB_CHECK(attempt < 6, ERR_CAPACITY, "tree balance buffers overflow");
         capf = 4 * capf;
@@ -1026,7 +1029,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     // 6: sorted parent boxes, per-level bounds, real sibling groups
     t_bal.reset();
     pkc.alloc(np, s);
-    sort_keys(pk.get(), pkc.get(), np, 0, 1 + mb + 5, s);
+    sort_keys(pk.get(), pkc.get(), np, 0, 1 + mb + 5, td.sort_fail.get(), s);
     pks.alloc(np, s);
     pxs.alloc(np, s);
     preal.alloc(np, s);
@@ -1059,7 +1062,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   td.dev_off.alloc(L + 1, s);
   k_level_offsets<<<1, 1, 0, s>>>(pb.get(), L, td.dev_off.get());
   FMMB_CUDA(cudaGetLastError());
-  begin_pending_counts(th, pb.get(), 2 * (L + 1), s);
+  begin_pending_counts(th, pb.get(), 2 * (L + 1), td.sort_fail.get(), s);
   // every parent box has 4 children: at most 1 + 4 np nodes, np real groups
   const int total_ub = 1 + 4 * int(np);
   td.rg.alloc(np > 0 ? np : 1, s);

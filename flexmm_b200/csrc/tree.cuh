@@ -50,6 +50,9 @@ struct TreeDev {
   // real leaves that are not X-list leaves, and fake leaves, holding points;
   // in node order (so level-major).  Count on the device.
   DevBuf<int> uplist, n_up;
+  // set to 1 by a radix sort of this tree (the build's or a target sort)
+  // whose grid barrier wait ran out; the sorted outputs are then invalid
+  DevBuf<int> sort_fail;
 };
 
 struct TreeHost {
@@ -87,17 +90,19 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
 // quadrant digits (enough to place them in boxes of levels <= sorted_digits);
 // returns the keys in that order and the permutation sorted -> original,
 // and (if sx, sy are given) the coordinates in that order.
+// The sort is stable (points with equal digits keep their input order).
+// fail (optional, device int) is set to 1 if the sort's grid barrier wait
+// ran out (the outputs are then invalid but hold valid indices).
 void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th,
                  DevBuf<uint64_t> &keys, DevBuf<int> &perm, cudaStream_t stream,
-                 int sorted_digits = MAXD, double *sx = nullptr, double *sy = nullptr);
+                 int sorted_digits = MAXD, double *sx = nullptr, double *sy = nullptr,
+                 int *fail = nullptr);
 
-// The same keys and sort into caller-provided memory: k0/k1 and i0/i1 are
-// ping-pong buffers of n entries, temp holds sort_points_scratch_bytes(n)
-// bytes.  *keys / *perm point at the buffers holding the sorted result.
-size_t sort_points_scratch_bytes(int64_t n);
+// The same into caller-provided memory: keys [n], perm [n], optional sx, sy
+// [n], and scratch of sort_points_scratch_bytes(n, sorted_digits) bytes.
+size_t sort_points_scratch_bytes(int64_t n, int sorted_digits);
 void sort_points_scratch(const double *x, const double *y, int64_t n, const TreeHost &th,
-                         uint64_t *k0, uint64_t *k1, int *i0, int *i1, void *temp,
-                         size_t temp_bytes, const uint64_t **keys, const int **perm,
-                         cudaStream_t stream);
+                         int sorted_digits, uint64_t *keys, int *perm, double *sx, double *sy,
+                         void *scratch, size_t scratch_bytes, int *fail, cudaStream_t stream);
 
 }  // namespace fmmb
