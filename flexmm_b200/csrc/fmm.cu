@@ -20,13 +20,13 @@
 //    activations sit in shared memory with padded rows (stride 4 mod 16
 //    doubles: conflict-free fragment loads), the operators are read through
 //    the read-only cache.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <type_traits>
 
 #include "fmm.cuh"
 #include "gemm.cuh"
+#include "scan.cuh"
 #include "timing.cuh"
 
 namespace fmmb {
@@ -872,11 +872,7 @@ void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &
                                                       td.flags.get(), tkeys, m, it.tb.get(),
                                                       it.te.get(), it.nch.get());
   FMMB_CUDA(cudaGetLastError());
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, it.nch.get(), it.choff.get(), total, s));
-  DevBuf<uint8_t> tmp;
-  tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, it.nch.get(), it.choff.get(), total, s));
+  prefix_sum<int, false>(it.nch.get(), it.choff.get(), total, td.sort_fail.get(), true, s);
   it.items.alloc(total + m / TCH + 1, s);
   it.n_items.alloc(1, s);
   k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), it.tb.get(),
@@ -1185,12 +1181,7 @@ void run_direct(int kernel_id, const KernelParams &kp, const double *sx, const d
   FMMB_CUDA(cudaGetLastError());
 }
 
-size_t evaluate_scratch_bytes(int total_nodes) {
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int *)nullptr, (int *)nullptr,
-                                          total_nodes));
-  return bytes;
-}
+size_t evaluate_scratch_bytes(int total_nodes) { return scan_scratch_bytes<int>(total_nodes); }
 
 void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *loc,
                           const double *txs, const double *tys, const uint64_t *tkeys,
@@ -1204,8 +1195,7 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   k_leaf_targets<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), td.code.get(),
                                                       td.flags.get(), tkeys, m, tb, te, nch);
   FMMB_CUDA(cudaGetLastError());
-  size_t bytes = temp_bytes;
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, nch, choff, total, s));
+  prefix_sum_run<int, false>(nch, choff, total, temp, temp_bytes, td.sort_fail.get(), true, s);
   k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), tb, te, nch, choff,
                                                     items, n_items);
   FMMB_CUDA(cudaGetLastError());

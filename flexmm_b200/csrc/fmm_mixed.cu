@@ -19,13 +19,13 @@
 //  * check-to-equivalent stays FP64 (the FP64 tensor-core tiles of fmm.cu).
 // Error against FP64 direct summation on the 1M clustered workload at
 // Nequiv 24: ~4e-7 relative L2 (the FP64 path at Nequiv 24: ~2e-7).
-#include <cub/cub.cuh>
 
 #include <cstdlib>
 #include <string>
 
 #include "fmm.cuh"
 #include "gemm.cuh"
+#include "scan.cuh"
 #include "tcgen05.cuh"
 #include "timing.cuh"
 
@@ -1216,11 +1216,7 @@ void node_charge_sums(const PassArgs &a, const double *tau_s, double *tsum, cuda
   DevBuf<double> pre;
   pre.alloc(n + 1, s);
   FMMB_CUDA(cudaMemsetAsync(pre.get(), 0, sizeof(double), s));
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, tau_s, pre.get() + 1, n, s));
-  DevBuf<uint8_t> tmp;
-  tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), bytes, tau_s, pre.get() + 1, n, s));
+  prefix_sum<double, true>(tau_s, pre.get() + 1, n, a.td->sort_fail.get(), false, s);
   k_node_charge_sums<<<grid_for(total, 256), 256, 0, s>>>(total, a.td->bot.get(), a.td->top.get(),
                                                           pre.get(), tsum);
   FMMB_CUDA(cudaGetLastError());

@@ -78,12 +78,12 @@ inline size_t radix_work_bytes(int64_t n, int passes) {
 // Grid barrier on a counter that only grows: barrier k of the launch is
 // passed once the count reaches (k + 1) * gridDim.x, so the last block to
 // arrive has nothing to release (arrival and release are one atomic).
-__device__ bool rs_grid_sync(const RadixWork &w) {
+__device__ bool grid_barrier(RadixSync *sync, int *fail) {
   __shared__ int ok;
   __syncthreads();
   if (gridDim.x == 1) return true;
   if (threadIdx.x == 0) {
-    unsigned int *cnt = &w.sync->count;
+    unsigned int *cnt = &sync->count;
     unsigned int old;
     asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(cnt) : "memory");
     const unsigned int target = (old / gridDim.x + 1) * gridDim.x;
@@ -91,8 +91,8 @@ __device__ bool rs_grid_sync(const RadixWork &w) {
     unsigned int tries = 0, cur = old + 1;
     while (cur < target) {
       if (++tries > RS_BARRIER_TRIES) {
-        atomicExch(&w.sync->timeout, 1);
-        if (w.fail) atomicExch(w.fail, 1);
+        atomicExch(&sync->timeout, 1);
+        if (fail) atomicExch(fail, 1);
         good = 0;
         break;
       }
@@ -103,6 +103,8 @@ __device__ bool rs_grid_sync(const RadixWork &w) {
   __syncthreads();
   return ok;
 }
+
+__device__ __forceinline__ bool rs_grid_sync(const RadixWork &w) { return grid_barrier(w.sync, w.fail); }
 
 // lanes of the warp holding the same 9-bit label as this lane: one ballot
 // per bit (cheaper than match.any here)

@@ -30,14 +30,13 @@
 // The host waits twice (for the split-box count and depth, then for the
 // balance closure's size); the per-level node counts come back without a
 // wait (finalize_tree).
-#include <cub/cub.cuh>
-
 #include <cmath>
 
 #include <memory>
 #include <mutex>
 
 #include "radix.cuh"
+#include "scan.cuh"
 #include "timing.cuh"
 #include "tree.cuh"
 
@@ -732,13 +731,8 @@ void sort_keys(const K *kin, K *kout, int64_t n, int begin_bit, int end_bit, int
 }
 
 template <class T>
-void exclusive_sum(const T *in, T *out, int64_t n, cudaStream_t s) {
-  if (n <= 0) return;
-  size_t bytes = 0;
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
-  DevBuf<uint8_t> tmp;
-  tmp.alloc(bytes, s);
-  FMMB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s));
+void exclusive_sum(const T *in, T *out, int64_t n, int *fail, bool offsets, cudaStream_t s) {
+  prefix_sum<T, false>(in, out, n, fail, offsets, s);
 }
 
 // blocks of a cooperative launch: all co-resident, one per SM (the grid
@@ -943,7 +937,8 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     k_split_counts<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, scount.get(),
                                                      cnt.get(), max_split);
     FMMB_CUDA(cudaGetLastError());
-    exclusive_sum(scount.get(), spos.get(), n, s);
+    // (k_split_emit checks its writes against the capacity)
+    exclusive_sum(scount.get(), spos.get(), n, td.sort_fail.get(), false, s);
     k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
                                                    s0raw.get(), cap0, cnt.get(), max_split);
     FMMB_CUDA(cudaGetLastError());
@@ -1039,7 +1034,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     k_parent_decode<<<grid_for(np, TPB), TPB, 0, s>>>(pkc.get(), np, mb, L, pks.get(), pxs.get(),
                                                        preal.get(), pb.get());
     FMMB_CUDA(cudaGetLastError());
-    exclusive_sum(preal.get(), ppos.get(), np, s);
+    exclusive_sum(preal.get(), ppos.get(), np, td.sort_fail.get(), true, s);
     k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1);
     FMMB_CUDA(cudaGetLastError());
   } else {
@@ -1110,7 +1105,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
                                                          td.flags.get(), td.bot.get(), td.top.get(),
                                                          f.get());
     FMMB_CUDA(cudaGetLastError());
-    exclusive_sum(f.get(), pos.get(), total_ub, s);
+    exclusive_sum(f.get(), pos.get(), total_ub, td.sort_fail.get(), true, s);
     k_up_scatter<<<grid_for(total_ub, TPB), TPB, 0, s>>>(td.dev_off.get(), L, total_ub, f.get(),
                                                            pos.get(), td.uplist.get(),
                                                            td.n_up.get());

@@ -342,3 +342,25 @@ def test_dipoles_match_reference(built_lib, case):
     assert rel_l2(us.cpu().numpy(), g["src_val"]) < PARITY
     assert rel_l2(ut, g["tgt_val"]) < PARITY
     assert rel_l2(us2, g["src_val"]) < PARITY
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_results_are_bitwise_reproducible(built_lib, precision):
+    """Two builds and evaluations of the same problem give the same bits:
+    the tree's sorts are stable, its prefix sums (split counts, charge sums)
+    group their additions by a fixed layout, and no result depends on
+    timing."""
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    d = workloads.clustered(n=300_000, n_grid=300, seed=9)
+    x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
+    tx, ty = torch.from_numpy(d["tx"]).cuda(), torch.from_numpy(d["ty"]).cuda()
+    helper = KI_Helper()
+    outs = []
+    for _ in range(2):
+        F = KI_FMM(x, y, "Laplace_Eval", 64, 24 if precision == "mixed" else 40, bbox=d["bbox"],
+                   helper=helper, precision=precision)
+        F.build_expansions(d["tau"])
+        outs.append((F.source_evaluation(x, y).cpu(), F.target_evaluation(tx, ty).cpu()))
+        F.status()
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
