@@ -318,28 +318,28 @@ __device__ bool grid_sync(Counters *cnt, unsigned long long *snap) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int *gen = &cnt->bar_gen;
-    const unsigned int g = *gen;
-    __threadfence();
+    unsigned int g, old;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(&cnt->bar_gen) : "memory");
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;"
+                 : "=r"(old) : "l"(&cnt->bar_count) : "memory");
     int good = 1;
-    if (atomicAdd(&cnt->bar_count, 1u) == gridDim.x - 1) {
-      atomicExch(&cnt->bar_count, 0u);
+    if (old == gridDim.x - 1) {
+      // last to arrive: reset the count and take the snapshot, then release
+      cnt->bar_count = 0u;
       if (snap) *snap = atomicAdd(&cnt->f_count, 0ull);
-      __threadfence();
-      atomicAdd(&cnt->bar_gen, 1u);
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&cnt->bar_gen), "r"(g + 1u) : "memory");
     } else {
-      unsigned int tries = 0;
-      while (*gen == g) {
+      unsigned int tries = 0, cur = g;
+      while (cur == g) {
         if (++tries > BARRIER_TRIES) {
           atomicExch(&cnt->bar_timeout, 1);
           good = 0;
           break;
         }
-        __nanosleep(32);
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&cnt->bar_gen) : "memory");
       }
     }
-    __threadfence();
-    ok = good && !*(volatile int *)&cnt->bar_timeout;
+    ok = good;
   }
   __syncthreads();
   return ok;
