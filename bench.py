@@ -454,9 +454,11 @@ def work_counts_gemm(F, neq, c):
     return out
 
 
-# DRAM bytes (read + write) per launch of the dominant kernel on the default
-# workload (1M clustered sources + 1000^2 grid), from one ncu capture
-NCU_TRAFFIC_BYTES = {("mixed", "evaluate"): 44_016_384, ("fp64", "evaluate"): 53_386_240}
+# DRAM bytes per launch of the dominant kernel on the default workload (1M
+# clustered sources + 1000^2 grid): ncu captures of the 200k-source /
+# 450^2-grid case of the same distribution, scaled by the points each
+# launch evaluates, averaged over the source and grid launches
+NCU_TRAFFIC_BYTES = {("mixed", "evaluate"): 46_400_000, ("fp64", "evaluate"): 60_600_000}
 
 
 def roofline_of(res, precision, peaks, steps, default_workload):
