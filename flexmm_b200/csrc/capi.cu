@@ -261,8 +261,12 @@ struct fmm_plan {
   cudaStream_t side = nullptr;  // from the device's pool, not owned
   cudaEvent_t ev_ready = nullptr, ev_near = nullptr, ev_far = nullptr;
   bool ready_recorded = false;
+  // mixed form: the split near field pauses during the M2L (SplitEval::hold)
+  cudaEvent_t ev_m2l = nullptr;
+  DevBuf<int> near_hold;
+  bool hold_armed = false;
   ~fmm_plan() {
-    for (cudaEvent_t e : {ev_ready, ev_near, ev_far})
+    for (cudaEvent_t e : {ev_ready, ev_near, ev_far, ev_m2l})
       if (e) cudaEventDestroy(e);
   }
 };
@@ -287,10 +291,30 @@ cudaStream_t side_stream() {
   return g_side[dev][g_side_next[dev]++ % SIDE_STREAMS];
 }
 
+// Whether own-source evaluation runs split (near field beside the level
+// passes).  Measured at 1M clustered sources: the FP64 form gains ~0.6 ms
+// (its level passes are DMMA tiles that share SMs well); the mixed form
+// loses (its persistent tcgen05 M2L and smem-staged level kernels slow down
+// more beside the near field than the near field saves), so it evaluates in
+// one pass unless FLEXMM_B200_SPLIT_EVAL=1.  FLEXMM_B200_SPLIT_EVAL=0 turns
+// the split off for both forms.
+std::atomic<int> g_split_mode{-2};  // -2: not yet read from the environment
+
+bool split_enabled(int precision) {
+  int mode = g_split_mode.load(std::memory_order_relaxed);
+  if (mode == -2) {
+    const char *e = getenv("FLEXMM_B200_SPLIT_EVAL");
+    int env = e ? (e[0] == '0' ? 0 : 1) : -1;
+    g_split_mode.compare_exchange_strong(mode, env);
+    mode = g_split_mode.load(std::memory_order_relaxed);
+  }
+  return mode < 0 ? precision == PREC_FP64 : mode == 1;
+}
+
 // the plan's split-evaluation events (created on first use) and side stream
 void split_prepare(fmm_plan *p) {
   if (!p->side) p->side = side_stream();
-  for (cudaEvent_t *e : {&p->ev_ready, &p->ev_near, &p->ev_far})
+  for (cudaEvent_t *e : {&p->ev_ready, &p->ev_near, &p->ev_far, &p->ev_m2l})
     if (!*e) FMMB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
 }
 }  // namespace
@@ -1103,6 +1127,14 @@ static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream) 
       p->lsum.zero(s);
       p->tsum.alloc(total, s);
       node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
+      // a split near field (if evaluation splits) runs beside the upward and
+      // downward passes and pauses while the M2L runs: hold clear now, set
+      // before the M2L; m2l_done recorded after it
+      p->hold_armed = split_enabled(PREC_MIXED);
+      if (p->hold_armed) {
+        p->near_hold.alloc(1, s);
+        p->near_hold.zero(s);
+      }
       // sorted charges and box charge sums are all the near field reads
       FMMB_CUDA(cudaEventRecord(p->ev_ready, s));
       p->ready_recorded = true;
@@ -1111,8 +1143,10 @@ static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream) 
                        p->mult_tc.get(), s);
       p->err.alloc(2, s);  // [0] error flag, [1] M2L tile counter
       p->err.zero(s);
+      if (p->hold_armed) FMMB_CUDA(cudaMemsetAsync(p->near_hold.get(), 1, 1, s));
       run_m2l_mixed(a, p->mult32.get(), p->mult_tc.get(), p->msum.get(), p->ple.get(),
                     p->err.get(), s);
+      if (p->hold_armed) FMMB_CUDA(cudaEventRecord(p->ev_m2l, s));
       run_downward_mixed(a, p->ple.get(), p->loc32.get(), p->lsum.get(), s);
     } else {
       p->mult.alloc(total * np, s);
@@ -1184,25 +1218,6 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
                  m, check, nout, out, ld_out, s);
 }
 
-// Whether own-source evaluation runs split (near field beside the level
-// passes).  Measured at 1M clustered sources: the FP64 form gains ~0.6 ms
-// (its level passes are DMMA tiles that share SMs well); the mixed form
-// loses (its persistent tcgen05 M2L and smem-staged level kernels slow down
-// more beside the near field than the near field saves), so it evaluates in
-// one pass unless FLEXMM_B200_SPLIT_EVAL=1.  FLEXMM_B200_SPLIT_EVAL=0 turns
-// the split off for both forms.
-std::atomic<int> g_split_mode{-2};  // -2: not yet read from the environment
-
-bool split_enabled(int precision) {
-  int mode = g_split_mode.load(std::memory_order_relaxed);
-  if (mode == -2) {
-    const char *e = getenv("FLEXMM_B200_SPLIT_EVAL");
-    int env = e ? (e[0] == '0' ? 0 : 1) : -1;
-    g_split_mode.compare_exchange_strong(mode, env);
-    mode = g_split_mode.load(std::memory_order_relaxed);
-  }
-  return mode < 0 ? precision == PREC_FP64 : mode == 1;
-}
 
 void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t ld_out,
                           cudaStream_t s) {
@@ -1224,7 +1239,11 @@ void evaluate_own_sources(fmm_plan *p, int nout, int check, double *out, int64_t
                     td.pkeys.get(), td.ordv.get(), m, check, nout, out, ld_out, s);
   else if (nout == 1 && p->ready_recorded && p->n_rhs == 1 && split_enabled(p->precision)) {
     // near field on the side stream, started when the charges were sorted
-    const SplitEval se{p->side, p->ev_ready, p->ev_near, p->ev_far};
+    SplitEval se{p->side, p->ev_ready, p->ev_near, p->ev_far};
+    if (p->precision == PREC_MIXED && p->hold_armed) {
+      se.hold = p->near_hold.get();
+      se.m2l_done = p->ev_m2l;
+    }
     if (p->precision == PREC_MIXED)
       run_evaluate_sources_split_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(),
                                        p->lsum.get(), check, out, s, se);

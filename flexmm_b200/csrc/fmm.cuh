@@ -120,12 +120,19 @@ void run_evaluate_multi(const PassArgs &a, const double *tau_sorted, int64_t n_s
 struct SplitEval {
   cudaStream_t side;
   cudaEvent_t ready, near_done, far_done;
+  // mixed form: the near field pauses while the M2L runs.  hold (device int)
+  // is set on the plan stream before the M2L and m2l_done recorded after
+  // it; the near-field kernel takes no new items while hold is set, and a
+  // second launch after m2l_done finishes the rest.  hold NULL: one launch.
+  int *hold = nullptr;
+  cudaEvent_t m2l_done = nullptr;
 };
 // near-field blocks per SM, leaving room for the level passes: FP64 (28 KB of
 // shared memory each) beside the DMMA M2L tiles; mixed (17 KB each) beside
 // one persistent tcgen05 M2L CTA (154 KB at Nequiv 24)
 constexpr int NEAR_BLOCKS_PER_SM = 4;
 constexpr int NEAR_BLOCKS_PER_SM_MIXED = 3;
+constexpr int NEAR_BLOCKS_PER_SM_MIXED_RESUME = 10;  // after the M2L, beside the downward pass
 void run_evaluate_sources_split(const PassArgs &a, const double *tau_sorted, const double *loc,
                                 int check, double *out, cudaStream_t s, const SplitEval &se);
 void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_sorted,

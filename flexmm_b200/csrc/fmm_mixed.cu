@@ -822,7 +822,8 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
                   const double *__restrict__ lsum, const double *__restrict__ txs,
                   const double *__restrict__ tys, const int *__restrict__ tperm, int check,
                   int self_eval, double *__restrict__ out, int64_t ld_out,
-                  int *__restrict__ next_item, double *__restrict__ near = nullptr) {
+                  int *__restrict__ next_item, double *__restrict__ near = nullptr,
+                  const int *hold = nullptr) {
   static_assert(PART == EVAL_FULL || NOUT == 1, "split evaluation: potential only");
   __shared__ EvalDesc D;
   __shared__ float4 src[SMAX];  // (x, y, charge, sorted index) in width units of the leaf
@@ -831,14 +832,31 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
   // otherwise lose the digits below 2^-24 of the leaf width
   __shared__ float2 src_lo[NOUT == 3 ? SMAX : 1];
   __shared__ double red[NOUT][TCH / 32];
-  __shared__ int s_next;
+  __shared__ int s_next, s_pair;
   const KF32 K(kp);
   const KF64 K64(kp);
   const int n_items = *n_items_ptr;
   const int *dw = reinterpret_cast<const int *>(desc);
   // items are handed out dynamically: the block works on `item`, holds the
-  // descriptor of `nxt` in registers and fetches the index after that
+  // descriptor of `nxt` in registers and fetches the index after that.
+  // With `hold` (a near field that pauses and resumes in a second launch)
+  // every item is claimed from the counter, and none while *hold is set.
+  auto claim = [&]() -> int {
+    if (*reinterpret_cast<const volatile int *>(hold)) return n_items;
+    return atomicAdd(next_item, 1);
+  };
   int item = blockIdx.x, nxt = blockIdx.x + gridDim.x;
+  if (hold) {
+    if (threadIdx.x == 0) {
+      const int a = claim();
+      s_next = a;
+      s_pair = a < n_items ? claim() : n_items;
+    }
+    __syncthreads();
+    item = s_next;
+    nxt = s_pair;
+    __syncthreads();
+  }
   int nextw = 0;
   if (item < n_items && threadIdx.x < 32) nextw = __ldg(dw + (size_t)item * 32 + threadIdx.x);
   while (item < n_items) {
@@ -846,7 +864,8 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
     __syncthreads();
     if (nxt < n_items && threadIdx.x < 32) nextw = __ldg(dw + (size_t)nxt * 32 + threadIdx.x);
     int after = 0;
-    if (threadIdx.x == 0) after = atomicAdd(next_item, 1) + 2 * gridDim.x;
+    if (threadIdx.x == 0)
+      after = hold ? (nxt < n_items ? claim() : n_items) : atomicAdd(next_item, 1) + 2 * gridDim.x;
     const int g = D.g, lev = D.lev, t0 = D.t0, cnt = D.cnt;
     const int ns = PART == EVAL_FAR ? 0 : D.rs[9];
     int G = 1;
@@ -1342,12 +1361,22 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
     }();
     (void)carveout_set;
     PhaseTimer timer(PH_EVAL, se.side);
-    k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>
-        <<<work_grid(total + m / TCH + 1, NEAR_BLOCKS_PER_SM_MIXED), TCH, 0, se.side>>>(
-            a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
-            a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
-            next_item.get(), near.get());
-    FMMB_CUDA(cudaGetLastError());
+    // beside the upward pass until the M2L starts (hold), then beside the
+    // downward pass, resuming from the same item counter
+    for (int part = 0; part < (se.hold ? 2 : 1); ++part) {
+      if (part == 1) {
+        FMMB_CUDA(cudaStreamWaitEvent(se.side, se.m2l_done, 0));
+        FMMB_CUDA(cudaMemsetAsync(se.hold, 0, sizeof(int), se.side));
+      }
+      k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>
+          <<<work_grid(total + m / TCH + 1, part == 0 ? NEAR_BLOCKS_PER_SM_MIXED
+                                                      : NEAR_BLOCKS_PER_SM_MIXED_RESUME),
+             TCH, 0, se.side>>>(a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(),
+                                td.sy.get(), tau_s, a.ops_dev, loc32, lsum, td.sx.get(),
+                                td.sy.get(), td.ordv.get(), check, 1, out, 0, next_item.get(),
+                                near.get(), se.hold);
+      FMMB_CUDA(cudaGetLastError());
+    }
   }
   FMMB_CUDA(cudaEventRecord(se.near_done, se.side));
   FMMB_CUDA(cudaStreamWaitEvent(s, se.near_done, 0));
@@ -1396,7 +1425,7 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
                                                                 it.n_items.get(),
                                         td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc32, lsum,
                                         txs, tys, tperm, check, self_eval, out, ld_out,
-                                        next_item.get(), nullptr);
+                                        next_item.get(), nullptr, nullptr);
       break;
     }
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
