@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, in
   const int ldp = pad_ld(np);
   double *P = smem;          // [TN][ldp] check potentials
   double *T = P + TN * ldp;  // [TN][ldp] C2E scratch
+  double *Bs = T + TN * ldp;  // C2E operators streamed through (gemm_stage_doubles(np))
   __shared__ double srcx[NT / 32][32], srcy[NT / 32][32], srct[NT / 32][32];
   __shared__ double srcdx[DIP ? NT / 32 : 1][32], srcdy[DIP ? NT / 32 : 1][32];
   __shared__ int node[TN], nlev[TN];
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(NT) k_s2m(KernelParams kp, int neq, int np, in
       if (threadIdx.x < TN)
         orow[threadIdx.x] = nlev[threadIdx.x] == m ? mult + (size_t)node[threadIdx.x] * np : nullptr;
       __syncthreads();
-      c2e_tile(ops[m], np, P, T, orow);
+      c2e_tile_staged(ops[m], np, P, T, orow, Bs);
     }
     __syncthreads();
   }
@@ -216,6 +217,7 @@ __global__ void __launch_bounds__(NT) k_m2m(int m, int np, int c_first, int n_gr
   double *P = smem;           // [TN][ldp] check potentials
   double *T = P + TN * ldp;   // [TN][ldp] C2E scratch
   double *A = T + TN * ldp;   // [TN][lda] children multipoles
+  double *Bs = A + TN * lda;  // operators streamed through (gemm_stage_doubles(np))
   __shared__ double *orow[TN];
   const LevelOpsDev &op = ops[m];
   const int e0 = blockIdx.x * TN, nloc = min(TN, n_groups - e0);
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(NT) k_m2m(int m, int np, int c_first, int n_gr
     const int r0 = 8 * (warp & 3), c0 = 8 * (warp >> 2);
     double acc[1][4][2];
     zero_acc(acc);
-    warp_gemm<1, 4>(A, lda, op.m2mct, np, 4 * np, r0, c0, 2, np, acc);
+    warp_gemm_staged<1, 4>(A, lda, op.m2mct, np, 4 * np, r0, c0, 2, np, acc, Bs);
     const int t = r0 + g;
 #pragma unroll
     for (int cb = 0; cb < 4; ++cb) {
@@ -248,7 +250,7 @@ __global__ void __launch_bounds__(NT) k_m2m(int m, int np, int c_first, int n_gr
     }
   }
   __syncthreads();
-  c2e_tile(op, np, P, T, orow);
+  c2e_tile_staged(op, np, P, T, orow, Bs);
 }
 
 // ------------------------------------------------------------------- M2L ----
@@ -356,6 +358,7 @@ __global__ void __launch_bounds__(NT) k_downward(int m, int np, int rg_lo, int r
   const int ldp = pad_ld(np);
   double *P = smem;           // [32][ldp] partial locals
   double *T = P + TN * ldp;   // [32][ldp] parent locals, then C2E scratch
+  double *Bs = T + TN * ldp;  // operators streamed through (gemm_stage_doubles(4 np))
   __shared__ int node[TN];
   __shared__ double *orow[TN];
   const LevelOpsDev &op = ops[m];
@@ -389,7 +392,7 @@ __global__ void __launch_bounds__(NT) k_downward(int m, int np, int rg_lo, int r
     // warp -> column blocks warp + 8*cb of the 4np columns
     double acc[1][4][2];
     zero_acc(acc);
-    warp_gemm<1, 4>(T, ldp, opp.m2mc, 4 * np, np, 0, 8 * warp, 8, 4 * np, acc);
+    warp_gemm_staged<1, 4>(T, ldp, opp.m2mc, 4 * np, np, 0, 8 * warp, 8, 4 * np, acc, Bs);
 #pragma unroll
     for (int cb = 0; cb < 4; ++cb) {
       const int col = 8 * warp + 64 * cb + 2 * q;  // column of the 4np-wide parent row
@@ -401,7 +404,7 @@ __global__ void __launch_bounds__(NT) k_downward(int m, int np, int rg_lo, int r
     }
     __syncthreads();
   }
-  c2e_tile(op, np, P, T, orow);
+  c2e_tile_staged(op, np, P, T, orow, Bs);
 }
 
 // ------------------------------------------------------------ evaluation ----
@@ -819,7 +822,7 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   const TreeDev &td = *a.td;
   const int np = a.np;
   if (th.L < 3) return;
-  const size_t s2m_bytes = sizeof(double) * (size_t)TN * pad_ld(np) * 2;
+  const size_t s2m_bytes = sizeof(double) * ((size_t)TN * pad_ld(np) * 2 + gemm_stage_doubles(np));
   smem_limit(k_s2m<KF>, s2m_bytes);
   // persistent over the S2M nodes; at most one block per TN nodes of the tree
   // (small trees launch small grids)
@@ -842,7 +845,8 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
         mult, nullptr, nullptr, tstride, cstride);
   }
   FMMB_CUDA(cudaGetLastError());
-  const size_t m2m_bytes = sizeof(double) * (size_t)TN * (2 * pad_ld(np) + pad_ld(4 * np));
+  const size_t m2m_bytes =
+      sizeof(double) * ((size_t)TN * (2 * pad_ld(np) + pad_ld(4 * np)) + gemm_stage_doubles(np));
   smem_limit(k_m2m, m2m_bytes);
   for (int m = th.L - 2; m >= 2; --m) {
     const int c_first = th.off[m + 1];
@@ -958,7 +962,9 @@ void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_
                   int64_t cstride) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
-  const size_t sm = sizeof(double) * (size_t)TN * pad_ld(a.np) * 2;
+  const size_t sm =
+      sizeof(double) * ((size_t)TN * pad_ld(a.np) * 2 + gemm_stage_doubles(4 * a.np));
+  smem_limit(k_downward, sm);
   for (int m = 2; m < th.L; ++m) {
     const int lo = th.rg_lo[m], cnt = th.rg_hi[m] - th.rg_lo[m];
     if (cnt <= 0) continue;

@@ -144,4 +144,100 @@ __device__ inline void c2e_tile(const LevelOpsDev &op, int np, const double *P, 
   c2e_tile<false>(c2e_global(op, np), np, P, T, out_row);
 }
 
+// ---- GEMMs with the B operand streamed through shared memory ----
+// B (row-major [K][ldb] in global memory, first ncols columns) is copied in
+// chunks of GS_KC rows into a double buffer Bs of gemm_stage_doubles(ncols)
+// doubles (row stride pad_ld(ncols)), the next chunk in flight while the
+// warps multiply the current one: the k-loop reads shared memory only,
+// where reading B from L2 inside it left each warp waiting on one L2 round
+// trip per few k-steps.  Called by every thread of the block (barriers
+// inside); ncols even, ldb and B 16-byte aligned, K a multiple of 4; no
+// copies of the caller may be in flight (they would join the first group).
+constexpr int GS_KC = 16;
+__host__ __device__ inline int gemm_stage_doubles(int ncols) { return 2 * GS_KC * pad_ld(ncols); }
+
+__device__ __forceinline__ void cp_async_commit_group() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int RB, int CB>
+__device__ void warp_gemm_staged(const double *A, int lda, const double *__restrict__ B, int ldb,
+                                 int K, int r0, int c0, int cstride, int ncols,
+                                 double (&acc)[RB][CB][2], double *Bs) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int ldbs = pad_ld(ncols), per_row = ncols / 2;
+  const int nch = (K + GS_KC - 1) / GS_KC;
+  auto stage = [&](int c) {
+    const int k0 = c * GS_KC, rows = min(GS_KC, K - k0);
+    double *dst = Bs + (c & 1) * GS_KC * ldbs;
+    for (int i = threadIdx.x; i < rows * per_row; i += blockDim.x) {
+      const int r = i / per_row, c2 = 2 * (i - r * per_row);
+      cp_async16(dst + r * ldbs + c2, B + (size_t)(k0 + r) * ldb + c2);
+    }
+    cp_async_commit_group();
+  };
+  stage(0);
+  const double *Ap = A + (r0 + g) * lda + q;
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) {
+      stage(c + 1);
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
+    __syncthreads();
+    const double *Bp = Bs + (c & 1) * GS_KC * ldbs + q * ldbs + c0 + g;
+    const int k0 = c * GS_KC, kn = min(GS_KC, K - k0);
+#pragma unroll 4
+    for (int k = 0; k < kn; k += 4) {
+      double a[RB], b[CB];
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb) a[rb] = Ap[8 * rb * lda + k0 + k];
+#pragma unroll
+      for (int cb = 0; cb < CB; ++cb)
+        b[cb] = (c0 + 8 * cb * cstride < ncols) ? Bp[k * ldbs + 8 * cb * cstride] : 0.0;
+#pragma unroll
+      for (int rb = 0; rb < RB; ++rb)
+#pragma unroll
+        for (int cb = 0; cb < CB; ++cb)
+          if (c0 + 8 * cb * cstride < ncols) dmma(acc[rb][cb], a[rb], b[cb]);
+    }
+    __syncthreads();  // buffer c & 1 is refilled by the next iteration's copies
+  }
+}
+
+// c2e_tile with U and VH streamed through Bs (gemm_stage_doubles(np))
+__device__ inline void c2e_tile_staged(const LevelOpsDev &op, int np, const double *P, double *T,
+                                       double *const *out_row, double *Bs) {
+  const int ldp = pad_ld(np);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int r0 = 8 * (warp & 3), c0 = 8 * (warp >> 2);
+  double acc[1][4][2];
+  zero_acc(acc);
+  warp_gemm_staged<1, 4>(P, ldp, op.u, np, np, r0, c0, 2, np, acc, Bs);
+#pragma unroll
+  for (int cb = 0; cb < 4; ++cb) {
+    const int col = c0 + 16 * cb + 2 * q;
+    if (col < np) {
+      T[(r0 + g) * ldp + col] = acc[0][cb][0] * __ldg(op.sinv + col);
+      T[(r0 + g) * ldp + col + 1] = acc[0][cb][1] * __ldg(op.sinv + col + 1);
+    }
+  }
+  __syncthreads();
+  zero_acc(acc);
+  warp_gemm_staged<1, 4>(T, ldp, op.vh, np, np, r0, c0, 2, np, acc, Bs);
+  double *o = out_row[r0 + g];
+  if (o) {
+#pragma unroll
+    for (int cb = 0; cb < 4; ++cb) {
+      const int col = c0 + 16 * cb + 2 * q;
+      if (col < np) *reinterpret_cast<double2 *>(o + col) = make_double2(acc[0][cb][0], acc[0][cb][1]);
+    }
+  }
+}
+
 }  // namespace fmmb
