@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *_
   const int ldp = pad_ld(np), ldw = pad_ld(32);
   double *G = smem;            // [TM][ldp] gathered source multipoles
   double *W = G + TM * ldp;    // [TM][ldw] SVD intermediate (rank <= 32)
+  double *Bs = W + TM * ldw;   // operators streamed through (gemm_stage_doubles(np))
   __shared__ int tgt[TM], srow[TM];
   // this block's (level, parity class, range of real groups)
   int slot = 0;
@@ -307,13 +308,13 @@ __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *_
     }
     __syncthreads();
     if (kind == M2L_DENSE) {
-      warp_gemm<2, 4>(G, ldp, op.m2l[o], np, np, r0, c0, 2, np, acc);
+      warp_gemm_staged<2, 4>(G, ldp, op.m2l[o], np, np, r0, c0, 2, np, acc, Bs);
     } else {
       const int rp = op.rp[o];
       // stage 1: W[64][rp] = G . M1^T ; warp -> rows 8*warp + [0,8), column blocks 0..3
       double w[1][4][2];
       zero_acc(w);
-      warp_gemm<1, 4>(G, ldp, op.m2l[o], rp, np, 8 * warp, 0, 1, rp, w);
+      warp_gemm_staged<1, 4>(G, ldp, op.m2l[o], rp, np, 8 * warp, 0, 1, rp, w, Bs);
 #pragma unroll
       for (int cb = 0; cb < 4; ++cb) {
         const int col = 8 * cb + 2 * q;
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *_
       }
       __syncthreads();
       // stage 2: acc += W . M2^T
-      warp_gemm<2, 4>(W, ldw, op.m2l[o] + (size_t)np * rp, np, rp, r0, c0, 2, np, acc);
+      warp_gemm_staged<2, 4>(W, ldw, op.m2l[o] + (size_t)np * rp, np, rp, r0, c0, 2, np, acc, Bs);
     }
     __syncthreads();
   }
@@ -950,8 +951,9 @@ void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s,
   }
   tl.tile_start[4 * th.L] = tiles;
   if (tiles == 0) return;
-  const size_t sm = sizeof(double) * (size_t)TM * (pad_ld(a.np) + pad_ld(32));
-  smem_limit(k_m2l, sizeof(double) * TM * (pad_ld(64) + pad_ld(32)));
+  const size_t sm =
+      sizeof(double) * ((size_t)TM * (pad_ld(a.np) + pad_ld(32)) + gemm_stage_doubles(a.np));
+  smem_limit(k_m2l, sizeof(double) * (TM * (pad_ld(64) + pad_ld(32)) + gemm_stage_doubles(64)));
   PhaseTimer timer(PH_M2L, s);
   k_m2l<<<dim3(tiles, n_rhs), NT, sm, s>>>(tl, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
                                            mult, ple, cstride);
