@@ -261,6 +261,21 @@ struct M2LTiles {
   int rg_cnt[FMM_MAX_LEVELS_DEV];
 };
 
+// One tile = 64 targets of one parity class of one level (the 27 offsets
+// that class can see).  The active offsets (an operator, and a source for
+// some target) are pipelined: the gathered source multipoles and the
+// offset's operators of offset a + 1 are copied into the second of two
+// shared buffers (cp.async) while the DMMA GEMMs of offset a run, so
+// neither the gather nor the operator reads wait on L2 inside the GEMM.
+// Dense offsets: acc += G . D^T; SVD offsets: W = G . M1^T, acc += W . M2^T.
+__host__ __device__ inline int m2l_op_doubles(int np) {
+  const int dense = np * pad_ld(np), svd = np * pad_ld(32) + 32 * pad_ld(np);
+  return dense > svd ? dense : svd;
+}
+__host__ __device__ inline size_t m2l_smem_doubles(int np) {
+  return (size_t)2 * TM * pad_ld(np) + (size_t)TM * pad_ld(32) + 2 * (size_t)m2l_op_doubles(np);
+}
+
 __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *__restrict__ rg,
                                             const int *__restrict__ il,
                                             const LevelOpsDev *__restrict__ ops,
@@ -269,52 +284,111 @@ __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *_
   mult += blockIdx.y * cstride;  // charge column blockIdx.y
   ple += blockIdx.y * cstride;
   extern __shared__ double smem[];
-  const int ldp = pad_ld(np), ldw = pad_ld(32);
-  double *G = smem;            // [TM][ldp] gathered source multipoles
-  double *W = G + TM * ldp;    // [TM][ldw] SVD intermediate (rank <= 32)
-  double *Bs = W + TM * ldw;   // operators streamed through (gemm_stage_doubles(np))
-  __shared__ int tgt[TM], srow[TM];
+  const int ldp = pad_ld(np), ldw = pad_ld(32), ldb = pad_ld(np);
+  double *Gb[2] = {smem, smem + TM * ldp};   // [TM][ldp] gathered source multipoles
+  double *W = smem + 2 * TM * ldp;           // [TM][ldw] SVD intermediate (rank <= 32)
+  double *Ob[2] = {W + TM * ldw, W + TM * ldw + m2l_op_doubles(np)};  // the offset's operators
+  __shared__ int tgt[TM];
+  __shared__ int s_src[27][TM];  // source node per class offset and target row
+  __shared__ int s_act[27];      // active class offsets, in order
+  __shared__ int s_nact;
+  __shared__ unsigned int s_mask;
   // this block's (level, parity class, range of real groups)
   int slot = 0;
   while (slot + 1 < 4 * tiles.n_levels && tiles.tile_start[slot + 1] <= (int)blockIdx.x) ++slot;
   const int m = slot >> 2, cls = slot & 3;
   const int q0 = TM * (blockIdx.x - tiles.tile_start[slot]);
   const int nloc = min(TM, tiles.rg_cnt[m] - q0);
-  if (threadIdx.x < TM)
-    tgt[threadIdx.x] = (threadIdx.x < nloc) ? rg[tiles.rg_lo[m] + q0 + threadIdx.x] + cls : -1;
-  __syncthreads();
   const LevelOpsDev &op = ops[m];
+  if (threadIdx.x == 0) s_mask = 0u;
+  __syncthreads();
+  if (threadIdx.x < TM) {
+    const int tg = (threadIdx.x < nloc) ? rg[tiles.rg_lo[m] + q0 + threadIdx.x] + cls : -1;
+    tgt[threadIdx.x] = tg;
+    int sidx[27];  // all loads issued together
+#pragma unroll
+    for (int oi = 0; oi < 27; ++oi) {
+      const int o = c_class_off[cls][oi];
+      sidx[oi] = (tg >= 0 && op.kind[o] != M2L_NULL) ? __ldg(il + (size_t)tg * N_OFFSETS + o) : -1;
+    }
+    unsigned int mask = 0;
+#pragma unroll
+    for (int oi = 0; oi < 27; ++oi) {
+      s_src[oi][threadIdx.x] = sidx[oi];
+      if (sidx[oi] >= 0) mask |= 1u << oi;
+    }
+    mask = __reduce_or_sync(0xffffffffu, mask);
+    if ((threadIdx.x & 31) == 0) atomicOr(&s_mask, mask);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int oi = 0; oi < 27; ++oi)
+      if ((s_mask >> oi) & 1u) s_act[n++] = oi;
+    s_nact = n;
+  }
+  __syncthreads();
+  const int nact = s_nact;
+  // copies of active offset a into buffer set b (one cp.async group)
+  auto prefetch = [&](int a, int b) {
+    const int oi = s_act[a], o = c_class_off[cls][oi];
+    double *G = Gb[b], *O = Ob[b];
+    const int h = np / 2;
+    for (int i = threadIdx.x; i < TM * h; i += NT) {
+      const int t = i / h, k2 = 2 * (i - t * h);
+      const int src = s_src[oi][t];
+      if (src >= 0) {
+        cp_async16(G + t * ldp + k2, mult + (size_t)src * np + k2);
+      } else {
+        G[t * ldp + k2] = 0.0;
+        G[t * ldp + k2 + 1] = 0.0;
+      }
+    }
+    const double *B = op.m2l[o];
+    if (op.kind[o] == M2L_DENSE) {
+      for (int i = threadIdx.x; i < np * h; i += NT) {
+        const int r = i / h, c2 = 2 * (i - r * h);
+        cp_async16(O + r * ldb + c2, B + (size_t)r * np + c2);
+      }
+    } else {
+      const int rp = op.rp[o], hr = rp / 2, ld1 = pad_ld(rp);
+      for (int i = threadIdx.x; i < np * hr; i += NT) {  // M1^T [np][rp]
+        const int r = i / hr, c2 = 2 * (i - r * hr);
+        cp_async16(O + r * ld1 + c2, B + (size_t)r * rp + c2);
+      }
+      const double *B2 = B + (size_t)np * rp;
+      double *O2 = O + np * ld1;
+      for (int i = threadIdx.x; i < rp * h; i += NT) {  // M2^T [rp][np]
+        const int r = i / h, c2 = 2 * (i - r * h);
+        cp_async16(O2 + r * ldb + c2, B2 + (size_t)r * np + c2);
+      }
+    }
+    cp_async_commit_group();
+  };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
   // dense / stage-2 mapping: rows 16*(warp&3) + [0,16), column blocks 8*(warp>>2) + 16*cb
   const int r0 = 16 * (warp & 3), c0 = 8 * (warp >> 2);
   double acc[2][4][2];
   zero_acc(acc);
-  for (int oi = 0; oi < 27; ++oi) {
-    const int o = c_class_off[cls][oi];
-    const int kind = op.kind[o];
-    if (kind == M2L_NULL) continue;
-    int src = -1;
-    if (threadIdx.x < TM && tgt[threadIdx.x] >= 0) src = il[(size_t)tgt[threadIdx.x] * N_OFFSETS + o];
-    if (threadIdx.x < TM) srow[threadIdx.x] = src;
-    if (!__syncthreads_or(src >= 0)) continue;
-    // gather 64 rows of np doubles (zero rows where there is no source)
-    for (int i = threadIdx.x; i < TM * (np / 2); i += NT) {
-      const int t = i / (np / 2), k2 = 2 * (i % (np / 2));
-      const int s = srow[t];
-      double2 v = make_double2(0.0, 0.0);
-      if (s >= 0) v = *reinterpret_cast<const double2 *>(mult + (size_t)s * np + k2);
-      G[t * ldp + k2] = v.x;
-      G[t * ldp + k2 + 1] = v.y;
+  if (nact > 0) prefetch(0, 0);
+  for (int a = 0; a < nact; ++a) {
+    const int b = a & 1;
+    if (a + 1 < nact) {
+      prefetch(a + 1, b ^ 1);
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
     }
     __syncthreads();
-    if (kind == M2L_DENSE) {
-      warp_gemm_staged<2, 4>(G, ldp, op.m2l[o], np, np, r0, c0, 2, np, acc, Bs);
+    const int o = c_class_off[cls][s_act[a]];
+    if (op.kind[o] == M2L_DENSE) {
+      warp_gemm<2, 4, true>(Gb[b], ldp, Ob[b], ldb, np, r0, c0, 2, np, acc);
     } else {
-      const int rp = op.rp[o];
+      const int rp = op.rp[o], ld1 = pad_ld(rp);
       // stage 1: W[64][rp] = G . M1^T ; warp -> rows 8*warp + [0,8), column blocks 0..3
       double w[1][4][2];
       zero_acc(w);
-      warp_gemm_staged<1, 4>(G, ldp, op.m2l[o], rp, np, 8 * warp, 0, 1, rp, w, Bs);
+      warp_gemm<1, 4, true>(Gb[b], ldp, Ob[b], ld1, np, 8 * warp, 0, 1, rp, w);
 #pragma unroll
       for (int cb = 0; cb < 4; ++cb) {
         const int col = 8 * cb + 2 * q;
@@ -325,9 +399,9 @@ __global__ void __launch_bounds__(NT) k_m2l(M2LTiles tiles, int np, const int *_
       }
       __syncthreads();
       // stage 2: acc += W . M2^T
-      warp_gemm_staged<2, 4>(W, ldw, op.m2l[o] + (size_t)np * rp, np, rp, r0, c0, 2, np, acc, Bs);
+      warp_gemm<2, 4, true>(W, ldw, Ob[b] + np * ld1, ldb, rp, r0, c0, 2, np, acc);
     }
-    __syncthreads();
+    __syncthreads();  // buffer set b is refilled by the next iteration's copies
   }
 #pragma unroll
   for (int rb = 0; rb < 2; ++rb) {
@@ -951,9 +1025,8 @@ void run_m2l(const PassArgs &a, const double *mult, double *ple, cudaStream_t s,
   }
   tl.tile_start[4 * th.L] = tiles;
   if (tiles == 0) return;
-  const size_t sm =
-      sizeof(double) * ((size_t)TM * (pad_ld(a.np) + pad_ld(32)) + gemm_stage_doubles(a.np));
-  smem_limit(k_m2l, sizeof(double) * (TM * (pad_ld(64) + pad_ld(32)) + gemm_stage_doubles(64)));
+  const size_t sm = sizeof(double) * m2l_smem_doubles(a.np);
+  smem_limit(k_m2l, sizeof(double) * m2l_smem_doubles(64));
   PhaseTimer timer(PH_M2L, s);
   k_m2l<<<dim3(tiles, n_rhs), NT, sm, s>>>(tl, a.np, a.td->rg.get(), a.td->il.get(), a.ops_dev,
                                            mult, ple, cstride);
