@@ -8,7 +8,8 @@
 // gathered parent row, or for M2L the source multipole at offset b) and W_b
 // rows b kb .. (b+1) kb - 1 of the operator W, row-major [K][ldw].  A block
 // computes a 64 x 64 tile of Y with mma.sync.m8n8k4.f64 (FP64 DMMA), staging
-// 8-deep K chunks of X and W in shared memory with cp.async.  An input block
+// 16-deep K chunks of X and W in shared memory with cp.async, double buffered
+// (the next chunk in flight while the current one is multiplied).  An input block
 // that no row of the tile reads (an M2L offset absent for the whole tile) is
 // skipped: M2L tiles hold rows of one parity class (position inside the
 // parent), so the 13 offsets that class never sees cost nothing.
@@ -23,9 +24,9 @@ namespace {
 
 constexpr int RG_TM = 64;       // output rows per block
 constexpr int RG_TN = 64;       // output columns per block
-constexpr int RG_KC = 8;        // K chunk staged per step (2 mma k-steps)
+constexpr int RG_KC = 16;       // K chunk staged per step (4 mma k-steps)
 constexpr int RG_THREADS = 256;
-constexpr int RG_LDX = 12;      // shared row stride of the X chunk (conflict-free fragments)
+constexpr int RG_LDX = 20;      // shared row stride of the X chunk (conflict-free fragments)
 constexpr int RG_LDW = 72;      // shared row stride of the W chunk
 
 // ---- loaders ----
@@ -122,8 +123,10 @@ template <class Load, class Store>
 __global__ void __launch_bounds__(RG_THREADS) k_rowgemm(Load ld, Store st,
                                                        const double *__restrict__ W, int ldw,
                                                        int M, int kb) {
-  __shared__ __align__(16) double Xs[RG_TM * RG_LDX];
-  __shared__ __align__(16) double Ws[RG_KC * RG_LDW];
+  // two buffers of each chunk: chunk c + 1 of an input block is copied while
+  // chunk c is multiplied
+  __shared__ __align__(16) double Xs[2][RG_TM * RG_LDX];
+  __shared__ __align__(16) double Ws[2][RG_KC * RG_LDW];
   __shared__ int rid[RG_TM];
   __shared__ const double *rsrc[RG_TM];
   const int tile = blockIdx.x, c0 = blockIdx.y * RG_TN;
@@ -132,7 +135,7 @@ __global__ void __launch_bounds__(RG_THREADS) k_rowgemm(Load ld, Store st,
   const int r0 = 16 * (warp & 3), cw = 32 * (warp >> 2);
   double acc[2][4][2];
   zero_acc(acc);
-  const int nb = ld.nblk();
+  const int nb = ld.nblk(), nch = (kb + RG_KC - 1) / RG_KC;
   for (int blk = 0; blk < nb; ++blk) {
     const double *p = nullptr;
     __syncthreads();  // rid written; rsrc of the previous block read
@@ -142,41 +145,54 @@ __global__ void __launch_bounds__(RG_THREADS) k_rowgemm(Load ld, Store st,
       rsrc[threadIdx.x] = p;
     }
     if (!__syncthreads_or(p != nullptr)) continue;  // no row of the tile reads this block
-    for (int k0 = 0; k0 < kb; k0 += RG_KC) {
-      {  // X chunk: 64 rows x 8 doubles, 16 bytes per thread
-        const int r = threadIdx.x >> 2, pr = (threadIdx.x & 3) * 2;
+    auto stage = [&](int c) {  // chunk c of this block into buffer c & 1 (one copy group)
+      const int k0 = c * RG_KC, bf = c & 1, kn = min(RG_KC, kb - k0);
+      // X chunk: 64 rows x RG_KC doubles (rows past kb or without a source: 0)
+      for (int i = threadIdx.x; i < RG_TM * (RG_KC / 2); i += RG_THREADS) {
+        const int r = i / (RG_KC / 2), pr = 2 * (i - r * (RG_KC / 2));
         const double *s = rsrc[r];
-        if (s) {
-          cp_async16(&Xs[r * RG_LDX + pr], s + k0 + pr);
+        if (s && pr < kn) {
+          cp_async16(&Xs[bf][r * RG_LDX + pr], s + k0 + pr);
         } else {
-          Xs[r * RG_LDX + pr] = 0.0;
-          Xs[r * RG_LDX + pr + 1] = 0.0;
+          Xs[bf][r * RG_LDX + pr] = 0.0;
+          Xs[bf][r * RG_LDX + pr + 1] = 0.0;
         }
       }
-      {  // W chunk: 8 rows x 64 columns
-        const int kr = threadIdx.x >> 5, cc = (threadIdx.x & 31) * 2;
-        if (c0 + cc < M) {
-          cp_async16(&Ws[kr * RG_LDW + cc], W + (size_t)(blk * kb + k0 + kr) * ldw + c0 + cc);
+      // W chunk: RG_KC rows x 64 columns
+      for (int i = threadIdx.x; i < RG_KC * (RG_TN / 2); i += RG_THREADS) {
+        const int kr = i / (RG_TN / 2), cc = 2 * (i - kr * (RG_TN / 2));
+        if (kr < kn && c0 + cc < M) {
+          cp_async16(&Ws[bf][kr * RG_LDW + cc], W + (size_t)(blk * kb + k0 + kr) * ldw + c0 + cc);
         } else {
-          Ws[kr * RG_LDW + cc] = 0.0;
-          Ws[kr * RG_LDW + cc + 1] = 0.0;
+          Ws[bf][kr * RG_LDW + cc] = 0.0;
+          Ws[bf][kr * RG_LDW + cc + 1] = 0.0;
         }
       }
-      cp_async_wait_all();
+      cp_async_commit_group();
+    };
+    stage(0);
+    for (int c = 0; c < nch; ++c) {
+      if (c + 1 < nch) {
+        stage(c + 1);
+        cp_async_wait_group<1>();
+      } else {
+        cp_async_wait_group<0>();
+      }
       __syncthreads();
+      const double *X = Xs[c & 1], *Wc = Ws[c & 1];
 #pragma unroll
       for (int ks = 0; ks < RG_KC; ks += 4) {
         double a[2], b[4];
 #pragma unroll
-        for (int rb = 0; rb < 2; ++rb) a[rb] = Xs[(r0 + 8 * rb + g) * RG_LDX + ks + q];
+        for (int rb = 0; rb < 2; ++rb) a[rb] = X[(r0 + 8 * rb + g) * RG_LDX + ks + q];
 #pragma unroll
-        for (int cb = 0; cb < 4; ++cb) b[cb] = Ws[(ks + q) * RG_LDW + cw + 8 * cb + g];
+        for (int cb = 0; cb < 4; ++cb) b[cb] = Wc[(ks + q) * RG_LDW + cw + 8 * cb + g];
 #pragma unroll
         for (int rb = 0; rb < 2; ++rb)
 #pragma unroll
           for (int cb = 0; cb < 4; ++cb) dmma(acc[rb][cb], a[rb], b[cb]);
       }
-      __syncthreads();
+      __syncthreads();  // buffer c & 1 is refilled by the next iteration's copies
     }
   }
 #pragma unroll
