@@ -390,10 +390,15 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 // Tiles of 128 targets of one parity class (MMA M = 128).  Per offset, the
 // gathered source multipoles (A: 128 x K, read pre-split as TF32 hi / lo
 // from the upward pass's mult_tc rows) and the deflated operator (B: N x K,
-// N = NP rounded up to 16) sit in shared memory in the K-major core-matrix
-// layout (8 rows x 16 bytes per core matrix, core matrices along K
-// contiguous: LBO = 128 B, SBO = NP/4 * 128 B) and are multiplied by
-// tcgen05.mma kind::tf32 into tensor memory.  Each k-step's three split
+// N = NP rounded up to 16) sit in shared memory in the K-major 128-byte
+// swizzle layout (one 128-byte row per target or operator row, 16-byte
+// chunk c of row r at chunk c ^ (r & 7), 8-row groups 1024 bytes apart) and
+// are multiplied by tcgen05.mma kind::tf32 into tensor memory.  Producer
+// thread r copies target row r's gathered chunks; the swizzle puts a warp's
+// 32 rows' chunk k in distinct banks.  (Measured at 1M: 0.152 ms against
+// 0.158 for the unswizzled core-matrix layout; copies ordered so consecutive
+// threads take consecutive chunks of one row took 0.178, and 4 TMEM buffers
+// or a copy lag of 3 changed nothing.)  Each k-step's three split
 // products (lo.hi, hi.lo, hi.hi) go to their own 32 TMEM columns (the tensor
 // cores truncate their FP32 accumulation); the k-step slots are added in
 // FP32 (round to nearest) and the result into FP64 registers.
@@ -409,12 +414,13 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 //   mdone[b]  TMEM buffer b written (tcgen05.commit)
 //   tfree[b]  TMEM buffer b read    (128 epilogue arrivals)
 // Use u of the pipeline (a running count of offsets over the CTA's tiles)
-// takes stage u % 5 and buffer u % 2; each barrier's k-th completion has
+// takes stage u % 5 and buffer u % TC_NBUF; each barrier's k-th completion has
 // parity k & 1.  Every wait is bounded: one that runs out sets the plan's
 // error flag and the CTA stops, after letting its copies and MMAs land.
 constexpr int TCM = 128;       // targets per tile = MMA M
 constexpr int TC_MAX_NP = 32;  // up to 4 k-steps x 32 TMEM columns per buffer
-constexpr int TC_COLS = 256;   // TMEM columns per CTA (2 buffers x 128)
+constexpr int TC_NBUF = 2;     // TMEM accumulator buffers (128 columns each)
+constexpr int TC_COLS = 128 * TC_NBUF;  // TMEM columns per CTA (a power of 2)
 constexpr int TC_STAGES = 5;   // operand stages in shared memory
 // producer: an offset is announced once the copies TC_LAG offsets later are
 // issued; a stage is refilled TC_STAGES - TC_LAG - 1 offsets after its MMAs
@@ -426,16 +432,22 @@ constexpr uint32_t TC_MAX_TRIES = 1u << 20;
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_lag() {
-  static_assert(TC_LAG == 2, "wait_group takes the lag as an immediate");
-  asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+  static_assert(TC_LAG >= 1 && TC_LAG <= 4, "wait_group takes the lag as an immediate");
+  if (TC_LAG == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+  if (TC_LAG == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+  if (TC_LAG == 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+  if (TC_LAG == 4) asm volatile("cp.async.wait_group 4;\n" ::: "memory");
 }
 
-// shared memory of one operand stage: A hi, A lo, B hi, B lo
-size_t m2l_tc_stage_bytes(int np) {
-  const size_t ntc = (np + 15) & ~15;
-  const size_t a_sz = (size_t(TCM) * np * 4 + 1023) & ~size_t(1023);
-  const size_t b_sz = (ntc * np * 4 + 1023) & ~size_t(1023);
-  return 2 * a_sz + 2 * b_sz;
+// shared memory of one operand stage: A hi, A lo, B hi, B lo (128-byte
+// rows, each part 1024-byte aligned)
+__host__ __device__ inline uint32_t m2l_tc_a_bytes() { return uint32_t(TCM) * 128u; }
+__host__ __device__ inline uint32_t m2l_tc_b_bytes(int np) {
+  return ((uint32_t((np + 15) & ~15) * 128u) + 1023u) & ~1023u;
+}
+// dynamic shared memory: the stages and slack to align them to 1024 bytes
+size_t m2l_tc_smem_bytes(int np) {
+  return size_t(TC_STAGES) * (2 * m2l_tc_a_bytes() + 2 * m2l_tc_b_bytes(np)) + 1024;
 }
 
 __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int n_tiles, int neq,
@@ -448,7 +460,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
                                                          int *tile_counter) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_sfree[TC_STAGES];
-  __shared__ __align__(8) uint64_t bar_mdone[2], bar_tfree[2], bar_drain;
+  __shared__ __align__(8) uint64_t bar_mdone[TC_NBUF], bar_tfree[TC_NBUF], bar_drain;
   __shared__ uint32_t tmem_base;
   __shared__ int s_src[27][TCM];  // source node per class offset and target row
   __shared__ int s_act[27];       // offsets with work, in class order
@@ -459,16 +471,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
   const int tid = threadIdx.x, warp = tid >> 5;
   const int ntc = (np + 15) & ~15;
   const int nks = np / 8, nk4 = np / 4;
-  const uint32_t a_sz = (uint32_t(TCM) * np * 4 + 1023u) & ~1023u;
-  const uint32_t b_sz = (uint32_t(ntc) * np * 4 + 1023u) & ~1023u;
+  const uint32_t a_sz = m2l_tc_a_bytes(), b_sz = m2l_tc_b_bytes(np);
   const uint32_t st_sz = 2 * a_sz + 2 * b_sz;
+  // the stages, 1024-byte aligned (the swizzle follows address bits 4-9)
+  unsigned char *const stages = smraw + ((1024u - (tc::smem_u32(smraw) & 1023u)) & 1023u);
   if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_base), TC_COLS);
   if (tid == 0) {
     for (int st = 0; st < TC_STAGES; ++st) {
       tc::mbar_init(tc::smem_u32(&bar_full[st]), TC_PROD);
       tc::mbar_init(tc::smem_u32(&bar_sfree[st]), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < TC_NBUF; ++b) {
       tc::mbar_init(tc::smem_u32(&bar_mdone[b]), 1);
       tc::mbar_init(tc::smem_u32(&bar_tfree[b]), TC_EPI);
     }
@@ -482,7 +495,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
   tc::fence_after_sync();
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = tc::idesc_tf32(TCM, ntc);
-  const uint32_t lbo = 128, sbo = uint32_t(nk4) * 128;
   const int units = ntc * nk4;  // 16-byte chunks of one B part
   auto fail = [&] {
     s_abort = 1;
@@ -544,8 +556,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
       }
       for (int a = 0; a < nact; ++a) {
         if (__any_sync(0xffffffffu, s_abort)) break;
-        const uint32_t u = gu + a, b = u & 1u;
-        const bool ok = tc::mbar_wait(tc::smem_u32(&bar_mdone[b]), (u >> 1) & 1u, TC_MAX_TRIES);
+        const uint32_t u = gu + a, b = u % TC_NBUF;
+        const bool ok = tc::mbar_wait(tc::smem_u32(&bar_mdone[b]), (u / TC_NBUF) & 1u, TC_MAX_TRIES);
         if (!__all_sync(0xffffffffu, ok)) {
           fail();
           break;
@@ -582,26 +594,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
           break;
         }
         const int oi = s_act[a], o = c_class_off_mx[cls][oi];
+        unsigned char *sp = stages + st * st_sz;
+        // row r of A (hi, lo): its 16-byte chunks to swizzled positions
         const int src = s_src[oi][r];
-        unsigned char *sp = smraw + st * st_sz;
-        unsigned char *ah = sp, *al = sp + a_sz;
         for (int k4 = 0; k4 < nk4; ++k4) {
-          const uint32_t off = uint32_t((r >> 3) * nk4 + k4) * 128u + uint32_t(r & 7) * 16u;
+          unsigned char *dh = sp + tc::sw128_offset(r, k4), *dl = dh + a_sz;
           if (src >= 0) {
-            const float *row = mult_tc + (size_t)src * 2 * np;
-            cp_async16(ah + off, row + 4 * k4);
-            cp_async16(al + off, row + np + 4 * k4);
+            cp_async16(dh, mult_tc + (size_t)src * 2 * np + 4 * k4);
+            cp_async16(dl, mult_tc + (size_t)src * 2 * np + np + 4 * k4);
           } else {
-            *reinterpret_cast<float4 *>(ah + off) = make_float4(0.f, 0.f, 0.f, 0.f);
-            *reinterpret_cast<float4 *>(al + off) = make_float4(0.f, 0.f, 0.f, 0.f);
+            *reinterpret_cast<float4 *>(dh) = make_float4(0.f, 0.f, 0.f, 0.f);
+            *reinterpret_cast<float4 *>(dl) = make_float4(0.f, 0.f, 0.f, 0.f);
           }
         }
         for (int q = r; q < 2 * units; q += TC_PROD) {
           const int part = q >= units, qq = part ? q - units : q;
           const int n = qq / nk4, k4 = qq - (qq / nk4) * nk4;
           const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
-          const uint32_t off = uint32_t((n >> 3) * nk4 + k4) * 128u + uint32_t(n & 7) * 16u;
-          cp_async16(sp + 2 * a_sz + part * b_sz + off, bsrc + (size_t)n * np + 4 * k4);
+          cp_async16(sp + 2 * a_sz + part * b_sz + tc::sw128_offset(n, k4), bsrc + (size_t)n * np + 4 * k4);
         }
         cp_async_commit();
         if (a >= TC_LAG) {  // the copies of offset a - TC_LAG have landed: announce them
@@ -620,26 +630,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
       // ---- MMA issue ----
       for (int a = 0; a < nact; ++a) {
         if (s_abort) break;
-        const uint32_t u = gu + a, st = u % TC_STAGES, b = u & 1u;
+        const uint32_t u = gu + a, st = u % TC_STAGES, b = u % TC_NBUF;
         if (!tc::mbar_wait(tc::smem_u32(&bar_full[st]), (u / TC_STAGES) & 1u, TC_MAX_TRIES)) {
           fail();
           break;
         }
-        if (u >= 2 &&
-            !tc::mbar_wait(tc::smem_u32(&bar_tfree[b]), ((u >> 1) - 1) & 1u, TC_MAX_TRIES)) {
+        if (u >= uint32_t(TC_NBUF) &&
+            !tc::mbar_wait(tc::smem_u32(&bar_tfree[b]), ((u / TC_NBUF) - 1) & 1u, TC_MAX_TRIES)) {
           fail();
           break;
         }
         tc::fence_after_sync();
-        unsigned char *sp = smraw + st * st_sz;
+        unsigned char *sp = stages + st * st_sz;
         for (int ks = 0; ks < nks; ++ks) {
           const uint32_t d = tmem + b * 128u + uint32_t(ks * 32);
 #pragma unroll
           for (int p = 0; p < 3; ++p) {  // lo.hi, hi.lo, hi.hi
             const int apart = p == 0 ? 1 : 0, bpart = p == 1 ? 1 : 0;
-            const uint64_t ad = tc::desc_kmajor(tc::smem_u32(sp + apart * a_sz) + ks * 256u, lbo, sbo);
-            const uint64_t bd =
-                tc::desc_kmajor(tc::smem_u32(sp + 2 * a_sz + bpart * b_sz) + ks * 256u, lbo, sbo);
+            const uint64_t ad = tc::desc_sw128(tc::smem_u32(sp + apart * a_sz) + ks * 32u);
+            const uint64_t bd = tc::desc_sw128(tc::smem_u32(sp + 2 * a_sz + bpart * b_sz) + ks * 32u);
             tc::mma_tf32(d, ad, bd, idesc, p > 0 ? 1u : 0u);
           }
         }
@@ -1287,7 +1296,7 @@ void run_m2l_mixed(const PassArgs &a, const float *mult32, const float *mult_tc,
     tc.tile_start[4 * th.L] = ctiles;
     // persistent: one CTA per SM (its shared memory admits no second one),
     // each walking tiles blockIdx.x, blockIdx.x + gridDim.x, ...
-    const size_t sm = TC_STAGES * m2l_tc_stage_bytes(a.np);
+    const size_t sm = m2l_tc_smem_bytes(a.np);
     smem_limit(k_m2l_tc, sm);
     int dev = 0, sms = 0;
     FMMB_CUDA(cudaGetDevice(&dev));

@@ -24,6 +24,26 @@ __device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, ui
   return d;                // base offset 0, no swizzle (layout type 0)
 }
 
+// Shared-memory descriptor of a K-major operand in the 128-byte swizzle
+// layout: rows of 128 bytes, 8-row groups 1024 bytes apart (SBO), the tile
+// 1024-byte aligned, 16-byte chunk c of row r stored at chunk c ^ (r & 7).
+// A K step inside the 128-byte row advances the start address (32 bytes per
+// 8 TF32 values); the leading byte offset is unused in this layout.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFFu);
+  d |= uint64_t(1) << 16;
+  d |= uint64_t(1024 >> 4) << 32;
+  d |= uint64_t(1) << 46;  // descriptor version used by tcgen05
+  d |= uint64_t(2) << 61;  // layout type: 128-byte swizzle
+  return d;
+}
+
+// byte offset of 16-byte chunk c of row r in a 128-byte-swizzled tile
+__device__ __forceinline__ uint32_t sw128_offset(int r, int c) {
+  return uint32_t(r) * 128u + uint32_t((c ^ (r & 7)) * 16);
+}
+
 // Instruction descriptor, kind::tf32: D = F32, A = B = TF32, both K-major.
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
