@@ -45,6 +45,13 @@ __constant__ int8_t c_class_off_mx[4][27] = {
     {1, 2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 15, 16, 17, 19, 20, 21, 23, 24, 25, 27, 28, 29, 30, 31, 32},
     {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12, 14, 15, 16, 18, 19, 20, 22, 23, 24, 26, 27, 28, 29, 30, 31}};
 
+// the inverse: class position of offset o in class cls, or -1
+__constant__ int8_t c_oi_of_mx[4][40] = {
+    {-1, -1, -1, -1, -1, -1, -1, -1, 0, 1, 2, 3, 4, 5, -1, 6, 7, 8, -1, 9, 10, 11, -1, 12, 13, 14, -1, 15, 16, 17, 18, 19, 20, -1, 21, 22, 23, 24, 25, 26},
+    {-1, -1, -1, -1, -1, -1, -1, 0, 1, 2, 3, 4, 5, -1, 6, 7, 8, -1, 9, 10, 11, -1, 12, 13, 14, -1, 15, 16, 17, 18, 19, 20, -1, 21, 22, 23, 24, 25, 26, -1},
+    {-1, 0, 1, 2, 3, 4, 5, -1, 6, 7, 8, 9, 10, 11, -1, 12, 13, 14, -1, 15, 16, 17, -1, 18, 19, 20, -1, 21, 22, 23, 24, 25, 26, -1, -1, -1, -1, -1, -1, -1},
+    {0, 1, 2, 3, 4, 5, -1, 6, 7, 8, 9, 10, 11, -1, 12, 13, 14, -1, 15, 16, 17, -1, 18, 19, 20, -1, 21, 22, 23, 24, 25, 26, -1, -1, -1, -1, -1, -1, -1, -1}};
+
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -395,10 +402,19 @@ __global__ void __launch_bounds__(128) k_m2l_mx(M2LTilesMx tiles, int neq, int n
 // chunk c of row r at chunk c ^ (r & 7), 8-row groups 1024 bytes apart) and
 // are multiplied by tcgen05.mma kind::tf32 into tensor memory.  Producer
 // thread r copies target row r's gathered chunks; the swizzle puts a warp's
-// 32 rows' chunk k in distinct banks.  (Measured at 1M: 0.152 ms against
-// 0.158 for the unswizzled core-matrix layout; copies ordered so consecutive
-// threads take consecutive chunks of one row took 0.178, and 4 TMEM buffers
-// or a copy lag of 3 changed nothing.)  Each k-step's three split
+// 32 rows' chunk k in distinct banks.
+//
+// Measured at 1M (clustered, Nequiv 24; M2L phase): 0.158 ms with the
+// unswizzled core-matrix layout, 0.152 swizzled, 0.131 with the per-tile
+// set-up loading whole interaction rows and the operator table once and the
+// epilogue reading its k-step slots in one TMEM load.  Per-role clock
+// counters show the producers issuing ~1600 cycles per offset (the copies'
+// issue, not their waits), with the MMA lane waiting on them ~25% of the
+// time.  Tried without gain: copies ordered so consecutive threads take
+// consecutive chunks of one row (0.150), sources read from a small hot
+// window (same time: not an L2 cost), tile::gather4 TMA loads of the rows
+// (0.24), 4 TMEM buffers, a copy lag of 3, per-tile rotation of the offset
+// order (0.138), per-warp instead of per-thread mbarrier arrivals (0.138).  Each k-step's three split
 // products (lo.hi, hi.lo, hi.hi) go to their own 32 TMEM columns (the tensor
 // cores truncate their FP32 accumulation); the k-step slots are added in
 // FP32 (round to nearest) and the result into FP64 registers.
@@ -439,6 +455,20 @@ __device__ __forceinline__ void cp_async_wait_lag() {
   if (TC_LAG == 4) asm volatile("cp.async.wait_group 4;\n" ::: "memory");
 }
 
+// sum of a TMEM buffer's NK k-step slots (32 columns each), in k order
+template <int NK>
+__device__ __forceinline__ void tmem_slot_sum(uint32_t taddr, float (&sum)[32]) {
+  float v[NK][32];
+  tc::tmem_ld32_slots<NK>(taddr, v);
+#pragma unroll
+  for (int c = 0; c < 32; ++c) {
+    float t = v[0][c];
+#pragma unroll
+    for (int k = 1; k < NK; ++k) t += v[k][c];
+    sum[c] = t;
+  }
+}
+
 // shared memory of one operand stage: A hi, A lo, B hi, B lo (128-byte
 // rows, each part 1024-byte aligned)
 __host__ __device__ inline uint32_t m2l_tc_a_bytes() { return uint32_t(TCM) * 128u; }
@@ -464,6 +494,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
   __shared__ uint32_t tmem_base;
   __shared__ int s_src[27][TCM];  // source node per class offset and target row
   __shared__ int s_act[27];       // offsets with work, in class order
+  __shared__ const float *s_bop[2][N_OFFSETS];  // the level's operators (hi, lo) per offset
+  __shared__ double s_c[N_OFFSETS];             // and their means
   __shared__ int s_nact;
   __shared__ unsigned int s_mask;
   __shared__ volatile int s_abort;
@@ -513,20 +545,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
     int tg = -1;
     if (tid < TC_EPI) {
       // this tile's offsets that have an operator and a source for some
-      // target, and every target's source per offset
+      // target, and every target's source per offset: the target's whole
+      // interaction row in ten 16-byte loads, the class's 27 kept
       tg = tid < nloc ? rg[tiles.rg_lo[m] + q0 + tid] + cls : -1;
-      // all 27 (kind, interaction) loads issued together, not one after another
-      int sidx[27];
-#pragma unroll
-      for (int oi = 0; oi < 27; ++oi) {
-        const int o = c_class_off_mx[cls][oi];
-        sidx[oi] = (tg >= 0 && __ldg(&op.kind[o]) != M2L_NULL) ? __ldg(il + (size_t)tg * N_OFFSETS + o) : -1;
+      if (tid < 2 * N_OFFSETS) {  // the operators' addresses and means, beside the loads
+        const int o = tid % N_OFFSETS;
+        s_bop[tid / N_OFFSETS][o] = tid < N_OFFSETS ? op.m2l_tc_hi[o] : op.m2l_tc_lo[o];
+        if (tid < N_OFFSETS) s_c[o] = op.c_m2l[o];
       }
+      const int4 *ilr = reinterpret_cast<const int4 *>(il + (size_t)max(tg, 0) * N_OFFSETS);
       unsigned int mask = 0;
 #pragma unroll
-      for (int oi = 0; oi < 27; ++oi) {
-        s_src[oi][tid] = sidx[oi];
-        if (sidx[oi] >= 0) mask |= 1u << oi;
+      for (int i = 0; i < N_OFFSETS / 4; ++i) {
+        const int4 q4 = tg >= 0 ? __ldg(ilr + i) : make_int4(-1, -1, -1, -1);
+        const int q[4] = {q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int o = 4 * i + j, oi = c_oi_of_mx[cls][o];
+          if (oi >= 0) {
+            const int v = __ldg(&op.kind[o]) != M2L_NULL ? q[j] : -1;
+            s_src[oi][tid] = v;
+            if (v >= 0) mask |= 1u << oi;
+          }
+        }
       }
       mask = __reduce_or_sync(0xffffffffu, mask);
       if ((tid & 31) == 0) atomicOr(&s_mask, mask);
@@ -552,7 +593,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
 #pragma unroll 4
       for (int a = 0; a < nact; ++a) {
         const int oi = s_act[a], src = s_src[oi][tid];
-        if (src >= 0) r1 += op.c_m2l[c_class_off_mx[cls][oi]] * __ldg(msum + src);
+        if (src >= 0) r1 += s_c[c_class_off_mx[cls][oi]] * __ldg(msum + src);
       }
       for (int a = 0; a < nact; ++a) {
         if (__any_sync(0xffffffffu, s_abort)) break;
@@ -564,11 +605,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
         }
         tc::fence_after_sync();
         float sum[32];
-        for (int ks = 0; ks < nks; ++ks) {
-          float v[32];
-          tc::tmem_ld32(tmem + (uint32_t(32 * warp) << 16) + b * 128u + uint32_t(ks * 32), v);
+        const uint32_t ta = tmem + (uint32_t(32 * warp) << 16) + b * 128u;
+        if (nks == 3) {  // Nequiv 21-24: the three k-step slots in one load
+          tmem_slot_sum<3>(ta, sum);
+        } else {  // added in k order either way
+          for (int ks = 0; ks < nks; ++ks) {
+            float v[32];
+            tc::tmem_ld32(ta + uint32_t(ks * 32), v);
 #pragma unroll
-          for (int c = 0; c < 32; ++c) sum[c] = ks == 0 ? v[c] : sum[c] + v[c];
+            for (int c = 0; c < 32; ++c) sum[c] = ks == 0 ? v[c] : sum[c] + v[c];
+          }
         }
         tc::fence_before_sync();
         tc::mbar_arrive(tc::smem_u32(&bar_tfree[b]));
@@ -610,7 +656,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(M2LTilesMx tiles, int 
         for (int q = r; q < 2 * units; q += TC_PROD) {
           const int part = q >= units, qq = part ? q - units : q;
           const int n = qq / nk4, k4 = qq - (qq / nk4) * nk4;
-          const float *bsrc = part ? op.m2l_tc_lo[o] : op.m2l_tc_hi[o];
+          const float *bsrc = s_bop[part][o];
           cp_async16(sp + 2 * a_sz + part * b_sz + tc::sw128_offset(n, k4), bsrc + (size_t)n * np + 4 * k4);
         }
         cp_async_commit();
