@@ -56,6 +56,7 @@ struct Counters {
   unsigned int bar_count;  // grid barrier of the cooperative balance kernel
   unsigned int bar_gen;
   int bar_timeout;
+  int sort_fail;  // copy of the tree's sort failure flag, read back with the counts
 };
 
 // The source keys are first sorted on their top SORT_DIGITS digits only; that
@@ -276,10 +277,14 @@ __global__ void k_split_counts(const uint64_t *__restrict__ keys, int64_t n, int
 __global__ void k_split_emit(const uint64_t *__restrict__ keys, int64_t n, int ppl,
                              const unsigned long long *__restrict__ counts,
                              const unsigned long long *__restrict__ pos, uint64_t *__restrict__ out,
-                             unsigned long long cap, Counters *cnt, int max_split) {
+                             unsigned long long cap, Counters *cnt, int max_split,
+                             const int *__restrict__ sort_fail) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    if (i == n - 1) cnt->s0_count = pos[i] + counts[i];
+    if (i == n - 1) {
+      cnt->s0_count = pos[i] + counts[i];
+      cnt->sort_fail = *sort_fail;  // the point sort and the scan ran before
+    }
     if (!counts[i]) continue;
     int cprev, cnext;
     split_range(keys, n, ppl, i, cprev, cnext, max_split);
@@ -354,9 +359,11 @@ __device__ bool grid_sync(Counters *cnt, unsigned long long *snap) {
 __global__ void __launch_bounds__(TPB) k_balance_xlist(
     int mtop, int L, const uint64_t *__restrict__ s0, int64_t n0, const int *__restrict__ s0b,
     uint64_t *forced, unsigned long long *fb, unsigned long long capf, uint64_t *xl,
-    unsigned long long capx, uint64_t *tab, uint64_t mask, Counters *cnt) {
+    unsigned long long capx, uint64_t *tab, uint64_t mask, Counters *cnt,
+    const int *sort_fail) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+  if (tid == 0) cnt->sort_fail = __ldcg(sort_fail);  // the split-box sort ran before
   for (int64_t i = tid; i < n0; i += nthr)
     if (hash_insert(tab, mask, s0[i]) < 0) atomicExch(&cnt->overflow, 1);
   if (!grid_sync(cnt, nullptr)) return;
@@ -457,9 +464,12 @@ __global__ void k_parent_decode(const uint64_t *__restrict__ keys, int64_t n, in
 }
 
 // real sibling groups: the children of split boxes (not of X-list leaves)
+// (rgb[L + 1]: the tree's sort failure flag, read back with the bounds)
 __global__ void k_real_bounds(const int *__restrict__ pos, const int *__restrict__ real, int64_t n,
-                              const int *__restrict__ pb, int L, int *__restrict__ rgb) {
+                              const int *__restrict__ pb, int L, int *__restrict__ rgb,
+                              const int *__restrict__ sort_fail) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l == L + 1) rgb[l] = *sort_fail;
   if (l > L) return;
   const int total = n ? pos[n - 1] + real[n - 1] : 0;
   rgb[l] = (pb[l] < n) ? pos[pb[l]] : total;
@@ -781,15 +791,12 @@ void pinned_release(int *p) {
   g_pinned_free.push_back(p);
 }
 
-// the counts and, after them, the tree's sort failure flag
-void begin_pending_counts(TreeHost &th, const int *dev_counts, int count, const int *dev_fail,
-                          cudaStream_t s) {
+// the counts and, after them (dev_counts[count]), the tree's sort failure flag
+void begin_pending_counts(TreeHost &th, const int *dev_counts, int count, cudaStream_t s) {
   FMMB_CHECK(count + 1 <= PINNED_INTS, ERR_INVALID_ARGUMENT, "too many levels");
   if (!th.pending_counts) th.pending_counts = pinned_acquire();
   if (!th.ready) FMMB_CUDA(cudaEventCreateWithFlags(&th.ready, cudaEventDisableTiming));
-  FMMB_CUDA(cudaMemcpyAsync(th.pending_counts, dev_counts, count * sizeof(int),
-                            cudaMemcpyDeviceToHost, s));
-  FMMB_CUDA(cudaMemcpyAsync(th.pending_counts + count, dev_fail, sizeof(int),
+  FMMB_CUDA(cudaMemcpyAsync(th.pending_counts, dev_counts, (count + 1) * sizeof(int),
                             cudaMemcpyDeviceToHost, s));
   FMMB_CUDA(cudaEventRecord(th.ready, s));
   th.pending = true;
@@ -916,7 +923,14 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
 
   DevBuf<Counters> cnt;
   cnt.alloc(1, s);
-  Counters hc;
+  // the counters come back through a pinned block: one copy per host wait
+  static_assert(sizeof(Counters) <= PINNED_INTS * sizeof(int), "pinned block too small");
+  std::unique_ptr<int, void (*)(int *)> hblk(pinned_acquire(), pinned_release);
+  Counters &hc = *reinterpret_cast<Counters *>(hblk.get());
+  auto read_counters = [&] {
+    FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+  };
   const unsigned long long cap0 = (unsigned long long)MAXD * (n / (ppl + 1) + 1) + 64;
   DevBuf<uint64_t> s0raw, s0;
   DevBuf<unsigned long long> scount, spos;
@@ -929,7 +943,6 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   td.sy.alloc(n, s);
   td.sort_fail.alloc(1, s);
   td.sort_fail.zero(s);
-  int hfail = 0;
   for (int digits = SORT_DIGITS;; digits = MAXD) {
     sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits, td.sx.get(), td.sy.get(),
                 td.sort_fail.get());
@@ -940,12 +953,11 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     // (k_split_emit checks its writes against the capacity)
     exclusive_sum(scount.get(), spos.get(), n, td.sort_fail.get(), false, s);
     k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
-                                                   s0raw.get(), cap0, cnt.get(), max_split);
+                                                   s0raw.get(), cap0, cnt.get(), max_split,
+                                                   td.sort_fail.get());
     FMMB_CUDA(cudaGetLastError());
-    FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
-    FMMB_CUDA(cudaMemcpyAsync(&hfail, td.sort_fail.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMMB_CUDA(cudaStreamSynchronize(s));
-    FMMB_CHECK(!hfail, ERR_CUDA, "point sort: a grid barrier wait ran out of time");
+    read_counters();
+    FMMB_CHECK(!hc.sort_fail, ERR_CUDA, "point sort: a grid barrier wait ran out of time");
     FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
                "more than Ncutoff points share a box of width bbox/2^29 (coincident points?)");
     FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
@@ -997,16 +1009,16 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
         uint64_t mask = hcap - 1;
         Counters *cp = cnt.get();
         int64_t n0k = n0;
-        void *args[] = {&mtop, &Lk, &s0p, &n0k, &s0bp, &fp, &fbp, &capf, &xp, &capx, &tp, &mask, &cp};
+        const int *sfp = td.sort_fail.get();
+        void *args[] = {&mtop, &Lk, &s0p, &n0k, &s0bp, &fp, &fbp, &capf, &xp, &capx, &tp, &mask, &cp,
+                        &sfp};
         FMMB_CUDA(cudaLaunchCooperativeKernel((const void *)k_balance_xlist,
                                               cooperative_grid((const void *)k_balance_xlist, TPB),
                                               TPB, args, 0, s));
       }
-      FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
-      FMMB_CUDA(cudaMemcpyAsync(&hfail, td.sort_fail.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-      FMMB_CUDA(cudaStreamSynchronize(s));
+      read_counters();
       FMMB_CHECK(!hc.bar_timeout, ERR_CUDA, "tree balance: a grid barrier wait ran out of time");
-      FMMB_CHECK(!hfail, ERR_CUDA, "split-box sort: a grid barrier wait ran out of time");
+      FMMB_CHECK(!hc.sort_fail, ERR_CUDA, "split-box sort: a grid barrier wait ran out of time");
       if (hc.overflow) {
         FMMB_CHECK(attempt < 6, ERR_CAPACITY, "tree balance buffers overflow");
         capf = 4 * capf;
@@ -1029,16 +1041,18 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
     pxs.alloc(np, s);
     preal.alloc(np, s);
     ppos.alloc(np, s);
-    // pb[0..L] and the real-group bounds rgb[0..L] share one buffer: one copy back
-    pb.alloc(2 * (L + 1), s);
+    // pb[0..L], the real-group bounds rgb[0..L] and the sort failure flag
+    // share one buffer: one copy back
+    pb.alloc(2 * (L + 1) + 1, s);
     k_parent_decode<<<grid_for(np, TPB), TPB, 0, s>>>(pkc.get(), np, mb, L, pks.get(), pxs.get(),
                                                        preal.get(), pb.get());
     FMMB_CUDA(cudaGetLastError());
     exclusive_sum(preal.get(), ppos.get(), np, td.sort_fail.get(), true, s);
-    k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1);
+    k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1,
+                                   td.sort_fail.get());
     FMMB_CUDA(cudaGetLastError());
   } else {
-    pb.alloc(2 * (L + 1), s);
+    pb.alloc(2 * (L + 1) + 1, s);
     pb.zero(s);
     pks.alloc(1, s);
     pxs.alloc(1, s);
@@ -1057,7 +1071,7 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   td.dev_off.alloc(L + 1, s);
   k_level_offsets<<<1, 1, 0, s>>>(pb.get(), L, td.dev_off.get());
   FMMB_CUDA(cudaGetLastError());
-  begin_pending_counts(th, pb.get(), 2 * (L + 1), td.sort_fail.get(), s);
+  begin_pending_counts(th, pb.get(), 2 * (L + 1), s);
   // every parent box has 4 children: at most 1 + 4 np nodes, np real groups
   const int total_ub = 1 + 4 * int(np);
   td.rg.alloc(np > 0 ? np : 1, s);
