@@ -364,3 +364,25 @@ def test_results_are_bitwise_reproducible(built_lib, precision):
         outs.append((F.source_evaluation(x, y).cpu(), F.target_evaluation(tx, ty).cpu()))
         F.status()
     assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pinned_host_charges_equal_device_charges(built_lib, precision):
+    """Charges given as a pinned host tensor are copied on a stream of their
+    own, beside the tree's last kernels: the results equal those of the same
+    charges given on the device, bit for bit, over repeated builds."""
+    import torch
+    from flexmm_b200 import KI_FMM, workloads
+    d = workloads.clustered(n=200_000, n_grid=100)
+    x, y = (torch.from_numpy(d[k]).cuda() for k in ("x", "y"))
+    tau_h = torch.from_numpy(d["tau"]).pin_memory()
+    neq = {"fp64": 60, "mixed": 24}[precision]
+
+    def run(tau):
+        F = KI_FMM(x, y, "Laplace_Eval", 64, neq, bbox=d["bbox"], precision=precision)
+        F.build_expansions(tau)
+        return F.source_evaluation(x, y).cpu()
+
+    ref = run(tau_h.cuda())
+    for _ in range(3):
+        assert torch.equal(run(tau_h), ref)
