@@ -293,11 +293,10 @@ cudaStream_t side_stream() {
 
 // Whether own-source evaluation runs split (near field beside the level
 // passes).  Measured at 1M clustered sources: the FP64 form gains ~0.6 ms
-// (its level passes are DMMA tiles that share SMs well); the mixed form
-// loses (its persistent tcgen05 M2L and smem-staged level kernels slow down
-// more beside the near field than the near field saves), so it evaluates in
-// one pass unless FLEXMM_B200_SPLIT_EVAL=1.  FLEXMM_B200_SPLIT_EVAL=0 turns
-// the split off for both forms.
+// (its level passes are DMMA tiles that share SMs well); the mixed form,
+// whose near field pauses while the persistent tcgen05 M2L runs, gains
+// ~0.03 ms (1.39 -> 1.36 ms).  On for both by default;
+// FLEXMM_B200_SPLIT_EVAL=0 turns it off, =1 on.
 std::atomic<int> g_split_mode{-2};  // -2: not yet read from the environment
 
 bool split_enabled(int precision) {
@@ -308,7 +307,8 @@ bool split_enabled(int precision) {
     g_split_mode.compare_exchange_strong(mode, env);
     mode = g_split_mode.load(std::memory_order_relaxed);
   }
-  return mode < 0 ? precision == PREC_FP64 : mode == 1;
+  (void)precision;  // the same default for both forms
+  return mode < 0 || mode == 1;
 }
 
 // the plan's split-evaluation events (created on first use) and side stream
@@ -317,6 +317,58 @@ void split_prepare(fmm_plan *p) {
   for (cudaEvent_t *e : {&p->ev_ready, &p->ev_near, &p->ev_far, &p->ev_m2l})
     if (!*e) FMMB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
 }
+
+// Zeroes up to 8 device buffers in one launch (instead of one memset each:
+// at the start of build_expansions these sit between the tree and the first
+// pass, where every launch's host and GPU overhead is on the critical path)
+struct ZeroList {
+  unsigned char *p[8];
+  size_t bytes[8];
+  int n;
+};
+
+__global__ void k_zero_buffers(ZeroList z) {
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t nthr = (size_t)gridDim.x * blockDim.x;
+  for (int b = 0; b < z.n; ++b) {
+    const size_t n16 = z.bytes[b] / 16;  // buffers are 16-byte aligned (checked by the host)
+    uint4 *w = reinterpret_cast<uint4 *>(z.p[b]);
+    for (size_t i = tid; i < n16; i += nthr) w[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (size_t i = 16 * n16 + tid; i < z.bytes[b]; i += nthr) z.p[b][i] = 0;
+  }
+}
+
+class ZeroBatch {
+ public:
+  explicit ZeroBatch(cudaStream_t s) : s_(s) {}
+  template <class T>
+  ZeroBatch &add(DevBuf<T> &b) {
+    if (!b.n) return *this;
+    if (z_.n == 8 || (reinterpret_cast<uintptr_t>(b.get()) & 15)) {
+      b.zero(s_);
+      return *this;
+    }
+    z_.p[z_.n] = reinterpret_cast<unsigned char *>(b.get());
+    z_.bytes[z_.n++] = b.n * sizeof(T);
+    return *this;
+  }
+  void run() {
+    if (!z_.n) return;
+    size_t total = 0;
+    for (int i = 0; i < z_.n; ++i) total += z_.bytes[i];
+    int dev = 0, sms = 0;
+    FMMB_CUDA(cudaGetDevice(&dev));
+    FMMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = (int)std::min<size_t>(size_t(sms) * 8, std::max<size_t>(1, total / 4096));
+    k_zero_buffers<<<blocks, 256, 0, s_>>>(z_);
+    FMMB_CUDA(cudaGetLastError());
+    z_.n = 0;
+  }
+
+ private:
+  cudaStream_t s_;
+  ZeroList z_{};
+};
 }  // namespace
 
 extern "C" {
@@ -1113,36 +1165,30 @@ static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream) 
     else
       p->tau_s.zero(s);
     p->ple.alloc(total * np, s);
-    p->ple.zero(s);
     if (p->precision == PREC_MIXED) {
       p->mult32.alloc(total * np, s);
       p->loc32.alloc(total * np, s);
       p->msum.alloc(total, s);
       p->lsum.alloc(total, s);
       p->mult_tc.alloc(total * 2 * np, s);
-      p->mult32.zero(s);
-      p->mult_tc.zero(s);
-      p->loc32.zero(s);
-      p->msum.zero(s);
-      p->lsum.zero(s);
-      p->tsum.alloc(total, s);
-      node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
       // a split near field (if evaluation splits) runs beside the upward and
       // downward passes and pauses while the M2L runs: hold clear now, set
       // before the M2L; m2l_done recorded after it
       p->hold_armed = split_enabled(PREC_MIXED);
-      if (p->hold_armed) {
-        p->near_hold.alloc(1, s);
-        p->near_hold.zero(s);
-      }
+      if (p->hold_armed) p->near_hold.alloc(1, s);
+      p->err.alloc(2, s);  // [0] error flag, [1] M2L tile counter
+      ZeroBatch zb(s);
+      zb.add(p->ple).add(p->mult32).add(p->mult_tc).add(p->loc32).add(p->msum).add(p->lsum).add(p->err);
+      if (p->hold_armed) zb.add(p->near_hold);
+      zb.run();
+      p->tsum.alloc(total, s);
+      node_charge_sums(a, p->tau_s.get(), p->tsum.get(), s);
       // sorted charges and box charge sums are all the near field reads
       FMMB_CUDA(cudaEventRecord(p->ev_ready, s));
       p->ready_recorded = true;
       t_prep.reset();
       run_upward_mixed(a, p->tau_s.get(), p->tsum.get(), p->mult32.get(), p->msum.get(),
                        p->mult_tc.get(), s);
-      p->err.alloc(2, s);  // [0] error flag, [1] M2L tile counter
-      p->err.zero(s);
       if (p->hold_armed) FMMB_CUDA(cudaMemsetAsync(p->near_hold.get(), 1, 1, s));
       run_m2l_mixed(a, p->mult32.get(), p->mult_tc.get(), p->msum.get(), p->ple.get(),
                     p->err.get(), s);
@@ -1151,8 +1197,7 @@ static void build_expansions_impl(fmm_plan *p, const double *tau, void *stream) 
     } else {
       p->mult.alloc(total * np, s);
       p->loc.alloc(total * np, s);
-      p->mult.zero(s);
-      p->loc.zero(s);
+      ZeroBatch(s).add(p->ple).add(p->mult).add(p->loc).run();
       FMMB_CUDA(cudaEventRecord(p->ev_ready, s));  // sorted charges: all the near field reads
       p->ready_recorded = true;
       t_prep.reset();

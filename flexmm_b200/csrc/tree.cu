@@ -464,11 +464,19 @@ __global__ void k_parent_decode(const uint64_t *__restrict__ keys, int64_t n, in
 }
 
 // real sibling groups: the children of split boxes (not of X-list leaves)
-// (rgb[L + 1]: the tree's sort failure flag, read back with the bounds)
+// (rgb[L + 1]: the tree's sort failure flag, read back with the bounds;
+// the last thread of the block writes the level offsets, as k_level_offsets)
+__device__ __forceinline__ void level_offsets(const int *__restrict__ pb, int L, int *__restrict__ off) {
+  off[0] = 0;
+  if (L >= 1) off[1] = 1;
+  for (int m = 1; m < L; ++m) off[m + 1] = off[m] + 4 * (pb[m] - pb[m - 1]);
+}
+
 __global__ void k_real_bounds(const int *__restrict__ pos, const int *__restrict__ real, int64_t n,
                               const int *__restrict__ pb, int L, int *__restrict__ rgb,
-                              const int *__restrict__ sort_fail) {
+                              const int *__restrict__ sort_fail, int *__restrict__ off) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l == (int)blockDim.x - 1) level_offsets(pb, L, off);  // blockDim.x > L + 1
   if (l == L + 1) rgb[l] = *sort_fail;
   if (l > L) return;
   const int total = n ? pos[n - 1] + real[n - 1] : 0;
@@ -499,12 +507,11 @@ __device__ __forceinline__ int level_of(const int *__restrict__ off, int L, int 
 }
 
 // --- 6. node arrays -----------------------------------------------------------
-// level offsets from the per-level parent-box bounds (one thread)
+// level offsets from the per-level parent-box bounds (one thread; a tree
+// without split boxes, else k_real_bounds writes them)
 __global__ void k_level_offsets(const int *__restrict__ pb, int L, int *__restrict__ off) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  off[0] = 0;
-  if (L >= 1) off[1] = 1;
-  for (int m = 1; m < L; ++m) off[m + 1] = off[m] + 4 * (pb[m] - pb[m - 1]);
+  level_offsets(pb, L, off);
 }
 
 // The node kernels are launched for an upper bound of the node count (the
@@ -1048,8 +1055,9 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
                                                        preal.get(), pb.get());
     FMMB_CUDA(cudaGetLastError());
     exclusive_sum(preal.get(), ppos.get(), np, td.sort_fail.get(), true, s);
+    td.dev_off.alloc(L + 1, s);
     k_real_bounds<<<1, 64, 0, s>>>(ppos.get(), preal.get(), np, pb.get(), L, pb.get() + L + 1,
-                                   td.sort_fail.get());
+                                   td.sort_fail.get(), td.dev_off.get());
     FMMB_CUDA(cudaGetLastError());
   } else {
     pb.alloc(2 * (L + 1) + 1, s);
@@ -1068,9 +1076,11 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   }
   // level offsets on the device; their host copy (with the real-group
   // bounds) travels back without a wait (finalize_tree)
-  td.dev_off.alloc(L + 1, s);
-  k_level_offsets<<<1, 1, 0, s>>>(pb.get(), L, td.dev_off.get());
-  FMMB_CUDA(cudaGetLastError());
+  if (n0 == 0) {  // (otherwise k_real_bounds wrote them)
+    td.dev_off.alloc(L + 1, s);
+    k_level_offsets<<<1, 1, 0, s>>>(pb.get(), L, td.dev_off.get());
+    FMMB_CUDA(cudaGetLastError());
+  }
   begin_pending_counts(th, pb.get(), 2 * (L + 1), s);
   // every parent box has 4 children: at most 1 + 4 np nodes, np real groups
   const int total_ub = 1 + 4 * int(np);

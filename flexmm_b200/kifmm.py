@@ -492,7 +492,7 @@ def direct_evaluation(kernel, sx, sy, tau, tx, ty, check=False, **kernel_params)
 def set_split_evaluation(mode=None):
     """Own-source evaluation split into a near-field kernel beside the level
     passes and a far-field kernel after them: True / False, or None for the
-    default (on for the FP64 form, off for the mixed form)."""
+    default (on for both forms)."""
     _lib.load()
     _lib.call("fmm_set_split_evaluation", -1 if mode is None else int(bool(mode)))
 

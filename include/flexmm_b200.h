@@ -299,9 +299,9 @@ int fmm_timing_read(double *ms /* [FMM_N_PHASES] */, int64_t *launches /* [FMM_N
 /* Whether evaluation at a plan's own sources runs split: the near field
  * (P2P) on a side stream, started once the charges are sorted, beside the
  * upward/M2L/downward passes, and the far field (L2T) after them.  mode 1 on,
- * 0 off (one evaluation kernel after the passes), -1 the default (on for the
- * FP64 form, off for the mixed form; the environment variable
- * FLEXMM_B200_SPLIT_EVAL=0/1 overrides the default).  Process-wide; results
+ * 0 off (one evaluation kernel after the passes), -1 the default (on for
+ * both forms; the environment variable FLEXMM_B200_SPLIT_EVAL=0/1 overrides
+ * the default).  Process-wide; results
  * agree to rounding either way.  No reference counterpart (the reference
  * evaluates after its passes, flexmm/flexmm2d/fmm.py:150-157). */
 int fmm_set_split_evaluation(int mode);
