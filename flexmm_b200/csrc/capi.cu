@@ -186,6 +186,11 @@ bool kernel_scaled(int kernel_id) {
   }
 }
 
+// kernels with an FP32 form for the mixed passes
+bool kernel_mixed(int kernel_id) {
+  return kernel_id == KERNEL_LAPLACE || kernel_id == KERNEL_MOD_HELMHOLTZ;
+}
+
 double kernel_offset(int kernel_id, const KernelParams &kp, double w) {
   switch (kernel_id) {
     case KERNEL_LAPLACE: return LaplaceF32::offset(w, kp);
@@ -779,8 +784,8 @@ int fmm_plan_set_precision(fmm_plan *p, int precision) {
     FMMB_CHECK(p, ERR_INVALID_ARGUMENT, "plan is NULL");
     FMMB_CHECK(precision == PREC_FP64 || precision == PREC_MIXED, ERR_INVALID_ARGUMENT,
                "precision must be FMM_PRECISION_FP64 or FMM_PRECISION_MIXED");
-    FMMB_CHECK(precision == PREC_FP64 || kernel_scaled(p->ops->kernel_id), ERR_UNSUPPORTED,
-               "the mixed form needs a scale-invariant kernel (Laplace)");
+    FMMB_CHECK(precision == PREC_FP64 || kernel_mixed(p->ops->kernel_id), ERR_UNSUPPORTED,
+               "the mixed form needs a kernel with an FP32 form (Laplace, modified Helmholtz)");
     FMMB_CHECK(precision == PREC_FP64 || p->ops->method == METHOD_KIFMM, ERR_UNSUPPORTED,
                "the black-box and Stokes FMMs have an FP64 form only");
     p->precision = precision;

@@ -868,8 +868,19 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // PART: EVAL_FULL (L2T + P2P), EVAL_NEAR (P2P and its kernel-offset term
 // only, into near[], caller's point order) or EVAL_FAR (L2T and its offset
 // term only, plus near[]: out = far + near).
+// resident blocks per SM the evaluation is built for (its register budget):
+// the K0 polynomials need more registers than the log kernel's one log2
+template <class KF32>
+struct EvalOcc {
+  static constexpr int blocks = EVAL_BLOCKS_PER_SM;
+};
+template <>
+struct EvalOcc<ModHelmholtzF32> {
+  static constexpr int blocks = 8;
+};
+
 template <class KF32, class KF64, int NOUT, int PART = EVAL_FULL>
-__global__ void __launch_bounds__(TCH, NOUT == 1 ? EVAL_BLOCKS_PER_SM : 6)
+__global__ void __launch_bounds__(TCH, NOUT == 1 ? EvalOcc<KF32>::blocks : 6)
     k_evaluate_mx(KernelParams kp, int neq, int np, const EvalDesc *__restrict__ desc,
                   const int *__restrict__ n_items_ptr, const double *__restrict__ sx,
                   const double *__restrict__ sy, const double *__restrict__ tau,
@@ -1300,6 +1311,9 @@ void run_upward_mixed(const PassArgs &a, const double *tau_s, const double *tsum
                       double *msum, float *mult_tc, cudaStream_t s) {
   switch (a.kernel_id) {
     case KERNEL_LAPLACE: upward_mx_impl<LaplaceF32>(a, tau_s, tsum, mult32, msum, mult_tc, s); break;
+    case KERNEL_MOD_HELMHOLTZ:
+      upward_mx_impl<ModHelmholtzF32>(a, tau_s, tsum, mult32, msum, mult_tc, s);
+      break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
 }
@@ -1382,14 +1396,13 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
   }
 }
 
-void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
-                                      const double *tsum, const float *loc32, const double *lsum,
-                                      int check, double *out, cudaStream_t s, const SplitEval &se) {
+template <class KF32, class KF64>
+void split_mixed_impl(const PassArgs &a, const double *tau_s, const double *tsum,
+                      const float *loc32, const double *lsum, int check, double *out,
+                      cudaStream_t s, const SplitEval &se) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int64_t m = th.n_points;
-  if (m == 0) return;
-  FMMB_CHECK(a.kernel_id == KERNEL_LAPLACE, ERR_UNSUPPORTED, "unknown kernel id");
   const int total = th.n_total();
   FMMB_CUDA(cudaStreamWaitEvent(se.side, se.ready, 0));
   EvalItems it;
@@ -1409,7 +1422,7 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
     // the SMs keep their largest shared-memory carveout while near-field
     // blocks sit on them, so the level passes' CTAs still fit beside them
     static const bool carveout_set = [] {
-      FMMB_CUDA(cudaFuncSetAttribute(k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>,
+      FMMB_CUDA(cudaFuncSetAttribute(k_evaluate_mx<KF32, KF64, 1, EVAL_NEAR>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                      cudaSharedmemCarveoutMaxShared));
       return true;
@@ -1423,7 +1436,7 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
         FMMB_CUDA(cudaStreamWaitEvent(se.side, se.m2l_done, 0));
         FMMB_CUDA(cudaMemsetAsync(se.hold, 0, sizeof(int), se.side));
       }
-      k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_NEAR>
+      k_evaluate_mx<KF32, KF64, 1, EVAL_NEAR>
           <<<work_grid(total + m / TCH + 1, part == 0 ? NEAR_BLOCKS_PER_SM_MIXED
                                                       : NEAR_BLOCKS_PER_SM_MIXED_RESUME),
              TCH, 0, se.side>>>(a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(),
@@ -1437,8 +1450,8 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
   FMMB_CUDA(cudaStreamWaitEvent(s, se.near_done, 0));
   {
     PhaseTimer timer(PH_EVAL, s);
-    k_evaluate_mx<LaplaceF32, LaplaceF64, 1, EVAL_FAR>
-        <<<work_grid(total + m / TCH + 1, EVAL_BLOCKS_PER_SM), TCH, 0, s>>>(
+    k_evaluate_mx<KF32, KF64, 1, EVAL_FAR>
+        <<<work_grid(total + m / TCH + 1, EvalOcc<KF32>::blocks), TCH, 0, s>>>(
         a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
         a.ops_dev, loc32, lsum, td.sx.get(), td.sy.get(), td.ordv.get(), check, 1, out, 0,
         next_item.get() + 1, near.get());
@@ -1446,6 +1459,22 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
   }
   FMMB_CUDA(cudaEventRecord(se.far_done, s));
   FMMB_CUDA(cudaStreamWaitEvent(se.side, se.far_done, 0));
+}
+
+void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
+                                      const double *tsum, const float *loc32, const double *lsum,
+                                      int check, double *out, cudaStream_t s, const SplitEval &se) {
+  if (a.th->n_points == 0) return;
+  switch (a.kernel_id) {
+    case KERNEL_LAPLACE:
+      split_mixed_impl<LaplaceF32, LaplaceF64>(a, tau_s, tsum, loc32, lsum, check, out, s, se);
+      break;
+    case KERNEL_MOD_HELMHOLTZ:
+      split_mixed_impl<ModHelmholtzF32, ModHelmholtzF64>(a, tau_s, tsum, loc32, lsum, check, out,
+                                                         s, se);
+      break;
+    default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
+  }
 }
 
 void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *tsum,
@@ -1481,6 +1510,16 @@ void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *ts
                                         td.sx.get(), td.sy.get(), tau_s, a.ops_dev, loc32, lsum,
                                         txs, tys, tperm, check, self_eval, out, ld_out,
                                         next_item.get(), nullptr, nullptr);
+      break;
+    }
+    case KERNEL_MOD_HELMHOLTZ: {  // potential only: the mixed gradient is the log kernel's
+      FMMB_CHECK(nout == 1, ERR_UNSUPPORTED,
+                 "the mixed form evaluates the modified Helmholtz potential only (gradients: FP64)");
+      k_evaluate_mx<ModHelmholtzF32, ModHelmholtzF64, 1>
+          <<<work_grid(total + m / TCH + 1, EvalOcc<ModHelmholtzF32>::blocks), TCH, 0, s>>>(
+              a.kp, a.neq, a.np, desc.get(), it.n_items.get(), td.sx.get(), td.sy.get(), tau_s,
+              a.ops_dev, loc32, lsum, txs, tys, tperm, check, self_eval, out, ld_out,
+              next_item.get(), nullptr, nullptr);
       break;
     }
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");

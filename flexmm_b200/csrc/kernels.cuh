@@ -12,6 +12,7 @@
 #pragma once
 #include <math.h>
 
+#include <cfloat>
 #include <cmath>
 
 #include "bessel.cuh"
@@ -252,6 +253,52 @@ struct LaplaceF32 {
   // coordinates (times 1/w for absolute units)
   static constexpr double kGradScale = -1.0 / (2.0 * M_PI);
   static double offset(double w, const KernelParams &) { return -std::log(w * w) / (4.0 * M_PI); }
+};
+
+// K0 in FP32 (A&S 9.8.1, 9.8.5, 9.8.6: Abramowitz & Stegun, Handbook of
+// Mathematical Functions, polynomial approximations of I0 and K0):
+//   x <= 2: K0(x) = -ln(x/2) I0(x) + P(t^2), t = x/2 (|error| < 1e-8), with
+//           I0(x) = Q((x/3.75)^2) (relative error < 1.6e-7);
+//   x > 2:  K0(x) = exp(-x) / sqrt(x) R(2/x) (relative error < 1.9e-7).
+// Both branches are computed and one selected (no divergence within a warp
+// of pairs at mixed distances).  K0(0) = +inf (the flushed log of 0).
+__device__ __forceinline__ float bessel_k0_f32(float x) {
+  const float y = (x * (1.f / 3.75f)) * (x * (1.f / 3.75f));
+  const float i0 = fmaf(y, fmaf(y, fmaf(y, fmaf(y, fmaf(y, fmaf(y, 0.0045813f, 0.0360768f), 0.2659732f),
+                                                   1.2067492f), 3.0899424f), 3.5156229f), 1.f);
+  const float t2 = 0.25f * x * x;
+  const float p = fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, 0.0000074f, 0.0001075f), 0.00262698f),
+                                                   0.0348859f), 0.23069756f), 0.4227842f), -0.57721566f);
+  // -ln(x/2) = (1 - log2 x) ln 2
+  const float small = fmaf((1.f - lg2_ftz(x)) * 0.69314718f, i0, p);
+  const float z = 2.f * __frcp_rn(fmaxf(x, 2.f));
+  const float r = fmaf(z, fmaf(z, fmaf(z, fmaf(z, fmaf(z, fmaf(z, 0.00053208f, -0.0025154f), 0.00587872f),
+                                                  -0.01062446f), 0.02189568f), -0.07832358f), 1.25331414f);
+  const float large = __expf(-x) * rsqrtf(fmaxf(x, 2.f)) * r;
+  return x <= 2.f ? small : large;
+}
+
+// FP32 evaluation of K0(k r) / (2 pi) for the mixed passes.  K0 has no scale
+// decomposition: the passes evaluate it on box-centred coordinates in the
+// caller's units (kScaled = false, offset 0); FP32 keeps a pair's distance
+// to ~1e-7 of the box width, which bounds the per-pair error as for the log
+// kernel on width-scaled coordinates.
+struct ModHelmholtzF32 {
+  static constexpr bool kScaled = false;
+  // radial(d2) is +inf for d2 below FLT_MIN (K0 at a flushed 0)
+  static constexpr bool kInfAtZero = true;
+  static constexpr float kScale = (float)(1.0 / (2.0 * M_PI));
+  float k;
+  __host__ __device__ explicit ModHelmholtzF32(const KernelParams &kp) : k((float)kp.p[0]) {}
+  // (squared distances below FLT_MIN flushed to 0: K0 = +inf there)
+  __device__ __forceinline__ float radial(float d2) const {
+    return bessel_k0_f32(k * (d2 < FLT_MIN ? 0.f : sqrtf(d2)));
+  }
+  // (dx, dy) = target - source
+  __device__ __forceinline__ float operator()(float dx, float dy) const {
+    return radial(dx * dx + dy * dy) * kScale;
+  }
+  static double offset(double, const KernelParams &) { return 0.0; }
 };
 
 }  // namespace fmmb

@@ -63,6 +63,40 @@ def test_mixed_coincident_points_are_skipped_exactly(built_lib):
     assert rel_l2(ut, g["direct_tgt"]) < BAR
 
 
+@pytest.mark.parametrize("k,recipe", [(10.0, "clustered"), (0.5, "clustered"), (10.0, "uniform")])
+def test_mixed_modified_helmholtz_vs_direct_sum(built_lib, k, recipe):
+    """K0(k r) / (2 pi) in the mixed form (FP32 K0 from the Abramowitz-Stegun
+    polynomials, box-centred coordinates, 3xTF32 translations) against the
+    FP64 direct sum (bar 1e-6), sources (own points skipped) and targets."""
+    from flexmm_b200 import KI_FMM, KI_Helper, direct_evaluation, workloads
+    d = getattr(workloads, recipe)(n=150_000, n_grid=300, seed=47)
+    F = KI_FMM(d["x"], d["y"], "Modified_Helmholtz_Eval", 64, 32, bbox=d["bbox"],
+               helper=KI_Helper(), precision="mixed", helmholtz_k=k)
+    F.build_expansions(d["tau"])
+    us, ut = F.source_evaluation(d["x"], d["y"]), F.target_evaluation(d["tx"], d["ty"])
+    F.status()
+    rng = np.random.default_rng(3)
+    si = rng.choice(d["x"].size, 2000, replace=False)
+    ti = rng.choice(d["tx"].size, 2000, replace=False)
+    kw = dict(helmholtz_k=k)
+    ds = direct_evaluation("Modified_Helmholtz_Eval", d["x"], d["y"], d["tau"], d["x"][si], d["y"][si],
+                           check=True, **kw)
+    dt = direct_evaluation("Modified_Helmholtz_Eval", d["x"], d["y"], d["tau"], d["tx"][ti], d["ty"][ti], **kw)
+    es, et = rel_l2(us[si], ds), rel_l2(ut[ti], dt)
+    assert es < BAR and et < BAR, (es, et)
+
+
+def test_mixed_modified_helmholtz_refuses_gradients(built_lib):
+    from flexmm_b200 import KI_FMM, KI_Helper, workloads
+    d = workloads.uniform(n=20_000, n_grid=30, seed=5)
+    F = KI_FMM(d["x"], d["y"], "Modified_Helmholtz_Eval", 64, 24, bbox=d["bbox"], helper=KI_Helper(),
+               precision="mixed", helmholtz_k=5.0)
+    F.build_expansions(d["tau"])
+    F.register_evaluator(None, None, "grad", 3)
+    with pytest.raises(RuntimeError, match="potential only"):
+        F.evaluate_to_points(d["tx"], d["ty"], "grad", False)
+
+
 _SYNC_SCRIPT = r"""
 import sys, numpy as np
 sys.path.insert(0, {repo!r})

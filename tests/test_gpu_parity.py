@@ -264,13 +264,14 @@ def test_mod_helmholtz_direct_sum_matches_scipy(built_lib, k):
     assert np.all(np.abs(got[~nz]) < 1e-290)
 
 
-def test_mixed_form_rejects_non_scale_invariant_kernel(built_lib):
-    from flexmm_b200 import KI_FMM, KI_Helper
+def test_mixed_form_rejects_kernels_without_fp32_form(built_lib):
+    """A tabulated radial kernel has no FP32 form: its mixed form is refused."""
+    from flexmm_b200 import KI_FMM, KI_Helper, kernels
     rng = np.random.default_rng(5)
     x, y = rng.uniform(-1, 1, 2000), rng.uniform(-1, 1, 2000)
-    with pytest.raises(RuntimeError, match="scale-invariant"):
-        KI_FMM(x, y, "Modified_Helmholtz_Eval", 32, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper(),
-               precision="mixed", helmholtz_k=5.0)
+    kern = kernels.radial(lambda r: np.exp(-r) / (1.0 + r), 1e-6, 4.0, name="ExpDecay")
+    with pytest.raises(RuntimeError, match="FP32 form"):
+        KI_FMM(x, y, kern, 32, 16, bbox=[-1, 1, -1, 1], helper=KI_Helper(), precision="mixed")
 
 
 def test_radial_table_kernel_device_matches_host_table(built_lib):
