@@ -59,6 +59,8 @@ def parse():
                    help="skip the differentiable black-box FMM (forward + backward) measurement")
     p.add_argument("--no-multi-rhs", action="store_true",
                    help="skip the multi-RHS (64 charge columns, modified Helmholtz) measurement")
+    p.add_argument("--no-helmholtz", action="store_true",
+                   help="skip the modified-Helmholtz mixed vs FP64 measurement")
     p.add_argument("--cpu-sample-n", type=int, default=200_000,
                    help="sources in the bounded reference sample of our arm's cpu_baseline")
     p.add_argument("--denested-steps", type=int, default=3,
@@ -560,10 +562,58 @@ def run_ours(args, world, rank, local):
         out["multi_rhs"] = measure_multi_rhs(args, world)
     if not args.no_adjoint:
         out["bbfmm_adjoint"] = measure_bb_adjoint(args, world)
+    if not args.no_helmholtz:
+        out["modified_helmholtz"] = measure_helmholtz(args, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_subprocess(args)
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def measure_helmholtz(args, world=1, steps=5, k=10.0, neq=32):
+    """K0(k r)/(2 pi), k = 10, on the headline workload (clustered sources +
+    grid targets, Ncutoff 64, Nequiv 32): the mixed form (FP32 K0, 3xTF32
+    translations) against the FP64 form, each step tree + expansions +
+    source and target evaluation on resident inputs, CUDA events; source
+    error of each against the FP64 direct sum at 2,000 sampled sources.
+    Each rank runs the same problem (replicas)."""
+    import numpy as np
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, direct_evaluation, workloads
+    d = workloads.clustered(n=args.n, n_grid=args.grid)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x, y, tau, tx, ty = (torch.from_numpy(d[c]).to(dev) for c in ("x", "y", "tau", "tx", "ty"))
+    si = np.random.default_rng(0).choice(d["x"].size, 2000, replace=False)
+    ds = direct_evaluation("Modified_Helmholtz_Eval", d["x"], d["y"], d["tau"], d["x"][si], d["y"][si],
+                           check=True, helmholtz_k=k)
+    pts = d["x"].size + d["tx"].size
+    res = {"workload": f"K0({k:g} r)/(2 pi), clustered {d['x'].size} sources + {args.grid}^2 grid "
+                       f"targets, Ncutoff {NCUT}, Nequiv {neq}, self + target evaluation",
+           "metric": "(sources + targets) / s", "unit": "Mpts/s"}
+    for prec in ("mixed", "fp64"):
+        helper = KI_Helper()
+
+        def step():
+            F = KI_FMM(x, y, "Modified_Helmholtz_Eval", NCUT, neq, bbox=d["bbox"], helper=helper,
+                       precision=prec, helmholtz_k=k)
+            F.build_expansions(tau)
+            return F.source_evaluation(x, y), F.target_evaluation(tx, ty)
+        for _ in range(2):
+            us, _ = step()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            us, _ = step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = dist_max(e0.elapsed_time(e1) / steps, world)
+        err = float(np.linalg.norm(us.cpu().numpy()[si] - ds) / np.linalg.norm(ds))
+        res[prec] = {"value": world * pts / (ms * 1e-3) / 1e6, "ms_per_step": ms,
+                     "src_rel_l2_vs_direct": err, "dtype": "f32+tf32x3/f64" if prec == "mixed" else "f64"}
+    res["mixed_over_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+    return res
 
 
 def measure_bb_adjoint(args, world=1, steps=3):

@@ -182,6 +182,10 @@ int fmm_plan_info(fmm_plan *plan, int *n_levels, double *widths, int *n_nodes);
  *                        split-precision (3xTF32) tensor-core M2M / M2L / L2L
  *                        with FP32 accumulate on mean-deflated operators,
  *                        FP64 check-to-equivalent and final accumulation.
+ *                        KIFMM plans of the Laplace kernel (potential and
+ *                        gradient) and the modified Helmholtz kernel
+ *                        (potential; FP32 K0 from the Abramowitz-Stegun
+ *                        polynomials); other plans return FMM_ERR_UNSUPPORTED.
  * Set before fmm_build_expansions (it invalidates previous expansions). */
 #define FMM_PRECISION_FP64 0
 #define FMM_PRECISION_MIXED 1
