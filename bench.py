@@ -689,43 +689,51 @@ def measure_multi_rhs(args, world=1, n=1_000_000, n_rhs=64, steps=3):
     lo, hi = column_blocks(n_rhs, world)[rank]
     x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
     tau = torch.from_numpy(np.ascontiguousarray(d["tau"][lo:hi])).cuda()
-    helper = KI_Helper()
-
-    def step():
-        F = KI_FMM(x, y, "Modified_Helmholtz_Eval", NCUT, 40, helper=helper, helmholtz_k=10.0)
-        F.build_expansions(tau)
-        return F, F.source_evaluation(x, y)
-    F, u = step()
-    torch.cuda.synchronize()
-    # accuracy: two columns at 1000 sampled sources against the FP64 direct sum
     from flexmm_b200 import direct_evaluation
     rng = np.random.default_rng(5)
     si = np.sort(rng.choice(n, 1000, replace=False))
-    errs = []
-    for r in (0, hi - lo - 1):
-        ds = direct_evaluation("Modified_Helmholtz_Eval", x, y, tau[r], x[si], y[si], check=True,
-                               helmholtz_k=10.0).cpu().numpy()
-        errs.append(float(np.linalg.norm(u[r].cpu().numpy()[si] - ds) / np.linalg.norm(ds)))
-    del F, u
-    barrier(world)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        step()
-    e1.record()
-    torch.cuda.synchronize()
-    barrier(world)
-    ms = dist_max(e0.elapsed_time(e1) / steps, world)
+    ds = {r: direct_evaluation("Modified_Helmholtz_Eval", x, y, tau[r], x[si], y[si], check=True,
+                               helmholtz_k=10.0).cpu().numpy() for r in (0, hi - lo - 1)}
+
+    def run(prec):
+        helper = KI_Helper()
+
+        def step():
+            F = KI_FMM(x, y, "Modified_Helmholtz_Eval", NCUT, 40, helper=helper, helmholtz_k=10.0,
+                       precision=prec)
+            F.build_expansions(tau)
+            return F, F.source_evaluation(x, y)
+        F, u = step()
+        torch.cuda.synchronize()
+        # accuracy: two columns at 1000 sampled sources against the FP64 direct sum
+        errs = [float(np.linalg.norm(u[r].cpu().numpy()[si] - v) / np.linalg.norm(v))
+                for r, v in ds.items()]
+        del F, u
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        return dist_max(e0.elapsed_time(e1) / steps, world), max(errs)
+    ms, err = run("fp64")
+    ms_mx, err_mx = run("mixed")
     return {"workload": f"{n} sources on a circle (r = 0.5 +- 1e-3), {n_rhs} charge columns, "
                         f"K0(10 r)/(2 pi), Nequiv 40, Ncutoff 64, self-evaluation, FP64",
             "metric": "point-RHS / s", "unit": "M point-RHS/s", "dtype": "f64",
             "value": n * n_rhs / (ms * 1e-3) / 1e6, "ms_per_step": ms, "steps": steps,
-            "rel_l2_vs_direct": max(errs),
+            "rel_l2_vs_direct": err,
             "accuracy_sample": "columns 0 and last of this rank, 1000 sources, FP64 direct sum",
             "note": "one launch per level for all columns (column = blockIdx.y); evaluation "
                     "shares each kernel value across 8 columns; inputs resident"
-                    + (f"; columns split over {world} ranks, slowest rank's time" if world > 1 else "")}
+                    + (f"; columns split over {world} ranks, slowest rank's time" if world > 1 else ""),
+            "mixed": {"value": n * n_rhs / (ms_mx * 1e-3) / 1e6, "ms_per_step": ms_mx,
+                      "rel_l2_vs_direct": err_mx, "dtype": "f32+tf32x3/f64",
+                      "note": "same workload in the mixed form: the tree once, then each column's "
+                              "expansions and source evaluation in turn"}}
 
 
 def measure_batched_stokes(args, world=1, n_problems=256):

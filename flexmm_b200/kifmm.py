@@ -302,8 +302,13 @@ class KI_FMM:
             k, n = td.shape
             if n != self.N:
                 raise ValueError(f"tau has {n} columns, expected {self.N}")
-            _lib.call("fmm_build_expansions_multi", self._plan, ctypes.c_void_p(td.data_ptr()), k, n,
-                      _stream())
+            if self.precision == "mixed":
+                # mixed form: each evaluation runs every column through the
+                # mixed passes on this tree (_evaluate_multi); nothing to build yet
+                self._check_mixed_columns()
+            else:
+                _lib.call("fmm_build_expansions_multi", self._plan, ctypes.c_void_p(td.data_ptr()), k,
+                          n, _stream())
             self._tau = td
             self._n_rhs = k
             self._expanded = True
@@ -397,9 +402,39 @@ class KI_FMM:
                   ctypes.c_void_p(out.data_ptr()), m, _stream())
         return _as_kind(out, kind, (nout, m))
 
+    def _check_mixed_columns(self):
+        if self.kernel.kernel_id not in (0, 1):
+            raise NotImplementedError("mixed charge columns: Laplace and modified Helmholtz only")
+
+    def _evaluate_columns_mixed(self, x, y, check, k):
+        """Mixed form, k charge columns: the columns' expansions are formed one
+        after another on this tree and each column is evaluated right after
+        its own, into row c of the [k, M] result."""
+        torch = _torch()
+        own = check and self._own_sources(x, y)
+        if own:
+            m, kind = self.N, ("cuda" if x.is_cuda else "cpu")
+        else:
+            xd, kind = _device_f64(x)
+            yd, _ = _device_f64(y)
+            m = xd.numel()
+        out = torch.empty((k, m), dtype=torch.float64, device="cuda")
+        for c in range(k):
+            _lib.call("fmm_build_expansions", self._plan, ctypes.c_void_p(self._tau[c].data_ptr()),
+                      _stream())
+            row = ctypes.c_void_p(out[c].data_ptr())
+            if own:
+                _lib.call("fmm_evaluate_sources", self._plan, 1, row, _stream())
+            else:
+                _lib.call("fmm_evaluate", self._plan, ctypes.c_void_p(xd.data_ptr()),
+                          ctypes.c_void_p(yd.data_ptr()), m, 1 if check else 0, row, _stream())
+        return _as_kind(out, kind, (k, m))
+
     def _evaluate_multi(self, x, y, check):
         torch = _torch()
         k = self._n_rhs
+        if self.precision == "mixed":
+            return self._evaluate_columns_mixed(x, y, check, k)
         if check and self._own_sources(x, y):
             out = torch.empty((k, self.N), dtype=torch.float64, device="cuda")
             _lib.call("fmm_evaluate_sources_multi", self._plan, 1, ctypes.c_void_p(out.data_ptr()),

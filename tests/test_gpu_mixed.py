@@ -86,6 +86,38 @@ def test_mixed_modified_helmholtz_vs_direct_sum(built_lib, k, recipe):
     assert es < BAR and et < BAR, (es, et)
 
 
+def test_mixed_charge_columns_vs_single_columns_and_direct_sum(built_lib):
+    """Charge columns [k, N] in the mixed form (each column's expansions formed
+    in turn on one tree), on the multi-RHS workload's kernel and points at a
+    smaller size: every row equals the single-column mixed result bit for bit
+    (sources and targets), and is within 1e-6 of the FP64 direct sum at 2,000
+    sampled sources (the aggregate bar of the mixed form; see the FP32 pair
+    sweep's close-pair limit in the design notes)."""
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, direct_evaluation, workloads
+    d = workloads.circle(n=100_000, n_rhs=3, seed=9)
+    x, y = torch.from_numpy(d["x"]).cuda(), torch.from_numpy(d["y"]).cuda()
+    tau = torch.from_numpy(d["tau"]).cuda()
+    rng = np.random.default_rng(2)
+    tx = torch.from_numpy(rng.uniform(-0.6, 0.6, 3000)).cuda()
+    ty = torch.from_numpy(rng.uniform(-0.6, 0.6, 3000)).cuda()
+    # a helper of its own per plan: a shared one snaps later bboxes to its cached widths
+    kw = dict(precision="mixed", helmholtz_k=10.0)
+    F = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, helper=KI_Helper(), **kw)
+    F.build_expansions(tau)
+    us, ut = F.source_evaluation(x, y).cpu().numpy(), F.target_evaluation(tx, ty).cpu().numpy()
+    assert us.shape == (3, 100_000) and ut.shape == (3, 3000)
+    si = rng.choice(100_000, 2000, replace=False)
+    for c in range(3):
+        G = KI_FMM(x, y, "Modified_Helmholtz_Eval", 64, 40, helper=KI_Helper(), **kw)
+        G.build_expansions(tau[c].contiguous())
+        assert np.array_equal(G.source_evaluation(x, y).cpu().numpy(), us[c])
+        assert np.array_equal(G.target_evaluation(tx, ty).cpu().numpy(), ut[c])
+        ds = direct_evaluation("Modified_Helmholtz_Eval", d["x"], d["y"], d["tau"][c], d["x"][si],
+                               d["y"][si], check=True, helmholtz_k=10.0)
+        assert rel_l2(us[c][si], ds) < BAR
+
+
 def test_mixed_modified_helmholtz_refuses_gradients(built_lib):
     from flexmm_b200 import KI_FMM, KI_Helper, workloads
     d = workloads.uniform(n=20_000, n_grid=30, seed=5)
