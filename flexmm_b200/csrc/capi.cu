@@ -1245,12 +1245,29 @@ void evaluate_points(fmm_plan *p, int nout, const double *tx, const double *ty, 
   DevBuf<uint64_t> tkeys;
   DevBuf<int> tperm;
   DevBuf<double> txs, tys;
+  txs.alloc(m, s);
+  tys.alloc(m, s);
+  if (p->ops->method == METHOD_KIFMM) {
+    // targets binned into their leaves (a descent along each key's digits and
+    // a count per leaf) instead of sorted
+    EvalItems it;
+    {
+      PhaseTimer timer(PH_SORT_TGT, s);
+      tperm.alloc(m, s);
+      eval_items_binned(a, tx, ty, m, it, txs.get(), tys.get(), tperm.get(), s);
+    }
+    if (p->precision == PREC_MIXED)
+      run_evaluate_mixed(a, p->tau_s.get(), p->tsum.get(), p->loc32.get(), p->lsum.get(), txs.get(),
+                         tys.get(), nullptr, tperm.get(), m, check, nout, out, ld_out, s, &it);
+    else
+      run_evaluate(a, p->tau_s.get(), p->loc.get(), txs.get(), tys.get(), nullptr, tperm.get(), m,
+                   check, nout, out, ld_out, s, &it);
+    return;
+  }
   // evaluator ids carry the output count; Stokes plans produce (u, v, p)
   {
     PhaseTimer timer(PH_SORT_TGT, s);
     // leaves live on levels <= L-1: their first L-1 digits decide everything
-    txs.alloc(m, s);
-    tys.alloc(m, s);
     sort_points(tx, ty, m, p->th, tkeys, tperm, s, p->th.L > 1 ? p->th.L - 1 : 1, txs.get(),
                 tys.get(), p->td.sort_fail.get());
   }

@@ -527,7 +527,7 @@ __global__ void k_leaf_targets(int total, int L, const int *__restrict__ off,
 __global__ void k_make_items(int total, int L, const int *__restrict__ off, const int *__restrict__ tb,
                              const int *__restrict__ te, const int *__restrict__ nch,
                              const int *__restrict__ choff, int4 *__restrict__ items,
-                             int *__restrict__ n_items) {
+                             int *__restrict__ n_items, int mark_multi) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
     if (g == total - 1) *n_items = choff[g] + nch[g];
     const int n = nch[g];
@@ -537,9 +537,10 @@ __global__ void k_make_items(int total, int L, const int *__restrict__ off, cons
       int mid = (lo + hi) >> 1;
       if (off[mid] <= g) lo = mid; else hi = mid;
     }
+    const int y = lo | (mark_multi && n > 1 ? EVAL_MULTI : 0);
     for (int c = 0; c < n; ++c) {
       const int t0 = tb[g] + c * TCH;
-      items[choff[g] + c] = make_int4(g, lo, t0, min(TCH, te[g] - t0));
+      items[choff[g] + c] = make_int4(g, y, t0, min(TCH, te[g] - t0));
     }
   }
 }
@@ -599,9 +600,10 @@ __global__ void __launch_bounds__(TCH) k_evaluate(KernelParams kp, int neq, int 
   const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int4 it = items[item];
-    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
+    const int g = it.x, lev = it.y & EVAL_LEVEL_MASK, t0 = it.z, cnt = it.w;
     int G = 1;
-    while (2 * G * cnt <= TCH) G *= 2;
+    if (!(it.y & EVAL_MULTI))
+      while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
     const bool valid = t < cnt;
     const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
@@ -778,9 +780,10 @@ __global__ void __launch_bounds__(TCH) k_evaluate_multi(KernelParams kp, int neq
   const int n_items = *n_items_ptr;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int4 it = items[item];
-    const int g = it.x, lev = it.y, t0 = it.z, cnt = it.w;
+    const int g = it.x, lev = it.y & EVAL_LEVEL_MASK, t0 = it.z, cnt = it.w;
     int G = 1;
-    while (2 * G * cnt <= TCH) G *= 2;
+    if (!(it.y & EVAL_MULTI))
+      while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
     const bool valid = t < cnt;
     const double x = valid ? txs[t0 + t] : 0.0, y = valid ? tys[t0 + t] : 0.0;
@@ -932,11 +935,6 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
   }
 }
 
-template <class KF>
-void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
-                   const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
-                   double *out, cudaStream_t s);
-
 }  // namespace
 
 void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s) {
@@ -956,7 +954,45 @@ void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &
   it.n_items.alloc(1, s);
   k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), it.tb.get(),
                                                     it.te.get(), it.nch.get(), it.choff.get(),
-                                                    it.items.get(), it.n_items.get());
+                                                    it.items.get(), it.n_items.get(), 0);
+  FMMB_CUDA(cudaGetLastError());
+}
+
+// per leaf: end of its target range and its item count (counts from binning)
+__global__ void k_leaf_ranges(int total, const int *__restrict__ count, const int *__restrict__ tb,
+                              int *__restrict__ te, int *__restrict__ nch) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    te[g] = tb[g] + count[g];
+    nch[g] = (count[g] + TCH - 1) / TCH;
+  }
+}
+
+void eval_items_binned(const PassArgs &a, const double *tx, const double *ty, int64_t m,
+                       EvalItems &it, double *txs, double *tys, int *tperm, cudaStream_t s) {
+  const TreeHost &th = *a.th;
+  const TreeDev &td = *a.td;
+  const int total = th.n_total();
+  DevBuf<int> count, leaf_of, slot;
+  count.alloc(total, s);
+  count.zero(s);
+  leaf_of.alloc(m, s);
+  slot.alloc(m, s);
+  bin_points(tx, ty, m, td, th, count.get(), leaf_of.get(), slot.get(), s);
+  it.tb.alloc(total, s);
+  it.te.alloc(total, s);
+  it.nch.alloc(total, s);
+  it.choff.alloc(total, s);
+  prefix_sum<int, false>(count.get(), it.tb.get(), total, td.sort_fail.get(), true, s);
+  scatter_binned(tx, ty, m, leaf_of.get(), slot.get(), it.tb.get(), txs, tys, tperm, s);
+  k_leaf_ranges<<<grid_for(total, 256), 256, 0, s>>>(total, count.get(), it.tb.get(), it.te.get(),
+                                                     it.nch.get());
+  FMMB_CUDA(cudaGetLastError());
+  prefix_sum<int, false>(it.nch.get(), it.choff.get(), total, td.sort_fail.get(), true, s);
+  it.items.alloc(total + m / TCH + 1, s);
+  it.n_items.alloc(1, s);
+  k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), it.tb.get(),
+                                                    it.te.get(), it.nch.get(), it.choff.get(),
+                                                    it.items.get(), it.n_items.get(), 1);
   FMMB_CUDA(cudaGetLastError());
 }
 
@@ -964,10 +1000,11 @@ namespace {
 template <class KF>
 void evaluate_impl(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
                    const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
-                   int nout, double *out, int64_t ld_out, cudaStream_t s) {
+                   int nout, double *out, int64_t ld_out, cudaStream_t s, const EvalItems *pre) {
   const TreeDev &td = *a.td;
-  EvalItems it;
-  eval_items(a, tkeys, m, it, s);
+  EvalItems own;
+  if (!pre) eval_items(a, tkeys, m, own, s);
+  const EvalItems &it = pre ? *pre : own;
   const int64_t units = a.th->n_total() + m / TCH + 1;  // work items, upper bound
   PhaseTimer timer(PH_EVAL, s);
   if (a.dvx) {
@@ -1053,21 +1090,21 @@ void run_downward(const PassArgs &a, const double *ple, double *loc, cudaStream_
 
 void run_evaluate(const PassArgs &a, const double *tau_s, const double *loc, const double *txs,
                   const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m, int check,
-                  int nout, double *out, int64_t ld_out, cudaStream_t s) {
+                  int nout, double *out, int64_t ld_out, cudaStream_t s, const EvalItems *pre) {
   if (m == 0) return;
   switch (a.kernel_id) {
     case KERNEL_LAPLACE:
       evaluate_impl<LaplaceF64T>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out, ld_out,
-                                 s);
+                                 s, pre);
       break;
     case KERNEL_MOD_HELMHOLTZ:
       evaluate_impl<ModHelmholtzF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
-                                     ld_out, s);
+                                     ld_out, s, pre);
       break;
     case KERNEL_RADIAL_TABLE:
       FMMB_CHECK(nout == 1, ERR_UNSUPPORTED, "tabulated kernels evaluate potentials only");
       evaluate_impl<RadialTableF64>(a, tau_s, loc, txs, tys, tkeys, tperm, m, check, nout, out,
-                                    ld_out, s);
+                                    ld_out, s, pre);
       break;
     default: throw Error(ERR_UNSUPPORTED, "unknown kernel id");
   }
@@ -1278,7 +1315,7 @@ void run_evaluate_scratch(const PassArgs &a, const double *tau_s, const double *
   FMMB_CUDA(cudaGetLastError());
   prefix_sum_run<int, false>(nch, choff, total, temp, temp_bytes, td.sort_fail.get(), true, s);
   k_make_items<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), tb, te, nch, choff,
-                                                    items, n_items);
+                                                    items, n_items, 0);
   FMMB_CUDA(cudaGetLastError());
   PhaseTimer timer(PH_EVAL, s);
   auto launch = [&](auto kern) {

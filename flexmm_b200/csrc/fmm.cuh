@@ -163,21 +163,33 @@ void run_local_evaluate(const PassArgs &a, const double *tau_sorted, const doubl
 void run_diag_log2(const double *x, int64_t n, double *out_tab, double *out_lib, cudaStream_t s);
 // nout = 1: potential into out[m]; nout = 3: potential and its gradient in the
 // target position into out[0..2][m] (row stride ld_out)
+struct EvalItems;
+// (pre: work items already built for txs, tys; else built from tkeys)
 void run_evaluate(const PassArgs &a, const double *tau_sorted, const double *loc,
                   const double *txs, const double *tys, const uint64_t *tkeys, const int *tperm,
-                  int64_t m, int check, int nout, double *out, int64_t ld_out, cudaStream_t s);
+                  int64_t m, int check, int nout, double *out, int64_t ld_out, cudaStream_t s,
+                  const EvalItems *pre = nullptr);
 
 // Evaluation work items: per leaf its range of sorted targets, split into
 // chunks of 128 targets; choff = exclusive scan of the chunk counts.
 struct EvalItems {
   DevBuf<int> tb, te, nch, choff;
-  DevBuf<int4> items;   // (leaf, level, first sorted target, count)
+  DevBuf<int4> items;   // (leaf, level | EVAL_MULTI, first sorted target, count)
   DevBuf<int> n_items;  // device count of items
 };
+// item .y: the leaf's level, plus EVAL_MULTI when the leaf's targets fill more
+// than one item (targets placed in no particular order inside the leaf): then
+// every item of the leaf gives one thread per target (G = 1), so that a
+// target's arithmetic does not depend on which item holds it
+constexpr int EVAL_LEVEL_MASK = 0xFF, EVAL_MULTI = 0x100;
 constexpr int EVAL_CHUNK = 128;  // targets per evaluation work item
 // parts of an evaluation: both, the near field (P2P) alone, the far field (L2T) alone
 constexpr int EVAL_FULL = 0, EVAL_NEAR = 1, EVAL_FAR = 2;
 void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s);
+// Work items for targets (tx, ty) in the caller's order, binned into the
+// leaves instead of sorted: writes txs, tys (leaf by leaf) and tperm.
+void eval_items_binned(const PassArgs &a, const double *tx, const double *ty, int64_t m,
+                       EvalItems &it, double *txs, double *tys, int *tperm, cudaStream_t s);
 
 // Mixed precision (fmm_mixed.cu): FP32 multipoles / locals with FP64 sums.
 void node_charge_sums(const PassArgs &a, const double *tau_sorted, double *tsum, cudaStream_t s);
@@ -191,7 +203,8 @@ void run_downward_mixed(const PassArgs &a, const double *ple, float *loc32, doub
 void run_evaluate_mixed(const PassArgs &a, const double *tau_sorted, const double *tsum,
                         const float *loc32, const double *lsum, const double *txs,
                         const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
-                        int check, int nout, double *out, int64_t ld_out, cudaStream_t s);
+                        int check, int nout, double *out, int64_t ld_out, cudaStream_t s,
+                        const EvalItems *pre = nullptr);
 
 // Evaluation with caller-provided scratch: tb, te, nch, choff hold one int
 // per tree node, temp holds evaluate_scratch_bytes(nodes) bytes.

@@ -814,7 +814,8 @@ struct __align__(16) EvalDesc {
   int g, lev, t0, cnt;
   int rb[9];   // first sorted source of each colleague
   int rs[10];  // exclusive prefix of the colleagues' source counts
-  int pad[3];
+  int multi;   // the leaf's targets fill several items (one thread per target)
+  int pad[2];
 };
 static_assert(sizeof(EvalDesc) == 128, "EvalDesc is read as 32 words");
 
@@ -829,7 +830,8 @@ __global__ void k_eval_desc(const int4 *__restrict__ items, const int *__restric
     const int4 it = items[item];
     EvalDesc d;
     d.g = it.x;
-    d.lev = it.y;
+    d.lev = it.y & EVAL_LEVEL_MASK;
+    d.multi = (it.y & EVAL_MULTI) ? 1 : 0;
     d.t0 = it.z;
     d.cnt = it.w;
     d.cx = xmid[it.x];
@@ -847,7 +849,7 @@ __global__ void k_eval_desc(const int4 *__restrict__ items, const int *__restric
       d.rs[c + 1] = acc;
     }
     d.csrc = cs;
-    d.pad[0] = d.pad[1] = d.pad[2] = 0;
+    d.pad[0] = d.pad[1] = 0;
     desc[item] = d;
   }
 }
@@ -935,7 +937,8 @@ __global__ void __launch_bounds__(TCH, NOUT == 1 ? EvalOcc<KF32>::blocks : 6)
     const int g = D.g, lev = D.lev, t0 = D.t0, cnt = D.cnt;
     const int ns = PART == EVAL_FAR ? 0 : D.rs[9];
     int G = 1;
-    while (2 * G * cnt <= TCH) G *= 2;
+    if (!D.multi)
+      while (2 * G * cnt <= TCH) G *= 2;
     const int t = threadIdx.x / G, sub = threadIdx.x % G;
     const bool valid = t < cnt;
     const double cx = D.cx, cy = D.cy;
@@ -1480,13 +1483,15 @@ void run_evaluate_sources_split_mixed(const PassArgs &a, const double *tau_s,
 void run_evaluate_mixed(const PassArgs &a, const double *tau_s, const double *tsum,
                         const float *loc32, const double *lsum, const double *txs,
                         const double *tys, const uint64_t *tkeys, const int *tperm, int64_t m,
-                        int check, int nout, double *out, int64_t ld_out, cudaStream_t s) {
+                        int check, int nout, double *out, int64_t ld_out, cudaStream_t s,
+                        const EvalItems *pre) {
   if (m == 0) return;
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
   const int total = th.n_total();
-  EvalItems it;
-  eval_items(a, tkeys, m, it, s);
+  EvalItems own;
+  if (!pre) eval_items(a, tkeys, m, own, s);
+  const EvalItems &it = pre ? *pre : own;
   DevBuf<EvalDesc> desc;
   desc.alloc(total + m / TCH + 1, s);
   DevBuf<int> next_item;

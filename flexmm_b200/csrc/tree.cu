@@ -916,6 +916,85 @@ void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th
                       fail, s);
 }
 
+// --- targets into leaves without a sort ---------------------------------------
+// Each point's key digits lead from the root down the tree to the first real
+// leaf (NF_LEAF, X-list leaves included): the leaf whose code is a prefix of
+// the key, the same leaf a lower-bound search of the sorted keys finds.  Its
+// slot inside the leaf is taken by an atomic count per leaf and warp (any
+// order).
+__global__ void k_bin_points(const double *__restrict__ x, const double *__restrict__ y, int64_t m,
+                             double x0, double y0, double w0, double scale, double margin, int L,
+                             const uint8_t *__restrict__ flags, const int *__restrict__ child,
+                             int *__restrict__ leaf_of, int *__restrict__ slot,
+                             int *__restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  unsigned lt;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+  // whole warps step together (the slot count below is per warp)
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); i0 < m; i0 += stride) {
+    const int64_t i = i0 + lane;
+    int g = -2;  // past m
+    if (i < m) {
+      const uint64_t key = point_key(__ldg(x + i), __ldg(y + i), x0, y0, w0, scale, margin);
+      g = 0;
+      for (int l = 0;; ++l) {
+        const uint8_t f = __ldg(flags + g);
+        if (f & NF_LEAF) break;
+        if (!(f & NF_CHILDREN) || l >= L - 1) {  // (never in a built tree)
+          g = -1;
+          break;
+        }
+        g = __ldg(child + g) + int((key >> (2 * (MAXD - 1 - l))) & 3u);
+      }
+    }
+    // one atomic per leaf met by the warp (neighbouring points share leaves)
+    const unsigned peers = __match_any_sync(0xffffffffu, g);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader && g >= 0) base = atomicAdd(count + g, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (i < m) {
+      leaf_of[i] = g;
+      slot[i] = g >= 0 ? base + __popc(peers & lt) : -1;
+    }
+  }
+}
+
+__global__ void k_scatter_binned(const double *__restrict__ x, const double *__restrict__ y,
+                                 int64_t m, const int *__restrict__ leaf_of,
+                                 const int *__restrict__ slot, const int *__restrict__ first,
+                                 double *__restrict__ xs, double *__restrict__ ys,
+                                 int *__restrict__ perm) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int g = leaf_of[i];
+    if (g < 0) continue;
+    const int pos = first[g] + slot[i];
+    xs[pos] = x[i];
+    ys[pos] = y[i];
+    perm[pos] = int(i);
+  }
+}
+
+void bin_points(const double *x, const double *y, int64_t m, const TreeDev &td, const TreeHost &th,
+                int *count, int *leaf_of, int *slot, cudaStream_t s) {
+  if (m <= 0) return;
+  double scale, margin;
+  key_params(th.x0, th.y0, th.w0, scale, margin);
+  k_bin_points<<<grid_for(m, TPB), TPB, 0, s>>>(x, y, m, th.x0, th.y0, th.w0, scale, margin, th.L,
+                                                td.flags.get(), td.child.get(), leaf_of, slot, count);
+  FMMB_CUDA(cudaGetLastError());
+}
+
+void scatter_binned(const double *x, const double *y, int64_t m, const int *leaf_of,
+                    const int *slot, const int *first, double *xs, double *ys, int *perm,
+                    cudaStream_t s) {
+  if (m <= 0) return;
+  k_scatter_binned<<<grid_for(m, TPB), TPB, 0, s>>>(x, y, m, leaf_of, slot, first, xs, ys, perm);
+  FMMB_CUDA(cudaGetLastError());
+}
+
 void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int64_t n, int ppl,
                 const double bbox[4], cudaStream_t s, int max_split) {
   FMMB_CHECK(n > 0, ERR_INVALID_ARGUMENT, "tree needs at least one point");

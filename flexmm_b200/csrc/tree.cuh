@@ -101,6 +101,17 @@ void sort_points(const double *x, const double *y, int64_t n, const TreeHost &th
 // The same into caller-provided memory: keys [n], perm [n], optional sx, sy
 // [n], and scratch of sort_points_scratch_bytes(n, sorted_digits) bytes.
 size_t sort_points_scratch_bytes(int64_t n, int sorted_digits);
+
+// Points into the tree's leaves without a sort: leaf_of[i] (the real leaf
+// holding point i, -1 for none) and slot[i] (its place among the leaf's
+// points, in no particular order); count[node] (zeroed by the caller) gets
+// the points per leaf.  scatter_binned then writes the points leaf by leaf
+// (first[node]: the exclusive scan of count) with perm (position -> point).
+void bin_points(const double *x, const double *y, int64_t m, const TreeDev &td, const TreeHost &th,
+                int *count, int *leaf_of, int *slot, cudaStream_t s);
+void scatter_binned(const double *x, const double *y, int64_t m, const int *leaf_of,
+                    const int *slot, const int *first, double *xs, double *ys, int *perm,
+                    cudaStream_t s);
 void sort_points_scratch(const double *x, const double *y, int64_t n, const TreeHost &th,
                          int sorted_digits, uint64_t *keys, int *perm, double *sx, double *sy,
                          void *scratch, size_t scratch_bytes, int *fail, cudaStream_t stream);
