@@ -14,7 +14,7 @@ N_OFFSETS = 40
 PRECISION = {"fp64": 0, "mixed": 1}
 EVALUATORS = {"potential": (0, 1), "gradient": (1, 3), "stokes": (2, 3)}   # id, outputs
 N_PHASES = 12
-PHASES = ["tree", "sort_targets", "upward", "m2l", "downward", "evaluate", "direct", "tree_splits",
+PHASES = ["tree", "targets", "upward", "m2l", "downward", "evaluate", "direct", "tree_splits",
           "tree_balance", "tree_nodes", "prep", "spare"]
 MAX_LEVELS = 30
 MAX_NEQUIV = 64

@@ -12,7 +12,7 @@ namespace fmmb {
 
 enum Phase : int {
   PH_TREE = 0,      // whole tree build (span, includes its two host waits)
-  PH_SORT_TGT = 1,  // target keys + sort + gather
+  PH_SORT_TGT = 1,  // targets into leaves: keys, binning (KIFMM) or sort (BB, Stokes), items
   PH_UPWARD = 2,    // k_upward launches (S2M + M2M + C2E)
   PH_M2L = 3,       // k_m2l launch
   PH_DOWNWARD = 4,  // k_downward launches (L2L + C2E)
