@@ -937,6 +937,20 @@ void upward_impl(const PassArgs &a, const double *tau_s, double *mult, cudaStrea
 
 }  // namespace
 
+// the tree's own sources: each leaf's range is its [bot, top) (the same
+// lower-bound searches of the same sorted keys, done by the node pass)
+__global__ void k_leaf_sources(int total, const uint8_t *__restrict__ flags,
+                               const int *__restrict__ bot, const int *__restrict__ top,
+                               int *__restrict__ tb, int *__restrict__ te, int *__restrict__ nchunk) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const bool leaf = flags[g] & NF_LEAF;
+    const int b = leaf ? bot[g] : 0, e = leaf ? top[g] : 0;
+    tb[g] = b;
+    te[g] = e;
+    nchunk[g] = (e - b + TCH - 1) / TCH;
+  }
+}
+
 void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &it, cudaStream_t s) {
   const TreeHost &th = *a.th;
   const TreeDev &td = *a.td;
@@ -945,9 +959,14 @@ void eval_items(const PassArgs &a, const uint64_t *tkeys, int64_t m, EvalItems &
   it.te.alloc(total, s);
   it.nch.alloc(total, s);
   it.choff.alloc(total, s);
-  k_leaf_targets<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), td.code.get(),
-                                                      td.flags.get(), tkeys, m, it.tb.get(),
-                                                      it.te.get(), it.nch.get());
+  if (tkeys == td.pkeys.get() && m == th.n_points)
+    k_leaf_sources<<<grid_for(total, 256), 256, 0, s>>>(total, td.flags.get(), td.bot.get(),
+                                                        td.top.get(), it.tb.get(), it.te.get(),
+                                                        it.nch.get());
+  else
+    k_leaf_targets<<<grid_for(total, 256), 256, 0, s>>>(total, th.L, td.dev_off.get(), td.code.get(),
+                                                        td.flags.get(), tkeys, m, it.tb.get(),
+                                                        it.te.get(), it.nch.get());
   FMMB_CUDA(cudaGetLastError());
   prefix_sum<int, false>(it.nch.get(), it.choff.get(), total, td.sort_fail.get(), true, s);
   it.items.alloc(total + m / TCH + 1, s);
