@@ -11,8 +11,8 @@ Same constructor, methods and results as flexmm/flexmm2d/kifmm.py:122-144
 Inputs may be numpy arrays (results come back as numpy) or torch tensors
 (results stay torch tensors on the GPU).  ``precision="mixed"`` selects the
 split-precision form (FP32 kernel evaluations, 3xTF32 tensor-core far-field
-GEMMs, FP64 check-to-equivalent); the default ``"fp64"`` matches the
-reference to 1e-12.  All work runs on the current CUDA
+GEMMs, FP64 check-to-equivalent; Laplace, and the modified Helmholtz
+potential); the default ``"fp64"`` matches the reference to 1e-12.  All work runs on the current CUDA
 device and torch's current stream, through ``libflexmm_b200.so``; there is
 no CPU path.
 """

@@ -292,7 +292,8 @@ int fmm_direct(int kernel_id, const double *kernel_params, const double *sx, con
  * verbose mode (flexmm/flexmm2d/fmm.py:24-30, 55-58, 106-107, 148-149).
  * fmm_timing_read returns, per phase, the summed milliseconds and the number
  * of timed launches since the last read, then clears them.  Phases:
- * 0 tree build (span), 1 target sort, 2 upward, 3 M2L, 4 downward,
+ * 0 tree build (span), 1 targets into leaves (binning for KIFMM plans, a
+ * sort for black-box and Stokes plans, and the work items), 2 upward, 3 M2L, 4 downward,
  * 5 evaluation (L2T + P2P), 6 direct sum, 7-9 the tree build's three
  * stages (keys/sort/initial splits, 2:1 closure and X-list, node arrays),
  * 10 expansion set-up (charge gather, buffers, charge sums). */
