@@ -387,3 +387,42 @@ def test_pinned_host_charges_equal_device_charges(built_lib, precision):
     ref = run(tau_h.cuda())
     for _ in range(3):
         assert torch.equal(run(tau_h), ref)
+
+
+def test_binned_targets_match_sorted_targets(built_lib):
+    """Targets are binned into their leaves (a descent along each key's
+    digits) by fmm_evaluate and sorted by fmm_evaluate_noalloc: every target
+    must land in the same leaf, so the two agree point by point to rounding --
+    including targets exactly on dyadic split lines, outside the bbox, and
+    at the sources themselves.  A target in another leaf would differ at the
+    FMM's truncation level (~1e-8 here)."""
+    import ctypes
+    import torch
+    from flexmm_b200 import KI_FMM, KI_Helper, _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(23)
+    x, y = rng.uniform(-1, 1, 50_000), rng.uniform(-1, 1, 50_000)
+    F = KI_FMM(x, y, "Laplace_Eval", 32, 24, bbox=[-1, 1, -1, 1], helper=KI_Helper())
+    F.build_expansions(rng.standard_normal(50_000))
+    g = -1 + np.arange(65) / 32.0                      # split lines of levels <= 5
+    gx, gy = np.meshgrid(g, g)
+    ox, oy = rng.uniform(-1.5, 1.5, 8000), rng.uniform(-1.5, 1.5, 8000)
+    out = (np.abs(ox) > 1) | (np.abs(oy) > 1)
+    cases = [(np.concatenate([gx.ravel(), rng.uniform(-1, 1, 20_000), ox[out]]),
+              np.concatenate([gy.ravel(), rng.uniform(-1, 1, 20_000), oy[out]]), 0),
+             (x[:20_000], y[:20_000], 1)]
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for tx, ty, check in cases:
+        txd, tyd = torch.from_numpy(tx).cuda(), torch.from_numpy(ty).cuda()
+        res = []
+        for fn in ("fmm_evaluate", "fmm_evaluate_noalloc"):
+            o = torch.full_like(txd, float("nan"))
+            rc = getattr(lib, fn)(F._plan, ctypes.c_void_p(txd.data_ptr()), ctypes.c_void_p(tyd.data_ptr()),
+                                  txd.numel(), check, ctypes.c_void_p(o.data_ptr()), stream)
+            assert rc == 0, lib.fmm_last_error()
+            torch.cuda.synchronize()
+            res.append(o.cpu().numpy())
+        binned, sorted_ = res
+        assert np.isfinite(binned).all()
+        scale = np.sqrt(np.mean(sorted_ ** 2))
+        assert np.max(np.abs(binned - sorted_)) < 1e-12 * scale
