@@ -36,6 +36,7 @@ constexpr int TN = 32;      // nodes per upward / downward tile
 constexpr int TM = 64;      // targets per M2L tile
 constexpr int NT = 256;     // threads per tile CTA
 constexpr int TCH = 128;    // targets per evaluation work item (= threads)
+static_assert(TCH == EVAL_CHUNK, "work items (built in fmm.cu) hold EVAL_CHUNK targets");
 constexpr int SMAX = 1024;  // sources staged per evaluation pass
 constexpr int EVAL_BLOCKS_PER_SM = 12;  // 40 registers, 17 KB shared memory per block
 
