@@ -129,9 +129,13 @@ struct SplitEval {
 };
 // near-field blocks per SM, leaving room for the level passes: FP64 (28 KB of
 // shared memory each) beside the DMMA M2L tiles; mixed (17 KB each) beside
-// one persistent tcgen05 M2L CTA (154 KB at Nequiv 24)
+// the upward pass until the M2L (which it leaves to the persistent tcgen05
+// CTAs), then beside the downward pass.  Mixed, measured at 1M (step ms,
+// two runs each, one box): before / after the M2L 3/10 1.277-1.281, 2/10
+// 1.282-1.286, 6/10 1.253-1.262, 8/10 1.245-1.247, 12/10 1.287, 6/8
+// 1.247-1.249, 6/12 1.273-1.277.
 constexpr int NEAR_BLOCKS_PER_SM = 4;
-constexpr int NEAR_BLOCKS_PER_SM_MIXED = 3;
+constexpr int NEAR_BLOCKS_PER_SM_MIXED = 8;
 constexpr int NEAR_BLOCKS_PER_SM_MIXED_RESUME = 10;  // after the M2L, beside the downward pass
 void run_evaluate_sources_split(const PassArgs &a, const double *tau_sorted, const double *loc,
                                 int check, double *out, cudaStream_t s, const SplitEval &se);
