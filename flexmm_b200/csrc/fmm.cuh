@@ -133,8 +133,9 @@ struct SplitEval {
 // CTAs), then beside the downward pass.  Mixed, measured at 1M (step ms,
 // two runs each, one box): before / after the M2L 3/10 1.277-1.281, 2/10
 // 1.282-1.286, 6/10 1.253-1.262, 8/10 1.245-1.247, 12/10 1.287, 6/8
-// 1.247-1.249, 6/12 1.273-1.277.
-constexpr int NEAR_BLOCKS_PER_SM = 4;
+// 1.247-1.249, 6/12 1.273-1.277.  FP64 (step ms, same way): 2 5.10, 3 3.86,
+// 4 3.350-3.351, 6 3.194, 8 3.197-3.204.
+constexpr int NEAR_BLOCKS_PER_SM = 6;
 constexpr int NEAR_BLOCKS_PER_SM_MIXED = 8;
 constexpr int NEAR_BLOCKS_PER_SM_MIXED_RESUME = 10;  // after the M2L, beside the downward pass
 void run_evaluate_sources_split(const PassArgs &a, const double *tau_sorted, const double *loc,
