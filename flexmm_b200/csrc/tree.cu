@@ -61,8 +61,10 @@ struct Counters {
 
 // The source keys are first sorted on their top SORT_DIGITS digits only; that
 // fixes every box of levels <= SORT_DIGITS.  A tree that would split a box of
-// level >= SORT_DIGITS is redone with a full sort.
-constexpr int SORT_DIGITS = 16;
+// level >= SORT_DIGITS is redone with a full sort.  12 digits are 24 bits of
+// the 32-bit sort keys: three radix passes (16 digits took four), enough for
+// trees up to 14 levels (the 1M clustered headline tree has 13).
+constexpr int SORT_DIGITS = 12;
 
 __device__ __forceinline__ int common_digits(uint64_t a, uint64_t b) {
   uint64_t d = a ^ b;
