@@ -65,6 +65,9 @@ struct RadixWork {
   int *ghist;        // [passes][256], zero before the launch (follows sync)
   unsigned *status;  // [passes][tiles][256]
   int *fail;         // optional: set to 1 when a wait ran out
+  // optional: the element count in device memory (written by an earlier
+  // kernel), at most the launch's n, which then only sizes grid and scratch
+  const unsigned long long *n_dev;
 };
 
 __host__ __device__ inline int64_t radix_tiles(int64_t n) { return (n + RS_TILE - 1) / RS_TILE; }
@@ -167,7 +170,8 @@ __global__ void __launch_bounds__(RS_THREADS, 2)
   extern __shared__ __align__(16) unsigned char rs_stage[];  // the tile in sorted order
   K *sk = reinterpret_cast<K *>(rs_stage);
   int *sv = reinterpret_cast<int *>(rs_stage + RS_TILE * sizeof(K));
-  const int n = (int)n64;  // < 2^30 (checked by the host): element indices fit in int
+  // < 2^30 (checked by the host): element indices fit in int
+  const int n = w.n_dev ? (int)min((unsigned long long)n64, __ldcg(w.n_dev)) : (int)n64;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned lt;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
@@ -389,7 +393,8 @@ size_t radix_scratch_bytes(int64_t n, int passes) {
 // radix_scratch_bytes<K, VALS>(n, passes) bytes on g = radix_grid(...) blocks.
 template <class K, bool VALS, class Src, class Emit>
 void radix_sort_run(const Src &src, const Emit &emit, int64_t n, int begin_bit, int end_bit,
-                    void *scratch, size_t bytes, int g, int *fail, cudaStream_t s) {
+                    void *scratch, size_t bytes, int g, int *fail, cudaStream_t s,
+                    const unsigned long long *n_dev = nullptr) {
   if (n <= 0) return;
   FMMB_CHECK(end_bit > begin_bit && end_bit <= int(8 * sizeof(K)) && n < (int64_t(1) << 30),
              ERR_INVALID_ARGUMENT, "radix sort: bad bit range or more than 2^30 elements");
@@ -413,6 +418,7 @@ void radix_sort_run(const Src &src, const Emit &emit, int64_t n, int begin_bit, 
   w.ghist = reinterpret_cast<int *>(at + sizeof(RadixSync));
   w.status = reinterpret_cast<unsigned *>(at + sizeof(RadixSync) + sizeof(int) * 256 * passes);
   w.fail = fail;
+  w.n_dev = n_dev;
   FMMB_CUDA(cudaMemsetAsync(w.sync, 0, sizeof(RadixSync) + sizeof(int) * 256 * passes, s));
   auto kern = k_radix_sort<K, Src, Emit, VALS>;
   void *args[] = {(void *)&src, (void *)&emit, (void *)&n, (void *)&begin_bit, (void *)&end_bit,
@@ -427,13 +433,13 @@ void radix_sort_run(const Src &src, const Emit &emit, int64_t n, int begin_bit, 
 // The same with scratch from the stream-ordered pool.
 template <class K, bool VALS, class Src, class Emit>
 void radix_sort(const Src &src, const Emit &emit, int64_t n, int begin_bit, int end_bit, int *fail,
-                cudaStream_t s) {
+                cudaStream_t s, const unsigned long long *n_dev = nullptr) {
   if (n <= 0) return;
   const int g = radix_grid<K, VALS>(k_radix_sort<K, Src, Emit, VALS>, n);
   const size_t bytes = radix_scratch_bytes<K, VALS>(n, (end_bit - begin_bit + 7) / 8);
   DevBuf<unsigned char> tmp;
   tmp.alloc(bytes, s);
-  radix_sort_run<K, VALS>(src, emit, n, begin_bit, end_bit, tmp.get(), bytes, g, fail, s);
+  radix_sort_run<K, VALS>(src, emit, n, begin_bit, end_bit, tmp.get(), bytes, g, fail, s, n_dev);
 }
 
 }  // namespace

@@ -301,9 +301,21 @@ __global__ void k_split_emit(const uint64_t *__restrict__ keys, int64_t n, int p
   }
 }
 
-// bounds[l] = first index of a code of level >= l, l = 0..L (codes sorted by level)
-__global__ void k_level_starts(const uint64_t *__restrict__ codes, int64_t n, int L,
-                               int *__restrict__ bounds) {
+// split-box count and level count of a tree from its split counters
+// (n0 = 0: the root alone, one level)
+__device__ __forceinline__ int64_t split_boxes(const Counters *split, unsigned long long cap) {
+  return (int64_t)min(__ldcg(&split->s0_count), cap);
+}
+__device__ __forceinline__ int split_levels(const Counters *split, int64_t n0) {
+  return n0 > 0 ? __ldcg(&split->max_level) + 2 : 1;
+}
+
+// bounds[l] = first index of a code of level >= l, l = 0..L + 1 (codes sorted
+// by level; n and the tree's L from its split counters, bounds [MAXD + 3])
+__global__ void k_level_starts(const uint64_t *__restrict__ codes, const Counters *split,
+                               unsigned long long cap, int *__restrict__ bounds) {
+  const int64_t n = split_boxes(split, cap);
+  const int L = split_levels(split, n) + 1;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int lv = min(code_level(codes[i]), L + 1);
@@ -359,12 +371,16 @@ __device__ bool grid_sync(Counters *cnt, unsigned long long *snap) {
 //    split box.
 // Boxes written by other blocks are read through L2 (__ldcg).
 __global__ void __launch_bounds__(TPB) k_balance_xlist(
-    int mtop, int L, const uint64_t *__restrict__ s0, int64_t n0, const int *__restrict__ s0b,
+    const uint64_t *__restrict__ s0, const int *__restrict__ s0b,
     uint64_t *forced, unsigned long long *fb, unsigned long long capf, uint64_t *xl,
     unsigned long long capx, uint64_t *tab, uint64_t mask, Counters *cnt,
-    const int *sort_fail) {
+    const int *sort_fail, const Counters *split, unsigned long long cap0) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+  // the split boxes' count and the tree's levels, from the split pass's
+  // counters (the host has not read them: it waits once, after this kernel)
+  const int64_t n0 = split_boxes(split, cap0);
+  const int L = split_levels(split, n0), mtop = L - 3;
   if (tid == 0) cnt->sort_fail = __ldcg(sort_fail);  // the split-box sort ran before
   for (int64_t i = tid; i < n0; i += nthr)
     if (hash_insert(tab, mask, s0[i]) < 0) atomicExch(&cnt->overflow, 1);
@@ -744,9 +760,9 @@ uint64_t next_pow2(uint64_t v) {
 // stable sort of keys on bits [begin_bit, end_bit)
 template <class K>
 void sort_keys(const K *kin, K *kout, int64_t n, int begin_bit, int end_bit, int *fail,
-               cudaStream_t s) {
+               cudaStream_t s, const unsigned long long *n_dev = nullptr) {
   radix_sort<K, false>(SrcKeys<K>{kin, nullptr}, EmitPairs<K>{kout, nullptr}, n, begin_bit, end_bit,
-                       fail, s);
+                       fail, s, n_dev);
 }
 
 template <class T>
@@ -1009,24 +1025,67 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   th.w0 = bbox[1] - bbox[0];
   FMMB_CHECK(th.w0 > 0, ERR_INVALID_ARGUMENT, "bbox has non-positive width");
 
+  // counters: [0] the split pass's (box count, deepest level, flags), [1] the
+  // balance kernel's; both come back through a pinned block in one copy, at
+  // the tree build's one host wait (after the balance kernel: the level sort
+  // and the balance kernel read the split counts on the device)
   DevBuf<Counters> cnt;
-  cnt.alloc(1, s);
-  // the counters come back through a pinned block: one copy per host wait
-  static_assert(sizeof(Counters) <= PINNED_INTS * sizeof(int), "pinned block too small");
+  cnt.alloc(2, s);
+  Counters *csplit = cnt.get(), *cbal = cnt.get() + 1;
+  static_assert(2 * sizeof(Counters) <= PINNED_INTS * sizeof(int), "pinned block too small");
   std::unique_ptr<int, void (*)(int *)> hblk(pinned_acquire(), pinned_release);
-  Counters &hc = *reinterpret_cast<Counters *>(hblk.get());
+  Counters *hcs = reinterpret_cast<Counters *>(hblk.get());
+  const Counters &hc = hcs[0], &hb = hcs[1];
   auto read_counters = [&] {
-    FMMB_CUDA(cudaMemcpyAsync(&hc, cnt.get(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaMemcpyAsync(hcs, cnt.get(), 2 * sizeof(Counters), cudaMemcpyDeviceToHost, s));
     FMMB_CUDA(cudaStreamSynchronize(s));
   };
   const unsigned long long cap0 = (unsigned long long)MAXD * (n / (ppl + 1) + 1) + 64;
   DevBuf<uint64_t> s0raw, s0;
   DevBuf<unsigned long long> scount, spos;
   s0raw.alloc(cap0, s);
+  s0.alloc(cap0, s);
   scount.alloc(n, s);
   spos.alloc(n, s);
-  // 1-3: keys, sort (top digits first), initial splits in point order
+  DevBuf<int> s0b;            // split boxes' level starts
+  s0b.alloc(MAXD + 3, s);
+  // balance buffers: first sized from an estimate of the split-box count
+  // (the true one is known only after the wait); an overflow is retried
+  // with capacities from the true count
+  const unsigned long long n0_est = 2ull * (unsigned long long)(n / (ppl + 1)) + 64;
+  unsigned long long capf = 8ull * n0_est + 4096, capx = 8ull * n0_est + 4096;
+  DevBuf<uint64_t> tab, forced, xl;
+  DevBuf<unsigned long long> fb;
+  uint64_t hcap = 0;
+  auto launch_balance = [&] {
+    hcap = next_pow2(2 * (n0_est + capf + capx));
+    tab.alloc(hcap, s);
+    FMMB_CUDA(cudaMemsetAsync(tab.get(), 0xff, hcap * sizeof(uint64_t), s));
+    forced.alloc(capf, s);
+    xl.alloc(capx, s);
+    fb.alloc(MAXD + 2, s);
+    fb.zero(s);
+    FMMB_CUDA(cudaMemsetAsync(cbal, 0, sizeof(Counters), s));
+    const uint64_t *s0p = s0.get();
+    const int *s0bp = s0b.get();
+    uint64_t *fp = forced.get(), *xp = xl.get(), *tp = tab.get();
+    unsigned long long *fbp = fb.get();
+    uint64_t mask = hcap - 1;
+    Counters *cp = cbal;
+    const Counters *sp = csplit;
+    const int *sfp = td.sort_fail.get();
+    unsigned long long c0 = cap0;
+    void *args[] = {&s0p, &s0bp, &fp, &fbp, &capf, &xp, &capx, &tp, &mask, &cp, &sfp, &sp, &c0};
+    FMMB_CUDA(cudaLaunchCooperativeKernel((const void *)k_balance_xlist,
+                                          cooperative_grid((const void *)k_balance_xlist, TPB), TPB,
+                                          args, 0, s));
+  };
+  // 1-5: keys, sort (top digits first), initial splits in point order, the
+  // split boxes by (level, morton) -- a stable sort on the level bits keeps
+  // the morton order every level already has -- and the balance closure
+  // with the X-list in one cooperative launch over a hash set
   std::unique_ptr<PhaseTimer> t_split(new PhaseTimer(PH_TREE_SPLITS, s));
+  std::unique_ptr<PhaseTimer> t_bal;
   td.sx.alloc(n, s);
   td.sy.alloc(n, s);
   td.sort_fail.alloc(1, s);
@@ -1034,27 +1093,34 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   for (int digits = SORT_DIGITS;; digits = MAXD) {
     sort_points(x, y, n, th, td.pkeys, td.ordv, s, digits, td.sx.get(), td.sy.get(),
                 td.sort_fail.get());
-    cnt.zero(s);
+    FMMB_CUDA(cudaMemsetAsync(csplit, 0, sizeof(Counters), s));
     k_split_counts<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, digits, scount.get(),
-                                                     cnt.get(), max_split);
+                                                     csplit, max_split);
     FMMB_CUDA(cudaGetLastError());
     // (k_split_emit checks its writes against the capacity)
     exclusive_sum(scount.get(), spos.get(), n, td.sort_fail.get(), false, s);
     k_split_emit<<<grid_for(n, TPB), TPB, 0, s>>>(td.pkeys.get(), n, ppl, scount.get(), spos.get(),
-                                                   s0raw.get(), cap0, cnt.get(), max_split,
+                                                   s0raw.get(), cap0, csplit, max_split,
                                                    td.sort_fail.get());
     FMMB_CUDA(cudaGetLastError());
+    t_split.reset();
+    t_bal.reset(new PhaseTimer(PH_TREE_BALANCE, s));
+    sort_keys(s0raw.get(), s0.get(), (int64_t)cap0, LEVEL_SHIFT, LEVEL_SHIFT + 5,
+              td.sort_fail.get(), s, &csplit->s0_count);
+    k_level_starts<<<grid_for((int64_t)cap0, TPB), TPB, 0, s>>>(s0.get(), csplit, cap0, s0b.get());
+    FMMB_CUDA(cudaGetLastError());
+    launch_balance();
     read_counters();
     FMMB_CHECK(!hc.sort_fail, ERR_CUDA, "point sort: a grid barrier wait ran out of time");
     FMMB_CHECK(!hc.too_deep, ERR_TREE_TOO_DEEP,
                "more than Ncutoff points share a box of width bbox/2^29 (coincident points?)");
     FMMB_CHECK(!hc.overflow, ERR_CAPACITY, "initial split buffer overflow");
     if (!hc.need_full_sort || digits == MAXD) break;
+    t_bal.reset();
+    t_split.reset(new PhaseTimer(PH_TREE_SPLITS, s));
   }
   scount.release();
   spos.release();
-  t_split.reset();
-  std::unique_ptr<PhaseTimer> t_bal(new PhaseTimer(PH_TREE_BALANCE, s));
   const int64_t n0 = (int64_t)hc.s0_count;
   const int L = (n0 > 0) ? hc.max_level + 2 : 1;
   th.L = L;
@@ -1063,64 +1129,25 @@ void build_tree(TreeDev &td, TreeHost &th, const double *x, const double *y, int
   DevBuf<uint8_t> pxs;
   DevBuf<int> pb, preal, ppos;
   int64_t np = 0;
+  const int mb = 2 * (L - 2);  // morton bits of the deepest parent level
   if (n0 > 0) {
-    // split boxes by (level, morton): a stable sort on the level bits keeps
-    // the morton order every level already has
-    s0.alloc(n0, s);
-    sort_keys(s0raw.get(), s0.get(), n0, LEVEL_SHIFT, LEVEL_SHIFT + 5, td.sort_fail.get(), s);
-    DevBuf<int> s0b;
-    s0b.alloc(L + 2, s);
-    k_level_starts<<<grid_for(n0, TPB), TPB, 0, s>>>(s0.get(), n0, L + 1, s0b.get());
-    FMMB_CUDA(cudaGetLastError());
-
-    // 4-5: balance closure and X-list in one cooperative launch over a hash
-    // set; capacities grow on overflow
-    const int mb = 2 * (L - 2);  // morton bits of the deepest parent level
-    unsigned long long capf = 8ull * n0 + 4096, capx = 8ull * n0 + 4096;
     for (int attempt = 0;; ++attempt) {
-      const uint64_t hcap = next_pow2(2 * (n0 + capf + capx));
-      DevBuf<uint64_t> tab, forced, xl;
-      DevBuf<unsigned long long> fb;
-      tab.alloc(hcap, s);
-      FMMB_CUDA(cudaMemsetAsync(tab.get(), 0xff, hcap * sizeof(uint64_t), s));
-      forced.alloc(capf, s);
-      xl.alloc(capx, s);
-      fb.alloc(L + 1, s);
-      fb.zero(s);
-      FMMB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(Counters), s));
-      {
-        int mtop = L - 3, Lk = L;
-        const uint64_t *s0p = s0.get();
-        const int *s0bp = s0b.get();
-        uint64_t *fp = forced.get(), *xp = xl.get(), *tp = tab.get();
-        unsigned long long *fbp = fb.get();
-        uint64_t mask = hcap - 1;
-        Counters *cp = cnt.get();
-        int64_t n0k = n0;
-        const int *sfp = td.sort_fail.get();
-        void *args[] = {&mtop, &Lk, &s0p, &n0k, &s0bp, &fp, &fbp, &capf, &xp, &capx, &tp, &mask, &cp,
-                        &sfp};
-        FMMB_CUDA(cudaLaunchCooperativeKernel((const void *)k_balance_xlist,
-                                              cooperative_grid((const void *)k_balance_xlist, TPB),
-                                              TPB, args, 0, s));
-      }
+      FMMB_CHECK(!hb.bar_timeout, ERR_CUDA, "tree balance: a grid barrier wait ran out of time");
+      FMMB_CHECK(!hb.sort_fail, ERR_CUDA, "split-box sort: a grid barrier wait ran out of time");
+      if (!hb.overflow) break;
+      // capacities grow on overflow (from the true split-box count now)
+      FMMB_CHECK(attempt < 6, ERR_CAPACITY, "tree balance buffers overflow");
+      capf = std::max(4 * capf, 8ull * n0 + 4096);
+      capx = std::max(4 * capx, 8ull * n0 + 4096);
+      launch_balance();
       read_counters();
-      FMMB_CHECK(!hc.bar_timeout, ERR_CUDA, "tree balance: a grid barrier wait ran out of time");
-      FMMB_CHECK(!hc.sort_fail, ERR_CUDA, "split-box sort: a grid barrier wait ran out of time");
-      if (hc.overflow) {
-        FMMB_CHECK(attempt < 6, ERR_CAPACITY, "tree balance buffers overflow");
-        capf = 4 * capf;
-        capx = 4 * capx;
-        continue;
-      }
-      const int64_t nf = (int64_t)hc.f_count, nx = (int64_t)hc.x_count;
-      np = n0 + nf + nx;
-      pk.alloc(np, s);
-      k_parent_keys<<<grid_for(np, TPB), TPB, 0, s>>>(s0.get(), n0, forced.get(), nf, xl.get(), nx,
-                                                       mb, pk.get());
-      FMMB_CUDA(cudaGetLastError());
-      break;
     }
+    const int64_t nf = (int64_t)hb.f_count, nx = (int64_t)hb.x_count;
+    np = n0 + nf + nx;
+    pk.alloc(np, s);
+    k_parent_keys<<<grid_for(np, TPB), TPB, 0, s>>>(s0.get(), n0, forced.get(), nf, xl.get(), nx,
+                                                     mb, pk.get());
+    FMMB_CUDA(cudaGetLastError());
     // 6: sorted parent boxes, per-level bounds, real sibling groups
     t_bal.reset();
     pkc.alloc(np, s);
